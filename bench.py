@@ -1,0 +1,333 @@
+"""Throughput of the DEM step on the silo-discharge workload (1,000,000
+polydisperse spheres), reported as particle-steps/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl blaze|reference]
+
+One process per GPU (torchrun for N > 1).  The DEM step does not shard: each
+rank runs an independent replica of the workload (weak scaling, no
+data-path collective); the barrier and the max-over-ranks time reduction use
+the process group only.
+
+Workload: the silo discharge configuration in its reference-law form (the
+form the reference's own code can run): cylinder r = 25 cm over a 30 degree
+conical hopper of 42 planar faces to a 6 cm outlet, 1,000,000 spheres with
+radius uniform in [0.2, 0.4] cm quantised to 6 particle objects, density
+2600 kg/m^3, linear spring-dashpot kn = 1e5 kg/s^2, restitution 0.6,
+mu 0.5, dt = 5e-6 s, FP32; synthetic seeded packing (no dataset exists).
+
+Timed region (value): K steps enqueued through the handle API on device-
+resident state, bracketed by CUDA events on the library's stream.
+e2e: the same K steps through the reference-facing C ABI with host
+buffers: every step uploads the full particle state from pinned host memory
+(Device_Set_System_State), runs Device_DEM_UpdateSim and reads the state
+back (Device_Get_System_State).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "softx-d-15-00085_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "particle-steps/s at 1M spheres"
+UNIT = "particle-steps/s"
+B_ALG = 96  # bytes per particle-step of the fused step: 3 float4 streams read + written
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="blaze", choices=["blaze", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--skin", type=float, default=0.04, help="Verlet skin, cm (0 = reference mode)")
+    ap.add_argument("--max-nbr", type=int, default=32)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(root, n):
+    from blaze import synth
+    return synth.silo_project(root, n=n)
+
+
+def config(args):
+    return {"workload": "silo_discharge_reference_law", "particles": args.n,
+            "radius_cm": [0.2, 0.4], "radius_bins": 6, "hopper_faces": 42,
+            "law": "linear spring-dashpot kn=1e5 e=0.6 mu=0.5", "dt_s": 5e-6,
+            "skin_cm": args.skin, "max_nbr": args.max_nbr,
+            "l2": "inputs larger than L2 (state 3x48 MB + neighbour slots %d MB per step)"
+                  % (args.n * args.max_nbr * 4 // 1000000),
+            "parallelism": "replicas", "global_particles": args.n * args.gpus}
+
+
+def peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the fused step kernel from the committed ncu
+    summary (profiles/k_step_silo.md, line 'traffic_bytes_per_launch: X'
+    with the particle count it was measured at), scaled to this N."""
+    path = os.path.join(REPO, "profiles", "k_step_silo.md")
+    try:
+        vals = {}
+        for line in open(path):
+            if ":" in line:
+                k, v = line.split(":", 1)
+                vals[k.strip().strip("-* ")] = v.strip()
+        return float(vals["traffic_bytes_per_launch"]), int(vals["particles"])
+    except Exception:
+        return None, None
+
+
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(P, st, seconds, max_steps=None):
+    """The reference's own kernels compiled as host C++ (oracle/_ref), all
+    host threads, reference mode, on this workload: particle-steps/s."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from bindings import RefHost, ref_available
+    if not ref_available():
+        return None
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    R = RefHost().init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=threads,
+                       capture=False)
+    R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    R.step(1)  # first step outside the clock (page-in)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        R.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or (max_steps and steps >= max_steps):
+            break
+    return {"value": P.num_particles * steps / el, "unit": UNIT, "cores": threads,
+            "kind": "reference",
+            "sample": "%d full steps of the %d-particle workload (%.1f s), reference mode"
+                      % (steps, P.num_particles, el)}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    with tempfile.TemporaryDirectory() as d:
+        P, st = make_workload(d, args.n)
+        budget = max(10.0, min(150.0, 0.5 * (args.steps + args.warmup)))
+        cb = cpu_reference_rate(P, st, budget, max_steps=args.steps)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libblaze_refhost.so not built (reference tree absent at build)"}))
+        return 0
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config(args), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    from blaze import device
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    tmp = tempfile.TemporaryDirectory()
+    P, st = make_workload(tmp.name, args.n)
+    n = P.num_particles
+
+    sim = device.Simulation(P, skin=args.skin, max_nbr=args.max_nbr)
+    sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    sim.step(args.warmup)
+    status = sim.sync()
+    stream = torch.cuda.ExternalStream(sim.device_state()[3])
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    phys = vis.split(",")[local] if vis else str(local)
+    sampler = ClockSampler(phys)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    rb0 = sim.num_rebuilds()
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    launches = sim.last_launches()
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    rebuilds = sim.num_rebuilds() - rb0
+    status |= sim.sync()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = n * world * args.steps / (ms * 1e-3)
+
+    # per-kernel timing for the roofline (separate pass, same workload)
+    sim.set_profile(True)
+    sim.step(min(args.steps, 200))
+    ms_rebuild, ms_step, nsteps = sim.profile()
+    sim.set_profile(False)
+    t_step = ms_step / max(nsteps, 1) * 1e-3
+    peak, peak_kind = peak_hbm()
+    achieved = n * B_ALG / t_step / 1e9
+    traffic, traffic_n = ncu_traffic()
+    if traffic is not None and traffic_n:
+        traffic = traffic * n / traffic_n
+
+    # reference mode (rebuild every step) for context
+    sim.set_options(skin=0.0)
+    sim.step(3)
+    sim.sync()
+    r0 = torch.cuda.Event(enable_timing=True)
+    r1 = torch.cuda.Event(enable_timing=True)
+    kref = min(args.steps, 100)
+    r0.record(stream)
+    sim.step(kref)
+    r1.record(stream)
+    r1.synchronize()
+    ref_mode_value = n * kref / (r0.elapsed_time(r1) * 1e-3)
+    sim.close()
+
+    # end to end through the reference-facing C ABI with host buffers
+    lib = device.load()
+    kd = device.KDevice(P.wobj, P.pobj, P.dobj, P.n_w, P.n_p, P.n_d, P.sim_info, P.init)
+    hp = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+    hv = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+    hw = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+    ht = torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    hi = torch.empty(n, dtype=torch.int32).pin_memory().numpy()
+    hp[:] = st["pos"]; hv[:] = st["vel"]; hw[:] = st["avel"]; ht[:] = st["type"]; hi[:] = st["pid"]
+    kd.IDevice_Set_ParticleSystem_State(hp, None, hv, hw, None, ht, hi)
+    kd.IDevice_DEM_UpdateSim()
+    kd.IDevice_Get_System_State(hp, None, hv, hw, None, ht, hi)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        kd.IDevice_Set_ParticleSystem_State(hp, None, hv, hw, None, ht, hi)
+        kd.IDevice_DEM_UpdateSim()
+        kd.IDevice_Get_System_State(hp, None, hv, hw, None, ht, hi)
+    el = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([el], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    kd.clean()
+    e2e_value = n * world * args.e2e_steps / el
+    state_bytes = n * (12 + 12 + 12 + 4 + 4)
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_rate(P, st, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(args),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
+                    "path": "Device_Set_System_State + Device_DEM_UpdateSim + "
+                            "Device_Get_System_State per step, pinned host buffers"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_step (fused contact + walls + integration)",
+                         "peak_source": peak_kind,
+                         "bytes_per_launch": n * B_ALG, "launch_ms": t_step * 1e3},
+            "cpu_baseline": cb,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "rebuilds_in_timed_region": rebuilds,
+            "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
+            "reference_mode_value": ref_mode_value,
+            "status": device.decode_status(status),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    tmp.cleanup()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

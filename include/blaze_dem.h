@@ -1,0 +1,142 @@
+/*
+ * blaze_dem.h -- C ABI of the B200 DEM step library (libblaze_b200.so).
+ *
+ * Part 1 mirrors the reference's simulation-step interface
+ * (V_02_2015/src/Device/DeviceInterface.h:16-95) name for name, so the
+ * reference's KDevice wrapper (V_02_2015/src/Interface/KDevice.h:17-99) and
+ * its callers compile against this header unchanged.  Differences in the
+ * contract, all deliberate:
+ *   - C linkage and an int status instead of void + exit(1):
+ *       0  ok
+ *       >0 StatusBits raised by the kernels since the last call that
+ *          synchronised (1 list overflow, 2 particle outside the grid,
+ *          4 non-finite state, 8 particle type outside the table,
+ *          16 bounded device wait gave up)
+ *       <0 -(1000 + cudaError_t) for a CUDA error, -1 bad argument,
+ *          -2 no simulation set up
+ *   - Device_DEM_UpdateSim only enqueues the step on the library's stream;
+ *     every Get/Set call orders after it, so callers observe the reference's
+ *     synchronous semantics.  Option sync_each_step=1 makes every step block.
+ *   - Removed particles are counted per check (the reference's Kill_count is
+ *     never reset, DeviceInterface.cu:2494).
+ * One simulation per process through Part 1, as in the reference.
+ *
+ * Part 2 (blaze_*) is additive: handles for several independent
+ * simulations, options (neighbour-list skin and capacity, wall culling,
+ * CUDA-graph stepping), device-resident state access and parity hooks.
+ */
+#ifndef BLAZE_DEM_H_
+#define BLAZE_DEM_H_
+
+#include "blaze_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- Part 1 */
+
+/* DeviceInterface.h:16-20 / DeviceInterface.cu:1499 */
+int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_DynamicOBJ,
+                              SimulationInfo* h_SimInfo, int h_Num_WorldOBJ,
+                              int h_Num_ParticleOBJ, int h_Num_DynamicOBJ,
+                              InitConfig* h_PosConfig);
+/* DeviceInterface.h:23-24 / DeviceInterface.cu:1116 (SpecType 1) */
+int Device_Set_Pos(float3* h_pos, Quaterion* h_Ornt, uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:27-29 / DeviceInterface.cu:1209 (SpecType 2) */
+int Device_Set_Pos_Velocity(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:32-35 / DeviceInterface.cu:1307 (SpecType 3/4; h_acc ignored, as there) */
+int Device_Set_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            float3* h_acc, uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:38 / DeviceInterface.cu:1429 */
+int Device_Set_Tallys(float* h_Tallys);
+/* DeviceInterface.h:44-49 / DeviceInterface.cu:2613 */
+int Device_Get_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            float3* h_acc, uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:52-53 / DeviceInterface.cu:2524 */
+int Device_Get_P_Positions(float3* Pos, Quaterion* Quart_ornt, uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:56-57 / DeviceInterface.cu:2692 */
+int Device_Get_P_Velocity(float3* H_Vel, float3* H_Rvel, int Flag, uint* h_ptype, int* h_pid);
+/* DeviceInterface.h:63 / DeviceInterface.cu:2769: wall force of the last step */
+int Device_Get_W_Forces(float3* WallForces, float3* WallContact_Point);
+/* DeviceInterface.h:65 / DeviceInterface.cu:2795 */
+int Device_Get_Energy(float* Energy);
+/* DeviceInterface.h:74 / DeviceInterface.cu:2826 */
+int Device_Update_DObjectPostions(DOBJ* h_DynamicOBJ);
+/* DeviceInterface.h:75 / DeviceInterface.cu:2838 */
+int Device_Update_WorldObjectPostions(WOBJ* h_WorldOBJ);
+/* DeviceInterface.h:77 / DeviceInterface.cu:2859 */
+int Device_OpenHatch(WOBJ* h_WorldOBJ, int h_Num_WorldOBJ);
+/* DeviceInterface.h:78 / DeviceInterface.cu:2902 */
+int Device_Clean(void);
+/* DeviceInterface.h:79 / DeviceInterface.cu:2787 */
+int Device_Reset_Energy(int num_values);
+/* DeviceInterface.h:82 / DeviceInterface.cu:2848 */
+int drum_rotation(bool cylinder_rotation);
+/* DeviceInterface.h:83 / DeviceInterface.cu:2781 */
+int Start_Bin(void);
+/* DeviceInterface.h:85-87 / DeviceInterface.cu:2872-2893 */
+int Device_AddForce(void);
+int Device_SubForce(void);
+int Device_ZeroForce(void);
+/* DeviceInterface.h:95 / DeviceInterface.cu:1825 */
+int Device_DEM_UpdateSim(void);
+
+/* ---------------------------------------------------------------- Part 2 */
+
+typedef struct blaze_sim blaze_sim;
+
+typedef struct blaze_options {
+  float skin;          /* neighbour-list skin, cm; 0 = contacts only, rebuilt every step */
+  int max_nbr;         /* neighbour slots per particle (reference: 32) */
+  int wall_grid;       /* 1 = cull wall faces per cell (exact), 0 = test every face */
+  int use_graph;       /* 1 = step through a captured CUDA graph */
+  int capture_forces;  /* 1 = keep the last step's per-particle forces (parity hooks) */
+  int sync_each_step;  /* 1 = every step blocks and returns its status */
+} blaze_options;
+
+/* Library defaults: skin 0, max_nbr 32, wall_grid 1, use_graph 0,
+ * capture_forces 0, sync_each_step 0 (the reference's semantics). */
+void blaze_default_options(blaze_options* o);
+
+int blaze_create(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
+                 int n_d, const SimulationInfo* si, const blaze_options* opt);
+int blaze_destroy(blaze_sim* s);
+int blaze_set_options(blaze_sim* s, const blaze_options* opt);
+int blaze_set_cylinder_rotation(blaze_sim* s, int on);
+/* Host arrays, AoS float3 / int, length Num_Particles (vel/avel may be NULL). */
+int blaze_set_state(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
+                    const uint* type, const int* pid);
+int blaze_get_state(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid);
+/* Enqueue nsteps steps (asynchronous unless sync_each_step). */
+int blaze_step(blaze_sim* s, int nsteps);
+/* Wait for the stream; returns the accumulated status (see Part 1). */
+int blaze_sync(blaze_sim* s);
+int blaze_num_current(blaze_sim* s);
+int blaze_num_rebuilds(blaze_sim* s);
+int blaze_update_wobj(blaze_sim* s, const WOBJ* w, int n_w);
+int blaze_update_dobj(blaze_sim* s, const DOBJ* d, int n_d);
+/* Last step's forces (capture_forces=1), AoS float3 x6: particle-particle
+ * (incl. gravity), wall, volume-object; translational then rotational. */
+int blaze_get_forces(blaze_sim* s, float* f_pp, float* t_pp, float* f_w, float* t_w, float* f_l,
+                     float* t_l);
+/* Neighbour list of the last rebuild: nn[i], list[i*max_nbr + k]. */
+int blaze_get_nlist(blaze_sim* s, uint* nn, uint* list);
+/* Device pointers of the current state (SoA float4: pos+radius, vel+type,
+ * angular velocity) and the CUDA stream the simulation runs on. */
+int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, void** stream);
+/* Number of kernel launches the last blaze_step enqueued. */
+int blaze_last_launches(blaze_sim* s);
+/* Per-phase CUDA-event timing of subsequent steps (on/off), and the totals
+ * since it was switched on: re-sort + neighbour-list phase and the fused
+ * step kernel, in ms, with the number of steps timed. */
+int blaze_set_profile(blaze_sim* s, int on);
+int blaze_profile(blaze_sim* s, float* ms_rebuild, float* ms_step, int* n_steps);
+/* The simulation behind Part 1 (NULL before Device_Set_SimulationData). */
+blaze_sim* blaze_default_sim(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

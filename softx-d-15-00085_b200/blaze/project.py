@@ -697,73 +697,94 @@ class Project:
                                bool(self.wobj[0].is_rotating))
 
 
-def read_state_file(path, n, particle_type=0, sim_type=0, rotating=False):
-    t = _Tokens(path)
-    with open(path, "r", errors="replace") as fh:
-        first = fh.readline()
-    # getline() consumes the first line whole
-    t.i = len(first.split())
-    t.skip(1)
-    spec = t.i_()
-    hdr = {}
+def _header_count(sim_type, rotating):
+    # token pairs after "SpecType:" per simulation type (FileIO.h:348-496)
     if sim_type == 1:
-        names = ["rev", "time", "revstate", "angle", "p0", "p1", "p2", "p3", "p4"]
-        for nm in names:
-            t.skip(1)
-            hdr[nm] = t.f()
-    elif sim_type == 2:
-        t.skip(1); hdr["time"] = t.f()
-        t.skip(1); hdr["num_rem"] = t.i_()
-    elif rotating:
-        t.skip(1); hdr["time"] = t.f()
-        t.skip(1); hdr["steps"] = t.i_()
-        t.skip(1); hdr["angle"] = t.f()
-    else:
-        t.skip(1); hdr["time"] = t.f()
-    pos = np.zeros((n, 3), np.float32)
-    vel = np.zeros((n, 3), np.float32)
-    acc = np.zeros((n, 3), np.float32)
-    avel = np.zeros((n, 3), np.float32)
-    quat = np.zeros((n, 4), np.float32)
-    quat[:, 0] = 1.0
-    ptype = np.zeros(n, np.uint32)
-    pid = np.zeros(n, np.int32)
+        return 9
+    if sim_type == 2:
+        return 2
+    if rotating:
+        return 3
+    return 1
+
+
+def read_state_file(path, n, particle_type=0, sim_type=0, rotating=False):
+    """Read a SpecType 1-4 state file (FileIO.h:327-652) into arrays in file
+    order: pos, quat, vel, avel, acc, type, pid, spec_type, header."""
+    with open(path, "r", errors="replace") as fh:
+        text = fh.read()
+    nl = text.find("\n")
+    body = text[nl + 1:] if nl >= 0 else ""
+    head = body.split(None, 2 + 2 * _header_count(sim_type, rotating))
+    if len(head) < 2:
+        raise ProjectError("truncated state file %s" % path)
+    try:
+        spec = int(head[1])
+    except ValueError:
+        raise ProjectError("bad SpecType in %s" % path)
+    hdr_tok = head[2:2 + 2 * _header_count(sim_type, rotating)]
+    hdr = {}
+    names = {1: ["rev", "time", "revstate", "angle", "p0", "p1", "p2", "p3", "p4"],
+             2: ["time", "num_rem"]}.get(sim_type, ["time", "steps", "angle"] if rotating else ["time"])
+    for k, nm in enumerate(names):
+        if 2 * k + 1 < len(hdr_tok):
+            try:
+                hdr[nm] = float(hdr_tok[2 * k + 1])
+            except ValueError:
+                raise ProjectError("bad header value in %s" % path)
+    rest = head[-1] if len(head) == 3 + 2 * _header_count(sim_type, rotating) else ""
     poly = particle_type == 1
-    for i in range(n):
-        if spec == 1:
-            pid[i] = t.i_(); ptype[i] = t.i_(); pos[i] = t.f3()
-            if poly:
-                quat[i] = (t.f(), t.f(), t.f(), t.f())
-        elif spec == 2:
-            pid[i] = t.i_(); ptype[i] = t.i_(); pos[i] = t.f3(); vel[i] = t.f3()
-            if poly:
-                quat[i] = (t.f(), t.f(), t.f(), t.f())
-            avel[i] = t.f3()
-        elif spec in (3, 4):
-            pid[i] = t.i_(); ptype[i] = t.i_(); pos[i] = t.f3(); vel[i] = t.f3()
-            if spec == 4:
-                acc[i] = t.f3()
-            if poly:
-                quat[i] = (t.f(), t.f(), t.f(), t.f())
-            avel[i] = t.f3()
-            if spec == 4:
-                t.skip(3)
-        else:
-            raise ProjectError("invalid SpecType %r" % spec)
-    return dict(pos=pos, vel=vel, acc=acc, avel=avel, quat=quat, type=ptype, pid=pid,
-                spec_type=spec, header=hdr)
+    cols = {1: 5 + (4 if poly else 0), 2: 11 + (4 if poly else 0),
+            3: 11 + (4 if poly else 0), 4: 17 + (4 if poly else 0)}.get(spec)
+    if cols is None:
+        raise ProjectError("invalid SpecType %r" % spec)
+    vals = np.array(rest.split()[:cols * n], dtype=np.float64)
+    if vals.size < cols * n:
+        raise ProjectError("state file %s holds fewer than %d particles" % (path, n))
+    t = vals.reshape(n, cols)
+    f32 = np.float32
+    pos = t[:, 2:5].astype(f32)
+    vel = np.zeros((n, 3), f32)
+    acc = np.zeros((n, 3), f32)
+    avel = np.zeros((n, 3), f32)
+    quat = np.zeros((n, 4), f32)
+    quat[:, 0] = 1.0
+    c = 5
+    if spec >= 2:
+        vel = t[:, 5:8].astype(f32)
+        c = 8
+    if spec == 4:
+        acc = t[:, 8:11].astype(f32)
+        c = 11
+    if poly:
+        quat = t[:, c:c + 4].astype(f32)
+        c += 4
+    if spec >= 2:
+        avel = t[:, c:c + 3].astype(f32)
+    return dict(pos=pos, vel=vel, acc=acc, avel=avel, quat=quat, type=t[:, 1].astype(np.uint32),
+                pid=t[:, 0].astype(np.int32), spec_type=spec, header=hdr)
 
 
-def write_state_file(path, state, time=0.0, spec_type=3, header_line="#  P_ID   PType_ID   Pos   Vel   AngVel"):
-    """Write a SpecType 3 state file in the layout Read_FromFile accepts
-    (general simulation type, spheres)."""
+def write_state_file(path, state, time=0.0, spec_type=3, sim_type=0,
+                     header_line="#  P_ID   PType_ID   Pos   Vel   AngVel"):
+    """Write a SpecType 3 state file (spheres) with the header line
+    Read_FromFile expects for the simulation type (FileIO.h:348-496).
+    Floats are written with 9 significant digits, which round-trips FP32."""
     pos, vel, avel = state["pos"], state["vel"], state["avel"]
     pid, ptype = state["pid"], state["type"]
+    n = len(pid)
     with open(path, "w") as fh:
         fh.write(header_line + "\n")
         fh.write("Specfication_Detail: %d\n" % spec_type)
-        fh.write("  Time: %r\n" % float(time))
-        for i in range(len(pid)):
-            fh.write("%d %d %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g\n" % (
-                pid[i], ptype[i], pos[i, 0], pos[i, 1], pos[i, 2], vel[i, 0], vel[i, 1], vel[i, 2],
-                avel[i, 0], avel[i, 1], avel[i, 2]))
+        if sim_type == 2:
+            fh.write("  Time: %r NumRem: %d\n" % (float(time), n))
+        else:
+            fh.write("  Time: %r\n" % float(time))
+        ints = np.stack([np.asarray(pid, np.int64), np.asarray(ptype, np.int64)], 1)
+        fl = np.concatenate([np.asarray(pos, np.float32), np.asarray(vel, np.float32),
+                             np.asarray(avel, np.float32)], 1).astype(np.float64)
+        ia = np.char.mod("%d", ints)
+        fa = np.char.mod("%.9g", fl)
+        rows = np.concatenate([ia, fa], 1)
+        fh.write("\n".join(" ".join(r) for r in rows.tolist()))
+        fh.write("\n")

@@ -1,0 +1,321 @@
+"""Seeded synthetic workloads, written as reference-format project trees
+(.World / .POBJ / .WOBJ and a SpecType-3 state file) so that every run goes
+through the project-input path a user of the reference would use.
+
+Units are the reference's: cm, kg, s (Kn in kg/s^2 has the same number in
+SI and in these units).  All randomness is numpy default_rng(seed).
+
+  box_project    10,000 monodisperse spheres in a closed cube
+                 (the Particles_Box plain configuration)
+  silo_project   polydisperse spheres in a cylindrical silo over a conical
+                 hopper approximated by planar faces (reference-law variant
+                 of the silo discharge configuration: at most 6 radius bins,
+                 linear law, hopper faces within the 8 x 16 face capacity)
+"""
+import math
+import os
+
+import numpy as np
+
+from .project import Project, write_state_file
+
+_WORLD = """Title: "{title}"
+ModelType(Specfic|0:TC_COR|1:KN_COR):     1
+Simulation_Type(0=General,1=mill,2=silo): {sim_type}
+Particle_Type(0=sphere,1=poly,2=mixed):   0
+Delta_t(s):       {dt!r}
+_________________________________________________
+             1_Geometrical-Information
+---------------------------------------
+ 1.1_World_Objects_(index__name)
+---------------------------------------
+Number: {n_w}
+{wobj_lines}
+---------------------------------------
+ 1.2_Particle_Objects_(index__name__number)
+---------------------------------------
+Number: {n_p}
+{pobj_lines}
+---------------------------------------
+ 1.3_Dynamic_Objects_(index__name)
+---------------------------------------
+Number: 0 Repeat: 0
+_________________________________________________
+_________________________________________________
+             2_Simulation_Setup
+Num_Particles:    {n}
+ForceField(cm/s^2): {g[0]!r} {g[1]!r} {g[2]!r}
+---------------------------------------------
+Rotation:         {rotation}
+RollRes:          {roll_res!r}
+GlobalDamp:       1.0
+VelLimit:         0.0
+_________________________________________________
+_________________________________________________
+            3_Spatial-Grid-Computation
+Origin:       {origin[0]!r} {origin[1]!r} {origin[2]!r}
+World_Size:   {world[0]!r} {world[1]!r} {world[2]!r}
+Cell_Size:    {cell!r} {cell!r} {cell!r}
+_________________________________________________
+_________________________________________________
+            4_Inital_Particle-Setup
+Read_FromFile: 1
+FileName: {state}
+_________________________________________________
+_________________________________________________
+             5_Output_Options
+Display:           0
+View:              0
+FPS:               50
+GL_DEBUG           0
+File_write(Steps): 0
+Total_Time:        0.0
+IS_Time_Limit:     0
+IS_Energy_diss(steps): 0
+IS_Wall_forces(steps): 0
+_________________________________________________
+{specific}"""
+
+_POBJ = """Title: "{title}"
+Descp: "synthetic"
+Geometry_Specfications
+Diameter: {diam!r}
+Density:  {rho!r}
+Particle_Particle
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Static_Friction:  {mu!r}
+Kinetic_Friction: {mu!r}
+Particle_Surface
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Static_Friction:  {mu!r}
+Kinetic_Friction: {mu!r}
+Particle_Lifter
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Static_Friction:  {mu!r}
+Kinetic_Friction: {mu!r}
+"""
+
+
+def _orient(verts, faces, inside):
+    """Order each face's vertices so the reference's face normal
+    cross(V2, V1) (KSimulationData.cpp:846-856) points towards `inside(centroid)`."""
+    out = []
+    for f in faces:
+        v = [np.asarray(verts[q], np.float64) for q in f]
+        n = np.cross(v[2] - v[1], v[1] - v[0])
+        c = np.mean(v, axis=0)
+        if np.dot(n, np.asarray(inside(c), np.float64) - c) < 0:
+            f = tuple(reversed(f))
+        out.append(tuple(f))
+    return out
+
+
+def _write_wobj(path, title, verts, faces, tol=1.0):
+    with open(path, "w") as fh:
+        fh.write('Title: "%s"\nDescp: "synthetic"\nGeometry-Specfications\n' % title)
+        fh.write("NUM_VERTEX: %d\n" % len(verts))
+        for k, v in enumerate(verts):
+            fh.write("%d %r %r %r\n" % (k + 1, float(v[0]), float(v[1]), float(v[2])))
+        fh.write("NUM_SURFACES: %d\n" % len(faces))
+        for k, f in enumerate(faces):
+            fh.write('%d "F%d" Area_Tol: %r\nNUM_VERTEX: %d\n' % (k + 1, k, float(tol), len(f)))
+            fh.write(" ".join(str(int(q) + 1) for q in f) + "\n")
+
+
+def _write_cylinder_wobj(path, title, radius, height, offset, axis_normal=(0.0, 1.0, 0.0)):
+    """Macro cylinder world object (KSimulationData.cpp:760-823): diameter,
+    height, no caps, axis from the bottom-cap normal."""
+    with open(path, "w") as fh:
+        fh.write('Title: "%s"\nDescp: "synthetic"\nGeometry-Specfications\n' % title)
+        fh.write("NUM_VERTEX: 0\nNUM_SURFACES: 1\n")
+        fh.write('-1 "Cyl"\nDiameter: %r\nHeight: %r\nTop_Cap: false\nBot_Cap: false\n'
+                 % (2.0 * radius, height))
+        fh.write("Top_Normal: %r %r %r\n" % (-axis_normal[0], -axis_normal[1], -axis_normal[2]))
+        fh.write("Bot_Normal: %r %r %r\n" % tuple(axis_normal))
+        fh.write("Offset: %r %r %r\n" % tuple(offset))
+
+
+def _write_project(root, name, world_name, *, title, sim_type, dt, wobjs, pobjs, counts, n, g,
+                   rotation, roll_res, origin, world, cell, state, specific=""):
+    base = os.path.join(root, name)
+    for sub in ("World", "SurfaceObjects", "ParticleObjects", "VolumeObjects"):
+        os.makedirs(os.path.join(base, sub), exist_ok=True)
+    wl = "\n".join("%d %s" % (k + 1, w) for k, w in enumerate(wobjs))
+    pl = "\n".join("1 %s %d" % (p, c) for p, c in zip(pobjs, counts))
+    with open(os.path.join(base, "World", world_name + ".World"), "w") as fh:
+        fh.write(_WORLD.format(title=title, sim_type=sim_type, dt=dt, n_w=len(wobjs), wobj_lines=wl,
+                               n_p=len(pobjs), pobj_lines=pl, n=n, g=g, rotation=rotation,
+                               roll_res=roll_res, origin=origin, world=world, cell=cell,
+                               state=state, specific=specific))
+    return base
+
+
+def box_project(root, n_side=(20, 20, 25), radius=0.1, rho=2500.0, box=10.0, kn=1.0e5, cor=0.5,
+                mu=0.4, dt=1e-5, pitch=0.3, start=0.3, jitter=0.02, seed=0, cell=0.2,
+                gravity=(0.0, 0.0, -981.0), name="Particles_Box", world="Box_plain"):
+    """Particles_Box plain configuration: spheres on a jittered cubic lattice
+    (x, y horizontal, z vertical) in a closed cube of six quad faces.
+    Returns (Project, state dict)."""
+    nx, ny, nz = n_side
+    n = nx * ny * nz
+    base = os.path.join(root, name)
+    os.makedirs(os.path.join(base, "SurfaceObjects"), exist_ok=True)
+    os.makedirs(os.path.join(base, "ParticleObjects"), exist_ok=True)
+    L = float(box)
+    verts = [(0, 0, 0), (L, 0, 0), (L, L, 0), (0, L, 0), (0, 0, L), (L, 0, L), (L, L, L), (0, L, L)]
+    # quads ordered so cross(V2, V1) (KSimulationData.cpp:846-856) points into the box
+    faces = [(0, 1, 2, 3), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (3, 7, 4, 0), (4, 7, 6, 5)]
+    faces = _orient(verts, faces, lambda c: (0.5 * L, 0.5 * L, 0.5 * L))
+    _write_wobj(os.path.join(base, "SurfaceObjects", "Box.WOBJ"), "Box", verts, faces)
+    with open(os.path.join(base, "ParticleObjects", "Sphere.POBJ"), "w") as fh:
+        fh.write(_POBJ.format(title="Sphere", diam=2.0 * radius, rho=rho, cor=cor, kn=kn, mu=mu))
+    rng = np.random.default_rng(seed)
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    lat = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1).astype(np.float64) * pitch + start
+    pos = (lat + rng.uniform(-jitter, jitter, size=lat.shape)).astype(np.float32)
+    state = dict(pos=pos, vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),
+                 pid=np.arange(n, dtype=np.int32), type=np.zeros(n, np.uint32))
+    write_state_file(os.path.join(base, "Start_" + world), state)
+    origin = (-cell, -cell, -cell)
+    _write_project(root, name, world, title="Particles_Box", sim_type=0, dt=dt, wobjs=["Box"],
+                   pobjs=["Sphere"], counts=[n], n=n, g=gravity, rotation=1, roll_res=0.0,
+                   origin=origin, world=(L + cell, L + cell, L + cell), cell=cell,
+                   state="Start_" + world)
+    proj = Project.load(root, name, world)
+    return proj, proj.read_state()
+
+
+def cone_hopper_faces(r_top, r_out, y_top, y_out, n_seg):
+    """Planar quads approximating a cone (axis +y, centred on x=z=r_top),
+    n_seg segments around; each quad's normal points inward/upward."""
+    quads = []
+    c = r_top
+    for k in range(n_seg):
+        a0 = 2 * math.pi * k / n_seg
+        a1 = 2 * math.pi * (k + 1) / n_seg
+        p = [(c + r_top * math.cos(a0), y_top, c + r_top * math.sin(a0)),
+             (c + r_top * math.cos(a1), y_top, c + r_top * math.sin(a1)),
+             (c + r_out * math.cos(a1), y_out, c + r_out * math.sin(a1)),
+             (c + r_out * math.cos(a0), y_out, c + r_out * math.sin(a0))]
+        quads.append(p)
+    return quads
+
+
+def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, silo_r=25.0,
+                 silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, seg_per_obj=7, n_hopper_objs=6,
+                 kn=1.0e5, cor=0.6, mu=0.5, dt=5e-6, seed=1, overlap=1e-3,
+                 name="Silo", world="Silo_discharge", gravity=(0.0, -981.0, 0.0)):
+    """Silo discharge, reference-law variant (y vertical, as the reference's
+    silo logic assumes, main.cpp:271 and GPU_Memory_Transfer.cuh:656):
+    cylinder r=silo_r over a conical hopper of half-angle half_angle_deg down
+    to an outlet of outlet_d, made of n_hopper_objs world objects of
+    seg_per_obj planar quads each; radii uniform in [r_min, r_max] quantised
+    to n_bins particle objects (the reference's 6-entry pair table); particles
+    on a jittered lattice filling the silo from the hopper up.
+    Returns (Project, state dict)."""
+    base = os.path.join(root, name)
+    for sub in ("SurfaceObjects", "ParticleObjects"):
+        os.makedirs(os.path.join(base, sub), exist_ok=True)
+    r_out = 0.5 * outlet_d
+    h_hop = (silo_r - r_out) / math.tan(math.radians(half_angle_deg))
+    y_out = 10.0
+    y_top = y_out + h_hop
+    n_seg = seg_per_obj * n_hopper_objs
+    quads = cone_hopper_faces(silo_r, r_out, y_top, y_out, n_seg)
+    wobjs = []
+    for o in range(n_hopper_objs):
+        vs, fs = [], []
+        for k in range(seg_per_obj):
+            q = quads[o * seg_per_obj + k]
+            if k == 0:
+                vs += [q[0], q[3]]
+            vs += [q[1], q[2]]
+            a = 2 * k
+            # vertices: top0 bot0 top1 bot1 ... ; quad (top_k, top_k+1, bot_k+1, bot_k)
+            fs.append((a, a + 2, a + 3, a + 1))
+        nm = "Hopper%d" % o
+        # normals point into the hopper: towards the axis, up the cone
+        fs = _orient(vs, fs, lambda c: (silo_r, c[1] + 10.0, silo_r))
+        _write_wobj(os.path.join(base, "SurfaceObjects", nm + ".WOBJ"), nm, vs, fs)
+        wobjs.append(nm)
+    _write_cylinder_wobj(os.path.join(base, "SurfaceObjects", "Barrel.WOBJ"), "Barrel", silo_r,
+                         silo_h + h_hop, (0.0, 0.0, 0.0))
+    wobjs.append("Barrel")
+    # last world object: the hatch under the outlet (the removal height is
+    # its first vertex's y - 5, main.cpp:771-773); opening it drops it
+    yh = y_out - 1.0
+    hv = [(silo_r - 2 * r_out, yh, silo_r - 2 * r_out), (silo_r + 2 * r_out, yh, silo_r - 2 * r_out),
+          (silo_r + 2 * r_out, yh, silo_r + 2 * r_out), (silo_r - 2 * r_out, yh, silo_r + 2 * r_out)]
+    _write_wobj(os.path.join(base, "SurfaceObjects", "Hatch.WOBJ"), "Hatch", hv,
+                _orient(hv, [(0, 1, 2, 3)], lambda c: (c[0], c[1] + 1.0, c[2])))
+    wobjs.append("Hatch")
+    edges = np.linspace(r_min, r_max, n_bins + 1)
+    radii = 0.5 * (edges[:-1] + edges[1:])
+    rng = np.random.default_rng(seed)
+    rs = rng.uniform(r_min, r_max, size=n)
+    types = np.clip(np.searchsorted(edges, rs, side="right") - 1, 0, n_bins - 1).astype(np.uint32)
+    counts = np.bincount(types, minlength=n_bins)
+    pobjs = []
+    for b in range(n_bins):
+        nm = "Sphere%d" % b
+        with open(os.path.join(base, "ParticleObjects", nm + ".POBJ"), "w") as fh:
+            fh.write(_POBJ.format(title=nm, diam=float(2.0 * radii[b]), rho=float(rho), cor=float(cor), kn=float(kn), mu=float(mu)))
+        pobjs.append(nm)
+    # Size-banded simple-cubic layers: the particles of each radius bin fill
+    # horizontal layers (largest bin lowest) on a lattice of pitch
+    # 2 r (1 - overlap), so the bed starts as a contact network under load
+    # (about six contacts per particle, solid fraction ~0.52) instead of a
+    # free fall; each layer is clipped to the hopper cone / barrel with a
+    # clearance of r / cos(half-angle) from the wall.
+    tan_a = math.tan(math.radians(half_angle_deg))
+    cos_a = math.cos(math.radians(half_angle_deg))
+    c = silo_r
+    pos = np.zeros((n, 3), np.float64)
+    types_out = np.zeros(n, np.uint32)
+    k = 0
+    y = y_out + 0.05
+    for b in range(n_bins - 1, -1, -1):
+        r = float(radii[b])
+        pitch = 2.0 * r * (1.0 - overlap)
+        need = int(counts[b])
+        y += r
+        while need > 0:
+            ra = (r_out + (y - y_out) * tan_a) if y < y_top else silo_r
+            ra -= r / cos_a + 0.05
+            if ra > 0:
+                m = int(ra / pitch)
+                g = np.arange(-m, m + 1) * pitch
+                xx, zz = np.meshgrid(g, g, indexing="ij")
+                keep = xx ** 2 + zz ** 2 <= ra * ra
+                xs, zs = xx[keep][:need], zz[keep][:need]
+                cnt = len(xs)
+                pos[k:k + cnt, 0] = c + xs
+                pos[k:k + cnt, 1] = y
+                pos[k:k + cnt, 2] = c + zs
+                types_out[k:k + cnt] = b
+                k += cnt
+                need -= cnt
+            y += pitch
+        y += r * 0.02
+    types = types_out
+    pos = pos.astype(np.float32)
+    state = dict(pos=pos, vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),
+                 pid=np.arange(n, dtype=np.int32), type=types)
+    write_state_file(os.path.join(base, "Start_" + world), state, sim_type=2)
+    cell = 2.0 * r_max
+    y_max = float(pos[:, 1].max()) + 4 * r_max
+    origin = (-cell, -cell, -cell)
+    worldsz = (2 * silo_r + cell, y_max, 2 * silo_r + cell)
+    specific = ("_________________________________________________\n"
+                "          6_Simulation_Specfic_Options\n"
+                "Hatch_mode:        1\nFlow_counter:      1 1000\nkill_after:        1\n"
+                "_________________________________________________\n")
+    _write_project(root, name, world, title="Silo", sim_type=2, dt=dt, wobjs=wobjs, pobjs=pobjs,
+                   counts=[int(c_) for c_ in counts], n=n, g=gravity, rotation=1, roll_res=0.0,
+                   origin=origin, world=tuple(float(v) for v in worldsz), cell=float(cell), state="Start_" + world,
+                   specific=specific)
+    proj = Project.load(root, name, world)
+    return proj, proj.read_state()

@@ -1,0 +1,892 @@
+// blaze_capi.cu -- host side of libblaze_b200.so: one simulation object per
+// handle (device buffers allocated once, a private CUDA stream), the step
+// pipeline, and the C ABI of include/blaze_dem.h.
+//
+// The reference allocates and frees its sort temporaries and contact list
+// inside every step and synchronises after every stage
+// (DeviceInterface.cu:1825-2513); here every buffer lives for the whole run
+// and a step is a fixed sequence of kernel launches on one stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "blaze_dem.h"
+#include "dem_kernels.cuh"
+#include "radix_sort.cuh"
+
+using namespace blaze;
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_); \
+  } while (0)
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+  std::fprintf(stderr, "blaze: CUDA error %d (%s)\n", (int)e, cudaGetErrorString(e));
+  return -(1000 + (int)e);
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+}  // namespace
+
+struct blaze_sim {
+  int n_max = 0;
+  SimulationInfo si{};
+  WOBJ w[8]{};
+  POBJ p[8]{};
+  DOBJ d[kMaxDobj]{};
+  int n_w = 0, n_p = 0, n_d = 0;
+  int num_wobj = 0;
+  blaze_options opt{};
+  int cyl_rot = 0;
+  SimParams hp{};
+  SimParams* dp = nullptr;
+  std::vector<WallOp> ops;
+  WallOp* d_ops = nullptr;
+  uint32_t* d_wall_off = nullptr;
+  uint16_t* d_wall_idx = nullptr;
+  bool walls_static = true;
+  // state
+  StateBuf S[3]{};  // S[0], S[1] ping-pong, S[2] sorted gather target
+  OrderBuf ob{};
+  int cur = 0;      // S[cur] holds the current state
+  RadixSortBuffers rs{};
+  uint32_t* cstart = nullptr;
+  uint32_t* cend = nullptr;
+  NbrList nl{};
+  StepCtl* ctl = nullptr;
+  StepCtl* h_ctl = nullptr;  // pinned mirror
+  ForceCapture cap{};
+  bool cap_alloc = false;
+  cudaStream_t stream = nullptr;
+  int key_bits = 1;
+  long long steps = 0;
+  int stepc = 0;        // steps since the last removal check
+  uint32_t status = 0;  // accumulated, reported at sync points
+  int last_launches = 0;
+  // tallies kept for the reference interface (float, host side)
+  float tallies[6]{};
+  float fc = 0.0f;
+  // optional per-phase event timing (non-graph stepping only)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_marks;  // (phase, event index) start/end pairs in order
+  int ev_used = 0;
+  // pinned host staging for state upload/download (n_max each)
+  float4* h4a = nullptr;
+  float4* h4b = nullptr;
+  float4* h4c = nullptr;
+  int* hpid = nullptr;
+};
+
+namespace {
+
+blaze_sim* g_default = nullptr;
+
+// ------------------------------------------------------------------ params
+void build_params(blaze_sim* s) {
+  SimParams& P = s->hp;
+  std::memset(&P, 0, sizeof(P));
+  const SimulationInfo& si = s->si;
+  P.origin = si.worldOrigin;
+  P.cell = si.cellSize;
+  P.ncells = si.num_NNCells;
+  const long long nx = si.num_NNCells.x, ny = si.num_NNCells.y, nz = si.num_NNCells.z;
+  const long long hmax = (nx - 1) + (nz - 1) * nz + (ny - 1) * nx * nz + 1;
+  const long long prod = nx * ny * nz;
+  P.ncell_tab = (uint32_t)std::max(hmax, prod);
+  P.gravity = si.Force_Field;
+  P.dt = si.InitalDelta_t;
+  P.roll_res = si.Roll_Res;
+  P.mill_rot_vel = si.MillRotVel;
+  P.drum_r = s->n_w > 0 ? s->w[0].cyl_geo.radius : 0.0f;
+  P.rotation = si.Rotation ? 1 : 0;
+  P.mode2d = si.Mode2D ? 1 : 0;
+  P.energy_calc = si.EnergyCalc ? 1 : 0;
+  P.is_mill = si.isMillSim ? 1 : 0;
+  P.rotating_wobj = si.Rotating_WObject ? 1 : 0;
+  P.cyl_rot = s->cyl_rot;
+  P.cent = si.cent;
+  P.dobj_cyl_bound_r = si.DObject_CylinderBoundR;
+  P.n_types = s->n_p;
+  for (int t = 0; t < s->n_p; ++t) {
+    const POBJ& o = s->p[t];
+    TypeParams& T = P.types[t];
+    T.radius = o.radius;
+    T.mass = o.mass;
+    T.iinv = o.InertiaT[0];
+    T.s_kn = o.surface_Kn; T.s_cn = o.surface_Cn;
+    T.s_mus = o.surface_Fric_static; T.s_muk = o.surface_Fric_kinetic;
+    T.d_kn = o.Dsurface_Kn; T.d_cn = o.Dsurface_Cn; T.d_muk = o.Dsurface_Fric_kinetic;
+    for (int q = 0; q < kMaxPP; ++q) T.pp[q] = o.PP[q];
+  }
+  P.n_dobj = s->n_d;
+  for (int k = 0; k < s->n_d; ++k) {
+    const DOBJ& D = s->d[k];
+    DobjDev& G = P.dobj[k];
+    G.com = D.COM;
+    G.axis = D.Axis;
+    G.bound_r = D.boundR;
+    G.num_faces = std::min(D.num_faces, 3);
+    G.num_edges = std::min(D.num_edges, 4);
+    G.attached = D.is_attached_DWorld ? 1 : 0;
+    G.translating = D.is_translating ? 1 : 0;
+    G.velocity = D.velocity;
+    for (int v = 0; v < 8; ++v) G.vert[v] = D.vertex[v];
+    for (int f = 0; f < 3; ++f) G.faces[f] = D.faces[f];
+    for (int e = 0; e < 4; ++e) {
+      G.edge0[e] = (int)(D.edge[e].point_vindex[0] & 7u);
+      G.edge1[e] = (int)(D.edge[e].point_vindex[1] & 7u);
+    }
+  }
+  P.max_nbr = s->opt.max_nbr;
+  P.skin = s->opt.skin;
+}
+
+// World objects -> the wall program, in world-object order
+// (DEM_Kernels_Compute.cuh:312-600).
+void build_ops(blaze_sim* s) {
+  s->ops.clear();
+  for (int k = 0; k < s->num_wobj && k < s->n_w; ++k) {
+    const WOBJ& W = s->w[k];
+    if (W.surface_type == plane) {
+      for (int f = 0; f < W.num_surfaces && f < 16; ++f) {
+        const Surface& S = W.surfaces[f];
+        WallOp op;
+        std::memset(&op, 0, sizeof(op));
+        op.kind = S.area == -1.0f ? kOpPlane : kOpFace;
+        op.nv = std::min(std::max(S.num_vertex, 0), 8);
+        op.area = S.area;
+        op.tol = S.Tol;
+        op.n = S.normal;
+        op.c = S.centroid;
+        for (int v = 0; v < op.nv; ++v) op.v[v] = W.vertex[S.vertex_Order[v] & 15];
+        s->ops.push_back(op);
+      }
+    } else if (W.surface_type == cylinder) {
+      const Macro_Cylinder& cg = W.cyl_geo;
+      WallOp op;
+      std::memset(&op, 0, sizeof(op));
+      op.kind = kOpCylinder;
+      op.radius = cg.radius;
+      op.axis = cg.AXIS;
+      op.cbot = cg.center_bot_cap;
+      s->ops.push_back(op);
+      if (cg.has_top_cap) {
+        WallOp t = op;
+        t.kind = kOpCapTop;
+        t.n = cg.normal_top_cap;
+        t.c = cg.center_top_cap;
+        s->ops.push_back(t);
+      }
+      if (cg.has_bot_cap) {
+        WallOp b = op;
+        b.kind = kOpCapBot;
+        b.n = cg.normal_bot_cap;
+        b.c = cg.center_bot_cap;
+        s->ops.push_back(b);
+      }
+    }
+  }
+  s->hp.n_ops = (int)s->ops.size();
+}
+
+// Per-cell candidate lists of wall ops, conservative: an op is dropped for a
+// cell only when no sphere centred in that cell (radius <= rmax) can pass
+// the op's contact test, so the forces are unchanged bit for bit.
+//   faces:   centre must lie within (0, r) above the face plane and project
+//            inside the polygon grown by the area tolerance
+//            (is_PointOnSurface accepts a point at distance d outside a
+//            convex polygon of area A while d * L <= Tol/100 * A for the
+//            edge length L nearest to it; the margin uses the shortest edge)
+//   planes:  centre within (0, r) above the plane
+//   cylinder ops and caps are always kept.
+void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint16_t>& idx) {
+  const SimParams& P = s->hp;
+  const uint32_t nt = P.ncell_tab;
+  float rmax = 0.0f;
+  for (int t = 0; t < s->n_p; ++t) rmax = std::max(rmax, s->p[t].radius);
+  struct Box { double lo[3], hi[3]; };
+  const int nops = (int)s->ops.size();
+  std::vector<Box> grown(nops);
+  std::vector<int> always(nops, 0);
+  for (int q = 0; q < nops; ++q) {
+    const WallOp& op = s->ops[q];
+    if (op.kind != kOpFace) { always[q] = 1; continue; }
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    double minedge = 1e300;
+    for (int v = 0; v < op.nv; ++v) {
+      const float3 a = op.v[v], b = op.v[(v + 1) % op.nv];
+      const double ax[3] = {a.x, a.y, a.z};
+      for (int c = 0; c < 3; ++c) { lo[c] = std::min(lo[c], ax[c]); hi[c] = std::max(hi[c], ax[c]); }
+      const double e = std::sqrt((double)(a.x - b.x) * (a.x - b.x) + (double)(a.y - b.y) * (a.y - b.y) +
+                                 (double)(a.z - b.z) * (a.z - b.z));
+      if (e > 0) minedge = std::min(minedge, e);
+    }
+    double margin = (double)op.tol / 100.0 * std::fabs((double)op.area) / std::max(minedge, 1e-12);
+    margin = margin * 1.01 + 1e-4 * (hi[0] - lo[0] + hi[1] - lo[1] + hi[2] - lo[2]) + rmax;
+    if (!std::isfinite(margin) || op.area <= 0.0f) { always[q] = 1; continue; }
+    for (int c = 0; c < 3; ++c) { grown[q].lo[c] = lo[c] - margin; grown[q].hi[c] = hi[c] + margin; }
+  }
+  off.assign((size_t)nt + 1, 0);
+  std::vector<std::vector<uint16_t>> per(0);
+  idx.clear();
+  const int3 nc = P.ncells;
+  // cells are visited in hash order so the CSR is built in one pass
+  std::vector<uint32_t> counts((size_t)nt, 0);
+  std::vector<std::vector<uint16_t>> lists;
+  // enumerate in-grid cells; hashes can alias (ncx != ncz): merge their ops
+  std::vector<std::vector<uint16_t>> by_hash((size_t)nt);
+  const double hd = 0.5 * std::sqrt((double)P.cell.x * P.cell.x + (double)P.cell.y * P.cell.y +
+                                    (double)P.cell.z * P.cell.z);
+  for (int gy = 0; gy < nc.y; ++gy)
+    for (int gz = 0; gz < nc.z; ++gz)
+      for (int gx = 0; gx < nc.x; ++gx) {
+        const uint32_t h = (uint32_t)((gx + gz * nc.z) + (gy * nc.x) * nc.z);
+        const double lo[3] = {P.origin.x + (double)gx * P.cell.x, P.origin.y + (double)gy * P.cell.y,
+                              P.origin.z + (double)gz * P.cell.z};
+        const double hi[3] = {lo[0] + P.cell.x, lo[1] + P.cell.y, lo[2] + P.cell.z};
+        const double ctr[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
+        std::vector<uint16_t>& L = by_hash[h];
+        for (int q = 0; q < nops; ++q) {
+          bool keep = always[q] != 0;
+          const WallOp& op = s->ops[q];
+          if (!keep && op.kind == kOpFace) {
+            bool ov = true;
+            for (int c = 0; c < 3; ++c)
+              if (hi[c] < grown[q].lo[c] || lo[c] > grown[q].hi[c]) ov = false;
+            if (ov) {
+              const double d = (double)op.n.x * (ctr[0] - op.c.x) + (double)op.n.y * (ctr[1] - op.c.y) +
+                               (double)op.n.z * (ctr[2] - op.c.z);
+              keep = d > -hd - 1e-3 && d < hd + rmax + 1e-3;
+            }
+          }
+          if (keep && (L.empty() || L.back() < q)) {
+            if (std::find(L.begin(), L.end(), (uint16_t)q) == L.end()) L.push_back((uint16_t)q);
+          }
+        }
+        if (L.size() > 1) std::sort(L.begin(), L.end());
+      }
+  for (uint32_t h = 0; h < nt; ++h) {
+    off[h] = (uint32_t)idx.size();
+    idx.insert(idx.end(), by_hash[h].begin(), by_hash[h].end());
+  }
+  off[nt] = (uint32_t)idx.size();
+}
+
+int upload_walls(blaze_sim* s) {
+  build_ops(s);
+  CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
+  if (s->d_ops) CK(cudaFree(s->d_ops));
+  s->d_ops = nullptr;
+  CK(dalloc(&s->d_ops, s->ops.size()));
+  if (!s->ops.empty())
+    CK(cudaMemcpyAsync(s->d_ops, s->ops.data(), sizeof(WallOp) * s->ops.size(),
+                       cudaMemcpyHostToDevice, s->stream));
+  if (s->d_wall_off) CK(cudaFree(s->d_wall_off));
+  if (s->d_wall_idx) CK(cudaFree(s->d_wall_idx));
+  s->d_wall_off = nullptr;
+  s->d_wall_idx = nullptr;
+  if (s->opt.wall_grid && s->walls_static && !s->ops.empty()) {
+    std::vector<uint32_t> off;
+    std::vector<uint16_t> idx;
+    build_wall_grid(s, off, idx);
+    CK(dalloc(&s->d_wall_off, off.size()));
+    CK(dalloc(&s->d_wall_idx, idx.size()));
+    CK(cudaMemcpyAsync(s->d_wall_off, off.data(), sizeof(uint32_t) * off.size(),
+                       cudaMemcpyHostToDevice, s->stream));
+    if (!idx.empty())
+      CK(cudaMemcpyAsync(s->d_wall_idx, idx.data(), sizeof(uint16_t) * idx.size(),
+                         cudaMemcpyHostToDevice, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int upload_params(blaze_sim* s) {
+  build_params(s);
+  return upload_walls(s);
+}
+
+int alloc_nlist(blaze_sim* s) {
+  if (s->nl.idx) CK(cudaFree(s->nl.idx));
+  if (s->nl.cnt) CK(cudaFree(s->nl.cnt));
+  s->nl.stride = s->n_max;
+  s->nl.cap = s->opt.max_nbr;
+  CK(dalloc(&s->nl.idx, (size_t)s->n_max * s->nl.cap));
+  CK(dalloc(&s->nl.cnt, s->n_max));
+  CK(cudaMemsetAsync(s->nl.cnt, 0, sizeof(uint32_t) * s->n_max, s->stream));
+  return 0;
+}
+
+int alloc_capture(blaze_sim* s) {
+  if (s->cap_alloc || !s->opt.capture_forces) return 0;
+  float** ps[6] = {&s->cap.f_pp, &s->cap.t_pp, &s->cap.f_w, &s->cap.t_w, &s->cap.f_l, &s->cap.t_l};
+  for (auto* q : ps) {
+    CK(dalloc(q, (size_t)3 * s->n_max));
+    CK(cudaMemsetAsync(*q, 0, sizeof(float) * 3 * s->n_max, s->stream));
+  }
+  s->cap_alloc = true;
+  return 0;
+}
+
+// --------------------------------------------------------------- the step
+int enqueue_rebuild(blaze_sim* s, const int* gate) {
+  const int n = s->n_max;
+  launch_hash(s->dp, s->S[s->cur], s->ob, n, s->rs.keys[0], s->ctl, gate, s->stream);
+  const int res = radix_sort_pairs(s->rs, n, s->key_bits, true, gate, s->stream);
+  const size_t cbytes = sizeof(uint32_t) * s->hp.ncell_tab;
+  CK(cudaMemsetAsync(s->cstart, 0xff, cbytes, s->stream));
+  launch_reorder(s->S[s->cur], s->S[2], s->ob, n, s->rs.keys[res], s->rs.vals[res], s->cstart,
+                 s->cend, s->hp.ncell_tab, s->n_d > 0, s->ctl, gate, s->stream);
+  launch_nlist(s->dp, s->S[2], n, s->cstart, s->cend, s->nl, s->ctl, gate, s->stream);
+  s->last_launches += 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits);
+  return 0;
+}
+
+cudaEvent_t prof_event(blaze_sim* s, int phase) {
+  if ((int)s->ev_pool.size() <= s->ev_used) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    s->ev_pool.push_back(e);
+  }
+  cudaEvent_t e = s->ev_pool[s->ev_used];
+  s->ev_marks.push_back({phase, s->ev_used});
+  s->ev_used++;
+  cudaEventRecord(e, s->stream);
+  return e;
+}
+
+int enqueue_step(blaze_sim* s) {
+  if (s->profile) prof_event(s, 0);
+  launch_gate(s->ctl, s->stream);
+  int rc = enqueue_rebuild(s, &s->ctl->rebuilt);
+  if (rc) return rc;
+  if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
+  launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
+              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl,
+              s->opt.capture_forces ? &s->cap : nullptr, s->stream);
+  s->last_launches += 2;
+  if (s->profile) prof_event(s, 1);
+  s->cur ^= 1;
+  s->steps++;
+  // silo / plant removal check every 1000 steps (DeviceInterface.cu:2463-2498)
+  if (s->si.Kill_Particles) {
+    s->stepc++;
+    if (s->stepc >= 1000) {
+      launch_kill(s->S[s->cur], s->ob, s->n_max, s->si.Silo_Kill_Height,
+                  s->si.Rotating_WObject ? 1 : 0, s->si.max_size, s->ctl, s->stream);
+      s->last_launches += 1;
+      s->stepc = 0;
+    }
+  }
+  return 0;
+}
+
+int sync_status(blaze_sim* s) {
+  CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  s->status |= s->h_ctl->status;
+  return (int)s->status;
+}
+
+int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
+                   const uint* type, const int* pid) {
+  const int n = s->n_max;
+  int dead = 0;
+  for (int i = 0; i < n; ++i) {
+    const uint t = type[i];
+    const float r = t < (uint)s->n_p ? s->p[t].radius : 0.0f;
+    s->h4a[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], r);
+    float tb;
+    int ti = (int)t;
+    std::memcpy(&tb, &ti, 4);
+    s->h4b[i] = vel3 ? make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], tb)
+                     : make_float4(0.0f, 0.0f, 0.0f, tb);
+    s->h4c[i] = avel3 ? make_float4(avel3[3 * i], avel3[3 * i + 1], avel3[3 * i + 2], 0.0f)
+                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    s->hpid[i] = pid[i];
+    if (pid[i] < 0) ++dead;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  CK(sync_status(s) < 0 ? cudaErrorUnknown : cudaSuccess);
+  const int e = s->h_ctl->epoch & 1;
+  const StateBuf& S = s->S[s->cur];
+  CK(cudaMemcpyAsync(S.pos, s->h4a, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(S.vel, s->h4b, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(S.angv, s->h4c, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->ob.pid[e], s->hpid, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+  if (s->n_d > 0) {
+    std::vector<int> l(n, -1);
+    CK(cudaMemcpyAsync(s->ob.lift[e], l.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  StepCtl c = *s->h_ctl;
+  c.rebuild_req = 1;
+  c.rebuilt = 0;
+  c.n_cur = n;
+  c.pending_dead = dead;
+  *s->h_ctl = c;
+  CK(cudaMemcpyAsync(s->ctl, s->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int get_state_impl(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid) {
+  int st = sync_status(s);
+  if (st < 0) return st;
+  const int n = s->n_max;
+  const int e = s->h_ctl->epoch & 1;
+  const StateBuf& S = s->S[s->cur];
+  if (pos3) CK(cudaMemcpyAsync(s->h4a, S.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (vel3 || type) CK(cudaMemcpyAsync(s->h4b, S.vel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (avel3) CK(cudaMemcpyAsync(s->h4c, S.angv, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (pid) CK(cudaMemcpyAsync(s->hpid, s->ob.pid[e], sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < n; ++i) {
+    if (pos3) { pos3[3 * i] = s->h4a[i].x; pos3[3 * i + 1] = s->h4a[i].y; pos3[3 * i + 2] = s->h4a[i].z; }
+    if (vel3) { vel3[3 * i] = s->h4b[i].x; vel3[3 * i + 1] = s->h4b[i].y; vel3[3 * i + 2] = s->h4b[i].z; }
+    if (avel3) { avel3[3 * i] = s->h4c[i].x; avel3[3 * i + 1] = s->h4c[i].y; avel3[3 * i + 2] = s->h4c[i].z; }
+    if (type) { int t; std::memcpy(&t, &s->h4b[i].w, 4); type[i] = (uint)t; }
+    if (pid) pid[i] = s->hpid[i];
+  }
+  return st;
+}
+
+void free_sim(blaze_sim* s) {
+  if (!s) return;
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  for (int b = 0; b < 3; ++b) { f(s->S[b].pos); f(s->S[b].vel); f(s->S[b].angv); }
+  for (int b = 0; b < 2; ++b) { f(s->ob.pid[b]); f(s->ob.lift[b]); f(s->rs.keys[b]); f(s->rs.vals[b]); }
+  f(s->rs.counts); f(s->rs.totals); f(s->cstart); f(s->cend); f(s->nl.idx); f(s->nl.cnt);
+  f(s->ctl); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
+  f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  for (void* hp : {(void*)s->h4a, (void*)s->h4b, (void*)s->h4c, (void*)s->hpid})
+    if (hp) cudaFreeHost(hp);
+  for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
+                int n_d, const SimulationInfo* si, const blaze_options* opt) {
+  if (!out || !si || n_w < 0 || n_w > 8 || n_p < 1 || n_p > kMaxTypes || n_d < 0 ||
+      n_d > kMaxDobj || si->Num_Particles <= 0 || (n_w && !w) || !p || (n_d && !d))
+    return -1;
+  if (si->particle_type != 0) {
+    std::fprintf(stderr, "blaze: polyhedral particles are not supported by this library\n");
+    return -1;
+  }
+  blaze_sim* s = new (std::nothrow) blaze_sim();
+  if (!s) return -1;
+  s->n_max = si->Num_Particles;
+  s->si = *si;
+  s->si.Num_ParticlesPerObject = nullptr;
+  if (n_w) std::memcpy(s->w, w, sizeof(WOBJ) * n_w);
+  std::memcpy(s->p, p, sizeof(POBJ) * n_p);
+  if (n_d) std::memcpy(s->d, d, sizeof(DOBJ) * n_d);
+  s->n_w = n_w; s->n_p = n_p; s->n_d = n_d;
+  s->num_wobj = si->Num_WorldObjects;
+  if (opt) s->opt = *opt;
+  else blaze_default_options(&s->opt);
+  if (s->opt.max_nbr <= 0) s->opt.max_nbr = 32;
+  const int n = s->n_max;
+  auto fail = [&](int rc) { free_sim(s); return rc; };
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+#define CKF(x) do { cudaError_t e2 = (x); if (e2 != cudaSuccess) return fail(cuda_fail(e2)); } while (0)
+  for (int b = 0; b < 3; ++b) {
+    CKF(dalloc(&s->S[b].pos, n)); CKF(dalloc(&s->S[b].vel, n)); CKF(dalloc(&s->S[b].angv, n));
+  }
+  for (int b = 0; b < 2; ++b) {
+    CKF(dalloc(&s->ob.pid[b], n));
+    CKF(dalloc(&s->ob.lift[b], n));
+    CKF(dalloc(&s->rs.keys[b], n));
+    CKF(dalloc(&s->rs.vals[b], n));
+  }
+  const int tiles = (n + kTileKeys - 1) / kTileKeys;
+  s->rs.max_n = n;
+  s->rs.max_tiles = tiles;
+  CKF(dalloc(&s->rs.counts, (size_t)kRadixDigits * std::max(tiles, 1)));
+  CKF(dalloc(&s->rs.totals, kRadixDigits));
+  CKF(dalloc(&s->dp, 1));
+  CKF(dalloc(&s->ctl, 1));
+  CKF(cudaMallocHost((void**)&s->h_ctl, sizeof(StepCtl)));
+  CKF(cudaMallocHost((void**)&s->h4a, sizeof(float4) * n));
+  CKF(cudaMallocHost((void**)&s->h4b, sizeof(float4) * n));
+  CKF(cudaMallocHost((void**)&s->h4c, sizeof(float4) * n));
+  CKF(cudaMallocHost((void**)&s->hpid, sizeof(int) * n));
+  std::memset(s->h_ctl, 0, sizeof(StepCtl));
+  s->h_ctl->n_cur = n;
+  s->h_ctl->rebuild_req = 1;
+  CKF(cudaMemcpy(s->ctl, s->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice));
+  int rc = upload_params(s);
+  if (rc) return fail(rc);
+  uint32_t top = s->hp.ncell_tab + 1u;
+  s->key_bits = 1;
+  while (s->key_bits < 32 && (top >> s->key_bits) != 0) s->key_bits++;
+  CKF(dalloc(&s->cstart, s->hp.ncell_tab));
+  CKF(dalloc(&s->cend, s->hp.ncell_tab));
+  CKF(cudaMemset(s->cstart, 0xff, sizeof(uint32_t) * s->hp.ncell_tab));
+  CKF(cudaMemset(s->cend, 0xff, sizeof(uint32_t) * s->hp.ncell_tab));
+  rc = alloc_nlist(s);
+  if (rc) return fail(rc);
+  rc = alloc_capture(s);
+  if (rc) return fail(rc);
+  // zero state until the caller sets one (Set_Init_Config_Device zeroes velocities)
+  for (int b = 0; b < 3; ++b) {
+    CKF(cudaMemset(s->S[b].pos, 0, sizeof(float4) * n));
+    CKF(cudaMemset(s->S[b].vel, 0, sizeof(float4) * n));
+    CKF(cudaMemset(s->S[b].angv, 0, sizeof(float4) * n));
+  }
+  for (int b = 0; b < 2; ++b) {
+    CKF(cudaMemset(s->ob.pid[b], 0, sizeof(int) * n));
+    CKF(cudaMemset(s->ob.lift[b], 0xff, sizeof(int) * n));
+  }
+  CKF(cudaDeviceSynchronize());
+#undef CKF
+  *out = s;
+  return 0;
+}
+
+}  // namespace
+
+// ======================================================================= ABI
+extern "C" {
+
+void blaze_default_options(blaze_options* o) {
+  if (!o) return;
+  o->skin = 0.0f;
+  o->max_nbr = 32;
+  o->wall_grid = 1;
+  o->use_graph = 0;
+  o->capture_forces = 0;
+  o->sync_each_step = 0;
+}
+
+int blaze_create(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
+                 int n_d, const SimulationInfo* si, const blaze_options* opt) {
+  return create_impl(out, w, n_w, p, n_p, d, n_d, si, opt);
+}
+
+int blaze_destroy(blaze_sim* s) {
+  if (!s) return -1;
+  if (s == g_default) g_default = nullptr;
+  cudaStreamSynchronize(s->stream);
+  free_sim(s);
+  return 0;
+}
+
+int blaze_set_options(blaze_sim* s, const blaze_options* opt) {
+  if (!s || !opt) return -1;
+  const blaze_options old = s->opt;
+  s->opt = *opt;
+  if (s->opt.max_nbr <= 0) s->opt.max_nbr = 32;
+  CK(cudaStreamSynchronize(s->stream));
+  int rc = 0;
+  if (s->opt.max_nbr != old.max_nbr) rc = alloc_nlist(s);
+  if (!rc) rc = alloc_capture(s);
+  if (!rc) rc = upload_params(s);
+  // a new skin or capacity invalidates the current list
+  s->h_ctl->rebuild_req = 1;
+  CK(cudaMemcpy(&s->ctl->rebuild_req, &s->h_ctl->rebuild_req, sizeof(int), cudaMemcpyHostToDevice));
+  return rc;
+}
+
+int blaze_set_cylinder_rotation(blaze_sim* s, int on) {
+  if (!s) return -1;
+  s->cyl_rot = on ? 1 : 0;
+  s->hp.cyl_rot = s->cyl_rot;
+  CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int blaze_set_state(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
+                    const uint* type, const int* pid) {
+  if (!s || !pos3 || !type || !pid) return -1;
+  return set_state_impl(s, pos3, vel3, avel3, type, pid);
+}
+
+int blaze_get_state(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid) {
+  if (!s) return -1;
+  return get_state_impl(s, pos3, vel3, avel3, type, pid);
+}
+
+int blaze_step(blaze_sim* s, int nsteps) {
+  if (!s || nsteps < 0) return -1;
+  s->last_launches = 0;
+  for (int k = 0; k < nsteps; ++k) {
+    int rc = enqueue_step(s);
+    if (rc) return rc;
+    if (s->opt.sync_each_step) {
+      rc = sync_status(s);
+      if (rc != 0) return rc;
+    }
+  }
+  CK(cudaGetLastError());
+  return s->opt.sync_each_step ? (int)s->status : 0;
+}
+
+int blaze_sync(blaze_sim* s) {
+  if (!s) return -1;
+  return sync_status(s);
+}
+
+int blaze_num_current(blaze_sim* s) {
+  if (!s) return -1;
+  int rc = sync_status(s);
+  if (rc < 0) return rc;
+  return s->h_ctl->n_cur - s->h_ctl->pending_dead;
+}
+
+int blaze_num_rebuilds(blaze_sim* s) {
+  if (!s) return -1;
+  int rc = sync_status(s);
+  if (rc < 0) return rc;
+  return s->h_ctl->epoch;
+}
+
+int blaze_update_wobj(blaze_sim* s, const WOBJ* w, int n_w) {
+  if (!s || !w || n_w < 0 || n_w > 8) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(s->w, w, sizeof(WOBJ) * n_w);
+  // moving geometry: the per-cell culling lists would go stale
+  s->walls_static = false;
+  return upload_params(s);
+}
+
+int blaze_update_dobj(blaze_sim* s, const DOBJ* d, int n_d) {
+  if (!s || !d || n_d < 0 || n_d > kMaxDobj) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(s->d, d, sizeof(DOBJ) * n_d);
+  build_params(s);
+  CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int blaze_get_forces(blaze_sim* s, float* f_pp, float* t_pp, float* f_w, float* t_w, float* f_l,
+                     float* t_l) {
+  if (!s || !s->cap_alloc) return -1;
+  int st = sync_status(s);
+  if (st < 0) return st;
+  float* dst[6] = {f_pp, t_pp, f_w, t_w, f_l, t_l};
+  float* src[6] = {s->cap.f_pp, s->cap.t_pp, s->cap.f_w, s->cap.t_w, s->cap.f_l, s->cap.t_l};
+  for (int q = 0; q < 6; ++q)
+    if (dst[q]) CK(cudaMemcpy(dst[q], src[q], sizeof(float) * 3 * s->n_max, cudaMemcpyDeviceToHost));
+  return st;
+}
+
+int blaze_get_nlist(blaze_sim* s, uint* nn, uint* list) {
+  if (!s || !nn || !list) return -1;
+  int st = sync_status(s);
+  if (st < 0) return st;
+  const int n = s->n_max, cap = s->nl.cap;
+  std::vector<uint32_t> cnt(n), idx((size_t)n * cap);
+  CK(cudaMemcpy(cnt.data(), s->nl.cnt, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(idx.data(), s->nl.idx, sizeof(uint32_t) * (size_t)n * cap, cudaMemcpyDeviceToHost));
+  const int live = s->h_ctl->n_cur;
+  for (int i = 0; i < n; ++i) {
+    nn[i] = i < live ? cnt[i] : 0u;
+    for (int k = 0; k < cap; ++k)
+      list[(size_t)i * cap + k] = (i < live && k < (int)cnt[i]) ? idx[(size_t)k * n + i] : 0u;
+  }
+  return st;
+}
+
+int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, void** stream) {
+  if (!s) return -1;
+  if (pos4) *pos4 = s->S[s->cur].pos;
+  if (vel4) *vel4 = s->S[s->cur].vel;
+  if (angv4) *angv4 = s->S[s->cur].angv;
+  if (stream) *stream = (void*)s->stream;
+  return 0;
+}
+
+int blaze_last_launches(blaze_sim* s) { return s ? s->last_launches : -1; }
+
+int blaze_set_profile(blaze_sim* s, int on) {
+  if (!s) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  s->profile = on != 0;
+  s->ev_marks.clear();
+  s->ev_used = 0;
+  return 0;
+}
+
+int blaze_profile(blaze_sim* s, float* ms_rebuild, float* ms_step, int* n_steps) {
+  if (!s) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  float tot[2] = {0.0f, 0.0f};
+  int steps = 0;
+  for (size_t k = 0; k + 1 < s->ev_marks.size(); k += 2) {
+    const int ph = s->ev_marks[k].first;
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, s->ev_pool[s->ev_marks[k].second], s->ev_pool[s->ev_marks[k + 1].second]));
+    tot[ph] += ms;
+    if (ph == 1) steps++;
+  }
+  if (ms_rebuild) *ms_rebuild = tot[0];
+  if (ms_step) *ms_step = tot[1];
+  if (n_steps) *n_steps = steps;
+  s->ev_marks.clear();
+  s->ev_used = 0;
+  return 0;
+}
+
+blaze_sim* blaze_default_sim(void) { return g_default; }
+
+// --------------------------------------------- reference interface (Part 1)
+int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_DynamicOBJ,
+                              SimulationInfo* h_SimInfo, int h_Num_WorldOBJ,
+                              int h_Num_ParticleOBJ, int h_Num_DynamicOBJ,
+                              InitConfig* h_PosConfig) {
+  (void)h_PosConfig;  // initial lattices / fill waves are produced by the caller
+  if (g_default) {
+    blaze_destroy(g_default);
+    g_default = nullptr;
+  }
+  blaze_sim* s = nullptr;
+  int rc = create_impl(&s, h_WorldOBJ, h_Num_WorldOBJ, h_ParticleOBJ, h_Num_ParticleOBJ,
+                       h_DynamicOBJ, h_Num_DynamicOBJ, h_SimInfo, nullptr);
+  if (rc) return rc;
+  g_default = s;
+  return 0;
+}
+
+#define DEF_SIM()             \
+  blaze_sim* s = g_default;   \
+  if (!s) return -2
+
+int Device_Set_Pos(float3* h_pos, Quaterion* h_Ornt, uint* h_ptype, int* h_pid) {
+  (void)h_Ornt;
+  DEF_SIM();
+  return set_state_impl(s, (const float*)h_pos, nullptr, nullptr, h_ptype, h_pid);
+}
+
+int Device_Set_Pos_Velocity(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            uint* h_ptype, int* h_pid) {
+  (void)h_Ornt;
+  DEF_SIM();
+  return set_state_impl(s, (const float*)h_pos, (const float*)h_vel, (const float*)h_Avel,
+                        h_ptype, h_pid);
+}
+
+int Device_Set_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            float3* h_acc, uint* h_ptype, int* h_pid) {
+  (void)h_Ornt;
+  (void)h_acc;
+  DEF_SIM();
+  return set_state_impl(s, (const float*)h_pos, (const float*)h_vel, (const float*)h_Avel,
+                        h_ptype, h_pid);
+}
+
+int Device_Set_Tallys(float* h_Tallys) {
+  DEF_SIM();
+  if (!h_Tallys) return -1;
+  for (int k = 0; k < 3; ++k) s->tallies[k] = h_Tallys[k];
+  return 0;
+}
+
+int Device_Get_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
+                            float3* h_acc, uint* h_ptype, int* h_pid) {
+  (void)h_acc;
+  DEF_SIM();
+  int rc = get_state_impl(s, (float*)h_pos, (float*)h_vel, (float*)h_Avel, h_ptype, h_pid);
+  if (rc >= 0 && h_Ornt && s->si.sphere_orient)
+    for (int i = 0; i < s->n_max; ++i) h_Ornt[i] = Quaterion{1.0f, 0.0f, 0.0f, 0.0f};
+  return rc;
+}
+
+int Device_Get_P_Positions(float3* Pos, Quaterion* Quart_ornt, uint* h_ptype, int* h_pid) {
+  (void)Quart_ornt;
+  DEF_SIM();
+  return get_state_impl(s, (float*)Pos, nullptr, nullptr, h_ptype, h_pid);
+}
+
+int Device_Get_P_Velocity(float3* H_Vel, float3* H_Rvel, int Flag, uint* h_ptype, int* h_pid) {
+  DEF_SIM();
+  return get_state_impl(s, nullptr, (float*)H_Vel, Flag == 1 ? (float*)H_Rvel : nullptr, h_ptype,
+                        h_pid);
+}
+
+int Device_Get_W_Forces(float3* WallForces, float3* WallContact_Point) {
+  (void)WallContact_Point;
+  DEF_SIM();
+  if (!WallForces) return -1;
+  if (!s->cap_alloc) {
+    // wall forces are only materialised when the step keeps its forces
+    std::memset(WallForces, 0, sizeof(float3) * s->n_max);
+    return -1;
+  }
+  return blaze_get_forces(s, nullptr, nullptr, (float*)WallForces, nullptr, nullptr, nullptr);
+}
+
+int Device_Get_Energy(float* Energy) {
+  DEF_SIM();
+  if (!Energy) return -1;
+  for (int k = 0; k < 3; ++k) Energy[k] = s->tallies[k] * 1E-4f;
+  return 0;
+}
+
+int Device_Update_DObjectPostions(DOBJ* h_DynamicOBJ) {
+  DEF_SIM();
+  return blaze_update_dobj(s, h_DynamicOBJ, s->n_d);
+}
+
+int Device_Update_WorldObjectPostions(WOBJ* h_WorldOBJ) {
+  DEF_SIM();
+  return blaze_update_wobj(s, h_WorldOBJ, s->n_w);
+}
+
+int Device_OpenHatch(WOBJ* h_WorldOBJ, int h_Num_WorldOBJ) {
+  DEF_SIM();
+  if (!h_WorldOBJ || h_Num_WorldOBJ < 0 || h_Num_WorldOBJ > 8) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(s->w, h_WorldOBJ, sizeof(WOBJ) * h_Num_WorldOBJ);
+  s->num_wobj = s->num_wobj - 1;  // Hatch(): the last world object is dropped
+  return upload_walls(s);
+}
+
+int Device_Clean(void) {
+  if (!g_default) return 0;
+  return blaze_destroy(g_default);
+}
+
+int Device_Reset_Energy(int num_values) {
+  DEF_SIM();
+  if (num_values <= 3)
+    for (int k = 0; k < 3; ++k) s->tallies[k] = 0.0f;
+  return 0;
+}
+
+int drum_rotation(bool cylinder_rotation) {
+  DEF_SIM();
+  return blaze_set_cylinder_rotation(s, cylinder_rotation ? 1 : 0);
+}
+
+int Start_Bin(void) { return 0; }
+
+int Device_AddForce(void) { DEF_SIM(); s->fc += 10.0f; return 0; }
+int Device_SubForce(void) { DEF_SIM(); s->fc -= 10.0f; return 0; }
+int Device_ZeroForce(void) { DEF_SIM(); s->fc = 0.0f; return 0; }
+
+int Device_DEM_UpdateSim(void) {
+  DEF_SIM();
+  return blaze_step(s, 1);
+}
+
+}  // extern "C"

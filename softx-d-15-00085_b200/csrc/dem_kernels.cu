@@ -1,0 +1,638 @@
+// dem_kernels.cu -- the per-step kernels of the sphere DEM path.
+//
+// Compiled with -fmad=false: every FP32 expression below keeps the operation
+// order of the reference source it cites, and with no contraction to FMA the
+// results equal the reference's bit for bit.
+//
+//   k_gate     one thread: latch the rebuild request for this step
+//   k_hash     cell key per particle          (BroadPhase.cuh:20-100)
+//   [radix sort, radix_sort.cu]               (BroadPhase.cuh:110-117)
+//   k_reorder  gather state into sorted order + cell start/end table
+//                                             (BroadPhase.cuh:126-325)
+//   k_nlist    27-cell neighbour search       (BroadPhase.cuh:335-513)
+//   k_step     particle-particle law + volume objects + world objects +
+//              symplectic Euler, fused, one thread per particle, gather only
+//                                             (DEM_Kernels_Compute.cuh:12-729,
+//                                              Collision_Response.cuh,
+//                                              Integration.cuh:6-184)
+#include "dem_kernels.cuh"
+
+namespace blaze {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int3 grid_pos(const SimParams& P, float3 p) {
+  int3 g;
+  g.x = (int)floorf((p.x - P.origin.x) / P.cell.x);
+  g.y = (int)floorf((p.y - P.origin.y) / P.cell.y);
+  g.z = (int)floorf((p.z - P.origin.z) / P.cell.z);
+  return g;
+}
+__device__ __forceinline__ uint32_t grid_hash(const SimParams& P, int3 g) {
+  return (uint32_t)((g.x + g.z * P.ncells.z) + (g.y * P.ncells.x) * P.ncells.z);
+}
+__device__ __forceinline__ bool in_grid(const SimParams& P, int3 g) {
+  return g.x >= 0 && g.y >= 0 && g.z >= 0 && g.x < P.ncells.x && g.y < P.ncells.y &&
+         g.z < P.ncells.z;
+}
+__device__ __forceinline__ void flag_status(StepCtl* ctl, uint32_t bits) {
+  // one atomic per warp
+  const unsigned m = __activemask();
+  const uint32_t all = __reduce_or_sync(m, bits);
+  if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
+}
+
+// --------------------------------------------------------------------- gate
+__global__ void k_gate(StepCtl* ctl) {
+  const int r = ctl->rebuild_req;
+  ctl->rebuilt = r;
+  ctl->rebuild_req = 0;
+}
+
+// --------------------------------------------------------------------- hash
+// Kernel_SpatialDecomp_CalcPHash (Collision_Detection_BroadPhase.cuh:75-100).
+// Removed particles (pid -1) take the largest key so they sort last, as the
+// reference's parking position max_size makes them; a live particle outside
+// the grid takes the key just below (the reference's table would be indexed
+// out of range) and raises kStatusOutOfGrid.
+__global__ void __launch_bounds__(kThreads)
+k_hash(const SimParams* __restrict__ P, const float4* __restrict__ pos, OrderBuf ob, int n_max,
+       uint32_t* __restrict__ keys, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_max) return;
+  const int* pid = (ctl->epoch & 1) ? ob.pid[1] : ob.pid[0];
+  uint32_t key;
+  uint32_t st = 0;
+  if (pid[i] < 0) {
+    key = P->ncell_tab + 1u;
+  } else {
+    const float4 p = pos[i];
+    const int3 g = grid_pos(*P, xyz(p));
+    if (in_grid(*P, g)) {
+      key = grid_hash(*P, g);
+    } else {
+      key = P->ncell_tab;
+      st = kStatusOutOfGrid;
+    }
+  }
+  keys[i] = key;
+  flag_status(ctl, st);
+}
+
+// ------------------------------------------------------------------ reorder
+// Kernel_SortArrays + Kernel_SpatialDecomp_ReorderPDA + Kernel_SpatialDecomp_BinData
+// (BroadPhase.cuh:126-325), as one gather into the spare buffer.
+__global__ void __launch_bounds__(kThreads)
+k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
+          const uint32_t* __restrict__ keys, const int32_t* __restrict__ perm,
+          uint32_t* __restrict__ cstart, uint32_t* __restrict__ cend, uint32_t ncell_tab,
+          int has_lift, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = ctl->epoch & 1;
+  if (i == 0) {
+    // the particles removed since the last re-sort are now at the end
+    ctl->n_cur -= ctl->pending_dead;
+    ctl->pending_dead = 0;
+  }
+  if (i >= n_max) return;
+  const int j = perm[i];
+  dst.pos[i] = src.pos[j];
+  dst.vel[i] = src.vel[j];
+  float4 w = src.angv[j];
+  w.w = 0.0f;
+  dst.angv[i] = w;
+  const int* pid_src = e ? ob.pid[1] : ob.pid[0];
+  int* pid_dst = e ? ob.pid[0] : ob.pid[1];
+  pid_dst[i] = pid_src[j];
+  if (has_lift) {
+    const int* l_src = e ? ob.lift[1] : ob.lift[0];
+    int* l_dst = e ? ob.lift[0] : ob.lift[1];
+    l_dst[i] = l_src[j];
+  }
+  const uint32_t k = keys[i];
+  if (k < ncell_tab) {
+    if (i == 0 || keys[i - 1] != k) cstart[k] = (uint32_t)i;
+    if (i == n_max - 1 || keys[i + 1] != k) cend[k] = (uint32_t)i + 1u;
+  }
+}
+
+// -------------------------------------------------------------------- nlist
+// Kernel_BroadCollisionDetection_NonSymmetry (BroadPhase.cuh:402-513) with
+// CollisionDetection_Filter_SphereNNCell (BroadPhase.cuh:335-392): the
+// clamped 3x3x3 block scanned in y, z, x order, j ascending inside a cell,
+// pairs kept when |xi - xj| - (ri + rj) < skin (skin 0: the reference's
+// contacts-only list).  Slots beyond the capacity are dropped and flagged
+// (the reference writes past its 32-slot row).
+__global__ void __launch_bounds__(kThreads)
+k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_max,
+        const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, NbrList nl,
+        StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ctl->epoch += 1;
+  const int n = ctl->n_cur;
+  if (i >= n) return;
+  const float4 pa4 = pos[i];
+  const float3 pa = xyz(pa4);
+  const float ra = pa4.w;
+  const float skin = P->skin;
+  const int3 g = grid_pos(*P, pa);
+  uint32_t cnt = 0;
+  uint32_t st = 0;
+  if (in_grid(*P, g)) {
+    const int xs = g.x == 0 ? 0 : -1, xe = g.x == P->ncells.x - 1 ? 0 : 1;
+    const int ys = g.y == 0 ? 0 : -1, ye = g.y == P->ncells.y - 1 ? 0 : 1;
+    const int zs = g.z == 0 ? 0 : -1, ze = g.z == P->ncells.z - 1 ? 0 : 1;
+    for (int y = ys; y <= ye; ++y)
+      for (int z = zs; z <= ze; ++z)
+        for (int x = xs; x <= xe; ++x) {
+          const uint32_t h = grid_hash(*P, make_int3(g.x + x, g.y + y, g.z + z));
+          const uint32_t s = __ldg(cstart + h);
+          if (s == 0xffffffffu) continue;
+          const uint32_t e = __ldg(cend + h);
+          for (uint32_t j = s; j < e; ++j) {
+            if ((int)j == i) continue;
+            const float4 pb = __ldg(pos + j);
+            const float sep = len3(pa - xyz(pb)) - (ra + pb.w);
+            if (sep < skin) {
+              if (cnt < (uint32_t)nl.cap) nl.idx[(size_t)cnt * nl.stride + i] = j;
+              else st |= kStatusListOverflow;
+              ++cnt;
+            }
+          }
+        }
+  }
+  nl.cnt[i] = cnt < (uint32_t)nl.cap ? cnt : (uint32_t)nl.cap;
+  flag_status(ctl, st);
+}
+
+// ------------------------------------------------------------ contact laws
+struct Forces { float3 trans, torque; };
+
+// Collision_Response_Particle_Particle, Collision_Response.cuh:374-494
+// (energy tallies excluded).
+__device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
+                                         float3 ra, float3 rb, float3 wa, float3 wb,
+                                         const PP_Parms& pp, float3 va, float3 vb, float ma,
+                                         float mb) {
+  Forces F;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = pp.Kn * pen;
+  const float3 fdiss = pp.Cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 vcpa = va + cross3(wa, ra);
+  const float3 vcpb = vb + cross3(wb, rb);
+  const float3 vcpna = dot3(vcpa, n) * n;
+  const float3 vcpnb = dot3(vcpb, n) * n;
+  const float3 vt = (vcpa - vcpna) - (vcpb - vcpnb);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = ((((0.50f * (ma + mb)) / P.dt) * 0.050f) * pp.Fric_kinetic) * (mag / velf);
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109
+__device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 pvel, float3 n,
+                                                     float pen, float3 r, float3 w,
+                                                     const TypeParams& T) {
+  Forces F;
+  const float3 vn = dot3(pvel, n) * n;
+  const float fn = T.s_kn * pen;
+  const float3 fdiss = T.s_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  float3 vt = pvel - vn;
+  if (P.rotation) vt = vt + cross3(w, r);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(pvel, pvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.s_mus * (mag / velf));
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_MovingSurface, Collision_Response.cuh:116-233
+__device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 n, float pen,
+                                                     float3 r, float3 w, const TypeParams& T,
+                                                     float3 va, float3 vs) {
+  Forces F;
+  const float3 rvel = va - vs;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = T.s_kn * pen;
+  const float3 fdiss = T.s_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  const float3 vcpa = va + cross3(w, r);
+  const float3 vcpna = dot3(vcpa, n) * n;
+  const float3 vt = (vcpa - vcpna) - (vs - dot3(vs, n) * n);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = T.s_muk * (mag / velf);
+    ft = (((-1.0f * tan_f) * (vt / mag)) * (T.mass / P.dt)) * 0.050f;
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_VolumeObject, Collision_Response.cuh:241-363,
+// with the zero object spin and lever the caller passes
+// (DEM_Kernels_Compute.cuh:206-216).
+__device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float pen, float3 r,
+                                             float3 w, const TypeParams& T, float3 va,
+                                             float3 vobj) {
+  Forces F;
+  const float3 rvel = va - vobj;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = T.d_kn * pen;
+  const float3 fdiss = T.d_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  const float3 z = f3(0.0f, 0.0f, 0.0f);
+  const float3 vcpa = va + cross3(w, r);
+  const float3 vcpb = vobj + cross3(z, z);
+  const float3 vt = (vcpa - dot3(vcpa, n) * n) - (vcpb - dot3(vcpb, n) * n);
+  float mag = dot3(vt, vt);
+  float3 ft = z;
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.d_muk * (mag / velf));
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : z;
+  return F;
+}
+
+// Collision_Response_EndPlate_Particle, Collision_Response.cuh:504-526
+__device__ __forceinline__ float3 law_end_plate(float3 rvel, float3 n, float pen,
+                                                const TypeParams& T) {
+  const float3 vn = dot3(rvel, n) * n;
+  const float3 fdiss = T.s_cn * vn;
+  const float fn = T.s_kn * pen;
+  return fn * n - fdiss;
+}
+
+// is_PointOnSurface, Utilities.cuh:20-53
+__device__ __forceinline__ bool point_on_polygon(int nv, const float3* v, float3 pt, float sarea,
+                                                 float tol) {
+  float area = 0.0f;
+  for (int i = 0; i < nv - 1; ++i) {
+    const float3 v1 = pt - v[i];
+    const float3 v2 = pt - v[i + 1];
+    area = area + 0.500000f * len3(cross3(v1, v2));
+  }
+  const float3 v1 = pt - v[nv - 1];
+  const float3 v2 = pt - v[0];
+  area = area + 0.500000f * len3(cross3(v1, v2));
+  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
+}
+
+__device__ __forceinline__ float3 drum_velocity(const SimParams& P, float3 cp) {
+  return cross3(f3(0.0f, 0.0f, -P.mill_rot_vel), cp - f3(P.drum_r, P.drum_r, 0.0f));
+}
+
+// WorldObject_InteractionParticle for spheres (DEM_Kernels_Compute.cuh:254-610):
+// one op per face / plane / cylinder / cap in world-object order.
+__device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& op, float3 p,
+                                              float r, float3 v, float3 w, const TypeParams& T,
+                                              float3& fw, float3& tw) {
+  if (op.kind == kOpFace || op.kind == kOpPlane) {
+    // Collision_Detection_Sphere_Surface / _Plane, Collision_Detection_Spheres.cuh:6-100
+    const float3 pt = p - r * op.n;
+    float dis = dot3(op.n, pt - op.c);
+    if (!(dis < 0.000000f && dis > -r)) return;
+    dis = fabsf(dis);
+    if (op.kind == kOpFace) {
+      const float3 q = pt + op.n * dis;
+      if (!point_on_polygon(op.nv, op.v, q, op.area, op.tol)) return;
+    }
+    Forces F;
+    if (P.rotating_wobj && P.cyl_rot)
+      F = law_moving_surface(P, op.n, dis, pt - p, w, T, v, drum_velocity(P, pt));
+    else
+      F = law_static_surface(P, v, op.n, dis, pt - p, w, T);
+    fw = fw + F.trans;
+    if (P.rotation) tw = tw + F.torque;
+  } else if (op.kind == kOpCylinder) {
+    // Collision_Detection_Sphere_Cylinder, Collision_Detection_Spheres.cuh:234-265
+    const float3 pv = vmul(p, op.axis) - op.cbot;
+    const float pd = len3(pv) + r;
+    if (!(pd > op.radius)) return;
+    float3 nrm = f3(-pv.x, -pv.y, -pv.z);
+    nrm = nrm * (1.0f / len3(nrm));
+    const float3 cp = p - nrm * r;
+    const float dis = fabsf(pd - op.radius);
+    Forces F;
+    if (P.cyl_rot)
+      F = law_moving_surface(P, nrm, dis, cp - p, w, T, v, drum_velocity(P, cp));
+    else
+      F = law_static_surface(P, v, nrm, dis, cp - p, w, T);
+    fw = F.trans;
+    if (P.rotation) tw = tw + F.torque;
+  } else {
+    // end plates: Collision_Detection_Sphere_Plane + Collision_Response_EndPlate_Particle
+    const float3 pt = p - r * op.n;
+    float dis = dot3(op.n, pt - op.c);
+    if (!(dis < 0.000000f && dis > -r)) return;
+    dis = fabsf(dis);
+    fw = law_end_plate(v, op.n, dis, T);
+  }
+}
+
+// Collision_Detection_Sphere_DObject, Collision_Detection_Spheres.cuh:108-225
+struct DobjHit { bool hit; int type; float dis; float3 n, cp; };
+__device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, float r,
+                                                  int hist_type) {
+  DobjHit c;
+  c.hit = false;
+  c.type = 0;
+  if (hist_type != 2) {
+    for (int j = 0; j < D.num_faces; ++j) {
+      const Surface& s = D.faces[j];
+      const float3 pt = p - r * s.normal;
+      float dis = dot3(s.normal, pt - s.centroid);
+      if (dis < 0.000000f && dis > -r * 0.50f) {
+        dis = fabsf(dis);
+        const float3 q = pt + s.normal * dis;
+        float3 pv[4];
+        const int nv = s.num_vertex < 4 ? s.num_vertex : 4;
+        for (int k = 0; k < nv; ++k) pv[k] = D.vert[s.vertex_Order[k] & 7];
+        if (point_on_polygon(nv, pv, q, s.area, s.Tol)) {
+          c.hit = true; c.type = 1; c.dis = dis; c.n = s.normal; c.cp = pt;
+          return c;
+        }
+      }
+    }
+  }
+  for (int e = 0; e < D.num_edges; ++e) {
+    const float3 p0 = D.vert[D.edge0[e]];
+    const float3 dir = D.vert[D.edge1[e]] - p0;
+    const float3 edir = dir / len3(dir);
+    const float dvec = dot3(edir, p - p0);
+    if (dvec > 0) {
+      const float3 p2 = p0 + dvec * edir;
+      const float3 d2 = p - p2;
+      const float d = len3(d2);
+      if (d < r) {
+        const float dis = fabsf(d - r);
+        if (dis < r) {
+          c.n = d2 * (1.0f / len3(d2));
+          c.cp = f3(0.0f, 0.0f, 0.0f);
+          c.type = 2; c.hit = true; c.dis = dis;
+          return c;
+        }
+      }
+    }
+  }
+  return c;
+}
+
+// ---------------------------------------------------------------------- step
+__global__ void __launch_bounds__(kThreads)
+k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGrid wg,
+       StateBuf in_plain, StateBuf in_sorted, StateBuf out, OrderBuf ob, int n_max,
+       NbrList nl, StepCtl* ctl, ForceCapture cap, int capture) {
+  __shared__ TypeParams sT[kMaxTypes];
+  {
+    const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
+    const int* src = reinterpret_cast<const int*>(Pg->types);
+    int* dst = reinterpret_cast<int*>(sT);
+    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  const SimParams& P = *Pg;
+  const bool rebuilt = ctl->rebuilt != 0;
+  const StateBuf in = rebuilt ? in_sorted : in_plain;
+  const int n = ctl->n_cur;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_max) return;
+  if (i >= n) {  // removed particles keep their parked state
+    out.pos[i] = in.pos[i];
+    out.vel[i] = in.vel[i];
+    out.angv[i] = in.angv[i];
+    return;
+  }
+  const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
+  const float3 pa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
+  const int ta = __float_as_int(va4.w);
+  const TypeParams& TA = sT[ta & (kMaxTypes - 1)];
+  const float ma = TA.mass, ra = pa4.w;
+  uint32_t st = (ta < 0 || ta >= P.n_types) ? kStatusTypeRange : 0u;
+
+  // particle-particle (Kernel_ParticleInteraction_Spheres_NonSymmetry)
+  float3 f = P.gravity * ma;
+  float3 fl = f3(0.0f, 0.0f, 0.0f);
+  const int cnt = (int)nl.cnt[i];
+  for (int k = 0; k < cnt; ++k) {
+    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
+    const float4 pb4 = __ldg(in.pos + j);
+    const float3 rel = pa - xyz(pb4);
+    const float dist = len3(rel);
+    if (!(dist - (ra + pb4.w) < 0.0f)) continue;  // skin candidate not in contact
+    const float4 vb4 = __ldg(in.vel + j);
+    const float4 wb4 = __ldg(in.angv + j);
+    const int tb = __float_as_int(vb4.w);
+    const float3 vb = xyz(vb4);
+    const float3 nrm = rel / dist;
+    const float dis = fabsf(dist - (ra + pb4.w)) + 0.000010f;
+    const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
+    const Forces F = law_pp(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
+                            pp, va, vb, ma, sT[tb & (kMaxTypes - 1)].mass);
+    f = f + F.trans;
+    fl = fl + F.torque;
+  }
+  const float3 f_pp = f;
+  const float3 t_pp = P.rotation ? fl : f3(0.0f, 0.0f, 0.0f);
+
+  // volume objects (VolumeObject_InteractionParticle, DEM_Kernels_Compute.cuh:12-246)
+  float3 f_l = f3(0.0f, 0.0f, 0.0f), t_l = f3(0.0f, 0.0f, 0.0f);
+  if (P.n_dobj > 0) {
+    int* lift = (ctl->epoch & 1) ? ob.lift[1] : ob.lift[0];
+    const int hist = lift[i];
+    int colltype = 0;
+    bool outer = P.dobj[0].translating || !P.is_mill || P.rotating_wobj;
+    if (!outer) outer = len3(f3(pa.x, pa.y, 0.0f) - P.cent) > (P.dobj_cyl_bound_r - 2.0f * TA.radius);
+    if (outer) {
+      for (int d = 0; d < P.n_dobj; ++d) {
+        const DobjDev& D = P.dobj[d];
+        const float3 bv = vmul(pa - D.com, D.axis);
+        if (!(len3(bv) < (D.bound_r + TA.radius))) continue;
+        DobjHit c = sphere_dobject(D, pa, TA.radius, hist);
+        colltype = c.type;
+        if (c.hit) {
+          if (c.type == 2) c.cp = pa;
+          float3 vobj = f3(0.0f, 0.0f, 0.0f);
+          if (D.attached) vobj = drum_velocity(P, c.cp);
+          else if (D.translating) vobj = D.velocity;
+          const Forces F = law_volume(P, c.n, c.dis, c.cp - pa, wa, TA, va, vobj);
+          f_l = f_l + F.trans;
+          if (P.rotation) t_l = t_l + F.torque;
+          break;
+        }
+      }
+    }
+    lift[i] = colltype;
+  }
+
+  // world objects
+  float3 f_w = f3(0.0f, 0.0f, 0.0f), t_w = f3(0.0f, 0.0f, 0.0f);
+  if (wg.off != nullptr) {
+    const int3 g = grid_pos(P, pa);
+    if (in_grid(P, g)) {
+      const uint32_t h = grid_hash(P, g);
+      const uint32_t o0 = __ldg(wg.off + h), o1 = __ldg(wg.off + h + 1);
+      for (uint32_t q = o0; q < o1; ++q) apply_wall_op(P, ops[__ldg(wg.ops + q)], pa, ra, va, wa, TA, f_w, t_w);
+    } else {
+      for (int q = 0; q < P.n_ops; ++q) apply_wall_op(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+    }
+  } else {
+    for (int q = 0; q < P.n_ops; ++q) apply_wall_op(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+  }
+  if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
+
+  // Integrate_Euler_NonSymmetry (Integration.cuh:6-184), spheres
+  float3 acc = f_w + f_pp;
+  if (P.n_dobj > 0) acc = acc + f_l;
+  acc = acc * (1.0f / ma);
+  float3 v = va + acc * P.dt;
+  const float3 p = pa + v * P.dt;
+  if (P.mode2d) v.z = 0.0f;
+  float3 tl = t_pp + t_w;
+  if (P.n_dobj > 0) tl = tl + t_l;
+  float3 w = wa;
+  if (P.rotation) {
+    if (dot3(tl, tl) > 0.0f) {
+      const float3 aa = TA.iinv * tl;
+      w = w + aa * P.dt;
+      w = w - w * P.roll_res;
+    }
+    if (P.mode2d) { w.x = 0.0f; w.y = 0.0f; }
+  }
+  float path = wa4.w;
+  if (P.skin > 0.0f) path = path + len3(v) * P.dt;
+  out.pos[i] = make_float4(p.x, p.y, p.z, ra);
+  out.vel[i] = make_float4(v.x, v.y, v.z, va4.w);
+  out.angv[i] = make_float4(w.x, w.y, w.z, path);
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
+
+  // Verlet-list validity: rebuild before any particle has moved half the
+  // skin; with no skin the contact list is rebuilt every step (reference).
+  if (P.skin <= 0.0f) {
+    if (i == 0) ctl->rebuild_req = 1;
+  } else {
+    const unsigned m = __activemask();
+    const unsigned b = __ballot_sync(m, path > 0.5f * P.skin);
+    if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicExch(&ctl->rebuild_req, 1);
+  }
+  flag_status(ctl, st);
+
+  if (capture) {
+    const float3 vals[6] = {f_pp, t_pp, f_w, t_w, f_l, t_l};
+    float* dsts[6] = {cap.f_pp, cap.t_pp, cap.f_w, cap.t_w, cap.f_l, cap.t_l};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      dsts[q][3 * i] = vals[q].x;
+      dsts[q][3 * i + 1] = vals[q].y;
+      dsts[q][3 * i + 2] = vals[q].z;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------- kill
+// Remove_Silo_Discharged_Particles / Remove_PL_Discharged_Particles
+// (GPU_Memory_Transfer.cuh:646-682): park at max_size, pid -1, count.  The
+// count is per check (the reference's Kill_count is never reset).
+__global__ void k_kill(StateBuf s, OrderBuf ob, int n_max, float kill_height, int rotating,
+                       float3 max_size, StepCtl* ctl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = ctl->n_cur;
+  if (i >= n || i >= n_max) return;
+  int* pid = (ctl->epoch & 1) ? ob.pid[1] : ob.pid[0];
+  if (pid[i] == -1) return;
+  const float4 p = s.pos[i];
+  bool kill;
+  if (rotating)
+    kill = p.z <= 41.0f || p.z >= 300 || p.y <= 50.0f || p.y >= 1500.0f || p.x <= 50.0f ||
+           p.x >= 1500.0f;
+  else
+    kill = p.y < kill_height;
+  if (kill) {
+    s.pos[i] = make_float4(max_size.x, max_size.y, max_size.z, p.w);
+    pid[i] = -1;
+    atomicAdd(&ctl->pending_dead, 1);
+    atomicAdd(&ctl->killed_total, 1);
+    ctl->rebuild_req = 1;
+  }
+}
+
+inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+void launch_gate(StepCtl* ctl, cudaStream_t st) { k_gate<<<1, 1, 0, st>>>(ctl); }
+
+void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
+                 uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st) {
+  k_hash<<<blocks(n_max), kThreads, 0, st>>>(dp, s.pos, ob, n_max, keys, ctl, gate);
+}
+
+void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
+                    const uint32_t* sorted_keys, const int32_t* perm, uint32_t* cell_start,
+                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, StepCtl* ctl,
+                    const int* gate, cudaStream_t st) {
+  k_reorder<<<blocks(n_max), kThreads, 0, st>>>(src, dst, ob, n_max, sorted_keys, perm, cell_start,
+                                                cell_end, ncell_tab, has_lift ? 1 : 0, ctl, gate);
+}
+
+void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
+                  const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
+                  cudaStream_t st) {
+  k_nlist<<<blocks(n_max), kThreads, 0, st>>>(dp, s.pos, n_max, cell_start, cell_end, nl, ctl,
+                                              gate);
+}
+
+void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
+                 const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
+                 NbrList nl, StepCtl* ctl, const ForceCapture* cap, cudaStream_t st) {
+  ForceCapture c = cap ? *cap : ForceCapture{};
+  k_step<<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl,
+                                             ctl, c, cap ? 1 : 0);
+}
+
+void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
+                 int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st) {
+  k_kill<<<blocks(n_max), kThreads, 0, st>>>(s, ob, n_max, kill_height, rotating, max_size, ctl);
+}
+
+}  // namespace blaze

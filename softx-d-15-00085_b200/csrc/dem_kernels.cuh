@@ -1,0 +1,64 @@
+// dem_kernels.cuh -- launch interface of the per-step kernels.
+#pragma once
+
+#include "dem_common.cuh"
+
+namespace blaze {
+
+struct StateBuf {
+  float4* pos;    // (x, y, z, radius)
+  float4* vel;    // (vx, vy, vz, type bits)
+  float4* angv;   // (wx, wy, wz, path since rebuild)
+};
+
+// Arrays that only change order when the particles are re-sorted: two
+// copies, selected by the parity of StepCtl::epoch (the re-sort count).
+struct OrderBuf {
+  int* pid[2];
+  int* lift[2];   // volume-object contact type (Contact_Info.cont_type)
+};
+
+struct ForceCapture {   // optional per-particle force dump (parity tests)
+  float* f_pp; float* t_pp; float* f_w; float* t_w; float* f_l; float* t_l;
+};
+
+struct StepCtl {        // device words the step pipeline communicates through
+  int rebuild_req;      // set by the step (or a removal) when the list must be rebuilt
+  int rebuilt;          // 1 while the current step consumes a fresh re-sort
+  uint32_t status;      // StatusBits of the current run
+  int epoch;            // number of re-sorts so far (selects OrderBuf copies)
+  int n_cur;            // live particles (removed ones sit at the end)
+  int pending_dead;     // removed since the last re-sort
+  int killed_total;
+  int pad;
+};
+
+struct NbrList {
+  uint32_t* idx;        // slot-major: idx[k * stride + i]
+  uint32_t* cnt;
+  int stride;           // >= n_max
+  int cap;
+};
+
+struct WallGrid {       // per-cell candidate wall ops (CSR), optional
+  const uint32_t* off;  // ncell_tab + 1 entries, or null = test every op
+  const uint16_t* ops;
+};
+
+void launch_gate(StepCtl* ctl, cudaStream_t st);
+void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
+                 uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
+void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
+                    const uint32_t* sorted_keys, const int32_t* perm, uint32_t* cell_start,
+                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, StepCtl* ctl,
+                    const int* gate, cudaStream_t st);
+void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
+                  const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
+                  cudaStream_t st);
+void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
+                 const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
+                 NbrList nl, StepCtl* ctl, const ForceCapture* cap, cudaStream_t st);
+void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
+                 int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
+
+}  // namespace blaze
