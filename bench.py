@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--skin", type=float, default=0.04, help="Verlet skin, cm (0 = reference mode)")
     ap.add_argument("--max-nbr", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--settle-steps", type=int, default=0,
+                    help="untimed settling of the packing with the hatch closed (0: the timed "
+                         "region starts from the generated packing, as the CPU arm does)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -149,7 +152,9 @@ def cpu_reference_rate(P, st, seconds, max_steps=None):
     if not ref_available():
         return None
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    R = RefHost().init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=threads,
+    si = type(P.sim_info).from_buffer_copy(bytes(P.sim_info))
+    si.Num_WorldObjects = P.n_w - 1  # hatch open (Device_OpenHatch drops the last object)
+    R = RefHost().init(si, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=threads,
                        capture=False)
     R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     R.step(1)  # first step outside the clock (page-in)
@@ -209,6 +214,15 @@ def main():
 
     sim = device.Simulation(P, skin=args.skin, max_nbr=args.max_nbr)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    if args.settle_steps > 0:
+        # optional untimed settling with the hatch closed; the settled state
+        # is then the workload of every GPU arm (value, e2e, CPU sample)
+        sim.step(args.settle_steps)
+        sim.sync()
+        settled = sim.state()
+        st = dict(pos=settled["pos"], vel=settled["vel"], avel=settled["avel"],
+                  type=settled["type"], pid=settled["pid"])
+    sim.open_hatch()  # the discharge: the last world object (hatch) is dropped
     sim.step(args.warmup)
     status = sim.sync()
     stream = torch.cuda.ExternalStream(sim.device_state()[3])
@@ -269,6 +283,7 @@ def main():
     # end to end through the reference-facing C ABI with host buffers
     lib = device.load()
     kd = device.KDevice(P.wobj, P.pobj, P.dobj, P.n_w, P.n_p, P.n_d, P.sim_info, P.init)
+    kd.IDevice_OpenHatch(P.wobj, P.n_w)
     hp = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
     hv = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
     hw = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()

@@ -133,6 +133,9 @@ int blaze_last_launches(blaze_sim* s);
  * step kernel, in ms, with the number of steps timed. */
 int blaze_set_profile(blaze_sim* s, int on);
 int blaze_profile(blaze_sim* s, float* ms_rebuild, float* ms_step, int* n_steps);
+/* Drop the last world object (the silo hatch), as Device_OpenHatch does
+ * without re-uploading the objects. */
+int blaze_open_hatch(blaze_sim* s);
 /* The simulation behind Part 1 (NULL before Device_Set_SimulationData). */
 blaze_sim* blaze_default_sim(void);
 

@@ -206,15 +206,19 @@ def cone_hopper_faces(r_top, r_out, y_top, y_out, n_seg):
 
 def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, silo_r=25.0,
                  silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, seg_per_obj=7, n_hopper_objs=6,
-                 kn=1.0e5, cor=0.6, mu=0.5, dt=5e-6, seed=1, overlap=1e-3,
+                 kn=1.0e5, cor=0.6, mu=0.5, dt=5e-6, seed=1, overlap=1e-5, rotation=0,
                  name="Silo", world="Silo_discharge", gravity=(0.0, -981.0, 0.0)):
     """Silo discharge, reference-law variant (y vertical, as the reference's
     silo logic assumes, main.cpp:271 and GPU_Memory_Transfer.cuh:656):
     cylinder r=silo_r over a conical hopper of half-angle half_angle_deg down
     to an outlet of outlet_d, made of n_hopper_objs world objects of
     seg_per_obj planar quads each; radii uniform in [r_min, r_max] quantised
-    to n_bins particle objects (the reference's 6-entry pair table); particles
-    on a jittered lattice filling the silo from the hopper up.
+    to n_bins particle objects (the reference's 6-entry pair table).
+    Rotation is off by default: the reference's tangential force scales with
+    |v_t| / |v_rel| where v_t carries the spin term and v_rel does not
+    (Collision_Response.cuh:430-466), which diverges for spinning particles
+    in resting contact; the reference's own box world runs without rotation
+    (Projects/1.Particles_Box/World/Spheres_128cm.World).
     Returns (Project, state dict)."""
     base = os.path.join(root, name)
     for sub in ("SurfaceObjects", "ParticleObjects"):
@@ -268,8 +272,10 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
     # horizontal layers (largest bin lowest) on a lattice of pitch
     # 2 r (1 - overlap), so the bed starts as a contact network under load
     # (about six contacts per particle, solid fraction ~0.52) instead of a
-    # free fall; each layer is clipped to the hopper cone / barrel with a
-    # clearance of r / cos(half-angle) from the wall.
+    # free fall; each layer is clipped to the inscribed radius of the
+    # faceted hopper (R cos(pi / segments)) / the barrel, with a clearance
+    # of r / cos(half-angle) + 0.002 cm from the wall, so the bed rests on
+    # the hopper almost at once.
     tan_a = math.tan(math.radians(half_angle_deg))
     cos_a = math.cos(math.radians(half_angle_deg))
     c = silo_r
@@ -283,8 +289,8 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
         need = int(counts[b])
         y += r
         while need > 0:
-            ra = (r_out + (y - y_out) * tan_a) if y < y_top else silo_r
-            ra -= r / cos_a + 0.05
+            ra = (r_out + (y - y_out) * tan_a) * math.cos(math.pi / n_seg) if y < y_top else silo_r
+            ra -= r / cos_a + 0.002
             if ra > 0:
                 m = int(ra / pitch)
                 g = np.arange(-m, m + 1) * pitch
@@ -299,7 +305,7 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
                 k += cnt
                 need -= cnt
             y += pitch
-        y += r * 0.02
+        y += r * 0.002
     types = types_out
     pos = pos.astype(np.float32)
     state = dict(pos=pos, vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),
@@ -314,7 +320,7 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
                 "Hatch_mode:        1\nFlow_counter:      1 1000\nkill_after:        1\n"
                 "_________________________________________________\n")
     _write_project(root, name, world, title="Silo", sim_type=2, dt=dt, wobjs=wobjs, pobjs=pobjs,
-                   counts=[int(c_) for c_ in counts], n=n, g=gravity, rotation=1, roll_res=0.0,
+                   counts=[int(c_) for c_ in counts], n=n, g=gravity, rotation=rotation, roll_res=0.0,
                    origin=origin, world=tuple(float(v) for v in worldsz), cell=float(cell), state="Start_" + world,
                    specific=specific)
     proj = Project.load(root, name, world)

@@ -718,6 +718,13 @@ int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, voi
 
 int blaze_last_launches(blaze_sim* s) { return s ? s->last_launches : -1; }
 
+int blaze_open_hatch(blaze_sim* s) {
+  if (!s || s->num_wobj <= 0) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  s->num_wobj -= 1;  // Hatch(), GPU_Memory_Transfer.cuh:703-706
+  return upload_walls(s);
+}
+
 int blaze_set_profile(blaze_sim* s, int on) {
   if (!s) return -1;
   CK(cudaStreamSynchronize(s->stream));
