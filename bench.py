@@ -46,7 +46,7 @@ B_ALG = 96  # bytes per particle-step of the fused step: 3 float4 streams read +
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="blaze", choices=["blaze", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
@@ -109,7 +109,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -212,7 +212,7 @@ def main():
     P, st = make_workload(tmp.name, args.n)
     n = P.num_particles
 
-    sim = device.Simulation(P, skin=args.skin, max_nbr=args.max_nbr)
+    sim = device.Simulation(P, skin=args.skin, max_nbr=args.max_nbr, use_graph=1)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     if args.settle_steps > 0:
         # optional untimed settling with the hatch closed; the settled state
@@ -254,7 +254,8 @@ def main():
         dist.barrier()
     value = n * world * args.steps / (ms * 1e-3)
 
-    # per-kernel timing for the roofline (separate pass, same workload)
+    # per-kernel timing for the roofline (separate pass, same workload; the
+    # event-timed path steps without the graph)
     sim.set_profile(True)
     sim.step(min(args.steps, 200))
     ms_rebuild, ms_step, nsteps = sim.profile()
@@ -267,12 +268,12 @@ def main():
         traffic = traffic * n / traffic_n
 
     # reference mode (rebuild every step) for context
-    sim.set_options(skin=0.0)
+    sim.set_options(skin=0.0, use_graph=1)
     sim.step(3)
     sim.sync()
     r0 = torch.cuda.Event(enable_timing=True)
     r1 = torch.cuda.Event(enable_timing=True)
-    kref = min(args.steps, 100)
+    kref = min(args.steps, 400)
     r0.record(stream)
     sim.step(kref)
     r1.record(stream)

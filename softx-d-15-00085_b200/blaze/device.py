@@ -16,7 +16,8 @@ import numpy as np
 
 from . import types as T
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libblaze_b200.so")
+LIB_PATH = os.environ.get("BLAZE_LIB") or os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                                       "libblaze_b200.so")
 
 STATUS_BITS = {1: "list_overflow", 2: "out_of_grid", 4: "non_finite", 8: "type_range",
                16: "timeout"}

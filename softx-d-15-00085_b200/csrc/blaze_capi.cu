@@ -69,6 +69,8 @@ struct blaze_sim {
   ForceCapture cap{};
   bool cap_alloc = false;
   cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;          // captures the IF-node bodies
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps, starting at cur = 0 / 1
   int key_bits = 1;
   long long steps = 0;
   int stepc = 0;        // steps since the last removal check
@@ -92,6 +94,8 @@ struct blaze_sim {
 namespace {
 
 blaze_sim* g_default = nullptr;
+
+void drop_graphs(blaze_sim* s);
 
 // ------------------------------------------------------------------ params
 void build_params(blaze_sim* s) {
@@ -203,26 +207,30 @@ void build_ops(blaze_sim* s) {
 
 // Per-cell candidate lists of wall ops, conservative: an op is dropped for a
 // cell only when no sphere centred in that cell (radius <= rmax) can pass
-// the op's contact test, so the forces are unchanged bit for bit.
-//   faces:   centre must lie within (0, r) above the face plane and project
-//            inside the polygon grown by the area tolerance
-//            (is_PointOnSurface accepts a point at distance d outside a
-//            convex polygon of area A while d * L <= Tol/100 * A for the
-//            edge length L nearest to it; the margin uses the shortest edge)
-//   planes:  centre within (0, r) above the plane
-//   cylinder ops and caps are always kept.
+// the op's contact test, so the forces are unchanged bit for bit.  Over the
+// eight corners of the cell (the tests are affine or convex in the centre):
+//   faces, planes, caps: contact needs n.(x - c) in (0, r); kept when the
+//            corner range of n.(x - c) meets (-eps, rmax + eps); faces also
+//            need the centre to project inside the polygon grown by the
+//            area tolerance (is_PointOnSurface accepts a point at distance d
+//            outside a convex polygon of area A while d * L <= Tol/100 * A
+//            for the edge length L nearest to it; the margin uses the
+//            shortest edge), tested as a box overlap
+//   cylinder: contact needs |x*AXIS - c_bot| + r > R; kept when the
+//            farthest corner reaches R - rmax - eps.
 void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint16_t>& idx) {
   const SimParams& P = s->hp;
   const uint32_t nt = P.ncell_tab;
   float rmax = 0.0f;
   for (int t = 0; t < s->n_p; ++t) rmax = std::max(rmax, s->p[t].radius);
+  const double eps = 1e-3;
   struct Box { double lo[3], hi[3]; };
   const int nops = (int)s->ops.size();
   std::vector<Box> grown(nops);
   std::vector<int> always(nops, 0);
   for (int q = 0; q < nops; ++q) {
     const WallOp& op = s->ops[q];
-    if (op.kind != kOpFace) { always[q] = 1; continue; }
+    if (op.kind != kOpFace) continue;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     double minedge = 1e300;
     for (int v = 0; v < op.nv; ++v) {
@@ -234,21 +242,15 @@ void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint1
       if (e > 0) minedge = std::min(minedge, e);
     }
     double margin = (double)op.tol / 100.0 * std::fabs((double)op.area) / std::max(minedge, 1e-12);
-    margin = margin * 1.01 + 1e-4 * (hi[0] - lo[0] + hi[1] - lo[1] + hi[2] - lo[2]) + rmax;
-    if (!std::isfinite(margin) || op.area <= 0.0f) { always[q] = 1; continue; }
+    margin = margin * 1.01 + 1e-4 * (hi[0] - lo[0] + hi[1] - lo[1] + hi[2] - lo[2]) + rmax + eps;
+    if (!std::isfinite(margin) || !(op.area > 0.0f) || op.nv < 3) { always[q] = 1; continue; }
     for (int c = 0; c < 3; ++c) { grown[q].lo[c] = lo[c] - margin; grown[q].hi[c] = hi[c] + margin; }
   }
   off.assign((size_t)nt + 1, 0);
-  std::vector<std::vector<uint16_t>> per(0);
   idx.clear();
   const int3 nc = P.ncells;
-  // cells are visited in hash order so the CSR is built in one pass
-  std::vector<uint32_t> counts((size_t)nt, 0);
-  std::vector<std::vector<uint16_t>> lists;
-  // enumerate in-grid cells; hashes can alias (ncx != ncz): merge their ops
+  // hashes alias when ncx != ncz: a hash's list is the union over its cells
   std::vector<std::vector<uint16_t>> by_hash((size_t)nt);
-  const double hd = 0.5 * std::sqrt((double)P.cell.x * P.cell.x + (double)P.cell.y * P.cell.y +
-                                    (double)P.cell.z * P.cell.z);
   for (int gy = 0; gy < nc.y; ++gy)
     for (int gz = 0; gz < nc.z; ++gz)
       for (int gx = 0; gx < nc.x; ++gx) {
@@ -256,24 +258,35 @@ void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint1
         const double lo[3] = {P.origin.x + (double)gx * P.cell.x, P.origin.y + (double)gy * P.cell.y,
                               P.origin.z + (double)gz * P.cell.z};
         const double hi[3] = {lo[0] + P.cell.x, lo[1] + P.cell.y, lo[2] + P.cell.z};
-        const double ctr[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
         std::vector<uint16_t>& L = by_hash[h];
         for (int q = 0; q < nops; ++q) {
-          bool keep = always[q] != 0;
           const WallOp& op = s->ops[q];
-          if (!keep && op.kind == kOpFace) {
-            bool ov = true;
-            for (int c = 0; c < 3; ++c)
-              if (hi[c] < grown[q].lo[c] || lo[c] > grown[q].hi[c]) ov = false;
-            if (ov) {
-              const double d = (double)op.n.x * (ctr[0] - op.c.x) + (double)op.n.y * (ctr[1] - op.c.y) +
-                               (double)op.n.z * (ctr[2] - op.c.z);
-              keep = d > -hd - 1e-3 && d < hd + rmax + 1e-3;
+          bool keep = always[q] != 0;
+          if (!keep) {
+            double dmin = 1e300, dmax = -1e300;
+            for (int k = 0; k < 8; ++k) {
+              const double x[3] = {(k & 1) ? hi[0] : lo[0], (k & 2) ? hi[1] : lo[1], (k & 4) ? hi[2] : lo[2]};
+              if (op.kind == kOpCylinder) {
+                const double px = x[0] * op.axis.x - op.cbot.x, py = x[1] * op.axis.y - op.cbot.y,
+                             pz = x[2] * op.axis.z - op.cbot.z;
+                dmax = std::max(dmax, std::sqrt(px * px + py * py + pz * pz));
+              } else {
+                const double d = (double)op.n.x * (x[0] - op.c.x) + (double)op.n.y * (x[1] - op.c.y) +
+                                 (double)op.n.z * (x[2] - op.c.z);
+                dmin = std::min(dmin, d);
+                dmax = std::max(dmax, d);
+              }
+            }
+            if (op.kind == kOpCylinder) {
+              keep = dmax + rmax + eps > (double)op.radius;
+            } else {
+              keep = dmax > -eps && dmin < rmax + eps;
+              if (keep && op.kind == kOpFace)
+                for (int c = 0; c < 3; ++c)
+                  if (hi[c] < grown[q].lo[c] || lo[c] > grown[q].hi[c]) keep = false;
             }
           }
-          if (keep && (L.empty() || L.back() < q)) {
-            if (std::find(L.begin(), L.end(), (uint16_t)q) == L.end()) L.push_back((uint16_t)q);
-          }
+          if (keep && std::find(L.begin(), L.end(), (uint16_t)q) == L.end()) L.push_back((uint16_t)q);
         }
         if (L.size() > 1) std::sort(L.begin(), L.end());
       }
@@ -285,6 +298,7 @@ void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint1
 }
 
 int upload_walls(blaze_sim* s) {
+  drop_graphs(s);
   build_ops(s);
   CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
   if (s->d_ops) CK(cudaFree(s->d_ops));
@@ -319,6 +333,7 @@ int upload_params(blaze_sim* s) {
 }
 
 int alloc_nlist(blaze_sim* s) {
+  drop_graphs(s);
   if (s->nl.idx) CK(cudaFree(s->nl.idx));
   if (s->nl.cnt) CK(cudaFree(s->nl.cnt));
   s->nl.stride = s->n_max;
@@ -331,6 +346,7 @@ int alloc_nlist(blaze_sim* s) {
 
 int alloc_capture(blaze_sim* s) {
   if (s->cap_alloc || !s->opt.capture_forces) return 0;
+  drop_graphs(s);
   float** ps[6] = {&s->cap.f_pp, &s->cap.t_pp, &s->cap.f_w, &s->cap.t_w, &s->cap.f_l, &s->cap.t_l};
   for (auto* q : ps) {
     CK(dalloc(q, (size_t)3 * s->n_max));
@@ -341,15 +357,15 @@ int alloc_capture(blaze_sim* s) {
 }
 
 // --------------------------------------------------------------- the step
-int enqueue_rebuild(blaze_sim* s, const int* gate) {
+int enqueue_rebuild(blaze_sim* s, const int* gate, cudaStream_t st) {
   const int n = s->n_max;
-  launch_hash(s->dp, s->S[s->cur], s->ob, n, s->rs.keys[0], s->ctl, gate, s->stream);
-  const int res = radix_sort_pairs(s->rs, n, s->key_bits, true, gate, s->stream);
+  launch_hash(s->dp, s->S[s->cur], s->ob, n, s->rs.keys[0], s->ctl, gate, st);
+  const int res = radix_sort_pairs(s->rs, n, s->key_bits, true, gate, st);
   const size_t cbytes = sizeof(uint32_t) * s->hp.ncell_tab;
-  CK(cudaMemsetAsync(s->cstart, 0xff, cbytes, s->stream));
+  CK(cudaMemsetAsync(s->cstart, 0xff, cbytes, st));
   launch_reorder(s->S[s->cur], s->S[2], s->ob, n, s->rs.keys[res], s->rs.vals[res], s->cstart,
-                 s->cend, s->hp.ncell_tab, s->n_d > 0, s->ctl, gate, s->stream);
-  launch_nlist(s->dp, s->S[2], n, s->cstart, s->cend, s->nl, s->ctl, gate, s->stream);
+                 s->cend, s->hp.ncell_tab, s->n_d > 0, s->ctl, gate, st);
+  launch_nlist(s->dp, s->S[2], n, s->cstart, s->cend, s->nl, s->ctl, gate, st);
   s->last_launches += 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits);
   return 0;
 }
@@ -370,7 +386,7 @@ cudaEvent_t prof_event(blaze_sim* s, int phase) {
 int enqueue_step(blaze_sim* s) {
   if (s->profile) prof_event(s, 0);
   launch_gate(s->ctl, s->stream);
-  int rc = enqueue_rebuild(s, &s->ctl->rebuilt);
+  int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
   if (rc) return rc;
   if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
   launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
@@ -389,6 +405,88 @@ int enqueue_step(blaze_sim* s) {
       s->last_launches += 1;
       s->stepc = 0;
     }
+  }
+  return 0;
+}
+
+void drop_graphs(blaze_sim* s) {
+  for (int c = 0; c < 2; ++c) {
+    if (s->graph[c]) cudaGraphExecDestroy(s->graph[c]);
+    s->graph[c] = nullptr;
+  }
+}
+
+// Two steps as one CUDA graph, starting from S[c]: per step a one-thread
+// gate kernel sets the IF node's condition from the device's rebuild
+// request, the IF body holds the re-sort + neighbour-list kernels, then the
+// fused step kernel runs.  No empty launches on steps that keep the list.
+int build_graph(blaze_sim* s, int c) {
+  const int saved = s->cur;
+  s->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h[2];
+  for (int k = 0; k < 2; ++k) CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, 0));
+  CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < 2; ++k) {
+    launch_gate_cond(s->ctl, h[k], s->stream);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(s->stream, &cs, nullptr, &capg, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
+    std::memset(cp_raw, 0, sizeof(cp_raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h[k];
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(s->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(s->aux, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_rebuild(s, nullptr, s->aux);
+    cudaGraph_t tmp = nullptr;
+    CK(cudaStreamEndCapture(s->aux, &tmp));
+    if (rc) return rc;
+    launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
+                s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl,
+                s->opt.capture_forces ? &s->cap : nullptr, s->stream);
+    s->cur ^= 1;
+  }
+  cudaGraph_t out = nullptr;
+  CK(cudaStreamEndCapture(s->stream, &out));
+  CK(cudaGraphInstantiate(&s->graph[c], out, 0));
+  CK(cudaGraphDestroy(out));
+  s->cur = saved;
+  return 0;
+}
+
+int graph_steps(blaze_sim* s, int nsteps) {
+  int done = 0;
+  while (done < nsteps) {
+    // removal checks and odd tails run as plain steps
+    const bool kill_soon = s->si.Kill_Particles && s->stepc + 2 >= 1000;
+    if (nsteps - done < 2 || kill_soon) {
+      int rc = enqueue_step(s);
+      if (rc) return rc;
+      done += 1;
+      continue;
+    }
+    const int c = s->cur;
+    if (!s->graph[c]) {
+      int rc = build_graph(s, c);
+      if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(s->graph[c], s->stream));
+    s->last_launches += 2 * (2 + 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits));
+    s->steps += 2;
+    if (s->si.Kill_Particles) s->stepc += 2;
+    done += 2;
   }
   return 0;
 }
@@ -505,6 +603,8 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   const int n = s->n_max;
   auto fail = [&](int rc) { free_sim(s); return rc; };
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
+  e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking);
   if (e != cudaSuccess) return fail(cuda_fail(e));
 #define CKF(x) do { cudaError_t e2 = (x); if (e2 != cudaSuccess) return fail(cuda_fail(e2)); } while (0)
   for (int b = 0; b < 3; ++b) {
@@ -628,6 +728,12 @@ int blaze_get_state(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* 
 int blaze_step(blaze_sim* s, int nsteps) {
   if (!s || nsteps < 0) return -1;
   s->last_launches = 0;
+  if (s->opt.use_graph && !s->opt.sync_each_step && !s->profile) {
+    int rc = graph_steps(s, nsteps);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return 0;
+  }
   for (int k = 0; k < nsteps; ++k) {
     int rc = enqueue_step(s);
     if (rc) return rc;

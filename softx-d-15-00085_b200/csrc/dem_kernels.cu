@@ -50,6 +50,14 @@ __global__ void k_gate(StepCtl* ctl) {
   ctl->rebuild_req = 0;
 }
 
+// The same latch, also steering a graph's IF node around the re-sort body.
+__global__ void k_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h) {
+  const int r = ctl->rebuild_req;
+  ctl->rebuilt = r;
+  ctl->rebuild_req = 0;
+  cudaGraphSetConditional(h, r ? 1u : 0u);
+}
+
 // --------------------------------------------------------------------- hash
 // Kernel_SpatialDecomp_CalcPHash (Collision_Detection_BroadPhase.cuh:75-100).
 // Removed particles (pid -1) take the largest key so they sort last, as the
@@ -419,10 +427,14 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 }
 
 // ---------------------------------------------------------------------- step
-__global__ void __launch_bounds__(kThreads)
+#ifndef BLAZE_STEP_MIN_BLOCKS
+#define BLAZE_STEP_MIN_BLOCKS 3
+#endif
+template <bool kCapture>
+__global__ void __launch_bounds__(kThreads, BLAZE_STEP_MIN_BLOCKS)
 k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGrid wg,
        StateBuf in_plain, StateBuf in_sorted, StateBuf out, OrderBuf ob, int n_max,
-       NbrList nl, StepCtl* ctl, ForceCapture cap, int capture) {
+       NbrList nl, StepCtl* ctl, ForceCapture cap) {
   __shared__ TypeParams sT[kMaxTypes];
   {
     const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
@@ -557,7 +569,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   }
   flag_status(ctl, st);
 
-  if (capture) {
+  if (kCapture) {
     const float3 vals[6] = {f_pp, t_pp, f_w, t_w, f_l, t_l};
     float* dsts[6] = {cap.f_pp, cap.t_pp, cap.f_w, cap.t_w, cap.f_l, cap.t_l};
 #pragma unroll
@@ -602,6 +614,10 @@ inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 
 void launch_gate(StepCtl* ctl, cudaStream_t st) { k_gate<<<1, 1, 0, st>>>(ctl); }
 
+void launch_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h, cudaStream_t st) {
+  k_gate_cond<<<1, 1, 0, st>>>(ctl, h);
+}
+
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st) {
   k_hash<<<blocks(n_max), kThreads, 0, st>>>(dp, s.pos, ob, n_max, keys, ctl, gate);
@@ -625,9 +641,12 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
                  NbrList nl, StepCtl* ctl, const ForceCapture* cap, cudaStream_t st) {
-  ForceCapture c = cap ? *cap : ForceCapture{};
-  k_step<<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl,
-                                             ctl, c, cap ? 1 : 0);
+  if (cap)
+    k_step<true><<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob,
+                                                     n_max, nl, ctl, *cap);
+  else
+    k_step<false><<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob,
+                                                      n_max, nl, ctl, ForceCapture{});
 }
 
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,

@@ -46,6 +46,7 @@ struct WallGrid {       // per-cell candidate wall ops (CSR), optional
 };
 
 void launch_gate(StepCtl* ctl, cudaStream_t st);
+void launch_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h, cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
 void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
