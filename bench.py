@@ -240,12 +240,13 @@ def main():
     e0.record(stream)
     sim.step(args.steps)
     e1.record(stream)
-    launches = sim.last_launches()
+    fixed_launches = sim.last_launches()
     e1.synchronize()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     rebuilds = sim.num_rebuilds() - rb0
+    launches = fixed_launches + rebuilds * sim.rebuild_kernels()
     status |= sim.sync()
     if world > 1:
         t = torch.tensor([ms], device="cuda")

@@ -126,8 +126,12 @@ int blaze_get_nlist(blaze_sim* s, uint* nn, uint* list);
 /* Device pointers of the current state (SoA float4: pos+radius, vel+type,
  * angular velocity) and the CUDA stream the simulation runs on. */
 int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, void** stream);
-/* Number of kernel launches the last blaze_step enqueued. */
+/* Kernel launches the last blaze_step enqueued unconditionally (gate and
+ * step kernels; graph re-sort bodies are counted by blaze_rebuild_kernels
+ * per re-sort). */
 int blaze_last_launches(blaze_sim* s);
+/* Kernels one re-sort + neighbour-list rebuild launches. */
+int blaze_rebuild_kernels(blaze_sim* s);
 /* Per-phase CUDA-event timing of subsequent steps (on/off), and the totals
  * since it was switched on: re-sort + neighbour-list phase and the fused
  * step kernel, in ms, with the number of steps timed. */

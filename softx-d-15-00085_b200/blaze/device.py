@@ -68,6 +68,7 @@ def load():
     lib.blaze_last_launches.argtypes = [C.c_void_p]
     lib.blaze_set_profile.argtypes = [C.c_void_p, C.c_int]
     lib.blaze_open_hatch.argtypes = [C.c_void_p]
+    lib.blaze_rebuild_kernels.argtypes = [C.c_void_p]
     lib.blaze_profile.argtypes = [C.c_void_p, _f, _f, _i]
     lib.blaze_default_sim.restype = C.c_void_p
     lib.Device_Set_SimulationData.argtypes = [P(T.WOBJ), P(T.POBJ), P(T.DOBJ), P(T.SimulationInfo),
@@ -218,6 +219,9 @@ class Simulation:
 
     def last_launches(self):
         return self.lib.blaze_last_launches(self.h)
+
+    def rebuild_kernels(self):
+        return self.lib.blaze_rebuild_kernels(self.h)
 
     def open_hatch(self):
         _check(self.lib.blaze_open_hatch(self.h), "blaze_open_hatch")

@@ -70,7 +70,9 @@ struct blaze_sim {
   bool cap_alloc = false;
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;          // captures the IF-node bodies
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps, starting at cur = 0 / 1
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // kGraphSteps steps, starting at cur = 0 / 1
+  int* d_rb = nullptr;                 // per graph step: nonzero when that step re-sorted
+  bool spin_free = false;              // rotation off and every angular velocity zero
   int key_bits = 1;
   long long steps = 0;
   int stepc = 0;        // steps since the last removal check
@@ -93,6 +95,7 @@ struct blaze_sim {
 
 namespace {
 
+constexpr int kGraphSteps = 8;
 blaze_sim* g_default = nullptr;
 
 void drop_graphs(blaze_sim* s);
@@ -391,6 +394,7 @@ int enqueue_step(blaze_sim* s) {
   if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
   launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
               s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl,
+              StepLink{&s->ctl->rebuilt, 0, 0}, s->spin_free,
               s->opt.capture_forces ? &s->cap : nullptr, s->stream);
   s->last_launches += 2;
   if (s->profile) prof_event(s, 1);
@@ -416,21 +420,24 @@ void drop_graphs(blaze_sim* s) {
   }
 }
 
-// Two steps as one CUDA graph, starting from S[c]: per step a one-thread
-// gate kernel sets the IF node's condition from the device's rebuild
-// request, the IF body holds the re-sort + neighbour-list kernels, then the
-// fused step kernel runs.  No empty launches on steps that keep the list.
+// kGraphSteps steps as one CUDA graph, starting from S[c].  A one-thread
+// gate kernel carries the rebuild request of the previous launch into the
+// first step's IF node; every later step's IF condition is set by the step
+// kernel before it (any particle past half the skin sets it).  An IF body
+// marks its step in d_rb, then re-sorts and rebuilds the neighbour list.
+// Steps that keep the list launch only the fused step kernel.
 int build_graph(blaze_sim* s, int c) {
   const int saved = s->cur;
   s->cur = c;
   cudaGraph_t g = nullptr;
   CK(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle h[2];
-  for (int k = 0; k < 2; ++k) CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, 0));
+  cudaGraphConditionalHandle h[kGraphSteps];
+  for (int k = 0; k < kGraphSteps; ++k)
+    CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
   CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
-  for (int k = 0; k < 2; ++k) {
-    launch_gate_cond(s->ctl, h[k], s->stream);
+  launch_gate_graph(s->ctl, h[0], s->d_rb, kGraphSteps, s->stream);
+  for (int k = 0; k < kGraphSteps; ++k) {
     cudaStreamCaptureStatus cs;
     cudaGraph_t capg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -449,12 +456,15 @@ int build_graph(blaze_sim* s, int c) {
     CK(cudaStreamUpdateCaptureDependencies(s->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
     CK(cudaStreamBeginCaptureToGraph(s->aux, body, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
+    CK(cudaMemsetAsync(s->d_rb + k, 0x01, sizeof(int), s->aux));
     int rc = enqueue_rebuild(s, nullptr, s->aux);
     cudaGraph_t tmp = nullptr;
     CK(cudaStreamEndCapture(s->aux, &tmp));
     if (rc) return rc;
+    const StepLink link = k + 1 < kGraphSteps ? StepLink{s->d_rb + k, h[k + 1], 1}
+                                               : StepLink{s->d_rb + k, 0, 0};
     launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
-                s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl,
+                s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free,
                 s->opt.capture_forces ? &s->cap : nullptr, s->stream);
     s->cur ^= 1;
   }
@@ -470,8 +480,8 @@ int graph_steps(blaze_sim* s, int nsteps) {
   int done = 0;
   while (done < nsteps) {
     // removal checks and odd tails run as plain steps
-    const bool kill_soon = s->si.Kill_Particles && s->stepc + 2 >= 1000;
-    if (nsteps - done < 2 || kill_soon) {
+    const bool kill_soon = s->si.Kill_Particles && s->stepc + kGraphSteps >= 1000;
+    if (nsteps - done < kGraphSteps || kill_soon) {
       int rc = enqueue_step(s);
       if (rc) return rc;
       done += 1;
@@ -483,10 +493,13 @@ int graph_steps(blaze_sim* s, int nsteps) {
       if (rc) return rc;
     }
     CK(cudaGraphLaunch(s->graph[c], s->stream));
-    s->last_launches += 2 * (2 + 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits));
-    s->steps += 2;
-    if (s->si.Kill_Particles) s->stepc += 2;
-    done += 2;
+    // launches that always run: the gate and one step kernel per step
+    // (re-sort bodies run only when a step asks for them)
+    s->last_launches += 1 + kGraphSteps;
+    s->steps += kGraphSteps;
+    if (s->si.Kill_Particles) s->stepc += kGraphSteps;
+    if (kGraphSteps & 1) s->cur ^= 1;
+    done += kGraphSteps;
   }
   return 0;
 }
@@ -503,6 +516,7 @@ int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const flo
                    const uint* type, const int* pid) {
   const int n = s->n_max;
   int dead = 0;
+  bool spin_free = !s->si.Rotation;
   for (int i = 0; i < n; ++i) {
     const uint t = type[i];
     const float r = t < (uint)s->n_p ? s->p[t].radius : 0.0f;
@@ -516,6 +530,12 @@ int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const flo
                       : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     s->hpid[i] = pid[i];
     if (pid[i] < 0) ++dead;
+    if (avel3 && (avel3[3 * i] != 0.0f || avel3[3 * i + 1] != 0.0f || avel3[3 * i + 2] != 0.0f))
+      spin_free = false;
+  }
+  if (spin_free != s->spin_free) {
+    drop_graphs(s);
+    s->spin_free = spin_free;
   }
   CK(cudaStreamSynchronize(s->stream));
   CK(sync_status(s) < 0 ? cudaErrorUnknown : cudaSuccess);
@@ -568,7 +588,7 @@ void free_sim(blaze_sim* s) {
   for (int b = 0; b < 3; ++b) { f(s->S[b].pos); f(s->S[b].vel); f(s->S[b].angv); }
   for (int b = 0; b < 2; ++b) { f(s->ob.pid[b]); f(s->ob.lift[b]); f(s->rs.keys[b]); f(s->rs.vals[b]); }
   f(s->rs.counts); f(s->rs.totals); f(s->cstart); f(s->cend); f(s->nl.idx); f(s->nl.cnt);
-  f(s->ctl); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
+  f(s->ctl); f(s->d_rb); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   for (void* hp : {(void*)s->h4a, (void*)s->h4b, (void*)s->h4c, (void*)s->hpid})
@@ -623,6 +643,8 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->rs.totals, kRadixDigits));
   CKF(dalloc(&s->dp, 1));
   CKF(dalloc(&s->ctl, 1));
+  CKF(dalloc(&s->d_rb, kGraphSteps));
+  CKF(cudaMemset(s->d_rb, 0, sizeof(int) * kGraphSteps));
   CKF(cudaMallocHost((void**)&s->h_ctl, sizeof(StepCtl)));
   CKF(cudaMallocHost((void**)&s->h4a, sizeof(float4) * n));
   CKF(cudaMallocHost((void**)&s->h4b, sizeof(float4) * n));
@@ -823,6 +845,11 @@ int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, voi
 }
 
 int blaze_last_launches(blaze_sim* s) { return s ? s->last_launches : -1; }
+
+int blaze_rebuild_kernels(blaze_sim* s) {
+  if (!s) return -1;
+  return 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits);
+}
 
 int blaze_open_hatch(blaze_sim* s) {
   if (!s || s->num_wobj <= 0) return -1;

@@ -50,12 +50,14 @@ __global__ void k_gate(StepCtl* ctl) {
   ctl->rebuild_req = 0;
 }
 
-// The same latch, also steering a graph's IF node around the re-sort body.
-__global__ void k_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h) {
+// First node of a step graph: latch the request carried over from the last
+// launch into the first step's IF condition and clear the per-step
+// "re-sorted" flags (an IF body marks its own step).
+__global__ void k_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb) {
   const int r = ctl->rebuild_req;
-  ctl->rebuilt = r;
   ctl->rebuild_req = 0;
-  cudaGraphSetConditional(h, r ? 1u : 0u);
+  for (int k = 0; k < nrb; ++k) rb[k] = 0;
+  cudaGraphSetConditional(h0, r ? 1u : 0u);
 }
 
 // --------------------------------------------------------------------- hash
@@ -181,7 +183,11 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
 struct Forces { float3 trans, torque; };
 
 // Collision_Response_Particle_Particle, Collision_Response.cuh:374-494
-// (energy tallies excluded).
+// (energy tallies excluded).  kSpin = false is the spin-free form used when
+// rotation is off and every angular velocity is exactly zero: then
+// v + cross(0, R) equals v up to the sign of an exact zero, so the forces
+// are the same numbers.
+template <bool kSpin>
 __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
                                          float3 ra, float3 rb, float3 wa, float3 wb,
                                          const PP_Parms& pp, float3 va, float3 vb, float ma,
@@ -191,8 +197,8 @@ __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3
   const float fn = pp.Kn * pen;
   const float3 fdiss = pp.Cn * vn;
   F.trans = fn * n - fdiss;
-  const float3 vcpa = va + cross3(wa, ra);
-  const float3 vcpb = vb + cross3(wb, rb);
+  const float3 vcpa = kSpin ? va + cross3(wa, ra) : va;
+  const float3 vcpb = kSpin ? vb + cross3(wb, rb) : vb;
   const float3 vcpna = dot3(vcpa, n) * n;
   const float3 vcpnb = dot3(vcpb, n) * n;
   const float3 vt = (vcpa - vcpna) - (vcpb - vcpnb);
@@ -207,7 +213,7 @@ __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3
     ft = (-1.0f * tan_f) * (vt / mag);
   }
   F.trans = F.trans + ft;
-  F.torque = P.rotation ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  F.torque = (kSpin && P.rotation) ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
   return F;
 }
 
@@ -240,6 +246,7 @@ __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 
 }
 
 // Collision_Response_Particle_MovingSurface, Collision_Response.cuh:116-233
+template <bool kSpin>
 __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 n, float pen,
                                                      float3 r, float3 w, const TypeParams& T,
                                                      float3 va, float3 vs) {
@@ -251,7 +258,7 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
   F.trans = fn * n - fdiss;
   const float3 fdir = F.trans / len3(F.trans);
   if (dot3(fdir, n) < 0) F.trans = fn * n;
-  const float3 vcpa = va + cross3(w, r);
+  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
   const float3 vcpna = dot3(vcpa, n) * n;
   const float3 vt = (vcpa - vcpna) - (vs - dot3(vs, n) * n);
   float mag = dot3(vt, vt);
@@ -272,6 +279,7 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
 // Collision_Response_Particle_VolumeObject, Collision_Response.cuh:241-363,
 // with the zero object spin and lever the caller passes
 // (DEM_Kernels_Compute.cuh:206-216).
+template <bool kSpin>
 __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float pen, float3 r,
                                              float3 w, const TypeParams& T, float3 va,
                                              float3 vobj) {
@@ -284,7 +292,7 @@ __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float
   const float3 fdir = F.trans / len3(F.trans);
   if (dot3(fdir, n) < 0) F.trans = fn * n;
   const float3 z = f3(0.0f, 0.0f, 0.0f);
-  const float3 vcpa = va + cross3(w, r);
+  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
   const float3 vcpb = vobj + cross3(z, z);
   const float3 vt = (vcpa - dot3(vcpa, n) * n) - (vcpb - dot3(vcpb, n) * n);
   float mag = dot3(vt, vt);
@@ -326,12 +334,28 @@ __device__ __forceinline__ bool point_on_polygon(int nv, const float3* v, float3
   return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
 }
 
+// is_PointOnSurface over vertices addressed through vertex_Order.
+__device__ __forceinline__ bool point_on_indexed_polygon(int nv, const float3* v, const int* order,
+                                                         float3 pt, float sarea, float tol) {
+  float area = 0.0f;
+  for (int i = 0; i < nv - 1; ++i) {
+    const float3 v1 = pt - v[order[i] & 7];
+    const float3 v2 = pt - v[order[i + 1] & 7];
+    area = area + 0.500000f * len3(cross3(v1, v2));
+  }
+  const float3 v1 = pt - v[order[nv - 1] & 7];
+  const float3 v2 = pt - v[order[0] & 7];
+  area = area + 0.500000f * len3(cross3(v1, v2));
+  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
+}
+
 __device__ __forceinline__ float3 drum_velocity(const SimParams& P, float3 cp) {
   return cross3(f3(0.0f, 0.0f, -P.mill_rot_vel), cp - f3(P.drum_r, P.drum_r, 0.0f));
 }
 
 // WorldObject_InteractionParticle for spheres (DEM_Kernels_Compute.cuh:254-610):
 // one op per face / plane / cylinder / cap in world-object order.
+template <bool kSpin>
 __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& op, float3 p,
                                               float r, float3 v, float3 w, const TypeParams& T,
                                               float3& fw, float3& tw) {
@@ -347,7 +371,7 @@ __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& 
     }
     Forces F;
     if (P.rotating_wobj && P.cyl_rot)
-      F = law_moving_surface(P, op.n, dis, pt - p, w, T, v, drum_velocity(P, pt));
+      F = law_moving_surface<kSpin>(P, op.n, dis, pt - p, w, T, v, drum_velocity(P, pt));
     else
       F = law_static_surface(P, v, op.n, dis, pt - p, w, T);
     fw = fw + F.trans;
@@ -363,7 +387,7 @@ __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& 
     const float dis = fabsf(pd - op.radius);
     Forces F;
     if (P.cyl_rot)
-      F = law_moving_surface(P, nrm, dis, cp - p, w, T, v, drum_velocity(P, cp));
+      F = law_moving_surface<kSpin>(P, nrm, dis, cp - p, w, T, v, drum_velocity(P, cp));
     else
       F = law_static_surface(P, v, nrm, dis, cp - p, w, T);
     fw = F.trans;
@@ -393,10 +417,8 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
       if (dis < 0.000000f && dis > -r * 0.50f) {
         dis = fabsf(dis);
         const float3 q = pt + s.normal * dis;
-        float3 pv[4];
-        const int nv = s.num_vertex < 4 ? s.num_vertex : 4;
-        for (int k = 0; k < nv; ++k) pv[k] = D.vert[s.vertex_Order[k] & 7];
-        if (point_on_polygon(nv, pv, q, s.area, s.Tol)) {
+        const int nv = s.num_vertex < 8 ? s.num_vertex : 8;
+        if (point_on_indexed_polygon(nv, D.vert, s.vertex_Order, q, s.area, s.Tol)) {
           c.hit = true; c.type = 1; c.dis = dis; c.n = s.normal; c.cp = pt;
           return c;
         }
@@ -428,13 +450,13 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 
 // ---------------------------------------------------------------------- step
 #ifndef BLAZE_STEP_MIN_BLOCKS
-#define BLAZE_STEP_MIN_BLOCKS 3
+#define BLAZE_STEP_MIN_BLOCKS 4
 #endif
-template <bool kCapture>
+template <bool kCapture, bool kSpin>
 __global__ void __launch_bounds__(kThreads, BLAZE_STEP_MIN_BLOCKS)
 k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGrid wg,
        StateBuf in_plain, StateBuf in_sorted, StateBuf out, OrderBuf ob, int n_max,
-       NbrList nl, StepCtl* ctl, ForceCapture cap) {
+       NbrList nl, StepCtl* ctl, StepLink link, ForceCapture cap) {
   __shared__ TypeParams sT[kMaxTypes];
   {
     const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
@@ -444,7 +466,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   }
   __syncthreads();
   const SimParams& P = *Pg;
-  const bool rebuilt = ctl->rebuilt != 0;
+  const bool rebuilt = *link.rebuilt != 0;
   const StateBuf in = rebuilt ? in_sorted : in_plain;
   const int n = ctl->n_cur;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -473,13 +495,13 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     const float dist = len3(rel);
     if (!(dist - (ra + pb4.w) < 0.0f)) continue;  // skin candidate not in contact
     const float4 vb4 = __ldg(in.vel + j);
-    const float4 wb4 = __ldg(in.angv + j);
+    const float4 wb4 = kSpin ? __ldg(in.angv + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const int tb = __float_as_int(vb4.w);
     const float3 vb = xyz(vb4);
     const float3 nrm = rel / dist;
     const float dis = fabsf(dist - (ra + pb4.w)) + 0.000010f;
     const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
-    const Forces F = law_pp(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
+    const Forces F = law_pp<kSpin>(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
                             pp, va, vb, ma, sT[tb & (kMaxTypes - 1)].mass);
     f = f + F.trans;
     fl = fl + F.torque;
@@ -507,7 +529,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
           float3 vobj = f3(0.0f, 0.0f, 0.0f);
           if (D.attached) vobj = drum_velocity(P, c.cp);
           else if (D.translating) vobj = D.velocity;
-          const Forces F = law_volume(P, c.n, c.dis, c.cp - pa, wa, TA, va, vobj);
+          const Forces F = law_volume<kSpin>(P, c.n, c.dis, c.cp - pa, wa, TA, va, vobj);
           f_l = f_l + F.trans;
           if (P.rotation) t_l = t_l + F.torque;
           break;
@@ -524,12 +546,12 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     if (in_grid(P, g)) {
       const uint32_t h = grid_hash(P, g);
       const uint32_t o0 = __ldg(wg.off + h), o1 = __ldg(wg.off + h + 1);
-      for (uint32_t q = o0; q < o1; ++q) apply_wall_op(P, ops[__ldg(wg.ops + q)], pa, ra, va, wa, TA, f_w, t_w);
+      for (uint32_t q = o0; q < o1; ++q) apply_wall_op<kSpin>(P, ops[__ldg(wg.ops + q)], pa, ra, va, wa, TA, f_w, t_w);
     } else {
-      for (int q = 0; q < P.n_ops; ++q) apply_wall_op(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+      for (int q = 0; q < P.n_ops; ++q) apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
     }
   } else {
-    for (int q = 0; q < P.n_ops; ++q) apply_wall_op(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+    for (int q = 0; q < P.n_ops; ++q) apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
   }
   if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
 
@@ -560,12 +582,14 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
 
   // Verlet-list validity: rebuild before any particle has moved half the
   // skin; with no skin the contact list is rebuilt every step (reference).
-  if (P.skin <= 0.0f) {
-    if (i == 0) ctl->rebuild_req = 1;
-  } else {
+  {
     const unsigned m = __activemask();
-    const unsigned b = __ballot_sync(m, path > 0.5f * P.skin);
-    if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicExch(&ctl->rebuild_req, 1);
+    const bool need = P.skin <= 0.0f || path > 0.5f * P.skin;
+    const unsigned b = __ballot_sync(m, need);
+    if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) {
+      if (link.has_next_h) cudaGraphSetConditional(link.next_h, 1u);
+      else atomicExch(&ctl->rebuild_req, 1);
+    }
   }
   flag_status(ctl, st);
 
@@ -614,8 +638,9 @@ inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 
 void launch_gate(StepCtl* ctl, cudaStream_t st) { k_gate<<<1, 1, 0, st>>>(ctl); }
 
-void launch_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h, cudaStream_t st) {
-  k_gate_cond<<<1, 1, 0, st>>>(ctl, h);
+void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
+                       cudaStream_t st) {
+  k_gate_graph<<<1, 1, 0, st>>>(ctl, h0, rb, nrb);
 }
 
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
@@ -640,13 +665,19 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
 
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
-                 NbrList nl, StepCtl* ctl, const ForceCapture* cap, cudaStream_t st) {
-  if (cap)
-    k_step<true><<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob,
-                                                     n_max, nl, ctl, *cap);
-  else
-    k_step<false><<<blocks(n_max), kThreads, 0, st>>>(dp, ops, wg, in_plain, in_sorted, out, ob,
-                                                      n_max, nl, ctl, ForceCapture{});
+                 NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
+                 const ForceCapture* cap, cudaStream_t st) {
+  const ForceCapture c = cap ? *cap : ForceCapture{};
+  const int g = blocks(n_max);
+#define BLAZE_STEP_ARGS dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl, ctl, link, c
+  if (cap) {
+    if (spin_free) k_step<true, false><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+    else k_step<true, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+  } else {
+    if (spin_free) k_step<false, false><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+    else k_step<false, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+  }
+#undef BLAZE_STEP_ARGS
 }
 
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,

@@ -40,13 +40,23 @@ struct NbrList {
   int cap;
 };
 
+// How a step learns whether it consumes a fresh re-sort, and how it asks for
+// the next one: through StepCtl (plain stepping) or, inside a CUDA graph,
+// through the IF-node condition of the next step.
+struct StepLink {
+  const int* rebuilt;                  // nonzero: read the sorted buffer
+  cudaGraphConditionalHandle next_h;   // next step's IF condition (graph)
+  int has_next_h;                      // 0: request through StepCtl::rebuild_req
+};
+
 struct WallGrid {       // per-cell candidate wall ops (CSR), optional
   const uint32_t* off;  // ncell_tab + 1 entries, or null = test every op
   const uint16_t* ops;
 };
 
 void launch_gate(StepCtl* ctl, cudaStream_t st);
-void launch_gate_cond(StepCtl* ctl, cudaGraphConditionalHandle h, cudaStream_t st);
+void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
+                       cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
 void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
@@ -58,7 +68,8 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
                   cudaStream_t st);
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
-                 NbrList nl, StepCtl* ctl, const ForceCapture* cap, cudaStream_t st);
+                 NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
+                 const ForceCapture* cap, cudaStream_t st);
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
 
