@@ -143,6 +143,37 @@ int blaze_open_hatch(blaze_sim* s);
 /* The simulation behind Part 1 (NULL before Device_Set_SimulationData). */
 blaze_sim* blaze_default_sim(void);
 
+/* Contact list of one set of spheres, computed without allocating any
+ * device memory.  No counterpart in the reference.
+ *
+ * For callers that may not allocate: a solver that calls the broad phase
+ * between its own kernels (coupled CFD-DEM, FEM) cannot afford cudaMalloc /
+ * cudaFree, which synchronise the whole device, and many such hosts own all
+ * device memory through their own pool.  The working memory is a fixed
+ * array inside the library (about 5.8 MB, held on every GPU that loads the
+ * library until the process exits), which limits a call to 65,536 spheres
+ * and 262,144 hash-table entries; larger calls return -3 with a message.
+ *
+ * Same broad phase as the step: cell keys from si->worldOrigin, cellSize and
+ * num_NNCells, stable sort by cell, and every pair with
+ * |xi - xj| - (ri + rj) < skin from the 27 surrounding cells.
+ *   pos4    device, n x (x, y, z, radius) floats, every particle live
+ *   perm    device, n: sorted slot k holds input particle perm[k]
+ *   nn      device, n: neighbour count of sorted particle i (<= max_nbr)
+ *   list    device, max_nbr * n, slot-major: list[k * n + i] is the k-th
+ *           neighbour of sorted particle i, as a sorted slot
+ *   status  device, 1 word (may be NULL): status bits (1 overflow, 2 outside
+ *           the grid)
+ *   stream  cudaStream_t the work is enqueued on (NULL: default stream)
+ * Returns 0 once the work is enqueued, -1 for a bad argument, -3 beyond the
+ * size limit, -(1000 + cudaError_t) for a CUDA error.  The first call on
+ * each device looks up the array's device address; make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int blaze_contact_list_static(const float* pos4, int n, const SimulationInfo* si, float skin,
+                              int max_nbr, int* perm, uint* nn, uint* list, uint* status,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif
