@@ -34,9 +34,11 @@ def wobj(src):
         for j in range(min(src.num_surfaces, 16)):
             _surface(d.surfaces[j], src.surfaces[j])
     else:
-        C.memmove(C.addressof(d.cyl_geo), C.addressof(src.cyl_geo), C.sizeof(T.Macro_Cylinder))
-        d.cyl_geo.normal_cyl = T.float3()
-        # bool padding bytes of Macro_Cylinder are not meaningful
+        # field by field: the two bytes of padding after the bools, and
+        # normal_cyl (never set by the reader), hold whatever the heap held
+        for f in ("height", "radius", "has_top_cap", "has_bot_cap", "normal_top_cap",
+                  "normal_bot_cap", "center_top_cap", "center_bot_cap", "AXIS"):
+            setattr(d.cyl_geo, f, getattr(src.cyl_geo, f))
     if src.is_rotating:
         d.cyl_geo.AXIS = src.cyl_geo.AXIS
         d.cyl_geo.radius = src.cyl_geo.radius
