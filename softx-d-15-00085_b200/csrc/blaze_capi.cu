@@ -86,11 +86,10 @@ struct blaze_sim {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_marks;  // (phase, event index) start/end pairs in order
   int ev_used = 0;
-  // pinned host staging for state upload/download (n_max each)
-  float4* h4a = nullptr;
-  float4* h4b = nullptr;
-  float4* h4c = nullptr;
-  int* hpid = nullptr;
+  // device staging of the reference interface's AoS host arrays (n_max
+  // each), packed / unpacked by a kernel, and its two result words (pinned)
+  HostStage stage{};
+  int* h_flags = nullptr;
 };
 
 namespace {
@@ -515,40 +514,28 @@ int sync_status(blaze_sim* s) {
 int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
                    const uint* type, const int* pid) {
   const int n = s->n_max;
-  int dead = 0;
-  bool spin_free = !s->si.Rotation;
-  for (int i = 0; i < n; ++i) {
-    const uint t = type[i];
-    const float r = t < (uint)s->n_p ? s->p[t].radius : 0.0f;
-    s->h4a[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], r);
-    float tb;
-    int ti = (int)t;
-    std::memcpy(&tb, &ti, 4);
-    s->h4b[i] = vel3 ? make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], tb)
-                     : make_float4(0.0f, 0.0f, 0.0f, tb);
-    s->h4c[i] = avel3 ? make_float4(avel3[3 * i], avel3[3 * i + 1], avel3[3 * i + 2], 0.0f)
-                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    s->hpid[i] = pid[i];
-    if (pid[i] < 0) ++dead;
-    if (avel3 && (avel3[3 * i] != 0.0f || avel3[3 * i + 1] != 0.0f || avel3[3 * i + 2] != 0.0f))
-      spin_free = false;
-  }
+  int rc = sync_status(s);
+  if (rc < 0) return rc;
+  const int e = s->h_ctl->epoch & 1;
+  const HostStage& hs = s->stage;
+  CK(cudaMemsetAsync(hs.flags, 0, 2 * sizeof(int), s->stream));
+  CK(cudaMemcpyAsync(hs.pos3, pos3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+  if (vel3)
+    CK(cudaMemcpyAsync(hs.vel3, vel3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+  if (avel3)
+    CK(cudaMemcpyAsync(hs.avel3, avel3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(hs.type, type, sizeof(uint) * n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(hs.pid, pid, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+  launch_pack_state(s->dp, hs, vel3 != nullptr, avel3 != nullptr, s->S[s->cur], s->ob.pid[e],
+                    s->n_d > 0 ? s->ob.lift[e] : nullptr, n, s->stream);
+  CK(cudaMemcpyAsync(s->h_flags, hs.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  const int dead = s->h_flags[0];
+  const bool spin_free = !s->si.Rotation && s->h_flags[1] == 0;
   if (spin_free != s->spin_free) {
     drop_graphs(s);
     s->spin_free = spin_free;
-  }
-  CK(cudaStreamSynchronize(s->stream));
-  CK(sync_status(s) < 0 ? cudaErrorUnknown : cudaSuccess);
-  const int e = s->h_ctl->epoch & 1;
-  const StateBuf& S = s->S[s->cur];
-  CK(cudaMemcpyAsync(S.pos, s->h4a, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemcpyAsync(S.vel, s->h4b, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemcpyAsync(S.angv, s->h4c, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
-  CK(cudaMemcpyAsync(s->ob.pid[e], s->hpid, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
-  if (s->n_d > 0) {
-    std::vector<int> l(n, -1);
-    CK(cudaMemcpyAsync(s->ob.lift[e], l.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
-    CK(cudaStreamSynchronize(s->stream));
   }
   StepCtl c = *s->h_ctl;
   c.rebuild_req = 1;
@@ -566,19 +553,15 @@ int get_state_impl(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* t
   if (st < 0) return st;
   const int n = s->n_max;
   const int e = s->h_ctl->epoch & 1;
-  const StateBuf& S = s->S[s->cur];
-  if (pos3) CK(cudaMemcpyAsync(s->h4a, S.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
-  if (vel3 || type) CK(cudaMemcpyAsync(s->h4b, S.vel, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
-  if (avel3) CK(cudaMemcpyAsync(s->h4c, S.angv, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
-  if (pid) CK(cudaMemcpyAsync(s->hpid, s->ob.pid[e], sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  const HostStage& hs = s->stage;
+  launch_unpack_state(hs, s->S[s->cur], s->ob.pid[e], n, s->stream);
+  if (pos3) CK(cudaMemcpyAsync(pos3, hs.pos3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (vel3) CK(cudaMemcpyAsync(vel3, hs.vel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (avel3) CK(cudaMemcpyAsync(avel3, hs.avel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (type) CK(cudaMemcpyAsync(type, hs.type, sizeof(uint) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (pid) CK(cudaMemcpyAsync(pid, hs.pid, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  for (int i = 0; i < n; ++i) {
-    if (pos3) { pos3[3 * i] = s->h4a[i].x; pos3[3 * i + 1] = s->h4a[i].y; pos3[3 * i + 2] = s->h4a[i].z; }
-    if (vel3) { vel3[3 * i] = s->h4b[i].x; vel3[3 * i + 1] = s->h4b[i].y; vel3[3 * i + 2] = s->h4b[i].z; }
-    if (avel3) { avel3[3 * i] = s->h4c[i].x; avel3[3 * i + 1] = s->h4c[i].y; avel3[3 * i + 2] = s->h4c[i].z; }
-    if (type) { int t; std::memcpy(&t, &s->h4b[i].w, 4); type[i] = (uint)t; }
-    if (pid) pid[i] = s->hpid[i];
-  }
+  CK(cudaGetLastError());
   return st;
 }
 
@@ -591,8 +574,9 @@ void free_sim(blaze_sim* s) {
   f(s->ctl); f(s->d_rb); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
-  for (void* hp : {(void*)s->h4a, (void*)s->h4b, (void*)s->h4c, (void*)s->hpid})
-    if (hp) cudaFreeHost(hp);
+  f(s->stage.pos3); f(s->stage.vel3); f(s->stage.avel3); f(s->stage.type); f(s->stage.pid);
+  f(s->stage.flags);
+  if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -646,10 +630,13 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->d_rb, kGraphSteps));
   CKF(cudaMemset(s->d_rb, 0, sizeof(int) * kGraphSteps));
   CKF(cudaMallocHost((void**)&s->h_ctl, sizeof(StepCtl)));
-  CKF(cudaMallocHost((void**)&s->h4a, sizeof(float4) * n));
-  CKF(cudaMallocHost((void**)&s->h4b, sizeof(float4) * n));
-  CKF(cudaMallocHost((void**)&s->h4c, sizeof(float4) * n));
-  CKF(cudaMallocHost((void**)&s->hpid, sizeof(int) * n));
+  CKF(dalloc(&s->stage.pos3, (size_t)3 * n));
+  CKF(dalloc(&s->stage.vel3, (size_t)3 * n));
+  CKF(dalloc(&s->stage.avel3, (size_t)3 * n));
+  CKF(dalloc(&s->stage.type, n));
+  CKF(dalloc(&s->stage.pid, n));
+  CKF(dalloc(&s->stage.flags, 2));
+  CKF(cudaMallocHost((void**)&s->h_flags, 2 * sizeof(int)));
   std::memset(s->h_ctl, 0, sizeof(StepCtl));
   s->h_ctl->n_cur = n;
   s->h_ctl->rebuild_req = 1;

@@ -632,6 +632,48 @@ __global__ void k_kill(StateBuf s, OrderBuf ob, int n_max, float kill_height, in
   }
 }
 
+// ------------------------------------------------------------ state staging
+// Set_PSystem_State / Get_SystemState (GPU_Memory_Transfer.cuh:377-418,
+// 486-520) as one pass each over the staged host arrays.
+__global__ void __launch_bounds__(kThreads)
+k_pack_state(const SimParams* __restrict__ P, HostStage hs, int has_vel, int has_avel, StateBuf s,
+             int* __restrict__ pid_dst, int* __restrict__ lift_dst, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t t = hs.type[i];
+  const float r = t < (uint32_t)P->n_types ? P->types[t].radius : 0.0f;
+  const float tb = __int_as_float((int)t);
+  s.pos[i] = make_float4(hs.pos3[3 * i], hs.pos3[3 * i + 1], hs.pos3[3 * i + 2], r);
+  s.vel[i] = has_vel ? make_float4(hs.vel3[3 * i], hs.vel3[3 * i + 1], hs.vel3[3 * i + 2], tb)
+                     : make_float4(0.0f, 0.0f, 0.0f, tb);
+  const float4 w = has_avel
+                       ? make_float4(hs.avel3[3 * i], hs.avel3[3 * i + 1], hs.avel3[3 * i + 2], 0.0f)
+                       : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.angv[i] = w;
+  const int id = hs.pid[i];
+  pid_dst[i] = id;
+  if (lift_dst) lift_dst[i] = -1;
+  const unsigned m = __activemask();
+  const int dead = __popc(__ballot_sync(m, id < 0));
+  const bool spin = __any_sync(m, w.x != 0.0f || w.y != 0.0f || w.z != 0.0f);
+  if ((threadIdx.x & 31) == (__ffs(m) - 1)) {
+    if (dead) atomicAdd(&hs.flags[0], dead);
+    if (spin) atomicOr(&hs.flags[1], 1);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_unpack_state(HostStage hs, StateBuf s, const int* __restrict__ pid_src, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = s.pos[i], v = s.vel[i], w = s.angv[i];
+  hs.pos3[3 * i] = p.x; hs.pos3[3 * i + 1] = p.y; hs.pos3[3 * i + 2] = p.z;
+  hs.vel3[3 * i] = v.x; hs.vel3[3 * i + 1] = v.y; hs.vel3[3 * i + 2] = v.z;
+  hs.avel3[3 * i] = w.x; hs.avel3[3 * i + 1] = w.y; hs.avel3[3 * i + 2] = w.z;
+  hs.type[i] = (uint32_t)__float_as_int(v.w);
+  hs.pid[i] = pid_src[i];
+}
+
 inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
@@ -678,6 +720,17 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
     else k_step<false, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
   }
 #undef BLAZE_STEP_ARGS
+}
+
+void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,
+                       const StateBuf& s, int* pid_dst, int* lift_dst, int n, cudaStream_t st) {
+  k_pack_state<<<blocks(n), kThreads, 0, st>>>(dp, hs, has_vel ? 1 : 0, has_avel ? 1 : 0, s,
+                                               pid_dst, lift_dst, n);
+}
+
+void launch_unpack_state(const HostStage& hs, const StateBuf& s, const int* pid_src, int n,
+                         cudaStream_t st) {
+  k_unpack_state<<<blocks(n), kThreads, 0, st>>>(hs, s, pid_src, n);
 }
 
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,

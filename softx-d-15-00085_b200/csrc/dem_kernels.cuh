@@ -54,6 +54,19 @@ struct WallGrid {       // per-cell candidate wall ops (CSR), optional
   const uint16_t* ops;
 };
 
+// Device copy of the host-side arrays of the reference interface (AoS
+// float3 positions/velocities, type, P_ID) and two result words: [0] the
+// number of removed particles (P_ID < 0), [1] nonzero when any angular
+// velocity is non-zero.
+struct HostStage {
+  float* pos3;
+  float* vel3;
+  float* avel3;
+  uint32_t* type;
+  int* pid;
+  int* flags;
+};
+
 void launch_gate(StepCtl* ctl, cudaStream_t st);
 void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
                        cudaStream_t st);
@@ -72,5 +85,13 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
                  const ForceCapture* cap, cudaStream_t st);
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
+
+// AoS stage -> SoA float4 state (radius from the particle type, type bits in
+// vel4.w), P_ID into `pid_dst`, volume-object history reset to -1.
+void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,
+                       const StateBuf& s, int* pid_dst, int* lift_dst, int n, cudaStream_t st);
+// SoA float4 state -> AoS stage (the inverse of launch_pack_state).
+void launch_unpack_state(const HostStage& hs, const StateBuf& s, const int* pid_src, int n,
+                         cudaStream_t st);
 
 }  // namespace blaze
