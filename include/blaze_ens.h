@@ -1,0 +1,108 @@
+/*
+ * blaze_ens.h -- C ABI of DEM ensembles in libblaze_b200.so: many independent
+ * sphere systems of uneven size stepped together on one GPU, with contact
+ * laws the reference does not have.
+ *
+ * The reference runs one system per process (DeviceInterface.cu:1499-1816)
+ * with a linear spring-dashpot and a velocity-proportional tangential force
+ * (Collision_Response.cuh:374-494).  An ensemble keeps the reference's step
+ * structure -- hash, stable sort by cell (BroadPhase.cuh:75-117), reorder and
+ * cell table (BroadPhase.cuh:126-325), 27-cell neighbour search
+ * (BroadPhase.cuh:402-513), per-particle force gather and symplectic Euler
+ * (DEM_Kernels_Compute.cuh:620-729, Integration.cuh:6-184) -- over all
+ * systems at once, with
+ *   - keys prefixed by the system (a particle only meets its own system),
+ *   - a Verlet list with skin, rebuilt when any particle has moved half of it,
+ *   - the linear (kn, kt) or Hertz-Mindlin (E, nu) normal/tangential spring
+ *     with restitution damping, a tangential history spring capped by
+ *     Coulomb friction, and rolling friction,
+ *   - walls: planes, cylinders (particles inside) and triangle meshes.
+ * Status codes as in blaze_dem.h (0 ok, >0 status bits, <0 errors).
+ * Units are the reference's: cm, kg, s.
+ */
+#ifndef BLAZE_ENS_H_
+#define BLAZE_ENS_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct blaze_ens blaze_ens;
+
+enum { BLAZE_LAW_LINEAR = 1, BLAZE_LAW_HERTZ_MINDLIN = 2 };
+enum { BLAZE_WALL_PLANE = 0, BLAZE_WALL_TRIANGLE = 1, BLAZE_WALL_CYLINDER = 2 };
+
+typedef struct blaze_wall {
+  int kind;     /* BLAZE_WALL_* */
+  float p[10];  /* plane:    p[0..2] unit normal pointing into the domain, p[3] = d
+                 *           (points x of the plane have n . x = d)
+                 * triangle: p[0..8] the three vertices
+                 * cylinder: p[0..2] a point on the axis, p[3..5] unit axis,
+                 *           p[6] radius (particles move inside)            */
+} blaze_wall;
+
+typedef struct blaze_system {
+  int n;              /* particles; systems are consecutive in the state arrays */
+  float origin[3];    /* hash grid origin, cm */
+  float cell;         /* cubic cell edge, cm; must be >= 2 r_max + skin */
+  int ncells[3];
+  float gravity[3];   /* cm/s^2 */
+  float density;      /* kg/cm^3: m = density 4/3 pi r^3, I = 0.4 m r^2 */
+  float kn;           /* linear law: normal stiffness, kg/s^2 */
+  float kt_ratio;     /* linear law: tangential / normal stiffness (e.g. 2/7) */
+  float youngs;       /* Hertz-Mindlin: Young's modulus, kg/(cm s^2) (1 Pa = 0.01) */
+  float poisson;      /* Hertz-Mindlin: Poisson ratio */
+  float restitution;  /* normal coefficient of restitution, (0, 1] */
+  float mu;           /* Coulomb friction, particle-particle */
+  float mu_wall;      /* Coulomb friction, particle-wall */
+  float mu_roll;      /* rolling friction coefficient (0: none) */
+  int wall0, nwalls;  /* planes and cylinders of this system: walls[wall0 .. +nwalls) */
+  int tri0, ntris;    /* triangles of this system: walls[tri0 .. +ntris) */
+} blaze_system;
+
+typedef struct blaze_ens_options {
+  int law;             /* BLAZE_LAW_LINEAR or BLAZE_LAW_HERTZ_MINDLIN */
+  float dt;            /* s */
+  float skin;          /* Verlet skin, cm, > 0 */
+  int max_nbr;         /* neighbour / history slots per particle, 1..32 */
+  int use_graph;       /* 1: steps run as CUDA graphs (re-sort in a conditional node) */
+  int capture_forces;  /* 1: keep each step's contact force and torque per particle */
+} blaze_ens_options;
+
+/* law 1, dt 1e-5, skin 0.02, max_nbr 32, use_graph 1, capture_forces 0 */
+void blaze_ens_default_options(blaze_ens_options* o);
+
+int blaze_ens_create(blaze_ens** out, const blaze_system* systems, int nsys,
+                     const blaze_wall* walls, int nwalls, const blaze_ens_options* opt);
+int blaze_ens_destroy(blaze_ens* e);
+/* Host arrays of all systems concatenated in system order: positions (3 per
+ * particle), radii, velocities and angular velocities (may be NULL: zero).
+ * Clears every contact history.  Radii must satisfy 2 r + skin <= cell. */
+int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, const float* vel3,
+                        const float* avel3);
+/* Current memory order (sorted by system and cell); sys[i] is the system of
+ * entry i and pid[i] its index in the set_state arrays.  NULL skips an array. */
+int blaze_ens_get_state(blaze_ens* e, float* pos3, float* radius, float* vel3, float* avel3,
+                        int* sys, int* pid);
+/* Enqueue nsteps steps on the ensemble's stream. */
+int blaze_ens_step(blaze_ens* e, int nsteps);
+/* Wait for the stream; the status bits raised since the state was set. */
+int blaze_ens_sync(blaze_ens* e);
+/* New law parameters (same sizes, grids and walls as at creation). */
+int blaze_ens_set_params(blaze_ens* e, const blaze_system* systems);
+/* capture_forces: contact force and torque of the last step (gravity not
+ * included), 3 floats per particle, current memory order. */
+int blaze_ens_get_forces(blaze_ens* e, float* force3, float* torque3);
+int blaze_ens_num_rebuilds(blaze_ens* e);
+/* Device pointers of the current state (float4 pos+radius, vel+bits,
+ * angular velocity+path) and the ensemble's CUDA stream. */
+int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4, void** stream);
+/* Kernels launched by the last blaze_ens_step that always run (re-sorts are
+ * counted by blaze_ens_rebuild_kernels each). */
+int blaze_ens_last_launches(blaze_ens* e);
+int blaze_ens_rebuild_kernels(blaze_ens* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

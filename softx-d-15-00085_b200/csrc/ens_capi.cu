@@ -1,0 +1,625 @@
+// ens_capi.cu -- host side of the ensemble path (include/blaze_ens.h): the
+// per-system constants, the triangle candidate lists per cell, the buffers
+// (allocated once), the step pipeline and its CUDA-graph form.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "blaze_dem.h"
+#include "blaze_ens.h"
+#include "ens_kernels.cuh"
+#include "radix_sort.cuh"
+
+using namespace blaze;
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+  std::fprintf(stderr, "blaze_ens: CUDA error %d (%s)\n", (int)e, cudaGetErrorString(e));
+  return -(1000 + (int)e);
+}
+
+#define CK(x)                                    \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) return cuda_fail(e_); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+constexpr int kGraphSteps = 8;
+
+}  // namespace
+
+struct blaze_ens {
+  blaze_ens_options opt{};
+  int nsys = 0, n = 0, nwalls = 0;
+  std::vector<blaze_system> sys;
+  std::vector<EnsSysDev> hsys;
+  std::vector<EnsWallDev> hwalls;
+  EnsSysDev* d_sys = nullptr;
+  EnsWallDev* d_walls = nullptr;
+  uint32_t* d_tri_off = nullptr;
+  uint32_t* d_tri_ids = nullptr;
+  uint32_t ncell_tab = 0;
+  int key_bits = 1;
+  EnsBufs b{};
+  int cur = 0;
+  RadixSortBuffers rs{};
+  uint32_t* cstart = nullptr;
+  uint32_t* cend = nullptr;
+  StepCtl* ctl = nullptr;
+  StepCtl* h_ctl = nullptr;
+  int* d_sys_of = nullptr;
+  float* st_pos3 = nullptr;   // staging of the caller's arrays
+  float* st_rad = nullptr;
+  float* st_vel3 = nullptr;
+  float* st_avel3 = nullptr;
+  int* st_sys = nullptr;
+  int* st_pid = nullptr;
+  int* d_flags = nullptr;
+  int* h_flags = nullptr;
+  EnsCapture cap{};
+  cudaStream_t stream = nullptr, aux = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int* d_rb = nullptr;
+  uint32_t status = 0;
+  int last_launches = 0;
+  bool state_set = false;
+};
+
+namespace {
+
+EnsGeom geom(const blaze_ens* e) {
+  EnsGeom g;
+  g.sys = e->d_sys;
+  g.walls = e->d_walls;
+  g.tri_off = e->d_tri_off;
+  g.tri_ids = e->d_tri_ids;
+  g.ncell_tab = e->ncell_tab;
+  g.law = e->opt.law;
+  g.dt = e->opt.dt;
+  g.skin = e->opt.skin;
+  return g;
+}
+
+// Per-system constants of the contact law, in double, rounded once to float.
+EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off) {
+  EnsSysDev d;
+  std::memset(&d, 0, sizeof(d));
+  d.origin = make_float3(s.origin[0], s.origin[1], s.origin[2]);
+  d.cell = s.cell;
+  d.nc = make_int3(s.ncells[0], s.ncells[1], s.ncells[2]);
+  d.cell_off = cell_off;
+  d.gravity = make_float3(s.gravity[0], s.gravity[1], s.gravity[2]);
+  const double pi = 3.14159265358979323846;
+  d.dens43pi = (float)((double)s.density * 4.0 / 3.0 * pi);
+  const double e = s.restitution;
+  const double le = std::log(e);
+  const double beta = -le / std::sqrt(le * le + pi * pi);
+  d.kn = s.kn;
+  d.kt = (float)((double)s.kn * (double)s.kt_ratio);
+  d.beta2 = (float)(2.0 * beta);
+  const double E = s.youngs, nu = s.poisson;
+  d.estar = (float)(E / (2.0 * (1.0 - nu * nu)));
+  d.gstar = (float)(E / (4.0 * (2.0 - nu) * (1.0 + nu)));
+  d.beta2h = (float)(2.0 * std::sqrt(5.0 / 6.0) * beta);
+  d.mu = s.mu;
+  d.mu_w = s.mu_wall;
+  d.mu_r = s.mu_roll;
+  d.wall0 = s.wall0;
+  d.nwall = s.nwalls;
+  return d;
+}
+
+EnsWallDev wall_dev(const blaze_wall& w) {
+  EnsWallDev d;
+  std::memset(&d, 0, sizeof(d));
+  d.kind = w.kind;
+  if (w.kind == BLAZE_WALL_PLANE) {
+    d.a = make_float3(w.p[0], w.p[1], w.p[2]);
+    d.r = w.p[3];
+  } else if (w.kind == BLAZE_WALL_TRIANGLE) {
+    d.a = make_float3(w.p[0], w.p[1], w.p[2]);
+    d.b = make_float3(w.p[3], w.p[4], w.p[5]);
+    d.c = make_float3(w.p[6], w.p[7], w.p[8]);
+  } else {
+    d.a = make_float3(w.p[0], w.p[1], w.p[2]);
+    d.b = make_float3(w.p[3], w.p[4], w.p[5]);
+    d.r = w.p[6];
+  }
+  return d;
+}
+
+// Candidate triangles per global cell: every cell whose box meets the
+// triangle's bounding box grown by half a cell (more than the largest radius
+// a system allows), so a sphere centred in the cell touches no triangle left
+// out.  Lists are in ascending triangle order.
+void build_tri_lists(const blaze_ens* e, std::vector<uint32_t>& off, std::vector<uint32_t>& ids) {
+  off.assign((size_t)e->ncell_tab + 1, 0);
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;  // (cell, triangle)
+  for (int s = 0; s < e->nsys; ++s) {
+    const blaze_system& S = e->sys[s];
+    const EnsSysDev& D = e->hsys[s];
+    const double margin = 0.5 * (double)S.cell + 1e-4 * (double)S.cell;
+    for (int t = S.tri0; t < S.tri0 + S.ntris; ++t) {
+      const EnsWallDev& W = e->hwalls[t];
+      const float3 v[3] = {W.a, W.b, W.c};
+      int lo[3], hi[3];
+      for (int c = 0; c < 3; ++c) {
+        double mn = 1e300, mx = -1e300;
+        for (int k = 0; k < 3; ++k) {
+          const double x = c == 0 ? v[k].x : (c == 1 ? v[k].y : v[k].z);
+          mn = std::min(mn, x);
+          mx = std::max(mx, x);
+        }
+        const double o = c == 0 ? D.origin.x : (c == 1 ? D.origin.y : D.origin.z);
+        const int ncs = c == 0 ? D.nc.x : (c == 1 ? D.nc.y : D.nc.z);
+        lo[c] = std::max(0, (int)std::floor((mn - margin - o) / (double)S.cell));
+        hi[c] = std::min(ncs - 1, (int)std::floor((mx + margin - o) / (double)S.cell));
+      }
+      for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+          for (int x = lo[0]; x <= hi[0]; ++x)
+            pairs.push_back({D.cell_off + (uint32_t)(x + D.nc.x * (y + D.nc.y * z)), (uint32_t)t});
+    }
+  }
+  std::stable_sort(pairs.begin(), pairs.end(),
+                   [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
+                     return a.first < b.first;
+                   });
+  ids.resize(pairs.size());
+  for (size_t k = 0; k < pairs.size(); ++k) {
+    off[pairs[k].first + 1]++;
+    ids[k] = pairs[k].second;
+  }
+  for (size_t c = 0; c < e->ncell_tab; ++c) off[c + 1] += off[c];
+}
+
+void drop_graphs(blaze_ens* e) {
+  for (int c = 0; c < 2; ++c) {
+    if (e->graph[c]) cudaGraphExecDestroy(e->graph[c]);
+    e->graph[c] = nullptr;
+  }
+}
+
+void free_ens(blaze_ens* e) {
+  if (!e) return;
+  drop_graphs(e);
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  for (int k = 0; k < 3; ++k) { f(e->b.S[k].pos); f(e->b.S[k].vel); f(e->b.S[k].angv); }
+  for (int k = 0; k < 2; ++k) {
+    f(e->b.pid[k]); f(e->b.wh[k]);
+    f(e->b.L[k].idx); f(e->b.L[k].cnt); f(e->b.L[k].mask);
+    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz);
+    f(e->rs.keys[k]); f(e->rs.vals[k]);
+  }
+  f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
+  f(e->d_sys); f(e->d_walls); f(e->d_tri_off); f(e->d_tri_ids); f(e->d_sys_of);
+  f(e->st_pos3); f(e->st_rad); f(e->st_vel3); f(e->st_avel3); f(e->st_sys); f(e->st_pid);
+  f(e->d_flags); f(e->cap.f); f(e->cap.t);
+  if (e->h_ctl) cudaFreeHost(e->h_ctl);
+  if (e->h_flags) cudaFreeHost(e->h_flags);
+  if (e->aux) cudaStreamDestroy(e->aux);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+bool valid_system(const blaze_system& s, int nwalls, float skin) {
+  if (s.n < 0 || !(s.cell > 0.0f) || s.ncells[0] < 1 || s.ncells[1] < 1 || s.ncells[2] < 1)
+    return false;
+  if (!(s.cell >= skin)) return false;
+  if (!(s.density > 0.0f) || !(s.restitution > 0.0f) || !(s.restitution <= 1.0f)) return false;
+  if (s.wall0 < 0 || s.nwalls < 0 || s.wall0 + s.nwalls > nwalls) return false;
+  if (s.tri0 < 0 || s.ntris < 0 || s.tri0 + s.ntris > nwalls) return false;
+  return true;
+}
+
+int upload_params(blaze_ens* e) {
+  uint32_t off = 0;
+  e->hsys.resize(e->nsys);
+  for (int s = 0; s < e->nsys; ++s) {
+    e->hsys[s] = system_constants(e->sys[s], off);
+    off += (uint32_t)e->sys[s].ncells[0] * (uint32_t)e->sys[s].ncells[1] *
+           (uint32_t)e->sys[s].ncells[2];
+  }
+  CK(cudaMemcpyAsync(e->d_sys, e->hsys.data(), sizeof(EnsSysDev) * e->nsys,
+                     cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int enqueue_rebuild(blaze_ens* e, const int* gate, cudaStream_t st) {
+  const int n = e->n;
+  const EnsGeom g = geom(e);
+  ens_launch_hash(g, e->b, e->cur, n, e->rs.keys[0], e->ctl, gate, st);
+  const int res = radix_sort_pairs(e->rs, n, e->key_bits, true, gate, st);
+  CK(cudaMemsetAsync(e->cstart, 0xff, sizeof(uint32_t) * e->ncell_tab, st));
+  ens_launch_reorder(e->b, e->cur, n, e->rs.keys[res], e->rs.vals[res], e->cstart, e->cend,
+                     e->ncell_tab, e->ctl, gate, st);
+  ens_launch_nlist(g, e->b, n, e->rs.vals[res], e->cstart, e->cend, e->ctl, gate, st);
+  ens_launch_epoch(e->ctl, gate, st);
+  return 0;
+}
+
+int rebuild_kernel_count(const blaze_ens* e) {
+  return 4 + 3 * std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits);
+}
+
+int enqueue_step(blaze_ens* e) {
+  launch_gate(e->ctl, e->stream);
+  int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
+  if (rc) return rc;
+  ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0},
+                  e->opt.capture_forces ? &e->cap : nullptr, e->stream);
+  e->last_launches += 2 + rebuild_kernel_count(e);
+  e->cur ^= 1;
+  return 0;
+}
+
+// kGraphSteps steps as one graph starting from S[c]: a gate kernel carries
+// the pending re-sort request into the first step's IF node; each step kernel
+// sets the next step's IF condition when any particle has moved half the skin.
+int build_graph(blaze_ens* e, int c) {
+  const int saved = e->cur;
+  e->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h[kGraphSteps];
+  for (int k = 0; k < kGraphSteps; ++k)
+    CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(e->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  launch_gate_graph(e->ctl, h[0], e->d_rb, kGraphSteps, e->stream);
+  for (int k = 0; k < kGraphSteps; ++k) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &capg, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    std::memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h[k];
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(e->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(e->aux, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    CK(cudaMemsetAsync(e->d_rb + k, 0x01, sizeof(int), e->aux));
+    int rc = enqueue_rebuild(e, nullptr, e->aux);
+    cudaGraph_t tmp = nullptr;
+    CK(cudaStreamEndCapture(e->aux, &tmp));
+    if (rc) return rc;
+    const StepLink link = k + 1 < kGraphSteps ? StepLink{e->d_rb + k, h[k + 1], 1}
+                                               : StepLink{e->d_rb + k, 0, 0};
+    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link,
+                    e->opt.capture_forces ? &e->cap : nullptr, e->stream);
+    e->cur ^= 1;
+  }
+  cudaGraph_t out = nullptr;
+  CK(cudaStreamEndCapture(e->stream, &out));
+  CK(cudaGraphInstantiate(&e->graph[c], out, 0));
+  CK(cudaGraphDestroy(out));
+  e->cur = saved;
+  return 0;
+}
+
+int sync_status(blaze_ens* e) {
+  CK(cudaMemcpyAsync(e->h_ctl, e->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaGetLastError());
+  e->status |= e->h_ctl->status;
+  return (int)e->status;
+}
+
+int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const blaze_wall* walls,
+                int nwalls, const blaze_ens_options* opt) {
+  if (!out || !systems || nsys < 1 || nsys > (int)kSysMask || nwalls < 0 || (nwalls && !walls))
+    return -1;
+  blaze_ens_options o;
+  if (opt) o = *opt;
+  else blaze_ens_default_options(&o);
+  if ((o.law != BLAZE_LAW_LINEAR && o.law != BLAZE_LAW_HERTZ_MINDLIN) || !(o.dt > 0.0f) ||
+      !(o.skin > 0.0f) || o.max_nbr < 1 || o.max_nbr > 32)
+    return -1;
+  long long ntot = 0, cells = 0;
+  for (int s = 0; s < nsys; ++s) {
+    if (!valid_system(systems[s], nwalls, o.skin)) return -1;
+    ntot += systems[s].n;
+    cells += (long long)systems[s].ncells[0] * systems[s].ncells[1] * systems[s].ncells[2];
+  }
+  for (int w = 0; w < nwalls; ++w)
+    if (walls[w].kind < BLAZE_WALL_PLANE || walls[w].kind > BLAZE_WALL_CYLINDER) return -1;
+  for (int s = 0; s < nsys; ++s) {
+    for (int w = systems[s].wall0; w < systems[s].wall0 + systems[s].nwalls; ++w)
+      if (walls[w].kind == BLAZE_WALL_TRIANGLE) return -1;
+    for (int w = systems[s].tri0; w < systems[s].tri0 + systems[s].ntris; ++w)
+      if (walls[w].kind != BLAZE_WALL_TRIANGLE) return -1;
+  }
+  if (ntot < 1 || ntot > (1ll << 30) || cells + 1 >= (1ll << 32)) return -1;
+
+  blaze_ens* e = new (std::nothrow) blaze_ens();
+  if (!e) return -1;
+  auto fail = [&](int rc) { free_ens(e); return rc; };
+#define CKF(x) do { cudaError_t e2 = (x); if (e2 != cudaSuccess) return fail(cuda_fail(e2)); } while (0)
+  e->opt = o;
+  e->nsys = nsys;
+  e->n = (int)ntot;
+  e->nwalls = nwalls;
+  e->sys.assign(systems, systems + nsys);
+  e->ncell_tab = (uint32_t)cells;
+  for (int w = 0; w < nwalls; ++w) e->hwalls.push_back(wall_dev(walls[w]));
+  const uint32_t top = e->ncell_tab + 1u;
+  e->key_bits = 1;
+  while (e->key_bits < 32 && (top >> e->key_bits) != 0) e->key_bits++;
+  CKF(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  CKF(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
+  const int n = e->n;
+  const int cap = o.max_nbr;
+  e->b.stride = n;
+  e->b.cap = cap;
+  for (int k = 0; k < 3; ++k) {
+    CKF(dalloc(&e->b.S[k].pos, n)); CKF(dalloc(&e->b.S[k].vel, n)); CKF(dalloc(&e->b.S[k].angv, n));
+  }
+  for (int k = 0; k < 2; ++k) {
+    CKF(dalloc(&e->b.pid[k], n));
+    CKF(dalloc(&e->b.wh[k], (size_t)kWallSlots * n));
+    CKF(dalloc(&e->b.L[k].idx, (size_t)cap * n));
+    CKF(dalloc(&e->b.L[k].cnt, n));
+    CKF(dalloc(&e->b.L[k].mask, n));
+    CKF(dalloc(&e->b.L[k].hx, (size_t)cap * n));
+    CKF(dalloc(&e->b.L[k].hy, (size_t)cap * n));
+    CKF(dalloc(&e->b.L[k].hz, (size_t)cap * n));
+    CKF(dalloc(&e->rs.keys[k], n));
+    CKF(dalloc(&e->rs.vals[k], n));
+    CKF(cudaMemset(e->b.L[k].cnt, 0, sizeof(uint32_t) * n));
+    CKF(cudaMemset(e->b.L[k].mask, 0, sizeof(uint32_t) * n));
+  }
+  const int tiles = (n + kTileKeys - 1) / kTileKeys;
+  e->rs.max_n = n;
+  e->rs.max_tiles = tiles;
+  CKF(dalloc(&e->rs.counts, (size_t)kRadixDigits * std::max(tiles, 1)));
+  CKF(dalloc(&e->rs.totals, kRadixDigits));
+  CKF(dalloc(&e->cstart, e->ncell_tab));
+  CKF(dalloc(&e->cend, e->ncell_tab));
+  CKF(dalloc(&e->ctl, 1));
+  CKF(dalloc(&e->d_rb, kGraphSteps));
+  CKF(cudaMemset(e->d_rb, 0, sizeof(int) * kGraphSteps));
+  CKF(dalloc(&e->d_sys, nsys));
+  CKF(dalloc(&e->d_walls, nwalls));
+  CKF(dalloc(&e->d_sys_of, n));
+  CKF(dalloc(&e->st_pos3, (size_t)3 * n));
+  CKF(dalloc(&e->st_rad, n));
+  CKF(dalloc(&e->st_vel3, (size_t)3 * n));
+  CKF(dalloc(&e->st_avel3, (size_t)3 * n));
+  CKF(dalloc(&e->st_sys, n));
+  CKF(dalloc(&e->st_pid, n));
+  CKF(dalloc(&e->d_flags, 2));
+  CKF(cudaMallocHost((void**)&e->h_flags, 2 * sizeof(int)));
+  CKF(cudaMallocHost((void**)&e->h_ctl, sizeof(StepCtl)));
+  if (o.capture_forces) {
+    CKF(dalloc(&e->cap.f, n));
+    CKF(dalloc(&e->cap.t, n));
+    CKF(cudaMemset(e->cap.f, 0, sizeof(float4) * n));
+    CKF(cudaMemset(e->cap.t, 0, sizeof(float4) * n));
+  }
+  for (int k = 0; k < 3; ++k) {
+    CKF(cudaMemset(e->b.S[k].pos, 0, sizeof(float4) * n));
+    CKF(cudaMemset(e->b.S[k].vel, 0, sizeof(float4) * n));
+    CKF(cudaMemset(e->b.S[k].angv, 0, sizeof(float4) * n));
+  }
+  {
+    std::vector<int> so(n);
+    int k = 0;
+    for (int s = 0; s < nsys; ++s)
+      for (int q = 0; q < systems[s].n; ++q) so[k++] = s;
+    CKF(cudaMemcpy(e->d_sys_of, so.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  }
+  if (nwalls)
+    CKF(cudaMemcpy(e->d_walls, e->hwalls.data(), sizeof(EnsWallDev) * nwalls,
+                   cudaMemcpyHostToDevice));
+  int rc = upload_params(e);
+  if (rc) return fail(rc);
+  bool any_tri = false;
+  for (int s = 0; s < nsys; ++s) any_tri = any_tri || systems[s].ntris > 0;
+  if (any_tri) {
+    std::vector<uint32_t> off, ids;
+    build_tri_lists(e, off, ids);
+    CKF(dalloc(&e->d_tri_off, off.size()));
+    CKF(dalloc(&e->d_tri_ids, ids.size()));
+    CKF(cudaMemcpy(e->d_tri_off, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice));
+    if (!ids.empty())
+      CKF(cudaMemcpy(e->d_tri_ids, ids.data(), sizeof(uint32_t) * ids.size(), cudaMemcpyHostToDevice));
+  }
+  std::memset(e->h_ctl, 0, sizeof(StepCtl));
+  e->h_ctl->n_cur = n;
+  e->h_ctl->rebuild_req = 1;
+  CKF(cudaMemcpy(e->ctl, e->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice));
+  CKF(cudaDeviceSynchronize());
+#undef CKF
+  *out = e;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void blaze_ens_default_options(blaze_ens_options* o) {
+  if (!o) return;
+  o->law = BLAZE_LAW_LINEAR;
+  o->dt = 1e-5f;
+  o->skin = 0.02f;
+  o->max_nbr = 32;
+  o->use_graph = 1;
+  o->capture_forces = 0;
+}
+
+int blaze_ens_create(blaze_ens** out, const blaze_system* systems, int nsys,
+                     const blaze_wall* walls, int nwalls, const blaze_ens_options* opt) {
+  return create_impl(out, systems, nsys, walls, nwalls, opt);
+}
+
+int blaze_ens_destroy(blaze_ens* e) {
+  if (!e) return -1;
+  cudaStreamSynchronize(e->stream);
+  free_ens(e);
+  return 0;
+}
+
+int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, const float* vel3,
+                        const float* avel3) {
+  if (!e || !pos3 || !radius) return -1;
+  const int n = e->n;
+  // every radius must fit its system's cell: 2 r + skin <= cell
+  {
+    int k = 0;
+    for (int s = 0; s < e->nsys; ++s) {
+      const float lim = 0.5f * (e->sys[s].cell - e->opt.skin);
+      for (int q = 0; q < e->sys[s].n; ++q, ++k)
+        if (!(radius[k] > 0.0f) || radius[k] > lim) return -1;
+    }
+  }
+  int rc = sync_status(e);
+  if (rc < 0) return rc;
+  CK(cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(int), e->stream));
+  CK(cudaMemcpyAsync(e->st_pos3, pos3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemcpyAsync(e->st_rad, radius, sizeof(float) * n, cudaMemcpyHostToDevice, e->stream));
+  if (vel3)
+    CK(cudaMemcpyAsync(e->st_vel3, vel3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, e->stream));
+  if (avel3)
+    CK(cudaMemcpyAsync(e->st_avel3, avel3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, e->stream));
+  const int ep = e->h_ctl->epoch & 1;
+  ens_launch_pack(e->st_pos3, e->st_rad, vel3 ? e->st_vel3 : nullptr, avel3 ? e->st_avel3 : nullptr,
+                  e->d_sys_of, e->b, e->cur, e->b.pid[ep], n, e->d_flags, e->stream);
+  CK(cudaMemcpyAsync(e->h_flags, e->d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaGetLastError());
+  if (e->h_flags[0]) return -1;
+  StepCtl c = *e->h_ctl;
+  c.rebuild_req = 1;
+  c.rebuilt = 0;
+  c.status = 0;
+  c.n_cur = n;
+  c.pending_dead = 0;
+  *e->h_ctl = c;
+  e->status = 0;
+  CK(cudaMemcpyAsync(e->ctl, e->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->state_set = true;
+  return 0;
+}
+
+int blaze_ens_get_state(blaze_ens* e, float* pos3, float* radius, float* vel3, float* avel3,
+                        int* sys, int* pid) {
+  if (!e) return -1;
+  int st = sync_status(e);
+  if (st < 0) return st;
+  const int n = e->n;
+  const int ep = e->h_ctl->epoch & 1;
+  ens_launch_unpack(e->b, e->cur, n, e->b.pid[ep], e->st_pos3, e->st_rad, e->st_vel3, e->st_avel3,
+                    e->st_sys, e->st_pid, e->stream);
+  if (pos3) CK(cudaMemcpyAsync(pos3, e->st_pos3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (radius) CK(cudaMemcpyAsync(radius, e->st_rad, sizeof(float) * n, cudaMemcpyDeviceToHost, e->stream));
+  if (vel3) CK(cudaMemcpyAsync(vel3, e->st_vel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (avel3) CK(cudaMemcpyAsync(avel3, e->st_avel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, e->stream));
+  if (sys) CK(cudaMemcpyAsync(sys, e->st_sys, sizeof(int) * n, cudaMemcpyDeviceToHost, e->stream));
+  if (pid) CK(cudaMemcpyAsync(pid, e->st_pid, sizeof(int) * n, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaGetLastError());
+  return st;
+}
+
+int blaze_ens_step(blaze_ens* e, int nsteps) {
+  if (!e || nsteps < 0 || !e->state_set) return -1;
+  e->last_launches = 0;
+  int done = 0;
+  while (done < nsteps) {
+    if (!e->opt.use_graph || nsteps - done < kGraphSteps) {
+      int rc = enqueue_step(e);
+      if (rc) return rc;
+      done += 1;
+      continue;
+    }
+    const int c = e->cur;
+    if (!e->graph[c]) {
+      int rc = build_graph(e, c);
+      if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(e->graph[c], e->stream));
+    e->last_launches += 1 + kGraphSteps;
+    if (kGraphSteps & 1) e->cur ^= 1;
+    done += kGraphSteps;
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int blaze_ens_sync(blaze_ens* e) {
+  if (!e) return -1;
+  return sync_status(e);
+}
+
+int blaze_ens_set_params(blaze_ens* e, const blaze_system* systems) {
+  if (!e || !systems) return -1;
+  for (int s = 0; s < e->nsys; ++s) {
+    const blaze_system& a = e->sys[s];
+    const blaze_system& b = systems[s];
+    if (b.n != a.n || b.cell != a.cell || b.ncells[0] != a.ncells[0] || b.ncells[1] != a.ncells[1] ||
+        b.ncells[2] != a.ncells[2] || b.origin[0] != a.origin[0] || b.origin[1] != a.origin[1] ||
+        b.origin[2] != a.origin[2] || b.wall0 != a.wall0 || b.nwalls != a.nwalls ||
+        b.tri0 != a.tri0 || b.ntris != a.ntris || !valid_system(b, e->nwalls, e->opt.skin))
+      return -1;
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  e->sys.assign(systems, systems + e->nsys);
+  return upload_params(e);
+}
+
+int blaze_ens_get_forces(blaze_ens* e, float* force3, float* torque3) {
+  if (!e || !e->opt.capture_forces) return -1;
+  int st = sync_status(e);
+  if (st < 0) return st;
+  const int n = e->n;
+  std::vector<float4> f(n), t(n);
+  CK(cudaMemcpy(f.data(), e->cap.f, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(t.data(), e->cap.t, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; ++i) {
+    if (force3) { force3[3 * i] = f[i].x; force3[3 * i + 1] = f[i].y; force3[3 * i + 2] = f[i].z; }
+    if (torque3) { torque3[3 * i] = t[i].x; torque3[3 * i + 1] = t[i].y; torque3[3 * i + 2] = t[i].z; }
+  }
+  return st;
+}
+
+int blaze_ens_num_rebuilds(blaze_ens* e) {
+  if (!e) return -1;
+  int rc = sync_status(e);
+  if (rc < 0) return rc;
+  return e->h_ctl->epoch;
+}
+
+int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4, void** stream) {
+  if (!e) return -1;
+  if (pos4) *pos4 = e->b.S[e->cur].pos;
+  if (vel4) *vel4 = e->b.S[e->cur].vel;
+  if (angv4) *angv4 = e->b.S[e->cur].angv;
+  if (stream) *stream = (void*)e->stream;
+  return 0;
+}
+
+int blaze_ens_last_launches(blaze_ens* e) { return e ? e->last_launches : -1; }
+
+int blaze_ens_rebuild_kernels(blaze_ens* e) { return e ? rebuild_kernel_count(e) : -1; }
+
+}  // extern "C"

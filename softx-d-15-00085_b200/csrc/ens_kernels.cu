@@ -1,0 +1,557 @@
+// ens_kernels.cu -- kernels of the ensemble path (see ens_kernels.cuh).
+//
+//   k_ens_hash     system-prefixed cell key per particle
+//   [radix sort, radix_sort.cu]
+//   k_ens_reorder  gather state, pid and wall history into sorted order + cell table
+//   k_ens_nlist    27-cell Verlet list inside the particle's own system, carrying
+//                  the tangential history of every surviving contact by partner pid
+//   k_ens_epoch    one thread: the new list becomes current
+//   k_ens_step     pair law + walls + symplectic Euler, fused, gather only
+//
+// The contact model (per pair, with m* = ma mb / (ma + mb), R* = ra rb / (ra + rb),
+// overlap d, unit normal n from b to a, v_n = (va - vb) . n):
+//   linear        f_n = kn d - c_n v_n,  c_n = 2 beta sqrt(m* kn);  k_t = kt,
+//                 c_t = 2 beta sqrt(m* kt)
+//   Hertz-Mindlin S_n = 2 E* sqrt(R* d), f_n = 2/3 S_n d - c_n v_n,
+//                 c_n = 2 sqrt(5/6) beta sqrt(S_n m*);  k_t = 8 G* sqrt(R* d),
+//                 c_t = 2 sqrt(5/6) beta sqrt(k_t m*)
+//   with beta = -ln e / sqrt(ln^2 e + pi^2); f_n is not clamped (the damping
+//   may pull at the end of a contact, so the linear law rebounds with e).
+//   Tangential: the history xi is turned into the tangent plane (length
+//   kept), advanced by v_t dt, f_t = -k_t xi - c_t v_t, capped at
+//   mu max(f_n, 0) (xi then set back to the spring length that gives the
+//   capped force).  Rolling friction: a torque -mu_r max(f_n, 0) R* w_rel / |w_rel|.
+//   Walls use the same law with R* = r, m* = m.
+#include "ens_kernels.cuh"
+
+namespace blaze {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void ens_flag(StepCtl* ctl, uint32_t bits) {
+  const unsigned m = __activemask();
+  const uint32_t all = __reduce_or_sync(m, bits);
+  if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
+}
+
+__device__ __forceinline__ int3 ens_cell(const EnsSysDev& S, float3 p) {
+  int3 c;
+  c.x = (int)floorf((p.x - S.origin.x) / S.cell);
+  c.y = (int)floorf((p.y - S.origin.y) / S.cell);
+  c.z = (int)floorf((p.z - S.origin.z) / S.cell);
+  return c;
+}
+__device__ __forceinline__ bool ens_in(const EnsSysDev& S, int3 c) {
+  return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < S.nc.x && c.y < S.nc.y && c.z < S.nc.z;
+}
+__device__ __forceinline__ uint32_t ens_key(const EnsSysDev& S, int3 c) {
+  return S.cell_off + (uint32_t)(c.x + S.nc.x * (c.y + S.nc.y * c.z));
+}
+__device__ __forceinline__ float sphere_mass(const EnsSysDev& S, float r) {
+  return S.dens43pi * ((r * r) * r);
+}
+
+// ------------------------------------------------------------- contact law
+template <int kLaw>
+__device__ __forceinline__ void contact_law(const EnsSysDev& S, float mu, float3 n, float delta,
+                                            float rs, float ms, float3 vrel, float3 vct,
+                                            float3 wrel, float arm, float dt, float3& xi,
+                                            float3& F, float3& T) {
+  const float vn = dot3(vrel, n);
+  float kn_e, cn, kt_e, ct;
+  if (kLaw == kLawLinear) {
+    kn_e = S.kn;
+    kt_e = S.kt;
+    cn = S.beta2 * sqrtf(ms * S.kn);
+    ct = S.beta2 * sqrtf(ms * S.kt);
+  } else {
+    const float sq = sqrtf(rs * delta);
+    const float sn = (2.0f * S.estar) * sq;
+    kn_e = 0.6666667f * sn;
+    kt_e = (8.0f * S.gstar) * sq;
+    cn = S.beta2h * sqrtf(sn * ms);
+    ct = S.beta2h * sqrtf(kt_e * ms);
+  }
+  const float fn = kn_e * delta - cn * vn;
+  const float fc = fn > 0.0f ? fn : 0.0f;  // compressive part: friction bound
+  const float3 vt = vct - dot3(vct, n) * n;
+  const float xn = dot3(xi, n);
+  if (xn != 0.0f) {
+    const float m0 = dot3(xi, xi);
+    xi = xi - xn * n;
+    const float m1 = dot3(xi, xi);
+    if (m1 > 0.0f) xi = xi * sqrtf(m0 / m1);
+  }
+  xi = xi + vt * dt;
+  float3 ft = xi * (-kt_e) - vt * ct;
+  const float cap = mu * fc;
+  const float f2 = dot3(ft, ft);
+  if (f2 > cap * cap) {
+    const float s = cap / sqrtf(f2);
+    ft = ft * s;
+    xi = (ft + vt * ct) * (-1.0f / kt_e);
+  }
+  F = n * fn + ft;
+  T = cross3(n * (-arm), F);
+  if (S.mu_r > 0.0f) {
+    const float w2 = dot3(wrel, wrel);
+    if (w2 > 0.0f) T = T + wrel * (-((S.mu_r * fc) * rs) / sqrtf(w2));
+  }
+}
+
+// Closest point of triangle (a, b, c) to p by Voronoi regions of the
+// vertices, edges and face (Ericson, Real-Time Collision Detection, 5.1.5).
+// region: 0 face interior, 1 edge, 2 vertex.
+__device__ __forceinline__ float3 closest_on_triangle(float3 p, float3 a, float3 b, float3 c,
+                                                      int& region) {
+  const float3 ab = b - a, ac = c - a, ap = p - a;
+  const float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) { region = 2; return a; }
+  const float3 bp = p - b;
+  const float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) { region = 2; return b; }
+  const float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+    region = 1;
+    return a + ab * (d1 / (d1 - d3));
+  }
+  const float3 cp = p - c;
+  const float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) { region = 2; return c; }
+  const float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+    region = 1;
+    return a + ac * (d2 / (d2 - d6));
+  }
+  const float va = d3 * d6 - d5 * d4;
+  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+    region = 1;
+    return b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
+  }
+  const float den = 1.0f / ((va + vb) + vc);
+  region = 0;
+  return a + ab * (vb * den) + ac * (vc * den);
+}
+
+// Contact of a sphere (centre p, radius r) with one wall: normal from the
+// wall to the centre, overlap; false when not touching.
+__device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float r, float3& n,
+                                           float& delta, int& region) {
+  region = 0;
+  if (W.kind == kWallPlane) {
+    const float s = dot3(W.a, p) - W.r;
+    if (!(s < r)) return false;
+    n = W.a;
+    delta = r - s;
+    return true;
+  }
+  if (W.kind == kWallCylinder) {
+    const float3 v = p - W.a;
+    const float3 rad = v - dot3(v, W.b) * W.b;
+    const float rho = len3(rad);
+    if (!(rho + r > W.r) || !(rho > 0.0f)) return false;
+    n = rad * (-1.0f / rho);
+    delta = (rho + r) - W.r;
+    return true;
+  }
+  const float3 q = closest_on_triangle(p, W.a, W.b, W.c, region);
+  const float3 d = p - q;
+  const float d2 = dot3(d, d);
+  if (!(d2 < r * r)) return false;
+  const float dist = sqrtf(d2);
+  if (!(dist > 0.0f)) return false;
+  n = d * (1.0f / dist);
+  delta = r - dist;
+  return true;
+}
+
+// ------------------------------------------------------------------- hash
+__global__ void __launch_bounds__(kThreads)
+k_ens_hash(EnsGeom g, const float4* __restrict__ pos, const float4* __restrict__ vel, int n,
+           uint32_t* __restrict__ keys, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t sys = __float_as_uint(vel[i].w) & kSysMask;
+  const EnsSysDev& S = g.sys[sys];
+  const int3 c = ens_cell(S, xyz(pos[i]));
+  uint32_t st = 0, key;
+  if (ens_in(S, c)) {
+    key = ens_key(S, c);
+  } else {
+    key = g.ncell_tab;
+    st = kStatusOutOfGrid;
+  }
+  keys[i] = key;
+  ens_flag(ctl, st);
+}
+
+// ---------------------------------------------------------------- reorder
+__global__ void __launch_bounds__(kThreads)
+k_ens_reorder(StateBuf src, StateBuf dst, EnsBufs b, int n, const uint32_t* __restrict__ keys,
+              const int32_t* __restrict__ perm, uint32_t* __restrict__ cstart,
+              uint32_t* __restrict__ cend, uint32_t ncell_tab, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = ctl->epoch & 1;
+  const int j = perm[i];
+  dst.pos[i] = src.pos[j];
+  const float4 v = src.vel[j];
+  dst.vel[i] = v;
+  float4 w = src.angv[j];
+  w.w = 0.0f;
+  dst.angv[i] = w;
+  b.pid[e ^ 1][i] = b.pid[e][j];
+  if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      b.wh[e ^ 1][(size_t)q * b.stride + i] = b.wh[e][(size_t)q * b.stride + j];
+  }
+  const uint32_t k = keys[i];
+  if (k < ncell_tab) {
+    if (i == 0 || keys[i - 1] != k) cstart[k] = (uint32_t)i;
+    if (i == n - 1 || keys[i + 1] != k) cend[k] = (uint32_t)i + 1u;
+  }
+}
+
+// ------------------------------------------------------------------ nlist
+// Pairs with |xi - xj|^2 < (ri + rj + skin)^2 from the 27 surrounding cells
+// of the particle's own system (z, y, x order; j ascending inside a cell).
+// The history of a slot of the old list moves to the new slot of the same
+// partner (matched by pid).
+__global__ void __launch_bounds__(kThreads)
+k_ens_nlist(EnsGeom g, EnsBufs b, const float4* __restrict__ pos, const float4* __restrict__ vel,
+            int n, const int32_t* __restrict__ perm, const uint32_t* __restrict__ cstart,
+            const uint32_t* __restrict__ cend, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = ctl->epoch & 1;
+  const EnsList Lo = b.L[e], Ln = b.L[e ^ 1];
+  const int* pid_old = b.pid[e];
+  const int* pid_new = b.pid[e ^ 1];
+  const size_t stride = (size_t)b.stride;
+  const float4 pa4 = pos[i];
+  const float3 pa = xyz(pa4);
+  const float ra = pa4.w;
+  const uint32_t sys = __float_as_uint(vel[i].w) & kSysMask;
+  const EnsSysDev& S = g.sys[sys];
+  const int3 c = ens_cell(S, pa);
+  const int io = perm[i];
+  const uint32_t cnt_o = Lo.cnt[io];
+  const uint32_t mask_o = Lo.mask[io];
+  uint32_t cnt = 0, mask = 0, st = 0;
+  if (ens_in(S, c)) {
+    const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < S.nc.x - 1 ? c.x + 1 : c.x;
+    const int y0 = c.y > 0 ? c.y - 1 : 0, y1 = c.y < S.nc.y - 1 ? c.y + 1 : c.y;
+    const int z0 = c.z > 0 ? c.z - 1 : 0, z1 = c.z < S.nc.z - 1 ? c.z + 1 : c.z;
+    for (int z = z0; z <= z1; ++z)
+      for (int y = y0; y <= y1; ++y) {
+        const uint32_t row = S.cell_off + (uint32_t)(S.nc.x * (y + S.nc.y * z));
+        for (int x = x0; x <= x1; ++x) {
+          const uint32_t h = row + (uint32_t)x;
+          const uint32_t s = __ldg(cstart + h);
+          if (s == 0xffffffffu) continue;
+          const uint32_t eo = __ldg(cend + h);
+          for (uint32_t j = s; j < eo; ++j) {
+            if ((int)j == i) continue;
+            const float4 pb = __ldg(pos + j);
+            const float3 rel = pa - xyz(pb);
+            const float lim = (ra + pb.w) + g.skin;
+            if (!(dot3(rel, rel) < lim * lim)) continue;
+            if (cnt < (uint32_t)b.cap) {
+              Ln.idx[cnt * stride + i] = j;
+              uint32_t mo = mask_o;
+              if (mo) {
+                const int pj = pid_new[j];
+                while (mo) {
+                  const int ko = __ffs(mo) - 1;
+                  mo &= mo - 1u;
+                  if ((uint32_t)ko >= cnt_o) break;
+                  const size_t so = (size_t)ko * stride + io;
+                  if (pid_old[Lo.idx[so]] == pj) {
+                    const size_t sn = (size_t)cnt * stride + i;
+                    Ln.hx[sn] = Lo.hx[so];
+                    Ln.hy[sn] = Lo.hy[so];
+                    Ln.hz[sn] = Lo.hz[so];
+                    mask |= 1u << cnt;
+                    break;
+                  }
+                }
+              }
+            } else {
+              st |= kStatusListOverflow;
+            }
+            ++cnt;
+          }
+        }
+      }
+  } else {
+    st |= kStatusOutOfGrid;
+  }
+  Ln.cnt[i] = cnt < (uint32_t)b.cap ? cnt : (uint32_t)b.cap;
+  Ln.mask[i] = mask;
+  ens_flag(ctl, st);
+}
+
+__global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  ctl->epoch += 1;
+}
+
+// ------------------------------------------------------------------- step
+template <int kLaw, bool kCapture>
+__global__ void __launch_bounds__(kThreads)
+k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
+           StepCtl* ctl, StepLink link, EnsCapture cap) {
+  const bool rebuilt = *link.rebuilt != 0;
+  const StateBuf in = rebuilt ? in_sorted : in_plain;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = ctl->epoch & 1;
+  const EnsList L = b.L[e];
+  const size_t stride = (size_t)b.stride;
+  const float dt = g.dt;
+  const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
+  const float3 pa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
+  const float ra = pa4.w;
+  const uint32_t bits = __float_as_uint(va4.w);
+  const uint32_t sys = bits & kSysMask;
+  const uint32_t wmask_o = bits >> kSysBits;
+  const EnsSysDev& S = g.sys[sys];
+  const float ma = sphere_mass(S, ra);
+  uint32_t st = 0;
+
+  // particle-particle contacts, in list order
+  float3 f = f3(0.0f, 0.0f, 0.0f), t = f3(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = L.cnt[i];
+  const uint32_t mask_o = L.mask[i];
+  uint32_t mask = 0;
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t sk = (size_t)k * stride + i;
+    const uint32_t j = L.idx[sk];
+    const float4 pb4 = __ldg(in.pos + j);
+    const float3 rel = pa - xyz(pb4);
+    const float rb = pb4.w;
+    const float sr = ra + rb;
+    const float d2 = dot3(rel, rel);
+    if (!(d2 < sr * sr)) continue;
+    const float dist = sqrtf(d2);
+    if (!(dist > 0.0f)) continue;
+    const float3 nrm = rel * (1.0f / dist);
+    const float delta = sr - dist;
+    const float4 vb4 = __ldg(in.vel + j), wb4 = __ldg(in.angv + j);
+    const float3 vb = xyz(vb4), wb = xyz(wb4);
+    const float mb = sphere_mass(S, rb);
+    float3 xi = f3(0.0f, 0.0f, 0.0f);
+    if ((mask_o >> k) & 1u) xi = f3(L.hx[sk], L.hy[sk], L.hz[sk]);
+    const float rs = (ra * rb) / (ra + rb);
+    const float ms = (ma * mb) / (ma + mb);
+    const float3 vcpa = va + cross3(wa, nrm * (-ra));
+    const float3 vcpb = vb + cross3(wb, nrm * rb);
+    float3 F, T;
+    contact_law<kLaw>(S, S.mu, nrm, delta, rs, ms, va - vb, vcpa - vcpb, wa - wb, ra, dt, xi,
+                      F, T);
+    L.hx[sk] = xi.x;
+    L.hy[sk] = xi.y;
+    L.hz[sk] = xi.z;
+    mask |= 1u << k;
+    f = f + F;
+    t = t + T;
+  }
+  if (mask != mask_o) L.mask[i] = mask;
+
+  // walls: old history slots (by wall id), new slots in processing order
+  float4 oh[kWallSlots], nh[kWallSlots];
+#pragma unroll
+  for (int q = 0; q < kWallSlots; ++q) {
+    oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+    nh[q] = oh[q];
+  }
+  if (wmask_o) {
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if ((wmask_o >> q) & 1u) oh[q] = b.wh[e][(size_t)q * stride + i];
+  }
+  int nw = 0;
+  auto wall_contact = [&](int id, float3 nrm, float delta) {
+    float3 xi = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if (__float_as_int(oh[q].w) == id) xi = f3(oh[q].x, oh[q].y, oh[q].z);
+    const float3 vcpa = va + cross3(wa, nrm * (-ra));
+    float3 F, T;
+    contact_law<kLaw>(S, S.mu_w, nrm, delta, ra, ma, va, vcpa, wa, ra, dt, xi, F, T);
+    f = f + F;
+    t = t + T;
+    if (nw < kWallSlots) {
+#pragma unroll
+      for (int q = 0; q < kWallSlots; ++q)
+        if (q == nw) nh[q] = make_float4(xi.x, xi.y, xi.z, __int_as_float(id));
+      ++nw;
+    } else {
+      st |= kStatusListOverflow;
+    }
+  };
+  for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
+    const EnsWallDev W = g.walls[w];
+    float3 nrm;
+    float delta;
+    int region;
+    if (wall_touch(W, pa, ra, nrm, delta, region)) wall_contact(w, nrm, delta);
+  }
+  if (g.tri_off) {
+    const int3 c = ens_cell(S, pa);
+    if (ens_in(S, c)) {
+      const uint32_t h = ens_key(S, c);
+      const uint32_t o0 = __ldg(g.tri_off + h), o1 = __ldg(g.tri_off + h + 1);
+      // face contacts all count; without one, only the deepest edge/vertex
+      // contact does (a sphere over a shared edge or vertex touches it once)
+      int nface = 0, best = -1;
+      float best_d = 0.0f;
+      for (uint32_t q = o0; q < o1; ++q) {
+        const int id = (int)__ldg(g.tri_ids + q);
+        float3 nrm;
+        float delta;
+        int region;
+        if (!wall_touch(g.walls[id], pa, ra, nrm, delta, region)) continue;
+        if (region == 0) ++nface;
+        else if (best < 0 || delta > best_d) { best = id; best_d = delta; }
+      }
+      for (uint32_t q = o0; q < o1; ++q) {
+        const int id = (int)__ldg(g.tri_ids + q);
+        float3 nrm;
+        float delta;
+        int region;
+        if (!wall_touch(g.walls[id], pa, ra, nrm, delta, region)) continue;
+        if ((nface > 0 && region == 0) || (nface == 0 && id == best)) wall_contact(id, nrm, delta);
+      }
+    }
+  }
+  if (wmask_o || nw) {
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if (q < nw) b.wh[e][(size_t)q * stride + i] = nh[q];
+  }
+  const uint32_t wmask = nw >= kWallSlots ? (1u << kWallSlots) - 1u : (1u << nw) - 1u;
+
+  // symplectic Euler
+  const float inv_m = 1.0f / ma;
+  const float3 acc = f * inv_m + S.gravity;
+  const float3 v = va + acc * dt;
+  const float3 p = pa + v * dt;
+  const float inertia = (0.4f * ma) * (ra * ra);
+  const float3 w = wa + (t * (1.0f / inertia)) * dt;
+  const float path = wa4.w + len3(v) * dt;
+  out.pos[i] = make_float4(p.x, p.y, p.z, ra);
+  out.vel[i] = make_float4(v.x, v.y, v.z, __uint_as_float(sys | (wmask << kSysBits)));
+  out.angv[i] = make_float4(w.x, w.y, w.z, path);
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
+  {
+    const unsigned m = __activemask();
+    const unsigned req = __ballot_sync(m, path > 0.5f * g.skin);
+    if (req && (threadIdx.x & 31) == (__ffs(m) - 1)) {
+      if (link.has_next_h) cudaGraphSetConditional(link.next_h, 1u);
+      else atomicExch(&ctl->rebuild_req, 1);
+    }
+  }
+  ens_flag(ctl, st);
+  if (kCapture) {
+    cap.f[i] = make_float4(f.x, f.y, f.z, 0.0f);
+    cap.t[i] = make_float4(t.x, t.y, t.z, 0.0f);
+  }
+}
+
+// ---------------------------------------------------------------- staging
+__global__ void __launch_bounds__(kThreads)
+k_ens_pack(const float* __restrict__ pos3, const float* __restrict__ rad,
+           const float* __restrict__ vel3, const float* __restrict__ avel3,
+           const int* __restrict__ sys_of, StateBuf s, int* __restrict__ pid, EnsList L0,
+           EnsList L1, int n, int* flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float r = rad[i];
+  s.pos[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], r);
+  const float sb = __uint_as_float((uint32_t)sys_of[i] & kSysMask);
+  s.vel[i] = vel3 ? make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], sb)
+                  : make_float4(0.0f, 0.0f, 0.0f, sb);
+  s.angv[i] = avel3 ? make_float4(avel3[3 * i], avel3[3 * i + 1], avel3[3 * i + 2], 0.0f)
+                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  pid[i] = i;
+  L0.cnt[i] = 0; L0.mask[i] = 0;
+  L1.cnt[i] = 0; L1.mask[i] = 0;
+  if (!(r > 0.0f) || !isfinite(r)) atomicOr(flags, 1);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_ens_unpack(StateBuf s, const int* __restrict__ pid_src, int n, float* pos3, float* rad,
+             float* vel3, float* avel3, int* sys, int* pid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = s.pos[i], v = s.vel[i], w = s.angv[i];
+  pos3[3 * i] = p.x; pos3[3 * i + 1] = p.y; pos3[3 * i + 2] = p.z;
+  rad[i] = p.w;
+  vel3[3 * i] = v.x; vel3[3 * i + 1] = v.y; vel3[3 * i + 2] = v.z;
+  avel3[3 * i] = w.x; avel3[3 * i + 1] = w.y; avel3[3 * i + 2] = w.z;
+  sys[i] = (int)(__float_as_uint(v.w) & kSysMask);
+  pid[i] = pid_src[i];
+}
+
+inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+void ens_launch_hash(const EnsGeom& g, const EnsBufs& b, int cur, int n, uint32_t* keys,
+                     StepCtl* ctl, const int* gate, cudaStream_t st) {
+  k_ens_hash<<<nblk(n), kThreads, 0, st>>>(g, b.S[cur].pos, b.S[cur].vel, n, keys, ctl, gate);
+}
+
+void ens_launch_reorder(const EnsBufs& b, int cur, int n, const uint32_t* keys,
+                        const int32_t* perm, uint32_t* cstart, uint32_t* cend, uint32_t ncell_tab,
+                        StepCtl* ctl, const int* gate, cudaStream_t st) {
+  k_ens_reorder<<<nblk(n), kThreads, 0, st>>>(b.S[cur], b.S[2], b, n, keys, perm, cstart, cend,
+                                              ncell_tab, ctl, gate);
+}
+
+void ens_launch_nlist(const EnsGeom& g, const EnsBufs& b, int n, const int32_t* perm,
+                      const uint32_t* cstart, const uint32_t* cend, StepCtl* ctl,
+                      const int* gate, cudaStream_t st) {
+  k_ens_nlist<<<nblk(n), kThreads, 0, st>>>(g, b, b.S[2].pos, b.S[2].vel, n, perm, cstart, cend,
+                                            ctl, gate);
+}
+
+void ens_launch_epoch(StepCtl* ctl, const int* gate, cudaStream_t st) {
+  k_ens_epoch<<<1, 1, 0, st>>>(ctl, gate);
+}
+
+void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
+                     StepLink link, const EnsCapture* cap, cudaStream_t st) {
+  const EnsCapture c = cap ? *cap : EnsCapture{nullptr, nullptr};
+#define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c
+  if (g.law == kLawHertz) {
+    if (cap) k_ens_step<kLawHertz, true><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawHertz, false><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+  } else {
+    if (cap) k_ens_step<kLawLinear, true><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawLinear, false><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+  }
+#undef ENS_ARGS
+}
+
+void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,
+                     const int* sys_of, const EnsBufs& b, int cur, int* pid_dst, int n,
+                     int* flags, cudaStream_t st) {
+  k_ens_pack<<<nblk(n), kThreads, 0, st>>>(pos3, rad, vel3, avel3, sys_of, b.S[cur], pid_dst,
+                                           b.L[0], b.L[1], n, flags);
+}
+
+void ens_launch_unpack(const EnsBufs& b, int cur, int n, const int* pid_src, float* pos3,
+                       float* rad, float* vel3, float* avel3, int* sys, int* pid,
+                       cudaStream_t st) {
+  k_ens_unpack<<<nblk(n), kThreads, 0, st>>>(b.S[cur], pid_src, n, pos3, rad, vel3, avel3, sys,
+                                             pid);
+}
+
+}  // namespace blaze
