@@ -1,0 +1,554 @@
+/*
+ * ens_oracle.c -- CPU restatement of the ensemble path (include/blaze_ens.h):
+ * system-prefixed cell keys, stable sort, Verlet list with tangential-history
+ * carry-over, the linear / Hertz-Mindlin contact law with history, Coulomb
+ * cap and rolling friction, plane / cylinder / triangle walls, symplectic
+ * Euler.  Compiled twice: DEM_REAL=float follows the product's FP32
+ * operation order (compile with -ffp-contract=off), DEM_REAL=double is the
+ * FP64 oracle the FP32 error is stated against.
+ *
+ * TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg load it as the checker; the product never does.
+ *
+ * The reference has no such laws (its law is Collision_Response.cuh:374-494),
+ * so this restatement is the only pin of these results: parity unpinned vs
+ * the reference.  The step structure follows the reference's step
+ * (DeviceInterface.cu:1825-2513): hash, stable sort, reorder, cell table,
+ * 27-cell search, per-particle force gather, symplectic Euler
+ * (Integration.cuh:6-184).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/blaze_ens.h"
+
+#ifndef DEM_REAL
+#define DEM_REAL double
+#endif
+typedef DEM_REAL real;
+
+#define IS_FLOAT (sizeof(real) == sizeof(float))
+static real SQRT(real x) { return IS_FLOAT ? (real)sqrtf((float)x) : (real)sqrt((double)x); }
+static real FLOOR(real x) { return IS_FLOAT ? (real)floorf((float)x) : (real)floor((double)x); }
+
+typedef struct { real x, y, z; } v3;
+static v3 mk(real x, real y, real z) { v3 r = {x, y, z}; return r; }
+static v3 add(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static v3 sub(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static v3 mul(v3 a, real s) { return mk(a.x * s, a.y * s, a.z * s); }
+static v3 smul(real s, v3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+static real dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static real len(v3 a) { return SQRT(dot(a, a)); }
+static v3 cross(v3 a, v3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+enum { WSLOTS = 4 };
+enum { ST_OVERFLOW = 1, ST_OUT_OF_GRID = 2, ST_NONFINITE = 4 };
+
+typedef struct {
+  v3 origin;
+  real cell;
+  int nc[3];
+  uint32_t cell_off;
+  v3 g;
+  real dens43pi, kn, kt, beta2, estar, gstar, beta2h, mu, mu_w, mu_r;
+  int wall0, nwall, tri0, ntri;
+} sysc;
+
+typedef struct {
+  int kind;
+  real r;
+  v3 a, b, c;
+} wallc;
+
+typedef struct {
+  v3 pos, vel, w;
+  real r, path;
+  int sys, pid;
+  uint32_t wmask;
+  real wh[WSLOTS][3];
+  int wid[WSLOTS];
+} part;
+
+typedef struct ens_oracle ens_oracle;
+struct ens_oracle {
+  int law, n, nsys, nwalls, cap;
+  real dt, skin;
+  sysc* S;
+  wallc* W;
+  uint32_t ncell_tab;
+  part* p;      /* current state, memory order */
+  part* q;      /* scratch */
+  /* two list copies: idx, cnt, mask, history */
+  uint32_t* idx[2];
+  uint32_t* cnt[2];
+  uint32_t* mask[2];
+  real* hist[2];    /* [k * n + i][3] */
+  int epoch;
+  int rebuild_req;
+  uint32_t status;
+  uint32_t* cstart;
+  uint32_t* cend;
+  v3* cap_f;
+  v3* cap_t;
+  int* sys_of;      /* system of each entry of the caller's arrays */
+};
+
+static void constants(sysc* d, const blaze_system* s, uint32_t off) {
+  const double pi = 3.14159265358979323846;
+  const double e = s->restitution;
+  const double le = log(e);
+  const double beta = -le / sqrt(le * le + pi * pi);
+  const double E = s->youngs, nu = s->poisson;
+  d->origin = mk(s->origin[0], s->origin[1], s->origin[2]);
+  d->cell = s->cell;
+  d->nc[0] = s->ncells[0]; d->nc[1] = s->ncells[1]; d->nc[2] = s->ncells[2];
+  d->cell_off = off;
+  d->g = mk(s->gravity[0], s->gravity[1], s->gravity[2]);
+  /* the FP32 build rounds each constant once, as the product's host code does */
+  d->dens43pi = (real)((double)s->density * 4.0 / 3.0 * pi);
+  d->kn = s->kn;
+  d->kt = (real)((double)s->kn * (double)s->kt_ratio);
+  d->beta2 = (real)(2.0 * beta);
+  d->estar = (real)(E / (2.0 * (1.0 - nu * nu)));
+  d->gstar = (real)(E / (4.0 * (2.0 - nu) * (1.0 + nu)));
+  d->beta2h = (real)(2.0 * sqrt(5.0 / 6.0) * beta);
+  d->mu = s->mu; d->mu_w = s->mu_wall; d->mu_r = s->mu_roll;
+  d->wall0 = s->wall0; d->nwall = s->nwalls; d->tri0 = s->tri0; d->ntri = s->ntris;
+}
+
+ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* walls, int nwalls,
+                       int law, double dt, double skin, int max_nbr) {
+  ens_oracle* o = (ens_oracle*)calloc(1, sizeof(ens_oracle));
+  o->law = law; o->nsys = nsys; o->nwalls = nwalls; o->cap = max_nbr;
+  o->dt = (real)(float)dt;
+  o->skin = (real)(float)skin;
+  o->S = (sysc*)calloc(nsys, sizeof(sysc));
+  uint32_t off = 0;
+  int n = 0;
+  for (int s = 0; s < nsys; ++s) {
+    constants(&o->S[s], &sys[s], off);
+    off += (uint32_t)sys[s].ncells[0] * sys[s].ncells[1] * sys[s].ncells[2];
+    n += sys[s].n;
+  }
+  o->ncell_tab = off;
+  o->n = n;
+  o->W = (wallc*)calloc(nwalls > 0 ? nwalls : 1, sizeof(wallc));
+  for (int w = 0; w < nwalls; ++w) {
+    const float* p = walls[w].p;
+    wallc* d = &o->W[w];
+    d->kind = walls[w].kind;
+    if (d->kind == BLAZE_WALL_PLANE) { d->a = mk(p[0], p[1], p[2]); d->r = p[3]; }
+    else if (d->kind == BLAZE_WALL_TRIANGLE) {
+      d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->c = mk(p[6], p[7], p[8]);
+    } else { d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->r = p[6]; }
+  }
+  o->p = (part*)calloc(n, sizeof(part));
+  o->q = (part*)calloc(n, sizeof(part));
+  for (int c = 0; c < 2; ++c) {
+    o->idx[c] = (uint32_t*)calloc((size_t)n * max_nbr, sizeof(uint32_t));
+    o->cnt[c] = (uint32_t*)calloc(n, sizeof(uint32_t));
+    o->mask[c] = (uint32_t*)calloc(n, sizeof(uint32_t));
+    o->hist[c] = (real*)calloc((size_t)n * max_nbr * 3, sizeof(real));
+  }
+  o->cstart = (uint32_t*)malloc(sizeof(uint32_t) * (o->ncell_tab ? o->ncell_tab : 1));
+  o->cend = (uint32_t*)malloc(sizeof(uint32_t) * (o->ncell_tab ? o->ncell_tab : 1));
+  o->cap_f = (v3*)calloc(n, sizeof(v3));
+  o->cap_t = (v3*)calloc(n, sizeof(v3));
+  o->sys_of = (int*)calloc(n, sizeof(int));
+  int k = 0;
+  for (int s = 0; s < nsys; ++s)
+    for (int m = 0; m < sys[s].n; ++m) o->sys_of[k++] = s;
+  return o;
+}
+
+void ens_destroy(ens_oracle* o) {
+  if (!o) return;
+  free(o->S); free(o->W); free(o->p); free(o->q);
+  for (int c = 0; c < 2; ++c) { free(o->idx[c]); free(o->cnt[c]); free(o->mask[c]); free(o->hist[c]); }
+  free(o->cstart); free(o->cend); free(o->cap_f); free(o->cap_t); free(o->sys_of);
+  free(o);
+}
+
+int ens_set_params(ens_oracle* o, const blaze_system* sys) {
+  for (int s = 0; s < o->nsys; ++s) constants(&o->S[s], &sys[s], o->S[s].cell_off);
+  return 0;
+}
+
+void ens_set_state(ens_oracle* o, const double* pos3, const double* rad, const double* vel3,
+                   const double* avel3) {
+  for (int i = 0; i < o->n; ++i) {
+    part* a = &o->p[i];
+    memset(a, 0, sizeof(*a));
+    a->sys = o->sys_of[i];
+    a->pos = mk((real)(float)pos3[3 * i], (real)(float)pos3[3 * i + 1], (real)(float)pos3[3 * i + 2]);
+    a->r = (real)(float)rad[i];
+    if (vel3) a->vel = mk((real)(float)vel3[3 * i], (real)(float)vel3[3 * i + 1], (real)(float)vel3[3 * i + 2]);
+    if (avel3) a->w = mk((real)(float)avel3[3 * i], (real)(float)avel3[3 * i + 1], (real)(float)avel3[3 * i + 2]);
+    a->pid = i;
+    for (int q = 0; q < WSLOTS; ++q) a->wid[q] = -1;
+  }
+  for (int c = 0; c < 2; ++c) {
+    memset(o->cnt[c], 0, sizeof(uint32_t) * o->n);
+    memset(o->mask[c], 0, sizeof(uint32_t) * o->n);
+  }
+  o->rebuild_req = 1;
+  o->status = 0;
+}
+
+static int cell_of(const sysc* S, v3 p, int c[3]) {
+  c[0] = (int)FLOOR((p.x - S->origin.x) / S->cell);
+  c[1] = (int)FLOOR((p.y - S->origin.y) / S->cell);
+  c[2] = (int)FLOOR((p.z - S->origin.z) / S->cell);
+  return c[0] >= 0 && c[1] >= 0 && c[2] >= 0 && c[0] < S->nc[0] && c[1] < S->nc[1] && c[2] < S->nc[2];
+}
+static uint32_t key_of(const sysc* S, const int c[3]) {
+  return S->cell_off + (uint32_t)(c[0] + S->nc[0] * (c[1] + S->nc[1] * c[2]));
+}
+
+typedef struct { uint32_t key; int idx; } kv;
+static int kv_cmp(const void* a, const void* b) {
+  const kv* x = (const kv*)a;
+  const kv* y = (const kv*)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+static void rebuild(ens_oracle* o) {
+  const int n = o->n, cap = o->cap;
+  const int e = o->epoch & 1;
+  kv* ks = (kv*)malloc(sizeof(kv) * n);
+  for (int i = 0; i < n; ++i) {
+    const sysc* S = &o->S[o->p[i].sys];
+    int c[3];
+    if (cell_of(S, o->p[i].pos, c)) ks[i].key = key_of(S, c);
+    else { ks[i].key = o->ncell_tab; o->status |= ST_OUT_OF_GRID; }
+    ks[i].idx = i;
+  }
+  qsort(ks, n, sizeof(kv), kv_cmp);   /* (key, index): the stable order */
+  for (uint32_t h = 0; h < o->ncell_tab; ++h) o->cstart[h] = 0xffffffffu;
+  for (int i = 0; i < n; ++i) {
+    o->q[i] = o->p[ks[i].idx];
+    o->q[i].path = 0;
+    const uint32_t k = ks[i].key;
+    if (k < o->ncell_tab) {
+      if (i == 0 || ks[i - 1].key != k) o->cstart[k] = (uint32_t)i;
+      if (i == n - 1 || ks[i + 1].key != k) o->cend[k] = (uint32_t)i + 1u;
+    }
+  }
+  /* neighbour list of the new order, history carried by partner pid */
+  uint32_t *Io = o->idx[e], *In = o->idx[e ^ 1];
+  uint32_t *Co = o->cnt[e], *Cn = o->cnt[e ^ 1];
+  uint32_t *Mo = o->mask[e], *Mn = o->mask[e ^ 1];
+  real *Ho = o->hist[e], *Hn = o->hist[e ^ 1];
+  for (int i = 0; i < n; ++i) {
+    const part* a = &o->q[i];
+    const sysc* S = &o->S[a->sys];
+    const int io = ks[i].idx;
+    const uint32_t cnt_o = Co[io], mask_o = Mo[io];
+    uint32_t cnt = 0, mask = 0;
+    int c[3];
+    if (cell_of(S, a->pos, c)) {
+      const int x0 = c[0] > 0 ? c[0] - 1 : 0, x1 = c[0] < S->nc[0] - 1 ? c[0] + 1 : c[0];
+      const int y0 = c[1] > 0 ? c[1] - 1 : 0, y1 = c[1] < S->nc[1] - 1 ? c[1] + 1 : c[1];
+      const int z0 = c[2] > 0 ? c[2] - 1 : 0, z1 = c[2] < S->nc[2] - 1 ? c[2] + 1 : c[2];
+      for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y)
+          for (int x = x0; x <= x1; ++x) {
+            const uint32_t h = S->cell_off + (uint32_t)(S->nc[0] * (y + S->nc[1] * z)) + (uint32_t)x;
+            const uint32_t s0 = o->cstart[h];
+            if (s0 == 0xffffffffu) continue;
+            for (uint32_t j = s0; j < o->cend[h]; ++j) {
+              if ((int)j == i) continue;
+              const part* b = &o->q[j];
+              const v3 rel = sub(a->pos, b->pos);
+              const real lim = (a->r + b->r) + o->skin;
+              if (!(dot(rel, rel) < lim * lim)) continue;
+              if (cnt < (uint32_t)cap) {
+                In[(size_t)cnt * n + i] = j;
+                for (uint32_t ko = 0; ko < cnt_o && ko < 32; ++ko) {
+                  if (!((mask_o >> ko) & 1u)) continue;
+                  const size_t so = (size_t)ko * n + io;
+                  if (o->p[Io[so]].pid == b->pid) {
+                    const size_t sn = (size_t)cnt * n + i;
+                    Hn[3 * sn] = Ho[3 * so]; Hn[3 * sn + 1] = Ho[3 * so + 1]; Hn[3 * sn + 2] = Ho[3 * so + 2];
+                    mask |= 1u << cnt;
+                    break;
+                  }
+                }
+              } else {
+                o->status |= ST_OVERFLOW;
+              }
+              ++cnt;
+            }
+          }
+    } else {
+      o->status |= ST_OUT_OF_GRID;
+    }
+    Cn[i] = cnt < (uint32_t)cap ? cnt : (uint32_t)cap;
+    Mn[i] = mask;
+  }
+  part* t = o->p; o->p = o->q; o->q = t;
+  o->epoch += 1;
+  free(ks);
+}
+
+static void contact_law(const ens_oracle* o, const sysc* S, real mu, v3 n, real delta, real rs,
+                        real ms, v3 vrel, v3 vct, v3 wrel, real arm, v3* xi, v3* F, v3* T) {
+  const real vn = dot(vrel, n);
+  real kn_e, cn, kt_e, ct;
+  if (o->law == BLAZE_LAW_LINEAR) {
+    kn_e = S->kn;
+    kt_e = S->kt;
+    cn = S->beta2 * SQRT(ms * S->kn);
+    ct = S->beta2 * SQRT(ms * S->kt);
+  } else {
+    const real sq = SQRT(rs * delta);
+    const real sn = ((real)2.0 * S->estar) * sq;
+    kn_e = (real)(2.0 / 3.0) * sn;
+    kt_e = ((real)8.0 * S->gstar) * sq;
+    cn = S->beta2h * SQRT(sn * ms);
+    ct = S->beta2h * SQRT(kt_e * ms);
+  }
+  const real fn = kn_e * delta - cn * vn;
+  const real fc = fn > 0 ? fn : 0;
+  const v3 vt = sub(vct, smul(dot(vct, n), n));
+  v3 x = *xi;
+  const real xn = dot(x, n);
+  if (xn != 0) {
+    const real m0 = dot(x, x);
+    x = sub(x, smul(xn, n));
+    const real m1 = dot(x, x);
+    if (m1 > 0) x = mul(x, SQRT(m0 / m1));
+  }
+  x = add(x, mul(vt, o->dt));
+  v3 ft = sub(mul(x, -kt_e), mul(vt, ct));
+  const real capf = mu * fc;
+  const real f2 = dot(ft, ft);
+  if (f2 > capf * capf) {
+    const real s = capf / SQRT(f2);
+    ft = mul(ft, s);
+    x = mul(add(ft, mul(vt, ct)), (real)-1.0 / kt_e);
+  }
+  *xi = x;
+  *F = add(mul(n, fn), ft);
+  *T = cross(mul(n, -arm), *F);
+  if (S->mu_r > 0) {
+    const real w2 = dot(wrel, wrel);
+    if (w2 > 0) *T = add(*T, mul(wrel, -((S->mu_r * fc) * rs) / SQRT(w2)));
+  }
+}
+
+static v3 closest_tri(v3 p, v3 a, v3 b, v3 c, int* region) {
+  const v3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+  const real d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0 && d2 <= 0) { *region = 2; return a; }
+  const v3 bp = sub(p, b);
+  const real d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0 && d4 <= d3) { *region = 2; return b; }
+  const real vc = d1 * d4 - d3 * d2;
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) { *region = 1; return add(a, mul(ab, d1 / (d1 - d3))); }
+  const v3 cp = sub(p, c);
+  const real d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0 && d5 <= d6) { *region = 2; return c; }
+  const real vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) { *region = 1; return add(a, mul(ac, d2 / (d2 - d6))); }
+  const real va = d3 * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+    *region = 1;
+    return add(b, mul(sub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+  }
+  const real den = (real)1.0 / ((va + vb) + vc);
+  *region = 0;
+  return add(add(a, mul(ab, vb * den)), mul(ac, vc * den));
+}
+
+static int wall_touch(const wallc* W, v3 p, real r, v3* n, real* delta, int* region) {
+  *region = 0;
+  if (W->kind == BLAZE_WALL_PLANE) {
+    const real s = dot(W->a, p) - W->r;
+    if (!(s < r)) return 0;
+    *n = W->a;
+    *delta = r - s;
+    return 1;
+  }
+  if (W->kind == BLAZE_WALL_CYLINDER) {
+    const v3 v = sub(p, W->a);
+    const v3 rad = sub(v, smul(dot(v, W->b), W->b));
+    const real rho = len(rad);
+    if (!(rho + r > W->r) || !(rho > 0)) return 0;
+    *n = mul(rad, (real)-1.0 / rho);
+    *delta = (rho + r) - W->r;
+    return 1;
+  }
+  const v3 q = closest_tri(p, W->a, W->b, W->c, region);
+  const v3 d = sub(p, q);
+  const real d2 = dot(d, d);
+  if (!(d2 < r * r)) return 0;
+  const real dist = SQRT(d2);
+  if (!(dist > 0)) return 0;
+  *n = mul(d, (real)1.0 / dist);
+  *delta = r - dist;
+  return 1;
+}
+
+typedef struct {
+  const ens_oracle* o;
+  const sysc* S;
+  const part* a;
+  real ma;
+  v3 f, t;
+  int nw;
+  real nh[WSLOTS][3];
+  int nid[WSLOTS];
+  uint32_t st;
+} wctx;
+
+static void wall_contact(wctx* c, int id, v3 n, real delta) {
+  const part* a = c->a;
+  v3 xi = mk(0, 0, 0);
+  for (int q = 0; q < WSLOTS; ++q)
+    if (((a->wmask >> q) & 1u) && a->wid[q] == id) xi = mk(a->wh[q][0], a->wh[q][1], a->wh[q][2]);
+  const v3 vcpa = add(a->vel, cross(a->w, mul(n, -a->r)));
+  v3 F, T;
+  contact_law(c->o, c->S, c->S->mu_w, n, delta, a->r, c->ma, a->vel, vcpa, a->w, a->r, &xi, &F, &T);
+  c->f = add(c->f, F);
+  c->t = add(c->t, T);
+  if (c->nw < WSLOTS) {
+    c->nh[c->nw][0] = xi.x; c->nh[c->nw][1] = xi.y; c->nh[c->nw][2] = xi.z;
+    c->nid[c->nw] = id;
+    c->nw++;
+  } else {
+    c->st |= ST_OVERFLOW;
+  }
+}
+
+static void step_once(ens_oracle* o) {
+  const int n = o->n;
+  const int rebuilt = o->rebuild_req;
+  o->rebuild_req = 0;
+  if (rebuilt) rebuild(o);
+  const int e = o->epoch & 1;
+  uint32_t* I = o->idx[e];
+  uint32_t* C = o->cnt[e];
+  uint32_t* M = o->mask[e];
+  real* H = o->hist[e];
+  const real dt = o->dt;
+  int req = 0;
+  for (int i = 0; i < n; ++i) {
+    const part* a = &o->p[i];
+    const sysc* S = &o->S[a->sys];
+    const real ra = a->r;
+    const real ma = S->dens43pi * ((ra * ra) * ra);
+    v3 f = mk(0, 0, 0), t = mk(0, 0, 0);
+    uint32_t mask = 0;
+    for (uint32_t k = 0; k < C[i]; ++k) {
+      const size_t sk = (size_t)k * n + i;
+      const part* b = &o->p[I[sk]];
+      const v3 rel = sub(a->pos, b->pos);
+      const real rb = b->r;
+      const real sr = ra + rb;
+      const real d2 = dot(rel, rel);
+      if (!(d2 < sr * sr)) continue;
+      const real dist = SQRT(d2);
+      if (!(dist > 0)) continue;
+      const v3 nrm = mul(rel, (real)1.0 / dist);
+      const real delta = sr - dist;
+      const real mb = S->dens43pi * ((rb * rb) * rb);
+      v3 xi = mk(0, 0, 0);
+      if ((M[i] >> k) & 1u) xi = mk(H[3 * sk], H[3 * sk + 1], H[3 * sk + 2]);
+      const real rs = (ra * rb) / (ra + rb);
+      const real ms = (ma * mb) / (ma + mb);
+      const v3 vcpa = add(a->vel, cross(a->w, mul(nrm, -ra)));
+      const v3 vcpb = add(b->vel, cross(b->w, mul(nrm, rb)));
+      v3 F, T;
+      contact_law(o, S, S->mu, nrm, delta, rs, ms, sub(a->vel, b->vel), sub(vcpa, vcpb),
+                  sub(a->w, b->w), ra, &xi, &F, &T);
+      H[3 * sk] = xi.x; H[3 * sk + 1] = xi.y; H[3 * sk + 2] = xi.z;
+      mask |= 1u << k;
+      f = add(f, F);
+      t = add(t, T);
+    }
+    M[i] = mask;
+    wctx c;
+    memset(&c, 0, sizeof(c));
+    c.o = o; c.S = S; c.a = a; c.ma = ma; c.f = f; c.t = t;
+    for (int w = S->wall0; w < S->wall0 + S->nwall; ++w) {
+      v3 nn; real d; int reg;
+      if (wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) wall_contact(&c, w, nn, d);
+    }
+    int cc[3];
+    if (S->ntri > 0 && cell_of(S, a->pos, cc)) {
+      int nface = 0, best = -1;
+      real best_d = 0;
+      for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+        v3 nn; real d; int reg;
+        if (!wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) continue;
+        if (reg == 0) ++nface;
+        else if (best < 0 || d > best_d) { best = w; best_d = d; }
+      }
+      for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+        v3 nn; real d; int reg;
+        if (!wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) continue;
+        if ((nface > 0 && reg == 0) || (nface == 0 && w == best)) wall_contact(&c, w, nn, d);
+      }
+    }
+    f = c.f; t = c.t;
+    o->status |= c.st;
+    part* out = &o->q[i];
+    *out = *a;
+    for (int q = 0; q < c.nw; ++q) {
+      out->wh[q][0] = c.nh[q][0]; out->wh[q][1] = c.nh[q][1]; out->wh[q][2] = c.nh[q][2];
+      out->wid[q] = c.nid[q];
+    }
+    out->wmask = c.nw >= WSLOTS ? (1u << WSLOTS) - 1u : (1u << c.nw) - 1u;
+    const real inv_m = (real)1.0 / ma;
+    const v3 acc = add(mul(f, inv_m), S->g);
+    const v3 v = add(a->vel, mul(acc, dt));
+    const v3 p = add(a->pos, mul(v, dt));
+    const real inertia = ((real)0.4 * ma) * (ra * ra);
+    const v3 w = add(a->w, mul(mul(t, (real)1.0 / inertia), dt));
+    out->pos = p;
+    out->vel = v;
+    out->w = w;
+    out->path = a->path + len(v) * dt;
+    if (!(isfinite((double)p.x) && isfinite((double)p.y) && isfinite((double)p.z)))
+      o->status |= ST_NONFINITE;
+    if (out->path > (real)0.5 * o->skin) req = 1;
+    o->cap_f[i] = f;
+    o->cap_t[i] = t;
+  }
+  part* tmp = o->p; o->p = o->q; o->q = tmp;
+  if (req) o->rebuild_req = 1;
+}
+
+int ens_step(ens_oracle* o, int nsteps) {
+  for (int s = 0; s < nsteps; ++s) step_once(o);
+  return (int)o->status;
+}
+
+void ens_get_state(const ens_oracle* o, double* pos3, double* rad, double* vel3, double* avel3,
+                   int* sys, int* pid) {
+  for (int i = 0; i < o->n; ++i) {
+    const part* a = &o->p[i];
+    if (pos3) { pos3[3 * i] = a->pos.x; pos3[3 * i + 1] = a->pos.y; pos3[3 * i + 2] = a->pos.z; }
+    if (rad) rad[i] = a->r;
+    if (vel3) { vel3[3 * i] = a->vel.x; vel3[3 * i + 1] = a->vel.y; vel3[3 * i + 2] = a->vel.z; }
+    if (avel3) { avel3[3 * i] = a->w.x; avel3[3 * i + 1] = a->w.y; avel3[3 * i + 2] = a->w.z; }
+    if (sys) sys[i] = a->sys;
+    if (pid) pid[i] = a->pid;
+  }
+}
+
+void ens_get_forces(const ens_oracle* o, double* f3, double* t3) {
+  for (int i = 0; i < o->n; ++i) {
+    f3[3 * i] = o->cap_f[i].x; f3[3 * i + 1] = o->cap_f[i].y; f3[3 * i + 2] = o->cap_f[i].z;
+    t3[3 * i] = o->cap_t[i].x; t3[3 * i + 1] = o->cap_t[i].y; t3[3 * i + 2] = o->cap_t[i].z;
+  }
+}
+
+int ens_num_rebuilds(const ens_oracle* o) { return o->epoch; }
+int ens_status(const ens_oracle* o) { return (int)o->status; }
