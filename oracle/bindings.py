@@ -283,3 +283,86 @@ class Restated:
         e = np.zeros(3)
         self.lib.dem_get_energy(self.h, _p(e, C.c_double))
         return e
+
+
+ENS_F32_SO = os.path.join(HERE, "libens_oracle_f32.so")
+ENS_F64_SO = os.path.join(HERE, "libens_oracle_f64.so")
+
+
+class EnsRestated:
+    """The C restatement of the ensemble path (ens_oracle.c) in FP32 or FP64.
+    Takes the same System / Wall structs as the product's binding."""
+
+    _libs = {}
+
+    def __init__(self, systems, walls, law, dt, skin, max_nbr=32, precision="f32"):
+        from blaze import ensemble as E
+        path = ENS_F32_SO if precision == "f32" else ENS_F64_SO
+        if path not in EnsRestated._libs:
+            if not os.path.isfile(path):
+                raise FileNotFoundError(path + " (build it with: make -C oracle)")
+            lib = C.CDLL(path)
+            _d = C.POINTER(C.c_double)
+            lib.ens_create.restype = C.c_void_p
+            lib.ens_create.argtypes = [C.POINTER(E.System), C.c_int, C.POINTER(E.Wall), C.c_int,
+                                       C.c_int, C.c_double, C.c_double, C.c_int]
+            lib.ens_destroy.argtypes = [C.c_void_p]
+            lib.ens_set_params.argtypes = [C.c_void_p, C.POINTER(E.System)]
+            lib.ens_set_state.argtypes = [C.c_void_p, _d, _d, _d, _d]
+            lib.ens_step.argtypes = [C.c_void_p, C.c_int]
+            lib.ens_get_state.argtypes = [C.c_void_p, _d, _d, _d, _d, _i, _i]
+            lib.ens_get_forces.argtypes = [C.c_void_p, _d, _d]
+            lib.ens_num_rebuilds.argtypes = [C.c_void_p]
+            lib.ens_status.argtypes = [C.c_void_p]
+            EnsRestated._libs[path] = lib
+        self.lib = EnsRestated._libs[path]
+        self.nsys = len(systems)
+        self._sys = (E.System * self.nsys)(*systems)
+        self._walls = (E.Wall * max(1, len(walls)))(*walls) if walls else (E.Wall * 1)()
+        self.n = sum(s.n for s in systems)
+        self.h = self.lib.ens_create(self._sys, self.nsys, self._walls, len(walls), int(law),
+                                     float(dt), float(skin), int(max_nbr))
+
+    def close(self):
+        if self.h:
+            self.lib.ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, systems):
+        from blaze import ensemble as E
+        self._sys = (E.System * self.nsys)(*systems)
+        self.lib.ens_set_params(self.h, self._sys)
+
+    def set_state(self, pos, radius, vel=None, avel=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        self._keep = [c(pos), c(radius), c(vel), c(avel)]
+        self.lib.ens_set_state(self.h, *[_p(a, C.c_double) for a in self._keep])
+
+    def step(self, n=1):
+        return self.lib.ens_step(self.h, int(n))
+
+    def state(self):
+        n = self.n
+        out = dict(pos=np.zeros((n, 3)), radius=np.zeros(n), vel=np.zeros((n, 3)),
+                   avel=np.zeros((n, 3)), sys=np.zeros(n, np.int32), pid=np.zeros(n, np.int32))
+        self.lib.ens_get_state(self.h, _p(out["pos"], C.c_double), _p(out["radius"], C.c_double),
+                               _p(out["vel"], C.c_double), _p(out["avel"], C.c_double),
+                               _p(out["sys"], C.c_int), _p(out["pid"], C.c_int))
+        out["status"] = self.lib.ens_status(self.h)
+        return out
+
+    def forces(self):
+        n = self.n
+        f = np.zeros((n, 3))
+        t = np.zeros((n, 3))
+        self.lib.ens_get_forces(self.h, _p(f, C.c_double), _p(t, C.c_double))
+        return f, t
+
+    def num_rebuilds(self):
+        return self.lib.ens_num_rebuilds(self.h)

@@ -1,0 +1,189 @@
+"""ctypes binding of the ensemble ABI (include/blaze_ens.h): many independent
+sphere systems stepped together on one GPU with the linear or Hertz-Mindlin
+contact law, tangential history spring, Coulomb cap and rolling friction.
+
+Loading fails loudly when the library or a GPU is missing: there is no CPU
+path in the product.
+"""
+import ctypes as C
+
+import numpy as np
+
+from .device import _check, _ptr, load as _load_lib
+
+LAW_LINEAR = 1
+LAW_HERTZ_MINDLIN = 2
+WALL_PLANE = 0
+WALL_TRIANGLE = 1
+WALL_CYLINDER = 2
+
+
+class Wall(C.Structure):
+    _fields_ = [("kind", C.c_int), ("p", C.c_float * 10)]
+
+
+class System(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("origin", C.c_float * 3), ("cell", C.c_float), ("ncells", C.c_int * 3),
+        ("gravity", C.c_float * 3), ("density", C.c_float), ("kn", C.c_float),
+        ("kt_ratio", C.c_float), ("youngs", C.c_float), ("poisson", C.c_float),
+        ("restitution", C.c_float), ("mu", C.c_float), ("mu_wall", C.c_float),
+        ("mu_roll", C.c_float), ("wall0", C.c_int), ("nwalls", C.c_int), ("tri0", C.c_int),
+        ("ntris", C.c_int),
+    ]
+
+
+class EnsOptions(C.Structure):
+    _fields_ = [("law", C.c_int), ("dt", C.c_float), ("skin", C.c_float), ("max_nbr", C.c_int),
+                ("use_graph", C.c_int), ("capture_forces", C.c_int)]
+
+
+_bound = False
+
+
+def load():
+    global _bound
+    lib = _load_lib()
+    if not _bound:
+        P = C.POINTER
+        _f = P(C.c_float)
+        _i = P(C.c_int)
+        lib.blaze_ens_default_options.argtypes = [P(EnsOptions)]
+        lib.blaze_ens_create.argtypes = [P(C.c_void_p), P(System), C.c_int, P(Wall), C.c_int,
+                                         P(EnsOptions)]
+        lib.blaze_ens_destroy.argtypes = [C.c_void_p]
+        lib.blaze_ens_set_state.argtypes = [C.c_void_p, _f, _f, _f, _f]
+        lib.blaze_ens_get_state.argtypes = [C.c_void_p, _f, _f, _f, _f, _i, _i]
+        lib.blaze_ens_step.argtypes = [C.c_void_p, C.c_int]
+        lib.blaze_ens_sync.argtypes = [C.c_void_p]
+        lib.blaze_ens_set_params.argtypes = [C.c_void_p, P(System)]
+        lib.blaze_ens_get_forces.argtypes = [C.c_void_p, _f, _f]
+        lib.blaze_ens_num_rebuilds.argtypes = [C.c_void_p]
+        lib.blaze_ens_device_state.argtypes = [C.c_void_p] + [P(C.c_void_p)] * 4
+        lib.blaze_ens_last_launches.argtypes = [C.c_void_p]
+        lib.blaze_ens_rebuild_kernels.argtypes = [C.c_void_p]
+        _bound = True
+    return lib
+
+
+def default_options(**kw):
+    o = EnsOptions()
+    load().blaze_ens_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def plane(normal, d):
+    """Plane n . x = d, n (normalised here) pointing into the domain."""
+    w = Wall()
+    w.kind = WALL_PLANE
+    n = np.asarray(normal, np.float64)
+    n = n / np.linalg.norm(n)
+    w.p[0], w.p[1], w.p[2], w.p[3] = float(n[0]), float(n[1]), float(n[2]), float(d)
+    return w
+
+
+def triangle(a, b, c):
+    w = Wall()
+    w.kind = WALL_TRIANGLE
+    for k, v in enumerate(list(a) + list(b) + list(c)):
+        w.p[k] = float(v)
+    return w
+
+
+def cylinder(point, axis, radius):
+    """Cylinder wall (particles inside) through `point` along `axis`."""
+    w = Wall()
+    w.kind = WALL_CYLINDER
+    ax = np.asarray(axis, np.float64)
+    ax = ax / np.linalg.norm(ax)
+    for k, v in enumerate(list(point) + list(ax) + [radius]):
+        w.p[k] = float(v)
+    return w
+
+
+class Ensemble:
+    """Systems + walls on the GPU.  State arrays are (N, 3) float32 for all
+    systems concatenated in system order."""
+
+    def __init__(self, systems, walls, **options):
+        self.lib = load()
+        self.nsys = len(systems)
+        self.systems = (System * self.nsys)(*systems)
+        self.walls = (Wall * max(1, len(walls)))(*walls) if walls else (Wall * 1)()
+        self.nwalls = len(walls)
+        self.opts = default_options(**options)
+        self.n = sum(s.n for s in systems)
+        h = C.c_void_p()
+        rc = self.lib.blaze_ens_create(C.byref(h), self.systems, self.nsys, self.walls,
+                                       self.nwalls, C.byref(self.opts))
+        _check(rc, "blaze_ens_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.blaze_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, pos, radius, vel=None, avel=None):
+        c = np.ascontiguousarray
+        n = self.n
+        pos = c(pos, np.float32).reshape(n, 3)
+        radius = c(radius, np.float32).reshape(n)
+        vel = None if vel is None else c(vel, np.float32).reshape(n, 3)
+        avel = None if avel is None else c(avel, np.float32).reshape(n, 3)
+        _check(self.lib.blaze_ens_set_state(self.h, _ptr(pos, C.c_float), _ptr(radius, C.c_float),
+                                            _ptr(vel, C.c_float), _ptr(avel, C.c_float)),
+               "blaze_ens_set_state")
+
+    def step(self, n=1):
+        return _check(self.lib.blaze_ens_step(self.h, int(n)), "blaze_ens_step")
+
+    def sync(self):
+        return _check(self.lib.blaze_ens_sync(self.h), "blaze_ens_sync")
+
+    def state(self):
+        n = self.n
+        out = dict(pos=np.zeros((n, 3), np.float32), radius=np.zeros(n, np.float32),
+                   vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),
+                   sys=np.zeros(n, np.int32), pid=np.zeros(n, np.int32))
+        st = _check(self.lib.blaze_ens_get_state(
+            self.h, _ptr(out["pos"], C.c_float), _ptr(out["radius"], C.c_float),
+            _ptr(out["vel"], C.c_float), _ptr(out["avel"], C.c_float),
+            _ptr(out["sys"], C.c_int), _ptr(out["pid"], C.c_int)), "blaze_ens_get_state")
+        out["status"] = st
+        return out
+
+    def forces(self):
+        n = self.n
+        f = np.zeros((n, 3), np.float32)
+        t = np.zeros((n, 3), np.float32)
+        _check(self.lib.blaze_ens_get_forces(self.h, _ptr(f, C.c_float), _ptr(t, C.c_float)),
+               "blaze_ens_get_forces")
+        return f, t
+
+    def set_params(self, systems):
+        self.systems = (System * self.nsys)(*systems)
+        _check(self.lib.blaze_ens_set_params(self.h, self.systems), "blaze_ens_set_params")
+
+    def num_rebuilds(self):
+        return _check(self.lib.blaze_ens_num_rebuilds(self.h), "blaze_ens_num_rebuilds")
+
+    def device_state(self):
+        ptrs = [C.c_void_p() for _ in range(4)]
+        _check(self.lib.blaze_ens_device_state(self.h, *[C.byref(p) for p in ptrs]),
+               "blaze_ens_device_state")
+        return tuple(p.value for p in ptrs)
+
+    def last_launches(self):
+        return self.lib.blaze_ens_last_launches(self.h)
+
+    def rebuild_kernels(self):
+        return self.lib.blaze_ens_rebuild_kernels(self.h)

@@ -325,3 +325,106 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
                    specific=specific)
     proj = Project.load(root, name, world)
     return proj, proj.read_state()
+
+
+# ---------------------------------------------------------------- ensembles
+def lattice_fill(n, lo, hi, pitch, rng, jitter=0.0):
+    """First n sites of a face-centred cubic lattice of nearest-neighbour
+    distance `pitch` inside the box [lo, hi] (filled bottom up, z last), each
+    moved by a uniform jitter in [-jitter, jitter]."""
+    a = pitch * math.sqrt(2.0)
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    m = np.floor((hi - lo) / a).astype(int) + 1
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) * a
+    pts = []
+    for iz in range(m[2]):
+        layer = []
+        for iy in range(m[1]):
+            for ix in range(m[0]):
+                layer.append(base + lo + np.array([ix, iy, iz]) * a)
+        layer = np.concatenate(layer)
+        layer = layer[np.all((layer >= lo) & (layer <= hi), axis=1)]
+        pts.append(layer[np.lexsort((layer[:, 0], layer[:, 1], layer[:, 2]))])
+        if sum(len(p) for p in pts) >= n:
+            break
+    pts = np.concatenate(pts)
+    if len(pts) < n:
+        raise ValueError("box holds %d lattice sites, %d requested" % (len(pts), n))
+    pts = pts[:n]
+    if jitter > 0:
+        pts = pts + rng.uniform(-jitter, jitter, size=pts.shape)
+    return pts
+
+
+def box_walls(L, H, z0=0.0):
+    """Six inward planes of the box [0, L] x [0, L] x [z0, z0 + H]."""
+    from . import ensemble as E
+    return [E.plane((1, 0, 0), 0.0), E.plane((-1, 0, 0), -L), E.plane((0, 1, 0), 0.0),
+            E.plane((0, -1, 0), -L), E.plane((0, 0, 1), z0), E.plane((0, 0, -1), -(z0 + H))]
+
+
+def box_system(n, L, H, cell, wall0, *, density, kn=1e5, kt_ratio=2.0 / 7.0, youngs=0.0,
+               poisson=0.3, restitution=0.5, mu=0.4, mu_wall=None, mu_roll=0.0,
+               gravity=(0.0, 0.0, -981.0)):
+    """A blaze_system for a box [0, L]^2 x [0, H] whose six planes are
+    walls[wall0 .. wall0 + 6)."""
+    from . import ensemble as E
+    s = E.System()
+    s.n = int(n)
+    margin = 0.5 * cell
+    for k in range(3):
+        s.origin[k] = -margin
+    s.cell = cell
+    ext = (L, L, H)
+    for k in range(3):
+        s.ncells[k] = int(math.ceil((ext[k] + 2 * margin) / cell))
+    for k in range(3):
+        s.gravity[k] = gravity[k]
+    s.density = density
+    s.kn, s.kt_ratio, s.youngs, s.poisson = kn, kt_ratio, youngs, poisson
+    s.restitution, s.mu = restitution, mu
+    s.mu_wall = mu if mu_wall is None else mu_wall
+    s.mu_roll = mu_roll
+    s.wall0, s.nwalls, s.tri0, s.ntris = wall0, 6, 0, 0
+    return s
+
+
+def box_ensemble(counts, *, r_min=0.1, r_max=0.2, solid_fraction=0.55, height_factor=3.0,
+                 rho=2500.0, kn=1e5, kt_ratio=2.0 / 7.0, mus=None, restitutions=None,
+                 skin=0.02, seed=3, gravity=(0.0, 0.0, -981.0)):
+    """Independent box-settling systems: system s holds counts[s] spheres with
+    radii uniform in [r_min, r_max] (cm), in a box of square base L_s with
+    L_s^3 = (total sphere volume) / solid_fraction and height
+    height_factor * L_s (room for the loose initial lattice above the settled
+    bed); spheres start on an FCC lattice of nearest-neighbour distance
+    2 r_max + skin / 2, jittered by 0.1 r_min, at rest.  Per-system friction
+    and restitution from `mus` / `restitutions`.  Returns (systems, walls,
+    pos, radius) with the arrays concatenated in system order."""
+    rng = np.random.default_rng(seed)
+    density = rho * 1e-6  # kg/cm^3
+    cell = 2.0 * r_max + skin
+    systems, walls, pos, rad = [], [], [], []
+    for s, n in enumerate(counts):
+        r = rng.uniform(r_min, r_max, size=int(n))
+        vol = float(np.sum(4.0 / 3.0 * math.pi * r ** 3))
+        L = (vol / solid_fraction) ** (1.0 / 3.0)
+        H = height_factor * L
+        pitch = 2.0 * r_max + 0.5 * skin
+        p = lattice_fill(int(n), (r_max + 0.01, r_max + 0.01, r_max + 0.01),
+                         (L - r_max - 0.01, L - r_max - 0.01, H - r_max - 0.01), pitch, rng,
+                         jitter=0.1 * r_min)
+        mu = 0.4 if mus is None else float(mus[s])
+        e = 0.5 if restitutions is None else float(restitutions[s])
+        systems.append(box_system(n, L, H, cell, len(walls), density=density, kn=kn,
+                                  kt_ratio=kt_ratio, restitution=e, mu=mu, gravity=gravity))
+        walls += box_walls(L, H)
+        pos.append(p.astype(np.float32))
+        rad.append(r.astype(np.float32))
+    return systems, walls, np.concatenate(pos), np.concatenate(rad)
+
+
+def batched_counts(nsys=512, n_min=2000, n_max=50000, seed=3):
+    """Particle counts log-uniform in [n_min, n_max] (the batched workload)."""
+    rng = np.random.default_rng(seed)
+    return np.round(np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=nsys))).astype(int)
