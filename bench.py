@@ -58,6 +58,9 @@ def parse():
                          "region starts from the generated packing, as the CPU arm does)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-ensemble leg (512 box-settling systems)")
+    ap.add_argument("--batched-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -142,6 +145,78 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def batched_leg(steps, warmup):
+    """The batched ensemble: 512 independent box-settling systems, particle
+    counts log-uniform in [2,000, 50,000] (seed 3), radii uniform in
+    [0.1, 0.2] cm, boxes sized to a 0.55 solid fraction, per-system mu in
+    [0.2, 0.8] and restitution in [0.3, 0.9], linear spring-dashpot with
+    tangential history (kn = 1e5, kt = 2/7 kn), dt = 1e-5 s, one launch
+    sequence per step (CUDA graph), skin and block size from the autotuner.
+    Compared with plain solves of single systems (same kernels, one system
+    per launch sequence) of 16 sizes spread over the range; the sequential
+    time of all 512 is their linear fit in N summed over the 512 counts."""
+    import torch
+    from blaze import autotune, synth
+    from blaze import ensemble as E
+    counts = synth.batched_counts(512, seed=3)
+    rng = np.random.default_rng(3)
+    mus = rng.uniform(0.2, 0.8, len(counts))
+    rests = rng.uniform(0.3, 0.9, len(counts))
+    S, W, p, r = synth.box_ensemble(counts, mus=mus, restitutions=rests, seed=3)
+    best, trials = autotune.tune(S, W, p, r, steps=32, warmup=max(3, warmup))
+    opts = dict(law=E.LAW_LINEAR, dt=1e-5, skin=best["skin"], use_graph=1, block=best["block"])
+    ens = E.Ensemble(best["systems"], W, **opts)
+    ens.set_state(p, r)
+    ens.step(max(3, warmup))
+    ens.sync()
+    stream = torch.cuda.ExternalStream(ens.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = ens.num_rebuilds()
+    a.record(stream)
+    ens.step(steps)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = ens.num_rebuilds() - rb0
+    launches = ens.last_launches() + rebuilds * ens.rebuild_kernels()
+    status = ens.sync()
+    n = ens.n
+    ens.close()
+    # single systems, one after another
+    off = np.concatenate([[0], np.cumsum(counts)])
+    pick = np.argsort(counts)[np.linspace(0, len(counts) - 1, 16).astype(int)]
+    single = []
+    for s_ in pick:
+        Ss = E.System.from_buffer_copy(bytes(best["systems"][s_]))
+        Ss.wall0 = 0
+        e1 = E.Ensemble([Ss], W[S[s_].wall0:S[s_].wall0 + 6], **opts)
+        e1.set_state(p[off[s_]:off[s_ + 1]], r[off[s_]:off[s_ + 1]])
+        e1.step(max(3, warmup))
+        e1.sync()
+        st1 = torch.cuda.ExternalStream(e1.device_state()[3])
+        a.record(st1)
+        e1.step(100)
+        b.record(st1)
+        b.synchronize()
+        single.append((int(counts[s_]), a.elapsed_time(b) / 100))
+        e1.close()
+    ns = np.array([x[0] for x in single], float)
+    ts = np.array([x[1] for x in single])
+    coef = np.linalg.lstsq(np.stack([np.ones_like(ns), ns], 1), ts, rcond=None)[0]
+    seq_ms = float(np.sum(coef[0] + coef[1] * counts))
+    return {"workload": "512 box-settling systems, N log-uniform in [2000, 50000], "
+                        "linear spring-dashpot + tangential history, dt 1e-5 s",
+            "particles": int(n), "systems": len(counts), "value": n / (ms * 1e-3),
+            "unit": UNIT, "ms_per_step": ms, "steps": steps, "rebuilds": rebuilds,
+            "gpu_launches": launches, "status": status,
+            "autotuned": {"skin_cm": best["skin"], "cell_cm": best["cell"],
+                          "block": best["block"],
+                          "trials": [[t[0], t[1], round(t[2], 4), t[3]] for t in trials]},
+            "sequential_plain_ms_per_step": seq_ms, "vs_sequential_plain": seq_ms / ms,
+            "single_samples": [[n_, round(t_, 5)] for n_, t_ in single]}
 
 
 def cpu_reference_rate(P, st, seconds, max_steps=None):
@@ -311,6 +386,10 @@ def main():
     e2e_value = n * world * args.e2e_steps / el
     state_bytes = n * (12 + 12 + 12 + 4 + 4)
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(args.batched_steps, args.warmup)
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_rate(P, st, args.cpu_seconds)
@@ -336,6 +415,7 @@ def main():
             "rebuilds_in_timed_region": rebuilds,
             "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
             "reference_mode_value": ref_mode_value,
+            "batched": batched,
             "status": device.decode_status(status),
         }
         print(json.dumps(line))

@@ -67,9 +67,10 @@ typedef struct blaze_ens_options {
   int max_nbr;         /* neighbour / history slots per particle, 1..32 */
   int use_graph;       /* 1: steps run as CUDA graphs (re-sort in a conditional node) */
   int capture_forces;  /* 1: keep each step's contact force and torque per particle */
+  int block;           /* threads per block of the step kernel: 64, 128, 256 or 512 */
 } blaze_ens_options;
 
-/* law 1, dt 1e-5, skin 0.02, max_nbr 32, use_graph 1, capture_forces 0 */
+/* law 1, dt 1e-5, skin 0.02, max_nbr 32, use_graph 1, capture_forces 0, block 256 */
 void blaze_ens_default_options(blaze_ens_options* o);
 
 int blaze_ens_create(blaze_ens** out, const blaze_system* systems, int nsys,

@@ -35,7 +35,7 @@ class System(C.Structure):
 
 class EnsOptions(C.Structure):
     _fields_ = [("law", C.c_int), ("dt", C.c_float), ("skin", C.c_float), ("max_nbr", C.c_int),
-                ("use_graph", C.c_int), ("capture_forces", C.c_int)]
+                ("use_graph", C.c_int), ("capture_forces", C.c_int), ("block", C.c_int)]
 
 
 _bound = False

@@ -398,7 +398,7 @@ def box_ensemble(counts, *, r_min=0.1, r_max=0.2, solid_fraction=0.55, height_fa
     L_s^3 = (total sphere volume) / solid_fraction and height
     height_factor * L_s (room for the loose initial lattice above the settled
     bed); spheres start on an FCC lattice of nearest-neighbour distance
-    2 r_max + skin / 2, jittered by 0.1 r_min, at rest.  Per-system friction
+    2 r_max + skin / 2, jittered by at most a fifth of the lattice gap, at rest.  Per-system friction
     and restitution from `mus` / `restitutions`.  Returns (systems, walls,
     pos, radius) with the arrays concatenated in system order."""
     rng = np.random.default_rng(seed)
@@ -411,9 +411,11 @@ def box_ensemble(counts, *, r_min=0.1, r_max=0.2, solid_fraction=0.55, height_fa
         L = (vol / solid_fraction) ** (1.0 / 3.0)
         H = height_factor * L
         pitch = 2.0 * r_max + 0.5 * skin
+        # jitter small enough that no two lattice neighbours start in contact
+        jitter = min(0.1 * r_min, 0.2 * (pitch - 2.0 * r_max))
         p = lattice_fill(int(n), (r_max + 0.01, r_max + 0.01, r_max + 0.01),
                          (L - r_max - 0.01, L - r_max - 0.01, H - r_max - 0.01), pitch, rng,
-                         jitter=0.1 * r_min)
+                         jitter=jitter)
         mu = 0.4 if mus is None else float(mus[s])
         e = 0.5 if restitutions is None else float(restitutions[s])
         systems.append(box_system(n, L, H, cell, len(walls), density=density, kn=kn,
@@ -428,3 +430,23 @@ def batched_counts(nsys=512, n_min=2000, n_max=50000, seed=3):
     """Particle counts log-uniform in [n_min, n_max] (the batched workload)."""
     rng = np.random.default_rng(seed)
     return np.round(np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=nsys))).astype(int)
+
+
+def box_c1(n_side=(20, 20, 25), radius=0.1, rho=2500.0, box=10.0, kn=1.0e5, cor=0.5, mu=0.4,
+           kt_ratio=2.0 / 7.0, pitch=0.3, start=0.3, jitter=0.02, seed=0, skin=0.02):
+    """The Particles_Box configuration with the tangential history law, as a
+    one-system ensemble: n_side spheres on a cubic lattice of pitch `pitch`
+    from `start` (x, y horizontal, z vertical), each jittered uniformly by
+    +-jitter (seed 0), at rest, in the cube [0, box]^3 of six planes; linear
+    spring-dashpot kn, restitution cor, Coulomb mu, kt = kt_ratio kn, gravity
+    -981 cm/s^2 along z.  Returns (systems, walls, pos, radius)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = n_side
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    lat = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1).astype(np.float64) * pitch + start
+    pos = (lat + rng.uniform(-jitter, jitter, size=lat.shape)).astype(np.float32)
+    n = len(pos)
+    cell = 2.0 * radius + skin
+    S = box_system(n, box, box, cell, 0, density=rho * 1e-6, kn=kn, kt_ratio=kt_ratio,
+                   restitution=cor, mu=mu)
+    return [S], box_walls(box, box), pos, np.full(n, radius, np.float32)

@@ -257,7 +257,7 @@ int enqueue_step(blaze_ens* e) {
   int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
   if (rc) return rc;
   ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0},
-                  e->opt.capture_forces ? &e->cap : nullptr, e->stream);
+                  e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
   e->last_launches += 2 + rebuild_kernel_count(e);
   e->cur ^= 1;
   return 0;
@@ -304,7 +304,7 @@ int build_graph(blaze_ens* e, int c) {
     const StepLink link = k + 1 < kGraphSteps ? StepLink{e->d_rb + k, h[k + 1], 1}
                                                : StepLink{e->d_rb + k, 0, 0};
     ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link,
-                    e->opt.capture_forces ? &e->cap : nullptr, e->stream);
+                    e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
     e->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
@@ -333,6 +333,8 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   if ((o.law != BLAZE_LAW_LINEAR && o.law != BLAZE_LAW_HERTZ_MINDLIN) || !(o.dt > 0.0f) ||
       !(o.skin > 0.0f) || o.max_nbr < 1 || o.max_nbr > 32)
     return -1;
+  if (o.block == 0) o.block = 256;
+  if (o.block < 64 || o.block > kMaxStepBlock || o.block % 32 != 0) return -1;
   long long ntot = 0, cells = 0;
   for (int s = 0; s < nsys; ++s) {
     if (!valid_system(systems[s], nwalls, o.skin)) return -1;
@@ -464,6 +466,7 @@ void blaze_ens_default_options(blaze_ens_options* o) {
   o->max_nbr = 32;
   o->use_graph = 1;
   o->capture_forces = 0;
+  o->block = 256;
 }
 
 int blaze_ens_create(blaze_ens** out, const blaze_system* systems, int nsys,

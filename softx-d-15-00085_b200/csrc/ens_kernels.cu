@@ -303,7 +303,7 @@ __global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
 
 // ------------------------------------------------------------------- step
 template <int kLaw, bool kCapture>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kMaxStepBlock)
 k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
            StepCtl* ctl, StepLink link, EnsCapture cap) {
   const bool rebuilt = *link.rebuilt != 0;
@@ -527,15 +527,17 @@ void ens_launch_epoch(StepCtl* ctl, const int* gate, cudaStream_t st) {
 }
 
 void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
-                     StepLink link, const EnsCapture* cap, cudaStream_t st) {
+                     StepLink link, const EnsCapture* cap, int block, cudaStream_t st) {
   const EnsCapture c = cap ? *cap : EnsCapture{nullptr, nullptr};
+  const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
+  const int gs = (n + bs - 1) / bs;
 #define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c
   if (g.law == kLawHertz) {
-    if (cap) k_ens_step<kLawHertz, true><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawHertz, false><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+    if (cap) k_ens_step<kLawHertz, true><<<gs, bs, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawHertz, false><<<gs, bs, 0, st>>>(ENS_ARGS);
   } else {
-    if (cap) k_ens_step<kLawLinear, true><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawLinear, false><<<nblk(n), kThreads, 0, st>>>(ENS_ARGS);
+    if (cap) k_ens_step<kLawLinear, true><<<gs, bs, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawLinear, false><<<gs, bs, 0, st>>>(ENS_ARGS);
   }
 #undef ENS_ARGS
 }

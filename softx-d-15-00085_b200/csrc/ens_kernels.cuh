@@ -96,8 +96,10 @@ void ens_launch_nlist(const EnsGeom& g, const EnsBufs& b, int n, const int32_t* 
                       const uint32_t* cstart, const uint32_t* cend, StepCtl* ctl,
                       const int* gate, cudaStream_t st);
 void ens_launch_epoch(StepCtl* ctl, const int* gate, cudaStream_t st);
+// `block`: threads per block (64 .. kMaxStepBlock, a multiple of 32).
+constexpr int kMaxStepBlock = 512;
 void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
-                     StepLink link, const EnsCapture* cap, cudaStream_t st);
+                     StepLink link, const EnsCapture* cap, int block, cudaStream_t st);
 // Staged caller arrays -> state S[cur], pid = index, both list copies and
 // every history cleared; flags[0] |= 1 for a radius that is not positive.
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,
