@@ -170,19 +170,23 @@ def test_cylinder_holds_particles_inside():
 
 
 def test_box_settles_fp32_error_stated():
-    """A two-system box settling run: FP32 against FP64 after 1 step (same
-    input) -- the error the product inherits, stated -- and a bounded state
-    after 1500 steps."""
+    """Two box systems settle for 2500 steps (FP32, bounded state); from the
+    settled state one step runs in FP32 and in FP64, and the FP32 contact
+    force error -- the error the product inherits -- is stated and bounded."""
     S, W, p, r = synth.box_ensemble([500, 900], seed=2, mus=[0.3, 0.7], restitutions=[0.4, 0.8])
-    o32, _ = run(S, W, p, r, dt=1e-5, steps=1, prec="f32", skin=0.02)
-    o64, _ = run(S, W, p, r, dt=1e-5, steps=1, prec="f64", skin=0.02)
+    o, st = run(S, W, p, r, dt=1e-5, steps=2500, prec="f32", skin=0.02)
+    assert st == 0
+    s = o.state()
+    assert np.abs(s["vel"]).max() < 100.0
+    # settled state in the caller's order (system-concatenated), as set_state wants it
+    order = np.argsort(s["pid"])
+    args = (s["pos"][order], s["radius"][order], s["vel"][order], s["avel"][order])
+    o32, _ = run(S, W, *args[:2], vel=args[2], avel=args[3], dt=1e-5, steps=1, prec="f32")
+    o64, _ = run(S, W, *args[:2], vel=args[2], avel=args[3], dt=1e-5, steps=1, prec="f64")
     f32, _ = o32.forces()
     f64, _ = o64.forces()
     scale = np.abs(f64).max()
+    assert scale > 0
     err = np.abs(f32 - f64).max() / scale
     print("FP32 vs FP64 contact force after one step: max %.2e of the largest force" % err)
-    assert err < 1e-5
-    st = o32.step(1500)
-    assert st == 0
-    v = o32.state()["vel"]
-    assert np.abs(v).max() < 100.0
+    assert err < 1e-4
