@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-ensemble leg (512 box-settling systems)")
-    ap.add_argument("--batched-steps", type=int, default=200)
+    ap.add_argument("--batched-steps", type=int, default=2000,
+                    help="timed steps of the batched leg (the workload's 2,000 settling steps)")
     return ap.parse_args()
 
 
@@ -154,9 +155,12 @@ def batched_leg(steps, warmup):
     [0.2, 0.8] and restitution in [0.3, 0.9], linear spring-dashpot with
     tangential history (kn = 1e5, kt = 2/7 kn), dt = 1e-5 s, one launch
     sequence per step (CUDA graph), skin and block size from the autotuner.
-    Compared with plain solves of single systems (same kernels, one system
-    per launch sequence) of 16 sizes spread over the range; the sequential
-    time of all 512 is their linear fit in N summed over the 512 counts."""
+    The timed region is the whole settling run from rest (2,000 steps by
+    default), re-sorts included.  Compared with plain solves of single
+    systems (same kernels and settings, one system per launch sequence) of
+    16 sizes spread over the range, each timed over the same steps; the
+    sequential time of all 512 is their linear fit in N summed over the 512
+    counts."""
     import torch
     from blaze import autotune, synth
     from blaze import ensemble as E
@@ -165,7 +169,7 @@ def batched_leg(steps, warmup):
     mus = rng.uniform(0.2, 0.8, len(counts))
     rests = rng.uniform(0.3, 0.9, len(counts))
     S, W, p, r = synth.box_ensemble(counts, mus=mus, restitutions=rests, seed=3)
-    best, trials = autotune.tune(S, W, p, r, steps=32, warmup=max(3, warmup))
+    best, trials = autotune.tune(S, W, p, r, steps=200, warmup=max(3, warmup), preroll_steps=600)
     opts = dict(law=E.LAW_LINEAR, dt=1e-5, skin=best["skin"], use_graph=1, block=best["block"])
     ens = E.Ensemble(best["systems"], W, **opts)
     ens.set_state(p, r)
@@ -198,10 +202,10 @@ def batched_leg(steps, warmup):
         e1.sync()
         st1 = torch.cuda.ExternalStream(e1.device_state()[3])
         a.record(st1)
-        e1.step(100)
+        e1.step(steps)
         b.record(st1)
         b.synchronize()
-        single.append((int(counts[s_]), a.elapsed_time(b) / 100))
+        single.append((int(counts[s_]), a.elapsed_time(b) / steps))
         e1.close()
     ns = np.array([x[0] for x in single], float)
     ts = np.array([x[1] for x in single])

@@ -53,14 +53,34 @@ def _time(systems, walls, pos, radius, vel, opts, steps, warmup):
         e.close()
 
 
+def preroll(systems, walls, pos, radius, vel, steps, *, law, dt, max_nbr, skin=0.02):
+    """State after `steps` steps with a default skin, in the caller's order
+    (trials then start where the particles already move as they will)."""
+    r_max = float(np.max(radius))
+    e = E.Ensemble(regrid(systems, skin, r_max), walls, law=law, dt=dt, skin=skin,
+                   max_nbr=max_nbr, use_graph=1)
+    try:
+        e.set_state(pos, radius, vel)
+        e.step(steps)
+        st = e.state()
+    finally:
+        e.close()
+    order = np.argsort(st["pid"])
+    return st["pos"][order], st["vel"][order]
+
+
 def tune(systems, walls, pos, radius, vel=None, *, law=E.LAW_LINEAR, dt=1e-5, max_nbr=32,
-         skins=SKINS, blocks=BLOCKS, steps=64, warmup=8):
+         skins=SKINS, blocks=BLOCKS, steps=200, warmup=8, preroll_steps=600):
     """Returns (best, trials): best = dict(skin, cell, block, ms_per_step,
     systems) with the re-gridded systems to create the ensemble with, and
-    trials the list of (skin, block, ms_per_step, status) measured.  Trials
-    whose run raised a status bit (list overflow, particle outside the grid)
-    are not chosen."""
+    trials the list of (skin, block, ms_per_step, status) measured.  The
+    trials start from the state after `preroll_steps` steps, so re-sorts
+    happen at the rate the run will see.  Trials whose run raised a status
+    bit (list overflow, particle outside the grid) are not chosen."""
     r_max = float(np.max(radius))
+    if preroll_steps > 0:
+        pos, vel = preroll(systems, walls, pos, radius, vel, preroll_steps, law=law, dt=dt,
+                           max_nbr=max_nbr)
     trials = []
     best = None
     for skin in skins:

@@ -363,13 +363,11 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   }
   if (mask != mask_o) L.mask[i] = mask;
 
-  // walls: old history slots (by wall id), new slots in processing order
-  float4 oh[kWallSlots], nh[kWallSlots];
+  // walls: old history slots (by wall id) held in registers; new slots are
+  // written in processing order straight over the old ones
+  float4 oh[kWallSlots];
 #pragma unroll
-  for (int q = 0; q < kWallSlots; ++q) {
-    oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-    nh[q] = oh[q];
-  }
+  for (int q = 0; q < kWallSlots; ++q) oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
   if (wmask_o) {
 #pragma unroll
     for (int q = 0; q < kWallSlots; ++q)
@@ -387,9 +385,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     f = f + F;
     t = t + T;
     if (nw < kWallSlots) {
-#pragma unroll
-      for (int q = 0; q < kWallSlots; ++q)
-        if (q == nw) nh[q] = make_float4(xi.x, xi.y, xi.z, __int_as_float(id));
+      b.wh[e][(size_t)nw * stride + i] = make_float4(xi.x, xi.y, xi.z, __int_as_float(id));
       ++nw;
     } else {
       st |= kStatusListOverflow;
@@ -429,11 +425,6 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
         if ((nface > 0 && region == 0) || (nface == 0 && id == best)) wall_contact(id, nrm, delta);
       }
     }
-  }
-  if (wmask_o || nw) {
-#pragma unroll
-    for (int q = 0; q < kWallSlots; ++q)
-      if (q < nw) b.wh[e][(size_t)q * stride + i] = nh[q];
   }
   const uint32_t wmask = nw >= kWallSlots ? (1u << kWallSlots) - 1u : (1u << nw) - 1u;
 
