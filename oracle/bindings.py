@@ -314,6 +314,10 @@ class EnsRestated:
             lib.ens_get_forces.argtypes = [C.c_void_p, _d, _d]
             lib.ens_num_rebuilds.argtypes = [C.c_void_p]
             lib.ens_status.argtypes = [C.c_void_p]
+            lib.ens_get_constants.argtypes = [C.c_void_p, C.c_int, _d]
+            lib.ens_set_constants.argtypes = [C.c_void_p, C.c_int, _d]
+            lib.ens_adj_record.argtypes = [C.c_void_p, C.c_int]
+            lib.ens_adj_reverse.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _d, _d]
             EnsRestated._libs[path] = lib
         self.lib = EnsRestated._libs[path]
         self.nsys = len(systems)
@@ -366,3 +370,32 @@ class EnsRestated:
 
     def num_rebuilds(self):
         return self.lib.ens_num_rebuilds(self.h)
+
+    def constants(self, s):
+        """kn, kt, 2 beta, mu, mu_wall of system s, in working precision."""
+        c = np.zeros(5)
+        self.lib.ens_get_constants(self.h, int(s), _p(c, C.c_double))
+        return c
+
+    def set_constants(self, s, c5):
+        c = np.ascontiguousarray(c5, np.float64)
+        self.lib.ens_set_constants(self.h, int(s), _p(c, C.c_double))
+
+    def adj_record(self, nsteps):
+        return self.lib.ens_adj_record(self.h, int(nsteps))
+
+    def adj_reverse(self, gx, gv, gw):
+        """Cotangents of the final state (final memory order) -> cotangents
+        of the recorded initial state (its memory order) and of the law
+        constants (nsys x 5)."""
+        n = self.n
+        c = lambda a: np.ascontiguousarray(a, np.float64)
+        gx, gv, gw = c(gx), c(gv), c(gw)
+        out = [np.zeros((n, 3)) for _ in range(3)]
+        th = np.zeros((self.nsys, 5))
+        rc = self.lib.ens_adj_reverse(self.h, _p(gx, C.c_double), _p(gv, C.c_double),
+                                      _p(gw, C.c_double), *[_p(a, C.c_double) for a in out],
+                                      _p(th, C.c_double))
+        if rc < 0:
+            raise RuntimeError("ens_adj_reverse failed: %d" % rc)
+        return out[0], out[1], out[2], th

@@ -32,6 +32,7 @@ typedef DEM_REAL real;
 #define IS_FLOAT (sizeof(real) == sizeof(float))
 static real SQRT(real x) { return IS_FLOAT ? (real)sqrtf((float)x) : (real)sqrt((double)x); }
 static real FLOOR(real x) { return IS_FLOAT ? (real)floorf((float)x) : (real)floor((double)x); }
+static real IN(double x) { return IS_FLOAT ? (real)(float)x : (real)x; }
 
 typedef struct { real x, y, z; } v3;
 static v3 mk(real x, real y, real z) { v3 r = {x, y, z}; return r; }
@@ -95,6 +96,8 @@ struct ens_oracle {
   v3* cap_f;
   v3* cap_t;
   int* sys_of;      /* system of each entry of the caller's arrays */
+  struct tstep_* tape; /* recorded steps of the reverse sweep */
+  int ntape;
 };
 
 static void constants(sysc* d, const blaze_system* s, uint32_t off) {
@@ -165,12 +168,27 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
   return o;
 }
 
+static void free_tape(ens_oracle* o);
 void ens_destroy(ens_oracle* o) {
   if (!o) return;
+  free_tape(o);
   free(o->S); free(o->W); free(o->p); free(o->q);
   for (int c = 0; c < 2; ++c) { free(o->idx[c]); free(o->cnt[c]); free(o->mask[c]); free(o->hist[c]); }
   free(o->cstart); free(o->cend); free(o->cap_f); free(o->cap_t); free(o->sys_of);
   free(o);
+}
+
+/* The five law constants of system s that the reverse sweep differentiates
+ * (kn, kt, 2 beta, mu, mu_wall), read or set directly in working precision
+ * (finite differences in FP64 go through these). */
+void ens_get_constants(const ens_oracle* o, int s, double* c5) {
+  const sysc* S = &o->S[s];
+  c5[0] = S->kn; c5[1] = S->kt; c5[2] = S->beta2; c5[3] = S->mu; c5[4] = S->mu_w;
+}
+void ens_set_constants(ens_oracle* o, int s, const double* c5) {
+  sysc* S = &o->S[s];
+  S->kn = (real)c5[0]; S->kt = (real)c5[1]; S->beta2 = (real)c5[2]; S->mu = (real)c5[3];
+  S->mu_w = (real)c5[4];
 }
 
 int ens_set_params(ens_oracle* o, const blaze_system* sys) {
@@ -184,10 +202,13 @@ void ens_set_state(ens_oracle* o, const double* pos3, const double* rad, const d
     part* a = &o->p[i];
     memset(a, 0, sizeof(*a));
     a->sys = o->sys_of[i];
-    a->pos = mk((real)(float)pos3[3 * i], (real)(float)pos3[3 * i + 1], (real)(float)pos3[3 * i + 2]);
+    /* the FP32 build takes the inputs as the product does (rounded to
+       float); the FP64 build keeps them exact, so finite differences of
+       size 1e-6 are resolved */
+    a->pos = mk(IN(pos3[3 * i]), IN(pos3[3 * i + 1]), IN(pos3[3 * i + 2]));
     a->r = (real)(float)rad[i];
-    if (vel3) a->vel = mk((real)(float)vel3[3 * i], (real)(float)vel3[3 * i + 1], (real)(float)vel3[3 * i + 2]);
-    if (avel3) a->w = mk((real)(float)avel3[3 * i], (real)(float)avel3[3 * i + 1], (real)(float)avel3[3 * i + 2]);
+    if (vel3) a->vel = mk(IN(vel3[3 * i]), IN(vel3[3 * i + 1]), IN(vel3[3 * i + 2]));
+    if (avel3) a->w = mk(IN(avel3[3 * i]), IN(avel3[3 * i + 1]), IN(avel3[3 * i + 2]));
     a->pid = i;
     for (int q = 0; q < WSLOTS; ++q) a->wid[q] = -1;
   }
@@ -217,7 +238,12 @@ static int kv_cmp(const void* a, const void* b) {
   return x->idx < y->idx ? -1 : (x->idx > y->idx);
 }
 
-static void rebuild(ens_oracle* o) {
+/* Re-sort + new list.  When `perm_out` / `src_out` are given they receive,
+ * for the tape of the reverse sweep, the old index of each new position and
+ * the old slot each new slot's history came from (-1: none). */
+static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out);
+static void rebuild(ens_oracle* o) { rebuild_rec(o, NULL, NULL); }
+static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out) {
   const int n = o->n, cap = o->cap;
   const int e = o->epoch & 1;
   kv* ks = (kv*)malloc(sizeof(kv) * n);
@@ -269,12 +295,14 @@ static void rebuild(ens_oracle* o) {
               if (!(dot(rel, rel) < lim * lim)) continue;
               if (cnt < (uint32_t)cap) {
                 In[(size_t)cnt * n + i] = j;
+                if (src_out) src_out[(size_t)cnt * n + i] = -1;
                 for (uint32_t ko = 0; ko < cnt_o && ko < 32; ++ko) {
                   if (!((mask_o >> ko) & 1u)) continue;
                   const size_t so = (size_t)ko * n + io;
                   if (o->p[Io[so]].pid == b->pid) {
                     const size_t sn = (size_t)cnt * n + i;
                     Hn[3 * sn] = Ho[3 * so]; Hn[3 * sn + 1] = Ho[3 * so + 1]; Hn[3 * sn + 2] = Ho[3 * so + 2];
+                    if (src_out) src_out[sn] = (int)ko;
                     mask |= 1u << cnt;
                     break;
                   }
@@ -291,6 +319,8 @@ static void rebuild(ens_oracle* o) {
     Cn[i] = cnt < (uint32_t)cap ? cnt : (uint32_t)cap;
     Mn[i] = mask;
   }
+  if (perm_out)
+    for (int i = 0; i < n; ++i) perm_out[i] = ks[i].idx;
   part* t = o->p; o->p = o->q; o->q = t;
   o->epoch += 1;
   free(ks);
@@ -426,16 +456,40 @@ static void wall_contact(wctx* c, int id, v3 n, real delta) {
   }
 }
 
-static void step_once(ens_oracle* o) {
+/* One recorded step of the reverse sweep's tape: the step's input state
+ * (after its re-sort), the list it used with masks and histories before the
+ * step, and for a re-sort step the permutation and history sources. */
+typedef struct tstep_ {
+  int rebuilt;
+  int* perm;
+  int* src;
+  part* p;
+  uint32_t* idx;
+  uint32_t* cnt;
+  uint32_t* mask;
+  real* hist;
+} tstep;
+
+static void step_once_rec(ens_oracle* o, tstep* t);
+static void step_once(ens_oracle* o) { step_once_rec(o, NULL); }
+static void step_once_rec(ens_oracle* o, tstep* t) {
   const int n = o->n;
   const int rebuilt = o->rebuild_req;
   o->rebuild_req = 0;
-  if (rebuilt) rebuild(o);
+  if (rebuilt) rebuild_rec(o, t ? t->perm : NULL, t ? t->src : NULL);
   const int e = o->epoch & 1;
   uint32_t* I = o->idx[e];
   uint32_t* C = o->cnt[e];
   uint32_t* M = o->mask[e];
   real* H = o->hist[e];
+  if (t) {
+    t->rebuilt = rebuilt;
+    memcpy(t->p, o->p, sizeof(part) * n);
+    memcpy(t->idx, I, sizeof(uint32_t) * (size_t)o->cap * n);
+    memcpy(t->cnt, C, sizeof(uint32_t) * n);
+    memcpy(t->mask, M, sizeof(uint32_t) * n);
+    memcpy(t->hist, H, sizeof(real) * 3 * (size_t)o->cap * n);
+  }
   const real dt = o->dt;
   int req = 0;
   for (int i = 0; i < n; ++i) {
@@ -552,3 +606,349 @@ void ens_get_forces(const ens_oracle* o, double* f3, double* t3) {
 
 int ens_num_rebuilds(const ens_oracle* o) { return o->epoch; }
 int ens_status(const ens_oracle* o) { return (int)o->status; }
+
+/* ======================================================== reverse sweep
+ * Discrete adjoint of the step for the linear law (no rolling friction)
+ * with plane walls: the exact derivative of the forward's arithmetic on the
+ * branch each contact took (contact or not, stick or slip, history turned or
+ * not), i.e. active-branch derivatives at contact onset and stick/slip
+ * switches. */
+
+typedef struct { real kn, kt, b2, mu; } lawbar;
+
+/* Cotangents of contact_law's inputs (n, delta, vrel, vct, xi) and of the
+ * law constants, for cotangents Fb (force on a), Tb (torque on a) and Xb
+ * (history after the step), linear law. */
+static void contact_vjp(const ens_oracle* o, const sysc* S, real mu, v3 n, real delta, real ms,
+                        v3 vrel, v3 vct, real arm, v3 x, v3 Fb, v3 Tb, v3 Xb, v3* nb_out,
+                        real* deltab_out, v3* vrelb_out, v3* vctb_out, v3* xb_out, lawbar* th) {
+  const real dt = o->dt;
+  const real kn = S->kn, kt = S->kt;
+  /* forward, with the intermediates the reverse needs */
+  const real sqn = SQRT(ms * kn), sqt = SQRT(ms * kt);
+  const real cn = S->beta2 * sqn, ct = S->beta2 * sqt;
+  const real vn = dot(vrel, n);
+  const real fn = kn * delta - cn * vn;
+  const real fc = fn > 0 ? fn : 0;
+  const real p = dot(vct, n);
+  const v3 vt = sub(vct, smul(p, n));
+  const real xn = dot(x, n);
+  const int rot = xn != 0;
+  real m0 = 0, m1 = 0, g = 1;
+  v3 x1 = x;
+  if (rot) {
+    m0 = dot(x, x);
+    x1 = sub(x, smul(xn, n));
+    m1 = dot(x1, x1);
+    if (m1 > 0) g = SQRT(m0 / m1);
+  }
+  const v3 x2 = (rot && m1 > 0) ? mul(x1, g) : x1;
+  const v3 x3 = add(x2, mul(vt, dt));
+  const v3 ft = sub(mul(x3, -kt), mul(vt, ct));
+  const real cap = mu * fc;
+  const real f2 = dot(ft, ft);
+  const int slip = f2 > cap * cap;
+  real fmag = 0, s = 1;
+  v3 ftp = ft;
+  if (slip) {
+    fmag = SQRT(f2);
+    s = cap / fmag;
+    ftp = mul(ft, s);
+  }
+  const v3 F = add(mul(n, fn), ftp);
+  /* reverse */
+  v3 nb = mk(0, 0, 0), vtb = mk(0, 0, 0), xb = mk(0, 0, 0), ftb, x3b;
+  real fcb = 0, ctb = 0, ktb = 0, knb = 0, cnb = 0, mub = 0;
+  const v3 u = mul(n, -arm);                   /* T = u x F */
+  nb = add(nb, mul(cross(F, Tb), -arm));
+  const v3 Ft = add(Fb, cross(Tb, u));
+  real fnb = dot(Ft, n);                       /* F = n fn + ftp */
+  nb = add(nb, mul(Ft, fn));
+  v3 ftpb = Ft;
+  if (slip) {
+    const real ik = (real)-1.0 / kt;           /* x4 = (ftp + vt ct) (-1/kt) */
+    const v3 A = add(ftp, mul(vt, ct));
+    ftpb = add(ftpb, mul(Xb, ik));
+    vtb = add(vtb, mul(Xb, ik * ct));
+    ctb += dot(vt, Xb) * ik;
+    ktb += dot(A, Xb) / (kt * kt);
+    ftb = mul(ftpb, s);                        /* ftp = ft s */
+    const real sb = dot(ft, ftpb);
+    const real capb = sb / fmag;               /* s = cap / |ft| */
+    const real fmagb = -sb * cap / (fmag * fmag);
+    ftb = add(ftb, mul(ft, fmagb / fmag));
+    mub += capb * fc;
+    fcb += capb * mu;
+    x3b = mk(0, 0, 0);
+  } else {
+    ftb = ftpb;
+    x3b = Xb;
+  }
+  x3b = add(x3b, mul(ftb, -kt));               /* ft = x3 (-kt) - vt ct */
+  ktb -= dot(x3, ftb);
+  ctb -= dot(vt, ftb);
+  vtb = add(vtb, mul(ftb, -ct));
+  const v3 x2b = x3b;                          /* x3 = x2 + vt dt */
+  vtb = add(vtb, mul(x3b, dt));
+  if (rot) {
+    v3 x1b = x2b;
+    if (m1 > 0) {
+      x1b = mul(x2b, g);                       /* x2 = x1 sqrt(m0 / m1) */
+      const real gb = dot(x1, x2b);
+      const real m0b = gb * g / (2 * m0);
+      const real m1b = -gb * g / (2 * m1);
+      x1b = add(x1b, mul(x1, 2 * m1b));
+      xb = add(xb, mul(x, 2 * m0b));
+    }
+    xb = add(xb, x1b);                         /* x1 = x - xn n */
+    const real xnb = -dot(n, x1b);
+    nb = add(nb, mul(x1b, -xn));
+    xb = add(xb, mul(n, xnb));                 /* xn = x . n */
+    nb = add(nb, mul(x, xnb));
+  } else {
+    xb = x2b;
+  }
+  if (fn > 0) fnb += fcb;                      /* fc = max(fn, 0) */
+  v3 vctb = vtb;                               /* vt = vct - (vct . n) n */
+  const real pb = -dot(n, vtb);
+  nb = add(nb, mul(vtb, -p));
+  vctb = add(vctb, mul(n, pb));
+  nb = add(nb, mul(vct, pb));
+  knb += fnb * delta;                          /* fn = kn delta - cn vn */
+  const real deltab = kn * fnb;
+  cnb -= fnb * vn;
+  const real vnb = -cn * fnb;
+  const v3 vrelb = mul(n, vnb);                /* vn = vrel . n */
+  nb = add(nb, mul(vrel, vnb));
+  th->b2 += cnb * sqn + ctb * sqt;             /* c = 2 beta sqrt(m* k) */
+  knb += cnb * S->beta2 * ms / (2 * sqn);
+  ktb += ctb * S->beta2 * ms / (2 * sqt);
+  th->kn += knb;
+  th->kt += ktb;
+  th->mu += mub;
+  *nb_out = nb;
+  *deltab_out = deltab;
+  *vrelb_out = vrelb;
+  *vctb_out = vctb;
+  *xb_out = xb;
+}
+
+/* Cotangents of a pair contact (a = this particle, b = its neighbour, as in
+ * step_once) for cotangents Fb, Tb on a's force and torque and Xb on the
+ * history after the step.  Adds to a's and b's state cotangents; returns
+ * the history cotangent before the step.  Needs the pair in contact. */
+typedef struct { v3 x, v, w; } sbar;
+static v3 pair_vjp(const ens_oracle* o, const sysc* S, const part* a, const part* b, v3 xi,
+                   v3 Fb, v3 Tb, v3 Xb, sbar* ab, sbar* bb, lawbar* th) {
+  const real ra = a->r, rb = b->r;
+  const v3 rel = sub(a->pos, b->pos);
+  const real dist = SQRT(dot(rel, rel));
+  const real inv = (real)1.0 / dist;
+  const v3 n = mul(rel, inv);
+  const real delta = (ra + rb) - dist;
+  const real ma = S->dens43pi * ((ra * ra) * ra), mb = S->dens43pi * ((rb * rb) * rb);
+  const real ms = (ma * mb) / (ma + mb);
+  const v3 ua = mul(n, -ra), ub = mul(n, rb);
+  const v3 vca = add(a->vel, cross(a->w, ua));
+  const v3 vcb = add(b->vel, cross(b->w, ub));
+  v3 nb, vrelb, vctb, xib;
+  real deltab;
+  contact_vjp(o, S, S->mu, n, delta, ms, sub(a->vel, b->vel), sub(vca, vcb), ra, xi, Fb, Tb, Xb,
+              &nb, &deltab, &vrelb, &vctb, &xib, th);
+  /* vct = vca - vcb, vca = va + wa x ua, vcb = vb + wb x ub */
+  ab->v = add(ab->v, vctb);
+  ab->w = add(ab->w, cross(ua, vctb));
+  nb = add(nb, mul(cross(vctb, a->w), -ra));
+  const v3 vcbb = mul(vctb, -1);
+  bb->v = add(bb->v, vcbb);
+  bb->w = add(bb->w, cross(ub, vcbb));
+  nb = add(nb, mul(cross(vcbb, b->w), rb));
+  ab->v = add(ab->v, vrelb);                   /* vrel = va - vb */
+  bb->v = sub(bb->v, vrelb);
+  real distb = -deltab;                        /* delta = (ra + rb) - dist */
+  v3 relb = mul(nb, inv);                      /* n = rel / dist */
+  distb -= dot(rel, nb) * inv * inv;
+  relb = add(relb, mul(rel, distb / dist));    /* dist = |rel| */
+  ab->x = add(ab->x, relb);
+  bb->x = sub(bb->x, relb);
+  return xib;
+}
+
+/* Cotangents of a plane-wall contact of particle a; the wall friction
+ * coefficient's cotangent is added to *mu_wb. */
+static v3 plane_vjp(const ens_oracle* o, const sysc* S, const wallc* W, const part* a, v3 xi,
+                    v3 Fb, v3 Tb, v3 Xb, sbar* ab, lawbar* th, real* mu_wb) {
+  const real r = a->r;
+  const v3 n = W->a;
+  const real delta = r - (dot(W->a, a->pos) - W->r);
+  const real ma = S->dens43pi * ((r * r) * r);
+  const v3 ua = mul(n, -r);
+  const v3 vca = add(a->vel, cross(a->w, ua));
+  v3 nb, vrelb, vctb, xib;
+  real deltab;
+  lawbar tw = {0, 0, 0, 0};
+  contact_vjp(o, S, S->mu_w, n, delta, ma, a->vel, vca, r, xi, Fb, Tb, Xb, &nb, &deltab, &vrelb,
+              &vctb, &xib, &tw);
+  th->kn += tw.kn;
+  th->kt += tw.kt;
+  th->b2 += tw.b2;
+  *mu_wb += tw.mu;
+  ab->v = add(ab->v, add(vrelb, vctb));        /* vrel = va, vct = va + wa x ua */
+  ab->w = add(ab->w, cross(ua, vctb));
+  ab->x = add(ab->x, mul(n, -deltab));         /* delta = r - (n . x - d); n is fixed */
+  return xib;
+}
+
+/* Reverse sweep.  ens_adj_record runs `nsteps` steps from the current state
+ * and keeps their tape (the state advances); ens_adj_reverse then
+ * propagates the cotangents of the final state (gx_f, gv_f, gw_f: 3 per
+ * particle, final memory order) back to the recorded initial state (gx0,
+ * gv0, gw0: its memory order) and to the five law constants of every system
+ * (gth: nsys x {kn, kt, 2 beta, mu, mu_wall}), and frees the tape.  Linear
+ * law, plane walls, no rolling friction; record returns -1 for anything
+ * else. */
+static void free_tape(ens_oracle* o) {
+  for (int s = 0; s < o->ntape; ++s) {
+    tstep* t = &o->tape[s];
+    free(t->perm); free(t->src); free(t->p); free(t->idx); free(t->cnt); free(t->mask);
+    free(t->hist);
+  }
+  free(o->tape);
+  o->tape = NULL;
+  o->ntape = 0;
+}
+
+int ens_adj_record(ens_oracle* o, int nsteps) {
+  const int n = o->n, cap = o->cap;
+  const size_t ns = (size_t)cap * n;
+  if (o->law != BLAZE_LAW_LINEAR) return -1;
+  for (int s = 0; s < o->nsys; ++s)
+    if (o->S[s].mu_r > 0 || o->S[s].ntri > 0) return -1;
+  for (int w = 0; w < o->nwalls; ++w)
+    if (o->W[w].kind != BLAZE_WALL_PLANE) return -1;
+  free_tape(o);
+  tstep* T = (tstep*)calloc(nsteps, sizeof(tstep));
+  o->tape = T;
+  o->ntape = nsteps;
+  for (int s = 0; s < nsteps; ++s) {
+    T[s].perm = (int*)malloc(sizeof(int) * n);
+    T[s].src = (int*)malloc(sizeof(int) * ns);
+    T[s].p = (part*)malloc(sizeof(part) * n);
+    T[s].idx = (uint32_t*)malloc(sizeof(uint32_t) * ns);
+    T[s].cnt = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    T[s].mask = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    T[s].hist = (real*)malloc(sizeof(real) * 3 * ns);
+    step_once_rec(o, &T[s]);
+  }
+  return (int)o->status;
+}
+
+int ens_adj_reverse(ens_oracle* o, const double* gx_f, const double* gv_f, const double* gw_f,
+                    double* gx0, double* gv0, double* gw0, double* gth) {
+  const int n = o->n, cap = o->cap, nsteps = o->ntape;
+  const size_t ns = (size_t)cap * n;
+  tstep* T = o->tape;
+  if (!T) return -1;
+  const real dt = o->dt;
+  sbar* g = (sbar*)calloc(n, sizeof(sbar));
+  sbar* gin = (sbar*)calloc(n, sizeof(sbar));
+  v3* gH = (v3*)calloc(ns, sizeof(v3));
+  v3* gHin = (v3*)calloc(ns, sizeof(v3));
+  v3* gW = (v3*)calloc((size_t)n * WSLOTS, sizeof(v3));
+  v3* gWin = (v3*)calloc((size_t)n * WSLOTS, sizeof(v3));
+  v3* Fb = (v3*)calloc(n, sizeof(v3));
+  v3* Tb = (v3*)calloc(n, sizeof(v3));
+  lawbar* th = (lawbar*)calloc(o->nsys, sizeof(lawbar));
+  real* muw = (real*)calloc(o->nsys, sizeof(real));
+  for (int i = 0; i < n; ++i) {
+    g[i].x = mk(gx_f[3 * i], gx_f[3 * i + 1], gx_f[3 * i + 2]);
+    g[i].v = mk(gv_f[3 * i], gv_f[3 * i + 1], gv_f[3 * i + 2]);
+    g[i].w = mk(gw_f[3 * i], gw_f[3 * i + 1], gw_f[3 * i + 2]);
+  }
+  int rc = (int)o->status;
+  for (int s = nsteps - 1; s >= 0 && rc >= 0; --s) {
+    const tstep* t = &T[s];
+    const part* P = t->p;
+    /* symplectic Euler: v' = v + (f/m + g) dt, x' = x + v' dt, w' = w + t/I dt */
+    for (int i = 0; i < n; ++i) {
+      const sysc* S = &o->S[P[i].sys];
+      const real r = P[i].r;
+      const real m = S->dens43pi * ((r * r) * r);
+      const real inertia = ((real)0.4 * m) * (r * r);
+      const v3 gv = add(g[i].v, mul(g[i].x, dt));
+      Fb[i] = mul(gv, dt / m);
+      Tb[i] = mul(g[i].w, dt / inertia);
+      gin[i].x = g[i].x;
+      gin[i].v = gv;
+      gin[i].w = g[i].w;
+    }
+    memset(gHin, 0, sizeof(v3) * ns);
+    memset(gWin, 0, sizeof(v3) * (size_t)n * WSLOTS);
+    for (int i = 0; i < n && rc >= 0; ++i) {
+      const part* a = &P[i];
+      const sysc* S = &o->S[a->sys];
+      lawbar* tb = &th[a->sys];
+      const real ra = a->r;
+      for (uint32_t k = 0; k < t->cnt[i]; ++k) {
+        const size_t sk = (size_t)k * n + i;
+        const part* b = &P[t->idx[sk]];
+        const v3 rel = sub(a->pos, b->pos);
+        const real sr = ra + b->r;
+        const real d2 = dot(rel, rel);
+        if (!(d2 < sr * sr) || !(SQRT(d2) > 0)) continue;
+        const int had = (t->mask[i] >> k) & 1u;
+        const v3 xi = had ? mk(t->hist[3 * sk], t->hist[3 * sk + 1], t->hist[3 * sk + 2]) : mk(0, 0, 0);
+        const v3 xib = pair_vjp(o, S, a, b, xi, Fb[i], Tb[i], gH[sk], &gin[i], &gin[t->idx[sk]], tb);
+        if (had) gHin[sk] = xib;
+      }
+      int nw = 0;
+      for (int w = S->wall0; w < S->wall0 + S->nwall; ++w) {
+        v3 nn;
+        real d;
+        int reg;
+        if (!wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) continue;
+        int q_old = -1;
+        for (int q = 0; q < WSLOTS; ++q)
+          if (((a->wmask >> q) & 1u) && a->wid[q] == w) q_old = q;
+        const v3 xi = q_old >= 0 ? mk(a->wh[q_old][0], a->wh[q_old][1], a->wh[q_old][2]) : mk(0, 0, 0);
+        const v3 Xb = nw < WSLOTS ? gW[(size_t)i * WSLOTS + nw] : mk(0, 0, 0);
+        const v3 xib = plane_vjp(o, S, &o->W[w], a, xi, Fb[i], Tb[i], Xb, &gin[i], tb, &muw[a->sys]);
+        if (q_old >= 0) gWin[(size_t)i * WSLOTS + q_old] = xib;
+        ++nw;
+      }
+    }
+    if (t->rebuilt) {
+      /* the step read the re-sorted state: send the cotangents back through
+         the permutation and the history carry-over */
+      memset(g, 0, sizeof(sbar) * n);
+      memset(gH, 0, sizeof(v3) * ns);
+      memset(gW, 0, sizeof(v3) * (size_t)n * WSLOTS);
+      for (int i = 0; i < n; ++i) {
+        const int io = t->perm[i];
+        g[io] = gin[i];
+        for (int q = 0; q < WSLOTS; ++q) gW[(size_t)io * WSLOTS + q] = gWin[(size_t)i * WSLOTS + q];
+        for (uint32_t k = 0; k < t->cnt[i]; ++k) {
+          const size_t sk = (size_t)k * n + i;
+          if (t->src[sk] >= 0) gH[(size_t)t->src[sk] * n + io] = gHin[sk];
+        }
+      }
+    } else {
+      memcpy(g, gin, sizeof(sbar) * n);
+      memcpy(gH, gHin, sizeof(v3) * ns);
+      memcpy(gW, gWin, sizeof(v3) * (size_t)n * WSLOTS);
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    gx0[3 * i] = g[i].x.x; gx0[3 * i + 1] = g[i].x.y; gx0[3 * i + 2] = g[i].x.z;
+    gv0[3 * i] = g[i].v.x; gv0[3 * i + 1] = g[i].v.y; gv0[3 * i + 2] = g[i].v.z;
+    gw0[3 * i] = g[i].w.x; gw0[3 * i + 1] = g[i].w.y; gw0[3 * i + 2] = g[i].w.z;
+  }
+  for (int s = 0; s < o->nsys; ++s) {
+    gth[5 * s] = th[s].kn; gth[5 * s + 1] = th[s].kt; gth[5 * s + 2] = th[s].b2;
+    gth[5 * s + 3] = th[s].mu; gth[5 * s + 4] = muw[s];
+  }
+  free_tape(o);
+  free(g); free(gin); free(gH); free(gHin); free(gW); free(gWin); free(Fb); free(Tb);
+  free(th); free(muw);
+  return rc;
+}
