@@ -103,6 +103,30 @@ int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4,
 int blaze_ens_last_launches(blaze_ens* e);
 int blaze_ens_rebuild_kernels(blaze_ens* e);
 
+/* ------------------------------------------------------------ reverse mode
+ * Gradients of a loss of the final state with respect to the initial state
+ * and the law constants, by the discrete adjoint of the step (linear law
+ * with tangential history and Coulomb cap, plane walls, no rolling
+ * friction).  The forward keeps a checkpoint of the full state every
+ * `segment` steps; the backward recomputes each segment into a tape and
+ * walks it back, segment by segment.  Derivatives are those of the branch
+ * each contact took (contact or not, stick or slip). */
+typedef struct blaze_ens_adj blaze_ens_adj;
+
+int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment);
+/* nsteps steps from the ensemble's current state, with checkpoints; the
+ * ensemble then holds the final state (read it with blaze_ens_get_state). */
+int blaze_ens_adj_forward(blaze_ens_adj* a);
+/* Cotangents of the final state (3 floats per particle, final memory order;
+ * NULL for zero) -> cotangents of the initial state (its memory order; NULL
+ * skips) and of the law constants of every system (nsys x 5 doubles: kn,
+ * kt, 2 beta, mu, mu_wall; beta = -ln e / sqrt(ln^2 e + pi^2)).  Leaves the
+ * ensemble at an intermediate state: set the state again before stepping. */
+int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
+                           const float* gavel, float* gpos0, float* gvel0, float* gavel0,
+                           double* gconst);
+int blaze_ens_adj_destroy(blaze_ens_adj* a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,11 @@ def load():
         lib.blaze_ens_device_state.argtypes = [C.c_void_p] + [P(C.c_void_p)] * 4
         lib.blaze_ens_last_launches.argtypes = [C.c_void_p]
         lib.blaze_ens_rebuild_kernels.argtypes = [C.c_void_p]
+        lib.blaze_ens_adj_create.argtypes = [P(C.c_void_p), C.c_void_p, C.c_int, C.c_int]
+        lib.blaze_ens_adj_forward.argtypes = [C.c_void_p]
+        lib.blaze_ens_adj_backward.argtypes = [C.c_void_p, _f, _f, _f, _f, _f, _f,
+                                               P(C.c_double)]
+        lib.blaze_ens_adj_destroy.argtypes = [C.c_void_p]
         _bound = True
     return lib
 
@@ -187,3 +192,71 @@ class Ensemble:
 
     def rebuild_kernels(self):
         return self.lib.blaze_ens_rebuild_kernels(self.h)
+
+
+class Adjoint:
+    """Reverse mode of an Ensemble over `nsteps` steps (linear law, plane
+    walls): forward() steps the ensemble from its current state keeping a
+    checkpoint every `segment` steps; backward() takes the cotangents of the
+    final state (final memory order) and returns those of the initial state
+    (its memory order) and of the law constants (nsys x 5: kn, kt, 2 beta,
+    mu, mu_wall)."""
+
+    def __init__(self, ens, nsteps, segment=100):
+        self.ens = ens
+        self.lib = ens.lib
+        h = C.c_void_p()
+        _check(self.lib.blaze_ens_adj_create(C.byref(h), ens.h, int(nsteps), int(segment)),
+               "blaze_ens_adj_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.blaze_ens_adj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self):
+        return _check(self.lib.blaze_ens_adj_forward(self.h), "blaze_ens_adj_forward")
+
+    def backward(self, gpos=None, gvel=None, gavel=None):
+        n = self.ens.n
+        c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(n, 3)
+        gpos, gvel, gavel = c(gpos), c(gvel), c(gavel)
+        out = [np.zeros((n, 3), np.float32) for _ in range(3)]
+        gc = np.zeros((self.ens.nsys, 5), np.float64)
+        _check(self.lib.blaze_ens_adj_backward(
+            self.h, _ptr(gpos, C.c_float), _ptr(gvel, C.c_float), _ptr(gavel, C.c_float),
+            *[_ptr(a, C.c_float) for a in out], gc.ctypes.data_as(C.POINTER(C.c_double))),
+            "blaze_ens_adj_backward")
+        return out[0], out[1], out[2], gc
+
+
+def beta2_of_e(e):
+    """2 beta with beta = -ln e / sqrt(ln^2 e + pi^2) (damping from restitution)."""
+    le = np.log(e)
+    return 2.0 * (-le / np.sqrt(le * le + np.pi ** 2))
+
+
+def dbeta2_de(e):
+    le = np.log(e)
+    return 2.0 * (-np.pi ** 2 / (e * (le * le + np.pi ** 2) ** 1.5))
+
+
+def user_param_grads(gconst, systems):
+    """Cotangents of (kn, kt_ratio, restitution, mu, mu_wall) per system from
+    those of the law constants (kn, kt = kt_ratio kn, 2 beta(e), mu, mu_wall)."""
+    out = np.zeros((len(systems), 5))
+    for s, S in enumerate(systems):
+        g = gconst[s]
+        out[s, 0] = g[0] + g[1] * S.kt_ratio
+        out[s, 1] = g[1] * S.kn
+        out[s, 2] = g[2] * dbeta2_de(S.restitution)
+        out[s, 3] = g[3]
+        out[s, 4] = g[4]
+    return out

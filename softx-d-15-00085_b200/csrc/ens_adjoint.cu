@@ -1,0 +1,405 @@
+// ens_adjoint.cu -- reverse-mode kernels of the ensemble step (see
+// ens_adjoint.cuh).  The contact-law reverse below follows the forward in
+// ens_kernels.cu (contact_law, linear law) statement by statement, in
+// reverse order.
+#include "ens_adjoint.cuh"
+
+namespace blaze {
+namespace {
+
+constexpr int kThreads = 128;
+
+struct LawBar { float kn, kt, b2, mu; };
+struct SBar { float3 x, v, w; };
+
+__device__ __forceinline__ float3 xyz4(float4 a) { return f3(a.x, a.y, a.z); }
+__device__ __forceinline__ float4 w4(float3 a) { return make_float4(a.x, a.y, a.z, 0.0f); }
+
+// Cotangents of contact_law's inputs (n, delta, vrel, vct, xi) and of the
+// law constants for cotangents Fb, Tb (force, torque on a) and Xb (history
+// after the step).
+__device__ void contact_vjp(const EnsSysDev& S, float mu, float3 n, float delta, float ms,
+                            float3 vrel, float3 vct, float arm, float3 x, float dt, float3 Fb,
+                            float3 Tb, float3 Xb, float3& nb, float& deltab, float3& vrelb,
+                            float3& vctb, float3& xb, LawBar& th) {
+  const float kn = S.kn, kt = S.kt;
+  const float sqn = sqrtf(ms * kn), sqt = sqrtf(ms * kt);
+  const float cn = S.beta2 * sqn, ct = S.beta2 * sqt;
+  const float vn = dot3(vrel, n);
+  const float fn = kn * delta - cn * vn;
+  const float fc = fn > 0.0f ? fn : 0.0f;
+  const float p = dot3(vct, n);
+  const float3 vt = vct - p * n;
+  const float xn = dot3(x, n);
+  const bool rot = xn != 0.0f;
+  float m0 = 0.0f, m1 = 0.0f, g = 1.0f;
+  float3 x1 = x;
+  if (rot) {
+    m0 = dot3(x, x);
+    x1 = x - xn * n;
+    m1 = dot3(x1, x1);
+    if (m1 > 0.0f) g = sqrtf(m0 / m1);
+  }
+  const float3 x2 = (rot && m1 > 0.0f) ? x1 * g : x1;
+  const float3 x3 = x2 + vt * dt;
+  const float3 ft = x3 * (-kt) - vt * ct;
+  const float cap = mu * fc;
+  const float f2 = dot3(ft, ft);
+  const bool slip = f2 > cap * cap;
+  float fmag = 0.0f, s = 1.0f;
+  float3 ftp = ft;
+  if (slip) {
+    fmag = sqrtf(f2);
+    s = cap / fmag;
+    ftp = ft * s;
+  }
+  const float3 F = n * fn + ftp;
+  // reverse
+  float3 vtb = f3(0.0f, 0.0f, 0.0f), ftb, x3b;
+  float fcb = 0.0f, ctb = 0.0f, ktb = 0.0f, knb = 0.0f, cnb = 0.0f, mub = 0.0f;
+  xb = f3(0.0f, 0.0f, 0.0f);
+  const float3 u = n * (-arm);                 // T = u x F
+  nb = cross3(F, Tb) * (-arm);
+  const float3 Ft = Fb + cross3(Tb, u);
+  float fnb = dot3(Ft, n);                     // F = n fn + ftp
+  nb = nb + Ft * fn;
+  float3 ftpb = Ft;
+  if (slip) {
+    const float ik = -1.0f / kt;               // x4 = (ftp + vt ct)(-1/kt)
+    const float3 A = ftp + vt * ct;
+    ftpb = ftpb + Xb * ik;
+    vtb = vtb + Xb * (ik * ct);
+    ctb += dot3(vt, Xb) * ik;
+    ktb += dot3(A, Xb) / (kt * kt);
+    ftb = ftpb * s;                            // ftp = ft s
+    const float sb = dot3(ft, ftpb);
+    const float capb = sb / fmag;              // s = cap / |ft|
+    const float fmagb = -sb * cap / (fmag * fmag);
+    ftb = ftb + ft * (fmagb / fmag);
+    mub += capb * fc;
+    fcb += capb * mu;
+    x3b = f3(0.0f, 0.0f, 0.0f);
+  } else {
+    ftb = ftpb;
+    x3b = Xb;
+  }
+  x3b = x3b + ftb * (-kt);                     // ft = x3 (-kt) - vt ct
+  ktb -= dot3(x3, ftb);
+  ctb -= dot3(vt, ftb);
+  vtb = vtb + ftb * (-ct);
+  const float3 x2b = x3b;                      // x3 = x2 + vt dt
+  vtb = vtb + x3b * dt;
+  if (rot) {
+    float3 x1b = x2b;
+    if (m1 > 0.0f) {
+      x1b = x2b * g;                           // x2 = x1 sqrt(m0 / m1)
+      const float gb = dot3(x1, x2b);
+      const float m0b = gb * g / (2.0f * m0);
+      const float m1b = -gb * g / (2.0f * m1);
+      x1b = x1b + x1 * (2.0f * m1b);
+      xb = xb + x * (2.0f * m0b);
+    }
+    xb = xb + x1b;                             // x1 = x - xn n
+    const float xnb = -dot3(n, x1b);
+    nb = nb + x1b * (-xn);
+    xb = xb + n * xnb;                         // xn = x . n
+    nb = nb + x * xnb;
+  } else {
+    xb = x2b;
+  }
+  if (fn > 0.0f) fnb += fcb;                   // fc = max(fn, 0)
+  vctb = vtb;                                  // vt = vct - (vct . n) n
+  const float pb = -dot3(n, vtb);
+  nb = nb + vtb * (-p);
+  vctb = vctb + n * pb;
+  nb = nb + vct * pb;
+  knb += fnb * delta;                          // fn = kn delta - cn vn
+  deltab = kn * fnb;
+  cnb -= fnb * vn;
+  const float vnb = -cn * fnb;
+  vrelb = n * vnb;                             // vn = vrel . n
+  nb = nb + vrel * vnb;
+  th.b2 += cnb * sqn + ctb * sqt;              // c = 2 beta sqrt(m* k)
+  knb += cnb * S.beta2 * ms / (2.0f * sqn);
+  ktb += ctb * S.beta2 * ms / (2.0f * sqt);
+  th.kn += knb;
+  th.kt += ktb;
+  th.mu += mub;
+}
+
+struct Body { float3 x, v, w; float r, m; };
+
+// Reverse of a pair contact (a = the particle, b = its neighbour): adds to
+// a's and b's state cotangents, returns the history cotangent before the
+// step.
+__device__ float3 pair_vjp(const EnsSysDev& S, const Body& a, const Body& b, float3 xi, float dt,
+                           float3 Fb, float3 Tb, float3 Xb, SBar& ab, SBar& bb, LawBar& th) {
+  const float3 rel = a.x - b.x;
+  const float dist = sqrtf(dot3(rel, rel));
+  const float inv = 1.0f / dist;
+  const float3 n = rel * inv;
+  const float delta = (a.r + b.r) - dist;
+  const float ms = (a.m * b.m) / (a.m + b.m);
+  const float3 ua = n * (-a.r), ub = n * b.r;
+  const float3 vca = a.v + cross3(a.w, ua);
+  const float3 vcb = b.v + cross3(b.w, ub);
+  float3 nb, vrelb, vctb, xib;
+  float deltab;
+  contact_vjp(S, S.mu, n, delta, ms, a.v - b.v, vca - vcb, a.r, xi, dt, Fb, Tb, Xb, nb, deltab,
+              vrelb, vctb, xib, th);
+  ab.v = ab.v + vctb;                          // vct = vca - vcb
+  ab.w = ab.w + cross3(ua, vctb);              // vca = va + wa x ua
+  nb = nb + cross3(vctb, a.w) * (-a.r);
+  const float3 vcbb = vctb * (-1.0f);
+  bb.v = bb.v + vcbb;                          // vcb = vb + wb x ub
+  bb.w = bb.w + cross3(ub, vcbb);
+  nb = nb + cross3(vcbb, b.w) * b.r;
+  ab.v = ab.v + vrelb;                         // vrel = va - vb
+  bb.v = bb.v - vrelb;
+  float distb = -deltab;                       // delta = (ra + rb) - dist
+  float3 relb = nb * inv;                      // n = rel / dist
+  distb -= dot3(rel, nb) * inv * inv;
+  relb = relb + rel * (distb / dist);          // dist = |rel|
+  ab.x = ab.x + relb;
+  bb.x = bb.x - relb;
+  return xib;
+}
+
+// Reverse of a plane-wall contact of particle a (the plane is fixed).
+__device__ float3 plane_vjp(const EnsSysDev& S, const EnsWallDev& W, const Body& a, float3 xi,
+                            float dt, float3 Fb, float3 Tb, float3 Xb, SBar& ab, LawBar& th,
+                            float& mu_wb) {
+  const float3 n = W.a;
+  const float delta = a.r - (dot3(W.a, a.x) - W.r);
+  const float3 ua = n * (-a.r);
+  const float3 vca = a.v + cross3(a.w, ua);
+  float3 nb, vrelb, vctb, xib;
+  float deltab;
+  LawBar tw = {0.0f, 0.0f, 0.0f, 0.0f};
+  contact_vjp(S, S.mu_w, n, delta, a.m, a.v, vca, a.r, xi, dt, Fb, Tb, Xb, nb, deltab, vrelb,
+              vctb, xib, tw);
+  th.kn += tw.kn;
+  th.kt += tw.kt;
+  th.b2 += tw.b2;
+  mu_wb += tw.mu;
+  ab.v = ab.v + vrelb + vctb;
+  ab.w = ab.w + cross3(ua, vctb);
+  ab.x = ab.x + n * (-deltab);
+  return xib;
+}
+
+__device__ __forceinline__ Body body(const EnsTape& tp, const EnsSysDev& S, size_t at) {
+  const float4 p = tp.pos[at], v = tp.vel[at], w = tp.angv[at];
+  Body B;
+  B.x = xyz4(p);
+  B.v = xyz4(v);
+  B.w = xyz4(w);
+  B.r = p.w;
+  B.m = S.dens43pi * ((p.w * p.w) * p.w);
+  return B;
+}
+
+// -------------------------------------------------------------- snapshot
+__global__ void __launch_bounds__(kThreads)
+k_adj_snap(EnsTape tp, int t, EnsBufs b, StateBuf plain, StateBuf sorted, int n,
+           const StepCtl* ctl, const int* rebuilt, const int32_t* perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int flag = *rebuilt != 0;
+  const int e = ctl->epoch & 1;
+  const StateBuf in = flag ? sorted : plain;
+  const size_t base = (size_t)t * n + i;
+  const size_t cbase = (size_t)t * b.cap * n;
+  const float4 v = in.vel[i];
+  tp.pos[base] = in.pos[i];
+  tp.vel[base] = v;
+  tp.angv[base] = in.angv[i];
+  const EnsList L = b.L[e];
+  const uint32_t c = L.cnt[i];
+  tp.cnt[base] = c;
+  tp.mask[base] = L.mask[i];
+  for (uint32_t k = 0; k < c; ++k) {
+    const size_t s = (size_t)k * b.stride + i;
+    const size_t d = cbase + (size_t)k * n + i;
+    tp.idx[d] = L.idx[s];
+    tp.hx[d] = L.hx[s];
+    tp.hy[d] = L.hy[s];
+    tp.hz[d] = L.hz[s];
+    if (flag) tp.src[d] = L.src[s];
+  }
+  if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      tp.wh[((size_t)t * kWallSlots + q) * n + i] = b.wh[e][(size_t)q * b.stride + i];
+  }
+  if (flag) tp.perm[base] = perm[i];
+  if (i == 0) tp.rb[t] = flag;
+}
+
+// --------------------------------------------------------------- reverse
+// Symplectic Euler backwards: cotangents of the step's force and torque, and
+// the state cotangents before the step that do not go through the forces.
+__global__ void __launch_bounds__(kThreads)
+k_adj_pre(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t at = (size_t)t * n + i;
+  const float4 p = tp.pos[at];
+  const uint32_t sys = __float_as_uint(tp.vel[at].w) & kSysMask;
+  const EnsSysDev& S = g.sys[sys];
+  const float r = p.w;
+  const float m = S.dens43pi * ((r * r) * r);
+  const float inertia = (0.4f * m) * (r * r);
+  const float3 gx = xyz4(a.gx[i]);
+  const float3 gv = xyz4(a.gv[i]) + gx * g.dt;
+  const float3 gw = xyz4(a.gw[i]);
+  a.Fb[i] = w4(gv * (g.dt / m));
+  a.Tb[i] = w4(gw * (g.dt / inertia));
+  a.ix[i] = w4(gx);
+  a.iv[i] = w4(gv);
+  a.iw[i] = w4(gw);
+}
+
+// Contacts backwards.  Particle i collects (1) the reverse of its own
+// contacts (its state, its histories, the law constants) and (2) for each
+// neighbour j in contact, the part of j's contact with i that goes to i,
+// evaluated from j's side with j's force/torque/history cotangents.
+__global__ void __launch_bounds__(kThreads)
+k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t at = (size_t)t * n + i;
+  const size_t cbase = (size_t)t * cap * n;
+  const uint32_t bits = __float_as_uint(tp.vel[at].w);
+  const EnsSysDev& S = g.sys[bits & kSysMask];
+  const Body A = body(tp, S, at);
+  const float3 Fb = xyz4(a.Fb[i]), Tb = xyz4(a.Tb[i]);
+  SBar ab;
+  ab.x = f3(0.0f, 0.0f, 0.0f);
+  ab.v = ab.x;
+  ab.w = ab.x;
+  LawBar th = {0.0f, 0.0f, 0.0f, 0.0f};
+  float mu_wb = 0.0f;
+  const uint32_t cnt = tp.cnt[at], mask = tp.mask[at];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t d = cbase + (size_t)k * n + i;
+    const uint32_t j = tp.idx[d];
+    const Body B = body(tp, S, (size_t)t * n + j);
+    const float3 rel = A.x - B.x;
+    const float sr = A.r + B.r;
+    const float d2 = dot3(rel, rel);
+    float4 hout = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (d2 < sr * sr && sqrtf(d2) > 0.0f) {
+      const bool had = (mask >> k) & 1u;
+      const float3 xi = had ? f3(tp.hx[d], tp.hy[d], tp.hz[d]) : f3(0.0f, 0.0f, 0.0f);
+      SBar dummy;
+      dummy.x = f3(0.0f, 0.0f, 0.0f);
+      dummy.v = dummy.x;
+      dummy.w = dummy.x;
+      const float3 xib = pair_vjp(S, A, B, xi, g.dt, Fb, Tb, xyz4(a.gH[d]), ab, dummy, th);
+      if (had) hout = w4(xib);
+      // j's contact with i, from j's side
+      const size_t jt = (size_t)t * n + j;
+      const uint32_t cj = tp.cnt[jt], mj = tp.mask[jt];
+      for (uint32_t q = 0; q < cj; ++q) {
+        const size_t dj = cbase + (size_t)q * n + j;
+        if (tp.idx[dj] != (uint32_t)i) continue;
+        const float3 xj = ((mj >> q) & 1u) ? f3(tp.hx[dj], tp.hy[dj], tp.hz[dj])
+                                           : f3(0.0f, 0.0f, 0.0f);
+        SBar jb;
+        jb.x = f3(0.0f, 0.0f, 0.0f);
+        jb.v = jb.x;
+        jb.w = jb.x;
+        LawBar tj = {0.0f, 0.0f, 0.0f, 0.0f};
+        pair_vjp(S, B, A, xj, g.dt, xyz4(a.Fb[j]), xyz4(a.Tb[j]), xyz4(a.gH[dj]), jb, ab, tj);
+        break;
+      }
+    }
+    a.iH[d] = hout;
+  }
+  // plane walls, in the forward's order; slot nw of the output history is
+  // the nw-th contact, slot q of the input the one with the same wall id
+  const uint32_t wmask = bits >> kSysBits;
+  float4 oh[kWallSlots];
+#pragma unroll
+  for (int q = 0; q < kWallSlots; ++q) {
+    oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+    if ((wmask >> q) & 1u) oh[q] = tp.wh[((size_t)t * kWallSlots + q) * n + i];
+  }
+  float4 win[kWallSlots];
+#pragma unroll
+  for (int q = 0; q < kWallSlots; ++q) win[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  int nw = 0;
+  for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
+    const EnsWallDev W = g.walls[w];
+    const float s = dot3(W.a, A.x) - W.r;
+    if (!(s < A.r)) continue;
+    float3 xi = f3(0.0f, 0.0f, 0.0f);
+    int qo = -1;
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if (__float_as_int(oh[q].w) == w) { xi = xyz4(oh[q]); qo = q; }
+    const float3 Xb = nw < kWallSlots ? xyz4(a.gW[(size_t)nw * n + i]) : f3(0.0f, 0.0f, 0.0f);
+    const float3 xib = plane_vjp(S, W, A, xi, g.dt, Fb, Tb, Xb, ab, th, mu_wb);
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if (q == qo) win[q] = w4(xib);
+    ++nw;
+  }
+#pragma unroll
+  for (int q = 0; q < kWallSlots; ++q) a.iW[(size_t)q * n + i] = win[q];
+  a.ix[i] = w4(xyz4(a.ix[i]) + ab.x);
+  a.iv[i] = w4(xyz4(a.iv[i]) + ab.v);
+  a.iw[i] = w4(xyz4(a.iw[i]) + ab.w);
+  float* tr = a.th + (size_t)5 * i;
+  tr[0] += th.kn;
+  tr[1] += th.kt;
+  tr[2] += th.b2;
+  tr[3] += th.mu;
+  tr[4] += mu_wb;
+}
+
+// A re-sort backwards: cotangents go to the old positions and, for carried
+// histories, to the old slots (the caller zeroes gH first).
+__global__ void __launch_bounds__(kThreads)
+k_adj_unsort(EnsTape tp, int t, int n, int cap, AdjBufs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t at = (size_t)t * n + i;
+  const size_t cbase = (size_t)t * cap * n;
+  const int io = tp.perm[at];
+  a.gx[io] = a.ix[i];
+  a.gv[io] = a.iv[i];
+  a.gw[io] = a.iw[i];
+#pragma unroll
+  for (int q = 0; q < kWallSlots; ++q) a.gW[(size_t)q * n + io] = a.iW[(size_t)q * n + i];
+  const uint32_t cnt = tp.cnt[at];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t d = cbase + (size_t)k * n + i;
+    const uint8_t s = tp.src[d];
+    if (s != 0xffu) a.gH[(size_t)s * n + io] = a.iH[d];
+  }
+}
+
+inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+void adj_launch_snap(const EnsTape& tp, int t, const EnsBufs& b, int cur, int n,
+                     const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
+                     cudaStream_t st) {
+  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, t, b, b.S[cur], b.S[2], n, ctl, rebuilt, perm);
+}
+
+void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,
+                     const AdjBufs& a, cudaStream_t st) {
+  k_adj_pre<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, a);
+  k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, cap, a);
+}
+
+void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,
+                       cudaStream_t st) {
+  k_adj_unsort<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
+}
+
+}  // namespace blaze

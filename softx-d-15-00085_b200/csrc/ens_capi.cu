@@ -10,6 +10,7 @@
 
 #include "blaze_dem.h"
 #include "blaze_ens.h"
+#include "ens_adjoint.cuh"
 #include "ens_kernels.cuh"
 #include "radix_sort.cuh"
 
@@ -197,7 +198,7 @@ void free_ens(blaze_ens* e) {
   for (int k = 0; k < 2; ++k) {
     f(e->b.pid[k]); f(e->b.wh[k]);
     f(e->b.L[k].idx); f(e->b.L[k].cnt); f(e->b.L[k].mask);
-    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz);
+    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz); f(e->b.L[k].src);
     f(e->rs.keys[k]); f(e->rs.vals[k]);
   }
   f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
@@ -383,6 +384,7 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
     CKF(dalloc(&e->b.L[k].hx, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].hy, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].hz, (size_t)cap * n));
+    CKF(dalloc(&e->b.L[k].src, (size_t)cap * n));
     CKF(dalloc(&e->rs.keys[k], n));
     CKF(dalloc(&e->rs.vals[k], n));
     CKF(cudaMemset(e->b.L[k].cnt, 0, sizeof(uint32_t) * n));
@@ -624,5 +626,277 @@ int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4,
 int blaze_ens_last_launches(blaze_ens* e) { return e ? e->last_launches : -1; }
 
 int blaze_ens_rebuild_kernels(blaze_ens* e) { return e ? rebuild_kernel_count(e) : -1; }
+
+}  // extern "C"
+
+// ============================================================ reverse mode
+struct EnsCheckpoint {
+  float4* pos = nullptr;
+  float4* vel = nullptr;
+  float4* angv = nullptr;
+  int* pid = nullptr;
+  uint32_t* idx = nullptr;
+  uint32_t* cnt = nullptr;
+  uint32_t* mask = nullptr;
+  float* hx = nullptr;
+  float* hy = nullptr;
+  float* hz = nullptr;
+  float4* wh = nullptr;
+  StepCtl ctl{};
+  int cur = 0;
+};
+
+struct blaze_ens_adj {
+  blaze_ens* e = nullptr;
+  int nsteps = 0, K = 0, nseg = 0;
+  EnsTape tape{};
+  std::vector<EnsCheckpoint> ck;
+  AdjBufs A{};
+  std::vector<int> rb;
+  bool forward_done = false;
+};
+
+namespace {
+
+int sort_result(const blaze_ens* e) {
+  const int passes = std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits);
+  return passes & 1;
+}
+
+void free_adj(blaze_ens_adj* a) {
+  if (!a) return;
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  EnsTape& t = a->tape;
+  f(t.rb); f(t.perm); f(t.src); f(t.pos); f(t.vel); f(t.angv); f(t.idx); f(t.cnt); f(t.mask);
+  f(t.hx); f(t.hy); f(t.hz); f(t.wh);
+  for (EnsCheckpoint& c : a->ck) {
+    f(c.pos); f(c.vel); f(c.angv); f(c.pid); f(c.idx); f(c.cnt); f(c.mask); f(c.hx); f(c.hy);
+    f(c.hz); f(c.wh);
+  }
+  AdjBufs& b = a->A;
+  for (float4* q : {b.gx, b.gv, b.gw, b.gH, b.gW, b.ix, b.iv, b.iw, b.iH, b.iW, b.Fb, b.Tb}) f(q);
+  f(b.th);
+  delete a;
+}
+
+int save_checkpoint(blaze_ens_adj* a, EnsCheckpoint& c) {
+  blaze_ens* e = a->e;
+  int rc = sync_status(e);
+  if (rc < 0) return rc;
+  const size_t n = e->n, cn = (size_t)e->opt.max_nbr * n;
+  const int ep = e->h_ctl->epoch & 1;
+  const EnsList& L = e->b.L[ep];
+  cudaStream_t st = e->stream;
+  CK(cudaMemcpyAsync(c.pos, e->b.S[e->cur].pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.vel, e->b.S[e->cur].vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.angv, e->b.S[e->cur].angv, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.pid, e->b.pid[ep], sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.idx, L.idx, sizeof(uint32_t) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.cnt, L.cnt, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.mask, L.mask, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.hx, L.hx, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.hy, L.hy, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.hz, L.hz, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(c.wh, e->b.wh[ep], sizeof(float4) * kWallSlots * n, cudaMemcpyDeviceToDevice, st));
+  c.ctl = *e->h_ctl;
+  c.cur = e->cur;
+  return 0;
+}
+
+int restore_checkpoint(blaze_ens_adj* a, const EnsCheckpoint& c) {
+  blaze_ens* e = a->e;
+  const size_t n = e->n, cn = (size_t)e->opt.max_nbr * n;
+  const int ep = c.ctl.epoch & 1;
+  const EnsList& L = e->b.L[ep];
+  cudaStream_t st = e->stream;
+  e->cur = c.cur;
+  CK(cudaMemcpyAsync(e->b.S[e->cur].pos, c.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(e->b.S[e->cur].vel, c.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(e->b.S[e->cur].angv, c.angv, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(e->b.pid[ep], c.pid, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.idx, c.idx, sizeof(uint32_t) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.cnt, c.cnt, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.mask, c.mask, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.hx, c.hx, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.hy, c.hy, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(L.hz, c.hz, sizeof(float) * cn, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(e->b.wh[ep], c.wh, sizeof(float4) * kWallSlots * n, cudaMemcpyDeviceToDevice, st));
+  *e->h_ctl = c.ctl;
+  CK(cudaMemcpyAsync(e->ctl, e->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+// Steps [s0, s0 + len) recomputed from the restored checkpoint into the tape.
+int record_segment(blaze_ens_adj* a, int len) {
+  blaze_ens* e = a->e;
+  const int res = sort_result(e);
+  for (int t = 0; t < len; ++t) {
+    launch_gate(e->ctl, e->stream);
+    int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
+    if (rc) return rc;
+    adj_launch_snap(a->tape, t, e->b, e->cur, e->n, e->ctl, &e->ctl->rebuilt, e->rs.vals[res],
+                    e->stream);
+    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0}, nullptr,
+                    e->opt.block, e->stream);
+    e->cur ^= 1;
+  }
+  CK(cudaMemcpyAsync(a->rb.data(), a->tape.rb, sizeof(int) * len, cudaMemcpyDeviceToHost, e->stream));
+  int st = sync_status(e);
+  return st < 0 ? st : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment) {
+  if (!out || !e || nsteps < 1 || segment < 1) return -1;
+  if (e->opt.law != BLAZE_LAW_LINEAR) return -1;
+  for (const blaze_system& s : e->sys)
+    if (s.mu_roll > 0.0f || s.ntris > 0) return -1;
+  for (const EnsWallDev& w : e->hwalls)
+    if (w.kind != kWallPlane) return -1;
+  blaze_ens_adj* a = new (std::nothrow) blaze_ens_adj();
+  if (!a) return -1;
+  auto fail = [&](int rc) { free_adj(a); return rc; };
+#define CKA(x) do { cudaError_t e2 = (x); if (e2 != cudaSuccess) return fail(cuda_fail(e2)); } while (0)
+  a->e = e;
+  a->nsteps = nsteps;
+  a->K = std::min(segment, nsteps);
+  a->nseg = (nsteps + a->K - 1) / a->K;
+  const size_t n = e->n, cap = e->opt.max_nbr, K = a->K;
+  EnsTape& t = a->tape;
+  t.K = a->K;
+  CKA(dalloc(&t.rb, K));
+  CKA(dalloc(&t.perm, K * n));
+  CKA(dalloc(&t.src, K * cap * n));
+  CKA(dalloc(&t.pos, K * n));
+  CKA(dalloc(&t.vel, K * n));
+  CKA(dalloc(&t.angv, K * n));
+  CKA(dalloc(&t.idx, K * cap * n));
+  CKA(dalloc(&t.cnt, K * n));
+  CKA(dalloc(&t.mask, K * n));
+  CKA(dalloc(&t.hx, K * cap * n));
+  CKA(dalloc(&t.hy, K * cap * n));
+  CKA(dalloc(&t.hz, K * cap * n));
+  CKA(dalloc(&t.wh, K * kWallSlots * n));
+  a->ck.resize(a->nseg);
+  for (EnsCheckpoint& c : a->ck) {
+    CKA(dalloc(&c.pos, n)); CKA(dalloc(&c.vel, n)); CKA(dalloc(&c.angv, n)); CKA(dalloc(&c.pid, n));
+    CKA(dalloc(&c.idx, cap * n)); CKA(dalloc(&c.cnt, n)); CKA(dalloc(&c.mask, n));
+    CKA(dalloc(&c.hx, cap * n)); CKA(dalloc(&c.hy, cap * n)); CKA(dalloc(&c.hz, cap * n));
+    CKA(dalloc(&c.wh, kWallSlots * n));
+  }
+  AdjBufs& b = a->A;
+  for (float4** q : {&b.gx, &b.gv, &b.gw, &b.ix, &b.iv, &b.iw, &b.Fb, &b.Tb}) CKA(dalloc(q, n));
+  CKA(dalloc(&b.gH, cap * n));
+  CKA(dalloc(&b.iH, cap * n));
+  CKA(dalloc(&b.gW, kWallSlots * n));
+  CKA(dalloc(&b.iW, kWallSlots * n));
+  CKA(dalloc(&b.th, 5 * n));
+  a->rb.assign(a->K, 0);
+#undef CKA
+  *out = a;
+  return 0;
+}
+
+int blaze_ens_adj_forward(blaze_ens_adj* a) {
+  if (!a || !a->e->state_set) return -1;
+  blaze_ens* e = a->e;
+  for (int s = 0; s < a->nsteps; ++s) {
+    if (s % a->K == 0) {
+      int rc = save_checkpoint(a, a->ck[s / a->K]);
+      if (rc) return rc;
+    }
+    int rc = enqueue_step(e);
+    if (rc) return rc;
+  }
+  int st = sync_status(e);
+  if (st < 0) return st;
+  a->forward_done = true;
+  return st;
+}
+
+int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
+                           const float* gavel, float* gpos0, float* gvel0, float* gavel0,
+                           double* gconst) {
+  if (!a || !a->forward_done) return -1;
+  blaze_ens* e = a->e;
+  const size_t n = e->n, cap = e->opt.max_nbr;
+  cudaStream_t st = e->stream;
+  AdjBufs& A = a->A;
+  {
+    std::vector<float4> h(n);
+    const float* src[3] = {gpos, gvel, gavel};
+    float4* dst[3] = {A.gx, A.gv, A.gw};
+    for (int q = 0; q < 3; ++q) {
+      for (size_t i = 0; i < n; ++i)
+        h[i] = src[q] ? make_float4(src[q][3 * i], src[q][3 * i + 1], src[q][3 * i + 2], 0.0f)
+                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      CK(cudaMemcpyAsync(dst[q], h.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  }
+  CK(cudaMemsetAsync(A.gH, 0, sizeof(float4) * cap * n, st));
+  CK(cudaMemsetAsync(A.gW, 0, sizeof(float4) * kWallSlots * n, st));
+  CK(cudaMemsetAsync(A.th, 0, sizeof(float) * 5 * n, st));
+  const EnsGeom g = geom(e);
+  for (int seg = a->nseg - 1; seg >= 0; --seg) {
+    const int len = std::min(a->K, a->nsteps - seg * a->K);
+    int rc = restore_checkpoint(a, a->ck[seg]);
+    if (rc) return rc;
+    rc = record_segment(a, len);
+    if (rc) return rc;
+    for (int t = len - 1; t >= 0; --t) {
+      adj_launch_step(g, a->tape, t, (int)n, (int)cap, A, st);
+      if (a->rb[t]) {
+        CK(cudaMemsetAsync(A.gH, 0, sizeof(float4) * cap * n, st));
+        adj_launch_unsort(a->tape, t, (int)n, (int)cap, A, st);
+      } else {
+        std::swap(A.gx, A.ix);
+        std::swap(A.gv, A.iv);
+        std::swap(A.gw, A.iw);
+        std::swap(A.gH, A.iH);
+        std::swap(A.gW, A.iW);
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  std::vector<float4> h(n);
+  float* outs[3] = {gpos0, gvel0, gavel0};
+  float4* srcs[3] = {A.gx, A.gv, A.gw};
+  for (int q = 0; q < 3; ++q) {
+    if (!outs[q]) continue;
+    CK(cudaMemcpyAsync(h.data(), srcs[q], sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < n; ++i) {
+      outs[q][3 * i] = h[i].x; outs[q][3 * i + 1] = h[i].y; outs[q][3 * i + 2] = h[i].z;
+    }
+  }
+  if (gconst) {
+    std::vector<float> th(5 * n);
+    CK(cudaMemcpyAsync(th.data(), A.th, sizeof(float) * 5 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // positions of system s are [off_s, off_s + n_s) in every order the run
+    // takes: keys sort by system first
+    size_t off = 0;
+    for (int s = 0; s < e->nsys; ++s) {
+      double acc[5] = {0, 0, 0, 0, 0};
+      for (int i = 0; i < e->sys[s].n; ++i)
+        for (int c = 0; c < 5; ++c) acc[c] += th[5 * (off + i) + c];
+      for (int c = 0; c < 5; ++c) gconst[5 * s + c] = acc[c];
+      off += e->sys[s].n;
+    }
+  }
+  return sync_status(e);
+}
+
+int blaze_ens_adj_destroy(blaze_ens_adj* a) {
+  if (!a) return -1;
+  cudaStreamSynchronize(a->e->stream);
+  free_adj(a);
+  return 0;
+}
 
 }  // extern "C"

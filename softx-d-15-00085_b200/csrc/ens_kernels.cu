@@ -263,6 +263,7 @@ k_ens_nlist(EnsGeom g, EnsBufs b, const float4* __restrict__ pos, const float4* 
             if (!(dot3(rel, rel) < lim * lim)) continue;
             if (cnt < (uint32_t)b.cap) {
               Ln.idx[cnt * stride + i] = j;
+              uint8_t from = 0xffu;
               uint32_t mo = mask_o;
               if (mo) {
                 const int pj = pid_new[j];
@@ -277,10 +278,12 @@ k_ens_nlist(EnsGeom g, EnsBufs b, const float4* __restrict__ pos, const float4* 
                     Ln.hy[sn] = Lo.hy[so];
                     Ln.hz[sn] = Lo.hz[so];
                     mask |= 1u << cnt;
+                    from = (uint8_t)ko;
                     break;
                   }
                 }
               }
+              if (Ln.src) Ln.src[cnt * stride + i] = from;
             } else {
               st |= kStatusListOverflow;
             }

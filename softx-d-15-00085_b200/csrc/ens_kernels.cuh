@@ -64,6 +64,7 @@ struct EnsList {        // one copy of the neighbour list + tangential history
   float* hx;
   float* hy;
   float* hz;
+  uint8_t* src;         // per slot: old slot its history came from (0xff none), or null
 };
 
 struct EnsBufs {
