@@ -282,7 +282,8 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   float mu_wb = 0.0f;
   const uint32_t cnt = tp.cnt[at], mask = tp.mask[at];
   for (uint32_t k = 0; k < cnt; ++k) {
-    const size_t d = cbase + (size_t)k * n + i;
+    const size_t d = cbase + (size_t)k * n + i;   // tape entry
+    const size_t sl = (size_t)k * n + i;          // cotangent slot (one step)
     const uint32_t j = tp.idx[d];
     const Body B = body(tp, S, (size_t)t * n + j);
     const float3 rel = A.x - B.x;
@@ -296,7 +297,7 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
       dummy.x = f3(0.0f, 0.0f, 0.0f);
       dummy.v = dummy.x;
       dummy.w = dummy.x;
-      const float3 xib = pair_vjp(S, A, B, xi, g.dt, Fb, Tb, xyz4(a.gH[d]), ab, dummy, th);
+      const float3 xib = pair_vjp(S, A, B, xi, g.dt, Fb, Tb, xyz4(a.gH[sl]), ab, dummy, th);
       if (had) hout = w4(xib);
       // j's contact with i, from j's side
       const size_t jt = (size_t)t * n + j;
@@ -311,11 +312,12 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
         jb.v = jb.x;
         jb.w = jb.x;
         LawBar tj = {0.0f, 0.0f, 0.0f, 0.0f};
-        pair_vjp(S, B, A, xj, g.dt, xyz4(a.Fb[j]), xyz4(a.Tb[j]), xyz4(a.gH[dj]), jb, ab, tj);
+        pair_vjp(S, B, A, xj, g.dt, xyz4(a.Fb[j]), xyz4(a.Tb[j]), xyz4(a.gH[(size_t)q * n + j]),
+                 jb, ab, tj);
         break;
       }
     }
-    a.iH[d] = hout;
+    a.iH[sl] = hout;
   }
   // plane walls, in the forward's order; slot nw of the output history is
   // the nw-th contact, slot q of the input the one with the same wall id
@@ -375,9 +377,8 @@ k_adj_unsort(EnsTape tp, int t, int n, int cap, AdjBufs a) {
   for (int q = 0; q < kWallSlots; ++q) a.gW[(size_t)q * n + io] = a.iW[(size_t)q * n + i];
   const uint32_t cnt = tp.cnt[at];
   for (uint32_t k = 0; k < cnt; ++k) {
-    const size_t d = cbase + (size_t)k * n + i;
-    const uint8_t s = tp.src[d];
-    if (s != 0xffu) a.gH[(size_t)s * n + io] = a.iH[d];
+    const uint8_t s = tp.src[cbase + (size_t)k * n + i];
+    if (s != 0xffu) a.gH[(size_t)s * n + io] = a.iH[(size_t)k * n + i];
   }
 }
 
