@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-ensemble leg (512 box-settling systems)")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the reverse-mode leg (64 x 20,000-sphere calibration ensemble)")
+    ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--batched-steps", type=int, default=2000,
                     help="timed steps of the batched leg (the workload's 2,000 settling steps)")
     return ap.parse_args()
@@ -221,6 +224,69 @@ def batched_leg(steps, warmup):
                           "trials": [[t[0], t[1], round(t[2], 4), t[3]] for t in trials]},
             "sequential_plain_ms_per_step": seq_ms, "vs_sequential_plain": seq_ms / ms,
             "single_samples": [[n_, round(t_, 5)] for n_, t_ in single]}
+
+
+def adjoint_leg(steps, segment=50):
+    """Reverse mode on the calibration ensemble: 64 systems x 20,000 spheres
+    (radii uniform in [0.1, 0.2] cm, seed 4) settling in 5 cm square-base
+    boxes, linear law with tangential history, dt = 1e-5 s.  Timed: the
+    plain forward (CUDA graphs, no tape), the checkpointing forward and the
+    backward (segment recomputation into the tape + reverse kernels) over
+    `steps` steps, each bracketed by CUDA events on the ensemble's stream;
+    the gradient of the calibration loss (bed height + 32-bin side-wall
+    force profile against targets from mu = 0.45, e = 0.55, kn = 8e4)
+    flows through the same reverse sweep."""
+    import torch
+    from blaze import calibrate as CAL
+    from blaze import ensemble as E
+    S, W, p, r = CAL.calibration_ensemble(nsys=64, n=20000, seed=4)
+    n = len(p)
+    plain = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, use_graph=1)
+    plain.set_state(p, r)
+    plain.step(8)
+    plain.sync()
+    stream = torch.cuda.ExternalStream(plain.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    plain.step(steps)
+    b.record(stream)
+    b.synchronize()
+    fwd_ms = a.elapsed_time(b) / steps
+    plain.close()
+    run = CAL.Runner(S, W, p, r, steps, segment)
+    st2 = torch.cuda.ExternalStream(run.ens.device_state()[3])
+    hidden = torch.tensor([[8e4, 0.55, 0.45, 0.45]] * len(S), dtype=torch.float64)
+    v0 = torch.zeros((n, 3), dtype=torch.float64)
+    with torch.no_grad():
+        pos, vel = CAL.EnsembleRun.apply(hidden, v0, run)
+        target = CAL.observables(pos, vel, hidden, S, r)
+    params = torch.tensor([[1e5, 0.5, 0.4, 0.4]] * len(S), dtype=torch.float64,
+                          requires_grad=True)
+    v0 = torch.zeros((n, 3), dtype=torch.float64, requires_grad=True)
+    a.record(st2)
+    pos, vel = CAL.EnsembleRun.apply(params, v0, run)
+    b.record(st2)
+    b.synchronize()
+    ckpt_fwd_ms = a.elapsed_time(b) / steps
+    loss = CAL.loss_fn(pos, vel, params, S, r, target)
+    a.record(st2)
+    loss.backward()
+    b.record(st2)
+    b.synchronize()
+    bwd_ms = a.elapsed_time(b) / steps
+    g = params.grad.numpy()
+    run.close()
+    return {"workload": "64 box-settling systems x 20,000 spheres, linear law + tangential "
+                        "history, dt 1e-5 s; loss: bed height + 32-bin side-wall force profile",
+            "particles": n, "steps": steps, "checkpoint_every": segment,
+            "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": ckpt_fwd_ms,
+            "backward_ms_per_step": bwd_ms,
+            "adjoint_vs_forward": (ckpt_fwd_ms + bwd_ms) / fwd_ms,
+            "backward_vs_forward": bwd_ms / fwd_ms,
+            "loss": float(loss.item()),
+            "mean_grad": {"kn": float(g[:, 0].mean()), "restitution": float(g[:, 1].mean()),
+                          "mu": float(g[:, 2].mean()), "mu_wall": float(g[:, 3].mean())}}
 
 
 def cpu_reference_rate(P, st, seconds, max_steps=None):
@@ -393,6 +459,9 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(args.batched_steps, args.warmup)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(args.adjoint_steps)
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -420,6 +489,7 @@ def main():
             "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
             "reference_mode_value": ref_mode_value,
             "batched": batched,
+            "adjoint": adjoint,
             "status": device.decode_status(status),
         }
         print(json.dumps(line))
