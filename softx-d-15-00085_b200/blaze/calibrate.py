@@ -58,6 +58,16 @@ def calibration_ensemble(nsys=64, n=20000, base=5.0, r_min=0.1, r_max=0.2, rho=2
     return systems, walls, np.concatenate(pos), np.concatenate(rad)
 
 
+def initial_velocity(n, seed=4, spread=30.0, down=50.0):
+    """Initial velocities of a calibration run (cm/s): normal with standard
+    deviation `spread` per component plus `down` towards the floor, so
+    neighbours and walls are hit from the first steps."""
+    rng = np.random.default_rng(seed + 1000)
+    v = rng.normal(scale=spread, size=(n, 3))
+    v[:, 2] -= down
+    return v
+
+
 def with_params(systems, params):
     """Copies of `systems` with (kn, restitution, mu, mu_wall) from the rows
     of `params` (nsys x 4)."""

@@ -27,18 +27,18 @@ def setup():
     hidden = np.array([[8e4, 0.55, 0.45, 0.45]] * 2)
     guess = np.array([[1e5, 0.5, 0.4, 0.4], [1.2e5, 0.6, 0.3, 0.5]])
     run = CAL.Runner(S, W, p, r, T, SEG)
-    v0 = torch.zeros((run.ens.n, 3), dtype=torch.float64)
+    v0 = torch.tensor(CAL.initial_velocity(run.ens.n).astype(np.float32).astype(np.float64))
     with torch.no_grad():
         hp = torch.tensor(hidden)
         pos, vel = CAL.EnsembleRun.apply(hp, v0, run)
         target = CAL.observables(pos, vel, hp, S, r)
-    return S, W, p, r, guess, run, target
+    return S, W, p, r, guess, run, target, v0
 
 
 def test_autograd_matches_restatement(setup):
-    S, W, p, r, guess, run, target = setup
+    S, W, p, r, guess, run, target, vinit = setup
     params = torch.tensor(guess, requires_grad=True)
-    v0 = torch.zeros((run.ens.n, 3), dtype=torch.float64, requires_grad=True)
+    v0 = vinit.clone().requires_grad_(True)
     pos, vel = CAL.EnsembleRun.apply(params, v0, run)
     loss = CAL.loss_fn(pos, vel, params, S, r, target)
     loss.backward()
@@ -49,7 +49,7 @@ def test_autograd_matches_restatement(setup):
     # the same loss through the FP32 restatement
     Sg = CAL.with_params(S, guess)
     o = EnsRestated(Sg, W, E.LAW_LINEAR, 1e-5, 0.02, 32, precision="f32")
-    o.set_state(p, r, np.zeros(p.shape))
+    o.set_state(p, r, vinit.numpy())
     assert o.adj_record(T) == 0
     st = o.state()
     order = np.argsort(st["pid"])
