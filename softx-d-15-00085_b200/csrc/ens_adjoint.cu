@@ -201,10 +201,11 @@ __device__ __forceinline__ Body body(const EnsTape& tp, const EnsSysDev& S, size
 
 // -------------------------------------------------------------- snapshot
 __global__ void __launch_bounds__(kThreads)
-k_adj_snap(EnsTape tp, int t, EnsBufs b, StateBuf plain, StateBuf sorted, int n,
-           const StepCtl* ctl, const int* rebuilt, const int32_t* perm) {
+k_adj_snap(EnsTape tp, int t_arg, const int* slot, EnsBufs b, StateBuf plain, StateBuf sorted,
+           int n, const StepCtl* ctl, const int* rebuilt, const int32_t* perm) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int t = slot ? *slot : t_arg;
   const int flag = *rebuilt != 0;
   const int e = ctl->epoch & 1;
   const StateBuf in = flag ? sorted : plain;
@@ -260,11 +261,11 @@ k_adj_pre(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   a.iw[i] = w4(gw);
 }
 
-// Contacts backwards.  Particle i collects (1) the reverse of its own
-// contacts (its state, its histories, the law constants) and (2) for each
-// neighbour j in contact, the part of j's contact with i that goes to i,
-// evaluated from j's side with j's force/torque/history cotangents.
-__global__ void __launch_bounds__(kThreads)
+// Contacts backwards.  Particle i evaluates the reverse of each of its own
+// contacts once: its state, history and law-constant cotangents are kept,
+// the share that goes to the neighbour is left in the slot (px, pv, pw) for
+// k_adj_gather to collect.
+__global__ void __launch_bounds__(kThreads, 4)
 k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -293,29 +294,15 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
     if (d2 < sr * sr && sqrtf(d2) > 0.0f) {
       const bool had = (mask >> k) & 1u;
       const float3 xi = had ? f3(tp.hx[d], tp.hy[d], tp.hz[d]) : f3(0.0f, 0.0f, 0.0f);
-      SBar dummy;
-      dummy.x = f3(0.0f, 0.0f, 0.0f);
-      dummy.v = dummy.x;
-      dummy.w = dummy.x;
-      const float3 xib = pair_vjp(S, A, B, xi, g.dt, Fb, Tb, xyz4(a.gH[sl]), ab, dummy, th);
+      SBar bb;
+      bb.x = f3(0.0f, 0.0f, 0.0f);
+      bb.v = bb.x;
+      bb.w = bb.x;
+      const float3 xib = pair_vjp(S, A, B, xi, g.dt, Fb, Tb, xyz4(a.gH[sl]), ab, bb, th);
       if (had) hout = w4(xib);
-      // j's contact with i, from j's side
-      const size_t jt = (size_t)t * n + j;
-      const uint32_t cj = tp.cnt[jt], mj = tp.mask[jt];
-      for (uint32_t q = 0; q < cj; ++q) {
-        const size_t dj = cbase + (size_t)q * n + j;
-        if (tp.idx[dj] != (uint32_t)i) continue;
-        const float3 xj = ((mj >> q) & 1u) ? f3(tp.hx[dj], tp.hy[dj], tp.hz[dj])
-                                           : f3(0.0f, 0.0f, 0.0f);
-        SBar jb;
-        jb.x = f3(0.0f, 0.0f, 0.0f);
-        jb.v = jb.x;
-        jb.w = jb.x;
-        LawBar tj = {0.0f, 0.0f, 0.0f, 0.0f};
-        pair_vjp(S, B, A, xj, g.dt, xyz4(a.Fb[j]), xyz4(a.Tb[j]), xyz4(a.gH[(size_t)q * n + j]),
-                 jb, ab, tj);
-        break;
-      }
+      a.px[sl] = w4(bb.x);
+      a.pv[sl] = w4(bb.v);
+      a.pw[sl] = w4(bb.w);
     }
     a.iH[sl] = hout;
   }
@@ -361,6 +348,41 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   tr[4] += mu_wb;
 }
 
+// Particle i collects, for each neighbour j in contact, the share of j's
+// contact with i that k_adj_pair left in j's slot for i.
+__global__ void __launch_bounds__(kThreads)
+k_adj_gather(EnsTape tp, int t, int n, int cap, AdjBufs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t at = (size_t)t * n + i;
+  const size_t cbase = (size_t)t * cap * n;
+  const float4 pa = tp.pos[at];
+  const float3 xa = xyz4(pa);
+  float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
+  const uint32_t cnt = tp.cnt[at];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t j = tp.idx[cbase + (size_t)k * n + i];
+    const size_t jt = (size_t)t * n + j;
+    const float4 pb = tp.pos[jt];
+    const float3 rel = xa - xyz4(pb);
+    const float sr = pa.w + pb.w;
+    const float d2 = dot3(rel, rel);
+    if (!(d2 < sr * sr && sqrtf(d2) > 0.0f)) continue;
+    const uint32_t cj = tp.cnt[jt];
+    for (uint32_t q = 0; q < cj; ++q) {
+      if (tp.idx[cbase + (size_t)q * n + j] != (uint32_t)i) continue;
+      const size_t sj = (size_t)q * n + j;
+      gx = gx + xyz4(a.px[sj]);
+      gv = gv + xyz4(a.pv[sj]);
+      gw = gw + xyz4(a.pw[sj]);
+      break;
+    }
+  }
+  a.ix[i] = w4(xyz4(a.ix[i]) + gx);
+  a.iv[i] = w4(xyz4(a.iv[i]) + gv);
+  a.iw[i] = w4(xyz4(a.iw[i]) + gw);
+}
+
 // A re-sort backwards: cotangents go to the old positions and, for carried
 // histories, to the old slots (the caller zeroes gH first).
 __global__ void __launch_bounds__(kThreads)
@@ -382,6 +404,8 @@ k_adj_unsort(EnsTape tp, int t, int n, int cap, AdjBufs a) {
   }
 }
 
+__global__ void k_adj_slot_next(int* slot) { *slot += 1; }
+
 inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
@@ -389,13 +413,23 @@ inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 void adj_launch_snap(const EnsTape& tp, int t, const EnsBufs& b, int cur, int n,
                      const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
                      cudaStream_t st) {
-  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, t, b, b.S[cur], b.S[2], n, ctl, rebuilt, perm);
+  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, t, nullptr, b, b.S[cur], b.S[2], n, ctl,
+                                            rebuilt, perm);
+}
+
+void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cur, int n,
+                          const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
+                          cudaStream_t st) {
+  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, 0, slot, b, b.S[cur], b.S[2], n, ctl, rebuilt,
+                                            perm);
+  k_adj_slot_next<<<1, 1, 0, st>>>(slot);
 }
 
 void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,
                      const AdjBufs& a, cudaStream_t st) {
   k_adj_pre<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, a);
   k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, cap, a);
+  k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
 }
 
 void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,

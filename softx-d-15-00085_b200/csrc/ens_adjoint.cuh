@@ -49,6 +49,9 @@ struct AdjBufs {        // cotangents, all in the memory order of the step they 
   float4* iW;
   float4* Fb;           // per particle: cotangent of its force and torque
   float4* Tb;
+  float4* px;           // per list slot (cap x n): the share of a contact's
+  float4* pv;           // cotangent that goes to the neighbour's state
+  float4* pw;
   float* th;            // per position: kn, kt, 2 beta, mu, mu_wall cotangents (n x 5)
 };
 
@@ -58,6 +61,12 @@ struct AdjBufs {        // cotangents, all in the memory order of the step they 
 void adj_launch_snap(const EnsTape& tp, int t, const EnsBufs& b, int cur, int n,
                      const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
                      cudaStream_t st);
+// The same with the tape step read from *slot on the device, followed by a
+// one-thread kernel that advances *slot (so a captured graph can record into
+// successive tape steps).
+void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cur, int n,
+                          const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
+                          cudaStream_t st);
 // Reverse of tape step t: cotangents after the step (gx..gW) -> before it
 // (ix..iW), law-constant cotangents added to th.
 void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,

@@ -546,12 +546,16 @@ int blaze_ens_get_state(blaze_ens* e, float* pos3, float* radius, float* vel3, f
   return st;
 }
 
-int blaze_ens_step(blaze_ens* e, int nsteps) {
-  if (!e || nsteps < 0 || !e->state_set) return -1;
-  e->last_launches = 0;
+}  // extern "C"
+
+namespace {
+
+// nsteps steps, as kGraphSteps-step CUDA graphs where `graphs` allows (the
+// remainder as plain steps).
+int advance(blaze_ens* e, int nsteps, bool graphs) {
   int done = 0;
   while (done < nsteps) {
-    if (!e->opt.use_graph || nsteps - done < kGraphSteps) {
+    if (!graphs || nsteps - done < kGraphSteps) {
       int rc = enqueue_step(e);
       if (rc) return rc;
       done += 1;
@@ -569,6 +573,16 @@ int blaze_ens_step(blaze_ens* e, int nsteps) {
   }
   CK(cudaGetLastError());
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int blaze_ens_step(blaze_ens* e, int nsteps) {
+  if (!e || nsteps < 0 || !e->state_set) return -1;
+  e->last_launches = 0;
+  return advance(e, nsteps, e->opt.use_graph != 0);
 }
 
 int blaze_ens_sync(blaze_ens* e) {
@@ -654,6 +668,8 @@ struct blaze_ens_adj {
   AdjBufs A{};
   std::vector<int> rb;
   bool forward_done = false;
+  int* d_slot = nullptr;                          // tape step the next snapshot writes
+  cudaGraphExec_t rgraph[2] = {nullptr, nullptr};  // recording graphs, from S[0] / S[1]
 };
 
 namespace {
@@ -674,8 +690,13 @@ void free_adj(blaze_ens_adj* a) {
     f(c.hz); f(c.wh);
   }
   AdjBufs& b = a->A;
-  for (float4* q : {b.gx, b.gv, b.gw, b.gH, b.gW, b.ix, b.iv, b.iw, b.iH, b.iW, b.Fb, b.Tb}) f(q);
+  for (float4* q : {b.gx, b.gv, b.gw, b.gH, b.gW, b.ix, b.iv, b.iw, b.iH, b.iW, b.Fb, b.Tb, b.px,
+                    b.pv, b.pw})
+    f(q);
   f(b.th);
+  f(a->d_slot);
+  for (int c = 0; c < 2; ++c)
+    if (a->rgraph[c]) cudaGraphExecDestroy(a->rgraph[c]);
   delete a;
 }
 
@@ -727,19 +748,88 @@ int restore_checkpoint(blaze_ens_adj* a, const EnsCheckpoint& c) {
   return 0;
 }
 
-// Steps [s0, s0 + len) recomputed from the restored checkpoint into the tape.
+// kGraphSteps recorded steps as one graph from S[c]: the step graph of
+// build_graph with a snapshot into the tape after each step's IF node.
+int build_record_graph(blaze_ens_adj* a, int c) {
+  blaze_ens* e = a->e;
+  const int res = sort_result(e);
+  const int saved = e->cur;
+  e->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h[kGraphSteps];
+  for (int k = 0; k < kGraphSteps; ++k)
+    CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(e->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  launch_gate_graph(e->ctl, h[0], e->d_rb, kGraphSteps, e->stream);
+  for (int k = 0; k < kGraphSteps; ++k) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &capg, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    std::memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h[k];
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(e->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(e->aux, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    CK(cudaMemsetAsync(e->d_rb + k, 0x01, sizeof(int), e->aux));
+    int rc = enqueue_rebuild(e, nullptr, e->aux);
+    cudaGraph_t tmp = nullptr;
+    CK(cudaStreamEndCapture(e->aux, &tmp));
+    if (rc) return rc;
+    adj_launch_snap_slot(a->tape, a->d_slot, e->b, e->cur, e->n, e->ctl, e->d_rb + k,
+                         e->rs.vals[res], e->stream);
+    const StepLink link = k + 1 < kGraphSteps ? StepLink{e->d_rb + k, h[k + 1], 1}
+                                               : StepLink{e->d_rb + k, 0, 0};
+    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, nullptr, e->opt.block, e->stream);
+    e->cur ^= 1;
+  }
+  cudaGraph_t out = nullptr;
+  CK(cudaStreamEndCapture(e->stream, &out));
+  CK(cudaGraphInstantiate(&a->rgraph[c], out, 0));
+  CK(cudaGraphDestroy(out));
+  e->cur = saved;
+  return 0;
+}
+
+// Steps [s0, s0 + len) recomputed from the restored checkpoint into the tape
+// (as recording graphs, the remainder as plain steps).
 int record_segment(blaze_ens_adj* a, int len) {
   blaze_ens* e = a->e;
   const int res = sort_result(e);
-  for (int t = 0; t < len; ++t) {
+  CK(cudaMemsetAsync(a->d_slot, 0, sizeof(int), e->stream));
+  int t = 0;
+  while (t < len) {
+    if (len - t >= kGraphSteps) {
+      const int c = e->cur;
+      if (!a->rgraph[c]) {
+        int rc = build_record_graph(a, c);
+        if (rc) return rc;
+      }
+      CK(cudaGraphLaunch(a->rgraph[c], e->stream));
+      if (kGraphSteps & 1) e->cur ^= 1;
+      t += kGraphSteps;
+      continue;
+    }
     launch_gate(e->ctl, e->stream);
     int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
     if (rc) return rc;
-    adj_launch_snap(a->tape, t, e->b, e->cur, e->n, e->ctl, &e->ctl->rebuilt, e->rs.vals[res],
-                    e->stream);
+    adj_launch_snap_slot(a->tape, a->d_slot, e->b, e->cur, e->n, e->ctl, &e->ctl->rebuilt,
+                         e->rs.vals[res], e->stream);
     ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0}, nullptr,
                     e->opt.block, e->stream);
     e->cur ^= 1;
+    ++t;
   }
   CK(cudaMemcpyAsync(a->rb.data(), a->tape.rb, sizeof(int) * len, cudaMemcpyDeviceToHost, e->stream));
   int st = sync_status(e);
@@ -790,11 +880,15 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
   }
   AdjBufs& b = a->A;
   for (float4** q : {&b.gx, &b.gv, &b.gw, &b.ix, &b.iv, &b.iw, &b.Fb, &b.Tb}) CKA(dalloc(q, n));
+  CKA(dalloc(&b.px, cap * n));
+  CKA(dalloc(&b.pv, cap * n));
+  CKA(dalloc(&b.pw, cap * n));
   CKA(dalloc(&b.gH, cap * n));
   CKA(dalloc(&b.iH, cap * n));
   CKA(dalloc(&b.gW, kWallSlots * n));
   CKA(dalloc(&b.iW, kWallSlots * n));
   CKA(dalloc(&b.th, 5 * n));
+  CKA(dalloc(&a->d_slot, 1));
   a->rb.assign(a->K, 0);
 #undef CKA
   *out = a;
@@ -804,12 +898,13 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
 int blaze_ens_adj_forward(blaze_ens_adj* a) {
   if (!a || !a->e->state_set) return -1;
   blaze_ens* e = a->e;
-  for (int s = 0; s < a->nsteps; ++s) {
-    if (s % a->K == 0) {
-      int rc = save_checkpoint(a, a->ck[s / a->K]);
-      if (rc) return rc;
-    }
-    int rc = enqueue_step(e);
+  // between checkpoints the steps run as CUDA graphs: graph and plain
+  // stepping give the same results, so the backward's plain recomputation
+  // reproduces this run exactly
+  for (int seg = 0; seg < a->nseg; ++seg) {
+    int rc = save_checkpoint(a, a->ck[seg]);
+    if (rc) return rc;
+    rc = advance(e, std::min(a->K, a->nsteps - seg * a->K), true);
     if (rc) return rc;
   }
   int st = sync_status(e);
