@@ -230,62 +230,75 @@ def adjoint_leg(steps, segment=50):
     """Reverse mode on the calibration ensemble: 64 systems x 20,000 spheres
     (radii uniform in [0.1, 0.2] cm, seed 4) settling in 5 cm square-base
     boxes, linear law with tangential history, dt = 1e-5 s, seeded initial
-    velocities (30 cm/s spread, 50 cm/s down) so contacts start at once.  Timed: the
-    plain forward (CUDA graphs, no tape), the checkpointing forward and the
-    backward (segment recomputation into the tape + reverse kernels) over
-    `steps` steps, each bracketed by CUDA events on the ensemble's stream;
-    the gradient of the calibration loss (bed height + 32-bin side-wall
-    force profile against targets from mu = 0.45, e = 0.55, kn = 8e4)
-    flows through the same reverse sweep."""
+    velocities (30 cm/s spread, 50 cm/s down) so contacts start at once.
+    Timed with CUDA events on the ensemble's stream over `steps` steps: the
+    plain forward (CUDA graphs, no tape), the checkpointing forward
+    (blaze_ens_adj_forward) and the backward (blaze_ens_adj_backward:
+    segment recomputation into the tape + reverse kernels), with the
+    cotangents of the calibration loss (bed height + 32-bin side-wall force
+    profile against targets from mu = 0.45, e = 0.55, kn = 8e4) already on
+    the host.  The whole autograd call (torch conversions included) is
+    reported beside it."""
     import torch
     from blaze import calibrate as CAL
     from blaze import ensemble as E
     S, W, p, r = CAL.calibration_ensemble(nsys=64, n=20000, seed=4)
     n = len(p)
-    plain = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, use_graph=1)
-    plain.set_state(p, r, CAL.initial_velocity(n))
-    plain.step(8)
-    plain.sync()
-    stream = torch.cuda.ExternalStream(plain.device_state()[3])
+    vinit = CAL.initial_velocity(n).astype(np.float32)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    plain.step(steps)
-    b.record(stream)
-    b.synchronize()
-    fwd_ms = a.elapsed_time(b) / steps
+
+    def timed(stream, fn):
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b), out
+
+    plain = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, use_graph=1)
+    plain.set_state(p, r, vinit)
+    plain.step(8)
+    plain.sync()
+    st1 = torch.cuda.ExternalStream(plain.device_state()[3])
+    fwd_ms = timed(st1, lambda: plain.step(steps))[0] / steps
     plain.close()
     run = CAL.Runner(S, W, p, r, steps, segment)
     st2 = torch.cuda.ExternalStream(run.ens.device_state()[3])
+    vt = torch.tensor(vinit.astype(np.float64))
     hidden = torch.tensor([[8e4, 0.55, 0.45, 0.45]] * len(S), dtype=torch.float64)
-    vinit = torch.tensor(CAL.initial_velocity(n).astype(np.float32).astype(np.float64))
-    v0 = vinit.clone()
     with torch.no_grad():
-        pos, vel = CAL.EnsembleRun.apply(hidden, v0, run)
+        pos, vel = CAL.EnsembleRun.apply(hidden, vt, run)   # also builds the graphs
         target = CAL.observables(pos, vel, hidden, S, r)
-    params = torch.tensor([[1e5, 0.5, 0.4, 0.4]] * len(S), dtype=torch.float64,
-                          requires_grad=True)
-    v0 = vinit.clone().requires_grad_(True)
-    a.record(st2)
+    guess = np.array([[1e5, 0.5, 0.4, 0.4]] * len(S))
+    params = torch.tensor(guess, requires_grad=True)
+    v0 = vt.clone().requires_grad_(True)
+    t0 = time.perf_counter()
     pos, vel = CAL.EnsembleRun.apply(params, v0, run)
-    b.record(st2)
-    b.synchronize()
-    ckpt_fwd_ms = a.elapsed_time(b) / steps
     loss = CAL.loss_fn(pos, vel, params, S, r, target)
-    a.record(st2)
     loss.backward()
-    b.record(st2)
-    b.synchronize()
-    bwd_ms = a.elapsed_time(b) / steps
+    autograd_s = time.perf_counter() - t0
     g = params.grad.numpy()
+    # device-side phases alone, same run, cotangents prepared beforehand
+    pos_t = pos.detach().clone().requires_grad_(True)
+    vel_t = vel.detach().clone().requires_grad_(True)
+    CAL.loss_fn(pos_t, vel_t, params.detach(), S, r, target).backward()
+    run.ens.set_params(CAL.with_params(S, guess))
+    run.ens.set_state(p, r, vinit)
+    ck_ms, status = timed(st2, run.adj.forward)
+    pid = run.ens.state()["pid"]
+    gx = pos_t.grad.numpy()[pid].astype(np.float32)
+    gv = vel_t.grad.numpy()[pid].astype(np.float32)
+    bwd_ms = timed(st2, lambda: run.adj.backward(gx, gv, None))[0]
     run.close()
     return {"workload": "64 box-settling systems x 20,000 spheres, linear law + tangential "
                         "history, dt 1e-5 s; loss: bed height + 32-bin side-wall force profile",
-            "particles": n, "steps": steps, "checkpoint_every": segment,
-            "forward_ms_per_step": fwd_ms, "forward_with_checkpoints_ms_per_step": ckpt_fwd_ms,
-            "backward_ms_per_step": bwd_ms,
-            "adjoint_vs_forward": (ckpt_fwd_ms + bwd_ms) / fwd_ms,
-            "backward_vs_forward": bwd_ms / fwd_ms,
+            "particles": n, "steps": steps, "checkpoint_every": segment, "status": status,
+            "forward_ms_per_step": fwd_ms,
+            "forward_with_checkpoints_ms_per_step": ck_ms / steps,
+            "backward_ms_per_step": bwd_ms / steps,
+            "adjoint_vs_forward": (ck_ms + bwd_ms) / steps / fwd_ms,
+            "backward_vs_forward": bwd_ms / steps / fwd_ms,
+            "autograd_call_s": autograd_s,
             "loss": float(loss.item()),
             "mean_grad": {"kn": float(g[:, 0].mean()), "restitution": float(g[:, 1].mean()),
                           "mu": float(g[:, 2].mean()), "mu_wall": float(g[:, 3].mean())}}
