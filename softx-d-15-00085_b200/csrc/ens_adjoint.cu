@@ -226,6 +226,7 @@ k_adj_snap(EnsTape tp, int t_arg, const int* slot, EnsBufs b, StateBuf plain, St
     tp.hx[d] = L.hx[s];
     tp.hy[d] = L.hy[s];
     tp.hz[d] = L.hz[s];
+    tp.twin[d] = L.twin[s];
     if (flag) tp.src[d] = L.src[s];
   }
   if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
@@ -238,33 +239,31 @@ k_adj_snap(EnsTape tp, int t_arg, const int* slot, EnsBufs b, StateBuf plain, St
 }
 
 // --------------------------------------------------------------- reverse
-// Symplectic Euler backwards: cotangents of the step's force and torque, and
-// the state cotangents before the step that do not go through the forces.
+// Twin slots of the current list (reverse mode only): slot k of particle i
+// holds neighbour j; twin[k][i] is the slot of j's list that holds i.
 __global__ void __launch_bounds__(kThreads)
-k_adj_pre(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
+k_adj_twin(EnsBufs b, int n, const StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const size_t at = (size_t)t * n + i;
-  const float4 p = tp.pos[at];
-  const uint32_t sys = __float_as_uint(tp.vel[at].w) & kSysMask;
-  const EnsSysDev& S = g.sys[sys];
-  const float r = p.w;
-  const float m = S.dens43pi * ((r * r) * r);
-  const float inertia = (0.4f * m) * (r * r);
-  const float3 gx = xyz4(a.gx[i]);
-  const float3 gv = xyz4(a.gv[i]) + gx * g.dt;
-  const float3 gw = xyz4(a.gw[i]);
-  a.Fb[i] = w4(gv * (g.dt / m));
-  a.Tb[i] = w4(gw * (g.dt / inertia));
-  a.ix[i] = w4(gx);
-  a.iv[i] = w4(gv);
-  a.iw[i] = w4(gw);
+  const EnsList L = b.L[ctl->epoch & 1];
+  const size_t stride = (size_t)b.stride;
+  const uint32_t cnt = L.cnt[i];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t j = L.idx[(size_t)k * stride + i];
+    const uint32_t cj = L.cnt[j];
+    uint8_t tw = 0xffu;
+    for (uint32_t q = 0; q < cj; ++q)
+      if (L.idx[(size_t)q * stride + j] == (uint32_t)i) { tw = (uint8_t)q; break; }
+    L.twin[(size_t)k * stride + i] = tw;
+  }
 }
 
-// Contacts backwards.  Particle i evaluates the reverse of each of its own
-// contacts once: its state, history and law-constant cotangents are kept,
-// the share that goes to the neighbour is left in the slot (px, pv, pw) for
-// k_adj_gather to collect.
+// The step backwards, per particle: symplectic Euler (v' = v + (f/m + g) dt,
+// x' = x + v' dt, w' = w + t/I dt) gives the cotangents of the particle's
+// force and torque; then the reverse of each of its own contacts, once: its
+// state, history and law-constant cotangents are kept, the share that goes
+// to the neighbour is left in the slot (px, pv, pw) for k_adj_gather.
 __global__ void __launch_bounds__(kThreads, 4)
 k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,11 +273,12 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   const uint32_t bits = __float_as_uint(tp.vel[at].w);
   const EnsSysDev& S = g.sys[bits & kSysMask];
   const Body A = body(tp, S, at);
-  const float3 Fb = xyz4(a.Fb[i]), Tb = xyz4(a.Tb[i]);
+  const float inertia = (0.4f * A.m) * (A.r * A.r);
   SBar ab;
-  ab.x = f3(0.0f, 0.0f, 0.0f);
-  ab.v = ab.x;
-  ab.w = ab.x;
+  ab.x = xyz4(a.gx[i]);
+  ab.v = xyz4(a.gv[i]) + ab.x * g.dt;
+  ab.w = xyz4(a.gw[i]);
+  const float3 Fb = ab.v * (g.dt / A.m), Tb = ab.w * (g.dt / inertia);
   LawBar th = {0.0f, 0.0f, 0.0f, 0.0f};
   float mu_wb = 0.0f;
   const uint32_t cnt = tp.cnt[at], mask = tp.mask[at];
@@ -337,9 +337,9 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   }
 #pragma unroll
   for (int q = 0; q < kWallSlots; ++q) a.iW[(size_t)q * n + i] = win[q];
-  a.ix[i] = w4(xyz4(a.ix[i]) + ab.x);
-  a.iv[i] = w4(xyz4(a.iv[i]) + ab.v);
-  a.iw[i] = w4(xyz4(a.iw[i]) + ab.w);
+  a.ix[i] = w4(ab.x);
+  a.iv[i] = w4(ab.v);
+  a.iw[i] = w4(ab.w);
   float* tr = a.th + (size_t)5 * i;
   tr[0] += th.kn;
   tr[1] += th.kt;
@@ -368,15 +368,12 @@ k_adj_gather(EnsTape tp, int t, int n, int cap, AdjBufs a) {
     const float sr = pa.w + pb.w;
     const float d2 = dot3(rel, rel);
     if (!(d2 < sr * sr && sqrtf(d2) > 0.0f)) continue;
-    const uint32_t cj = tp.cnt[jt];
-    for (uint32_t q = 0; q < cj; ++q) {
-      if (tp.idx[cbase + (size_t)q * n + j] != (uint32_t)i) continue;
-      const size_t sj = (size_t)q * n + j;
-      gx = gx + xyz4(a.px[sj]);
-      gv = gv + xyz4(a.pv[sj]);
-      gw = gw + xyz4(a.pw[sj]);
-      break;
-    }
+    const uint8_t q = tp.twin[cbase + (size_t)k * n + i];
+    if (q == 0xffu) continue;
+    const size_t sj = (size_t)q * n + j;
+    gx = gx + xyz4(a.px[sj]);
+    gv = gv + xyz4(a.pv[sj]);
+    gw = gw + xyz4(a.pw[sj]);
   }
   a.ix[i] = w4(xyz4(a.ix[i]) + gx);
   a.iv[i] = w4(xyz4(a.iv[i]) + gv);
@@ -427,9 +424,13 @@ void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cu
 
 void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,
                      const AdjBufs& a, cudaStream_t st) {
-  k_adj_pre<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, a);
   k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, cap, a);
   k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
+}
+
+void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gate,
+                     cudaStream_t st) {
+  k_adj_twin<<<nblk(n), kThreads, 0, st>>>(b, n, ctl, gate);
 }
 
 void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,

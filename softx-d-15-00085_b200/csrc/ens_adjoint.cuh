@@ -34,6 +34,7 @@ struct EnsTape {
   float* hy;
   float* hz;
   float4* wh;           // per step, kWallSlots x n: wall histories before the step
+  uint8_t* twin;        // per step, cap x n: the neighbour's slot for this particle
 };
 
 struct AdjBufs {        // cotangents, all in the memory order of the step they belong to
@@ -47,7 +48,7 @@ struct AdjBufs {        // cotangents, all in the memory order of the step they 
   float4* iw;
   float4* iH;
   float4* iW;
-  float4* Fb;           // per particle: cotangent of its force and torque
+  float4* Fb;           // (unused: the force and torque cotangents stay in registers)
   float4* Tb;
   float4* px;           // per list slot (cap x n): the share of a contact's
   float4* pv;           // cotangent that goes to the neighbour's state
@@ -67,6 +68,11 @@ void adj_launch_snap(const EnsTape& tp, int t, const EnsBufs& b, int cur, int n,
 void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cur, int n,
                           const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
                           cudaStream_t st);
+// For every slot of the current list, the neighbour's slot that holds this
+// particle (0xff if the neighbour's list overflowed); `gate` as in the
+// re-sort kernels.
+void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gate,
+                     cudaStream_t st);
 // Reverse of tape step t: cotangents after the step (gx..gW) -> before it
 // (ix..iW), law-constant cotangents added to th.
 void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,

@@ -198,7 +198,7 @@ void free_ens(blaze_ens* e) {
   for (int k = 0; k < 2; ++k) {
     f(e->b.pid[k]); f(e->b.wh[k]);
     f(e->b.L[k].idx); f(e->b.L[k].cnt); f(e->b.L[k].mask);
-    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz); f(e->b.L[k].src);
+    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz); f(e->b.L[k].src); f(e->b.L[k].twin);
     f(e->rs.keys[k]); f(e->rs.vals[k]);
   }
   f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
@@ -385,6 +385,7 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
     CKF(dalloc(&e->b.L[k].hy, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].hz, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].src, (size_t)cap * n));
+    CKF(dalloc(&e->b.L[k].twin, (size_t)cap * n));
     CKF(dalloc(&e->rs.keys[k], n));
     CKF(dalloc(&e->rs.vals[k], n));
     CKF(cudaMemset(e->b.L[k].cnt, 0, sizeof(uint32_t) * n));
@@ -684,7 +685,7 @@ void free_adj(blaze_ens_adj* a) {
   auto f = [](void* p) { if (p) cudaFree(p); };
   EnsTape& t = a->tape;
   f(t.rb); f(t.perm); f(t.src); f(t.pos); f(t.vel); f(t.angv); f(t.idx); f(t.cnt); f(t.mask);
-  f(t.hx); f(t.hy); f(t.hz); f(t.wh);
+  f(t.hx); f(t.hy); f(t.hz); f(t.wh); f(t.twin);
   for (EnsCheckpoint& c : a->ck) {
     f(c.pos); f(c.vel); f(c.angv); f(c.pid); f(c.idx); f(c.cnt); f(c.mask); f(c.hx); f(c.hy);
     f(c.hz); f(c.wh);
@@ -784,6 +785,7 @@ int build_record_graph(blaze_ens_adj* a, int c) {
                                      cudaStreamCaptureModeThreadLocal));
     CK(cudaMemsetAsync(e->d_rb + k, 0x01, sizeof(int), e->aux));
     int rc = enqueue_rebuild(e, nullptr, e->aux);
+    adj_launch_twin(e->b, e->n, e->ctl, nullptr, e->aux);
     cudaGraph_t tmp = nullptr;
     CK(cudaStreamEndCapture(e->aux, &tmp));
     if (rc) return rc;
@@ -808,6 +810,7 @@ int record_segment(blaze_ens_adj* a, int len) {
   blaze_ens* e = a->e;
   const int res = sort_result(e);
   CK(cudaMemsetAsync(a->d_slot, 0, sizeof(int), e->stream));
+  adj_launch_twin(e->b, e->n, e->ctl, nullptr, e->stream);   // the restored list
   int t = 0;
   while (t < len) {
     if (len - t >= kGraphSteps) {
@@ -824,6 +827,7 @@ int record_segment(blaze_ens_adj* a, int len) {
     launch_gate(e->ctl, e->stream);
     int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
     if (rc) return rc;
+    adj_launch_twin(e->b, e->n, e->ctl, &e->ctl->rebuilt, e->stream);
     adj_launch_snap_slot(a->tape, a->d_slot, e->b, e->cur, e->n, e->ctl, &e->ctl->rebuilt,
                          e->rs.vals[res], e->stream);
     ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0}, nullptr,
@@ -871,6 +875,7 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
   CKA(dalloc(&t.hy, K * cap * n));
   CKA(dalloc(&t.hz, K * cap * n));
   CKA(dalloc(&t.wh, K * kWallSlots * n));
+  CKA(dalloc(&t.twin, K * cap * n));
   a->ck.resize(a->nseg);
   for (EnsCheckpoint& c : a->ck) {
     CKA(dalloc(&c.pos, n)); CKA(dalloc(&c.vel, n)); CKA(dalloc(&c.angv, n)); CKA(dalloc(&c.pid, n));
@@ -879,7 +884,7 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
     CKA(dalloc(&c.wh, kWallSlots * n));
   }
   AdjBufs& b = a->A;
-  for (float4** q : {&b.gx, &b.gv, &b.gw, &b.ix, &b.iv, &b.iw, &b.Fb, &b.Tb}) CKA(dalloc(q, n));
+  for (float4** q : {&b.gx, &b.gv, &b.gw, &b.ix, &b.iv, &b.iw}) CKA(dalloc(q, n));
   CKA(dalloc(&b.px, cap * n));
   CKA(dalloc(&b.pv, cap * n));
   CKA(dalloc(&b.pw, cap * n));

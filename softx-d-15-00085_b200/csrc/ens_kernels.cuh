@@ -65,6 +65,7 @@ struct EnsList {        // one copy of the neighbour list + tangential history
   float* hy;
   float* hz;
   uint8_t* src;         // per slot: old slot its history came from (0xff none), or null
+  uint8_t* twin;        // per slot: the neighbour's slot for this particle (reverse mode)
 };
 
 struct EnsBufs {
