@@ -217,17 +217,25 @@ k_adj_snap(EnsTape tp, int t_arg, const int* slot, EnsBufs b, StateBuf plain, St
   tp.angv[base] = in.angv[i];
   const EnsList L = b.L[e];
   const uint32_t c = L.cnt[i];
-  tp.cnt[base] = c;
-  tp.mask[base] = L.mask[i];
+  const uint32_t mask = L.mask[i];
+  tp.mask[base] = mask;
+  // the list (indices, twins, count) only where it changed: a re-sort step
+  // or the first step of the tape; histories only where they are active
+  const bool list_step = flag || t == 0;
+  if (list_step) tp.cnt[base] = c;
   for (uint32_t k = 0; k < c; ++k) {
     const size_t s = (size_t)k * b.stride + i;
     const size_t d = cbase + (size_t)k * n + i;
-    tp.idx[d] = L.idx[s];
-    tp.hx[d] = L.hx[s];
-    tp.hy[d] = L.hy[s];
-    tp.hz[d] = L.hz[s];
-    tp.twin[d] = L.twin[s];
-    if (flag) tp.src[d] = L.src[s];
+    if (list_step) {
+      tp.idx[d] = L.idx[s];
+      tp.twin[d] = L.twin[s];
+      if (flag) tp.src[d] = L.src[s];
+    }
+    if ((mask >> k) & 1u) {
+      tp.hx[d] = L.hx[s];
+      tp.hy[d] = L.hy[s];
+      tp.hz[d] = L.hz[s];
+    }
   }
   if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
 #pragma unroll
@@ -265,11 +273,12 @@ k_adj_twin(EnsBufs b, int n, const StepCtl* ctl, const int* gate) {
 // state, history and law-constant cotangents are kept, the share that goes
 // to the neighbour is left in the slot (px, pv, pw) for k_adj_gather.
 __global__ void __launch_bounds__(kThreads, 4)
-k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
+k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t at = (size_t)t * n + i;
-  const size_t cbase = (size_t)t * cap * n;
+  const size_t cbase = (size_t)t * cap * n;      // histories of step t
+  const size_t lbase = (size_t)tl * cap * n;     // the list step t used
   const uint32_t bits = __float_as_uint(tp.vel[at].w);
   const EnsSysDev& S = g.sys[bits & kSysMask];
   const Body A = body(tp, S, at);
@@ -281,11 +290,11 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
   const float3 Fb = ab.v * (g.dt / A.m), Tb = ab.w * (g.dt / inertia);
   LawBar th = {0.0f, 0.0f, 0.0f, 0.0f};
   float mu_wb = 0.0f;
-  const uint32_t cnt = tp.cnt[at], mask = tp.mask[at];
+  const uint32_t cnt = tp.cnt[(size_t)tl * n + i], mask = tp.mask[at];
   for (uint32_t k = 0; k < cnt; ++k) {
-    const size_t d = cbase + (size_t)k * n + i;   // tape entry
+    const size_t d = cbase + (size_t)k * n + i;   // tape history entry
     const size_t sl = (size_t)k * n + i;          // cotangent slot (one step)
-    const uint32_t j = tp.idx[d];
+    const uint32_t j = tp.idx[lbase + (size_t)k * n + i];
     const Body B = body(tp, S, (size_t)t * n + j);
     const float3 rel = A.x - B.x;
     const float sr = A.r + B.r;
@@ -351,15 +360,15 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, int cap, AdjBufs a) {
 // Particle i collects, for each neighbour j in contact, the share of j's
 // contact with i that k_adj_pair left in j's slot for i.
 __global__ void __launch_bounds__(kThreads)
-k_adj_gather(EnsTape tp, int t, int n, int cap, AdjBufs a) {
+k_adj_gather(EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t at = (size_t)t * n + i;
-  const size_t cbase = (size_t)t * cap * n;
+  const size_t cbase = (size_t)tl * cap * n;     // the list step t used
   const float4 pa = tp.pos[at];
   const float3 xa = xyz4(pa);
   float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
-  const uint32_t cnt = tp.cnt[at];
+  const uint32_t cnt = tp.cnt[(size_t)tl * n + i];
   for (uint32_t k = 0; k < cnt; ++k) {
     const uint32_t j = tp.idx[cbase + (size_t)k * n + i];
     const size_t jt = (size_t)t * n + j;
@@ -422,10 +431,10 @@ void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cu
   k_adj_slot_next<<<1, 1, 0, st>>>(slot);
 }
 
-void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,
+void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int tl, int n, int cap,
                      const AdjBufs& a, cudaStream_t st) {
-  k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, cap, a);
-  k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
+  k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, tl, n, cap, a);
+  k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, tl, n, cap, a);
 }
 
 void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gate,

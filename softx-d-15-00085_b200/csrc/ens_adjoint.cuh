@@ -73,9 +73,10 @@ void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cu
 // re-sort kernels.
 void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gate,
                      cudaStream_t st);
-// Reverse of tape step t: cotangents after the step (gx..gW) -> before it
-// (ix..iW), law-constant cotangents added to th.
-void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, int cap,
+// Reverse of tape step t, which used the list stored at tape step tl (the
+// last re-sort step <= t, or the tape's first step): cotangents after the
+// step (gx..gW) -> before it (ix..iW), law-constant cotangents added to th.
+void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int tl, int n, int cap,
                      const AdjBufs& a, cudaStream_t st);
 // Reverse of the re-sort of tape step t: cotangents before the step (ix..iW,
 // sorted order) -> after the previous step (gx..gW, order before the sort).

@@ -948,8 +948,10 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
     if (rc) return rc;
     rc = record_segment(a, len);
     if (rc) return rc;
+    std::vector<int> list_at(len, 0);   // tape step holding the list step t used
+    for (int t = 1; t < len; ++t) list_at[t] = a->rb[t] ? t : list_at[t - 1];
     for (int t = len - 1; t >= 0; --t) {
-      adj_launch_step(g, a->tape, t, (int)n, (int)cap, A, st);
+      adj_launch_step(g, a->tape, t, list_at[t], (int)n, (int)cap, A, st);
       if (a->rb[t]) {
         CK(cudaMemsetAsync(A.gH, 0, sizeof(float4) * cap * n, st));
         adj_launch_unsort(a->tape, t, (int)n, (int)cap, A, st);
