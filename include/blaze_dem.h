@@ -11,7 +11,9 @@
  *       >0 StatusBits raised by the kernels since the last call that
  *          synchronised (1 list overflow, 2 particle outside the grid,
  *          4 non-finite state, 8 particle type outside the table,
- *          16 bounded device wait gave up)
+ *          16 bounded device wait gave up, 32 a polyhedron contact met a
+ *          case the reference leaves undefined and got the library's
+ *          defined result)
  *       <0 -(1000 + cudaError_t) for a CUDA error, -1 bad argument,
  *          -2 no simulation set up
  *   - Device_DEM_UpdateSim only enqueues the step on the library's stream;
@@ -109,6 +111,15 @@ int blaze_set_cylinder_rotation(blaze_sim* s, int on);
 int blaze_set_state(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
                     const uint* type, const int* pid);
 int blaze_get_state(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid);
+/* The same with orientations, (w, x, y, z) per particle (Quaterion order;
+ * NULL = identity on set, not returned on get).  Polyhedra (particle_type
+ * 1): positions are set as centres of mass and returned relative to the
+ * object file's origin (pos - COM), as Set_PSystem_State / Get_SystemState
+ * do (GPU_Memory_Transfer.cuh:400-440, 486-520). */
+int blaze_set_state_ornt(blaze_sim* s, const float* pos3, const float* quat4, const float* vel3,
+                         const float* avel3, const uint* type, const int* pid);
+int blaze_get_state_ornt(blaze_sim* s, float* pos3, float* quat4, float* vel3, float* avel3,
+                         uint* type, int* pid);
 /* Enqueue nsteps steps (asynchronous unless sync_each_step). */
 int blaze_step(blaze_sim* s, int nsteps);
 /* Wait for the stream; returns the accumulated status (see Part 1). */

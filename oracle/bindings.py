@@ -11,6 +11,7 @@ product.
 import ctypes as C
 import os
 import shutil
+import subprocess
 import sys
 import tempfile
 
@@ -151,6 +152,35 @@ class RefHost:
         e = np.zeros(3, np.float32)
         self.lib.refh_get_energy(_p(e, C.c_float))
         return e
+
+    @staticmethod
+    def parse_isolated(projects_root, project, world):
+        """The reference's parser in its own sanitizer-built process
+        (oracle/_ref/refparse; polyhedral objects need it, see
+        ref_host/refparse_main.cpp).  Same return values as parse()."""
+        exe = os.path.join(HERE, "_ref", "refparse")
+        tmp = tempfile.mkdtemp(prefix="blaze_refparse_")
+        try:
+            shutil.copytree(os.path.join(projects_root, project),
+                            os.path.join(tmp, "Projects", project))
+            os.makedirs(os.path.join(tmp, "run"))
+            out = os.path.join(tmp, "out.bin")
+            env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0")
+            r = subprocess.run([exe, os.path.join(tmp, "run"), project, world, out],
+                               env=env, capture_output=True, text=True, timeout=120)
+            if r.returncode:
+                raise RuntimeError("refparse failed (%d): %s" % (r.returncode, r.stderr[-400:]))
+            raw = open(out, "rb").read()
+            rp = RefProject.from_buffer_copy(raw[:C.sizeof(RefProject)])
+            off = C.sizeof(RefProject)
+            w = (T.WOBJ * 8).from_buffer_copy(raw[off:off + C.sizeof(T.WOBJ * 8)])
+            off += C.sizeof(T.WOBJ * 8)
+            p = (T.POBJ * 8).from_buffer_copy(raw[off:off + C.sizeof(T.POBJ * 8)])
+            off += C.sizeof(T.POBJ * 8)
+            d = (T.DOBJ * 32).from_buffer_copy(raw[off:off + C.sizeof(T.DOBJ * 32)])
+            return rp, w, p, d
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
 
     def parse(self, projects_root, project, world):
         """Parse with the reference's KSimulationData from a scratch copy of

@@ -56,6 +56,30 @@ def pobj_sphere(src, n_types):
     return bytes(d)
 
 
+def pobj_poly(src, n_types):
+    """A polyhedral particle object: geometry, mass, inertia tensor (as the
+    parser leaves it, before the run setup scales it) and contact
+    properties; face tolerances are never set for polyhedra."""
+    d = T.POBJ()
+    d.radius, d.mass, d.COM = src.radius, src.mass, src.COM
+    d.num_vertex, d.num_faces, d.num_edges = src.num_vertex, src.num_faces, src.num_edges
+    for k in range(min(src.num_vertex, 32)):
+        d.vertex[k] = src.vertex[k]
+        d.Local_Vertex[k] = src.Local_Vertex[k]
+    for j in range(min(src.num_faces, 32)):
+        _surface(d.face[j], src.face[j])
+        d.face[j].Tol = 0.0
+    for k in range(min(src.num_edges, 32)):
+        d.edge[k] = src.edge[k]
+    for g in range(9):
+        d.InertiaT[g] = src.InertiaT[g]
+    for j in range(n_types):
+        d.PP[j] = src.PP[j]
+    for f in ("surface_Kn", "surface_Cn", "surface_Fric_static", "surface_Fric_kinetic",
+              "Dsurface_Kn", "Dsurface_Cn", "Dsurface_Fric_static", "Dsurface_Fric_kinetic"):
+        setattr(d, f, getattr(src, f))
+    return bytes(d)
+
 def dobj(src):
     d = T.DOBJ()
     d.btype = src.btype

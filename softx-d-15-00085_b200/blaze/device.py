@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("BLAZE_LIB") or os.path.join(os.path.dirname(os.path.a
                                                        "libblaze_b200.so")
 
 STATUS_BITS = {1: "list_overflow", 2: "out_of_grid", 4: "non_finite", 8: "type_range",
-               16: "timeout"}
+               16: "timeout", 32: "poly_undefined"}
 
 _f = C.POINTER(C.c_float)
 _u = C.POINTER(C.c_uint)
@@ -56,6 +56,8 @@ def load():
     lib.blaze_set_cylinder_rotation.argtypes = [C.c_void_p, C.c_int]
     lib.blaze_set_state.argtypes = [C.c_void_p, _f, _f, _f, _u, _i]
     lib.blaze_get_state.argtypes = [C.c_void_p, _f, _f, _f, _u, _i]
+    lib.blaze_set_state_ornt.argtypes = [C.c_void_p, _f, _f, _f, _f, _u, _i]
+    lib.blaze_get_state_ornt.argtypes = [C.c_void_p, _f, _f, _f, _f, _u, _i]
     lib.blaze_step.argtypes = [C.c_void_p, C.c_int]
     lib.blaze_sync.argtypes = [C.c_void_p]
     lib.blaze_num_current.argtypes = [C.c_void_p]
@@ -126,6 +128,7 @@ class Simulation:
             pobj, n_p, dobj, n_d = project.pobj, project.n_p, project.dobj, project.n_d
         self.lib = lib
         self.n = sim_info.Num_Particles
+        self.poly = sim_info.particle_type == 1
         self.opts = default_options(**options)
         h = C.c_void_p()
         rc = lib.blaze_create(C.byref(h), wobj, n_w, pobj, n_p, dobj, n_d, C.byref(sim_info),
@@ -154,16 +157,20 @@ class Simulation:
     def set_cylinder_rotation(self, on):
         _check(self.lib.blaze_set_cylinder_rotation(self.h, 1 if on else 0), "cylinder rotation")
 
-    def set_state(self, pos, vel=None, avel=None, ptype=None, pid=None):
+    def set_state(self, pos, vel=None, avel=None, ptype=None, pid=None, quat=None):
+        """Positions (centres of mass), velocities, angular velocities,
+        types, P_IDs and, for polyhedra, orientations (w, x, y, z)."""
         n = self.n
         c = np.ascontiguousarray
         pos = c(pos, np.float32).reshape(n, 3)
         vel = None if vel is None else c(vel, np.float32).reshape(n, 3)
         avel = None if avel is None else c(avel, np.float32).reshape(n, 3)
+        quat = None if quat is None else c(quat, np.float32).reshape(n, 4)
         ptype = np.zeros(n, np.uint32) if ptype is None else c(ptype, np.uint32)
         pid = np.arange(n, dtype=np.int32) if pid is None else c(pid, np.int32)
-        rc = self.lib.blaze_set_state(self.h, _ptr(pos, C.c_float), _ptr(vel, C.c_float),
-                                      _ptr(avel, C.c_float), _ptr(ptype, C.c_uint), _ptr(pid, C.c_int))
+        rc = self.lib.blaze_set_state_ornt(self.h, _ptr(pos, C.c_float), _ptr(quat, C.c_float),
+                                           _ptr(vel, C.c_float), _ptr(avel, C.c_float),
+                                           _ptr(ptype, C.c_uint), _ptr(pid, C.c_int))
         _check(rc, "blaze_set_state")
 
     def step(self, n=1):
@@ -179,10 +186,15 @@ class Simulation:
         avel = np.zeros((n, 3), np.float32)
         ptype = np.zeros(n, np.uint32)
         pid = np.zeros(n, np.int32)
-        st = _check(self.lib.blaze_get_state(self.h, _ptr(pos, C.c_float), _ptr(vel, C.c_float),
-                                             _ptr(avel, C.c_float), _ptr(ptype, C.c_uint),
-                                             _ptr(pid, C.c_int)), "blaze_get_state")
-        return dict(pos=pos, vel=vel, avel=avel, type=ptype, pid=pid, status=st)
+        quat = np.zeros((n, 4), np.float32) if self.poly else None
+        st = _check(self.lib.blaze_get_state_ornt(self.h, _ptr(pos, C.c_float),
+                                                  _ptr(quat, C.c_float), _ptr(vel, C.c_float),
+                                                  _ptr(avel, C.c_float), _ptr(ptype, C.c_uint),
+                                                  _ptr(pid, C.c_int)), "blaze_get_state")
+        out = dict(pos=pos, vel=vel, avel=avel, type=ptype, pid=pid, status=st)
+        if self.poly:
+            out["quat"] = quat
+        return out
 
     def forces(self):
         n = self.n
@@ -255,6 +267,11 @@ class KDevice:
     def _f3(a):
         return None if a is None else a.ctypes.data_as(C.POINTER(T.float3))
 
+    @staticmethod
+    def _q(a):
+        """Orientations, float32 (N, 4) as (w, x, y, z), or None."""
+        return None if a is None else a.ctypes.data_as(C.POINTER(T.Quaterion))
+
     def clean(self):
         return self.lib.Device_Clean()
 
@@ -282,12 +299,13 @@ class KDevice:
 
     def IDevice_Get_System_State(self, h_pos, h_Ornt, h_vel, h_Avel, h_acc, h_type, h_pid):
         return _check(self.lib.Device_Get_System_State(
-            self._f3(h_pos), None, self._f3(h_vel), self._f3(h_Avel), self._f3(h_acc),
+            self._f3(h_pos), self._q(h_Ornt), self._f3(h_vel), self._f3(h_Avel), self._f3(h_acc),
             _ptr(h_type, C.c_uint), _ptr(h_pid, C.c_int)), "Device_Get_System_State")
 
     def IDevice_Get_Positions(self, h_pos, h_Quart_ornt, h_type, P_ID):
-        return _check(self.lib.Device_Get_P_Positions(self._f3(h_pos), None, _ptr(h_type, C.c_uint),
-                                                      _ptr(P_ID, C.c_int)), "Device_Get_P_Positions")
+        return _check(self.lib.Device_Get_P_Positions(self._f3(h_pos), self._q(h_Quart_ornt),
+                                                      _ptr(h_type, C.c_uint), _ptr(P_ID, C.c_int)),
+                      "Device_Get_P_Positions")
 
     def IDevice_Get_Particle_Velocity(self, H_Vel, H_Rvel, flag, h_type, P_ID):
         return _check(self.lib.Device_Get_P_Velocity(self._f3(H_Vel), self._f3(H_Rvel), int(flag),
@@ -302,17 +320,18 @@ class KDevice:
 
     def IDevice_Set_ParticleSystem_State(self, h_pos, h_Ornt, h_vel, h_Avel, h_acc, h_type, h_pid):
         return _check(self.lib.Device_Set_System_State(
-            self._f3(h_pos), None, self._f3(h_vel), self._f3(h_Avel), self._f3(h_acc),
+            self._f3(h_pos), self._q(h_Ornt), self._f3(h_vel), self._f3(h_Avel), self._f3(h_acc),
             _ptr(h_type, C.c_uint), _ptr(h_pid, C.c_int)), "Device_Set_System_State")
 
     def IDevice_Set_ParticleSystem_Pos(self, h_pos, h_Ornt, h_type, h_pid):
-        return _check(self.lib.Device_Set_Pos(self._f3(h_pos), None, _ptr(h_type, C.c_uint),
-                                              _ptr(h_pid, C.c_int)), "Device_Set_Pos")
+        return _check(self.lib.Device_Set_Pos(self._f3(h_pos), self._q(h_Ornt),
+                                              _ptr(h_type, C.c_uint), _ptr(h_pid, C.c_int)),
+                      "Device_Set_Pos")
 
     def IDevice_Set_ParticleSystem_PosV(self, h_pos, h_Ornt, h_vel, h_Avel, h_type, h_pid):
         return _check(self.lib.Device_Set_Pos_Velocity(
-            self._f3(h_pos), None, self._f3(h_vel), self._f3(h_Avel), _ptr(h_type, C.c_uint),
-            _ptr(h_pid, C.c_int)), "Device_Set_Pos_Velocity")
+            self._f3(h_pos), self._q(h_Ornt), self._f3(h_vel), self._f3(h_Avel),
+            _ptr(h_type, C.c_uint), _ptr(h_pid, C.c_int)), "Device_Set_Pos_Velocity")
 
     def IStart_Bin(self):
         return self.lib.Start_Bin()

@@ -6,6 +6,7 @@ It restates, in order, the token reads and derived quantities of
   KSimulationData::ReadWObject           KSimulationData.cpp:704-883
   Set_SpringConstants*_KN / *_TC         KSimulationData.cpp:887-1071
   KSimulationData::ReadPObject_Sphere    KSimulationData.cpp:1076-1178
+  KSimulationData::ReadPObject_Poly      KSimulationData.cpp:1183-1624
   KSimulationData::ReadDObject           KSimulationData.cpp:1650-1780
   KSimulationData::Repeat_Lifters        KSimulationData.cpp:1885-2028
   Set_SimInfo (headless part)            V_02_2015/src/main.cpp:469-832
@@ -252,6 +253,141 @@ class Project:
         den = t.f()
         r = float(F(P.radius))
         P.mass = float(F((4.0 / 3.0) * 2.0 * math.asin(1.0) * math.pow(r, 3.0) * den * 1e-6))
+        self._read_contact_props(t, i, cor)
+
+    def _read_pobj_poly(self, i, path, cor):
+        """KSimulationData::ReadPObject_Poly (KSimulationData.cpp:1219-1624)
+        with Make_Particle_LocalInfo (1183-1215): vertices (Format 1 adds an
+        offset, faces list comma-separated vertex numbers), centre of mass as
+        the vertex mean, face centroids, normals from three face vertices,
+        areas and volume by fans about the face centroid, mass from the
+        density, the inertia tensor inverted element by element, body-frame
+        vertices and the bounding radius, then the contact properties."""
+        t = _Tokens(path)
+        P = self.pobj[i]
+        t.skip(2)
+        t.skip(2)
+        t.skip(1)
+        fmt = t.i_()
+        offset = v3(0, 0, 0)
+        if fmt == 1:
+            t.skip(1)
+            offset = t.f3()
+        t.skip(3)
+        t.skip(1)
+        nv = t.i_()
+        if nv < 1 or nv > 32:
+            raise ProjectError("polyhedron %d has %d vertices (1..32)" % (i, nv))
+        P.num_vertex = nv
+        verts = []
+        size = [F(0), F(0), F(0)]
+        acc = v3(0, 0, 0)
+        for k in range(nv):
+            if fmt == 0:
+                t.skip(1)
+                v = t.f3()
+            else:
+                v = vadd(t.f3(), offset)
+            verts.append(v)
+            setf3(P.vertex[k], v)
+            for c in range(3):
+                if v[c] > size[c]:
+                    size[c] = v[c]
+            acc = vadd(acc, v)
+        setf3(self.init.p_size[i], size)
+        com = vscale(F(F(1.0) / F(nv)), acc)
+        setf3(P.COM, com)
+        t.skip(1)
+        nf = t.i_()
+        if nf < 1 or nf > 32:
+            raise ProjectError("polyhedron %d has %d faces (1..32)" % (i, nf))
+        P.num_faces = nf
+        vol = F(0)
+        tot_area = None  # the reference's TotArea carries over between faces
+        for j in range(nf):
+            S = P.face[j]
+            if fmt == 0:
+                t.skip(2)
+            fv = t.i_()
+            if fv < 3 or fv > 8:
+                raise ProjectError("polyhedron %d face %d has %d vertices (3..8)" % (i, j, fv))
+            S.num_vertex = fv
+            facc = v3(0, 0, 0)
+            for f in range(fv):
+                tok = t.s()
+                if fmt == 1 and f < fv - 1:
+                    tok = tok.rstrip(",")
+                try:
+                    o = int(tok) - 1
+                except ValueError:
+                    raise ProjectError("expected a vertex number, got %r in %s" % (tok, path))
+                if o < 0 or o >= nv:
+                    raise ProjectError("polyhedron %d face %d names vertex %d" % (i, j, o + 1))
+                S.vertex_Order[f] = o
+                facc = vadd(facc, verts[o])
+            cen = vscale(F(F(1.0) / F(fv)), facc)
+            setf3(S.centroid, cen)
+            o = [S.vertex_Order[f] for f in range(fv)]
+
+            def tet(a, b, c):
+                return F(vdot(vsub(a, com), vcross(vsub(b, com), vsub(c, com))) / F(6.0))
+
+            if fv == 3:
+                n = vcross(vsub(verts[o[1]], verts[o[2]]), vsub(verts[o[2]], verts[o[0]]))
+                setf3(S.normal, vdiv(n, vlen(n)))
+                ad, bd, cd = (vsub(verts[o[k]], com) for k in range(3))
+                vol = F(vol + F(F(np.sqrt(vdot(ad, vcross(bd, cd)))) / F(6.0)))
+                if tot_area is None:
+                    # the reference stores an uninitialised TotArea here
+                    tot_area = F(F(0.5) * vlen(n))
+            else:
+                n = vcross(vsub(verts[o[2]], verts[o[3]]), vsub(verts[o[3]], verts[o[0]]))
+                setf3(S.normal, vdiv(n, vlen(n)))
+                tot_area = F(F(0.5) * vlen(vcross(vsub(verts[o[fv - 1]], cen),
+                                                  vsub(verts[o[0]], cen))))
+                vol = F(vol + tet(verts[o[fv - 1]], verts[o[0]], cen))
+                for tr in range(fv - 1):
+                    vol = F(vol + tet(verts[o[tr]], verts[o[tr + 1]], cen))
+                    tot_area = F(tot_area + F(F(0.5) * vlen(vcross(vsub(verts[o[tr]], cen),
+                                                                   vsub(verts[o[tr + 1]], cen)))))
+            S.area = float(tot_area)
+        t.skip(1)
+        ne = t.i_()
+        if ne < 0 or ne > 32:
+            raise ProjectError("polyhedron %d has %d edges (0..32)" % (i, ne))
+        P.num_edges = ne
+        for k in range(ne):
+            a, b = t.i_() - 1, t.i_() - 1
+            if not (0 <= a < nv and 0 <= b < nv):
+                raise ProjectError("polyhedron %d edge %d names a missing vertex" % (i, k))
+            P.edge[k].point_vindex[0] = a
+            P.edge[k].point_vindex[1] = b
+        t.skip(3)
+        t.skip(1)
+        density = F(t.f())
+        P.mass = float(F(float(F(density * vol)) * 1e-6))
+        t.skip(1)
+        for k in range(9):
+            x = F(t.f())
+            P.InertiaT[k] = float(F(1.0 / float(x))) if x > 0.0 else float(x)
+        rad = F(0)
+        for k in range(nv):
+            lv = vsub(verts[k], com)
+            setf3(P.Local_Vertex[k], lv)
+            d = vlen(lv)
+            if d > rad:
+                rad = d
+        P.radius = float(rad)
+        t.skip(3)
+        self._read_contact_props(t, i, cor)
+
+    def _read_contact_props(self, t, i, cor):
+        """The contact-property blocks shared by sphere and polyhedron
+        objects (KSimulationData.cpp:1100-1175, 1543-1620): particle, surface
+        and volume-object restitution with Kn (KN mode) or contact time (TC
+        mode), friction coefficients, and the surface damping derived from
+        them."""
+        P = self.pobj[i]
         if self.force_spec == 0:
             t.skip(1)
             t.skip(1); cor[i] = t.f()
@@ -509,9 +645,11 @@ class Project:
             t.skip(1)
             name = t.s()
             self.per_object[i] = t.i_()
-            if self.particle_type != 0:
-                raise ProjectError("polyhedral particle objects are read by the reference's parser only")
-            self._read_pobj_sphere(i, os.path.join(base, "ParticleObjects", name + ".POBJ"), cor)
+            path = os.path.join(base, "ParticleObjects", name + ".POBJ")
+            if self.particle_type == 1:
+                self._read_pobj_poly(i, path, cor)
+            else:
+                self._read_pobj_sphere(i, path, cor)
         for i in range(self.n_p):
             for j in range(self.n_p):
                 if self.force_spec == 0:
@@ -647,9 +785,14 @@ class Project:
         si.unit_test = self.is_debug
         for i in range(self.n_p):
             P = self.pobj[i]
+            r, m = F(P.radius), F(P.mass)
+            scale = F(F(1.0) / F(F(F(F(0.4) * r) * r) * m))
             if self.particle_type == 0:
-                r, m = F(P.radius), F(P.mass)
-                P.InertiaT[0] = float(F(F(1.0) / F(F(F(F(0.4) * r) * r) * m)))
+                P.InertiaT[0] = float(scale)
+            else:
+                # main.cpp:622-626: the inverted tensor scaled by 1/(0.4 m r^2)
+                for g in range(9):
+                    P.InertiaT[g] = float(F(scale * F(P.InertiaT[g])))
         si.Vel_Limit = float(self.vel_limit)
         if self.sim_type == 1:
             si.Simulation_Type = 1

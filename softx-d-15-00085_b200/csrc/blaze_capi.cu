@@ -15,6 +15,7 @@
 
 #include "blaze_dem.h"
 #include "dem_kernels.cuh"
+#include "poly_kernels.cuh"
 #include "radix_sort.cuh"
 
 using namespace blaze;
@@ -90,6 +91,11 @@ struct blaze_sim {
   // each), packed / unpacked by a kernel, and its two result words (pinned)
   HostStage stage{};
   int* h_flags = nullptr;
+  // convex polyhedra (particle_type 1): body-frame objects and the
+  // world-frame geometry the step rebuilds
+  bool poly = false;
+  PolyShape* d_shapes = nullptr;
+  PolyGeom geom{};
 };
 
 namespace {
@@ -131,6 +137,7 @@ void build_params(blaze_sim* s) {
     T.radius = o.radius;
     T.mass = o.mass;
     T.iinv = o.InertiaT[0];
+    T.com = o.COM;
     T.s_kn = o.surface_Kn; T.s_cn = o.surface_Cn;
     T.s_mus = o.surface_Fric_static; T.s_muk = o.surface_Fric_kinetic;
     T.d_kn = o.Dsurface_Kn; T.d_cn = o.Dsurface_Cn; T.d_muk = o.Dsurface_Fric_kinetic;
@@ -385,17 +392,30 @@ cudaEvent_t prof_event(blaze_sim* s, int phase) {
   return e;
 }
 
+// The kernels of one step after the (conditional) re-sort, reading S[cur]
+// or the sorted copy S[2] as `link` says and writing S[cur ^ 1]; returns the
+// number of launches.
+int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
+  const ForceCapture* cap = s->opt.capture_forces ? &s->cap : nullptr;
+  if (s->poly) {
+    launch_poly_geom(s->d_shapes, s->geom, s->S[s->cur], s->S[2], s->ob, s->n_max,
+                     s->si.Rotation ? 1 : 0, s->ctl, link.rebuilt, st);
+    launch_poly_step(s->dp, s->d_shapes, s->geom, s->d_ops, s->S[s->cur], s->S[2],
+                     s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, cap, st);
+    return 2;
+  }
+  launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
+              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, st);
+  return 1;
+}
+
 int enqueue_step(blaze_sim* s) {
   if (s->profile) prof_event(s, 0);
   launch_gate(s->ctl, s->stream);
   int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
   if (rc) return rc;
   if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
-  launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
-              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl,
-              StepLink{&s->ctl->rebuilt, 0, 0}, s->spin_free,
-              s->opt.capture_forces ? &s->cap : nullptr, s->stream);
-  s->last_launches += 2;
+  s->last_launches += 1 + enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0}, s->stream);
   if (s->profile) prof_event(s, 1);
   s->cur ^= 1;
   s->steps++;
@@ -462,9 +482,7 @@ int build_graph(blaze_sim* s, int c) {
     if (rc) return rc;
     const StepLink link = k + 1 < kGraphSteps ? StepLink{s->d_rb + k, h[k + 1], 1}
                                                : StepLink{s->d_rb + k, 0, 0};
-    launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
-                s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free,
-                s->opt.capture_forces ? &s->cap : nullptr, s->stream);
+    enqueue_step_kernels(s, link, s->stream);
     s->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
@@ -492,9 +510,9 @@ int graph_steps(blaze_sim* s, int nsteps) {
       if (rc) return rc;
     }
     CK(cudaGraphLaunch(s->graph[c], s->stream));
-    // launches that always run: the gate and one step kernel per step
+    // launches that always run: the gate and the step kernels of each step
     // (re-sort bodies run only when a step asks for them)
-    s->last_launches += 1 + kGraphSteps;
+    s->last_launches += 1 + kGraphSteps * (s->poly ? 2 : 1);
     s->steps += kGraphSteps;
     if (s->si.Kill_Particles) s->stepc += kGraphSteps;
     if (kGraphSteps & 1) s->cur ^= 1;
@@ -511,8 +529,8 @@ int sync_status(blaze_sim* s) {
   return (int)s->status;
 }
 
-int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
-                   const uint* type, const int* pid) {
+int set_state_impl(blaze_sim* s, const float* pos3, const float* quat4, const float* vel3,
+                   const float* avel3, const uint* type, const int* pid) {
   const int n = s->n_max;
   int rc = sync_status(s);
   if (rc < 0) return rc;
@@ -526,13 +544,17 @@ int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const flo
     CK(cudaMemcpyAsync(hs.avel3, avel3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(hs.type, type, sizeof(uint) * n, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(hs.pid, pid, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+  const bool has_q = s->poly && quat4 != nullptr;
+  if (has_q)
+    CK(cudaMemcpyAsync(hs.quat4, quat4, sizeof(float) * 4 * n, cudaMemcpyHostToDevice, s->stream));
   launch_pack_state(s->dp, hs, vel3 != nullptr, avel3 != nullptr, s->S[s->cur], s->ob.pid[e],
-                    s->n_d > 0 ? s->ob.lift[e] : nullptr, n, s->stream);
+                    s->n_d > 0 ? s->ob.lift[e] : nullptr, s->poly ? s->ob.ornt[e] : nullptr,
+                    has_q, n, s->stream);
   CK(cudaMemcpyAsync(s->h_flags, hs.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
   const int dead = s->h_flags[0];
-  const bool spin_free = !s->si.Rotation && s->h_flags[1] == 0;
+  const bool spin_free = !s->poly && !s->si.Rotation && s->h_flags[1] == 0;
   if (spin_free != s->spin_free) {
     drop_graphs(s);
     s->spin_free = spin_free;
@@ -548,13 +570,17 @@ int set_state_impl(blaze_sim* s, const float* pos3, const float* vel3, const flo
   return 0;
 }
 
-int get_state_impl(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid) {
+int get_state_impl(blaze_sim* s, float* pos3, float* quat4, float* vel3, float* avel3, uint* type,
+                   int* pid) {
   int st = sync_status(s);
   if (st < 0) return st;
   const int n = s->n_max;
   const int e = s->h_ctl->epoch & 1;
   const HostStage& hs = s->stage;
-  launch_unpack_state(hs, s->S[s->cur], s->ob.pid[e], n, s->stream);
+  launch_unpack_state(s->dp, hs, s->S[s->cur], s->ob.pid[e], s->poly ? s->ob.ornt[e] : nullptr, n,
+                      s->stream);
+  if (quat4 && s->poly)
+    CK(cudaMemcpyAsync(quat4, hs.quat4, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, s->stream));
   if (pos3) CK(cudaMemcpyAsync(pos3, hs.pos3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
   if (vel3) CK(cudaMemcpyAsync(vel3, hs.vel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
   if (avel3) CK(cudaMemcpyAsync(avel3, hs.avel3, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
@@ -575,11 +601,89 @@ void free_sim(blaze_sim* s) {
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   f(s->stage.pos3); f(s->stage.vel3); f(s->stage.avel3); f(s->stage.type); f(s->stage.pid);
-  f(s->stage.flags);
+  f(s->stage.flags); f(s->stage.quat4);
+  f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
+  f(s->geom.vert); f(s->geom.fnorm); f(s->geom.fcent);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
+}
+
+// A polyhedral particle object must fit the fixed-size tables of POBJ and
+// index only its own vertices.
+bool poly_object_valid(const POBJ& o, int t) {
+  auto bad = [&](const char* what) {
+    std::fprintf(stderr, "blaze: polyhedral particle object %d: %s\n", t, what);
+    return false;
+  };
+  if (o.num_vertex < 1 || o.num_vertex > kPolyMaxV) return bad("num_vertex outside 1..32");
+  if (o.num_faces < 1 || o.num_faces > kPolyMaxF) return bad("num_faces outside 1..32");
+  if (o.num_edges < 0 || o.num_edges > kPolyMaxE) return bad("num_edges outside 0..32");
+  for (int f = 0; f < o.num_faces; ++f) {
+    const Surface& F = o.face[f];
+    if (F.num_vertex < 1 || F.num_vertex > kPolyFaceV) return bad("face vertex count outside 1..8");
+    for (int k = 0; k < F.num_vertex; ++k)
+      if (F.vertex_Order[k] < 0 || F.vertex_Order[k] >= o.num_vertex)
+        return bad("face vertex index outside the object");
+  }
+  for (int e = 0; e < o.num_edges; ++e)
+    for (int k = 0; k < 2; ++k)
+      if (o.edge[e].point_vindex[k] >= (uint)o.num_vertex)
+        return bad("edge vertex index outside the object");
+  return true;
+}
+
+// Body-frame objects to the device, orientation copies, world-frame
+// geometry buffers sized by the largest object, orientation staging.
+int setup_poly(blaze_sim* s) {
+  std::vector<PolyShape> shapes(kMaxTypes);
+  std::memset(shapes.data(), 0, sizeof(PolyShape) * kMaxTypes);
+  int kv = 1, kf = 1;
+  for (int t = 0; t < s->n_p; ++t) {
+    const POBJ& o = s->p[t];
+    PolyShape& S = shapes[t];
+    S.nv = o.num_vertex;
+    S.nf = o.num_faces;
+    S.ne = o.num_edges;
+    for (int k = 0; k < S.nv; ++k)
+      S.vert[k] = make_float4(o.Local_Vertex[k].x, o.Local_Vertex[k].y, o.Local_Vertex[k].z, 0.0f);
+    for (int f = 0; f < S.nf; ++f) {
+      const Surface& F = o.face[f];
+      S.fnorm[f] = make_float4(F.normal.x, F.normal.y, F.normal.z, 0.0f);
+      // face.centroid - COM, the body-frame offset RotatePolyhedra rotates
+      S.fcent[f] = make_float4(F.centroid.x - o.COM.x, F.centroid.y - o.COM.y,
+                               F.centroid.z - o.COM.z, 0.0f);
+      S.farea[f] = F.area;
+      S.fnv[f] = F.num_vertex;
+      for (int k = 0; k < F.num_vertex; ++k) S.ford[f][k] = (uint8_t)F.vertex_Order[k];
+    }
+    for (int e = 0; e < S.ne; ++e) {
+      S.edge[e][0] = (uint8_t)o.edge[e].point_vindex[0];
+      S.edge[e][1] = (uint8_t)o.edge[e].point_vindex[1];
+    }
+    for (int k = 0; k < 9; ++k) S.inertia[k] = o.InertiaT[k];
+    S.com[0] = o.COM.x; S.com[1] = o.COM.y; S.com[2] = o.COM.z;
+    kv = std::max(kv, S.nv);
+    kf = std::max(kf, S.nf);
+  }
+  const size_t n = (size_t)s->n_max;
+  CK(dalloc(&s->d_shapes, kMaxTypes));
+  CK(cudaMemcpy(s->d_shapes, shapes.data(), sizeof(PolyShape) * kMaxTypes,
+                cudaMemcpyHostToDevice));
+  s->geom.kv = kv;
+  s->geom.kf = kf;
+  CK(dalloc(&s->geom.vert, n * kv));
+  CK(dalloc(&s->geom.fnorm, n * kf));
+  CK(dalloc(&s->geom.fcent, n * kf));
+  for (int b = 0; b < 2; ++b) {
+    CK(dalloc(&s->ob.ornt[b], n));
+    std::vector<float4> ident(n, make_float4(1.0f, 0.0f, 0.0f, 0.0f));
+    CK(cudaMemcpy(s->ob.ornt[b], ident.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+  }
+  CK(dalloc(&s->stage.quat4, 4 * n));
+  s->poly = true;
+  return 0;
 }
 
 int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
@@ -587,9 +691,18 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   if (!out || !si || n_w < 0 || n_w > 8 || n_p < 1 || n_p > kMaxTypes || n_d < 0 ||
       n_d > kMaxDobj || si->Num_Particles <= 0 || (n_w && !w) || !p || (n_d && !d))
     return -1;
-  if (si->particle_type != 0) {
-    std::fprintf(stderr, "blaze: polyhedral particles are not supported by this library\n");
+  if (si->particle_type != 0 && si->particle_type != 1) {
+    std::fprintf(stderr, "blaze: particle_type %d is not supported (0 spheres, 1 polyhedra)\n",
+                 si->particle_type);
     return -1;
+  }
+  if (si->particle_type == 1) {
+    if (n_d > 0) {
+      std::fprintf(stderr, "blaze: volume objects with polyhedral particles are not supported\n");
+      return -1;
+    }
+    for (int t = 0; t < n_p; ++t)
+      if (!poly_object_valid(p[t], t)) return -1;
   }
   blaze_sim* s = new (std::nothrow) blaze_sim();
   if (!s) return -1;
@@ -654,6 +767,10 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   if (rc) return fail(rc);
   rc = alloc_capture(s);
   if (rc) return fail(rc);
+  if (si->particle_type == 1) {
+    rc = setup_poly(s);
+    if (rc) return fail(rc);
+  }
   // zero state until the caller sets one (Set_Init_Config_Device zeroes velocities)
   for (int b = 0; b < 3; ++b) {
     CKF(cudaMemset(s->S[b].pos, 0, sizeof(float4) * n));
@@ -726,12 +843,24 @@ int blaze_set_cylinder_rotation(blaze_sim* s, int on) {
 int blaze_set_state(blaze_sim* s, const float* pos3, const float* vel3, const float* avel3,
                     const uint* type, const int* pid) {
   if (!s || !pos3 || !type || !pid) return -1;
-  return set_state_impl(s, pos3, vel3, avel3, type, pid);
+  return set_state_impl(s, pos3, nullptr, vel3, avel3, type, pid);
 }
 
 int blaze_get_state(blaze_sim* s, float* pos3, float* vel3, float* avel3, uint* type, int* pid) {
   if (!s) return -1;
-  return get_state_impl(s, pos3, vel3, avel3, type, pid);
+  return get_state_impl(s, pos3, nullptr, vel3, avel3, type, pid);
+}
+
+int blaze_set_state_ornt(blaze_sim* s, const float* pos3, const float* quat4, const float* vel3,
+                         const float* avel3, const uint* type, const int* pid) {
+  if (!s || !pos3 || !type || !pid) return -1;
+  return set_state_impl(s, pos3, quat4, vel3, avel3, type, pid);
+}
+
+int blaze_get_state_ornt(blaze_sim* s, float* pos3, float* quat4, float* vel3, float* avel3,
+                         uint* type, int* pid) {
+  if (!s) return -1;
+  return get_state_impl(s, pos3, quat4, vel3, avel3, type, pid);
 }
 
 int blaze_step(blaze_sim* s, int nsteps) {
@@ -899,26 +1028,24 @@ int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_Dyn
   if (!s) return -2
 
 int Device_Set_Pos(float3* h_pos, Quaterion* h_Ornt, uint* h_ptype, int* h_pid) {
-  (void)h_Ornt;
   DEF_SIM();
-  return set_state_impl(s, (const float*)h_pos, nullptr, nullptr, h_ptype, h_pid);
+  return set_state_impl(s, (const float*)h_pos, (const float*)h_Ornt, nullptr, nullptr, h_ptype,
+                        h_pid);
 }
 
 int Device_Set_Pos_Velocity(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
                             uint* h_ptype, int* h_pid) {
-  (void)h_Ornt;
   DEF_SIM();
-  return set_state_impl(s, (const float*)h_pos, (const float*)h_vel, (const float*)h_Avel,
-                        h_ptype, h_pid);
+  return set_state_impl(s, (const float*)h_pos, (const float*)h_Ornt, (const float*)h_vel,
+                        (const float*)h_Avel, h_ptype, h_pid);
 }
 
 int Device_Set_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
                             float3* h_acc, uint* h_ptype, int* h_pid) {
-  (void)h_Ornt;
   (void)h_acc;
   DEF_SIM();
-  return set_state_impl(s, (const float*)h_pos, (const float*)h_vel, (const float*)h_Avel,
-                        h_ptype, h_pid);
+  return set_state_impl(s, (const float*)h_pos, (const float*)h_Ornt, (const float*)h_vel,
+                        (const float*)h_Avel, h_ptype, h_pid);
 }
 
 int Device_Set_Tallys(float* h_Tallys) {
@@ -932,21 +1059,21 @@ int Device_Get_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, flo
                             float3* h_acc, uint* h_ptype, int* h_pid) {
   (void)h_acc;
   DEF_SIM();
-  int rc = get_state_impl(s, (float*)h_pos, (float*)h_vel, (float*)h_Avel, h_ptype, h_pid);
+  int rc = get_state_impl(s, (float*)h_pos, (float*)h_Ornt, (float*)h_vel, (float*)h_Avel, h_ptype,
+                          h_pid);
   if (rc >= 0 && h_Ornt && s->si.sphere_orient)
     for (int i = 0; i < s->n_max; ++i) h_Ornt[i] = Quaterion{1.0f, 0.0f, 0.0f, 0.0f};
   return rc;
 }
 
 int Device_Get_P_Positions(float3* Pos, Quaterion* Quart_ornt, uint* h_ptype, int* h_pid) {
-  (void)Quart_ornt;
   DEF_SIM();
-  return get_state_impl(s, (float*)Pos, nullptr, nullptr, h_ptype, h_pid);
+  return get_state_impl(s, (float*)Pos, (float*)Quart_ornt, nullptr, nullptr, h_ptype, h_pid);
 }
 
 int Device_Get_P_Velocity(float3* H_Vel, float3* H_Rvel, int Flag, uint* h_ptype, int* h_pid) {
   DEF_SIM();
-  return get_state_impl(s, nullptr, (float*)H_Vel, Flag == 1 ? (float*)H_Rvel : nullptr, h_ptype,
+  return get_state_impl(s, nullptr, nullptr, (float*)H_Vel, Flag == 1 ? (float*)H_Rvel : nullptr, h_ptype,
                         h_pid);
 }
 

@@ -36,6 +36,8 @@ enum StatusBits : uint32_t {
   kStatusNonFinite = 4u,      // non-finite position after integration
   kStatusTypeRange = 8u,      // particle type outside the particle-object table
   kStatusTimeout = 16u,       // a bounded device wait gave up
+  kStatusPolyUndefined = 32u, // a polyhedron contact met a case the reference
+                              // leaves undefined (see poly_kernels.cu)
 };
 
 // One step of the wall program: planar faces, infinite planes, a macro
@@ -65,6 +67,7 @@ struct WallOp {
 
 struct TypeParams {
   float radius, mass, iinv;
+  float3 com;        // polyhedra: centre of mass in the object file's frame
   float s_kn, s_cn, s_mus, s_muk;
   float d_kn, d_cn, d_muk;
   PP_Parms pp[kMaxPP];

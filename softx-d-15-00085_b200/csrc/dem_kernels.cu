@@ -16,6 +16,7 @@
 //                                              Collision_Response.cuh,
 //                                              Integration.cuh:6-184)
 #include "dem_kernels.cuh"
+#include "dem_laws.cuh"
 
 namespace blaze {
 namespace {
@@ -122,6 +123,11 @@ k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
     int* l_dst = e ? ob.lift[0] : ob.lift[1];
     l_dst[i] = l_src[j];
   }
+  if (ob.ornt[0]) {
+    const float4* q_src = e ? ob.ornt[1] : ob.ornt[0];
+    float4* q_dst = e ? ob.ornt[0] : ob.ornt[1];
+    q_dst[i] = q_src[j];
+  }
   const uint32_t k = keys[i];
   if (k < ncell_tab) {
     if (i == 0 || keys[i - 1] != k) cstart[k] = (uint32_t)i;
@@ -179,179 +185,6 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
   flag_status(ctl, st);
 }
 
-// ------------------------------------------------------------ contact laws
-struct Forces { float3 trans, torque; };
-
-// Collision_Response_Particle_Particle, Collision_Response.cuh:374-494
-// (energy tallies excluded).  kSpin = false is the spin-free form used when
-// rotation is off and every angular velocity is exactly zero: then
-// v + cross(0, R) equals v up to the sign of an exact zero, so the forces
-// are the same numbers.
-template <bool kSpin>
-__device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
-                                         float3 ra, float3 rb, float3 wa, float3 wb,
-                                         const PP_Parms& pp, float3 va, float3 vb, float ma,
-                                         float mb) {
-  Forces F;
-  const float3 vn = dot3(rvel, n) * n;
-  const float fn = pp.Kn * pen;
-  const float3 fdiss = pp.Cn * vn;
-  F.trans = fn * n - fdiss;
-  const float3 vcpa = kSpin ? va + cross3(wa, ra) : va;
-  const float3 vcpb = kSpin ? vb + cross3(wb, rb) : vb;
-  const float3 vcpna = dot3(vcpa, n) * n;
-  const float3 vcpnb = dot3(vcpb, n) * n;
-  const float3 vt = (vcpa - vcpna) - (vcpb - vcpnb);
-  float mag = dot3(vt, vt);
-  float3 ft = f3(0.0f, 0.0f, 0.0f);
-  if (mag > 0.0f) {
-    mag = sqrtf(mag);
-    float velf = dot3(rvel, rvel);
-    if (velf > 0) velf = sqrtf(velf);
-    else velf = 1.0f;
-    const float tan_f = ((((0.50f * (ma + mb)) / P.dt) * 0.050f) * pp.Fric_kinetic) * (mag / velf);
-    ft = (-1.0f * tan_f) * (vt / mag);
-  }
-  F.trans = F.trans + ft;
-  F.torque = (kSpin && P.rotation) ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
-  return F;
-}
-
-// Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109
-__device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 pvel, float3 n,
-                                                     float pen, float3 r, float3 w,
-                                                     const TypeParams& T) {
-  Forces F;
-  const float3 vn = dot3(pvel, n) * n;
-  const float fn = T.s_kn * pen;
-  const float3 fdiss = T.s_cn * vn;
-  F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
-  if (dot3(fdir, n) < 0) F.trans = fn * n;
-  float3 vt = pvel - vn;
-  if (P.rotation) vt = vt + cross3(w, r);
-  float mag = dot3(vt, vt);
-  float3 ft = f3(0.0f, 0.0f, 0.0f);
-  if (mag > 0.0f) {
-    mag = sqrtf(mag);
-    float velf = dot3(pvel, pvel);
-    if (velf > 0) velf = sqrtf(velf);
-    else velf = 1.0f;
-    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.s_mus * (mag / velf));
-    ft = (-1.0f * tan_f) * (vt / mag);
-  }
-  F.trans = F.trans + ft;
-  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
-  return F;
-}
-
-// Collision_Response_Particle_MovingSurface, Collision_Response.cuh:116-233
-template <bool kSpin>
-__device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 n, float pen,
-                                                     float3 r, float3 w, const TypeParams& T,
-                                                     float3 va, float3 vs) {
-  Forces F;
-  const float3 rvel = va - vs;
-  const float3 vn = dot3(rvel, n) * n;
-  const float fn = T.s_kn * pen;
-  const float3 fdiss = T.s_cn * vn;
-  F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
-  if (dot3(fdir, n) < 0) F.trans = fn * n;
-  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
-  const float3 vcpna = dot3(vcpa, n) * n;
-  const float3 vt = (vcpa - vcpna) - (vs - dot3(vs, n) * n);
-  float mag = dot3(vt, vt);
-  float3 ft = f3(0.0f, 0.0f, 0.0f);
-  if (mag > 0.0f) {
-    mag = sqrtf(mag);
-    float velf = dot3(rvel, rvel);
-    if (velf > 0) velf = sqrtf(velf);
-    else velf = 1.0f;
-    const float tan_f = T.s_muk * (mag / velf);
-    ft = (((-1.0f * tan_f) * (vt / mag)) * (T.mass / P.dt)) * 0.050f;
-  }
-  F.trans = F.trans + ft;
-  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
-  return F;
-}
-
-// Collision_Response_Particle_VolumeObject, Collision_Response.cuh:241-363,
-// with the zero object spin and lever the caller passes
-// (DEM_Kernels_Compute.cuh:206-216).
-template <bool kSpin>
-__device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float pen, float3 r,
-                                             float3 w, const TypeParams& T, float3 va,
-                                             float3 vobj) {
-  Forces F;
-  const float3 rvel = va - vobj;
-  const float3 vn = dot3(rvel, n) * n;
-  const float fn = T.d_kn * pen;
-  const float3 fdiss = T.d_cn * vn;
-  F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
-  if (dot3(fdir, n) < 0) F.trans = fn * n;
-  const float3 z = f3(0.0f, 0.0f, 0.0f);
-  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
-  const float3 vcpb = vobj + cross3(z, z);
-  const float3 vt = (vcpa - dot3(vcpa, n) * n) - (vcpb - dot3(vcpb, n) * n);
-  float mag = dot3(vt, vt);
-  float3 ft = z;
-  if (mag > 0.0f) {
-    mag = sqrtf(mag);
-    float velf = dot3(rvel, rvel);
-    if (velf > 0) velf = sqrtf(velf);
-    else velf = 1.0f;
-    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.d_muk * (mag / velf));
-    ft = (-1.0f * tan_f) * (vt / mag);
-  }
-  F.trans = F.trans + ft;
-  F.torque = P.rotation ? cross3(r, F.trans) : z;
-  return F;
-}
-
-// Collision_Response_EndPlate_Particle, Collision_Response.cuh:504-526
-__device__ __forceinline__ float3 law_end_plate(float3 rvel, float3 n, float pen,
-                                                const TypeParams& T) {
-  const float3 vn = dot3(rvel, n) * n;
-  const float3 fdiss = T.s_cn * vn;
-  const float fn = T.s_kn * pen;
-  return fn * n - fdiss;
-}
-
-// is_PointOnSurface, Utilities.cuh:20-53
-__device__ __forceinline__ bool point_on_polygon(int nv, const float3* v, float3 pt, float sarea,
-                                                 float tol) {
-  float area = 0.0f;
-  for (int i = 0; i < nv - 1; ++i) {
-    const float3 v1 = pt - v[i];
-    const float3 v2 = pt - v[i + 1];
-    area = area + 0.500000f * len3(cross3(v1, v2));
-  }
-  const float3 v1 = pt - v[nv - 1];
-  const float3 v2 = pt - v[0];
-  area = area + 0.500000f * len3(cross3(v1, v2));
-  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
-}
-
-// is_PointOnSurface over vertices addressed through vertex_Order.
-__device__ __forceinline__ bool point_on_indexed_polygon(int nv, const float3* v, const int* order,
-                                                         float3 pt, float sarea, float tol) {
-  float area = 0.0f;
-  for (int i = 0; i < nv - 1; ++i) {
-    const float3 v1 = pt - v[order[i] & 7];
-    const float3 v2 = pt - v[order[i + 1] & 7];
-    area = area + 0.500000f * len3(cross3(v1, v2));
-  }
-  const float3 v1 = pt - v[order[nv - 1] & 7];
-  const float3 v2 = pt - v[order[0] & 7];
-  area = area + 0.500000f * len3(cross3(v1, v2));
-  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
-}
-
-__device__ __forceinline__ float3 drum_velocity(const SimParams& P, float3 cp) {
-  return cross3(f3(0.0f, 0.0f, -P.mill_rot_vel), cp - f3(P.drum_r, P.drum_r, 0.0f));
-}
 
 // WorldObject_InteractionParticle for spheres (DEM_Kernels_Compute.cuh:254-610):
 // one op per face / plane / cylinder / cap in world-object order.
@@ -637,7 +470,8 @@ __global__ void k_kill(StateBuf s, OrderBuf ob, int n_max, float kill_height, in
 // 486-520) as one pass each over the staged host arrays.
 __global__ void __launch_bounds__(kThreads)
 k_pack_state(const SimParams* __restrict__ P, HostStage hs, int has_vel, int has_avel, StateBuf s,
-             int* __restrict__ pid_dst, int* __restrict__ lift_dst, int n) {
+             int* __restrict__ pid_dst, int* __restrict__ lift_dst, float4* __restrict__ ornt_dst,
+             int has_ornt, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t t = hs.type[i];
@@ -653,6 +487,12 @@ k_pack_state(const SimParams* __restrict__ P, HostStage hs, int has_vel, int has
   const int id = hs.pid[i];
   pid_dst[i] = id;
   if (lift_dst) lift_dst[i] = -1;
+  // Set_PSystem_State (GPU_Memory_Transfer.cuh:400-440): polyhedra take the
+  // caller's orientation, positions as given (the centre of mass)
+  if (ornt_dst)
+    ornt_dst[i] = has_ornt ? make_float4(hs.quat4[4 * i], hs.quat4[4 * i + 1], hs.quat4[4 * i + 2],
+                                         hs.quat4[4 * i + 3])
+                           : make_float4(1.0f, 0.0f, 0.0f, 0.0f);
   const unsigned m = __activemask();
   const int dead = __popc(__ballot_sync(m, id < 0));
   const bool spin = __any_sync(m, w.x != 0.0f || w.y != 0.0f || w.z != 0.0f);
@@ -663,11 +503,23 @@ k_pack_state(const SimParams* __restrict__ P, HostStage hs, int has_vel, int has
 }
 
 __global__ void __launch_bounds__(kThreads)
-k_unpack_state(HostStage hs, StateBuf s, const int* __restrict__ pid_src, int n) {
+k_unpack_state(const SimParams* __restrict__ P, HostStage hs, StateBuf s,
+               const int* __restrict__ pid_src, const float4* __restrict__ ornt_src, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 p = s.pos[i], v = s.vel[i], w = s.angv[i];
-  hs.pos3[3 * i] = p.x; hs.pos3[3 * i + 1] = p.y; hs.pos3[3 * i + 2] = p.z;
+  if (ornt_src) {
+    // Get_SystemState (GPU_Memory_Transfer.cuh:486-520): a polyhedron's
+    // position is returned relative to its object file's origin (pos - COM)
+    const int t = __float_as_int(v.w);
+    const float3 c = P->types[t & (kMaxTypes - 1)].com;
+    hs.pos3[3 * i] = p.x - c.x; hs.pos3[3 * i + 1] = p.y - c.y; hs.pos3[3 * i + 2] = p.z - c.z;
+    const float4 q = ornt_src[i];
+    hs.quat4[4 * i] = q.x; hs.quat4[4 * i + 1] = q.y; hs.quat4[4 * i + 2] = q.z;
+    hs.quat4[4 * i + 3] = q.w;
+  } else {
+    hs.pos3[3 * i] = p.x; hs.pos3[3 * i + 1] = p.y; hs.pos3[3 * i + 2] = p.z;
+  }
   hs.vel3[3 * i] = v.x; hs.vel3[3 * i + 1] = v.y; hs.vel3[3 * i + 2] = v.z;
   hs.avel3[3 * i] = w.x; hs.avel3[3 * i + 1] = w.y; hs.avel3[3 * i + 2] = w.z;
   hs.type[i] = (uint32_t)__float_as_int(v.w);
@@ -723,14 +575,15 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
 }
 
 void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,
-                       const StateBuf& s, int* pid_dst, int* lift_dst, int n, cudaStream_t st) {
+                       const StateBuf& s, int* pid_dst, int* lift_dst, float4* ornt_dst,
+                       bool has_ornt, int n, cudaStream_t st) {
   k_pack_state<<<blocks(n), kThreads, 0, st>>>(dp, hs, has_vel ? 1 : 0, has_avel ? 1 : 0, s,
-                                               pid_dst, lift_dst, n);
+                                               pid_dst, lift_dst, ornt_dst, has_ornt ? 1 : 0, n);
 }
 
-void launch_unpack_state(const HostStage& hs, const StateBuf& s, const int* pid_src, int n,
-                         cudaStream_t st) {
-  k_unpack_state<<<blocks(n), kThreads, 0, st>>>(hs, s, pid_src, n);
+void launch_unpack_state(const SimParams* dp, const HostStage& hs, const StateBuf& s,
+                         const int* pid_src, const float4* ornt_src, int n, cudaStream_t st) {
+  k_unpack_state<<<blocks(n), kThreads, 0, st>>>(dp, hs, s, pid_src, ornt_src, n);
 }
 
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,

@@ -15,7 +15,8 @@ struct StateBuf {
 // copies, selected by the parity of StepCtl::epoch (the re-sort count).
 struct OrderBuf {
   int* pid[2];
-  int* lift[2];   // volume-object contact type (Contact_Info.cont_type)
+  int* lift[2];      // volume-object contact type (Contact_Info.cont_type)
+  float4* ornt[2];   // polyhedra: orientation (w, x, y, z); null for spheres
 };
 
 struct ForceCapture {   // optional per-particle force dump (parity tests)
@@ -60,6 +61,7 @@ struct WallGrid {       // per-cell candidate wall ops (CSR), optional
 // velocity is non-zero.
 struct HostStage {
   float* pos3;
+  float* quat4;   // polyhedra: (w, x, y, z) per particle
   float* vel3;
   float* avel3;
   uint32_t* type;
@@ -87,11 +89,14 @@ void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_he
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
 
 // AoS stage -> SoA float4 state (radius from the particle type, type bits in
-// vel4.w), P_ID into `pid_dst`, volume-object history reset to -1.
+// vel4.w), P_ID into `pid_dst`, volume-object history reset to -1, and for
+// polyhedra the orientation into `ornt_dst` (identity when none is given).
 void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,
-                       const StateBuf& s, int* pid_dst, int* lift_dst, int n, cudaStream_t st);
-// SoA float4 state -> AoS stage (the inverse of launch_pack_state).
-void launch_unpack_state(const HostStage& hs, const StateBuf& s, const int* pid_src, int n,
-                         cudaStream_t st);
+                       const StateBuf& s, int* pid_dst, int* lift_dst, float4* ornt_dst,
+                       bool has_ornt, int n, cudaStream_t st);
+// SoA float4 state -> AoS stage (the inverse of launch_pack_state; polyhedron
+// positions come back relative to the object file's origin).
+void launch_unpack_state(const SimParams* dp, const HostStage& hs, const StateBuf& s,
+                         const int* pid_src, const float4* ornt_src, int n, cudaStream_t st);
 
 }  // namespace blaze

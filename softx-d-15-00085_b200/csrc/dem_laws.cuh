@@ -1,0 +1,184 @@
+// dem_laws.cuh -- the reference's contact laws and point-in-polygon test as
+// FP32 device functions, shared by the sphere and polyhedron step kernels.
+// Every expression keeps the reference's operation order (the translation
+// units that include this file are compiled with -fmad=false).
+#pragma once
+
+#include "dem_common.cuh"
+
+namespace blaze {
+
+struct Forces { float3 trans, torque; };
+
+// Collision_Response_Particle_Particle, Collision_Response.cuh:374-494
+// (energy tallies excluded).  kSpin = false is the spin-free form used when
+// rotation is off and every angular velocity is exactly zero: then
+// v + cross(0, R) equals v up to the sign of an exact zero, so the forces
+// are the same numbers.
+template <bool kSpin>
+__device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
+                                         float3 ra, float3 rb, float3 wa, float3 wb,
+                                         const PP_Parms& pp, float3 va, float3 vb, float ma,
+                                         float mb) {
+  Forces F;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = pp.Kn * pen;
+  const float3 fdiss = pp.Cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 vcpa = kSpin ? va + cross3(wa, ra) : va;
+  const float3 vcpb = kSpin ? vb + cross3(wb, rb) : vb;
+  const float3 vcpna = dot3(vcpa, n) * n;
+  const float3 vcpnb = dot3(vcpb, n) * n;
+  const float3 vt = (vcpa - vcpna) - (vcpb - vcpnb);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = ((((0.50f * (ma + mb)) / P.dt) * 0.050f) * pp.Fric_kinetic) * (mag / velf);
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = (kSpin && P.rotation) ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109
+__device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 pvel, float3 n,
+                                                     float pen, float3 r, float3 w,
+                                                     const TypeParams& T) {
+  Forces F;
+  const float3 vn = dot3(pvel, n) * n;
+  const float fn = T.s_kn * pen;
+  const float3 fdiss = T.s_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  float3 vt = pvel - vn;
+  if (P.rotation) vt = vt + cross3(w, r);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(pvel, pvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.s_mus * (mag / velf));
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_MovingSurface, Collision_Response.cuh:116-233
+template <bool kSpin>
+__device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 n, float pen,
+                                                     float3 r, float3 w, const TypeParams& T,
+                                                     float3 va, float3 vs) {
+  Forces F;
+  const float3 rvel = va - vs;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = T.s_kn * pen;
+  const float3 fdiss = T.s_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
+  const float3 vcpna = dot3(vcpa, n) * n;
+  const float3 vt = (vcpa - vcpna) - (vs - dot3(vs, n) * n);
+  float mag = dot3(vt, vt);
+  float3 ft = f3(0.0f, 0.0f, 0.0f);
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = T.s_muk * (mag / velf);
+    ft = (((-1.0f * tan_f) * (vt / mag)) * (T.mass / P.dt)) * 0.050f;
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
+// Collision_Response_Particle_VolumeObject, Collision_Response.cuh:241-363,
+// with the zero object spin and lever the caller passes
+// (DEM_Kernels_Compute.cuh:206-216).
+template <bool kSpin>
+__device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float pen, float3 r,
+                                             float3 w, const TypeParams& T, float3 va,
+                                             float3 vobj) {
+  Forces F;
+  const float3 rvel = va - vobj;
+  const float3 vn = dot3(rvel, n) * n;
+  const float fn = T.d_kn * pen;
+  const float3 fdiss = T.d_cn * vn;
+  F.trans = fn * n - fdiss;
+  const float3 fdir = F.trans / len3(F.trans);
+  if (dot3(fdir, n) < 0) F.trans = fn * n;
+  const float3 z = f3(0.0f, 0.0f, 0.0f);
+  const float3 vcpa = kSpin ? va + cross3(w, r) : va;
+  const float3 vcpb = vobj + cross3(z, z);
+  const float3 vt = (vcpa - dot3(vcpa, n) * n) - (vcpb - dot3(vcpb, n) * n);
+  float mag = dot3(vt, vt);
+  float3 ft = z;
+  if (mag > 0.0f) {
+    mag = sqrtf(mag);
+    float velf = dot3(rvel, rvel);
+    if (velf > 0) velf = sqrtf(velf);
+    else velf = 1.0f;
+    const float tan_f = (0.050f * (T.mass / P.dt)) * (T.d_muk * (mag / velf));
+    ft = (-1.0f * tan_f) * (vt / mag);
+  }
+  F.trans = F.trans + ft;
+  F.torque = P.rotation ? cross3(r, F.trans) : z;
+  return F;
+}
+
+// Collision_Response_EndPlate_Particle, Collision_Response.cuh:504-526
+__device__ __forceinline__ float3 law_end_plate(float3 rvel, float3 n, float pen,
+                                                const TypeParams& T) {
+  const float3 vn = dot3(rvel, n) * n;
+  const float3 fdiss = T.s_cn * vn;
+  const float fn = T.s_kn * pen;
+  return fn * n - fdiss;
+}
+
+// is_PointOnSurface, Utilities.cuh:20-53
+__device__ __forceinline__ bool point_on_polygon(int nv, const float3* v, float3 pt, float sarea,
+                                                 float tol) {
+  float area = 0.0f;
+  for (int i = 0; i < nv - 1; ++i) {
+    const float3 v1 = pt - v[i];
+    const float3 v2 = pt - v[i + 1];
+    area = area + 0.500000f * len3(cross3(v1, v2));
+  }
+  const float3 v1 = pt - v[nv - 1];
+  const float3 v2 = pt - v[0];
+  area = area + 0.500000f * len3(cross3(v1, v2));
+  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
+}
+
+// is_PointOnSurface over vertices addressed through vertex_Order.
+__device__ __forceinline__ bool point_on_indexed_polygon(int nv, const float3* v, const int* order,
+                                                         float3 pt, float sarea, float tol) {
+  float area = 0.0f;
+  for (int i = 0; i < nv - 1; ++i) {
+    const float3 v1 = pt - v[order[i] & 7];
+    const float3 v2 = pt - v[order[i + 1] & 7];
+    area = area + 0.500000f * len3(cross3(v1, v2));
+  }
+  const float3 v1 = pt - v[order[nv - 1] & 7];
+  const float3 v2 = pt - v[order[0] & 7];
+  area = area + 0.500000f * len3(cross3(v1, v2));
+  return (fabsf(area - sarea) / sarea) * 100.0000f <= tol;
+}
+
+__device__ __forceinline__ float3 drum_velocity(const SimParams& P, float3 cp) {
+  return cross3(f3(0.0f, 0.0f, -P.mill_rot_vel), cp - f3(P.drum_r, P.drum_r, 0.0f));
+}
+
+}  // namespace blaze

@@ -1,0 +1,766 @@
+// poly_kernels.cu -- convex polyhedra: world-frame geometry and the fused
+// polyhedron step.
+//
+// Compiled with -fmad=false like the sphere kernels.  Every FP32 expression
+// keeps the operation order of the reference source it cites
+// (Collision_Detection_Polyhedra.cuh, Utilities.cuh,
+// DEM_Kernels_Compute.cuh:254-610 and 736-992, Integration.cuh:6-184), so
+// contacts, forces and states equal the reference's bit for bit; the one
+// exception is the half-angle sine and cosine of the quaternion update,
+// evaluated here in FP64 and rounded to FP32 (see quat_step).
+//
+// Cases the reference leaves undefined get a defined result here and raise
+// kStatusPolyUndefined:
+//   * the first vertex found inside the other polyhedron has no face whose
+//     plane has the vertex owner's centre on its outer side (the reference
+//     then reads face -1): no vertex-face contact is reported;
+//   * more than 8 vertices inside the other polyhedron (the reference's
+//     8-entry arrays overflow): every vertex is counted;
+//   * three or more vertices inside and none of the three candidate faces
+//     confirmed by the ray test (the reference returns an uninitialised depth
+//     and normal): the first candidate face is used.
+#include "poly_kernels.cuh"
+#include "dem_laws.cuh"
+
+namespace blaze {
+namespace {
+
+constexpr int kThreads = 128;
+
+// collision classes of CollData (GPU_Memory_Transfer.cuh:41-53) that change
+// what the step does with a contact
+enum ContactClass : int { kNoContact = 0, kVertexFace = 1, kEdgeFace = 2, kFaceFace = 3 };
+
+struct Hit {
+  bool hit;
+  int cls;
+  float dis;
+  float3 cp, n;
+};
+
+__device__ __forceinline__ Hit no_hit() {
+  Hit h;
+  h.hit = false;
+  h.cls = kNoContact;
+  h.dis = 0.0f;
+  h.cp = f3(0.0f, 0.0f, 0.0f);
+  h.n = f3(0.0f, 0.0f, 0.0f);
+  return h;
+}
+
+// ---------------------------------------------------------------- quaternions
+// Quaterion is (w, x, y, z) in memory (Types.h:15-21); a float4 holds it as
+// (.x, .y, .z, .w) = (w, x, y, z).
+struct Quat { float w, x, y, z; };
+
+__device__ __forceinline__ Quat to_quat(float4 q) { return Quat{q.x, q.y, q.z, q.w}; }
+__device__ __forceinline__ float4 to_f4(Quat q) { return make_float4(q.w, q.x, q.y, q.z); }
+
+// Hamilton product, each component summed in the order of the reference's
+// operator* (Opertators.cuh:866-875).
+__device__ __forceinline__ Quat qmul(Quat a, Quat b) {
+  Quat r;
+  float t;
+  t = a.x * b.w; t = t + a.y * b.z; t = t - a.z * b.y; r.x = t + a.w * b.x;
+  t = -(a.x * b.z); t = t + a.y * b.w; t = t + a.z * b.x; r.y = t + a.w * b.y;
+  t = a.x * b.y; t = t - a.y * b.x; t = t + a.z * b.w; r.z = t + a.w * b.z;
+  t = -(a.x * b.x); t = t - a.y * b.y; t = t - a.z * b.z; r.w = t + a.w * b.w;
+  return r;
+}
+
+// q (0, v) q*, as RotatePolyhedra forms it (Utilities.cuh:420-479)
+__device__ __forceinline__ float3 rotate(Quat q, float3 v) {
+  const Quat qc{q.w, -q.x, -q.y, -q.z};
+  const Quat r = qmul(qmul(q, Quat{0.0f, v.x, v.y, v.z}), qc);
+  return f3(r.x, r.y, r.z);
+}
+
+// ------------------------------------------------------------------ geometry
+__device__ __forceinline__ float3 ld3(const float4* p) {
+  const float4 a = __ldg(p);
+  return f3(a.x, a.y, a.z);
+}
+
+// One particle's world-frame geometry.
+struct PolyRef {
+  const float4* v;      // vertices
+  const float4* fn;     // face normals
+  const float4* fc;     // face centroids
+  const PolyShape* s;   // body-frame object (face vertex order, areas, edges)
+  float3 pos;
+};
+
+// is_SP_Poly_Poly (Utilities.cuh:105-156): a face plane of `a` with the
+// centre of `b` on its outer side and every vertex of `b` strictly outside.
+__device__ bool separated_by_face(const PolyRef& a, const PolyRef& b) {
+  const int nf = a.s->nf, nv = b.s->nv;
+  for (int f = 0; f < nf; ++f) {
+    const float3 n = ld3(a.fn + f), c = ld3(a.fc + f);
+    if (!(dot3(n, b.pos - c) > 0.0f)) continue;
+    bool touching = false;
+    for (int k = 0; k < nv; ++k)
+      if (dot3(n, ld3(b.v + k) - c) <= 0.00000f) { touching = true; break; }
+    if (!touching) return true;
+  }
+  return false;
+}
+
+// Collision_Detection_Vertex_InPoly_3Faces (CDP:287-382): is `v` behind
+// every face plane of `b`, and which three faces (with the owner's centre on
+// their outer side) are nearest to it.
+struct Inside {
+  bool in;
+  int face[3];
+  float dist[3];
+};
+
+__device__ Inside vertex_inside(float3 owner, float3 v, const PolyRef& b) {
+  Inside r;
+  r.in = false;
+  r.face[0] = r.face[1] = r.face[2] = -1;
+  r.dist[0] = r.dist[1] = r.dist[2] = 10.0f;
+  const int nf = b.s->nf;
+  for (int f = 0; f < nf; ++f) {
+    const float3 n = ld3(b.fn + f), c = ld3(b.fc + f);
+    const float vd = dot3(n, v - c);
+    if (!(vd < -0.0000100f)) return r;
+    if (dot3(n, owner - c) > 0.0f) {
+      const float ad = fabsf(vd);
+      if (ad < r.dist[0]) {
+        if (r.face[0] > -1) {
+          if (r.face[1] > -1) { r.dist[2] = r.dist[1]; r.face[2] = r.face[1]; }
+          r.dist[1] = r.dist[0]; r.face[1] = r.face[0];
+        }
+        r.dist[0] = ad; r.face[0] = f;
+      } else if (ad < r.dist[1]) {
+        if (r.face[1] > -1) { r.dist[2] = r.dist[1]; r.face[2] = r.face[1]; }
+        r.dist[1] = ad; r.face[1] = f;
+      } else if (ad < r.dist[2]) {
+        r.dist[2] = ad; r.face[2] = f;
+      }
+    }
+  }
+  r.in = true;
+  return r;
+}
+
+// is_PointOnSurface (Utilities.cuh:20-53) on face k of `b`: the fan area
+// around `pt` against the face area, within tol percent.
+__device__ bool on_face(const PolyRef& b, int k, float3 pt, float tol) {
+  const int nv = b.s->fnv[k];
+  const uint8_t* o = b.s->ford[k];
+  float area = 0.000000f;
+  for (int i = 0; i < nv - 1; ++i) {
+    const float3 v1 = pt - ld3(b.v + o[i]);
+    const float3 v2 = pt - ld3(b.v + o[i + 1]);
+    area = area + 0.500000f * len3(cross3(v1, v2));
+  }
+  const float3 v1 = pt - ld3(b.v + o[nv - 1]);
+  const float3 v2 = pt - ld3(b.v + o[0]);
+  area = area + 0.500000f * len3(cross3(v1, v2));
+  const float sa = b.s->farea[k];
+  return (fabsf(area - sa) / sa) * 100.0000f <= tol;
+}
+
+// The ray from `from` through `to`, cut with the plane of face k of `b`:
+// does the cut point lie on the face (CDP:1233-1258, repeated for every
+// candidate face)?
+__device__ bool ray_meets_face(const PolyRef& b, int k, float3 from, float3 to, float tol) {
+  float3 ray = to - from;
+  const float len = len3(ray);
+  ray = f3(ray.x / len, ray.y / len, ray.z / len);
+  const float3 n = ld3(b.fn + k), c = ld3(b.fc + k);
+  const float dir = dot3(ray, n);
+  if (!(fabsf(dir) > 0.0f)) return false;
+  const float d = dot3(c - from, n) / dir;
+  return on_face(b, k, from + d * ray, tol);
+}
+
+// Collision_Detection_Polyhedara_Polyhedra_VertexFaces (CDP:1154-1630):
+// vertices of `a` inside `b`.  One vertex: vertex-face contact on the nearest
+// face the ray from a's centre confirms; two: edge-face at their midpoint;
+// more: face-face at their mean.
+__device__ Hit vertex_face(const PolyRef& a, const PolyRef& b, uint32_t& st) {
+  Hit h = no_hit();
+  int count = 0, i0 = -1, i1 = -1, s1_face1 = -1;
+  Inside s0;
+  s0.in = false;
+  float3 sum = f3(0.0f, 0.0f, 0.0f);
+  const int nv = a.s->nv;
+  for (int k = 0; k < nv; ++k) {
+    const float3 v = ld3(a.v + k);
+    const Inside t = vertex_inside(a.pos, v, b);
+    if (!t.in) continue;
+    if (count == 0) { s0 = t; i0 = k; }
+    else if (count == 1) { s1_face1 = t.face[1]; i1 = k; }
+    sum = sum + v;
+    ++count;
+  }
+  if (count == 0) return h;
+  if (count > 8 || s0.face[0] < 0) st |= kStatusPolyUndefined;
+  if (s0.face[0] < 0) return h;
+  h.hit = true;
+  const float3 va0 = ld3(a.v + i0);
+  const int f0 = s0.face[0];
+  if (count == 1) {
+    h.cls = kVertexFace;
+    h.dis = s0.dist[0];
+    h.n = ld3(b.fn + f0);
+    h.cp = va0;
+    if (s0.face[1] == -1) return h;
+    if (ray_meets_face(b, f0, a.pos, va0, 0.10f)) return h;
+    for (int s = 1; s < 3; ++s) {
+      const int fs = s0.face[s];
+      if (fs > -1 && ray_meets_face(b, fs, a.pos, va0, 0.10f)) {
+        h.n = ld3(b.fn + fs);
+        h.dis = s0.dist[s];
+        return h;
+      }
+    }
+    return h;  // the reference warns and keeps the nearest face
+  }
+  if (count == 2) {
+    h.cls = kEdgeFace;
+    h.cp = (va0 + ld3(a.v + i1)) * 0.50f;
+    h.n = ld3(b.fn + f0);
+    h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + f0)));
+    if (s0.face[1] == -1 && s1_face1 == -1) return h;
+    for (int s = 0; s < 3; ++s) {
+      const int fs = s0.face[s];
+      if ((s == 0 || fs > -1) && ray_meets_face(b, fs, a.pos, h.cp, 0.10f)) {
+        h.n = ld3(b.fn + fs);
+        h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fs)));
+        return h;
+      }
+    }
+    h.n = ld3(b.fn + f0);
+    h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + f0)));
+    return h;  // the reference warns and keeps the nearest face
+  }
+  h.cls = kFaceFace;
+  h.cp = sum / (float)count;
+  const float tol[3] = {0.10f, 0.010f, 0.10f};
+  for (int s = 0; s < 3; ++s) {
+    const int fs = s0.face[s];
+    if ((s == 0 || fs > -1) && ray_meets_face(b, fs, a.pos, h.cp, tol[s])) {
+      h.n = ld3(b.fn + fs);
+      h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fs)));
+      return h;
+    }
+  }
+  st |= kStatusPolyUndefined;
+  h.n = ld3(b.fn + f0);
+  h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + f0)));
+  return h;
+}
+
+// isPointinPoly (Utilities.cuh:60-98)
+__device__ bool point_in_poly(const PolyRef& b, float3 pt) {
+  const int nf = b.s->nf;
+  for (int f = 0; f < nf; ++f)
+    if (!(dot3(ld3(b.fn + f), pt - ld3(b.fc + f)) <= 0.000100f)) return false;
+  return true;
+}
+
+// Collision_Detection_Polyhedra_Polyhedra_Edges (CDP:537-707): the closest
+// pair of points between an edge of `a` and an edge of `b` (parameters
+// within [-0.01, 1.01]), normal along the edges' cross product turned
+// towards `relpos`.
+__device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos) {
+  Hit h = no_hit();
+  float best = 5.0f;
+  bool found = false;
+  float3 nrm = f3(0.0f, 0.0f, 0.0f), qa_sel = nrm, qb_sel = nrm;
+  const int nea = a.s->ne, neb = b.s->ne;
+  for (int i = 0; i < nea; ++i) {
+    const float3 ap = ld3(a.v + a.s->edge[i][0]);
+    const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
+    const float daa = dot3(ad, ad);
+    for (int j = 0; j < neb; ++j) {
+      const float3 bp = ld3(b.v + b.s->edge[j][0]);
+      const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
+      const float3 c = cross3(ad, bd);
+      if (!(dot3(c, c) > 0.00000f)) continue;
+      const float3 dv = ap - bp;
+      const float dbb = dot3(bd, bd);
+      const float dab = dot3(ad, bd);
+      const float dav = dot3(ad, dv);
+      const float dbv = dot3(bd, dv);
+      const float inv = 1.00000f / (dab * dab - daa * dbb);
+      const float ta = inv * (dbb * dav - dab * dbv);
+      if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
+      const float tb = inv * (dab * dav - daa * dbv);
+      if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
+      const float3 qa = ap + ad * ta;
+      const float3 qb = bp + bd * tb;
+      const float3 d = qa - qb;
+      float dist = dot3(d, d);
+      if (!(dist > 0.00000f)) continue;
+      dist = sqrtf(dist);
+      if (dist < best) {
+        found = true;
+        best = dist;
+        nrm = c;
+        qa_sel = qa;
+        qb_sel = qb;
+      }
+    }
+  }
+  if (!found) return h;
+  nrm = nrm * (1.0f / len3(nrm));
+  if (len3(b.pos - qb_sel) < len3(b.pos - qa_sel) && !point_in_poly(b, qa_sel)) return h;
+  h.hit = true;
+  h.cls = kNoContact;  // edge-edge: no class the step treats specially
+  const float s = dot3(relpos, nrm);
+  if (fabsf(s) > 0.0f) {
+    nrm = (s / fabsf(s)) * nrm;
+    h.cp = qa_sel;
+  } else {
+    nrm = relpos / len3(relpos);
+    h.cp = b.pos;
+  }
+  h.n = nrm;
+  h.dis = fabsf(dot3(nrm, qb_sel - qa_sel)) + 0.000010f;
+  return h;
+}
+
+// Narrow phase of one pair (DEM_Kernels_Compute.cuh:818-931): separating
+// face planes either way, vertices of A in B, vertices of B in A (normal
+// reversed), edge-edge (depth capped at 0.025 r_A).
+__device__ Hit pair_contact(const PolyRef& A, const PolyRef& B, float ra, float3 relpos,
+                            uint32_t& st) {
+  Hit h = no_hit();
+  if (separated_by_face(A, B) || separated_by_face(B, A)) return h;
+  h = vertex_face(A, B, st);
+  if (h.hit) return h;
+  h = vertex_face(B, A, st);
+  h.n = h.n * -1.0f;
+  if (h.hit) return h;
+  h = edge_edge(A, B, relpos);
+  if (h.hit) h.dis = fminf(0.025f * ra, h.dis);
+  return h;
+}
+
+// ------------------------------------------------------------- world objects
+// Collision_Detection_Polyhedra_Surface + _Vertcies_Surface (CDP:85-177,
+// 489-529): the centre within the bounding radius on the face's outer side,
+// then the vertices behind the face plane whose projection lies on the face.
+__device__ Hit poly_surface(const WallOp& op, const PolyRef& a, float bound_r) {
+  Hit h = no_hit();
+  if (!(dot3(op.n, a.pos - op.c) > 0.000000f)) return h;
+  if (!(dot3(op.n, a.pos - op.c) <= bound_r)) return h;
+  int count = 0;
+  float dmax = 0.0f;
+  bool any = false;
+  float3 cp = f3(0.0f, 0.0f, 0.0f);
+  const int nv = a.s->nv;
+  for (int k = 0; k < nv; ++k) {
+    const float3 v = ld3(a.v + k);
+    const float vd = dot3(op.n, v - op.c);
+    if (!(vd < 0.000000f)) continue;
+    const float3 hp = v + fabsf(vd) * op.n;
+    if (!point_on_polygon(op.nv, op.v, hp, op.area, op.tol)) continue;
+    ++count;
+    cp = cp + hp;
+    if (fabsf(vd) > dmax) {
+      any = true;
+      dmax = fabsf(vd);
+    }
+    if (count > 2) {  // face on face: no moment, contact at the centre
+      h.hit = true; h.cls = kFaceFace; h.n = op.n; h.dis = dmax; h.cp = a.pos;
+      return h;
+    }
+  }
+  if (!any) return h;
+  h.hit = true;
+  h.cls = count == 1 ? kVertexFace : kEdgeFace;
+  h.n = op.n;
+  h.dis = dmax;
+  h.cp = cp / (float)count;
+  return h;
+}
+
+// Collision_Detection_Polyhedra_Cylinder (CDP:2010-2132): vertices beyond
+// the drum radius; depth = their mean radial excess (the reference scales by
+// a double reciprocal of the count), face-face capped at 0.001.
+__device__ Hit poly_cylinder(const WallOp& op, const PolyRef& a, float bound_r) {
+  Hit h = no_hit();
+  const float3 pv = vmul(a.pos, op.axis) - op.cbot;
+  if (!(len3(pv) + bound_r > op.radius)) return h;
+  float dis = 0.0f;
+  int count = 0;
+  float3 sp = f3(0.0f, 0.0f, 0.0f);
+  float3 nrm = f3(-pv.x, -pv.y, -pv.z);
+  nrm = nrm * (1.0f / len3(nrm));
+  const int nv = a.s->nv;
+  for (int k = 0; k < nv; ++k) {
+    const float3 v = ld3(a.v + k);
+    const float rc = len3(vmul(v, op.axis) - op.cbot);
+    if (!(rc > op.radius)) continue;
+    ++count;
+    sp = sp + v;
+    dis = dis + (rc - op.radius);
+    if (count > 2) {
+      dis = (float)((double)dis * (1.0 / (double)(float)count));
+      h.hit = true; h.cls = kFaceFace; h.n = nrm; h.dis = fminf(0.00100f, fabsf(dis));
+      h.cp = a.pos;
+      return h;
+    }
+  }
+  if (count == 0) return h;
+  h.hit = true;
+  h.n = nrm;
+  dis = (float)((double)dis * (1.0 / (double)(float)count));
+  if (count == 2) {
+    h.cls = kEdgeFace;
+    h.cp = sp / (float)count;
+    h.dis = fabsf(dis);
+  } else {
+    h.cls = kVertexFace;
+    h.cp = sp;
+    h.dis = dis;
+  }
+  return h;
+}
+
+// Collision_Detection_Vertcies_Plane (CDP:6-75), used for the drum's end
+// plates: every vertex behind the plane; depth of the deepest.
+__device__ Hit vertices_plane(const PolyRef& a, float3 n, float3 c) {
+  Hit h = no_hit();
+  int count = 0;
+  float dmax = 0.0f;
+  float3 cp = f3(0.0f, 0.0f, 0.0f);
+  const int nv = a.s->nv;
+  for (int k = 0; k < nv; ++k) {
+    const float3 v = ld3(a.v + k);
+    const float vd = dot3(n, v - c);
+    if (!(vd < 0.000000f)) continue;
+    ++count;
+    cp = cp + v;
+    if (fabsf(vd) > dmax) dmax = fabsf(vd);
+  }
+  if (count == 0) return h;
+  h.hit = true;
+  h.cls = count == 2 ? kEdgeFace : kFaceFace;  // the reference's if/else leaves one vertex as face-face
+  h.cp = cp / (float)count;
+  h.n = n;
+  h.dis = dmax;
+  return h;
+}
+
+// WorldObject_InteractionParticle for polyhedra (DEM_Kernels_Compute.cuh:
+// 254-610).  The reference keeps one contact record across the loop and
+// assigns nothing for an infinite plane (it has no polyhedron method), so a
+// plane applies the record the previous world-object step left behind.
+__device__ void poly_walls(const SimParams& P, const WallOp* __restrict__ ops, const PolyRef& A,
+                           const TypeParams& T, float3 va, float3 wa, float3& fw, float3& tw) {
+  Hit last = no_hit();
+  for (int q = 0; q < P.n_ops; ++q) {
+    const WallOp& op = ops[q];
+    if (op.kind == kOpFace || op.kind == kOpPlane) {
+      if (op.kind == kOpFace) last = poly_surface(op, A, T.radius);
+      if (!last.hit) continue;
+      Forces F;
+      if (P.rotating_wobj && P.cyl_rot)
+        F = law_moving_surface<true>(P, last.n, last.dis, last.cp - A.pos, wa, T, va,
+                                     drum_velocity(P, last.cp));
+      else
+        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T);
+      fw = fw + F.trans;
+      if (P.rotation && last.cls != kFaceFace) tw = tw + F.torque;
+    } else if (op.kind == kOpCylinder) {
+      last = poly_cylinder(op, A, T.radius);
+      if (!last.hit) continue;
+      Forces F;
+      if (P.cyl_rot)
+        F = law_moving_surface<true>(P, last.n, last.dis, last.cp - A.pos, wa, T, va,
+                                     drum_velocity(P, last.cp));
+      else
+        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T);
+      fw = F.trans;
+      if (P.rotation && last.cls != kFaceFace) tw = tw + F.torque;
+    } else {  // end plates (Collision_Response_EndPlate_Particle: no torque)
+      last = vertices_plane(A, op.n, op.c);
+      if (!last.hit) continue;
+      fw = law_end_plate(va, last.n, last.dis, T);
+      if (P.rotation) tw = tw + f3(0.0f, 0.0f, 0.0f);
+    }
+  }
+}
+
+// -------------------------------------------------------------- integration
+// Get_Angular_Acc (Utilities.cuh:486-608): I(t)^-1 tau with
+// I(t)^-1 = R(q) I0^-1 R(q)^T, sums in the reference's loop order.
+__device__ float3 angular_acc(Quat q, const float* __restrict__ I0, float3 tau) {
+  float R[9];
+  R[0] = q.w * q.w + q.x * q.x - q.y * q.y - q.z * q.z;
+  R[1] = 2.0f * q.x * q.y - 2.0f * q.w * q.z;
+  R[2] = 2.0f * q.x * q.z + 2.0f * q.w * q.y;
+  R[3] = 2.0f * q.x * q.y + 2.0f * q.w * q.z;
+  R[4] = q.w * q.w - q.x * q.x + q.y * q.y - q.z * q.z;
+  R[5] = 2.0f * q.y * q.z - 2.0f * q.w * q.x;
+  R[6] = 2.0f * q.x * q.z - 2.0f * q.w * q.y;
+  R[7] = 2.0f * q.y * q.z + 2.0f * q.w * q.x;
+  R[8] = q.w * q.w - q.x * q.x - q.y * q.y + q.z * q.z;
+  float I[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) I[k] = __ldg(I0 + k);
+  float RI[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float s = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s += R[r * 3 + k] * I[k * 3 + c];
+      RI[r * 3 + c] = s;
+    }
+  float W[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float s = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s += RI[k * 3 + c] * R[k * 3 + r];
+      W[r * 3 + c] = s;
+    }
+  const float t[3] = {tau.x, tau.y, tau.z};
+  float a[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s += W[r * 3 + k] * t[k];
+    a[r] = s;
+  }
+  return f3(a[0], a[1], a[2]);
+}
+
+// Orientation update of Integrate_Euler_NonSymmetry (Integration.cuh:
+// 132-164): dq = (cos(|w| dt / 2), sin(|w| dt / 2) w / |w|),
+// q <- normalise(dq q), or dq when that lands on w <= -1.  The reference
+// calls the FP32 cosine and sine; here both are the FP64 library functions
+// rounded to FP32 (the correctly rounded FP32 values except within ~1e-16
+// relative of a rounding boundary).  The sine's products with w / |w| are
+// exact in the reference's FP64 and rounded once, the same as FP32 products.
+__device__ float4 quat_step(float4 q4, float3 w, float dt) {
+  float mag = dot3(w, w);
+  Quat dq{1.000000f, 0.000000f, 0.000000f, 0.000000f};
+  if (mag > 0.000000f) {
+    mag = sqrtf(mag);
+    const float3 dir = w / mag;
+    const float half = 0.5000f * mag * dt;
+    dq.w = (float)cos((double)half);
+    const float s = (float)sin((double)half);
+    dq.x = s * dir.x;
+    dq.y = s * dir.y;
+    dq.z = s * dir.z;
+  }
+  const Quat p = qmul(dq, to_quat(q4));
+  const float sq = p.w * p.w + p.x * p.x + p.y * p.y + p.z * p.z;
+  const float inv = sq > 0.0f ? 1.0f / sqrtf(sq) : 0.0f;
+  const Quat qn{p.w * inv, p.x * inv, p.y * inv, p.z * inv};
+  return to_f4(qn.w <= -1.00000f ? dq : qn);
+}
+
+// ------------------------------------------------------------------- kernels
+__global__ void __launch_bounds__(kThreads)
+k_poly_geom(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
+            StateBuf in_sorted, OrderBuf ob, int rotation, const StepCtl* ctl,
+            const int* rebuilt) {
+  const int ke = g.kv > g.kf ? g.kv : g.kf;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t / ke);
+  const int e = (int)(t - (long long)i * ke);
+  if (i >= ctl->n_cur) return;
+  const StateBuf in = *rebuilt ? in_sorted : in_plain;
+  const float3 p = xyz(in.pos[i]);
+  const int ty = __float_as_int(in.vel[i].w) & (kMaxTypes - 1);
+  const PolyShape& S = shapes[ty];
+  Quat q{1.0f, 0.0f, 0.0f, 0.0f};
+  if (rotation) q = to_quat(((ctl->epoch & 1) ? ob.ornt[1] : ob.ornt[0])[i]);
+  if (e < S.nv) {
+    const float3 lv = xyz(S.vert[e]);
+    const float3 v = (rotation ? rotate(q, lv) : lv) + p;
+    g.vert[(size_t)i * g.kv + e] = make_float4(v.x, v.y, v.z, 0.0f);
+  }
+  if (e < S.nf) {
+    const float3 n = xyz(S.fnorm[e]);
+    const float3 c = xyz(S.fcent[e]);
+    const float3 nw = rotation ? rotate(q, n) : n;
+    const float3 cw = (rotation ? rotate(q, c) : c) + p;
+    g.fnorm[(size_t)i * g.kf + e] = make_float4(nw.x, nw.y, nw.z, 0.0f);
+    g.fcent[(size_t)i * g.kf + e] = make_float4(cw.x, cw.y, cw.z, 0.0f);
+  }
+}
+
+// The fused polyhedron step: Kernel_ParticleInteraction_Polyhedra_NonSymmetry
+// (DEM_Kernels_Compute.cuh:736-992), WorldObject_InteractionParticle and
+// Integrate_Euler_NonSymmetry with the quaternion update, one thread per
+// particle.  Volume objects are rejected for polyhedra by the host.
+template <bool kCapture>
+__global__ void __launch_bounds__(kThreads)
+k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
+            const WallOp* __restrict__ ops, StateBuf in_plain, StateBuf in_sorted, StateBuf out,
+            OrderBuf ob, int n_max, NbrList nl, StepCtl* ctl, StepLink link, ForceCapture cap) {
+  __shared__ TypeParams sT[kMaxTypes];
+  {
+    const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
+    const int* src = reinterpret_cast<const int*>(Pg->types);
+    int* dst = reinterpret_cast<int*>(sT);
+    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  const SimParams& P = *Pg;
+  const bool rebuilt = *link.rebuilt != 0;
+  const StateBuf in = rebuilt ? in_sorted : in_plain;
+  const int n = ctl->n_cur;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_max) return;
+  if (i >= n) {  // removed particles keep their parked state
+    out.pos[i] = in.pos[i];
+    out.vel[i] = in.vel[i];
+    out.angv[i] = in.angv[i];
+    return;
+  }
+  const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
+  const float3 pa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
+  const int ta = __float_as_int(va4.w);
+  uint32_t st = (ta < 0 || ta >= P.n_types) ? kStatusTypeRange : 0u;
+  const int tA = ta & (kMaxTypes - 1);
+  const TypeParams& TA = sT[tA];
+  const float ma = TA.mass, ra = pa4.w;
+  const PolyRef A{g.vert + (size_t)i * g.kv, g.fnorm + (size_t)i * g.kf,
+                  g.fcent + (size_t)i * g.kf, shapes + tA, pa};
+
+  // particle-particle
+  float3 f = P.gravity * ma;
+  float3 fl = f3(0.0f, 0.0f, 0.0f);
+  const int cnt = (int)nl.cnt[i];
+  for (int k = 0; k < cnt; ++k) {
+    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
+    const float4 pb4 = __ldg(in.pos + j);
+    const float3 pb = xyz(pb4);
+    if (!(len3(pa - pb) - (ra + pb4.w) < 0.0f)) continue;  // skin candidate, bounding spheres apart
+    const float4 vb4 = __ldg(in.vel + j);
+    const float3 vb = xyz(vb4), wb = xyz(__ldg(in.angv + j));
+    const int tb = __float_as_int(vb4.w);
+    const int tB = tb & (kMaxTypes - 1);
+    const PolyRef B{g.vert + (size_t)j * g.kv, g.fnorm + (size_t)j * g.kf,
+                    g.fcent + (size_t)j * g.kf, shapes + tB, pb};
+    const float3 rvel = va - vb;
+    const float3 d = pa - pb;
+    const float3 relpos = d / len3(d);
+    Hit h = pair_contact(A, B, TA.radius, relpos, st);
+    if (!h.hit) continue;
+    // depth limits of the reference (DEM_Kernels_Compute.cuh:917-950)
+    if (h.dis > 0.1500f * TA.radius) {
+      h.n = relpos / len3(relpos);
+      h.dis = 0.025f * TA.radius;
+      h.cp = pa;
+    }
+    if (h.dis > 0.0500f * TA.radius) {
+      h.n = relpos / len3(relpos);
+      h.dis = len3(rvel) > 50.0f ? 0.010f * TA.radius : 0.0030f * TA.radius;
+      h.cp = pa;
+    }
+    const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
+    const Forces F = law_pp<true>(P, rvel, h.n, h.dis, h.cp - pa, h.cp - pb, wa, wb, pp, va, vb,
+                                  ma, sT[tB].mass);
+    f = f + F.trans;
+    fl = fl + F.torque;
+  }
+  const float3 f_pp = f;
+  const float3 t_pp = P.rotation ? fl : f3(0.0f, 0.0f, 0.0f);
+
+  // world objects
+  float3 f_w = f3(0.0f, 0.0f, 0.0f), t_w = f3(0.0f, 0.0f, 0.0f);
+  poly_walls(P, ops, A, TA, va, wa, f_w, t_w);
+  if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
+  const float3 f_l = f3(0.0f, 0.0f, 0.0f), t_l = f3(0.0f, 0.0f, 0.0f);
+
+  // Integrate_Euler_NonSymmetry (Integration.cuh:6-184), polyhedra
+  float3 acc = f_w + f_pp;
+  acc = acc * (1.0f / ma);
+  float3 v = va + acc * P.dt;
+  const float3 p = pa + v * P.dt;
+  if (P.mode2d) v.z = 0.0f;
+  const float3 tl = t_pp + t_w;
+  float3 w = wa;
+  if (P.rotation) {
+    float4* qarr = (ctl->epoch & 1) ? ob.ornt[1] : ob.ornt[0];
+    const float4 q0 = qarr[i];
+    if (dot3(tl, tl) > 0.0f) {
+      const float3 aa = angular_acc(to_quat(q0), shapes[tA].inertia, tl);
+      w = w + aa * P.dt;
+      w = w - w * P.roll_res;
+    }
+    float4 q1 = quat_step(q0, w, P.dt);
+    if (P.mode2d) { q1.y = 0.0f; q1.z = 0.0f; }  // x and y of (w, x, y, z)
+    qarr[i] = q1;
+    if (P.mode2d) { w.x = 0.0f; w.y = 0.0f; }
+  }
+  float path = wa4.w;
+  if (P.skin > 0.0f) path = path + len3(v) * P.dt;
+  out.pos[i] = make_float4(p.x, p.y, p.z, ra);
+  out.vel[i] = make_float4(v.x, v.y, v.z, va4.w);
+  out.angv[i] = make_float4(w.x, w.y, w.z, path);
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
+
+  // Verlet-list validity on the bounding spheres, as for spheres
+  {
+    const unsigned m = __activemask();
+    const bool need = P.skin <= 0.0f || path > 0.5f * P.skin;
+    const unsigned b = __ballot_sync(m, need);
+    if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) {
+      if (link.has_next_h) cudaGraphSetConditional(link.next_h, 1u);
+      else atomicExch(&ctl->rebuild_req, 1);
+    }
+  }
+  {  // one atomic per warp
+    const unsigned m = __activemask();
+    const uint32_t all = __reduce_or_sync(m, st);
+    if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
+  }
+
+  if (kCapture) {
+    const float3 vals[6] = {f_pp, t_pp, f_w, t_w, f_l, t_l};
+    float* dsts[6] = {cap.f_pp, cap.t_pp, cap.f_w, cap.t_w, cap.f_l, cap.t_l};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      dsts[q][3 * i] = vals[q].x;
+      dsts[q][3 * i + 1] = vals[q].y;
+      dsts[q][3 * i + 2] = vals[q].z;
+    }
+  }
+}
+
+inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+
+void launch_poly_geom(const PolyShape* shapes, PolyGeom g, const StateBuf& in_plain,
+                      const StateBuf& in_sorted, const OrderBuf& ob, int n_max, int rotation,
+                      const StepCtl* ctl, const int* rebuilt, cudaStream_t st) {
+  const long long ke = g.kv > g.kf ? g.kv : g.kf;
+  k_poly_geom<<<blocks_for((long long)n_max * ke), kThreads, 0, st>>>(shapes, g, in_plain,
+                                                                       in_sorted, ob, rotation,
+                                                                       ctl, rebuilt);
+}
+
+void launch_poly_step(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
+                      const WallOp* ops, const StateBuf& in_plain, const StateBuf& in_sorted,
+                      const StateBuf& out, const OrderBuf& ob, int n_max, NbrList nl,
+                      StepCtl* ctl, StepLink link, const ForceCapture* cap, cudaStream_t st) {
+  const ForceCapture c = cap ? *cap : ForceCapture{};
+  const int gr = blocks_for(n_max);
+  if (cap)
+    k_poly_step<true><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
+                                               n_max, nl, ctl, link, c);
+  else
+    k_poly_step<false><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
+                                                n_max, nl, ctl, link, c);
+}
+
+}  // namespace blaze

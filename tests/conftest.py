@@ -42,22 +42,32 @@ class Golden:
 
     def init(self):
         z = self.z
-        return dict(pos=z["init_pos"], vel=z["init_vel"], avel=z["init_avel"],
-                    type=z["init_type"], pid=z["init_pid"])
+        out = dict(pos=z["init_pos"], vel=z["init_vel"], avel=z["init_avel"],
+                   type=z["init_type"], pid=z["init_pid"])
+        if "init_quat" in z.files:
+            out["quat"] = z["init_quat"]
+        return out
 
     def at(self, k):
         z = self.z
-        out = {key: z["s%d_%s" % (k, key)] for key in
-               ("pos", "vel", "avel", "type", "pid", "f_pp", "t_pp", "f_wall", "t_wall",
-                "f_lift", "t_lift", "nn", "list")}
-        return out
+        keys = ["pos", "vel", "avel", "type", "pid", "f_pp", "t_pp", "f_wall", "t_wall",
+                "f_lift", "t_lift", "nn", "list"]
+        if "s%d_quat" % k in z.files:
+            keys.append("quat")
+        return {key: z["s%d_%s" % (k, key)] for key in keys}
 
 
 GOLDEN_NAMES = ["silo_sph90", "mill_sph30"]
+POLY_GOLDEN_NAMES = ["box_poly"]
 
 
 @pytest.fixture(params=GOLDEN_NAMES)
 def golden(request):
+    return Golden(request.param)
+
+
+@pytest.fixture(params=POLY_GOLDEN_NAMES)
+def golden_poly(request):
     return Golden(request.param)
 
 

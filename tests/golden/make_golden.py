@@ -5,7 +5,7 @@ DEM kernels compiled as host C++, oracle/_ref/libblaze_refhost.so).
 Run in a container that has the reference tree (its path is the first
 argument, default /root/reference) after `make -C oracle ref`:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [fixture ...]
 
 Each fixture is an .npz with
   wobj, pobj, dobj, sim_info   raw bytes of the boundary structs as this
@@ -16,6 +16,8 @@ Each fixture is an .npz with
   s{K}_*                       oracle A after K steps: pos, vel, avel, type,
                                pid, the force arrays of step K before
                                integration, and the contact list of step K
+Polyhedron fixtures add init_quat / s{K}_quat (w, x, y, z); their positions
+are the reference's outputs (pos - COM), their inputs centres of mass.
 """
 import ctypes as C
 import os
@@ -81,10 +83,95 @@ def make(ref_root, name, project, world, cyl_rot):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def random_quaternions(rng, n):
+    """Uniformly distributed unit quaternions (w, x, y, z), w >= 0."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q[q[:, 0] < 0] *= -1.0
+    return q.astype(np.float32)
+
+
+# (fixture name, project, world, particles, lattice spacing cm, seed)
+POLY_FIXTURES = [
+    ("box_poly", "1.Particles_Box", "Poly_128cm", 1440, 0.93, 7),
+]
+POLY_CHECKPOINTS = (1, 2, 10, 50)
+
+
+def make_poly(ref_root, name, project, world, n, spacing, seed):
+    """Dodecahedra of the project's own object file on a jittered lattice
+    just above the floor of its container, random orientations and
+    velocities, so the first steps hold vertex-face, edge-face, face-face and
+    edge-edge contacts between particles and with the floor.  The particle
+    count replaces the world file's (8,192, lattice-filled and falling for
+    thousands of steps before the first contact)."""
+    projects = os.path.join(ref_root, "Projects")
+    P = Project.load(projects, project, world)
+    rp, w, p, d = RefHost.parse_isolated(projects, project, world)
+    assert canon.pobj_poly(p[0], 1) == canon.pobj_poly(
+        _unscaled(P.pobj[0], p[0]), 1), "project mirror differs from the reference parser"
+    P.sim_info.Num_Particles = n
+    P.per_object[0] = n
+    rng = np.random.default_rng(seed)
+    nx = nz = 12
+    ny = (n + nx * nz - 1) // (nx * nz)
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
+                 axis=-1).reshape(-1, 3)[:n]
+    r_b = float(P.pobj[0].radius)
+    base = np.array([60.0, 0.94 * r_b, 60.0])
+    pos = (base + g * spacing + rng.uniform(-0.02, 0.02, size=(n, 3))).astype(np.float32)
+    quat = random_quaternions(rng, n)
+    vel = rng.normal(scale=10.0, size=(n, 3)).astype(np.float32)
+    avel = rng.normal(scale=20.0, size=(n, 3)).astype(np.float32)
+    ptype = np.zeros(n, np.uint32)
+    pid = np.arange(n, dtype=np.int32)
+    R = RefHost()
+    R.init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=8, capture=True)
+    R.set_state(pos, vel, avel, ptype, pid, quat=quat)
+    out = dict(
+        wobj=np.frombuffer(bytes(P.wobj), np.uint8), pobj=np.frombuffer(bytes(P.pobj), np.uint8),
+        dobj=np.frombuffer(bytes(P.dobj), np.uint8),
+        sim_info=np.frombuffer(bytes(P.sim_info), np.uint8),
+        n_w=P.n_w, n_p=P.n_p, n_d=P.n_d, cyl_rot=0,
+        init_pos=pos, init_vel=vel, init_avel=avel, init_quat=quat, init_type=ptype,
+        init_pid=pid, source="%s/World/%s.World, %d particles, seed %d" % (project, world, n, seed))
+    done = 0
+    for k in POLY_CHECKPOINTS:
+        rc = R.step(k - done)
+        assert rc == 0, rc
+        done = k
+        s = R.state()
+        f = R.forces()
+        nn, lst = R.nlist()
+        for key in ("pos", "quat", "vel", "avel", "type", "pid"):
+            out["s%d_%s" % (k, key)] = s[key]
+        for key, v in f.items():
+            out["s%d_%s" % (k, key)] = v
+        out["s%d_nn" % k] = nn
+        out["s%d_list" % k] = lst[:, :max(1, int(nn.max()))]
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def _unscaled(mine, ref):
+    """The mirror's object with the parser's inertia tensor (the run setup
+    scales it afterwards; the scaling has its own test)."""
+    c = type(mine).from_buffer_copy(bytes(mine))
+    for g in range(9):
+        c.InertiaT[g] = ref.InertiaT[g]
+    return c
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    which = sys.argv[2:] or None
     for name, project, world, rot in FIXTURES:
-        make(ref_root, name, project, world, rot)
+        if which is None or name in which:
+            make(ref_root, name, project, world, rot)
+    for name, project, world, n, spacing, seed in POLY_FIXTURES:
+        if which is None or name in which:
+            make_poly(ref_root, name, project, world, n, spacing, seed)
 
 
 if __name__ == "__main__":

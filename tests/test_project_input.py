@@ -15,6 +15,9 @@ REF_PROJECTS = "/root/reference/Projects"
 need_ref_tree = pytest.mark.skipif(not os.path.isdir(REF_PROJECTS),
                                    reason="reference project tree not present")
 need_ref_lib = pytest.mark.skipif(not bindings.ref_available(), reason="oracle/_ref not built")
+need_ref_parse = pytest.mark.skipif(
+    not os.path.isfile(os.path.join(os.path.dirname(bindings.REF_SO), "refparse")),
+    reason="oracle/_ref/refparse not built")
 
 
 @need_ref_lib
@@ -42,6 +45,33 @@ def test_parser_matches_reference(project, world):
     assert np.float32(rp.delta_t) == P.delta_t
     assert (rp.grid_size.x, rp.grid_size.y, rp.grid_size.z) == tuple(float(v) for v in P.grid_size)
 
+
+
+@need_ref_parse
+@need_ref_tree
+@pytest.mark.parametrize("project,world", [("1.Particles_Box", "Poly_128cm"),
+                                           ("4.UnitTests", "2P")])
+def test_polyhedron_parser_matches_reference(project, world):
+    """ReadPObject_Poly: the dodecahedron (Format 1: offset vertices,
+    comma-separated faces) and the cube (Format 0), field by field; the
+    run setup's inertia scaling (main.cpp:622-626) on top of the parser's
+    inverted tensor."""
+    rp, w, p, d = bindings.RefHost.parse_isolated(REF_PROJECTS, project, world)
+    P = Project.load(REF_PROJECTS, project, world)
+    assert P.particle_type == 1 and rp.particle_type == 1
+    for i in range(rp.n_p):
+        ref = p[i]
+        mine = T.POBJ.from_buffer_copy(bytes(P.pobj[i]))
+        scale = np.float32(np.float32(1.0) / np.float32(np.float32(np.float32(
+            np.float32(0.4) * np.float32(ref.radius)) * np.float32(ref.radius)) *
+            np.float32(ref.mass)))
+        for g in range(9):
+            expect = np.float32(scale * np.float32(ref.InertiaT[g]))
+            assert np.float32(mine.InertiaT[g]) == expect, (i, g)
+            mine.InertiaT[g] = ref.InertiaT[g]
+        assert canon.pobj_poly(ref, rp.n_p) == canon.pobj_poly(mine, P.n_p), i
+    for i in range(rp.n_w):
+        assert canon.wobj(w[i]) == canon.wobj(P.wobj[i])
 
 @need_ref_tree
 def test_state_file_spec4_silo():
