@@ -21,7 +21,10 @@ are the reference's outputs (pos - COM), their inputs centres of mass.
 """
 import ctypes as C
 import os
+import re
+import shutil
 import sys
+import tempfile
 
 import numpy as np
 
@@ -154,6 +157,102 @@ def make_poly(ref_root, name, project, world, n, spacing, seed):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def poly_drum_project(ref_root, dst, n):
+    """A polyhedron project assembled from the reference's own pieces: the
+    90 cm mill drum with both end plates (3.BallMill Drum90cm.WOBJ) filled
+    with the dodecahedron of 1.Particles_Box (Poly_1cm.POBJ), the world file
+    of Mill_SPH30 with particle type 1, n particles, no lifters and 1 cm
+    cells.
+    Returns (projects root, project, world)."""
+    src = os.path.join(ref_root, "Projects")
+    proj = os.path.join(dst, "Projects", "MillPoly")
+    for sub in ("World", "SurfaceObjects", "ParticleObjects", "LifterObjects"):
+        os.makedirs(os.path.join(proj, sub), exist_ok=True)
+    shutil.copy(os.path.join(src, "3.BallMill", "SurfaceObjects", "Drum90cm.WOBJ"),
+                os.path.join(proj, "SurfaceObjects"))
+    shutil.copy(os.path.join(src, "1.Particles_Box", "ParticleObjects", "Poly_1cm.POBJ"),
+                os.path.join(proj, "ParticleObjects"))
+    text = open(os.path.join(src, "3.BallMill", "World", "Mill_SPH30.World")).read()
+    reps = [("Particle_Type(0=sphere,1=poly,2=mixed): 0", "Particle_Type(0=sphere,1=poly,2=mixed): 1"),
+            ("1 Ball_5cm  242", "1 Poly_1cm  %d" % n),
+            ("Num_Particles:    242", "Num_Particles:    %d" % n),
+            ("Cell_Size:     5.0   5.0    5.0", "Cell_Size:     1.0   1.0    1.0")]
+    for a, b in reps:
+        assert a in text, a
+        text = text.replace(a, b)
+    text, k = re.subn(r"Number: 1 Repeat: 8\s+1 Square_Lifter16", "Number: 0 Repeat: 0", text)
+    assert k == 1
+    open(os.path.join(proj, "World", "Mill_POLY.World"), "w").write(text)
+    return os.path.join(dst, "Projects"), "MillPoly", "Mill_POLY"
+
+
+def make_poly_drum(ref_root, name, n, seed):
+    """Dodecahedra in the bottom of the rotating mill drum: drum wall
+    (moving-surface law), both end plates, particle contacts."""
+    tmp = tempfile.mkdtemp(prefix="blaze_polydrum_")
+    try:
+        projects, project, world = poly_drum_project(ref_root, tmp, n)
+        P = Project.load(projects, project, world)
+        rp, w, p, d = RefHost.parse_isolated(projects, project, world)
+        assert canon.pobj_poly(p[0], 1) == canon.pobj_poly(_unscaled(P.pobj[0], p[0]), 1)
+        assert canon.wobj(w[0]) == canon.wobj(P.wobj[0])
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    rng = np.random.default_rng(seed)
+    cyl = P.wobj[0].cyl_geo
+    R = float(cyl.radius)
+    cx, cy = float(cyl.center_bot_cap.x), float(cyl.center_bot_cap.y)
+    H = float(cyl.height)
+    r_b = float(P.pobj[0].radius)
+    sp = 0.93
+    cand = []
+    # rings about the drum axis from the wall inwards, in the lowest 40
+    # degrees of arc, the outer ring close enough for vertices to reach the
+    # wall; z layers between the end plates
+    for ring in range(12):
+        rad = R - 0.91 * r_b - ring * sp
+        dth = sp / rad
+        for th in np.arange(-0.35, 0.35, dth):
+            for z in np.arange(0.94 * r_b, H - 0.94 * r_b, sp):
+                cand.append((cx + rad * np.sin(th), cy - rad * np.cos(th), z))
+    pos = np.array(cand[:n])
+    assert len(pos) == n
+    pos = (pos + rng.uniform(-0.02, 0.02, size=pos.shape)).astype(np.float32)
+    quat = random_quaternions(rng, n)
+    vel = rng.normal(scale=10.0, size=(n, 3)).astype(np.float32)
+    avel = rng.normal(scale=20.0, size=(n, 3)).astype(np.float32)
+    ptype = np.zeros(n, np.uint32)
+    pid = np.arange(n, dtype=np.int32)
+    Rh = RefHost()
+    Rh.init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=8, capture=True)
+    Rh.set_cylinder_rotation(True)
+    Rh.set_state(pos, vel, avel, ptype, pid, quat=quat)
+    out = dict(
+        wobj=np.frombuffer(bytes(P.wobj), np.uint8), pobj=np.frombuffer(bytes(P.pobj), np.uint8),
+        dobj=np.frombuffer(bytes(P.dobj), np.uint8),
+        sim_info=np.frombuffer(bytes(P.sim_info), np.uint8),
+        n_w=P.n_w, n_p=P.n_p, n_d=P.n_d, cyl_rot=1,
+        init_pos=pos, init_vel=vel, init_avel=avel, init_quat=quat, init_type=ptype,
+        init_pid=pid, source="Drum90cm.WOBJ + Poly_1cm.POBJ, %d particles, seed %d" % (n, seed))
+    done = 0
+    for k in POLY_CHECKPOINTS:
+        rc = Rh.step(k - done)
+        assert rc == 0, rc
+        done = k
+        st = Rh.state()
+        f = Rh.forces()
+        nn, lst = Rh.nlist()
+        for key in ("pos", "quat", "vel", "avel", "type", "pid"):
+            out["s%d_%s" % (k, key)] = st[key]
+        for key, v in f.items():
+            out["s%d_%s" % (k, key)] = v
+        out["s%d_nn" % k] = nn
+        out["s%d_list" % k] = lst[:, :max(1, int(nn.max()))]
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def _unscaled(mine, ref):
     """The mirror's object with the parser's inertia tensor (the run setup
     scales it afterwards; the scaling has its own test)."""
@@ -172,6 +271,8 @@ def main():
     for name, project, world, n, spacing, seed in POLY_FIXTURES:
         if which is None or name in which:
             make_poly(ref_root, name, project, world, n, spacing, seed)
+    if which is None or "drum_poly" in which:
+        make_poly_drum(ref_root, "drum_poly", 1200, 11)
 
 
 if __name__ == "__main__":

@@ -1,17 +1,25 @@
 """Convex polyhedra on the GPU through the C ABI, against the reference's own
-polyhedron kernels (oracle A fixture tests/golden/box_poly.npz: 1,440
-dodecahedra of the reference's Poly_1cm object in its Container_128 box,
-random orientations and spins, contacts of every kind from the first step).
+polyhedron kernels: the oracle-A fixtures (tests/golden/box_poly.npz, 1,440
+dodecahedra of the reference's Poly_1cm object in its Container_128 box;
+tests/golden/drum_poly.npz, 1,200 in the rotating 90 cm mill drum with end
+plates), random orientations and spins, contacts of every kind from the
+first step; and variants run against oracle A live (oracle/_ref travels with
+the repository): rotation off, 2-D mode, an infinite plane after a face.
 
 Bar: bit for bit at every checkpoint (contact lists, particle-particle and
 wall forces and torques, positions, velocities, spins, orientations).  The
 orientation update's half-angle sine and cosine are evaluated differently
 from the reference's (csrc/poly_kernels.cu, quat_step); on this fixture they
 agree with the host library's everywhere."""
+import ctypes
+
 import numpy as np
 import pytest
 
+import bindings
 from blaze import device
+from blaze import types as T
+from conftest import Golden
 
 pytestmark = pytest.mark.gpu
 
@@ -22,6 +30,7 @@ FORCE_KEYS = ("f_pp", "t_pp", "f_wall", "t_wall", "f_lift", "t_lift")
 def gpu_sim(g, **opts):
     s = device.Simulation(sim_info=g.sim_info, wobj=g.wobj, n_w=g.n_w, pobj=g.pobj, n_p=g.n_p,
                           dobj=g.dobj, n_d=g.n_d, **opts)
+    s.set_cylinder_rotation(g.cyl_rot)
     st = g.init()
     s.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
     return s
@@ -112,6 +121,7 @@ def test_poly_reference_abi(golden_poly):
     g = golden_poly
     st0 = g.init()
     kd = device.KDevice(g.wobj, g.pobj, g.dobj, g.n_w, g.n_p, g.n_d, g.sim_info, None)
+    kd.IDevice_drum_rotation(g.cyl_rot)
     pos = np.ascontiguousarray(st0["pos"], np.float32)
     quat = np.ascontiguousarray(st0["quat"], np.float32)
     vel = np.ascontiguousarray(st0["vel"], np.float32)
@@ -133,4 +143,59 @@ def test_poly_reference_abi(golden_poly):
     np.testing.assert_array_equal(out["pos"], b["pos"])
     np.testing.assert_array_equal(q, b["quat"])
     np.testing.assert_array_equal(pid, b["pid"])
+    s.close()
+
+
+need_ref_lib = pytest.mark.skipif(not bindings.ref_available(), reason="oracle/_ref not built")
+
+
+def box_variant(g, kind):
+    """The box fixture's structs with one setting changed."""
+    si = T.SimulationInfo.from_buffer_copy(bytes(g.sim_info))
+    wobj = (T.WOBJ * 8).from_buffer_copy(bytes(g.wobj))
+    n_w = g.n_w
+    if kind == "no_rotation":
+        si.Rotation = False
+    elif kind == "mode2d":
+        si.Mode2D = True
+    elif kind == "plane_after_face":
+        # a second world object: a copy of the floor face, then an infinite
+        # plane (area -1), for which the reference has no polyhedron test and
+        # re-applies the contact the floor copy left behind
+        W = wobj[1]
+        ctypes.memmove(ctypes.addressof(W), ctypes.addressof(wobj[0]), ctypes.sizeof(T.WOBJ))
+        W.num_surfaces = 2
+        W.surfaces[0] = wobj[0].surfaces[0]
+        W.surfaces[1] = wobj[0].surfaces[0]
+        W.surfaces[1].area = -1.0
+        n_w = 2
+        si.Num_WorldObjects = 2
+    return si, wobj, n_w
+
+
+@need_ref_lib
+@pytest.mark.parametrize("kind", ["no_rotation", "mode2d", "plane_after_face"])
+def test_poly_variants_vs_live_reference(kind):
+    g = Golden("box_poly")
+    si, wobj, n_w = box_variant(g, kind)
+    st0 = g.init()
+    R = bindings.RefHost()
+    R.init(si, wobj, n_w, g.pobj, g.n_p, g.dobj, g.n_d, threads=8, capture=True)
+    R.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"], quat=st0["quat"])
+    s = device.Simulation(sim_info=si, wobj=wobj, n_w=n_w, pobj=g.pobj, n_p=g.n_p, dobj=g.dobj,
+                          n_d=g.n_d, capture_forces=1)
+    s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"], quat=st0["quat"])
+    for chunk in (1, 9):
+        assert R.step(chunk) == 0
+        s.step(chunk)
+        a, b = s.state(), R.state()
+        assert a["status"] == 0, device.decode_status(a["status"])
+        np.testing.assert_array_equal(a["pid"], b["pid"])
+        for key in STATE_KEYS:
+            assert mismatches(a[key], b[key]) == 0, "%s %s" % (kind, key)
+        fa, fb = s.forces(), R.forces()
+        for key in FORCE_KEYS:
+            assert mismatches(fa[key], fb[key]) == 0, "%s %s" % (kind, key)
+        if chunk == 1:  # the first step has floor contacts to compare
+            assert int((np.abs(fb["f_wall"]).sum(axis=1) > 0).sum()) > 20
     s.close()

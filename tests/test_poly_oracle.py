@@ -17,6 +17,7 @@ def test_reference_replays_fixture(golden_poly):
     g = golden_poly
     R = bindings.RefHost()
     R.init(g.sim_info, g.wobj, g.n_w, g.pobj, g.n_p, g.dobj, g.n_d, threads=4, capture=True)
+    R.set_cylinder_rotation(g.cyl_rot)
     s0 = g.init()
     R.set_state(s0["pos"], s0["vel"], s0["avel"], s0["type"], s0["pid"], quat=s0["quat"])
     done = 0
@@ -41,6 +42,8 @@ def test_fixture_exercises_contacts(golden_poly):
     s1 = g.at(1)
     assert int((np.abs(s1["t_pp"]).sum(axis=1) > 0).sum()) > 0.3 * g.n
     assert int((np.abs(s1["f_wall"]).sum(axis=1) > 0).sum()) > 20
+    if g.cyl_rot:  # drum wall contacts carry torque (end plates do not)
+        assert int((np.abs(s1["t_wall"]).sum(axis=1) > 0).sum()) > 100
     s0 = g.init()
     order0 = np.argsort(s0["pid"])
     order1 = np.argsort(s1["pid"])
