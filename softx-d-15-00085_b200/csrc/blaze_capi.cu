@@ -152,6 +152,7 @@ void build_params(blaze_sim* s) {
     G.bound_r = D.boundR;
     G.num_faces = std::min(D.num_faces, 3);
     G.num_edges = std::min(D.num_edges, 4);
+    G.num_vertex = std::min(std::max(D.num_vertex, 0), 8);
     G.attached = D.is_attached_DWorld ? 1 : 0;
     G.translating = D.is_translating ? 1 : 0;
     G.velocity = D.velocity;
@@ -697,10 +698,6 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
     return -1;
   }
   if (si->particle_type == 1) {
-    if (n_d > 0) {
-      std::fprintf(stderr, "blaze: volume objects with polyhedral particles are not supported\n");
-      return -1;
-    }
     for (int t = 0; t < n_p; ++t)
       if (!poly_object_valid(p[t], t)) return -1;
   }

@@ -77,6 +77,7 @@ struct DobjDev {
   float3 com, axis;
   float bound_r;
   int num_faces, num_edges;
+  int num_vertex;      // vertices the polyhedron tests read (at most 8)
   int attached, translating;
   float3 velocity;
   float3 vert[8];

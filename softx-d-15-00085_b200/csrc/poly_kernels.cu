@@ -18,7 +18,13 @@
 //     8-entry arrays overflow): every vertex is counted;
 //   * three or more vertices inside and none of the three candidate faces
 //     confirmed by the ray test (the reference returns an uninitialised depth
-//     and normal): the first candidate face is used.
+//     and normal): the first candidate face is used;
+//   * against a volume object: three or more vertices inside with no face
+//     common to all of them (uninitialised depth and normal): the first
+//     vertex's nearest face; edge pairs found but none within 0.1 of each
+//     other (unset normal and points): no contact.  The per-particle contact
+//     type after a test that found nothing is 0 (the reference stores an
+//     unset value).
 #include "poly_kernels.cuh"
 #include "dem_laws.cuh"
 
@@ -341,6 +347,278 @@ __device__ Hit pair_contact(const PolyRef& A, const PolyRef& B, float ra, float3
   return h;
 }
 
+// ------------------------------------------------------------ volume objects
+// A volume object (lifter) seen from a polyhedral particle: its faces,
+// vertices and edges are world-frame already (the host moves them).
+
+// is_SP_VolumeObject_Poly / is_SP_Poly_VolumeObject (Utilities.cuh:212-318)
+__device__ bool dobject_face_separates(const DobjDev& D, const PolyRef& a) {
+  const int nv = a.s->nv;
+  for (int f = 0; f < D.num_faces; ++f) {
+    const float3 n = D.faces[f].normal, c = D.faces[f].centroid;
+    if (!(dot3(n, a.pos - c) > 0.0f)) continue;
+    bool touching = false;
+    for (int k = 0; k < nv; ++k)
+      if (dot3(n, ld3(a.v + k) - c) <= 0.00000f) { touching = true; break; }
+    if (!touching) return true;
+  }
+  return false;
+}
+
+__device__ bool particle_face_separates(const PolyRef& a, const DobjDev& D) {
+  const int nf = a.s->nf;
+  for (int f = 0; f < nf; ++f) {
+    const float3 n = ld3(a.fn + f), c = ld3(a.fc + f);
+    if (!(dot3(n, D.com - c) > 0.0f)) continue;
+    bool touching = false;
+    for (int k = 0; k < D.num_vertex; ++k)
+      if (dot3(n, D.vert[k] - c) <= 0.00000f) { touching = true; break; }
+    if (!touching) return true;
+  }
+  return false;
+}
+
+// Collision_Detection_Vertex_InDObject_3Faces (CDP:383-476): as
+// vertex_inside, with the volume object's faces and thresholds.
+__device__ Inside vertex_in_dobject(float3 owner, float3 v, const DobjDev& D) {
+  Inside r;
+  r.in = false;
+  r.face[0] = r.face[1] = r.face[2] = -1;
+  r.dist[0] = r.dist[1] = r.dist[2] = 10.0f;
+  for (int f = 0; f < D.num_faces; ++f) {
+    const float3 n = D.faces[f].normal, c = D.faces[f].centroid;
+    const float vd = dot3(n, v - c);
+    if (!(vd <= 0.000010f)) return r;
+    if (dot3(n, owner - c) > 0.0f) {
+      const float ad = fabsf(vd);
+      if (ad < r.dist[0]) {
+        if (r.face[0] > -1) {
+          if (r.face[1] > -1) { r.dist[2] = r.dist[1]; r.face[2] = r.face[1]; }
+          r.dist[1] = r.dist[0]; r.face[1] = r.face[0];
+        }
+        r.dist[0] = ad; r.face[0] = f;
+      } else if (ad < r.dist[1]) {
+        if (r.face[1] > -1) { r.dist[2] = r.dist[1]; r.face[2] = r.face[1]; }
+        r.dist[1] = ad; r.face[1] = f;
+      } else if (ad < r.dist[2]) {
+        r.dist[2] = ad; r.face[2] = f;
+      }
+    }
+  }
+  r.in = true;
+  return r;
+}
+
+__device__ bool ray_meets_dface(const DobjDev& D, int k, float3 from, float3 to, float tol) {
+  float3 ray = to - from;
+  const float len = len3(ray);
+  ray = f3(ray.x / len, ray.y / len, ray.z / len);
+  const Surface& S = D.faces[k];
+  const float dir = dot3(ray, S.normal);
+  if (!(fabsf(dir) > 0.0f)) return false;
+  const float d = dot3(S.centroid - from, S.normal) / dir;
+  const int nv = S.num_vertex < 8 ? S.num_vertex : 8;
+  return point_on_indexed_polygon(nv, D.vert, S.vertex_Order, from + d * ray, S.area, tol);
+}
+
+// Collision_Detection_Polyhedara_VolumeObject_VertexFace (CDP:1638-2002):
+// vertices of the particle inside the volume object.  Face-face contact
+// takes the face every such vertex has among its three nearest, at the
+// smallest distance any of them records.
+__device__ Hit vertex_dobject(const PolyRef& a, const DobjDev& D, uint32_t& st) {
+  Hit h = no_hit();
+  int count = 0, i0 = -1, i1 = -1, s1_face1 = -1;
+  Inside s0;
+  s0.in = false;
+  s0.face[0] = -1;
+  float3 sum = f3(0.0f, 0.0f, 0.0f);
+  int fcnt[3] = {0, 0, 0};
+  float fmin[3] = {10.0f, 10.0f, 10.0f};
+  const int nv = a.s->nv;
+  for (int k = 0; k < nv; ++k) {
+    const float3 v = ld3(a.v + k);
+    const Inside t = vertex_in_dobject(a.pos, v, D);
+    if (!t.in) continue;
+    if (count == 0) { s0 = t; i0 = k; }
+    else if (count == 1) { s1_face1 = t.face[1]; i1 = k; }
+    sum = sum + v;
+    ++count;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int f = t.face[j];
+      if (f > -1) {
+        fcnt[f]++;
+        if (t.dist[j] < fmin[f]) fmin[f] = t.dist[j];
+      }
+    }
+  }
+  if (count == 0) return h;
+  if (count > 8) st |= kStatusPolyUndefined;
+  const int f0 = s0.face[0];
+  if (count <= 2 && f0 < 0) {
+    st |= kStatusPolyUndefined;
+    return h;
+  }
+  h.hit = true;
+  const float3 va0 = ld3(a.v + i0);
+  if (count == 1) {
+    h.cls = kVertexFace;
+    h.dis = s0.dist[0];
+    h.n = D.faces[f0].normal;
+    h.cp = va0;
+    if (s0.face[1] == -1) return h;
+    if (ray_meets_dface(D, f0, a.pos, va0, 0.1f)) return h;
+    for (int s = 1; s < 3; ++s) {
+      const int fs = s0.face[s];
+      if (fs > -1 && ray_meets_dface(D, fs, a.pos, va0, 0.10f)) {
+        h.n = D.faces[fs].normal;
+        h.dis = s0.dist[s];
+        return h;
+      }
+    }
+    return h;
+  }
+  if (count == 2) {
+    h.cls = kEdgeFace;
+    h.cp = (va0 + ld3(a.v + i1)) * 0.50f;
+    h.n = D.faces[f0].normal;
+    h.dis = fabsf(dot3(h.n, h.cp - D.faces[f0].centroid));
+    if (s0.face[1] == -1 && s1_face1 == -1) return h;
+    for (int s = 0; s < 3; ++s) {
+      const int fs = s0.face[s];
+      if ((s == 0 || fs > -1) && ray_meets_dface(D, fs, a.pos, h.cp, 0.10f)) {
+        h.n = D.faces[fs].normal;
+        h.dis = fabsf(dot3(h.n, h.cp - D.faces[fs].centroid));
+        return h;
+      }
+    }
+    h.n = D.faces[f0].normal;
+    h.dis = fabsf(dot3(h.n, h.cp - D.faces[f0].centroid));
+    return h;
+  }
+  h.cls = kFaceFace;
+  h.cp = sum / (float)count;
+  for (int f = 0; f < D.num_faces; ++f)
+    if (fcnt[f] == count) {
+      h.dis = fmin[f];
+      h.n = D.faces[f].normal;
+      return h;
+    }
+  // no face common to every vertex: the reference returns an uninitialised
+  // depth and normal
+  st |= kStatusPolyUndefined;
+  if (f0 < 0) return no_hit();
+  h.dis = s0.dist[0];
+  h.n = D.faces[f0].normal;
+  return h;
+}
+
+// Collision_Detection_DObject_Polyhedra_Edges (CDP:716-897): edge pairs
+// whose closest point on the particle's edge is nearer the particle's centre
+// than the one on the volume object's; contact point their mean, normal from
+// the nearest pair (within 0.1), turned against `relpos`.
+__device__ Hit dobject_edges(const DobjDev& D, const PolyRef& b, float3 relpos, uint32_t& st) {
+  Hit h = no_hit();
+  float best = 0.10f;
+  bool found = false, chosen = false;
+  int count = 0;
+  float3 cps = f3(0.0f, 0.0f, 0.0f), nrm = cps, qa_sel = cps, qb_sel = cps;
+  const int neb = b.s->ne;
+  for (int i = 0; i < D.num_edges; ++i) {
+    const float3 ap = D.vert[D.edge0[i]];
+    const float3 ad = D.vert[D.edge1[i]] - ap;
+    const float daa = dot3(ad, ad);
+    for (int j = 0; j < neb; ++j) {
+      const float3 bp = ld3(b.v + b.s->edge[j][0]);
+      const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
+      const float3 c = cross3(ad / len3(ad), bd / len3(bd));
+      if (!(dot3(c, c) > 0.00000f)) continue;
+      const float3 dv = ap - bp;
+      const float dbb = dot3(bd, bd);
+      const float dab = dot3(ad, bd);
+      const float dav = dot3(ad, dv);
+      const float dbv = dot3(bd, dv);
+      const float inv = 1.00000f / (dab * dab - daa * dbb);
+      const float ta = inv * (dbb * dav - dab * dbv);
+      if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
+      const float tb = inv * (dab * dav - daa * dbv);
+      if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
+      const float3 qa = ap + ad * ta;
+      const float3 qb = bp + bd * tb;
+      const float3 d = qa - qb;
+      float dist = dot3(d, d);
+      if (!(dist > 0.00000f)) continue;
+      dist = sqrtf(dist);
+      if (!(len3(b.pos - qb) > len3(b.pos - qa))) continue;
+      ++count;
+      cps = cps + qa;
+      found = true;
+      if (dist <= best) {
+        best = dist;
+        nrm = cross3(ad, bd);
+        qa_sel = qa;
+        qb_sel = qb;
+        chosen = true;
+      }
+    }
+  }
+  if (!found) return h;
+  if (!chosen) {  // the reference reads an unset normal and points
+    st |= kStatusPolyUndefined;
+    return h;
+  }
+  nrm = nrm * (1.0f / len3(nrm));
+  h.hit = true;
+  h.cls = kNoContact;
+  const float s = dot3(relpos, nrm);
+  if (fabsf(s) > 0.0f) {
+    nrm = (-1.0f * (s / fabsf(s))) * nrm;
+    h.dis = fabsf(dot3(nrm, qb_sel - qa_sel));
+    h.cp = cps / (float)count;
+  } else {
+    nrm = (-1.0f * relpos) / len3(relpos);
+    h.cp = b.pos;
+    h.dis = fabsf(dot3(nrm, qb_sel - qa_sel)) + 0.000010f;
+  }
+  h.n = nrm;
+  return h;
+}
+
+// VolumeObject_InteractionParticle for polyhedra (DEM_Kernels_Compute.cuh:
+// 12-246): the first volume object in contact acts (one at a time); the
+// contact type (1 vertex-face, 2 edge-edge, 0 none) is kept per particle.
+__device__ void poly_dobjects(const SimParams& P, const PolyRef& A, const TypeParams& T,
+                              float3 va, float3 wa, int& colltype, float3& fl, float3& tl,
+                              uint32_t& st) {
+  bool outer = P.dobj[0].translating || !P.is_mill || P.rotating_wobj;
+  if (!outer) outer = len3(f3(A.pos.x, A.pos.y, 0.0f) - P.cent) > (P.dobj_cyl_bound_r - 2.0f * T.radius);
+  if (!outer) return;
+  for (int d = 0; d < P.n_dobj; ++d) {
+    const DobjDev& D = P.dobj[d];
+    const float3 bv = vmul(A.pos - D.com, D.axis);
+    if (!(len3(bv) < (D.bound_r + T.radius))) continue;
+    if (dobject_face_separates(D, A) || particle_face_separates(A, D)) continue;
+    Hit h = vertex_dobject(A, D, st);
+    int ct = 1;
+    if (!h.hit) {
+      float3 pd = D.com;
+      pd.z = A.pos.z;
+      const float3 rp = pd - A.pos;
+      h = dobject_edges(D, A, rp / len3(rp), st);
+      ct = 2;
+    }
+    colltype = h.hit ? ct : 0;
+    if (!h.hit) continue;
+    float3 vobj = f3(0.0f, 0.0f, 0.0f);
+    if (D.attached) vobj = drum_velocity(P, h.cp);
+    else if (D.translating) vobj = D.velocity;
+    const Forces F = law_volume<true>(P, h.n, h.dis, h.cp - A.pos, wa, T, va, vobj);
+    fl = fl + F.trans;
+    if (P.rotation) tl = tl + F.torque;
+    break;
+  }
+}
+
 // ------------------------------------------------------------- world objects
 // Collision_Detection_Polyhedra_Surface + _Vertcies_Surface (CDP:85-177,
 // 489-529): the centre within the bounding radius on the face's outer side,
@@ -596,9 +874,9 @@ k_poly_geom(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
 }
 
 // The fused polyhedron step: Kernel_ParticleInteraction_Polyhedra_NonSymmetry
-// (DEM_Kernels_Compute.cuh:736-992), WorldObject_InteractionParticle and
-// Integrate_Euler_NonSymmetry with the quaternion update, one thread per
-// particle.  Volume objects are rejected for polyhedra by the host.
+// (DEM_Kernels_Compute.cuh:736-992), WorldObject_InteractionParticle,
+// VolumeObject_InteractionParticle, Integrate_Euler_NonSymmetry with the
+// quaternion update, one thread per particle.
 template <bool kCapture>
 __global__ void __launch_bounds__(kThreads)
 k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
@@ -674,19 +952,29 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
   const float3 f_pp = f;
   const float3 t_pp = P.rotation ? fl : f3(0.0f, 0.0f, 0.0f);
 
+  // volume objects
+  float3 f_l = f3(0.0f, 0.0f, 0.0f), t_l = f3(0.0f, 0.0f, 0.0f);
+  if (P.n_dobj > 0) {
+    int* lift = (ctl->epoch & 1) ? ob.lift[1] : ob.lift[0];
+    int colltype = 0;
+    poly_dobjects(P, A, TA, va, wa, colltype, f_l, t_l, st);
+    lift[i] = colltype;
+  }
+
   // world objects
   float3 f_w = f3(0.0f, 0.0f, 0.0f), t_w = f3(0.0f, 0.0f, 0.0f);
   poly_walls(P, ops, A, TA, va, wa, f_w, t_w);
   if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
-  const float3 f_l = f3(0.0f, 0.0f, 0.0f), t_l = f3(0.0f, 0.0f, 0.0f);
 
   // Integrate_Euler_NonSymmetry (Integration.cuh:6-184), polyhedra
   float3 acc = f_w + f_pp;
+  if (P.n_dobj > 0) acc = acc + f_l;
   acc = acc * (1.0f / ma);
   float3 v = va + acc * P.dt;
   const float3 p = pa + v * P.dt;
   if (P.mode2d) v.z = 0.0f;
-  const float3 tl = t_pp + t_w;
+  float3 tl = t_pp + t_w;
+  if (P.n_dobj > 0) tl = tl + t_l;
   float3 w = wa;
   if (P.rotation) {
     float4* qarr = (ctl->epoch & 1) ? ob.ornt[1] : ob.ornt[0];

@@ -58,7 +58,7 @@ class Golden:
 
 
 GOLDEN_NAMES = ["silo_sph90", "mill_sph30"]
-POLY_GOLDEN_NAMES = ["box_poly", "drum_poly"]
+POLY_GOLDEN_NAMES = ["box_poly", "drum_poly", "lifter_poly"]
 
 
 @pytest.fixture(params=GOLDEN_NAMES)

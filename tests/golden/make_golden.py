@@ -157,7 +157,7 @@ def make_poly(ref_root, name, project, world, n, spacing, seed):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
-def poly_drum_project(ref_root, dst, n):
+def poly_drum_project(ref_root, dst, n, lifters=False):
     """A polyhedron project assembled from the reference's own pieces: the
     90 cm mill drum with both end plates (3.BallMill Drum90cm.WOBJ) filled
     with the dodecahedron of 1.Particles_Box (Poly_1cm.POBJ), the world file
@@ -172,6 +172,8 @@ def poly_drum_project(ref_root, dst, n):
                 os.path.join(proj, "SurfaceObjects"))
     shutil.copy(os.path.join(src, "1.Particles_Box", "ParticleObjects", "Poly_1cm.POBJ"),
                 os.path.join(proj, "ParticleObjects"))
+    shutil.copy(os.path.join(src, "3.BallMill", "LifterObjects", "Square_Lifter16.DOBJ"),
+                os.path.join(proj, "LifterObjects"))
     text = open(os.path.join(src, "3.BallMill", "World", "Mill_SPH30.World")).read()
     reps = [("Particle_Type(0=sphere,1=poly,2=mixed): 0", "Particle_Type(0=sphere,1=poly,2=mixed): 1"),
             ("1 Ball_5cm  242", "1 Poly_1cm  %d" % n),
@@ -180,22 +182,27 @@ def poly_drum_project(ref_root, dst, n):
     for a, b in reps:
         assert a in text, a
         text = text.replace(a, b)
-    text, k = re.subn(r"Number: 1 Repeat: 8\s+1 Square_Lifter16", "Number: 0 Repeat: 0", text)
-    assert k == 1
+    if not lifters:
+        text, k = re.subn(r"Number: 1 Repeat: 8\s+1 Square_Lifter16", "Number: 0 Repeat: 0", text)
+        assert k == 1
     open(os.path.join(proj, "World", "Mill_POLY.World"), "w").write(text)
     return os.path.join(dst, "Projects"), "MillPoly", "Mill_POLY"
 
 
-def make_poly_drum(ref_root, name, n, seed):
+def make_poly_drum(ref_root, name, n, seed, lifters=False):
     """Dodecahedra in the bottom of the rotating mill drum: drum wall
-    (moving-surface law), both end plates, particle contacts."""
+    (moving-surface law), both end plates, particle contacts, and with
+    `lifters` the reference's eight Square_Lifter16 volume objects."""
     tmp = tempfile.mkdtemp(prefix="blaze_polydrum_")
     try:
-        projects, project, world = poly_drum_project(ref_root, tmp, n)
+        projects, project, world = poly_drum_project(ref_root, tmp, n, lifters)
         P = Project.load(projects, project, world)
         rp, w, p, d = RefHost.parse_isolated(projects, project, world)
         assert canon.pobj_poly(p[0], 1) == canon.pobj_poly(_unscaled(P.pobj[0], p[0]), 1)
         assert canon.wobj(w[0]) == canon.wobj(P.wobj[0])
+        assert rp.n_d == P.n_d
+        for i in range(P.n_d):
+            assert canon.dobj(d[i]) == canon.dobj(P.dobj[i])
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     rng = np.random.default_rng(seed)
@@ -215,10 +222,14 @@ def make_poly_drum(ref_root, name, n, seed):
         for th in np.arange(-0.35, 0.35, dth):
             for z in np.arange(0.94 * r_b, H - 0.94 * r_b, sp):
                 cand.append((cx + rad * np.sin(th), cy - rad * np.cos(th), z))
-    pos = np.array(cand[:n])
-    assert len(pos) == n
-    pos = (pos + rng.uniform(-0.02, 0.02, size=pos.shape)).astype(np.float32)
-    quat = random_quaternions(rng, n)
+    cand = np.array(cand)
+    cand = (cand + rng.uniform(-0.02, 0.02, size=cand.shape)).astype(np.float32)
+    qc = random_quaternions(rng, len(cand))
+    if P.n_d:
+        keep = lifter_safe(P, cand, qc)
+        cand, qc = cand[keep], qc[keep]
+    assert len(cand) >= n, len(cand)
+    pos, quat = cand[:n], qc[:n]
     vel = rng.normal(scale=10.0, size=(n, 3)).astype(np.float32)
     avel = rng.normal(scale=20.0, size=(n, 3)).astype(np.float32)
     ptype = np.zeros(n, np.uint32)
@@ -253,6 +264,54 @@ def make_poly_drum(ref_root, name, n, seed):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def rotate(q, v):
+    """Rotate body-frame points v (k, 3) by unit quaternion q (w, x, y, z)."""
+    w, x, y, z = (float(c) for c in q)
+    R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                  [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                  [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+    return v @ R.T
+
+
+def lifter_safe(P, pos, quat, margin=0.005):
+    """Sites whose particle either meets no volume object's bounding
+    cylinder, or is cut off from it by a face plane (all vertices at least
+    `margin` in front), or has one or two vertices behind all of its faces
+    with a `margin` either way: the contacts the reference resolves with its
+    vertex-face and edge-face tests.  Deeper contacts can overflow the
+    reference's 8-entry vertex arrays, and edge-only ones can leave its
+    normal unset, so the fixture starts without them."""
+    o = P.pobj[0]
+    lv = np.array([[o.Local_Vertex[k].x, o.Local_Vertex[k].y, o.Local_Vertex[k].z]
+                   for k in range(o.num_vertex)])
+    r_b = float(o.radius)
+    keep = np.ones(len(pos), bool)
+    for i in range(len(pos)):
+        p = pos[i].astype(np.float64)
+        for d in range(P.n_d):
+            D = P.dobj[d]
+            com = np.array([D.COM.x, D.COM.y, D.COM.z])
+            ax = np.array([D.Axis.x, D.Axis.y, D.Axis.z])
+            if np.linalg.norm((p - com) * ax) >= float(D.boundR) + r_b + margin:
+                continue
+            v = rotate(quat[i], lv) + p
+            dist = []
+            for f in range(D.num_faces):
+                S = D.faces[f]
+                n = np.array([S.normal.x, S.normal.y, S.normal.z])
+                c = np.array([S.centroid.x, S.centroid.y, S.centroid.z])
+                dist.append((v - c) @ n)
+            dist = np.array(dist)
+            if np.any(np.all(dist >= margin, axis=1)):
+                continue  # one lifter face has every vertex well in front
+            inside_hi = int(np.all(dist <= margin, axis=0).sum())
+            inside_lo = int(np.all(dist <= -margin, axis=0).sum())
+            if not (inside_lo == inside_hi and 1 <= inside_hi <= 2):
+                keep[i] = False
+                break
+    return keep
+
+
 def _unscaled(mine, ref):
     """The mirror's object with the parser's inertia tensor (the run setup
     scales it afterwards; the scaling has its own test)."""
@@ -273,6 +332,8 @@ def main():
             make_poly(ref_root, name, project, world, n, spacing, seed)
     if which is None or "drum_poly" in which:
         make_poly_drum(ref_root, "drum_poly", 1200, 11)
+    if which is None or "lifter_poly" in which:
+        make_poly_drum(ref_root, "lifter_poly", 1200, 13, lifters=True)
 
 
 if __name__ == "__main__":

@@ -1,8 +1,9 @@
 """Convex polyhedra on the GPU through the C ABI, against the reference's own
 polyhedron kernels: the oracle-A fixtures (tests/golden/box_poly.npz, 1,440
 dodecahedra of the reference's Poly_1cm object in its Container_128 box;
-tests/golden/drum_poly.npz, 1,200 in the rotating 90 cm mill drum with end
-plates), random orientations and spins, contacts of every kind from the
+drum_poly.npz, 1,200 in the rotating 90 cm mill drum with end plates;
+lifter_poly.npz, the same drum with its eight Square_Lifter16 volume
+objects), random orientations and spins, contacts of every kind from the
 first step; and variants run against oracle A live (oracle/_ref travels with
 the repository): rotation off, 2-D mode, an infinite plane after a face.
 

@@ -44,6 +44,8 @@ def test_fixture_exercises_contacts(golden_poly):
     assert int((np.abs(s1["f_wall"]).sum(axis=1) > 0).sum()) > 20
     if g.cyl_rot:  # drum wall contacts carry torque (end plates do not)
         assert int((np.abs(s1["t_wall"]).sum(axis=1) > 0).sum()) > 100
+    if g.n_d:  # lifter contacts, with torque
+        assert int((np.abs(s1["t_lift"]).sum(axis=1) > 0).sum()) > 5
     s0 = g.init()
     order0 = np.argsort(s0["pid"])
     order1 = np.argsort(s1["pid"])
