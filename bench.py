@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--batched-steps", type=int, default=2000,
                     help="timed steps of the batched leg (the workload's 2,000 settling steps)")
+    ap.add_argument("--no-poly", action="store_true",
+                    help="skip the convex-polyhedra leg (100,000 polyhedra in a box)")
+    ap.add_argument("--poly-steps", type=int, default=500)
+    ap.add_argument("--poly-only", action="store_true",
+                    help="run only the convex-polyhedra leg and print its object")
     return ap.parse_args()
 
 
@@ -304,19 +309,108 @@ def adjoint_leg(steps, segment=50):
                           "mu": float(g[:, 2].mean()), "mu_wall": float(g[:, 3].mean())}}
 
 
-def cpu_reference_rate(P, st, seconds, max_steps=None):
+def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=True):
+    """Convex polyhedra on the reference path: 100,000 particles (the
+    polyhedron count of the mill configuration) in a closed box, a third
+    each dodecahedra, cubes and hexagonal prisms of circumradius 0.5 cm on a
+    0.93 cm jittered lattice (every bounding sphere overlaps its lattice
+    neighbours', so contacts exist from the first step), random orientations,
+    velocities N(0, 10 cm/s), spins N(0, 20 rad/s), linear law kn = 1e5,
+    e = 0.5, mu = 0.4, dt = 1e-5 s, rotation on.  GPU: CUDA graphs with a
+    `skin` Verlet list on the bounding spheres (value) and the reference's
+    rebuild-every-step mode (reference_mode_value).  CPU: the reference's own
+    polyhedron kernels (oracle/_ref) on all host threads, reference mode, a
+    bounded sample of whole steps of the same workload."""
+    import torch
+    from blaze import device, synth
+    with tempfile.TemporaryDirectory() as d:
+        P, st = synth.poly_box_project(d, n=n)
+    sim = device.Simulation(P, skin=skin, use_graph=1)
+    sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
+    sim.step(max(3, warmup))
+    status = sim.sync()
+    stream = torch.cuda.ExternalStream(sim.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = sim.num_rebuilds()
+    a.record(stream)
+    sim.step(steps)
+    b.record(stream)
+    fixed = sim.last_launches()
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = sim.num_rebuilds() - rb0
+    launches = fixed + rebuilds * sim.rebuild_kernels()
+    status |= sim.sync()
+    sim.set_profile(True)
+    sim.step(min(steps, 100))
+    ms_rebuild, ms_step, nprof = sim.profile()
+    sim.set_profile(False)
+    sim.set_options(skin=0.0, use_graph=1)
+    sim.step(3)
+    sim.sync()
+    kref = min(steps, 200)
+    a.record(stream)
+    sim.step(kref)
+    b.record(stream)
+    b.synchronize()
+    ref_ms = a.elapsed_time(b) / kref
+    status |= sim.sync()
+    sim.close()
+    out = {"workload": "100,000 convex polyhedra (dodecahedra, cubes, hexagonal prisms, "
+                       "circumradius 0.5 cm) in contact in a closed box, linear law kn=1e5 "
+                       "e=0.5 mu=0.4, dt 1e-5 s, rotation on",
+           "particles": n, "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "steps": steps, "skin_cm": skin, "rebuilds": rebuilds, "gpu_launches": launches,
+           "step_kernels_ms": ms_step / max(nprof, 1),
+           "rebuild_ms_per_step": ms_rebuild / max(nprof, 1),
+           "reference_mode_value": n / (ref_ms * 1e-3), "reference_mode_ms_per_step": ref_ms,
+           "status": device.decode_status(status)}
+    if want_cpu:
+        cb = cpu_reference_rate(P, st, cpu_seconds, hatch=False)
+        out["cpu_baseline"] = cb
+        if cb:
+            out["vs_cpu_reference"] = out["value"] / cb["value"]
+            out["reference_mode_vs_cpu_reference"] = out["reference_mode_value"] / cb["value"]
+    return out
+
+
+class _StdoutToStderr:
+    """Send file descriptor 1 to stderr while the reference's kernels run:
+    their printf warnings would otherwise mix with the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
+def cpu_reference_rate(P, st, seconds, max_steps=None, hatch=True):
     """The reference's own kernels compiled as host C++ (oracle/_ref), all
     host threads, reference mode, on this workload: particle-steps/s."""
+    with _StdoutToStderr():
+        return _cpu_reference_rate(P, st, seconds, max_steps, hatch)
+
+
+def _cpu_reference_rate(P, st, seconds, max_steps, hatch):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from bindings import RefHost, ref_available
     if not ref_available():
         return None
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     si = type(P.sim_info).from_buffer_copy(bytes(P.sim_info))
-    si.Num_WorldObjects = P.n_w - 1  # hatch open (Device_OpenHatch drops the last object)
+    if hatch:
+        si.Num_WorldObjects = P.n_w - 1  # hatch open (Device_OpenHatch drops the last object)
     R = RefHost().init(si, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=threads,
                        capture=False)
-    R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st.get("quat"))
     R.step(1)  # first step outside the clock (page-in)
     steps = 0
     t0 = time.perf_counter()
@@ -366,6 +460,10 @@ def main():
     from blaze import device
 
     torch.cuda.set_device(local)
+    if args.poly_only:
+        print(json.dumps(poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                                  want_cpu=not args.no_cpu_baseline)))
+        return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     tmp = tempfile.TemporaryDirectory()
@@ -471,6 +569,10 @@ def main():
     e2e_value = n * world * args.e2e_steps / el
     state_bytes = n * (12 + 12 + 12 + 4 + 4)
 
+    poly = None
+    if not args.no_poly:
+        poly = poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                        want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
     batched = None
     if not args.no_batched:
         batched = batched_leg(args.batched_steps, args.warmup)
@@ -503,6 +605,7 @@ def main():
             "rebuilds_in_timed_region": rebuilds,
             "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
             "reference_mode_value": ref_mode_value,
+            "polyhedra": poly,
             "batched": batched,
             "adjoint": adjoint,
             "status": device.decode_status(status),

@@ -9,6 +9,9 @@ run these).
         calibration ensemble of NSYS x 20,000 spheres (64), seeded initial
         velocities, reverse mode over STEPS steps (60) with checkpoints every
         SEGMENT (30), random cotangents of the final state.
+    python softx-d-15-00085_b200/blaze/cases.py poly [N] [STEPS]
+        the convex-polyhedra workload of bench.py at N particles (20,000),
+        reference mode, STEPS plain steps (10).
 """
 import os
 import sys
@@ -39,6 +42,22 @@ def ens_step(steps=30):
     return status
 
 
+def poly(n=20000, steps=10):
+    """The convex-polyhedra bench workload at n particles, reference mode
+    (contact list rebuilt every step), `steps` plain steps."""
+    import tempfile
+    from blaze import device
+    with tempfile.TemporaryDirectory() as d:
+        P, st = synth.poly_box_project(d, n=n)
+    sim = device.Simulation(P)
+    sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
+    sim.step(steps)
+    status = sim.sync()
+    print("poly: n %d status %d" % (n, status))
+    sim.close()
+    return status
+
+
 def adjoint(nsys=64, steps=60, segment=30):
     S, W, p, r = calibrate.calibration_ensemble(nsys=nsys, n=20000, seed=4)
     ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, use_graph=0)
@@ -57,5 +76,5 @@ def adjoint(nsys=64, steps=60, segment=30):
 if __name__ == "__main__":
     name = sys.argv[1] if len(sys.argv) > 1 else "ens_step"
     args = [int(a) for a in sys.argv[2:]]
-    rc = {"ens_step": ens_step, "adjoint": adjoint}[name](*args)
+    rc = {"ens_step": ens_step, "adjoint": adjoint, "poly": poly}[name](*args)
     sys.exit(1 if rc else 0)

@@ -11,6 +11,9 @@ SI and in these units).  All randomness is numpy default_rng(seed).
                  hopper approximated by planar faces (reference-law variant
                  of the silo discharge configuration: at most 6 radius bins,
                  linear law, hopper faces within the 8 x 16 face capacity)
+  poly_box_project
+                 convex polyhedra (dodecahedra, cubes, hexagonal prisms) in
+                 a closed box, every particle in contact from the start
 """
 import math
 import os
@@ -22,7 +25,7 @@ from .project import Project, write_state_file
 _WORLD = """Title: "{title}"
 ModelType(Specfic|0:TC_COR|1:KN_COR):     1
 Simulation_Type(0=General,1=mill,2=silo): {sim_type}
-Particle_Type(0=sphere,1=poly,2=mixed):   0
+Particle_Type(0=sphere,1=poly,2=mixed):   {ptype}
 Delta_t(s):       {dt!r}
 _________________________________________________
              1_Geometrical-Information
@@ -139,18 +142,182 @@ def _write_cylinder_wobj(path, title, radius, height, offset, axis_normal=(0.0, 
 
 
 def _write_project(root, name, world_name, *, title, sim_type, dt, wobjs, pobjs, counts, n, g,
-                   rotation, roll_res, origin, world, cell, state, specific=""):
+                   rotation, roll_res, origin, world, cell, state, specific="", particle_type=0):
     base = os.path.join(root, name)
     for sub in ("World", "SurfaceObjects", "ParticleObjects", "VolumeObjects"):
         os.makedirs(os.path.join(base, sub), exist_ok=True)
     wl = "\n".join("%d %s" % (k + 1, w) for k, w in enumerate(wobjs))
-    pl = "\n".join("1 %s %d" % (p, c) for p, c in zip(pobjs, counts))
+    pl = "\n".join("%d %s %d" % (k + 1, p, c) for k, (p, c) in enumerate(zip(pobjs, counts)))
     with open(os.path.join(base, "World", world_name + ".World"), "w") as fh:
-        fh.write(_WORLD.format(title=title, sim_type=sim_type, dt=dt, n_w=len(wobjs), wobj_lines=wl,
+        fh.write(_WORLD.format(title=title, sim_type=sim_type, ptype=particle_type, dt=dt,
+                               n_w=len(wobjs), wobj_lines=wl,
                                n_p=len(pobjs), pobj_lines=pl, n=n, g=g, rotation=rotation,
                                roll_res=roll_res, origin=origin, world=world, cell=cell,
                                state=state, specific=specific))
     return base
+
+
+_POBJ_POLY_PROPS = """------------------------
+     2_POLY_PROP
+------------------------
+DENSITY:  {rho!r}
+INERTIA_TENSOR:
+1.0 0.0 0.0
+0.0 1.0 0.0
+0.0 0.0 1.0
+------------------------
+     3_SPRING_DATA
+------------------------
+Particle_Particle
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Friction:  {mu!r}
+Friction:  {mu!r}
+Particle_Surface
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Friction:  {mu!r}
+Friction:  {mu!r}
+Particle_Lifter
+COR:       {cor!r}
+Kn(N/cm):  {kn!r}
+Friction:  {mu!r}
+Friction:  {mu!r}
+"""
+
+
+def dodecahedron(r):
+    """Regular dodecahedron of circumradius r: 20 vertices, 12 pentagons
+    (outward counter-clockwise), 30 edges."""
+    phi = (1.0 + math.sqrt(5.0)) / 2.0
+    v = [(x, y, z) for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)]
+    for a in (-1, 1):
+        for b in (-1, 1):
+            v += [(0, a / phi, b * phi), (a / phi, b * phi, 0), (b * phi, 0, a / phi)]
+    v = np.array(v, np.float64)
+    v *= r / np.linalg.norm(v[0])
+    return _hull_polygons(v)
+
+
+def cube(r):
+    """Cube of circumradius r: 8 vertices, 6 squares, 12 edges."""
+    h = r / math.sqrt(3.0)
+    v = np.array([(x, y, z) for x in (-h, h) for y in (-h, h) for z in (-h, h)], np.float64)
+    return _hull_polygons(v)
+
+
+def hex_prism(r, aspect=1.0):
+    """Hexagonal prism of circumradius r (height/width = aspect): 12
+    vertices, 2 hexagons and 6 rectangles, 18 edges."""
+    a = r / math.sqrt(1.0 + aspect * aspect)
+    h = aspect * a
+    v = [(a * math.cos(k * math.pi / 3), a * math.sin(k * math.pi / 3), z)
+         for z in (-h, h) for k in range(6)]
+    return _hull_polygons(np.array(v, np.float64))
+
+
+def _hull_polygons(v):
+    """Convex polyhedron from its vertices: faces as vertex lists ordered
+    counter-clockwise seen from outside (merged coplanar hull triangles),
+    and the edges."""
+    from scipy.spatial import ConvexHull
+    hull = ConvexHull(v)
+    planes = {}
+    for eq in hull.equations:
+        key = tuple(np.round(eq, 6))
+        planes[key] = eq
+    faces = []
+    for eq in planes.values():
+        n, d = eq[:3], eq[3]
+        idx = [i for i in range(len(v)) if abs(v[i] @ n + d) < 1e-9]
+        c = v[idx].mean(axis=0)
+        e1 = v[idx[0]] - c
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(n, e1)
+        ang = [math.atan2((v[i] - c) @ e2, (v[i] - c) @ e1) for i in idx]
+        faces.append([idx[i] for i in np.argsort(ang)])
+    edges = set()
+    for f in faces:
+        for k in range(len(f)):
+            a, b = f[k], f[(k + 1) % len(f)]
+            edges.add((min(a, b), max(a, b)))
+    return v, faces, sorted(edges)
+
+
+def _write_pobj_poly(path, title, v, faces, edges, rho, kn, cor, mu):
+    """A Format-0 polyhedral particle object (KSimulationData.cpp:1219-1624).
+    The reference's parser takes a face normal from the face's vertices 3, 4
+    and 1 (cross(V[2]-V[3], V[3]-V[0])), which points outwards for faces
+    listed counter-clockwise seen from outside, as written here."""
+    with open(path, "w") as fh:
+        fh.write('Title: "%s"\nDescp: "synthetic"\nFormat(0=Man,1=Math): 0\n' % title)
+        fh.write("------------------------\n1_Geometry_Specfications\n------------------------\n")
+        fh.write("NUM_VERTEX: %d\n" % len(v))
+        for k, p in enumerate(v):
+            fh.write("%d %r %r %r\n" % (k + 1, float(p[0]), float(p[1]), float(p[2])))
+        fh.write("NUM_FACES: %d\n" % len(faces))
+        for k, f in enumerate(faces):
+            fh.write("%d NUM_VERTEX: %d\n" % (k + 1, len(f)))
+            fh.write(" ".join(str(q + 1) for q in f) + "\n")
+        fh.write("NUM_EDGES: %d\n" % len(edges))
+        for a, b in edges:
+            fh.write("%d %d\n" % (a + 1, b + 1))
+        fh.write(_POBJ_POLY_PROPS.format(rho=rho, kn=kn, cor=cor, mu=mu))
+
+
+def random_quaternions(rng, n):
+    """Uniformly distributed unit quaternions (w, x, y, z) with w >= 0."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q[q[:, 0] < 0] *= -1.0
+    return q.astype(np.float32)
+
+
+def poly_box_project(root, n=100_000, r=0.5, spacing=0.93, rho=2700.0, kn=1.0e5, cor=0.5,
+                     mu=0.4, dt=1e-5, seed=2, name="PolyBox", world="Poly_box"):
+    """Convex polyhedra in a closed box: dodecahedra, cubes and hexagonal
+    prisms of circumradius r (types 0, 1, 2 in turn) on a jittered cubic
+    lattice of the given spacing, so that bounding spheres of lattice
+    neighbours overlap and every particle starts with contacts (the first
+    layer touches the three lower walls); random
+    orientations, velocities N(0, 10 cm/s), spins N(0, 20 rad/s); y vertical.
+    Returns (Project, state dict with a `quat` entry)."""
+    base = os.path.join(root, name)
+    for sub in ("SurfaceObjects", "ParticleObjects"):
+        os.makedirs(os.path.join(base, sub), exist_ok=True)
+    side = int(math.ceil(n ** (1.0 / 3.0)))
+    L = side * spacing + 2.0 * r + 1.0
+    verts = [(0, 0, 0), (L, 0, 0), (L, L, 0), (0, L, 0), (0, 0, L), (L, 0, L), (L, L, L), (0, L, L)]
+    faces = [(0, 1, 2, 3), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (3, 7, 4, 0), (4, 7, 6, 5)]
+    faces = _orient(verts, faces, lambda c: (0.5 * L, 0.5 * L, 0.5 * L))
+    _write_wobj(os.path.join(base, "SurfaceObjects", "Box.WOBJ"), "Box", verts, faces)
+    shapes = [("Dodeca", dodecahedron(r)), ("Cube", cube(r)), ("HexPrism", hex_prism(r))]
+    for title, (v, f, e) in shapes:
+        _write_pobj_poly(os.path.join(base, "ParticleObjects", title + ".POBJ"), title, v, f, e,
+                         rho, kn, cor, mu)
+    counts = [len(range(t, n, len(shapes))) for t in range(len(shapes))]
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij"),
+                 axis=-1).reshape(-1, 3)[:n]
+    # the first lattice layer 0.94 r from the three lower walls: vertices
+    # that point at a wall touch it
+    pos = (g * spacing + 0.94 * r + rng.uniform(-0.02, 0.02, size=(n, 3)))
+    # the parser's objects carry their centre of mass in the file frame
+    # (here the origin up to rounding); positions are centres of mass
+    ptype = np.arange(n, dtype=np.uint32) % len(shapes)
+    order = np.argsort(ptype, kind="stable")
+    state = dict(pos=pos[order].astype(np.float32),
+                 vel=rng.normal(scale=10.0, size=(n, 3)).astype(np.float32),
+                 avel=rng.normal(scale=20.0, size=(n, 3)).astype(np.float32),
+                 quat=random_quaternions(rng, n), pid=np.arange(n, dtype=np.int32),
+                 type=ptype[order])
+    cell = 2.0 * r
+    _write_project(root, name, world, title="Poly_box", sim_type=0, dt=dt, wobjs=["Box"],
+                   pobjs=[t for t, _ in shapes], counts=counts, n=n, g=(0.0, -981.0, 0.0),
+                   rotation=1, roll_res=0.0, origin=(-cell, -cell, -cell),
+                   world=(L + cell, L + cell, L + cell), cell=cell, state="none",
+                   particle_type=1)
+    return Project.load(root, name, world), state
 
 
 def box_project(root, n_side=(20, 20, 25), radius=0.1, rho=2500.0, box=10.0, kn=1.0e5, cor=0.5,

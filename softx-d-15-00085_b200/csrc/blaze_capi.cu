@@ -96,6 +96,7 @@ struct blaze_sim {
   bool poly = false;
   PolyShape* d_shapes = nullptr;
   PolyGeom geom{};
+  PolyPairs pairs{};
 };
 
 namespace {
@@ -342,6 +343,33 @@ int upload_params(blaze_sim* s) {
   return upload_walls(s);
 }
 
+// Per-slot narrow-phase buffers of the polyhedron passes, sized by the
+// neighbour list (slots are indexed with 32 bits).
+int alloc_poly_pairs(blaze_sim* s) {
+  PolyPairs& pp = s->pairs;
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  f(pp.status); f(pp.con); f(pp.qv); f(pp.qe); f(pp.counts);
+  pp = PolyPairs{};
+  const size_t slots = (size_t)s->nl.cap * (size_t)s->nl.stride;
+  if (slots >= (size_t)0xffffffffu) {
+    std::fprintf(stderr, "blaze: %zu neighbour slots exceed the polyhedron passes' 32-bit index\n",
+                 slots);
+    return -1;
+  }
+  CK(dalloc(&pp.status, slots));
+  CK(dalloc(&pp.con, 2 * slots));
+  CK(dalloc(&pp.qv, slots));
+  CK(dalloc(&pp.qe, slots));
+  CK(dalloc(&pp.counts, 2));
+  CK(cudaMemset(pp.counts, 0, 2 * sizeof(int)));
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  pp.grid_v = 8 * sms;
+  pp.grid_e = 8 * sms;
+  return 0;
+}
+
 int alloc_nlist(blaze_sim* s) {
   drop_graphs(s);
   if (s->nl.idx) CK(cudaFree(s->nl.idx));
@@ -351,6 +379,7 @@ int alloc_nlist(blaze_sim* s) {
   CK(dalloc(&s->nl.idx, (size_t)s->n_max * s->nl.cap));
   CK(dalloc(&s->nl.cnt, s->n_max));
   CK(cudaMemsetAsync(s->nl.cnt, 0, sizeof(uint32_t) * s->n_max, s->stream));
+  if (s->poly) return alloc_poly_pairs(s);
   return 0;
 }
 
@@ -401,9 +430,11 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
   if (s->poly) {
     launch_poly_geom(s->d_shapes, s->geom, s->S[s->cur], s->S[2], s->ob, s->n_max,
                      s->si.Rotation ? 1 : 0, s->ctl, link.rebuilt, st);
+    const int np = launch_poly_pairs(s->dp, s->d_shapes, s->geom, s->S[s->cur], s->S[2],
+                                     s->n_max, s->nl, s->ctl, link.rebuilt, s->pairs, st);
     launch_poly_step(s->dp, s->d_shapes, s->geom, s->d_ops, s->S[s->cur], s->S[2],
-                     s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, cap, st);
-    return 2;
+                     s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->pairs, s->ctl, link, cap, st);
+    return 2 + np;
   }
   launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
               s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, st);
@@ -513,7 +544,7 @@ int graph_steps(blaze_sim* s, int nsteps) {
     CK(cudaGraphLaunch(s->graph[c], s->stream));
     // launches that always run: the gate and the step kernels of each step
     // (re-sort bodies run only when a step asks for them)
-    s->last_launches += 1 + kGraphSteps * (s->poly ? 2 : 1);
+    s->last_launches += 1 + kGraphSteps * (s->poly ? 5 : 1);
     s->steps += kGraphSteps;
     if (s->si.Kill_Particles) s->stepc += kGraphSteps;
     if (kGraphSteps & 1) s->cur ^= 1;
@@ -605,6 +636,7 @@ void free_sim(blaze_sim* s) {
   f(s->stage.flags); f(s->stage.quat4);
   f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
   f(s->geom.vert); f(s->geom.fnorm); f(s->geom.fcent);
+  f(s->pairs.status); f(s->pairs.con); f(s->pairs.qv); f(s->pairs.qe); f(s->pairs.counts);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -684,7 +716,7 @@ int setup_poly(blaze_sim* s) {
   }
   CK(dalloc(&s->stage.quat4, 4 * n));
   s->poly = true;
-  return 0;
+  return alloc_poly_pairs(s);
 }
 
 int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,

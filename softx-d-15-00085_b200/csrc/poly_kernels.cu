@@ -96,6 +96,13 @@ struct PolyRef {
   float3 pos;
 };
 
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float3 shfl3(float3 v, int src) {
+  return f3(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src),
+            __shfl_sync(kFull, v.z, src));
+}
+
 // is_SP_Poly_Poly (Utilities.cuh:105-156): a face plane of `a` with the
 // centre of `b` on its outer side and every vertex of `b` strictly outside.
 __device__ bool separated_by_face(const PolyRef& a, const PolyRef& b) {
@@ -182,31 +189,52 @@ __device__ bool ray_meets_face(const PolyRef& b, int k, float3 from, float3 to, 
   return on_face(b, k, from + d * ray, tol);
 }
 
-// Collision_Detection_Polyhedara_Polyhedra_VertexFaces (CDP:1154-1630):
-// vertices of `a` inside `b`.  One vertex: vertex-face contact on the nearest
-// face the ray from a's centre confirms; two: edge-face at their midpoint;
-// more: face-face at their mean.
-__device__ Hit vertex_face(const PolyRef& a, const PolyRef& b, uint32_t& st) {
-  Hit h = no_hit();
-  int count = 0, i0 = -1, i1 = -1, s1_face1 = -1;
+// What the vertex loop of the vertex-face test hands to its branch logic:
+// how many vertices of `a` lie inside `b`, the first two (index order), the
+// first one's nearest faces, the second one's second-nearest face, and the
+// in-order sum of all of them.
+struct VertexScan {
+  int count, i0, i1, s1_face1;
   Inside s0;
-  s0.in = false;
-  float3 sum = f3(0.0f, 0.0f, 0.0f);
+  float3 sum;
+};
+
+// The vertex loop of the vertex-face test, in vertex order.
+__device__ VertexScan scan_vertices(const PolyRef& a, const PolyRef& b) {
+  VertexScan r;
+  r.count = 0;
+  r.i0 = r.i1 = r.s1_face1 = -1;
+  r.s0.in = false;
+  r.s0.face[0] = r.s0.face[1] = r.s0.face[2] = -1;
+  r.s0.dist[0] = r.s0.dist[1] = r.s0.dist[2] = 10.0f;
+  r.sum = f3(0.0f, 0.0f, 0.0f);
   const int nv = a.s->nv;
   for (int k = 0; k < nv; ++k) {
     const float3 v = ld3(a.v + k);
     const Inside t = vertex_inside(a.pos, v, b);
     if (!t.in) continue;
-    if (count == 0) { s0 = t; i0 = k; }
-    else if (count == 1) { s1_face1 = t.face[1]; i1 = k; }
-    sum = sum + v;
-    ++count;
+    if (r.count == 0) { r.s0 = t; r.i0 = k; }
+    else if (r.count == 1) { r.s1_face1 = t.face[1]; r.i1 = k; }
+    r.sum = r.sum + v;
+    ++r.count;
   }
+  return r;
+}
+
+// Collision_Detection_Polyhedara_Polyhedra_VertexFaces (CDP:1154-1630),
+// after the vertex loop: one vertex inside gives a vertex-face contact on
+// the nearest face the ray from a's centre confirms; two, edge-face at their
+// midpoint; more, face-face at their mean.
+__device__ Hit resolve_vertex_face(const PolyRef& a, const PolyRef& b, const VertexScan& vs,
+                                   uint32_t& st) {
+  Hit h = no_hit();
+  const int count = vs.count;
   if (count == 0) return h;
+  const Inside& s0 = vs.s0;
   if (count > 8 || s0.face[0] < 0) st |= kStatusPolyUndefined;
   if (s0.face[0] < 0) return h;
   h.hit = true;
-  const float3 va0 = ld3(a.v + i0);
+  const float3 va0 = ld3(a.v + vs.i0);
   const int f0 = s0.face[0];
   if (count == 1) {
     h.cls = kVertexFace;
@@ -215,11 +243,11 @@ __device__ Hit vertex_face(const PolyRef& a, const PolyRef& b, uint32_t& st) {
     h.cp = va0;
     if (s0.face[1] == -1) return h;
     if (ray_meets_face(b, f0, a.pos, va0, 0.10f)) return h;
-    for (int s = 1; s < 3; ++s) {
-      const int fs = s0.face[s];
-      if (fs > -1 && ray_meets_face(b, fs, a.pos, va0, 0.10f)) {
-        h.n = ld3(b.fn + fs);
-        h.dis = s0.dist[s];
+    for (int q = 1; q < 3; ++q) {
+      const int fq = s0.face[q];
+      if (fq > -1 && ray_meets_face(b, fq, a.pos, va0, 0.10f)) {
+        h.n = ld3(b.fn + fq);
+        h.dis = s0.dist[q];
         return h;
       }
     }
@@ -227,15 +255,15 @@ __device__ Hit vertex_face(const PolyRef& a, const PolyRef& b, uint32_t& st) {
   }
   if (count == 2) {
     h.cls = kEdgeFace;
-    h.cp = (va0 + ld3(a.v + i1)) * 0.50f;
+    h.cp = (va0 + ld3(a.v + vs.i1)) * 0.50f;
     h.n = ld3(b.fn + f0);
     h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + f0)));
-    if (s0.face[1] == -1 && s1_face1 == -1) return h;
-    for (int s = 0; s < 3; ++s) {
-      const int fs = s0.face[s];
-      if ((s == 0 || fs > -1) && ray_meets_face(b, fs, a.pos, h.cp, 0.10f)) {
-        h.n = ld3(b.fn + fs);
-        h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fs)));
+    if (s0.face[1] == -1 && vs.s1_face1 == -1) return h;
+    for (int q = 0; q < 3; ++q) {
+      const int fq = s0.face[q];
+      if ((q == 0 || fq > -1) && ray_meets_face(b, fq, a.pos, h.cp, 0.10f)) {
+        h.n = ld3(b.fn + fq);
+        h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fq)));
         return h;
       }
     }
@@ -244,13 +272,13 @@ __device__ Hit vertex_face(const PolyRef& a, const PolyRef& b, uint32_t& st) {
     return h;  // the reference warns and keeps the nearest face
   }
   h.cls = kFaceFace;
-  h.cp = sum / (float)count;
+  h.cp = vs.sum / (float)count;
   const float tol[3] = {0.10f, 0.010f, 0.10f};
-  for (int s = 0; s < 3; ++s) {
-    const int fs = s0.face[s];
-    if ((s == 0 || fs > -1) && ray_meets_face(b, fs, a.pos, h.cp, tol[s])) {
-      h.n = ld3(b.fn + fs);
-      h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fs)));
+  for (int q = 0; q < 3; ++q) {
+    const int fq = s0.face[q];
+    if ((q == 0 || fq > -1) && ray_meets_face(b, fq, a.pos, h.cp, tol[q])) {
+      h.n = ld3(b.fn + fq);
+      h.dis = fabsf(dot3(h.n, h.cp - ld3(b.fc + fq)));
       return h;
     }
   }
@@ -271,48 +299,64 @@ __device__ bool point_in_poly(const PolyRef& b, float3 pt) {
 // Collision_Detection_Polyhedra_Polyhedra_Edges (CDP:537-707): the closest
 // pair of points between an edge of `a` and an edge of `b` (parameters
 // within [-0.01, 1.01]), normal along the edges' cross product turned
-// towards `relpos`.
-__device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos) {
+// towards `relpos`.  Lane l scans the pairs l, l + 32, ... of the (edge of
+// a, edge of b) sequence, keeping its first strict minimum; the warp then
+// takes the smallest distance, the lowest pair index among equals, which is
+// the pair the reference's sequential scan selects.
+__device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos, int lane) {
   Hit h = no_hit();
-  float best = 5.0f;
-  bool found = false;
-  float3 nrm = f3(0.0f, 0.0f, 0.0f), qa_sel = nrm, qb_sel = nrm;
   const int nea = a.s->ne, neb = b.s->ne;
-  for (int i = 0; i < nea; ++i) {
+  const int total = nea * neb;
+  float best = 5.0f;
+  int bidx = 0x7fffffff;
+  float3 nrm = f3(0.0f, 0.0f, 0.0f), qa_sel = nrm, qb_sel = nrm;
+  for (int t = lane; t < total; t += 32) {
+    const int i = t / neb, j = t - i * neb;
     const float3 ap = ld3(a.v + a.s->edge[i][0]);
     const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
+    const float3 bp = ld3(b.v + b.s->edge[j][0]);
+    const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
+    const float3 c = cross3(ad, bd);
+    if (!(dot3(c, c) > 0.00000f)) continue;
     const float daa = dot3(ad, ad);
-    for (int j = 0; j < neb; ++j) {
-      const float3 bp = ld3(b.v + b.s->edge[j][0]);
-      const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
-      const float3 c = cross3(ad, bd);
-      if (!(dot3(c, c) > 0.00000f)) continue;
-      const float3 dv = ap - bp;
-      const float dbb = dot3(bd, bd);
-      const float dab = dot3(ad, bd);
-      const float dav = dot3(ad, dv);
-      const float dbv = dot3(bd, dv);
-      const float inv = 1.00000f / (dab * dab - daa * dbb);
-      const float ta = inv * (dbb * dav - dab * dbv);
-      if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
-      const float tb = inv * (dab * dav - daa * dbv);
-      if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
-      const float3 qa = ap + ad * ta;
-      const float3 qb = bp + bd * tb;
-      const float3 d = qa - qb;
-      float dist = dot3(d, d);
-      if (!(dist > 0.00000f)) continue;
-      dist = sqrtf(dist);
-      if (dist < best) {
-        found = true;
-        best = dist;
-        nrm = c;
-        qa_sel = qa;
-        qb_sel = qb;
-      }
+    const float3 dv = ap - bp;
+    const float dbb = dot3(bd, bd);
+    const float dab = dot3(ad, bd);
+    const float dav = dot3(ad, dv);
+    const float dbv = dot3(bd, dv);
+    const float inv = 1.00000f / (dab * dab - daa * dbb);
+    const float ta = inv * (dbb * dav - dab * dbv);
+    if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
+    const float tb = inv * (dab * dav - daa * dbv);
+    if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
+    const float3 qa = ap + ad * ta;
+    const float3 qb = bp + bd * tb;
+    const float3 d = qa - qb;
+    float dist = dot3(d, d);
+    if (!(dist > 0.00000f)) continue;
+    dist = sqrtf(dist);
+    if (dist < best) {
+      best = dist;
+      bidx = t;
+      nrm = c;
+      qa_sel = qa;
+      qb_sel = qb;
     }
   }
-  if (!found) return h;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ob = __shfl_xor_sync(kFull, best, off);
+    const int oi = __shfl_xor_sync(kFull, bidx, off);
+    if (ob < best || (ob == best && oi < bidx)) {
+      best = ob;
+      bidx = oi;
+    }
+  }
+  if (bidx == 0x7fffffff) return h;
+  const int src = bidx & 31;
+  nrm = shfl3(nrm, src);
+  qa_sel = shfl3(qa_sel, src);
+  qb_sel = shfl3(qb_sel, src);
   nrm = nrm * (1.0f / len3(nrm));
   if (len3(b.pos - qb_sel) < len3(b.pos - qa_sel) && !point_in_poly(b, qa_sel)) return h;
   h.hit = true;
@@ -327,23 +371,6 @@ __device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos) {
   }
   h.n = nrm;
   h.dis = fabsf(dot3(nrm, qb_sel - qa_sel)) + 0.000010f;
-  return h;
-}
-
-// Narrow phase of one pair (DEM_Kernels_Compute.cuh:818-931): separating
-// face planes either way, vertices of A in B, vertices of B in A (normal
-// reversed), edge-edge (depth capped at 0.025 r_A).
-__device__ Hit pair_contact(const PolyRef& A, const PolyRef& B, float ra, float3 relpos,
-                            uint32_t& st) {
-  Hit h = no_hit();
-  if (separated_by_face(A, B) || separated_by_face(B, A)) return h;
-  h = vertex_face(A, B, st);
-  if (h.hit) return h;
-  h = vertex_face(B, A, st);
-  h.n = h.n * -1.0f;
-  if (h.hit) return h;
-  h = edge_edge(A, B, relpos);
-  if (h.hit) h.dis = fminf(0.025f * ra, h.dis);
   return h;
 }
 
@@ -873,15 +900,158 @@ k_poly_geom(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
   }
 }
 
-// The fused polyhedron step: Kernel_ParticleInteraction_Polyhedra_NonSymmetry
-// (DEM_Kernels_Compute.cuh:736-992), WorldObject_InteractionParticle,
-// VolumeObject_InteractionParticle, Integrate_Euler_NonSymmetry with the
-// quaternion update, one thread per particle.
+// ------------------------------------------------------------ narrow phase
+// The pairs of a step go through the reference's tests in three passes,
+// each with the parallelism its test wants; a pass records its verdict per
+// neighbour slot (slot = k * stride + i) and queues the slots the next test
+// must see.  Every pair is evaluated with the reference's arithmetic, and the
+// step sums the contacts in slot order, so the results do not depend on the
+// order in which queued slots are taken.
+enum SlotState : uint8_t { kSlotNone = 0, kSlotVertex = 1, kSlotContact = 2, kSlotEdge = 3 };
+
+__device__ __forceinline__ PolyRef poly_ref(const PolyGeom& g, const PolyShape* shapes, int i,
+                                            float4 p4, float4 v4) {
+  const int t = __float_as_int(v4.w) & (kMaxTypes - 1);
+  return PolyRef{g.vert + (size_t)i * g.kv, g.fnorm + (size_t)i * g.kf,
+                 g.fcent + (size_t)i * g.kf, shapes + t, xyz(p4)};
+}
+
+__device__ __forceinline__ void store_contact(const PolyPairs& pp, uint32_t slot, const Hit& h) {
+  pp.con[2 * (size_t)slot] = make_float4(h.n.x, h.n.y, h.n.z, h.dis);
+  pp.con[2 * (size_t)slot + 1] = make_float4(h.cp.x, h.cp.y, h.cp.z, 0.0f);
+  pp.status[slot] = kSlotContact;
+}
+
+__device__ __forceinline__ void flag_status_warp(StepCtl* ctl, uint32_t bits) {
+  const unsigned m = __activemask();
+  const uint32_t all = __reduce_or_sync(m, bits);
+  if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
+}
+
+// Pass 1, one thread per neighbour slot: bounding spheres
+// (Collision_Detection_BroadPhase.cuh:369-384; a no-op in reference mode,
+// where the list holds overlapping pairs only), then the separating face
+// planes of A against B and of B against A (DEM_Kernels_Compute.cuh:842-860).
+// One queue append per block.
+__global__ void __launch_bounds__(kThreads)
+k_poly_sep(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
+           StateBuf in_sorted, NbrList nl, const StepCtl* ctl, const int* rebuilt, PolyPairs pp) {
+  __shared__ int s_cnt, s_base;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  const uint32_t slot = (uint32_t)k * (uint32_t)nl.stride + (uint32_t)i;
+  bool queue = false;
+  if (i < ctl->n_cur && k < (int)nl.cnt[i]) {
+    const StateBuf in = *rebuilt ? in_sorted : in_plain;
+    const int j = (int)nl.idx[slot];
+    const float4 pa4 = in.pos[i], pb4 = __ldg(in.pos + j);
+    uint8_t v = kSlotNone;
+    if (len3(xyz(pa4) - xyz(pb4)) - (pa4.w + pb4.w) < 0.0f) {
+      const PolyRef A = poly_ref(g, shapes, i, pa4, in.vel[i]);
+      const PolyRef B = poly_ref(g, shapes, j, pb4, __ldg(in.vel + j));
+      if (!(separated_by_face(A, B) || separated_by_face(B, A))) {
+        v = kSlotVertex;
+        queue = true;
+      }
+    }
+    pp.status[slot] = v;
+  }
+  int off = 0;
+  if (queue) off = atomicAdd(&s_cnt, 1);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_cnt) s_base = atomicAdd(&pp.counts[0], s_cnt);
+  __syncthreads();
+  if (queue) pp.qv[s_base + off] = slot;
+}
+
+// Pass 2, one thread per queued slot: vertices of A in B, then of B in A
+// with the normal reversed (DEM_Kernels_Compute.cuh:862-890).  Slots
+// without a vertex inside queue for the edge test.  Every thread runs the
+// same number of rounds so the block can append its queue entries at once.
+__global__ void __launch_bounds__(kThreads)
+k_poly_vf(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
+          StateBuf in_sorted, NbrList nl, StepCtl* ctl, const int* rebuilt, PolyPairs pp) {
+  __shared__ int s_cnt, s_base;
+  const int total = pp.counts[0];
+  const int nthreads = gridDim.x * blockDim.x;
+  const int rounds = (total + nthreads - 1) / nthreads;
+  const StateBuf in = *rebuilt ? in_sorted : in_plain;
+  uint32_t st = 0;
+  for (int r = 0; r < rounds; ++r) {
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const int e = r * nthreads + blockIdx.x * blockDim.x + threadIdx.x;
+    bool queue = false;
+    uint32_t slot = 0;
+    if (e < total) {
+      slot = pp.qv[e];
+      const int i = (int)(slot % (uint32_t)nl.stride);
+      const int j = (int)nl.idx[slot];
+      const float4 pa4 = in.pos[i], pb4 = in.pos[j];
+      const PolyRef A = poly_ref(g, shapes, i, pa4, in.vel[i]);
+      const PolyRef B = poly_ref(g, shapes, j, pb4, in.vel[j]);
+      Hit h = resolve_vertex_face(A, B, scan_vertices(A, B), st);
+      if (!h.hit) {
+        h = resolve_vertex_face(B, A, scan_vertices(B, A), st);
+        h.n = h.n * -1.0f;
+      }
+      if (h.hit) {
+        store_contact(pp, slot, h);
+      } else {
+        pp.status[slot] = kSlotEdge;
+        queue = true;
+      }
+    }
+    int off = 0;
+    if (queue) off = atomicAdd(&s_cnt, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt) s_base = atomicAdd(&pp.counts[1], s_cnt);
+    __syncthreads();
+    if (queue) pp.qe[s_base + off] = slot;
+  }
+  flag_status_warp(ctl, st);
+}
+
+// Pass 3, one warp per queued slot: the edge-edge test, depth capped at
+// 0.025 r_A (DEM_Kernels_Compute.cuh:894-915).
+__global__ void __launch_bounds__(kThreads)
+k_poly_ee(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
+          StateBuf in_plain, StateBuf in_sorted, NbrList nl, const int* rebuilt, PolyPairs pp) {
+  const int total = pp.counts[1];
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  const StateBuf in = *rebuilt ? in_sorted : in_plain;
+  for (int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < total; e += nwarps) {
+    const uint32_t slot = pp.qe[e];
+    const int i = (int)(slot % (uint32_t)nl.stride);
+    const int j = (int)nl.idx[slot];
+    const float4 pa4 = in.pos[i], pb4 = in.pos[j], va4 = in.vel[i];
+    const PolyRef A = poly_ref(g, shapes, i, pa4, va4);
+    const PolyRef B = poly_ref(g, shapes, j, pb4, in.vel[j]);
+    const float3 d = A.pos - B.pos;
+    Hit h = edge_edge(A, B, d / len3(d), lane);
+    if (h.hit) h.dis = fminf(0.025f * Pg->types[__float_as_int(va4.w) & (kMaxTypes - 1)].radius, h.dis);
+    if (lane == 0) {
+      if (h.hit) store_contact(pp, slot, h);
+      else pp.status[slot] = kSlotNone;
+    }
+  }
+}
+
+// The polyhedron step: the particle-particle sum of
+// Kernel_ParticleInteraction_Polyhedra_NonSymmetry (DEM_Kernels_Compute.cuh:
+// 736-992) over the contacts the passes found, in slot order, with the
+// reference's depth limits; VolumeObject_InteractionParticle,
+// WorldObject_InteractionParticle and Integrate_Euler_NonSymmetry with the
+// quaternion update.  One thread per particle.
 template <bool kCapture>
 __global__ void __launch_bounds__(kThreads)
 k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
             const WallOp* __restrict__ ops, StateBuf in_plain, StateBuf in_sorted, StateBuf out,
-            OrderBuf ob, int n_max, NbrList nl, StepCtl* ctl, StepLink link, ForceCapture cap) {
+            OrderBuf ob, int n_max, NbrList nl, PolyPairs pp, StepCtl* ctl, StepLink link,
+            ForceCapture cap) {
   __shared__ TypeParams sT[kMaxTypes];
   {
     const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
@@ -917,35 +1087,34 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
   float3 fl = f3(0.0f, 0.0f, 0.0f);
   const int cnt = (int)nl.cnt[i];
   for (int k = 0; k < cnt; ++k) {
-    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
+    const size_t slot = (size_t)k * nl.stride + i;
+    if (pp.status[slot] != kSlotContact) continue;
+    const int j = (int)nl.idx[slot];
     const float4 pb4 = __ldg(in.pos + j);
     const float3 pb = xyz(pb4);
-    if (!(len3(pa - pb) - (ra + pb4.w) < 0.0f)) continue;  // skin candidate, bounding spheres apart
     const float4 vb4 = __ldg(in.vel + j);
     const float3 vb = xyz(vb4), wb = xyz(__ldg(in.angv + j));
     const int tb = __float_as_int(vb4.w);
-    const int tB = tb & (kMaxTypes - 1);
-    const PolyRef B{g.vert + (size_t)j * g.kv, g.fnorm + (size_t)j * g.kf,
-                    g.fcent + (size_t)j * g.kf, shapes + tB, pb};
+    const float4 c0 = pp.con[2 * slot], c1 = pp.con[2 * slot + 1];
+    float3 n = xyz(c0), cp = xyz(c1);
+    float dis = c0.w;
     const float3 rvel = va - vb;
     const float3 d = pa - pb;
     const float3 relpos = d / len3(d);
-    Hit h = pair_contact(A, B, TA.radius, relpos, st);
-    if (!h.hit) continue;
     // depth limits of the reference (DEM_Kernels_Compute.cuh:917-950)
-    if (h.dis > 0.1500f * TA.radius) {
-      h.n = relpos / len3(relpos);
-      h.dis = 0.025f * TA.radius;
-      h.cp = pa;
+    if (dis > 0.1500f * TA.radius) {
+      n = relpos / len3(relpos);
+      dis = 0.025f * TA.radius;
+      cp = pa;
     }
-    if (h.dis > 0.0500f * TA.radius) {
-      h.n = relpos / len3(relpos);
-      h.dis = len3(rvel) > 50.0f ? 0.010f * TA.radius : 0.0030f * TA.radius;
-      h.cp = pa;
+    if (dis > 0.0500f * TA.radius) {
+      n = relpos / len3(relpos);
+      dis = len3(rvel) > 50.0f ? 0.010f * TA.radius : 0.0030f * TA.radius;
+      cp = pa;
     }
-    const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
-    const Forces F = law_pp<true>(P, rvel, h.n, h.dis, h.cp - pa, h.cp - pb, wa, wb, pp, va, vb,
-                                  ma, sT[tB].mass);
+    const PP_Parms& ppar = TA.pp[tb < kMaxPP ? tb : 0];
+    const Forces F = law_pp<true>(P, rvel, n, dis, cp - pa, cp - pb, wa, wb, ppar, va, vb, ma,
+                                  sT[tb & (kMaxTypes - 1)].mass);
     f = f + F.trans;
     fl = fl + F.torque;
   }
@@ -1006,11 +1175,7 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
       else atomicExch(&ctl->rebuild_req, 1);
     }
   }
-  {  // one atomic per warp
-    const unsigned m = __activemask();
-    const uint32_t all = __reduce_or_sync(m, st);
-    if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
-  }
+  flag_status_warp(ctl, st);
 
   if (kCapture) {
     const float3 vals[6] = {f_pp, t_pp, f_w, t_w, f_l, t_l};
@@ -1037,18 +1202,30 @@ void launch_poly_geom(const PolyShape* shapes, PolyGeom g, const StateBuf& in_pl
                                                                        ctl, rebuilt);
 }
 
+int launch_poly_pairs(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
+                      const StateBuf& in_plain, const StateBuf& in_sorted, int n_max, NbrList nl,
+                      StepCtl* ctl, const int* rebuilt, PolyPairs pp, cudaStream_t st) {
+  cudaMemsetAsync(pp.counts, 0, 2 * sizeof(int), st);
+  const dim3 g1(blocks_for(n_max), nl.cap);
+  k_poly_sep<<<g1, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, ctl, rebuilt, pp);
+  k_poly_vf<<<pp.grid_v, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, ctl, rebuilt, pp);
+  k_poly_ee<<<pp.grid_e, kThreads, 0, st>>>(dp, shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
+  return 3;
+}
+
 void launch_poly_step(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const WallOp* ops, const StateBuf& in_plain, const StateBuf& in_sorted,
                       const StateBuf& out, const OrderBuf& ob, int n_max, NbrList nl,
-                      StepCtl* ctl, StepLink link, const ForceCapture* cap, cudaStream_t st) {
+                      PolyPairs pp, StepCtl* ctl, StepLink link, const ForceCapture* cap,
+                      cudaStream_t st) {
   const ForceCapture c = cap ? *cap : ForceCapture{};
   const int gr = blocks_for(n_max);
   if (cap)
     k_poly_step<true><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
-                                               n_max, nl, ctl, link, c);
+                                               n_max, nl, pp, ctl, link, c);
   else
     k_poly_step<false><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
-                                                n_max, nl, ctl, link, c);
+                                                n_max, nl, pp, ctl, link, c);
 }
 
 }  // namespace blaze

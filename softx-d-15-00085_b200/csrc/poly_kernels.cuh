@@ -6,9 +6,13 @@
 //   k_poly_geom  world-frame vertices and face planes of every particle,
 //                written once (the reference rotates particle B again for
 //                every pair, DEM_Kernels_Compute.cuh:820);
-//   k_poly_step  particle-particle narrow phase and law, world objects and
-//                symplectic Euler with the quaternion update, fused, one
-//                thread per particle, gather only.
+//   k_poly_sep, k_poly_vf, k_poly_ee
+//                the narrow phase in three passes over the neighbour slots
+//                (separating planes per slot, vertex-face per queued slot,
+//                edge-edge per queued slot with a warp each);
+//   k_poly_step  particle-particle law over the contacts found, volume and
+//                world objects, symplectic Euler with the quaternion update,
+//                one thread per particle, gather only.
 // Orientations live beside P_ID (two copies selected by the re-sort count),
 // gathered by the re-sort and updated in place by the step.
 #pragma once
@@ -47,13 +51,31 @@ struct PolyGeom {
   int kv, kf;
 };
 
+// Narrow-phase state of one step, per neighbour slot (slot = k * stride + i):
+// the verdict of the passes and, for a contact, its normal, depth and point.
+struct PolyPairs {
+  uint8_t* status;    // cap x stride: 0 none, 1 vertex test pending, 2 contact, 3 edge test pending
+  float4* con;        // 2 x cap x stride: (normal, depth), (contact point, 0)
+  uint32_t* qv;       // slots queued for the vertex-face test
+  uint32_t* qe;       // slots queued for the edge-edge test
+  int* counts;        // [0] vertex-face queue length, [1] edge-edge queue length
+  int grid_v, grid_e; // blocks of the two queue passes (persistent grids)
+};
+
 void launch_poly_geom(const PolyShape* shapes, PolyGeom g, const StateBuf& in_plain,
                       const StateBuf& in_sorted, const OrderBuf& ob, int n_max, int rotation,
                       const StepCtl* ctl, const int* rebuilt, cudaStream_t st);
 
+// The three narrow-phase passes (separating planes, vertex-face, edge-edge)
+// over the step's neighbour slots; returns the number of kernel launches.
+int launch_poly_pairs(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
+                      const StateBuf& in_plain, const StateBuf& in_sorted, int n_max, NbrList nl,
+                      StepCtl* ctl, const int* rebuilt, PolyPairs pp, cudaStream_t st);
+
 void launch_poly_step(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const WallOp* ops, const StateBuf& in_plain, const StateBuf& in_sorted,
                       const StateBuf& out, const OrderBuf& ob, int n_max, NbrList nl,
-                      StepCtl* ctl, StepLink link, const ForceCapture* cap, cudaStream_t st);
+                      PolyPairs pp, StepCtl* ctl, StepLink link, const ForceCapture* cap,
+                      cudaStream_t st);
 
 }  // namespace blaze
