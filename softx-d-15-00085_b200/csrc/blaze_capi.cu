@@ -360,8 +360,12 @@ int alloc_poly_pairs(blaze_sim* s) {
   CK(dalloc(&pp.con, 2 * slots));
   CK(dalloc(&pp.qv, slots));
   CK(dalloc(&pp.qe, slots));
-  CK(dalloc(&pp.counts, 2));
-  CK(cudaMemset(pp.counts, 0, 2 * sizeof(int)));
+  CK(dalloc(&pp.counts, 3));
+  CK(cudaMemset(pp.counts, 0, 3 * sizeof(int)));
+  // the contact-list kernel also lists every filled slot for the passes
+  if (s->nl.flat) CK(cudaFree(s->nl.flat));
+  CK(dalloc(&s->nl.flat, slots));
+  s->nl.flat_n = pp.counts + 2;
   int dev = 0, sms = 148;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -374,6 +378,9 @@ int alloc_nlist(blaze_sim* s) {
   drop_graphs(s);
   if (s->nl.idx) CK(cudaFree(s->nl.idx));
   if (s->nl.cnt) CK(cudaFree(s->nl.cnt));
+  if (s->nl.flat) CK(cudaFree(s->nl.flat));
+  s->nl.flat = nullptr;
+  s->nl.flat_n = nullptr;
   s->nl.stride = s->n_max;
   s->nl.cap = s->opt.max_nbr;
   CK(dalloc(&s->nl.idx, (size_t)s->n_max * s->nl.cap));
@@ -403,7 +410,7 @@ int enqueue_rebuild(blaze_sim* s, const int* gate, cudaStream_t st) {
   const size_t cbytes = sizeof(uint32_t) * s->hp.ncell_tab;
   CK(cudaMemsetAsync(s->cstart, 0xff, cbytes, st));
   launch_reorder(s->S[s->cur], s->S[2], s->ob, n, s->rs.keys[res], s->rs.vals[res], s->cstart,
-                 s->cend, s->hp.ncell_tab, s->n_d > 0, s->ctl, gate, st);
+                 s->cend, s->hp.ncell_tab, s->n_d > 0, s->nl.flat_n, s->ctl, gate, st);
   launch_nlist(s->dp, s->S[2], n, s->cstart, s->cend, s->nl, s->ctl, gate, st);
   s->last_launches += 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits);
   return 0;
@@ -637,6 +644,7 @@ void free_sim(blaze_sim* s) {
   f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
   f(s->geom.vert); f(s->geom.fnorm); f(s->geom.fcent);
   f(s->pairs.status); f(s->pairs.con); f(s->pairs.qv); f(s->pairs.qe); f(s->pairs.counts);
+  f(s->nl.flat);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);

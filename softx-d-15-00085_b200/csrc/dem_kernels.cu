@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kThreads)
 k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
           const uint32_t* __restrict__ keys, const int32_t* __restrict__ perm,
           uint32_t* __restrict__ cstart, uint32_t* __restrict__ cend, uint32_t ncell_tab,
-          int has_lift, StepCtl* ctl, const int* gate) {
+          int has_lift, int* flat_n, StepCtl* ctl, const int* gate) {
   if (gate && *gate == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int e = ctl->epoch & 1;
@@ -107,6 +107,7 @@ k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
     // the particles removed since the last re-sort are now at the end
     ctl->n_cur -= ctl->pending_dead;
     ctl->pending_dead = 0;
+    if (flat_n) *flat_n = 0;  // the contact-list kernel lists the slots anew
   }
   if (i >= n_max) return;
   const int j = perm[i];
@@ -181,7 +182,24 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
           }
         }
   }
-  nl.cnt[i] = cnt < (uint32_t)nl.cap ? cnt : (uint32_t)nl.cap;
+  const uint32_t kept = cnt < (uint32_t)nl.cap ? cnt : (uint32_t)nl.cap;
+  nl.cnt[i] = kept;
+  if (nl.flat) {
+    // append this particle's slots to the flat list: one atomic per warp;
+    // the lanes still here (i < n) are a prefix of the warp
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31;
+    uint32_t x = kept;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(m, x, d);
+      if (lane >= d) x += y;
+    }
+    const int last = 31 - __clz((int)m);
+    uint32_t base = 0;
+    if (lane == last) base = (uint32_t)atomicAdd(nl.flat_n, (int)x);
+    base = __shfl_sync(m, base, last) + (x - kept);
+    for (uint32_t k = 0; k < kept; ++k) nl.flat[base + k] = k * (uint32_t)nl.stride + (uint32_t)i;
+  }
   flag_status(ctl, st);
 }
 
@@ -544,10 +562,11 @@ void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int
 
 void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
                     const uint32_t* sorted_keys, const int32_t* perm, uint32_t* cell_start,
-                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, StepCtl* ctl,
-                    const int* gate, cudaStream_t st) {
+                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, int* flat_n,
+                    StepCtl* ctl, const int* gate, cudaStream_t st) {
   k_reorder<<<blocks(n_max), kThreads, 0, st>>>(src, dst, ob, n_max, sorted_keys, perm, cell_start,
-                                                cell_end, ncell_tab, has_lift ? 1 : 0, ctl, gate);
+                                                cell_end, ncell_tab, has_lift ? 1 : 0, flat_n,
+                                                ctl, gate);
 }
 
 void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,

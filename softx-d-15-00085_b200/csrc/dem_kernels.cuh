@@ -39,6 +39,8 @@ struct NbrList {
   uint32_t* cnt;
   int stride;           // >= n_max
   int cap;
+  uint32_t* flat;       // optional: every filled slot k * stride + i, particle by particle
+  int* flat_n;          // entries in `flat` (reset before each rebuild)
 };
 
 // How a step learns whether it consumes a fresh re-sort, and how it asks for
@@ -74,10 +76,11 @@ void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int
                        cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
+// (flat_n, when given, is reset for the contact-list kernel's flat list)
 void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob, int n_max,
                     const uint32_t* sorted_keys, const int32_t* perm, uint32_t* cell_start,
-                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, StepCtl* ctl,
-                    const int* gate, cudaStream_t st);
+                    uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, int* flat_n,
+                    StepCtl* ctl, const int* gate, cudaStream_t st);
 void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
                   const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
                   cudaStream_t st);

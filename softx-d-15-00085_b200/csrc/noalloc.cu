@@ -166,12 +166,14 @@ extern "C" int blaze_contact_list_static(const float* pos4, int n, const Simulat
   launch_hash(dp, src, ob, n, rs.keys[0], ctl, nullptr, st);
   const int res = radix_sort_pairs(rs, n, bits, true, nullptr, st);
   launch_reorder(src, dst, ob, n, rs.keys[res], rs.vals[res], cstart, cend, (uint32_t)ntab,
-                 false, ctl, nullptr, st);
+                 false, nullptr, ctl, nullptr, st);
   NbrList nl;
   nl.idx = list;
   nl.cnt = nn;
   nl.stride = n;
   nl.cap = max_nbr;
+  nl.flat = nullptr;
+  nl.flat_n = nullptr;
   launch_nlist(dp, dst, n, cstart, cend, nl, ctl, nullptr, st);
   CKS(cudaMemcpyAsync(perm, rs.vals[res], sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
   if (status)

@@ -103,35 +103,65 @@ __device__ __forceinline__ float3 shfl3(float3 v, int src) {
             __shfl_sync(kFull, v.z, src));
 }
 
-// is_SP_Poly_Poly (Utilities.cuh:105-156): a face plane of `a` with the
-// centre of `b` on its outer side and every vertex of `b` strictly outside.
-__device__ bool separated_by_face(const PolyRef& a, const PolyRef& b) {
-  const int nf = a.s->nf, nv = b.s->nv;
-  for (int f = 0; f < nf; ++f) {
-    const float3 n = ld3(a.fn + f), c = ld3(a.fc + f);
-    if (!(dot3(n, b.pos - c) > 0.0f)) continue;
-    bool touching = false;
-    for (int k = 0; k < nv; ++k)
-      if (dot3(n, ld3(b.v + k) - c) <= 0.00000f) { touching = true; break; }
-    if (!touching) return true;
+// The face of `a` whose normal points most nearly at `p` (first of equals).
+__device__ int face_towards(const PolyRef& a, float3 p) {
+  const float3 d = p - a.pos;
+  int best = 0;
+  float bd = dot3(ld3(a.fn), d);
+  for (int f = 1; f < a.s->nf; ++f) {
+    const float t = dot3(ld3(a.fn + f), d);
+    if (t > bd) { bd = t; best = f; }
   }
+  return best;
+}
+
+// One face of is_SP_Poly_Poly: the centre of `b` on the face's outer side
+// and every vertex of `b` strictly outside its plane.  The vertices are
+// loaded four at a time (the test is an AND over them).
+__device__ bool face_separates(const PolyRef& a, int f, const PolyRef& b) {
+  const float3 n = ld3(a.fn + f), c = ld3(a.fc + f);
+  if (!(dot3(n, b.pos - c) > 0.0f)) return false;
+  const int nv = b.s->nv;
+  int k = 0;
+  for (; k + 4 <= nv; k += 4) {
+    const float3 v0 = ld3(b.v + k), v1 = ld3(b.v + k + 1);
+    const float3 v2 = ld3(b.v + k + 2), v3 = ld3(b.v + k + 3);
+    const bool out = dot3(n, v0 - c) > 0.00000f && dot3(n, v1 - c) > 0.00000f &&
+                     dot3(n, v2 - c) > 0.00000f && dot3(n, v3 - c) > 0.00000f;
+    if (!out) return false;
+  }
+  for (; k < nv; ++k)
+    if (dot3(n, ld3(b.v + k) - c) <= 0.00000f) return false;
+  return true;
+}
+
+// is_SP_Poly_Poly (Utilities.cuh:105-156): does any face plane of `a`
+// separate `b`?
+__device__ bool separated_by_face(const PolyRef& a, const PolyRef& b) {
+  const int nf = a.s->nf;
+  for (int f = 0; f < nf; ++f)
+    if (face_separates(a, f, b)) return true;
   return false;
 }
 
 // Collision_Detection_Vertex_InPoly_3Faces (CDP:287-382): is `v` behind
 // every face plane of `b`, and which three faces (with the owner's centre on
-// their outer side) are nearest to it.
+// their outer side) are nearest to it, in the reference's face order.
 struct Inside {
   bool in;
   int face[3];
   float dist[3];
 };
 
-__device__ Inside vertex_inside(float3 owner, float3 v, const PolyRef& b) {
+__device__ Inside vertex_inside(float3 owner, float3 v, const PolyRef& b, int reject) {
   Inside r;
   r.in = false;
   r.face[0] = r.face[1] = r.face[2] = -1;
   r.dist[0] = r.dist[1] = r.dist[2] = 10.0f;
+  // a vertex outside any one face plane is not inside (the reference stops
+  // at the first such face, whichever it is, and reports only that); the
+  // face `reject` is the likeliest one and is tried first
+  if (!(dot3(ld3(b.fn + reject), v - ld3(b.fc + reject)) < -0.0000100f)) return r;
   const int nf = b.s->nf;
   for (int f = 0; f < nf; ++f) {
     const float3 n = ld3(b.fn + f), c = ld3(b.fc + f);
@@ -208,10 +238,11 @@ __device__ VertexScan scan_vertices(const PolyRef& a, const PolyRef& b) {
   r.s0.face[0] = r.s0.face[1] = r.s0.face[2] = -1;
   r.s0.dist[0] = r.s0.dist[1] = r.s0.dist[2] = 10.0f;
   r.sum = f3(0.0f, 0.0f, 0.0f);
+  const int reject = face_towards(b, a.pos);  // b's face turned to a
   const int nv = a.s->nv;
   for (int k = 0; k < nv; ++k) {
     const float3 v = ld3(a.v + k);
-    const Inside t = vertex_inside(a.pos, v, b);
+    const Inside t = vertex_inside(a.pos, v, b, reject);
     if (!t.in) continue;
     if (r.count == 0) { r.s0 = t; r.i0 = k; }
     else if (r.count == 1) { r.s1_face1 = t.face[1]; r.i1 = k; }
@@ -299,10 +330,10 @@ __device__ bool point_in_poly(const PolyRef& b, float3 pt) {
 // Collision_Detection_Polyhedra_Polyhedra_Edges (CDP:537-707): the closest
 // pair of points between an edge of `a` and an edge of `b` (parameters
 // within [-0.01, 1.01]), normal along the edges' cross product turned
-// towards `relpos`.  Lane l scans the pairs l, l + 32, ... of the (edge of
-// a, edge of b) sequence, keeping its first strict minimum; the warp then
-// takes the smallest distance, the lowest pair index among equals, which is
-// the pair the reference's sequential scan selects.
+// towards `relpos`.  Lane l scans the pairs t = l, l + 32, ... of the
+// sequence t = i * ne_b + j (edges of a outer, edges of b inner), keeping its
+// first strict minimum; the warp then takes the smallest distance, the
+// lowest t among equals: the pair the reference's sequential scan selects.
 __device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos, int lane) {
   Hit h = no_hit();
   const int nea = a.s->ne, neb = b.s->ne;
@@ -310,37 +341,45 @@ __device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos, int 
   float best = 5.0f;
   int bidx = 0x7fffffff;
   float3 nrm = f3(0.0f, 0.0f, 0.0f), qa_sel = nrm, qb_sel = nrm;
-  for (int t = lane; t < total; t += 32) {
-    const int i = t / neb, j = t - i * neb;
-    const float3 ap = ld3(a.v + a.s->edge[i][0]);
-    const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
-    const float3 bp = ld3(b.v + b.s->edge[j][0]);
-    const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
-    const float3 c = cross3(ad, bd);
-    if (!(dot3(c, c) > 0.00000f)) continue;
-    const float daa = dot3(ad, ad);
-    const float3 dv = ap - bp;
-    const float dbb = dot3(bd, bd);
-    const float dab = dot3(ad, bd);
-    const float dav = dot3(ad, dv);
-    const float dbv = dot3(bd, dv);
-    const float inv = 1.00000f / (dab * dab - daa * dbb);
-    const float ta = inv * (dbb * dav - dab * dbv);
-    if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
-    const float tb = inv * (dab * dav - daa * dbv);
-    if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
-    const float3 qa = ap + ad * ta;
-    const float3 qb = bp + bd * tb;
-    const float3 d = qa - qb;
-    float dist = dot3(d, d);
-    if (!(dist > 0.00000f)) continue;
-    dist = sqrtf(dist);
-    if (dist < best) {
-      best = dist;
-      bidx = t;
-      nrm = c;
-      qa_sel = qa;
-      qb_sel = qb;
+  if (total > 0) {
+    // (i, j) of t = lane, advanced by 32 = q ne_b + r each round
+    const int q = 32 / neb, r = 32 - q * neb;
+    int i = lane / neb, j = lane - i * neb;
+    for (int t = lane; t < total; t += 32) {
+      const float3 ap = ld3(a.v + a.s->edge[i][0]);
+      const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
+      const float3 bp = ld3(b.v + b.s->edge[j][0]);
+      const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
+      const int ti = i, tj = j;
+      i += q;
+      j += r;
+      if (j >= neb) { j -= neb; ++i; }
+      const float3 c = cross3(ad, bd);
+      if (!(dot3(c, c) > 0.00000f)) continue;
+      const float daa = dot3(ad, ad);
+      const float3 dv = ap - bp;
+      const float dbb = dot3(bd, bd);
+      const float dab = dot3(ad, bd);
+      const float dav = dot3(ad, dv);
+      const float dbv = dot3(bd, dv);
+      const float inv = __frcp_rn(dab * dab - daa * dbb);  // = 1.0f / (...), correctly rounded
+      const float ta = inv * (dbb * dav - dab * dbv);
+      if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
+      const float tb = inv * (dab * dav - daa * dbv);
+      if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
+      const float3 qa = ap + ad * ta;
+      const float3 qb = bp + bd * tb;
+      const float3 d = qa - qb;
+      float dist = dot3(d, d);
+      if (!(dist > 0.00000f)) continue;
+      dist = sqrtf(dist);
+      if (dist < best) {
+        best = dist;
+        bidx = ti * neb + tj;
+        nrm = c;
+        qa_sel = qa;
+        qb_sel = qb;
+      }
     }
   }
 #pragma unroll
@@ -928,42 +967,49 @@ __device__ __forceinline__ void flag_status_warp(StepCtl* ctl, uint32_t bits) {
   if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
 }
 
-// Pass 1, one thread per neighbour slot: bounding spheres
-// (Collision_Detection_BroadPhase.cuh:369-384; a no-op in reference mode,
-// where the list holds overlapping pairs only), then the separating face
-// planes of A against B and of B against A (DEM_Kernels_Compute.cuh:842-860).
-// One queue append per block.
+// Pass 1, one thread per filled neighbour slot (the contact-list kernel's
+// flat list): bounding spheres (Collision_Detection_BroadPhase.cuh:369-384;
+// a no-op in reference mode, where the list holds overlapping pairs only),
+// then the separating face planes of A against B and of B against A
+// (DEM_Kernels_Compute.cuh:842-860).  Every thread runs the same number of
+// rounds so the block can append its queue entries at once.
 __global__ void __launch_bounds__(kThreads)
 k_poly_sep(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
-           StateBuf in_sorted, NbrList nl, const StepCtl* ctl, const int* rebuilt, PolyPairs pp) {
+           StateBuf in_sorted, NbrList nl, const int* rebuilt, PolyPairs pp) {
   __shared__ int s_cnt, s_base;
-  if (threadIdx.x == 0) s_cnt = 0;
-  __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  const uint32_t slot = (uint32_t)k * (uint32_t)nl.stride + (uint32_t)i;
-  bool queue = false;
-  if (i < ctl->n_cur && k < (int)nl.cnt[i]) {
-    const StateBuf in = *rebuilt ? in_sorted : in_plain;
-    const int j = (int)nl.idx[slot];
-    const float4 pa4 = in.pos[i], pb4 = __ldg(in.pos + j);
-    uint8_t v = kSlotNone;
-    if (len3(xyz(pa4) - xyz(pb4)) - (pa4.w + pb4.w) < 0.0f) {
-      const PolyRef A = poly_ref(g, shapes, i, pa4, in.vel[i]);
-      const PolyRef B = poly_ref(g, shapes, j, pb4, __ldg(in.vel + j));
-      if (!(separated_by_face(A, B) || separated_by_face(B, A))) {
-        v = kSlotVertex;
-        queue = true;
+  const int total = *nl.flat_n;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int rounds = (total + nthreads - 1) / nthreads;
+  const StateBuf in = *rebuilt ? in_sorted : in_plain;
+  for (int r = 0; r < rounds; ++r) {
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const int e = r * nthreads + blockIdx.x * blockDim.x + threadIdx.x;
+    bool queue = false;
+    uint32_t slot = 0;
+    if (e < total) {
+      slot = nl.flat[e];
+      const int i = (int)(slot % (uint32_t)nl.stride);
+      const int j = (int)nl.idx[slot];
+      const float4 pa4 = in.pos[i], pb4 = __ldg(in.pos + j);
+      uint8_t v = kSlotNone;
+      if (len3(xyz(pa4) - xyz(pb4)) - (pa4.w + pb4.w) < 0.0f) {
+        const PolyRef A = poly_ref(g, shapes, i, pa4, in.vel[i]);
+        const PolyRef B = poly_ref(g, shapes, j, pb4, __ldg(in.vel + j));
+        if (!(separated_by_face(A, B) || separated_by_face(B, A))) {
+          v = kSlotVertex;
+          queue = true;
+        }
       }
+      pp.status[slot] = v;
     }
-    pp.status[slot] = v;
+    int off = 0;
+    if (queue) off = atomicAdd(&s_cnt, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt) s_base = atomicAdd(&pp.counts[0], s_cnt);
+    __syncthreads();
+    if (queue) pp.qv[s_base + off] = slot;
   }
-  int off = 0;
-  if (queue) off = atomicAdd(&s_cnt, 1);
-  __syncthreads();
-  if (threadIdx.x == 0 && s_cnt) s_base = atomicAdd(&pp.counts[0], s_cnt);
-  __syncthreads();
-  if (queue) pp.qv[s_base + off] = slot;
 }
 
 // Pass 2, one thread per queued slot: vertices of A in B, then of B in A
@@ -1206,8 +1252,7 @@ int launch_poly_pairs(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const StateBuf& in_plain, const StateBuf& in_sorted, int n_max, NbrList nl,
                       StepCtl* ctl, const int* rebuilt, PolyPairs pp, cudaStream_t st) {
   cudaMemsetAsync(pp.counts, 0, 2 * sizeof(int), st);
-  const dim3 g1(blocks_for(n_max), nl.cap);
-  k_poly_sep<<<g1, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, ctl, rebuilt, pp);
+  k_poly_sep<<<pp.grid_v, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
   k_poly_vf<<<pp.grid_v, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, ctl, rebuilt, pp);
   k_poly_ee<<<pp.grid_e, kThreads, 0, st>>>(dp, shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
   return 3;

@@ -58,7 +58,8 @@ struct PolyPairs {
   float4* con;        // 2 x cap x stride: (normal, depth), (contact point, 0)
   uint32_t* qv;       // slots queued for the vertex-face test
   uint32_t* qe;       // slots queued for the edge-edge test
-  int* counts;        // [0] vertex-face queue length, [1] edge-edge queue length
+  int* counts;        // [0] vertex-face queue length, [1] edge-edge queue length,
+                      // [2] filled neighbour slots (NbrList::flat_n)
   int grid_v, grid_e; // blocks of the two queue passes (persistent grids)
 };
 
