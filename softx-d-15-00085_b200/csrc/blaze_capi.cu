@@ -705,6 +705,20 @@ int setup_poly(blaze_sim* s) {
     }
     for (int k = 0; k < 9; ++k) S.inertia[k] = o.InertiaT[k];
     S.com[0] = o.COM.x; S.com[1] = o.COM.y; S.com[2] = o.COM.z;
+    // bounds the edge-edge pruning relies on, rounded up (rotation preserves
+    // lengths up to a few units in the last place)
+    double rmax = 0.0, emax = 0.0;
+    for (int k = 0; k < S.nv; ++k) {
+      const double x = o.Local_Vertex[k].x, y = o.Local_Vertex[k].y, z = o.Local_Vertex[k].z;
+      rmax = std::max(rmax, std::sqrt(x * x + y * y + z * z));
+    }
+    for (int e = 0; e < S.ne; ++e) {
+      const float3 a = o.Local_Vertex[S.edge[e][0]], b = o.Local_Vertex[S.edge[e][1]];
+      const double dx = (double)b.x - a.x, dy = (double)b.y - a.y, dz = (double)b.z - a.z;
+      emax = std::max(emax, std::sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    S.rmax = (float)(rmax * (1.0 + 1e-5) + 1e-6);
+    S.emax = (float)(emax * (1.0 + 1e-5) + 1e-6);
     kv = std::max(kv, S.nv);
     kf = std::max(kf, S.nf);
   }

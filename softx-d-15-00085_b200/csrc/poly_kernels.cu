@@ -327,72 +327,161 @@ __device__ bool point_in_poly(const PolyRef& b, float3 pt) {
   return true;
 }
 
+// One edge pair of Collision_Detection_Polyhedra_Polyhedra_Edges
+// (CDP:537-707) with the reference's arithmetic: false when the pair is
+// rejected (parallel edges, a closest-point parameter outside
+// [-0.01, 1.01], coincident points), else the points' distance, the edges'
+// cross product and the two points.
+struct EdgePair {
+  float dist;
+  float3 c, qa, qb;
+};
+
+__device__ __forceinline__ bool eval_edge_pair(const PolyRef& a, const PolyRef& b, int i, int j,
+                                               EdgePair& out) {
+  const float3 ap = ld3(a.v + a.s->edge[i][0]);
+  const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
+  const float3 bp = ld3(b.v + b.s->edge[j][0]);
+  const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
+  const float3 c = cross3(ad, bd);
+  if (!(dot3(c, c) > 0.00000f)) return false;
+  const float daa = dot3(ad, ad);
+  const float3 dv = ap - bp;
+  const float dbb = dot3(bd, bd);
+  const float dab = dot3(ad, bd);
+  const float dav = dot3(ad, dv);
+  const float dbv = dot3(bd, dv);
+  const float inv = __frcp_rn(dab * dab - daa * dbb);  // = 1.0f / (...), correctly rounded
+  const float ta = inv * (dbb * dav - dab * dbv);
+  if (!(ta >= -0.010f && ta <= 1.0100f)) return false;
+  const float tb = inv * (dab * dav - daa * dbv);
+  if (!(tb >= -0.0100f && tb <= 1.010f)) return false;
+  const float3 qa = ap + ad * ta;
+  const float3 qb = bp + bd * tb;
+  const float3 d = qa - qb;
+  float dist = dot3(d, d);
+  if (!(dist > 0.00000f)) return false;
+  out.dist = sqrtf(dist);
+  out.c = c;
+  out.qa = qa;
+  out.qb = qb;
+  return true;
+}
+
+// Distance from p to the edge (ap, ap + ad) extended by 1% at both ends
+// (where the reference's closest points may lie).
+__device__ __forceinline__ float extended_edge_distance(float3 p, float3 ap, float3 ad) {
+  const float dd = dot3(ad, ad);
+  float t = dd > 0.0f ? dot3(p - ap, ad) / dd : 0.0f;
+  t = fminf(fmaxf(t, -0.01f), 1.01f);
+  return len3(p - (ap + ad * t));
+}
+
+// The lanes holding the three smallest values (lowest lane among equals), or
+// -1 past the values there are.
+__device__ __forceinline__ void three_smallest(float v, int lane, int out[3]) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    float mv = v;
+    int ml = lane;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float ov = __shfl_xor_sync(kFull, mv, off);
+      const int ol = __shfl_xor_sync(kFull, ml, off);
+      if (ov < mv || (ov == mv && ol < ml)) { mv = ov; ml = ol; }
+    }
+    out[r] = mv < INFINITY ? ml : -1;
+    if (lane == ml) v = INFINITY;
+  }
+}
+
 // Collision_Detection_Polyhedra_Polyhedra_Edges (CDP:537-707): the closest
 // pair of points between an edge of `a` and an edge of `b` (parameters
-// within [-0.01, 1.01]), normal along the edges' cross product turned
-// towards `relpos`.  Lane l scans the pairs t = l, l + 32, ... of the
-// sequence t = i * ne_b + j (edges of a outer, edges of b inner), keeping its
-// first strict minimum; the warp then takes the smallest distance, the
-// lowest t among equals: the pair the reference's sequential scan selects.
-__device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos, int lane) {
+// within [-0.01, 1.01]), the first minimum in the order (edges of a outer,
+// edges of b inner), normal along the edges' cross product turned towards
+// `relpos`.
+//
+// Not every pair needs evaluating.  An edge of a at distance L from b's
+// centre, with every point of b's edges within R of it, is at least L - R
+// from any of them; with a rounding margin that is a lower bound for all
+// pairs in its row (likewise for columns).  The exact distances of the
+// 3 x 3 pairs of smallest bounds give an upper bound U on the minimum; a row
+// or column whose bound exceeds U holds only pairs farther than U, so the
+// minimum and the first pair attaining it lie among the remaining rows and
+// columns, which the lanes evaluate exactly.  Ties go to the lowest pair
+// index, as in the sequential scan.  s_idx: 64 ints of shared memory for
+// this warp.
+__device__ Hit edge_edge(const PolyRef& a, const PolyRef& b, float3 relpos, int lane,
+                         int* s_idx) {
   Hit h = no_hit();
   const int nea = a.s->ne, neb = b.s->ne;
-  const int total = nea * neb;
+  if (nea <= 0 || neb <= 0) return h;
+  // coordinate scale of the rounding margin
+  const float M = 1.0f + a.s->rmax + b.s->rmax +
+                  fmaxf(fmaxf(fmaxf(fabsf(a.pos.x), fabsf(a.pos.y)), fabsf(a.pos.z)),
+                        fmaxf(fmaxf(fabsf(b.pos.x), fabsf(b.pos.y)), fabsf(b.pos.z)));
+  const float marg = 1e-5f + 8e-6f * M;
+  float lba = INFINITY, lbb = INFINITY;
+  if (lane < nea) {
+    const float3 ap = ld3(a.v + a.s->edge[lane][0]);
+    const float3 ad = ld3(a.v + a.s->edge[lane][1]) - ap;
+    lba = extended_edge_distance(b.pos, ap, ad) - (b.s->rmax + 0.0101f * b.s->emax) - marg;
+  }
+  if (lane < neb) {
+    const float3 bp = ld3(b.v + b.s->edge[lane][0]);
+    const float3 bd = ld3(b.v + b.s->edge[lane][1]) - bp;
+    lbb = extended_edge_distance(a.pos, bp, bd) - (a.s->rmax + 0.0101f * a.s->emax) - marg;
+  }
+  int rs[3], cs[3];
+  three_smallest(lba, lane, rs);
+  three_smallest(lbb, lane, cs);
   float best = 5.0f;
   int bidx = 0x7fffffff;
   float3 nrm = f3(0.0f, 0.0f, 0.0f), qa_sel = nrm, qb_sel = nrm;
-  if (total > 0) {
-    // (i, j) of t = lane, advanced by 32 = q ne_b + r each round
-    const int q = 32 / neb, r = 32 - q * neb;
-    int i = lane / neb, j = lane - i * neb;
-    for (int t = lane; t < total; t += 32) {
-      const float3 ap = ld3(a.v + a.s->edge[i][0]);
-      const float3 ad = ld3(a.v + a.s->edge[i][1]) - ap;
-      const float3 bp = ld3(b.v + b.s->edge[j][0]);
-      const float3 bd = ld3(b.v + b.s->edge[j][1]) - bp;
-      const int ti = i, tj = j;
-      i += q;
-      j += r;
-      if (j >= neb) { j -= neb; ++i; }
-      const float3 c = cross3(ad, bd);
-      if (!(dot3(c, c) > 0.00000f)) continue;
-      const float daa = dot3(ad, ad);
-      const float3 dv = ap - bp;
-      const float dbb = dot3(bd, bd);
-      const float dab = dot3(ad, bd);
-      const float dav = dot3(ad, dv);
-      const float dbv = dot3(bd, dv);
-      const float inv = __frcp_rn(dab * dab - daa * dbb);  // = 1.0f / (...), correctly rounded
-      const float ta = inv * (dbb * dav - dab * dbv);
-      if (!(ta >= -0.010f && ta <= 1.0100f)) continue;
-      const float tb = inv * (dab * dav - daa * dbv);
-      if (!(tb >= -0.0100f && tb <= 1.010f)) continue;
-      const float3 qa = ap + ad * ta;
-      const float3 qb = bp + bd * tb;
-      const float3 d = qa - qb;
-      float dist = dot3(d, d);
-      if (!(dist > 0.00000f)) continue;
-      dist = sqrtf(dist);
-      if (dist < best) {
-        best = dist;
-        bidx = ti * neb + tj;
-        nrm = c;
-        qa_sel = qa;
-        qb_sel = qb;
-      }
+  auto consider = [&](int i, int j) {
+    EdgePair e;
+    if (!eval_edge_pair(a, b, i, j, e)) return;
+    const int t = i * neb + j;
+    if (e.dist < best || (e.dist == best && t < bidx)) {
+      best = e.dist;
+      bidx = t;
+      nrm = e.c;
+      qa_sel = e.qa;
+      qb_sel = e.qb;
     }
+  };
+  if (lane < 9) {
+    const int i = rs[lane / 3], j = cs[lane % 3];
+    if (i >= 0 && j >= 0) consider(i, j);
   }
+  float ub = best;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) ub = fminf(ub, __shfl_xor_sync(kFull, ub, off));
+  const unsigned mr = __ballot_sync(kFull, lane < nea && !(lba > ub));
+  const unsigned mc = __ballot_sync(kFull, lane < neb && !(lbb > ub));
+  const unsigned below = (1u << lane) - 1u;
+  if ((mr >> lane) & 1u) s_idx[__popc(mr & below)] = lane;
+  if ((mc >> lane) & 1u) s_idx[32 + __popc(mc & below)] = lane;
+  __syncwarp();
+  const int nr = __popc(mr), nc = __popc(mc);
+  for (int t = lane; t < nr * nc; t += 32) {
+    const int ri = t / nc;
+    consider(s_idx[ri], s_idx[32 + t - ri * nc]);
+  }
+  __syncwarp();
+  int src = lane;
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     const float ob = __shfl_xor_sync(kFull, best, off);
     const int oi = __shfl_xor_sync(kFull, bidx, off);
+    const int os = __shfl_xor_sync(kFull, src, off);
     if (ob < best || (ob == best && oi < bidx)) {
       best = ob;
       bidx = oi;
+      src = os;
     }
   }
   if (bidx == 0x7fffffff) return h;
-  const int src = bidx & 31;
   nrm = shfl3(nrm, src);
   qa_sel = shfl3(qa_sel, src);
   qb_sel = shfl3(qb_sel, src);
@@ -1065,6 +1154,7 @@ k_poly_vf(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
 __global__ void __launch_bounds__(kThreads)
 k_poly_ee(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
           StateBuf in_plain, StateBuf in_sorted, NbrList nl, const int* rebuilt, PolyPairs pp) {
+  __shared__ int s_idx[kThreads / 32][64];
   const int total = pp.counts[1];
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
@@ -1077,7 +1167,7 @@ k_poly_ee(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes
     const PolyRef A = poly_ref(g, shapes, i, pa4, va4);
     const PolyRef B = poly_ref(g, shapes, j, pb4, in.vel[j]);
     const float3 d = A.pos - B.pos;
-    Hit h = edge_edge(A, B, d / len3(d), lane);
+    Hit h = edge_edge(A, B, d / len3(d), lane, s_idx[threadIdx.x >> 5]);
     if (h.hit) h.dis = fminf(0.025f * Pg->types[__float_as_int(va4.w) & (kMaxTypes - 1)].radius, h.dis);
     if (lane == 0) {
       if (h.hit) store_contact(pp, slot, h);

@@ -39,6 +39,8 @@ struct PolyShape {
   uint8_t edge[kPolyMaxE][2];      // point_vindex
   float inertia[9];                // InertiaT as the host scaled it (main.cpp:622-626)
   float com[3];
+  float rmax;                      // upper bounds on the vertices' distance from the
+  float emax;                      // centre and on the edge lengths (edge-edge pruning)
 };
 
 // World-frame geometry of every particle, rebuilt each step: particle i's
