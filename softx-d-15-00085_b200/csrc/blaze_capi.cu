@@ -348,7 +348,7 @@ int upload_params(blaze_sim* s) {
 int alloc_poly_pairs(blaze_sim* s) {
   PolyPairs& pp = s->pairs;
   auto f = [](void* p) { if (p) cudaFree(p); };
-  f(pp.status); f(pp.con); f(pp.qv); f(pp.qe); f(pp.counts);
+  f(pp.status); f(pp.hint); f(pp.con); f(pp.qv); f(pp.qe); f(pp.counts);
   pp = PolyPairs{};
   const size_t slots = (size_t)s->nl.cap * (size_t)s->nl.stride;
   if (slots >= (size_t)0xffffffffu) {
@@ -357,6 +357,8 @@ int alloc_poly_pairs(blaze_sim* s) {
     return -1;
   }
   CK(dalloc(&pp.status, slots));
+  CK(dalloc(&pp.hint, slots));
+  CK(cudaMemset(pp.hint, 0xff, slots));
   CK(dalloc(&pp.con, 2 * slots));
   CK(dalloc(&pp.qv, slots));
   CK(dalloc(&pp.qe, slots));
@@ -369,6 +371,7 @@ int alloc_poly_pairs(blaze_sim* s) {
   int dev = 0, sms = 148;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  pp.grid_s = 16 * sms;
   pp.grid_v = 8 * sms;
   pp.grid_e = 8 * sms;
   return 0;
@@ -643,7 +646,7 @@ void free_sim(blaze_sim* s) {
   f(s->stage.flags); f(s->stage.quat4);
   f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
   f(s->geom.vert); f(s->geom.fnorm); f(s->geom.fcent);
-  f(s->pairs.status); f(s->pairs.con); f(s->pairs.qv); f(s->pairs.qe); f(s->pairs.counts);
+  f(s->pairs.status); f(s->pairs.hint); f(s->pairs.con); f(s->pairs.qv); f(s->pairs.qe); f(s->pairs.counts);
   f(s->nl.flat);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);

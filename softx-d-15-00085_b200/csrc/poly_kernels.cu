@@ -136,12 +136,14 @@ __device__ bool face_separates(const PolyRef& a, int f, const PolyRef& b) {
 }
 
 // is_SP_Poly_Poly (Utilities.cuh:105-156): does any face plane of `a`
-// separate `b`?
-__device__ bool separated_by_face(const PolyRef& a, const PolyRef& b) {
+// separate `b`?  Returns the face, or -1.  `first` (or -1) is tried before
+// the others: the answer is an OR over the faces, so the order is free.
+__device__ int separating_face(const PolyRef& a, const PolyRef& b, int first) {
   const int nf = a.s->nf;
+  if (first >= 0 && first < nf && face_separates(a, first, b)) return first;
   for (int f = 0; f < nf; ++f)
-    if (face_separates(a, f, b)) return true;
-  return false;
+    if (f != first && face_separates(a, f, b)) return f;
+  return -1;
 }
 
 // Collision_Detection_Vertex_InPoly_3Faces (CDP:287-382): is `v` behind
@@ -1060,8 +1062,9 @@ __device__ __forceinline__ void flag_status_warp(StepCtl* ctl, uint32_t bits) {
 // flat list): bounding spheres (Collision_Detection_BroadPhase.cuh:369-384;
 // a no-op in reference mode, where the list holds overlapping pairs only),
 // then the separating face planes of A against B and of B against A
-// (DEM_Kernels_Compute.cuh:842-860).  Every thread runs the same number of
-// rounds so the block can append its queue entries at once.
+// (DEM_Kernels_Compute.cuh:842-860), starting from the face that separated
+// the slot's pair last step.  Every thread runs the same number of rounds so
+// the block can append its queue entries at once.
 __global__ void __launch_bounds__(kThreads)
 k_poly_sep(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
            StateBuf in_sorted, NbrList nl, const int* rebuilt, PolyPairs pp) {
@@ -1085,7 +1088,17 @@ k_poly_sep(const PolyShape* __restrict__ shapes, PolyGeom g, StateBuf in_plain,
       if (len3(xyz(pa4) - xyz(pb4)) - (pa4.w + pb4.w) < 0.0f) {
         const PolyRef A = poly_ref(g, shapes, i, pa4, in.vel[i]);
         const PolyRef B = poly_ref(g, shapes, j, pb4, __ldg(in.vel + j));
-        if (!(separated_by_face(A, B) || separated_by_face(B, A))) {
+        // the face that separated this slot's pair last step, if any, first
+        const int hint = pp.hint[slot];
+        int hint_b = hint != 0xff && (hint & 0x80) ? hint & 0x3f : -1;
+        int f = separating_face(A, B, hint != 0xff && !(hint & 0x80) ? hint : -1);
+        int newhint = f >= 0 ? f : 0xff;
+        if (f < 0) {
+          f = separating_face(B, A, hint_b);
+          newhint = f >= 0 ? (0x80 | f) : 0xff;
+        }
+        if (newhint != hint) pp.hint[slot] = (uint8_t)newhint;
+        if (f < 0) {
           v = kSlotVertex;
           queue = true;
         }
@@ -1342,7 +1355,7 @@ int launch_poly_pairs(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const StateBuf& in_plain, const StateBuf& in_sorted, int n_max, NbrList nl,
                       StepCtl* ctl, const int* rebuilt, PolyPairs pp, cudaStream_t st) {
   cudaMemsetAsync(pp.counts, 0, 2 * sizeof(int), st);
-  k_poly_sep<<<pp.grid_v, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
+  k_poly_sep<<<pp.grid_s, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
   k_poly_vf<<<pp.grid_v, kThreads, 0, st>>>(shapes, g, in_plain, in_sorted, nl, ctl, rebuilt, pp);
   k_poly_ee<<<pp.grid_e, kThreads, 0, st>>>(dp, shapes, g, in_plain, in_sorted, nl, rebuilt, pp);
   return 3;

@@ -57,12 +57,14 @@ struct PolyGeom {
 // the verdict of the passes and, for a contact, its normal, depth and point.
 struct PolyPairs {
   uint8_t* status;    // cap x stride: 0 none, 1 vertex test pending, 2 contact, 3 edge test pending
+  uint8_t* hint;      // cap x stride: the face that last separated the slot's pair
+                      // (bit 7: a face of the neighbour), 0xff none
   float4* con;        // 2 x cap x stride: (normal, depth), (contact point, 0)
   uint32_t* qv;       // slots queued for the vertex-face test
   uint32_t* qe;       // slots queued for the edge-edge test
   int* counts;        // [0] vertex-face queue length, [1] edge-edge queue length,
                       // [2] filled neighbour slots (NbrList::flat_n)
-  int grid_v, grid_e; // blocks of the two queue passes (persistent grids)
+  int grid_s, grid_v, grid_e;  // blocks of the three passes (persistent grids)
 };
 
 void launch_poly_geom(const PolyShape* shapes, PolyGeom g, const StateBuf& in_plain,
