@@ -65,6 +65,12 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--batched-steps", type=int, default=2000,
                     help="timed steps of the batched leg (the workload's 2,000 settling steps)")
+    ap.add_argument("--no-silo-full", action="store_true",
+                    help="skip the full silo form (Hertz-Mindlin, 4,096-triangle hopper, 1M)")
+    ap.add_argument("--silo-full-steps", type=int, default=10000,
+                    help="timed steps of the full silo form (the workload's 10,000 steps)")
+    ap.add_argument("--silo-full-only", action="store_true",
+                    help="run only the full silo form and print its object")
     ap.add_argument("--no-poly", action="store_true",
                     help="skip the convex-polyhedra leg (100,000 polyhedra in a box)")
     ap.add_argument("--poly-steps", type=int, default=500)
@@ -392,6 +398,56 @@ class _StdoutToStderr:
         return False
 
 
+def device_status_names(st):
+    from blaze import device
+    return device.decode_status(st)
+
+
+def silo_full_leg(steps, warmup, skin=0.04, block=256):
+    """The silo discharge in the full form of the workload definition: 1,000,000
+    spheres, radii uniform in [0.2, 0.4] cm, density 2600 kg/m^3, cylinder
+    r = 25 cm over a 30 degree hopper of 4,096 triangles to a 6 cm outlet,
+    Hertz-Mindlin (E = 1e7 Pa, nu = 0.3), restitution 0.6, mu = 0.5, rolling
+    mu = 0.01, dt = 5e-6 s, FP32; one-system ensemble (tangential history,
+    Coulomb cap, rolling friction, triangle walls through per-cell lists),
+    CUDA graphs, Verlet skin.  Timed from the layered packing with the outlet
+    open.  The reference has no Hertz-Mindlin law, history spring, rolling
+    friction or triangle walls, so there is no reference arm for this line."""
+    import torch
+    from blaze import ensemble as E
+    from blaze import synth
+    S, W, p, r = synth.silo_full_ensemble(skin=skin)
+    ens = E.Ensemble(S, W, law=E.LAW_HERTZ_MINDLIN, dt=5e-6, skin=skin, use_graph=1, block=block)
+    ens.set_state(p, r)
+    ens.step(max(3, warmup))
+    status = ens.sync()
+    stream = torch.cuda.ExternalStream(ens.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = ens.num_rebuilds()
+    a.record(stream)
+    ens.step(steps)
+    b.record(stream)
+    fixed = ens.last_launches()
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = ens.num_rebuilds() - rb0
+    launches = fixed + rebuilds * ens.rebuild_kernels()
+    status |= ens.sync()
+    n = ens.n
+    ens.close()
+    return {"workload": "silo discharge, full form: 1,000,000 spheres r U[0.2, 0.4] cm, "
+                        "Hertz-Mindlin E=1e7 Pa nu=0.3 e=0.6 mu=0.5 mu_roll=0.01, "
+                        "4,096-triangle hopper, dt 5e-6 s",
+            "particles": n, "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "skin_cm": skin, "block": block, "rebuilds": rebuilds,
+            "gpu_launches": launches, "triangles": int(S[0].ntris),
+            "status": device_status_names(status),
+            "cpu_baseline": None,
+            "cpu_baseline_note": "the reference has no Hertz-Mindlin law, history spring, "
+                                 "rolling friction or triangle walls"}
+
+
 def cpu_reference_rate(P, st, seconds, max_steps=None, hatch=True):
     """The reference's own kernels compiled as host C++ (oracle/_ref), all
     host threads, reference mode, on this workload: particle-steps/s."""
@@ -460,6 +516,9 @@ def main():
     from blaze import device
 
     torch.cuda.set_device(local)
+    if args.silo_full_only:
+        print(json.dumps(silo_full_leg(args.silo_full_steps, args.warmup)))
+        return 0
     if args.poly_only:
         print(json.dumps(poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                                   want_cpu=not args.no_cpu_baseline)))
@@ -569,6 +628,9 @@ def main():
     e2e_value = n * world * args.e2e_steps / el
     state_bytes = n * (12 + 12 + 12 + 4 + 4)
 
+    silo_full = None
+    if not args.no_silo_full:
+        silo_full = silo_full_leg(args.silo_full_steps, args.warmup)
     poly = None
     if not args.no_poly:
         poly = poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
@@ -605,6 +667,7 @@ def main():
             "rebuilds_in_timed_region": rebuilds,
             "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
             "reference_mode_value": ref_mode_value,
+            "silo_full": silo_full,
             "polyhedra": poly,
             "batched": batched,
             "adjoint": adjoint,

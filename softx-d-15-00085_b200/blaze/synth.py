@@ -14,6 +14,9 @@ SI and in these units).  All randomness is numpy default_rng(seed).
   poly_box_project
                  convex polyhedra (dodecahedra, cubes, hexagonal prisms) in
                  a closed box, every particle in contact from the start
+  silo_full_ensemble
+                 the silo discharge in its full form (Hertz-Mindlin, rolling
+                 friction, a 4,096-triangle hopper) as a one-system ensemble
 """
 import math
 import os
@@ -591,6 +594,113 @@ def box_ensemble(counts, *, r_min=0.1, r_max=0.2, solid_fraction=0.55, height_fa
         pos.append(p.astype(np.float32))
         rad.append(r.astype(np.float32))
     return systems, walls, np.concatenate(pos), np.concatenate(rad)
+
+
+def cone_hopper_triangles(silo_r, r_out, y_top, y_out, n_seg=64, n_ring=32, centre=None):
+    """A cone (axis +y) from radius r_out at y_out to silo_r at y_top as
+    n_seg x n_ring quads, each split into two triangles (2 n_seg n_ring
+    triangles), vertices on the cone."""
+    c = silo_r if centre is None else centre
+    tris = []
+    for k in range(n_ring):
+        y0 = y_out + (y_top - y_out) * k / n_ring
+        y1 = y_out + (y_top - y_out) * (k + 1) / n_ring
+        r0 = r_out + (silo_r - r_out) * k / n_ring
+        r1 = r_out + (silo_r - r_out) * (k + 1) / n_ring
+        for m in range(n_seg):
+            a0 = 2 * math.pi * m / n_seg
+            a1 = 2 * math.pi * (m + 1) / n_seg
+            p00 = (c + r0 * math.cos(a0), y0, c + r0 * math.sin(a0))
+            p01 = (c + r0 * math.cos(a1), y0, c + r0 * math.sin(a1))
+            p10 = (c + r1 * math.cos(a0), y1, c + r1 * math.sin(a0))
+            p11 = (c + r1 * math.cos(a1), y1, c + r1 * math.sin(a1))
+            tris.append((p00, p01, p11))
+            tris.append((p00, p11, p10))
+    return tris
+
+
+def silo_full_ensemble(n=1_000_000, r_min=0.2, r_max=0.4, rho=2600.0, silo_r=25.0,
+                       silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, n_seg=64, n_ring=32,
+                       youngs_pa=1e7, poisson=0.3, restitution=0.6, mu=0.5, mu_roll=0.01,
+                       skin=0.04, seed=1, overlap=1e-5, gravity=(0.0, -981.0, 0.0)):
+    """Silo discharge, full variant, as a one-system ensemble: 1,000,000
+    spheres with radii uniform in [0.2, 0.4] cm (seed 1), density 2600
+    kg/m^3, in a cylinder r = 25 cm, h = 100 cm over a 30 degree conical
+    hopper of 2 x 64 x 32 = 4,096 triangles to a 6 cm outlet (open), a floor
+    30 cm below the outlet to catch the discharge; Hertz-Mindlin with
+    E = 1e7 Pa, nu = 0.3, restitution 0.6, mu = 0.5, rolling mu = 0.01; y
+    vertical.  The spheres start in 24 size bands of horizontal layers on a
+    lattice of pitch 2 r_band (1 - overlap) (largest band lowest, r_band the
+    band's largest radius), clipped to the hopper's inscribed radius and the
+    barrel with a small clearance, at rest: a contact network under load
+    from the first step.  The layers are looser than a poured bed, so the
+    column reaches above the 100 cm barrel (the silo has no lid; the grid
+    covers it).  Returns (systems, walls, pos, radius)."""
+    from . import ensemble as E
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(r_min, r_max, size=n)
+    r_out = 0.5 * outlet_d
+    tan_a = math.tan(math.radians(half_angle_deg))
+    cos_a = math.cos(math.radians(half_angle_deg))
+    h_hop = (silo_r - r_out) / tan_a
+    y_floor = 0.0
+    y_out = y_floor + 30.0
+    y_top = y_out + h_hop
+    c = silo_r
+    # layers by radius band, largest band lowest; the pitch of a band is set
+    # by its largest radius
+    order = np.argsort(-r, kind="stable")
+    r = r[order]
+    bands = np.array_split(np.arange(n), 24)
+    pos = np.zeros((n, 3), np.float64)
+    k = 0
+    y = y_out + 0.05
+    inscribed = math.cos(math.pi / n_seg)
+    for idx in bands:
+        rb = float(r[idx[0]])
+        pitch = 2.0 * rb * (1.0 - overlap)
+        need = len(idx)
+        y += rb
+        while need > 0:
+            ra = (r_out + (y - y_out) * tan_a) * inscribed if y < y_top else silo_r
+            ra -= rb / cos_a + 0.002
+            if ra > 0:
+                m = int(ra / pitch)
+                g = np.arange(-m, m + 1) * pitch
+                xx, zz = np.meshgrid(g, g, indexing="ij")
+                keep = xx ** 2 + zz ** 2 <= ra * ra
+                xs, zs = xx[keep][:need], zz[keep][:need]
+                cnt = len(xs)
+                pos[k:k + cnt, 0] = c + xs
+                pos[k:k + cnt, 1] = y
+                pos[k:k + cnt, 2] = c + zs
+                k += cnt
+                need -= cnt
+            y += pitch
+        y += rb * 0.002
+    # the silo has no lid: a packing taller than the barrel (the simple-cubic
+    # layers are looser than a poured bed) continues above it
+    y_max = max(float(pos[:, 1].max()) + 2.0 * r_max, y_top + silo_h)
+    walls = [E.cylinder((c, 0.0, c), (0.0, 1.0, 0.0), silo_r), E.plane((0.0, 1.0, 0.0), y_floor)]
+    tri = cone_hopper_triangles(silo_r, r_out, y_top, y_out, n_seg, n_ring)
+    walls += [E.triangle(*t) for t in tri]
+    cell = 2.0 * r_max + skin
+    s = E.System()
+    s.n = int(n)
+    origin = (-cell, y_floor - cell, -cell)
+    ext = (2.0 * silo_r + 2.0 * cell, y_max - y_floor + 2.0 * cell, 2.0 * silo_r + 2.0 * cell)
+    for q in range(3):
+        s.origin[q] = origin[q]
+        s.ncells[q] = int(math.ceil(ext[q] / cell))
+        s.gravity[q] = gravity[q]
+    s.cell = cell
+    s.density = rho * 1e-6
+    s.kn, s.kt_ratio = 0.0, 2.0 / 7.0
+    s.youngs = youngs_pa * 0.01  # kg/(cm s^2)
+    s.poisson = poisson
+    s.restitution, s.mu, s.mu_wall, s.mu_roll = restitution, mu, mu, mu_roll
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 2, 2, len(tri)
+    return [s], walls, pos.astype(np.float32), r.astype(np.float32)
 
 
 def batched_counts(nsys=512, n_min=2000, n_max=50000, seed=3):
