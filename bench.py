@@ -300,6 +300,7 @@ def adjoint_leg(steps, segment=50):
     gx = pos_t.grad.numpy()[pid].astype(np.float32)
     gv = vel_t.grad.numpy()[pid].astype(np.float32)
     bwd_ms = timed(st2, lambda: run.adj.backward(gx, gv, None))[0]
+    restore_ms, record_ms, reverse_ms = run.adj.profile()
     run.close()
     return {"workload": "64 box-settling systems x 20,000 spheres, linear law + tangential "
                         "history, dt 1e-5 s; loss: bed height + 32-bin side-wall force profile",
@@ -309,6 +310,9 @@ def adjoint_leg(steps, segment=50):
             "backward_ms_per_step": bwd_ms / steps,
             "adjoint_vs_forward": (ck_ms + bwd_ms) / steps / fwd_ms,
             "backward_vs_forward": bwd_ms / steps / fwd_ms,
+            "backward_phases_ms_per_step": {"restore": restore_ms / steps,
+                                            "record": record_ms / steps,
+                                            "reverse": reverse_ms / steps},
             "autograd_call_s": autograd_s,
             "loss": float(loss.item()),
             "mean_grad": {"kn": float(g[:, 0].mean()), "restitution": float(g[:, 1].mean()),

@@ -125,6 +125,10 @@ int blaze_ens_adj_forward(blaze_ens_adj* a);
 int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
                            const float* gavel, float* gpos0, float* gvel0, float* gavel0,
                            double* gconst);
+/* Device time of the last backward call by phase, ms: restoring the
+ * checkpoints, recomputing the segments into the tape, the reverse sweep. */
+int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,
+                          float* ms_reverse);
 int blaze_ens_adj_destroy(blaze_ens_adj* a);
 
 #ifdef __cplusplus

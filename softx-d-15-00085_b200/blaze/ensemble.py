@@ -67,6 +67,7 @@ def load():
         lib.blaze_ens_adj_backward.argtypes = [C.c_void_p, _f, _f, _f, _f, _f, _f,
                                                P(C.c_double)]
         lib.blaze_ens_adj_destroy.argtypes = [C.c_void_p]
+        lib.blaze_ens_adj_profile.argtypes = [C.c_void_p, _f, _f, _f]
         _bound = True
     return lib
 
@@ -235,6 +236,14 @@ class Adjoint:
             *[_ptr(a, C.c_float) for a in out], gc.ctypes.data_as(C.POINTER(C.c_double))),
             "blaze_ens_adj_backward")
         return out[0], out[1], out[2], gc
+
+    def profile(self):
+        """Device ms of the last backward by phase: (restoring checkpoints,
+        recomputing segments into the tape, reversing them)."""
+        v = [C.c_float() for _ in range(3)]
+        _check(self.lib.blaze_ens_adj_profile(self.h, *[C.byref(x) for x in v]),
+               "blaze_ens_adj_profile")
+        return tuple(x.value for x in v)
 
 
 def beta2_of_e(e):

@@ -771,6 +771,11 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   if (opt) s->opt = *opt;
   else blaze_default_options(&s->opt);
   if (s->opt.max_nbr <= 0) s->opt.max_nbr = 32;
+  if (s->opt.max_nbr > 32) {  // the reference's 32 slots; the step masks them in 32 bits
+    std::fprintf(stderr, "blaze: max_nbr %d exceeds 32 neighbour slots\n", s->opt.max_nbr);
+    delete s;
+    return -1;
+  }
   const int n = s->n_max;
   auto fail = [&](int rc) { free_sim(s); return rc; };
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
@@ -872,6 +877,10 @@ int blaze_destroy(blaze_sim* s) {
 int blaze_set_options(blaze_sim* s, const blaze_options* opt) {
   if (!s || !opt) return -1;
   const blaze_options old = s->opt;
+  if (opt->max_nbr > 32) {  // the reference's 32 slots; the step masks them in 32 bits
+    std::fprintf(stderr, "blaze: max_nbr %d exceeds 32 neighbour slots\n", opt->max_nbr);
+    return -1;
+  }
   s->opt = *opt;
   if (s->opt.max_nbr <= 0) s->opt.max_nbr = 32;
   CK(cudaStreamSynchronize(s->stream));

@@ -15,11 +15,18 @@ struct Forces { float3 trans, torque; };
 // rotation is off and every angular velocity is exactly zero: then
 // v + cross(0, R) equals v up to the sign of an exact zero, so the forces
 // are the same numbers.
+// The tangential force's factor (((0.5 (m_a + m_b)) / dt) 0.05) mu_k, which
+// depends on the two particle types only; law_pp_pre takes it precomputed.
+__device__ __forceinline__ float tangential_prefactor(const SimParams& P, const PP_Parms& pp,
+                                                      float ma, float mb) {
+  return (((0.50f * (ma + mb)) / P.dt) * 0.050f) * pp.Fric_kinetic;
+}
+
 template <bool kSpin>
-__device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
-                                         float3 ra, float3 rb, float3 wa, float3 wb,
-                                         const PP_Parms& pp, float3 va, float3 vb, float ma,
-                                         float mb) {
+__device__ __forceinline__ Forces law_pp_pre(const SimParams& P, float3 rvel, float3 n, float pen,
+                                             float3 ra, float3 rb, float3 wa, float3 wb,
+                                             const PP_Parms& pp, float3 va, float3 vb,
+                                             float tan_pre) {
   Forces F;
   const float3 vn = dot3(rvel, n) * n;
   const float fn = pp.Kn * pen;
@@ -37,12 +44,21 @@ __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3
     float velf = dot3(rvel, rvel);
     if (velf > 0) velf = sqrtf(velf);
     else velf = 1.0f;
-    const float tan_f = ((((0.50f * (ma + mb)) / P.dt) * 0.050f) * pp.Fric_kinetic) * (mag / velf);
+    const float tan_f = tan_pre * (mag / velf);
     ft = (-1.0f * tan_f) * (vt / mag);
   }
   F.trans = F.trans + ft;
   F.torque = (kSpin && P.rotation) ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
   return F;
+}
+
+template <bool kSpin>
+__device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
+                                         float3 ra, float3 rb, float3 wa, float3 wb,
+                                         const PP_Parms& pp, float3 va, float3 vb, float ma,
+                                         float mb) {
+  return law_pp_pre<kSpin>(P, rvel, n, pen, ra, rb, wa, wb, pp, va, vb,
+                           tangential_prefactor(P, pp, ma, mb));
 }
 
 // Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109

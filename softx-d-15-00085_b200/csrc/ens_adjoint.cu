@@ -412,6 +412,53 @@ k_adj_unsort(EnsTape tp, int t, int n, int cap, AdjBufs a) {
 
 __global__ void k_adj_slot_next(int* slot) { *slot += 1; }
 
+// Host-layout cotangents (3 floats per particle) to and from the float4
+// buffers of the sweep.
+__global__ void __launch_bounds__(kThreads)
+k_adj_f3_to_f4(const float* __restrict__ src, float4* __restrict__ dst, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dst[i] = src ? make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f)
+               : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_adj_f4_to_f3(const float4* __restrict__ src, float* __restrict__ dst, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 v = src[i];
+  dst[3 * i] = v.x;
+  dst[3 * i + 1] = v.y;
+  dst[3 * i + 2] = v.z;
+}
+
+// Law-constant cotangents summed per system in FP64: one block per system,
+// each thread a strided partial sum, then a fixed tree over the block (the
+// order depends only on the system's size, so repeated calls agree).
+constexpr int kSumThreads = 256;
+
+__global__ void __launch_bounds__(kSumThreads)
+k_adj_sum_constants(const float* __restrict__ th, const int* __restrict__ off,
+                    double* __restrict__ out) {
+  __shared__ double part[5][kSumThreads];
+  const int s = blockIdx.x;
+  const int lo = off[s], hi = off[s + 1];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = lo + threadIdx.x; i < hi; i += kSumThreads)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[c] += (double)th[5 * (size_t)i + c];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) part[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) part[c][threadIdx.x] += part[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) out[5 * s + threadIdx.x] = part[threadIdx.x][0];
+}
+
 inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
@@ -445,6 +492,19 @@ void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gat
 void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,
                        cudaStream_t st) {
   k_adj_unsort<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
+}
+
+void adj_launch_f3_to_f4(const float* src, float4* dst, int n, cudaStream_t st) {
+  k_adj_f3_to_f4<<<nblk(n), kThreads, 0, st>>>(src, dst, n);
+}
+
+void adj_launch_f4_to_f3(const float4* src, float* dst, int n, cudaStream_t st) {
+  k_adj_f4_to_f3<<<nblk(n), kThreads, 0, st>>>(src, dst, n);
+}
+
+void adj_launch_sum_constants(const float* th, const int* off, int nsys, double* out,
+                              cudaStream_t st) {
+  if (nsys > 0) k_adj_sum_constants<<<nsys, kSumThreads, 0, st>>>(th, off, out);
 }
 
 }  // namespace blaze

@@ -48,7 +48,7 @@ struct AdjBufs {        // cotangents, all in the memory order of the step they 
   float4* iw;
   float4* iH;
   float4* iW;
-  float4* Fb;           // (unused: the force and torque cotangents stay in registers)
+  float4* Fb;           // host cotangent stage (the force cotangents stay in registers)
   float4* Tb;
   float4* px;           // per list slot (cap x n): the share of a contact's
   float4* pv;           // cotangent that goes to the neighbour's state
@@ -82,5 +82,14 @@ void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int tl, int n, 
 // sorted order) -> after the previous step (gx..gW, order before the sort).
 void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,
                        cudaStream_t st);
+
+// Host-layout (3 floats per particle) cotangents to and from float4;
+// src == nullptr gives zeros.
+void adj_launch_f3_to_f4(const float* src, float4* dst, int n, cudaStream_t st);
+void adj_launch_f4_to_f3(const float4* src, float* dst, int n, cudaStream_t st);
+// out[5 s + c] = sum over the particles [off[s], off[s + 1]) of th[5 i + c],
+// in FP64, in particle order.
+void adj_launch_sum_constants(const float* th, const int* off, int nsys, double* out,
+                              cudaStream_t st);
 
 }  // namespace blaze

@@ -671,6 +671,12 @@ struct blaze_ens_adj {
   bool forward_done = false;
   int* d_slot = nullptr;                          // tape step the next snapshot writes
   cudaGraphExec_t rgraph[2] = {nullptr, nullptr};  // recording graphs, from S[0] / S[1]
+  // per-phase device time of the last backward call (restoring checkpoints,
+  // recording segments into the tape, reversing them), from events
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float ms_phase[3] = {0.0f, 0.0f, 0.0f};
+  int* d_sys_off = nullptr;     // nsys + 1 particle offsets of the systems
+  double* d_gconst = nullptr;   // 5 per system: summed law-constant cotangents
 };
 
 namespace {
@@ -682,6 +688,8 @@ int sort_result(const blaze_ens* e) {
 
 void free_adj(blaze_ens_adj* a) {
   if (!a) return;
+  for (cudaEvent_t ev : a->ev)
+    if (ev) cudaEventDestroy(ev);
   auto f = [](void* p) { if (p) cudaFree(p); };
   EnsTape& t = a->tape;
   f(t.rb); f(t.perm); f(t.src); f(t.pos); f(t.vel); f(t.angv); f(t.idx); f(t.cnt); f(t.mask);
@@ -696,6 +704,8 @@ void free_adj(blaze_ens_adj* a) {
     f(q);
   f(b.th);
   f(a->d_slot);
+  f(a->d_sys_off);
+  f(a->d_gconst);
   for (int c = 0; c < 2; ++c)
     if (a->rgraph[c]) cudaGraphExecDestroy(a->rgraph[c]);
   delete a;
@@ -893,7 +903,16 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
   CKA(dalloc(&b.gW, kWallSlots * n));
   CKA(dalloc(&b.iW, kWallSlots * n));
   CKA(dalloc(&b.th, 5 * n));
+  CKA(dalloc(&b.Fb, n));   // host cotangent stage (12 B of every 16 used)
   CKA(dalloc(&a->d_slot, 1));
+  CKA(dalloc(&a->d_sys_off, e->nsys + 1));
+  CKA(dalloc(&a->d_gconst, 5 * (size_t)e->nsys));
+  {
+    std::vector<int> off(e->nsys + 1, 0);
+    for (int s = 0; s < e->nsys; ++s) off[s + 1] = off[s] + e->sys[s].n;
+    CKA(cudaMemcpy(a->d_sys_off, off.data(), sizeof(int) * (e->nsys + 1),
+                   cudaMemcpyHostToDevice));
+  }
   a->rb.assign(a->K, 0);
 #undef CKA
   *out = a;
@@ -927,27 +946,33 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
   cudaStream_t st = e->stream;
   AdjBufs& A = a->A;
   {
-    std::vector<float4> h(n);
+    // host cotangents through a device stage (A.Fb, 16 B per particle,
+    // holds the 12 B of one array)
+    float* stage = reinterpret_cast<float*>(A.Fb);
     const float* src[3] = {gpos, gvel, gavel};
     float4* dst[3] = {A.gx, A.gv, A.gw};
     for (int q = 0; q < 3; ++q) {
-      for (size_t i = 0; i < n; ++i)
-        h[i] = src[q] ? make_float4(src[q][3 * i], src[q][3 * i + 1], src[q][3 * i + 2], 0.0f)
-                      : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      CK(cudaMemcpyAsync(dst[q], h.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, st));
-      CK(cudaStreamSynchronize(st));
+      if (src[q])
+        CK(cudaMemcpyAsync(stage, src[q], sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+      adj_launch_f3_to_f4(src[q] ? stage : nullptr, dst[q], (int)n, st);
     }
   }
   CK(cudaMemsetAsync(A.gH, 0, sizeof(float4) * cap * n, st));
   CK(cudaMemsetAsync(A.gW, 0, sizeof(float4) * kWallSlots * n, st));
   CK(cudaMemsetAsync(A.th, 0, sizeof(float) * 5 * n, st));
   const EnsGeom g = geom(e);
+  for (cudaEvent_t& ev : a->ev)
+    if (!ev) CK(cudaEventCreate(&ev));
+  for (float& m : a->ms_phase) m = 0.0f;
   for (int seg = a->nseg - 1; seg >= 0; --seg) {
     const int len = std::min(a->K, a->nsteps - seg * a->K);
+    CK(cudaEventRecord(a->ev[0], st));
     int rc = restore_checkpoint(a, a->ck[seg]);
     if (rc) return rc;
+    CK(cudaEventRecord(a->ev[1], st));
     rc = record_segment(a, len);
     if (rc) return rc;
+    CK(cudaEventRecord(a->ev[2], st));
     std::vector<int> list_at(len, 0);   // tape step holding the list step t used
     for (int t = 1; t < len; ++t) list_at[t] = a->rb[t] ? t : list_at[t - 1];
     for (int t = len - 1; t >= 0; --t) {
@@ -963,35 +988,42 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
         std::swap(A.gW, A.iW);
       }
     }
+    CK(cudaEventRecord(a->ev[3], st));
+    CK(cudaEventSynchronize(a->ev[3]));
+    float m = 0.0f;
+    for (int q = 0; q < 3; ++q) {
+      CK(cudaEventElapsedTime(&m, a->ev[q], a->ev[q + 1]));
+      a->ms_phase[q] += m;
+    }
   }
   CK(cudaGetLastError());
-  std::vector<float4> h(n);
   float* outs[3] = {gpos0, gvel0, gavel0};
   float4* srcs[3] = {A.gx, A.gv, A.gw};
+  float* stage = reinterpret_cast<float*>(A.Fb);
   for (int q = 0; q < 3; ++q) {
     if (!outs[q]) continue;
-    CK(cudaMemcpyAsync(h.data(), srcs[q], sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < n; ++i) {
-      outs[q][3 * i] = h[i].x; outs[q][3 * i + 1] = h[i].y; outs[q][3 * i + 2] = h[i].z;
-    }
+    adj_launch_f4_to_f3(srcs[q], stage, (int)n, st);
+    CK(cudaMemcpyAsync(outs[q], stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
   }
   if (gconst) {
-    std::vector<float> th(5 * n);
-    CK(cudaMemcpyAsync(th.data(), A.th, sizeof(float) * 5 * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
     // positions of system s are [off_s, off_s + n_s) in every order the run
-    // takes: keys sort by system first
-    size_t off = 0;
-    for (int s = 0; s < e->nsys; ++s) {
-      double acc[5] = {0, 0, 0, 0, 0};
-      for (int i = 0; i < e->sys[s].n; ++i)
-        for (int c = 0; c < 5; ++c) acc[c] += th[5 * (off + i) + c];
-      for (int c = 0; c < 5; ++c) gconst[5 * s + c] = acc[c];
-      off += e->sys[s].n;
-    }
+    // takes (keys sort by system first); the per-system sums run on the
+    // device, in particle order, in FP64
+    adj_launch_sum_constants(A.th, a->d_sys_off, e->nsys, a->d_gconst, st);
+    CK(cudaMemcpyAsync(gconst, a->d_gconst, sizeof(double) * 5 * e->nsys, cudaMemcpyDeviceToHost,
+                       st));
   }
+  CK(cudaStreamSynchronize(st));
   return sync_status(e);
+}
+
+int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,
+                          float* ms_reverse) {
+  if (!a) return -1;
+  if (ms_restore) *ms_restore = a->ms_phase[0];
+  if (ms_record) *ms_record = a->ms_phase[1];
+  if (ms_reverse) *ms_reverse = a->ms_phase[2];
+  return 0;
 }
 
 int blaze_ens_adj_destroy(blaze_ens_adj* a) {
