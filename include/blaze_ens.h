@@ -108,12 +108,30 @@ int blaze_ens_rebuild_kernels(blaze_ens* e);
  * and the law constants, by the discrete adjoint of the step (linear law
  * with tangential history and Coulomb cap, plane walls, no rolling
  * friction).  The forward keeps a checkpoint of the full state every
- * `segment` steps; the backward recomputes each segment into a tape and
- * walks it back, segment by segment.  Derivatives are those of the branch
+ * `segment` steps and records the trailing segments into a tape; the
+ * backward walks the tape back segment by segment, recomputing from its
+ * checkpoint each segment the tape no longer holds.  Derivatives are those of the branch
  * each contact took (contact or not, stick or slip). */
 typedef struct blaze_ens_adj blaze_ens_adj;
 
 int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment);
+/* The same with a tape budget.  The tape is one arena holding, per recorded
+ * step, the input state and history mask (68 B per particle) and the step's
+ * active histories, and per re-sort the new list.  The forward records the
+ * trailing segments that fit as it runs (a ring of segments), and the
+ * backward recomputes only the others.
+ *   tape_bytes == 0: one segment, with room for the most it can take (every
+ *                    list slot an active history, a re-sort every step);
+ *   tape_bytes  > 0: an arena of that many bytes;
+ *   tape_bytes  < 0: 90 % of the device memory the reverse mode's other
+ *                    buffers leave free, less 4 GiB.
+ * Returns -2 when the arena cannot hold one segment's states; a backward
+ * whose recomputed segment does not fit the arena also returns -2. */
+int blaze_ens_adj_create_ex(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment,
+                            long long tape_bytes);
+/* The same with the arena size given in bytes. */
+int blaze_ens_adj_create_tape(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment,
+                              unsigned long long arena_bytes);
 /* nsteps steps from the ensemble's current state, with checkpoints; the
  * ensemble then holds the final state (read it with blaze_ens_get_state). */
 int blaze_ens_adj_forward(blaze_ens_adj* a);
@@ -129,6 +147,11 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
  * checkpoints, recomputing the segments into the tape, the reverse sweep. */
 int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,
                           float* ms_reverse);
+/* Arena size, how many segments the last forward left on the tape (the
+ * backward recomputes the others from their checkpoints), and the most pool
+ * bytes (histories and lists) one recorded segment has taken so far. */
+int blaze_ens_adj_tape_info(blaze_ens_adj* a, unsigned long long* arena_bytes, int* on_tape,
+                            unsigned long long* pool_bytes_max);
 int blaze_ens_adj_destroy(blaze_ens_adj* a);
 
 #ifdef __cplusplus

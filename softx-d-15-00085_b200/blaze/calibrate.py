@@ -84,14 +84,14 @@ class Runner:
     calibration run of `nsteps` steps with checkpoints every `segment`."""
 
     def __init__(self, systems, walls, pos, radius, nsteps, segment=100, dt=1e-5, skin=0.02,
-                 max_nbr=32):
+                 max_nbr=32, tape_bytes=0):
         self.systems = systems
         self.walls = walls
         self.pos0 = np.ascontiguousarray(pos, np.float32)
         self.radius = np.ascontiguousarray(radius, np.float32)
         self.ens = E.Ensemble(systems, walls, law=E.LAW_LINEAR, dt=dt, skin=skin,
                               max_nbr=max_nbr, use_graph=0)
-        self.adj = E.Adjoint(self.ens, nsteps, segment)
+        self.adj = E.Adjoint(self.ens, nsteps, segment, tape_bytes)
         self.cur = systems
 
     def close(self):

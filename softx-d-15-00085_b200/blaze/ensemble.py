@@ -68,6 +68,12 @@ def load():
                                                P(C.c_double)]
         lib.blaze_ens_adj_destroy.argtypes = [C.c_void_p]
         lib.blaze_ens_adj_profile.argtypes = [C.c_void_p, _f, _f, _f]
+        lib.blaze_ens_adj_create_ex.argtypes = [P(C.c_void_p), C.c_void_p, C.c_int, C.c_int,
+                                                C.c_longlong]
+        lib.blaze_ens_adj_tape_info.argtypes = [C.c_void_p, P(C.c_ulonglong), P(C.c_int),
+                                                P(C.c_ulonglong)]
+        lib.blaze_ens_adj_create_tape.argtypes = [P(C.c_void_p), C.c_void_p, C.c_int, C.c_int,
+                                                  C.c_ulonglong]
         _bound = True
     return lib
 
@@ -201,15 +207,37 @@ class Adjoint:
     checkpoint every `segment` steps; backward() takes the cotangents of the
     final state (final memory order) and returns those of the initial state
     (its memory order) and of the law constants (nsys x 5: kn, kt, 2 beta,
-    mu, mu_wall)."""
+    mu, mu_wall).
 
-    def __init__(self, ens, nsteps, segment=100):
+    tape_bytes: 0 keeps one segment on the tape (the forward records the
+    last one; the backward recomputes the others from their checkpoints);
+    a positive value is a budget in bytes; -1 takes 90 % of the free device
+    memory less 4 GiB.  The trailing segments that fit are recorded by the
+    forward and not recomputed."""
+
+    def __init__(self, ens, nsteps, segment=100, tape_bytes=0, arena_bytes=None):
+        """arena_bytes: the tape's arena size exactly, instead of tape_bytes."""
         self.ens = ens
         self.lib = ens.lib
         h = C.c_void_p()
-        _check(self.lib.blaze_ens_adj_create(C.byref(h), ens.h, int(nsteps), int(segment)),
-               "blaze_ens_adj_create")
+        if arena_bytes is not None:
+            _check(self.lib.blaze_ens_adj_create_tape(C.byref(h), ens.h, int(nsteps),
+                                                      int(segment), int(arena_bytes)),
+                   "blaze_ens_adj_create_tape")
+        else:
+            _check(self.lib.blaze_ens_adj_create_ex(C.byref(h), ens.h, int(nsteps),
+                                                    int(segment), int(tape_bytes)),
+                   "blaze_ens_adj_create_ex")
         self.h = h
+
+    def tape_info(self):
+        """(arena bytes, segments the last forward left on the tape, most pool
+        bytes one recorded segment took)."""
+        ab, pm = C.c_ulonglong(), C.c_ulonglong()
+        m = C.c_int()
+        _check(self.lib.blaze_ens_adj_tape_info(self.h, C.byref(ab), C.byref(m), C.byref(pm)),
+               "blaze_ens_adj_tape_info")
+        return ab.value, m.value, pm.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -188,8 +188,8 @@ __device__ float3 plane_vjp(const EnsSysDev& S, const EnsWallDev& W, const Body&
   return xib;
 }
 
-__device__ __forceinline__ Body body(const EnsTape& tp, const EnsSysDev& S, size_t at) {
-  const float4 p = tp.pos[at], v = tp.vel[at], w = tp.angv[at];
+__device__ __forceinline__ Body body(const TapeView& tv, const EnsSysDev& S, uint32_t i) {
+  const float4 p = tv.pos[i], v = tv.vel[i], w = tv.angv[i];
   Body B;
   B.x = xyz4(p);
   B.v = xyz4(v);
@@ -199,89 +199,94 @@ __device__ __forceinline__ Body body(const EnsTape& tp, const EnsSysDev& S, size
   return B;
 }
 
-// -------------------------------------------------------------- snapshot
+// ------------------------------------------------------------- recording
+// A segment of `len` steps from step slot0: dense blocks from arena word
+// `origin`, pool space after them up to `lim`.
+__global__ void k_adj_seg_start(EnsTape tp, int slot0, int len, unsigned long long origin,
+                                unsigned long long stride, unsigned long long lim) {
+  for (int q = threadIdx.x; q < len; q += blockDim.x)
+    tp.steps[slot0 + q].block = origin + (unsigned long long)q * stride;
+  if (threadIdx.x == 0) {
+    TapeCtl* c = tp.ctl;
+    c->cur = origin + (unsigned long long)len * stride;
+    c->lim = lim;
+    c->lsnap = c->cur;
+    c->slot = slot0 - 1;
+    c->lslot = slot0;
+    c->overflow = 0;
+  }
+}
+
+// The current list as the list of the step about to begin (ctl->slot + 1):
+// count, entries (neighbour, twin | src << 8) and, at a re-sort, the
+// permutation.  twin: the neighbour's slot that holds this particle (0xff
+// when the neighbour's list overflowed).
 __global__ void __launch_bounds__(kThreads)
-k_adj_snap(EnsTape tp, int t_arg, const int* slot, EnsBufs b, StateBuf plain, StateBuf sorted,
-           int n, const StepCtl* ctl, const int* rebuilt, const int32_t* perm) {
+k_adj_list(EnsBufs b, EnsTape tp, int n, const StepCtl* ctl, const int* gate, int resorted,
+           const int32_t* __restrict__ perm) {
+  if (gate && *gate == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  TapeCtl* tc = tp.ctl;
+  const int t = tc->slot + 1;
+  const unsigned long long base = tc->lsnap;
+  const TapeView tv = tape_view(tp, tp.steps[t].block, n);
+  const EnsList L = b.L[ctl->epoch & 1];
+  const size_t stride = (size_t)b.stride;
+  const uint32_t cnt = i < n ? L.cnt[i] : 0u;
+  bool ok;
+  const uint32_t off = tape_reserve(2u * cnt, &tc->cur, tc->lim, base, &tc->overflow, ok);
+  if (i == 0) {
+    tp.steps[t].lbase = base;
+    tc->lslot = t;
+  }
   if (i >= n) return;
-  const int t = slot ? *slot : t_arg;
-  const int flag = *rebuilt != 0;
-  const int e = ctl->epoch & 1;
-  const StateBuf in = flag ? sorted : plain;
-  const size_t base = (size_t)t * n + i;
-  const size_t cbase = (size_t)t * b.cap * n;
-  const float4 v = in.vel[i];
-  tp.pos[base] = in.pos[i];
-  tp.vel[base] = v;
-  tp.angv[base] = in.angv[i];
-  const EnsList L = b.L[e];
-  const uint32_t c = L.cnt[i];
-  const uint32_t mask = L.mask[i];
-  tp.mask[base] = mask;
-  // the list (indices, twins, count) only where it changed: a re-sort step
-  // or the first step of the tape; histories only where they are active
-  const bool list_step = flag || t == 0;
-  if (list_step) tp.cnt[base] = c;
-  for (uint32_t k = 0; k < c; ++k) {
-    const size_t s = (size_t)k * b.stride + i;
-    const size_t d = cbase + (size_t)k * n + i;
-    if (list_step) {
-      tp.idx[d] = L.idx[s];
-      tp.twin[d] = L.twin[s];
-      if (flag) tp.src[d] = L.src[s];
-    }
-    if ((mask >> k) & 1u) {
-      tp.hx[d] = L.hx[s];
-      tp.hy[d] = L.hy[s];
-      tp.hz[d] = L.hz[s];
-    }
+  tv.cnt[i] = cnt;
+  tv.loff[i] = off;
+  if (resorted) tv.perm[i] = perm[i];
+  if (!ok) return;
+  uint2* ent = reinterpret_cast<uint2*>(tp.arena + base + off);
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t sk = (size_t)k * stride + i;
+    const uint32_t j = L.idx[sk];
+    const uint32_t cj = L.cnt[j];
+    uint32_t tw = 0xffu;
+    for (uint32_t q = 0; q < cj; ++q)
+      if (L.idx[(size_t)q * stride + j] == (uint32_t)i) { tw = q; break; }
+    const uint32_t src = resorted ? (uint32_t)L.src[sk] : 0xffu;
+    ent[k] = make_uint2(j, tw | (src << 8));
   }
-  if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
-#pragma unroll
-    for (int q = 0; q < kWallSlots; ++q)
-      tp.wh[((size_t)t * kWallSlots + q) * n + i] = b.wh[e][(size_t)q * b.stride + i];
-  }
-  if (flag) tp.perm[base] = perm[i];
-  if (i == 0) tp.rb[t] = flag;
+}
+
+__global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
+  TapeCtl* c = tp.ctl;
+  const int t = c->slot + 1;
+  c->slot = t;
+  TapeStep& s = tp.steps[t];
+  s.rb = *rebuilt != 0;
+  s.lat = c->lslot;
+  s.hbase = c->cur;
+  c->lsnap = c->cur;
 }
 
 // --------------------------------------------------------------- reverse
-// Twin slots of the current list (reverse mode only): slot k of particle i
-// holds neighbour j; twin[k][i] is the slot of j's list that holds i.
-__global__ void __launch_bounds__(kThreads)
-k_adj_twin(EnsBufs b, int n, const StepCtl* ctl, const int* gate) {
-  if (gate && *gate == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const EnsList L = b.L[ctl->epoch & 1];
-  const size_t stride = (size_t)b.stride;
-  const uint32_t cnt = L.cnt[i];
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t j = L.idx[(size_t)k * stride + i];
-    const uint32_t cj = L.cnt[j];
-    uint8_t tw = 0xffu;
-    for (uint32_t q = 0; q < cj; ++q)
-      if (L.idx[(size_t)q * stride + j] == (uint32_t)i) { tw = (uint8_t)q; break; }
-    L.twin[(size_t)k * stride + i] = tw;
-  }
-}
-
 // The step backwards, per particle: symplectic Euler (v' = v + (f/m + g) dt,
 // x' = x + v' dt, w' = w + t/I dt) gives the cotangents of the particle's
 // force and torque; then the reverse of each of its own contacts, once: its
 // state, history and law-constant cotangents are kept, the share that goes
 // to the neighbour is left in the slot (px, pv, pw) for k_adj_gather.
 __global__ void __launch_bounds__(kThreads, 4)
-k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
+k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const size_t at = (size_t)t * n + i;
-  const size_t cbase = (size_t)t * cap * n;      // histories of step t
-  const size_t lbase = (size_t)tl * cap * n;     // the list step t used
-  const uint32_t bits = __float_as_uint(tp.vel[at].w);
+  const TapeStep ts = tp.steps[t];
+  const TapeStep tl = tp.steps[ts.lat];
+  const TapeView tv = tape_view(tp, ts.block, n);
+  const TapeView lv = tape_view(tp, tl.block, n);
+  const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + tl.lbase + lv.loff[i]);
+  const float* hp = reinterpret_cast<const float*>(tp.arena + ts.hbase + tv.hoff[i]);
+  const uint32_t bits = __float_as_uint(tv.vel[i].w);
   const EnsSysDev& S = g.sys[bits & kSysMask];
-  const Body A = body(tp, S, at);
+  const Body A = body(tv, S, (uint32_t)i);
   const float inertia = (0.4f * A.m) * (A.r * A.r);
   SBar ab;
   ab.x = xyz4(a.gx[i]);
@@ -290,19 +295,22 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
   const float3 Fb = ab.v * (g.dt / A.m), Tb = ab.w * (g.dt / inertia);
   LawBar th = {0.0f, 0.0f, 0.0f, 0.0f};
   float mu_wb = 0.0f;
-  const uint32_t cnt = tp.cnt[(size_t)tl * n + i], mask = tp.mask[at];
+  const uint32_t cnt = lv.cnt[i], mask = tv.mask[i];
   for (uint32_t k = 0; k < cnt; ++k) {
-    const size_t d = cbase + (size_t)k * n + i;   // tape history entry
     const size_t sl = (size_t)k * n + i;          // cotangent slot (one step)
-    const uint32_t j = tp.idx[lbase + (size_t)k * n + i];
-    const Body B = body(tp, S, (size_t)t * n + j);
+    const uint32_t j = ent[k].x;
+    const Body B = body(tv, S, j);
     const float3 rel = A.x - B.x;
     const float sr = A.r + B.r;
     const float d2 = dot3(rel, rel);
+    const bool had = (mask >> k) & 1u;
     float4 hout = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (d2 < sr * sr && sqrtf(d2) > 0.0f) {
-      const bool had = (mask >> k) & 1u;
-      const float3 xi = had ? f3(tp.hx[d], tp.hy[d], tp.hz[d]) : f3(0.0f, 0.0f, 0.0f);
+      float3 xi = f3(0.0f, 0.0f, 0.0f);
+      if (had) {
+        const float* h = hp + 3 * __popc(mask & ((1u << k) - 1u));
+        xi = f3(h[0], h[1], h[2]);
+      }
       SBar bb;
       bb.x = f3(0.0f, 0.0f, 0.0f);
       bb.v = bb.x;
@@ -313,16 +321,22 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
       a.pv[sl] = w4(bb.v);
       a.pw[sl] = w4(bb.w);
     }
-    a.iH[sl] = hout;
+    if (had) a.iH[sl] = hout;
   }
   // plane walls, in the forward's order; slot nw of the output history is
   // the nw-th contact, slot q of the input the one with the same wall id
   const uint32_t wmask = bits >> kSysBits;
   float4 oh[kWallSlots];
 #pragma unroll
-  for (int q = 0; q < kWallSlots; ++q) {
-    oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-    if ((wmask >> q) & 1u) oh[q] = tp.wh[((size_t)t * kWallSlots + q) * n + i];
+  for (int q = 0; q < kWallSlots; ++q) oh[q] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+  if (wmask) {
+    const float* hw = hp + 3 * __popc(mask);
+#pragma unroll
+    for (int q = 0; q < kWallSlots; ++q)
+      if ((wmask >> q) & 1u) {
+        const float* h = hw + 4 * __popc(wmask & ((1u << q) - 1u));
+        oh[q] = make_float4(h[0], h[1], h[2], h[3]);
+      }
   }
   float4 win[kWallSlots];
 #pragma unroll
@@ -345,7 +359,8 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
     ++nw;
   }
 #pragma unroll
-  for (int q = 0; q < kWallSlots; ++q) a.iW[(size_t)q * n + i] = win[q];
+  for (int q = 0; q < kWallSlots; ++q)
+    if ((wmask >> q) & 1u) a.iW[(size_t)q * n + i] = win[q];
   a.ix[i] = w4(ab.x);
   a.iv[i] = w4(ab.v);
   a.iw[i] = w4(ab.w);
@@ -360,24 +375,27 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
 // Particle i collects, for each neighbour j in contact, the share of j's
 // contact with i that k_adj_pair left in j's slot for i.
 __global__ void __launch_bounds__(kThreads)
-k_adj_gather(EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
+k_adj_gather(EnsTape tp, int t, int n, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const size_t at = (size_t)t * n + i;
-  const size_t cbase = (size_t)tl * cap * n;     // the list step t used
-  const float4 pa = tp.pos[at];
+  const TapeStep ts = tp.steps[t];
+  const TapeStep tl = tp.steps[ts.lat];
+  const TapeView tv = tape_view(tp, ts.block, n);
+  const TapeView lv = tape_view(tp, tl.block, n);
+  const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + tl.lbase + lv.loff[i]);
+  const float4 pa = tv.pos[i];
   const float3 xa = xyz4(pa);
   float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
-  const uint32_t cnt = tp.cnt[(size_t)tl * n + i];
+  const uint32_t cnt = lv.cnt[i];
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t j = tp.idx[cbase + (size_t)k * n + i];
-    const size_t jt = (size_t)t * n + j;
-    const float4 pb = tp.pos[jt];
+    const uint2 e = ent[k];
+    const uint32_t j = e.x;
+    const float4 pb = tv.pos[j];
     const float3 rel = xa - xyz4(pb);
     const float sr = pa.w + pb.w;
     const float d2 = dot3(rel, rel);
     if (!(d2 < sr * sr && sqrtf(d2) > 0.0f)) continue;
-    const uint8_t q = tp.twin[cbase + (size_t)k * n + i];
+    const uint32_t q = e.y & 0xffu;
     if (q == 0xffu) continue;
     const size_t sj = (size_t)q * n + j;
     gx = gx + xyz4(a.px[sj]);
@@ -390,27 +408,28 @@ k_adj_gather(EnsTape tp, int t, int tl, int n, int cap, AdjBufs a) {
 }
 
 // A re-sort backwards: cotangents go to the old positions and, for carried
-// histories, to the old slots (the caller zeroes gH first).
+// histories, to the old slots.
 __global__ void __launch_bounds__(kThreads)
-k_adj_unsort(EnsTape tp, int t, int n, int cap, AdjBufs a) {
+k_adj_unsort(EnsTape tp, int t, int n, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const size_t at = (size_t)t * n + i;
-  const size_t cbase = (size_t)t * cap * n;
-  const int io = tp.perm[at];
+  const TapeStep ts = tp.steps[t];
+  const TapeView tv = tape_view(tp, ts.block, n);
+  const int io = tv.perm[i];
   a.gx[io] = a.ix[i];
   a.gv[io] = a.iv[i];
   a.gw[io] = a.iw[i];
+  const uint32_t wmask = __float_as_uint(tv.vel[i].w) >> kSysBits;
 #pragma unroll
-  for (int q = 0; q < kWallSlots; ++q) a.gW[(size_t)q * n + io] = a.iW[(size_t)q * n + i];
-  const uint32_t cnt = tp.cnt[at];
+  for (int q = 0; q < kWallSlots; ++q)
+    if ((wmask >> q) & 1u) a.gW[(size_t)q * n + io] = a.iW[(size_t)q * n + i];
+  const uint32_t cnt = tv.cnt[i];
+  const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + ts.lbase + tv.loff[i]);
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint8_t s = tp.src[cbase + (size_t)k * n + i];
+    const uint32_t s = (ent[k].y >> 8) & 0xffu;
     if (s != 0xffu) a.gH[(size_t)s * n + io] = a.iH[(size_t)k * n + i];
   }
 }
-
-__global__ void k_adj_slot_next(int* slot) { *slot += 1; }
 
 // Host-layout cotangents (3 floats per particle) to and from the float4
 // buffers of the sweep.
@@ -463,35 +482,28 @@ inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
 
-void adj_launch_snap(const EnsTape& tp, int t, const EnsBufs& b, int cur, int n,
-                     const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
+void adj_launch_seg_start(const EnsTape& tp, int slot0, int len, unsigned long long origin,
+                          unsigned long long stride, unsigned long long lim, cudaStream_t st) {
+  k_adj_seg_start<<<1, 256, 0, st>>>(tp, slot0, len, origin, stride, lim);
+}
+
+void adj_launch_list(const EnsBufs& b, const EnsTape& tp, int n, const StepCtl* ctl,
+                     const int* gate, int resorted, const int32_t* perm, cudaStream_t st) {
+  k_adj_list<<<nblk(n), kThreads, 0, st>>>(b, tp, n, ctl, gate, resorted, perm);
+}
+
+void adj_launch_tick(const EnsTape& tp, const int* rebuilt, cudaStream_t st) {
+  k_adj_tick<<<1, 1, 0, st>>>(tp, rebuilt);
+}
+
+void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int n, const AdjBufs& a,
                      cudaStream_t st) {
-  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, t, nullptr, b, b.S[cur], b.S[2], n, ctl,
-                                            rebuilt, perm);
+  k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, n, a);
+  k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, n, a);
 }
 
-void adj_launch_snap_slot(const EnsTape& tp, int* slot, const EnsBufs& b, int cur, int n,
-                          const StepCtl* ctl, const int* rebuilt, const int32_t* perm,
-                          cudaStream_t st) {
-  k_adj_snap<<<nblk(n), kThreads, 0, st>>>(tp, 0, slot, b, b.S[cur], b.S[2], n, ctl, rebuilt,
-                                            perm);
-  k_adj_slot_next<<<1, 1, 0, st>>>(slot);
-}
-
-void adj_launch_step(const EnsGeom& g, const EnsTape& tp, int t, int tl, int n, int cap,
-                     const AdjBufs& a, cudaStream_t st) {
-  k_adj_pair<<<nblk(n), kThreads, 0, st>>>(g, tp, t, tl, n, cap, a);
-  k_adj_gather<<<nblk(n), kThreads, 0, st>>>(tp, t, tl, n, cap, a);
-}
-
-void adj_launch_twin(const EnsBufs& b, int n, const StepCtl* ctl, const int* gate,
-                     cudaStream_t st) {
-  k_adj_twin<<<nblk(n), kThreads, 0, st>>>(b, n, ctl, gate);
-}
-
-void adj_launch_unsort(const EnsTape& tp, int t, int n, int cap, const AdjBufs& a,
-                       cudaStream_t st) {
-  k_adj_unsort<<<nblk(n), kThreads, 0, st>>>(tp, t, n, cap, a);
+void adj_launch_unsort(const EnsTape& tp, int t, int n, const AdjBufs& a, cudaStream_t st) {
+  k_adj_unsort<<<nblk(n), kThreads, 0, st>>>(tp, t, n, a);
 }
 
 void adj_launch_f3_to_f4(const float* src, float4* dst, int n, cudaStream_t st) {

@@ -198,7 +198,7 @@ void free_ens(blaze_ens* e) {
   for (int k = 0; k < 2; ++k) {
     f(e->b.pid[k]); f(e->b.wh[k]);
     f(e->b.L[k].idx); f(e->b.L[k].cnt); f(e->b.L[k].mask);
-    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz); f(e->b.L[k].src); f(e->b.L[k].twin);
+    f(e->b.L[k].hx); f(e->b.L[k].hy); f(e->b.L[k].hz); f(e->b.L[k].src);
     f(e->rs.keys[k]); f(e->rs.vals[k]);
   }
   f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
@@ -385,7 +385,6 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
     CKF(dalloc(&e->b.L[k].hy, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].hz, (size_t)cap * n));
     CKF(dalloc(&e->b.L[k].src, (size_t)cap * n));
-    CKF(dalloc(&e->b.L[k].twin, (size_t)cap * n));
     CKF(dalloc(&e->rs.keys[k], n));
     CKF(dalloc(&e->rs.vals[k], n));
     CKF(cudaMemset(e->b.L[k].cnt, 0, sizeof(uint32_t) * n));
@@ -661,15 +660,30 @@ struct EnsCheckpoint {
   int cur = 0;
 };
 
+// Where a recorded segment lies in the tape arena: words [o, e).  `valid`
+// while nothing recorded later overlapped them and its own reservations all
+// fit.
+struct TapeSeg {
+  unsigned long long o = 0, e = 0;
+  bool valid = false;
+  std::vector<int> rb;          // per step: 1 when it re-sorted
+};
+
 struct blaze_ens_adj {
   blaze_ens* e = nullptr;
   int nsteps = 0, K = 0, nseg = 0;
   EnsTape tape{};
+  unsigned long long words = 0;            // arena size
+  unsigned long long stride = 0;           // dense block of one step, words
+  TapeCtl* h_tc = nullptr;                 // pinned copy of the tape cursors
+  std::vector<TapeStep> h_steps;           // staging for the re-sort flags
   std::vector<EnsCheckpoint> ck;
+  std::vector<TapeSeg> seg;
+  int on_tape = 0;                         // segments the last forward left on the tape
+  unsigned long long pool_max = 0;         // most pool words one recorded segment took
+  double pool_step = 0.0;                  // most pool words per step of a segment
   AdjBufs A{};
-  std::vector<int> rb;
   bool forward_done = false;
-  int* d_slot = nullptr;                          // tape step the next snapshot writes
   cudaGraphExec_t rgraph[2] = {nullptr, nullptr};  // recording graphs, from S[0] / S[1]
   // per-phase device time of the last backward call (restoring checkpoints,
   // recording segments into the tape, reversing them), from events
@@ -691,19 +705,19 @@ void free_adj(blaze_ens_adj* a) {
   for (cudaEvent_t ev : a->ev)
     if (ev) cudaEventDestroy(ev);
   auto f = [](void* p) { if (p) cudaFree(p); };
-  EnsTape& t = a->tape;
-  f(t.rb); f(t.perm); f(t.src); f(t.pos); f(t.vel); f(t.angv); f(t.idx); f(t.cnt); f(t.mask);
-  f(t.hx); f(t.hy); f(t.hz); f(t.wh); f(t.twin);
+  f(a->tape.arena);
+  f(a->tape.steps);
+  f(a->tape.ctl);
+  if (a->h_tc) cudaFreeHost(a->h_tc);
   for (EnsCheckpoint& c : a->ck) {
     f(c.pos); f(c.vel); f(c.angv); f(c.pid); f(c.idx); f(c.cnt); f(c.mask); f(c.hx); f(c.hy);
     f(c.hz); f(c.wh);
   }
   AdjBufs& b = a->A;
-  for (float4* q : {b.gx, b.gv, b.gw, b.gH, b.gW, b.ix, b.iv, b.iw, b.iH, b.iW, b.Fb, b.Tb, b.px,
+  for (float4* q : {b.gx, b.gv, b.gw, b.gH, b.gW, b.ix, b.iv, b.iw, b.iH, b.iW, b.Fb, b.px,
                     b.pv, b.pw})
     f(q);
   f(b.th);
-  f(a->d_slot);
   f(a->d_sys_off);
   f(a->d_gconst);
   for (int c = 0; c < 2; ++c)
@@ -760,7 +774,8 @@ int restore_checkpoint(blaze_ens_adj* a, const EnsCheckpoint& c) {
 }
 
 // kGraphSteps recorded steps as one graph from S[c]: the step graph of
-// build_graph with a snapshot into the tape after each step's IF node.
+// build_graph, with the list recorded inside each step's IF node (a
+// re-sort), then the tape tick and the recording step.
 int build_record_graph(blaze_ens_adj* a, int c) {
   blaze_ens* e = a->e;
   const int res = sort_result(e);
@@ -795,15 +810,15 @@ int build_record_graph(blaze_ens_adj* a, int c) {
                                      cudaStreamCaptureModeThreadLocal));
     CK(cudaMemsetAsync(e->d_rb + k, 0x01, sizeof(int), e->aux));
     int rc = enqueue_rebuild(e, nullptr, e->aux);
-    adj_launch_twin(e->b, e->n, e->ctl, nullptr, e->aux);
+    adj_launch_list(e->b, a->tape, e->n, e->ctl, nullptr, 1, e->rs.vals[res], e->aux);
     cudaGraph_t tmp = nullptr;
     CK(cudaStreamEndCapture(e->aux, &tmp));
     if (rc) return rc;
-    adj_launch_snap_slot(a->tape, a->d_slot, e->b, e->cur, e->n, e->ctl, e->d_rb + k,
-                         e->rs.vals[res], e->stream);
+    adj_launch_tick(a->tape, e->d_rb + k, e->stream);
     const StepLink link = k + 1 < kGraphSteps ? StepLink{e->d_rb + k, h[k + 1], 1}
                                                : StepLink{e->d_rb + k, 0, 0};
-    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, nullptr, e->opt.block, e->stream);
+    ens_launch_step_record(geom(e), e->b, e->cur, e->n, e->ctl, link, a->tape, e->opt.block,
+                           e->stream);
     e->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
@@ -814,13 +829,17 @@ int build_record_graph(blaze_ens_adj* a, int c) {
   return 0;
 }
 
-// Steps [s0, s0 + len) recomputed from the restored checkpoint into the tape
-// (as recording graphs, the remainder as plain steps).
-int record_segment(blaze_ens_adj* a, int len) {
+// Steps the ensemble through segment `s` from its current state, recording
+// it into the arena from word `origin` (dense blocks, then pool space up to
+// `lim`).  Fills `sg`; sg.valid is false when a reservation did not fit.
+int record_segment(blaze_ens_adj* a, int s, unsigned long long origin, unsigned long long lim,
+                   TapeSeg& sg) {
   blaze_ens* e = a->e;
   const int res = sort_result(e);
-  CK(cudaMemsetAsync(a->d_slot, 0, sizeof(int), e->stream));
-  adj_launch_twin(e->b, e->n, e->ctl, nullptr, e->stream);   // the restored list
+  const int slot0 = s * a->K, len = std::min(a->K, a->nsteps - slot0);
+  cudaStream_t st = e->stream;
+  adj_launch_seg_start(a->tape, slot0, len, origin, a->stride, lim, st);
+  adj_launch_list(e->b, a->tape, e->n, e->ctl, nullptr, 0, nullptr, st);   // the current list
   int t = 0;
   while (t < len) {
     if (len - t >= kGraphSteps) {
@@ -829,33 +848,50 @@ int record_segment(blaze_ens_adj* a, int len) {
         int rc = build_record_graph(a, c);
         if (rc) return rc;
       }
-      CK(cudaGraphLaunch(a->rgraph[c], e->stream));
+      CK(cudaGraphLaunch(a->rgraph[c], st));
       if (kGraphSteps & 1) e->cur ^= 1;
       t += kGraphSteps;
       continue;
     }
-    launch_gate(e->ctl, e->stream);
-    int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
+    launch_gate(e->ctl, st);
+    int rc = enqueue_rebuild(e, &e->ctl->rebuilt, st);
     if (rc) return rc;
-    adj_launch_twin(e->b, e->n, e->ctl, &e->ctl->rebuilt, e->stream);
-    adj_launch_snap_slot(a->tape, a->d_slot, e->b, e->cur, e->n, e->ctl, &e->ctl->rebuilt,
-                         e->rs.vals[res], e->stream);
-    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0}, nullptr,
-                    e->opt.block, e->stream);
+    adj_launch_list(e->b, a->tape, e->n, e->ctl, &e->ctl->rebuilt, 1, e->rs.vals[res], st);
+    adj_launch_tick(a->tape, &e->ctl->rebuilt, st);
+    ens_launch_step_record(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0},
+                           a->tape, e->opt.block, st);
     e->cur ^= 1;
     ++t;
   }
-  CK(cudaMemcpyAsync(a->rb.data(), a->tape.rb, sizeof(int) * len, cudaMemcpyDeviceToHost, e->stream));
-  int st = sync_status(e);
-  return st < 0 ? st : 0;
+  CK(cudaMemcpyAsync(a->h_steps.data(), a->tape.steps + slot0, sizeof(TapeStep) * len,
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(a->h_tc, a->tape.ctl, sizeof(TapeCtl), cudaMemcpyDeviceToHost, st));
+  int rc = sync_status(e);
+  if (rc < 0) return rc;
+  sg.rb.assign(len, 0);
+  for (int q = 0; q < len; ++q) sg.rb[q] = a->h_steps[q].rb;
+  sg.o = origin;
+  sg.e = std::min(a->h_tc->cur, lim);
+  sg.valid = a->h_tc->overflow == 0;
+  if (sg.valid) {
+    const unsigned long long pool = sg.e - origin - (unsigned long long)len * a->stride;
+    a->pool_max = std::max(a->pool_max, pool);
+    a->pool_step = std::max(a->pool_step, (double)pool / len);
+  }
+  return 0;
 }
+
+bool overlaps(const TapeSeg& x, const TapeSeg& y) { return x.o < y.e && y.o < x.e; }
 
 }  // namespace
 
 extern "C" {
 
-int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment) {
+int blaze_ens_adj_create_tape(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment,
+                              unsigned long long arena_bytes) {
   if (!out || !e || nsteps < 1 || segment < 1) return -1;
+  const unsigned long long aw = arena_bytes / 4 & ~3ull;
+  if (aw < (unsigned long long)std::min(segment, nsteps) * tape_block_words(e->n)) return -2;
   if (e->opt.law != BLAZE_LAW_LINEAR) return -1;
   for (const blaze_system& s : e->sys)
     if (s.mu_roll > 0.0f || s.ntris > 0) return -1;
@@ -869,23 +905,8 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
   a->nsteps = nsteps;
   a->K = std::min(segment, nsteps);
   a->nseg = (nsteps + a->K - 1) / a->K;
+  a->seg.resize(a->nseg);
   const size_t n = e->n, cap = e->opt.max_nbr, K = a->K;
-  EnsTape& t = a->tape;
-  t.K = a->K;
-  CKA(dalloc(&t.rb, K));
-  CKA(dalloc(&t.perm, K * n));
-  CKA(dalloc(&t.src, K * cap * n));
-  CKA(dalloc(&t.pos, K * n));
-  CKA(dalloc(&t.vel, K * n));
-  CKA(dalloc(&t.angv, K * n));
-  CKA(dalloc(&t.idx, K * cap * n));
-  CKA(dalloc(&t.cnt, K * n));
-  CKA(dalloc(&t.mask, K * n));
-  CKA(dalloc(&t.hx, K * cap * n));
-  CKA(dalloc(&t.hy, K * cap * n));
-  CKA(dalloc(&t.hz, K * cap * n));
-  CKA(dalloc(&t.wh, K * kWallSlots * n));
-  CKA(dalloc(&t.twin, K * cap * n));
   a->ck.resize(a->nseg);
   for (EnsCheckpoint& c : a->ck) {
     CKA(dalloc(&c.pos, n)); CKA(dalloc(&c.vel, n)); CKA(dalloc(&c.angv, n)); CKA(dalloc(&c.pid, n));
@@ -904,7 +925,6 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
   CKA(dalloc(&b.iW, kWallSlots * n));
   CKA(dalloc(&b.th, 5 * n));
   CKA(dalloc(&b.Fb, n));   // host cotangent stage (12 B of every 16 used)
-  CKA(dalloc(&a->d_slot, 1));
   CKA(dalloc(&a->d_sys_off, e->nsys + 1));
   CKA(dalloc(&a->d_gconst, 5 * (size_t)e->nsys));
   {
@@ -913,26 +933,93 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
     CKA(cudaMemcpy(a->d_sys_off, off.data(), sizeof(int) * (e->nsys + 1),
                    cudaMemcpyHostToDevice));
   }
-  a->rb.assign(a->K, 0);
+  // the tape: the arena and one step record per step of the run
+  a->words = aw;
+  a->stride = tape_block_words(e->n);
+  a->h_steps.resize(a->K);
+  CKA(dalloc(&a->tape.arena, (size_t)aw));
+  CKA(dalloc(&a->tape.steps, (size_t)nsteps));
+  CKA(dalloc(&a->tape.ctl, 1));
+  CKA(cudaMallocHost((void**)&a->h_tc, sizeof(TapeCtl)));
 #undef CKA
   *out = a;
   return 0;
 }
 
+int blaze_ens_adj_create_ex(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment,
+                            long long tape_bytes) {
+  if (!out || !e || nsteps < 1 || segment < 1) return -1;
+  const size_t n = e->n, cap = e->opt.max_nbr, K = (size_t)std::min(segment, nsteps);
+  if (tape_bytes == 0) {
+    // one segment with the most pool space it can take: every list slot an
+    // active history, every wall slot used, a list at every step
+    const size_t words = K * tape_block_words(e->n) + K * n * (3 * cap + 4 * kWallSlots) +
+                         (K + 1) * (n * 2 * cap + 256);
+    return blaze_ens_adj_create_tape(out, e, nsteps, segment, 4ull * (words + 64));
+  }
+  size_t budget;
+  if (tape_bytes > 0) {
+    budget = (size_t)tape_bytes;
+  } else {
+    // what the other buffers of the reverse mode leave free: all device
+    // memory but 4 GiB, less 10 %
+    const int nseg = (nsteps + (int)K - 1) / (int)K;
+    const size_t ckpt = n * (3 * sizeof(float4) + 3 * sizeof(uint32_t) + sizeof(int) +
+                             kWallSlots * sizeof(float4)) + cap * n * 4 * sizeof(float);
+    const size_t bufs = n * (7 * sizeof(float4) + 5 * sizeof(float) +
+                             2 * kWallSlots * sizeof(float4)) + cap * n * 5 * sizeof(float4);
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const size_t other = ckpt * (size_t)nseg + bufs + ((size_t)4 << 30);
+    budget = fr > other ? (fr - other) / 10 * 9 : 0;
+  }
+  return blaze_ens_adj_create_tape(out, e, nsteps, segment, (unsigned long long)budget);
+}
+
+int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment) {
+  return blaze_ens_adj_create_ex(out, e, nsteps, segment, 0);
+}
+
 int blaze_ens_adj_forward(blaze_ens_adj* a) {
   if (!a || !a->e->state_set) return -1;
   blaze_ens* e = a->e;
-  // between checkpoints the steps run as CUDA graphs: graph and plain
-  // stepping give the same results, so the backward's plain recomputation
-  // reproduces this run exactly
-  for (int seg = 0; seg < a->nseg; ++seg) {
-    int rc = save_checkpoint(a, a->ck[seg]);
+  // the trailing segments expected to fit (dense blocks, plus the most pool
+  // space per step seen so far) are recorded as they run (recording graphs);
+  // the others run as plain step graphs between checkpoints.  Graph and
+  // plain stepping give the same results, so a later recomputation
+  // reproduces this run exactly.
+  const double per_step = (double)a->stride + a->pool_step;
+  auto seg_len = [&](int s) { return std::min(a->K, a->nsteps - s * a->K); };
+  int first = a->nseg;
+  for (double need = 0.0; first > 0; --first) {
+    need += per_step * seg_len(first - 1);
+    if (need > (double)a->words) break;
+  }
+  unsigned long long pos = 0;
+  for (TapeSeg& sg : a->seg) sg.valid = false;
+  for (int s = 0; s < a->nseg; ++s) {
+    int rc = save_checkpoint(a, a->ck[s]);
     if (rc) return rc;
-    rc = advance(e, std::min(a->K, a->nsteps - seg * a->K), true);
+    const int len = seg_len(s);
+    if (s < first) {
+      rc = advance(e, len, true);
+      if (rc) return rc;
+      continue;
+    }
+    // a ring of segments in the arena: wrap to its start when the segment is
+    // not expected to fit before the end
+    if ((double)pos + per_step * len > (double)a->words) pos = 0;
+    TapeSeg& sg = a->seg[s];
+    rc = record_segment(a, s, pos, a->words, sg);
     if (rc) return rc;
+    for (int r = first; r < s; ++r)
+      if (a->seg[r].valid && overlaps(a->seg[r], sg)) a->seg[r].valid = false;
+    pos = sg.valid ? (sg.e + 3) & ~3ull : a->words;
   }
   int st = sync_status(e);
   if (st < 0) return st;
+  a->on_tape = 0;
+  for (const TapeSeg& sg : a->seg) a->on_tape += sg.valid ? 1 : 0;
   a->forward_done = true;
   return st;
 }
@@ -964,22 +1051,27 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
   for (cudaEvent_t& ev : a->ev)
     if (!ev) CK(cudaEventCreate(&ev));
   for (float& m : a->ms_phase) m = 0.0f;
-  for (int seg = a->nseg - 1; seg >= 0; --seg) {
-    const int len = std::min(a->K, a->nsteps - seg * a->K);
+  for (int s = a->nseg - 1; s >= 0; --s) {
+    const int len = std::min(a->K, a->nsteps - s * a->K);
+    TapeSeg& sg = a->seg[s];
     CK(cudaEventRecord(a->ev[0], st));
-    int rc = restore_checkpoint(a, a->ck[seg]);
-    if (rc) return rc;
+    if (!sg.valid) {
+      int rc = restore_checkpoint(a, a->ck[s]);
+      if (rc) return rc;
+    }
     CK(cudaEventRecord(a->ev[1], st));
-    rc = record_segment(a, len);
-    if (rc) return rc;
+    if (!sg.valid) {
+      int rc = record_segment(a, s, 0, a->words, sg);
+      if (rc) return rc;
+      if (!sg.valid) return -2;                  // one segment does not fit the tape
+      for (int r = 0; r < s; ++r) a->seg[r].valid = false;
+    }
     CK(cudaEventRecord(a->ev[2], st));
-    std::vector<int> list_at(len, 0);   // tape step holding the list step t used
-    for (int t = 1; t < len; ++t) list_at[t] = a->rb[t] ? t : list_at[t - 1];
-    for (int t = len - 1; t >= 0; --t) {
-      adj_launch_step(g, a->tape, t, list_at[t], (int)n, (int)cap, A, st);
-      if (a->rb[t]) {
-        CK(cudaMemsetAsync(A.gH, 0, sizeof(float4) * cap * n, st));
-        adj_launch_unsort(a->tape, t, (int)n, (int)cap, A, st);
+    for (int q = len - 1; q >= 0; --q) {
+      const int t = s * a->K + q;
+      adj_launch_step(g, a->tape, t, (int)n, A, st);
+      if (sg.rb[q]) {
+        adj_launch_unsort(a->tape, t, (int)n, A, st);
       } else {
         std::swap(A.gx, A.ix);
         std::swap(A.gv, A.iv);
@@ -1007,8 +1099,7 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
   }
   if (gconst) {
     // positions of system s are [off_s, off_s + n_s) in every order the run
-    // takes (keys sort by system first); the per-system sums run on the
-    // device, in particle order, in FP64
+    // takes (keys sort by system first)
     adj_launch_sum_constants(A.th, a->d_sys_off, e->nsys, a->d_gconst, st);
     CK(cudaMemcpyAsync(gconst, a->d_gconst, sizeof(double) * 5 * e->nsys, cudaMemcpyDeviceToHost,
                        st));
@@ -1023,6 +1114,15 @@ int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,
   if (ms_restore) *ms_restore = a->ms_phase[0];
   if (ms_record) *ms_record = a->ms_phase[1];
   if (ms_reverse) *ms_reverse = a->ms_phase[2];
+  return 0;
+}
+
+int blaze_ens_adj_tape_info(blaze_ens_adj* a, unsigned long long* arena_bytes, int* on_tape,
+                            unsigned long long* pool_bytes_max) {
+  if (!a) return -1;
+  if (arena_bytes) *arena_bytes = 4 * a->words;
+  if (on_tape) *on_tape = a->on_tape;
+  if (pool_bytes_max) *pool_bytes_max = 4 * a->pool_max;
   return 0;
 }
 

@@ -305,16 +305,35 @@ __global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
 }
 
 // ------------------------------------------------------------------- step
-template <int kLaw, bool kCapture>
+// kRecord: also write what the step reads into tape slot tp.ctl->slot (the
+// history words are reserved first, by every thread of the block).
+template <int kLaw, bool kCapture, bool kRecord>
 __global__ void __launch_bounds__(kMaxStepBlock)
 k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
-           StepCtl* ctl, StepLink link, EnsCapture cap) {
+           StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
   const bool rebuilt = *link.rebuilt != 0;
   const StateBuf in = rebuilt ? in_sorted : in_plain;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const int e = ctl->epoch & 1;
   const EnsList L = b.L[e];
+  TapeView tv{};
+  float* hrec = nullptr;
+  if constexpr (kRecord) {
+    const TapeStep ts = tp.steps[tp.ctl->slot];
+    tv = tape_view(tp, ts.block, n);
+    uint32_t words = 0;
+    if (i < n)
+      words = 3u * (uint32_t)__popc(L.mask[i]) +
+              4u * (uint32_t)__popc(__float_as_uint(in.vel[i].w) >> kSysBits);
+    bool ok;
+    const uint32_t off =
+        tape_reserve(words, &tp.ctl->cur, tp.ctl->lim, ts.hbase, &tp.ctl->overflow, ok);
+    if (i < n) {
+      tv.hoff[i] = off;
+      if (ok) hrec = reinterpret_cast<float*>(tp.arena + ts.hbase + off);
+    }
+  }
+  if (i >= n) return;
   const size_t stride = (size_t)b.stride;
   const float dt = g.dt;
   const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
@@ -331,6 +350,12 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   float3 f = f3(0.0f, 0.0f, 0.0f), t = f3(0.0f, 0.0f, 0.0f);
   const uint32_t cnt = L.cnt[i];
   const uint32_t mask_o = L.mask[i];
+  if constexpr (kRecord) {
+    tv.pos[i] = pa4;
+    tv.vel[i] = va4;
+    tv.angv[i] = wa4;
+    tv.mask[i] = mask_o;
+  }
   uint32_t mask = 0;
   for (uint32_t k = 0; k < cnt; ++k) {
     const size_t sk = (size_t)k * stride + i;
@@ -349,7 +374,17 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);
     float3 xi = f3(0.0f, 0.0f, 0.0f);
-    if ((mask_o >> k) & 1u) xi = f3(L.hx[sk], L.hy[sk], L.hz[sk]);
+    if ((mask_o >> k) & 1u) {
+      xi = f3(L.hx[sk], L.hy[sk], L.hz[sk]);
+      if constexpr (kRecord) {
+        if (hrec) {
+          float* h = hrec + 3 * __popc(mask_o & ((1u << k) - 1u));
+          h[0] = xi.x;
+          h[1] = xi.y;
+          h[2] = xi.z;
+        }
+      }
+    }
     const float rs = (ra * rb) / (ra + rb);
     const float ms = (ma * mb) / (ma + mb);
     const float3 vcpa = va + cross3(wa, nrm * (-ra));
@@ -375,6 +410,20 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
 #pragma unroll
     for (int q = 0; q < kWallSlots; ++q)
       if ((wmask_o >> q) & 1u) oh[q] = b.wh[e][(size_t)q * stride + i];
+    if constexpr (kRecord) {
+      if (hrec) {
+        float* h = hrec + 3 * __popc(mask_o);
+#pragma unroll
+        for (int q = 0; q < kWallSlots; ++q)
+          if ((wmask_o >> q) & 1u) {
+            float* hq = h + 4 * __popc(wmask_o & ((1u << q) - 1u));
+            hq[0] = oh[q].x;
+            hq[1] = oh[q].y;
+            hq[2] = oh[q].z;
+            hq[3] = oh[q].w;
+          }
+      }
+    }
   }
   int nw = 0;
   auto wall_contact = [&](int id, float3 nrm, float delta) {
@@ -525,15 +574,23 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
   const EnsCapture c = cap ? *cap : EnsCapture{nullptr, nullptr};
   const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
   const int gs = (n + bs - 1) / bs;
-#define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c
+#define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c, EnsTape{}
   if (g.law == kLawHertz) {
-    if (cap) k_ens_step<kLawHertz, true><<<gs, bs, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawHertz, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+    if (cap) k_ens_step<kLawHertz, true, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawHertz, false, false><<<gs, bs, 0, st>>>(ENS_ARGS);
   } else {
-    if (cap) k_ens_step<kLawLinear, true><<<gs, bs, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawLinear, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+    if (cap) k_ens_step<kLawLinear, true, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+    else k_ens_step<kLawLinear, false, false><<<gs, bs, 0, st>>>(ENS_ARGS);
   }
 #undef ENS_ARGS
+}
+
+void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
+                            StepLink link, const EnsTape& tape, int block, cudaStream_t st) {
+  const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
+  const int gs = (n + bs - 1) / bs;
+  k_ens_step<kLawLinear, false, true><<<gs, bs, 0, st>>>(
+      g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, EnsCapture{nullptr, nullptr}, tape);
 }
 
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,

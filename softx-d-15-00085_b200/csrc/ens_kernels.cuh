@@ -65,7 +65,6 @@ struct EnsList {        // one copy of the neighbour list + tangential history
   float* hy;
   float* hz;
   uint8_t* src;         // per slot: old slot its history came from (0xff none), or null
-  uint8_t* twin;        // per slot: the neighbour's slot for this particle (reverse mode)
 };
 
 struct EnsBufs {
@@ -89,6 +88,115 @@ struct EnsGeom {
 
 struct EnsCapture { float4* f; float4* t; };
 
+// Reverse-mode tape: one arena of 32-bit words holding, per recorded
+// segment, the dense blocks of its steps followed by the pool space its
+// steps reserved.  The dense block of a step (n particles; word offsets):
+//   pos 0, vel 4n, angv 8n (float4: the step's input state), mask 12n
+//   (active histories before the step), hoff 13n (the particle's history
+//   words, from TapeStep::hbase), and at a list step (a re-sort, or the
+//   first step of a segment) cnt 14n, loff 15n (the particle's list entries,
+//   from TapeStep::lbase), perm 16n (a re-sort: old index of each new
+//   position); 17n words rounded up to a multiple of 4.
+// Pool space, reserved a thread block at a time: per particle and step, 3
+// words per active history (slot order) then 4 per wall history (xi, wall
+// id); per particle and list, 2 words per list slot: (neighbour,
+// twin | src << 8), twin = the neighbour's slot that holds this particle
+// (0xff: none), src = the old slot a re-sort carried the history from (0xff:
+// none).  Reservations are an even number of words, so list entries are
+// 8-byte aligned.
+struct TapeStep {
+  unsigned long long block;   // arena word of the step's dense block
+  unsigned long long hbase;   // the step's history words count from here
+  unsigned long long lbase;   // the list recorded for the step counts from here
+  int rb;                     // 1 when the step re-sorted
+  int lat;                    // step whose list this step used
+};
+
+struct TapeCtl {
+  unsigned long long cur;     // next free arena word
+  unsigned long long lim;     // reservations must end at or below this
+  unsigned long long lsnap;   // cur when the current step began
+  int slot;                   // the step last begun
+  int lslot;                  // the step holding the current list
+  int overflow;               // a reservation did not fit (nothing written)
+  int pad;
+};
+
+struct EnsTape {
+  uint32_t* arena;
+  TapeStep* steps;            // one per step of the run
+  TapeCtl* ctl;
+};
+
+__host__ __device__ constexpr unsigned long long tape_block_words(int n) {
+  return ((unsigned long long)n * 17ull + 3ull) & ~3ull;
+}
+
+struct TapeView {
+  float4* pos;
+  float4* vel;
+  float4* angv;
+  uint32_t* mask;
+  uint32_t* hoff;
+  uint32_t* cnt;
+  uint32_t* loff;
+  int32_t* perm;
+};
+
+__device__ __forceinline__ TapeView tape_view(const EnsTape& tp, unsigned long long block, int n) {
+  uint32_t* b = tp.arena + block;
+  const size_t m = (size_t)n;
+  TapeView v;
+  v.pos = reinterpret_cast<float4*>(b);
+  v.vel = reinterpret_cast<float4*>(b + 4 * m);
+  v.angv = reinterpret_cast<float4*>(b + 8 * m);
+  v.mask = b + 12 * m;
+  v.hoff = b + 13 * m;
+  v.cnt = b + 14 * m;
+  v.loff = b + 15 * m;
+  v.perm = reinterpret_cast<int32_t*>(b + 16 * m);
+  return v;
+}
+
+// Reserves `words` consecutive pool units for the calling thread, a thread
+// block at a time (one atomic per block on *cur).  Every thread of the block
+// calls it; blockDim.x is a multiple of 32.  Returns the thread's first unit
+// counted from `base`; ok is false (and *overflow raised) when the block's
+// reservation would end past `lim` or 2^32 or more units after `base`, in
+// which case nothing may be written.
+__device__ __forceinline__ uint32_t tape_reserve(uint32_t words, unsigned long long* cur,
+                                                 unsigned long long lim, unsigned long long base,
+                                                 int* overflow, bool& ok) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ unsigned long long s_start;
+  __shared__ int s_ok;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = words;                       // inclusive scan over the warp
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) s_warp[w] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      const uint32_t v = s_warp[q];
+      s_warp[q] = (uint32_t)tot;
+      tot += v;
+    }
+    tot += tot & 1ull;                      // keep the cursor even
+    const unsigned long long start = atomicAdd(cur, tot);
+    const bool fits = start + tot <= lim && start + tot - base <= 0xffffffffull;
+    if (!fits) atomicExch(overflow, 1);
+    s_start = start;
+    s_ok = fits ? 1 : 0;
+  }
+  __syncthreads();
+  ok = s_ok != 0;
+  return (uint32_t)(s_start - base) + s_warp[w] + (x - words);
+}
+
 void ens_launch_hash(const EnsGeom& g, const EnsBufs& b, int cur, int n, uint32_t* keys,
                      StepCtl* ctl, const int* gate, cudaStream_t st);
 void ens_launch_reorder(const EnsBufs& b, int cur, int n, const uint32_t* keys,
@@ -102,6 +210,10 @@ void ens_launch_epoch(StepCtl* ctl, const int* gate, cudaStream_t st);
 constexpr int kMaxStepBlock = 512;
 void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
                      StepLink link, const EnsCapture* cap, int block, cudaStream_t st);
+// The same step (linear law) writing what it reads into the tape as step
+// tape.ctl->slot: input state, history mask, active and wall histories.
+void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
+                            StepLink link, const EnsTape& tape, int block, cudaStream_t st);
 // Staged caller arrays -> state S[cur], pid = index, both list copies and
 // every history cleared; flags[0] |= 1 for a radius that is not positive.
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,

@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 
 from bindings import EnsRestated
+from blaze import device
 from blaze import ensemble as E
 from blaze import synth
 
@@ -95,3 +96,81 @@ def test_law_constant_gradient(gpu_grads, oracle_grads):
     prec = oracle_grads[4]
     print("law-constant gradients vs %s, relative error per (system, constant):\n" % prec, rel)
     assert np.all(rel < TOL[prec]), rel
+
+
+def run_with_tape(case, **kw):
+    S, W, p, r, v0, wx, wv = case
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, max_nbr=32, use_graph=0)
+    ens.set_state(p, r, v0)
+    adj = E.Adjoint(ens, T, SEG, **kw)
+    assert adj.forward() == 0
+    info = adj.tape_info()
+    st = ens.state()
+    out = adj.backward(wx[st["pid"]], wv[st["pid"]], None)
+    info_after = adj.tape_info()
+    adj.close()
+    ens.close()
+    return out, info, info_after
+
+
+def assert_same_grads(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_tape_holding_every_segment(case, gpu_grads):
+    """A budget that holds the whole run: the forward records all four
+    segments, the backward recomputes none, and the gradients are those of
+    the one-segment tape bit for bit (a recomputed segment reproduces the
+    forward's tape exactly)."""
+    out, info, _ = run_with_tape(case, tape_bytes=64 << 20)
+    assert info[1] == 4, info
+    assert_same_grads(out, gpu_grads[1:])
+
+
+def state_bytes(n, steps):
+    """Arena bytes of `steps` recorded steps' dense blocks (17 words per
+    particle, rounded up to 4 words)."""
+    return 4 * ((17 * n + 3) // 4 * 4) * steps
+
+
+def test_tape_ring(case, gpu_grads):
+    """An arena with room for one 64-step segment and its pools: the forward
+    records the last two segments (their states fit), the last one wrapping
+    to the start of the arena when the one before leaves no room; the
+    backward reverses what is left, recomputes the rest, and the gradients
+    are unchanged bit for bit."""
+    n = len(case[2])
+    _, _, full = run_with_tape(case, tape_bytes=64 << 20)
+    pool_max = full[2]
+    assert pool_max > 0
+    out, info, _ = run_with_tape(case, arena_bytes=state_bytes(n, SEG) + pool_max + 1024)
+    assert 1 <= info[1] < 4, info
+    assert_same_grads(out, gpu_grads[1:])
+
+
+def test_tape_pool_overflow(case):
+    """Pool space for half the largest segment: the recording kernels find
+    that their reservations do not fit and write nothing, and the backward
+    reports it (-2) instead of reversing a segment it could not record."""
+    n = len(case[2])
+    _, _, full = run_with_tape(case, tape_bytes=64 << 20)
+    S, W, p, r, v0, wx, wv = case
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, max_nbr=32, use_graph=0)
+    ens.set_state(p, r, v0)
+    adj = E.Adjoint(ens, T, SEG, arena_bytes=state_bytes(n, SEG) + full[2] // 2)
+    assert adj.forward() == 0
+    assert adj.tape_info()[1] < 4
+    st = ens.state()
+    with pytest.raises(device.BlazeError):
+        adj.backward(wx[st["pid"]], wv[st["pid"]], None)
+    adj.close()
+    ens.close()
+
+
+def test_tape_too_small_for_a_segment(case):
+    S, W, p, r, v0, wx, wv = case
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, max_nbr=32, use_graph=0)
+    with pytest.raises(device.BlazeError):
+        E.Adjoint(ens, T, SEG, tape_bytes=1 << 10)
+    ens.close()
