@@ -274,7 +274,7 @@ __global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
 // force and torque; then the reverse of each of its own contacts, once: its
 // state, history and law-constant cotangents are kept, the share that goes
 // to the neighbour is left in the slot (px, pv, pw) for k_adj_gather.
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 5)
 k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -299,13 +299,20 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   for (uint32_t k = 0; k < cnt; ++k) {
     const size_t sl = (size_t)k * n + i;          // cotangent slot (one step)
     const uint32_t j = ent[k].x;
-    const Body B = body(tv, S, j);
-    const float3 rel = A.x - B.x;
-    const float sr = A.r + B.r;
+    const float4 pb = tv.pos[j];
+    const float3 rel = A.x - xyz4(pb);
+    const float sr = A.r + pb.w;
     const float d2 = dot3(rel, rel);
     const bool had = (mask >> k) & 1u;
     float4 hout = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (d2 < sr * sr && sqrtf(d2) > 0.0f) {
+      const float4 vb = tv.vel[j], wb = tv.angv[j];
+      Body B;
+      B.x = xyz4(pb);
+      B.v = xyz4(vb);
+      B.w = xyz4(wb);
+      B.r = pb.w;
+      B.m = S.dens43pi * ((pb.w * pb.w) * pb.w);
       float3 xi = f3(0.0f, 0.0f, 0.0f);
       if (had) {
         const float* h = hp + 3 * __popc(mask & ((1u << k) - 1u));
