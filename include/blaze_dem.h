@@ -128,6 +128,25 @@ int blaze_num_current(blaze_sim* s);
 int blaze_num_rebuilds(blaze_sim* s);
 int blaze_update_wobj(blaze_sim* s, const WOBJ* w, int n_w);
 int blaze_update_dobj(blaze_sim* s, const DOBJ* d, int n_d);
+/* Turn the volume objects attached to the drum (is_attached_DWorld) by
+ * rad_per_step about the axis through (about_x, about_y) parallel to z
+ * before every step, on the device, as the mill driver's
+ * Rotate_VolObject_Inc does on the host before each Device_DEM_UpdateSim
+ * (Processing_Mills.h:4-75, main.cpp:113-124): vertices and centre of mass
+ * turned, face centroids, normals and areas recomputed, in its FP32
+ * operation order with the host's cosf / sinf of the angle.  on = 0 stops. */
+int blaze_set_dobj_rotation(blaze_sim* s, float about_x, float about_y, float rad_per_step,
+                            int on);
+/* The volume objects as they are now (turned ones included). */
+int blaze_get_dobj(blaze_sim* s, DOBJ* d, int n_d);
+/* Energy tallies (SimulationInfo::EnergyCalc): energy dissipated in
+ * particle-particle, volume-object and world-object contacts since the
+ * last reset, in Device_Get_Energy's units (tally x 1e-4), summed in FP64 in
+ * a fixed order (the reference adds FP32 values with float atomics).
+ * Spheres only: polyhedral runs leave them at zero. */
+int blaze_get_energy(blaze_sim* s, double* e3);
+/* Set the raw tallies (Device_Set_Tallys); NULL zeroes them. */
+int blaze_set_energy(blaze_sim* s, const double* raw3);
 /* Last step's forces (capture_forces=1), AoS float3 x6: particle-particle
  * (incl. gravity), wall, volume-object; translational then rotational. */
 int blaze_get_forces(blaze_sim* s, float* f_pp, float* t_pp, float* f_w, float* t_w, float* f_l,

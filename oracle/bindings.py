@@ -80,6 +80,10 @@ class RefHost:
             lib.refh_update_wobj.argtypes = [C.POINTER(T.WOBJ), C.c_int]
             lib.refh_update_dobj.argtypes = [C.POINTER(T.DOBJ), C.c_int]
             lib.refh_open_hatch.argtypes = [C.POINTER(T.WOBJ), C.c_int]
+            lib.refh_set_dobj_rotation.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int]
+            lib.refh_get_dobj.argtypes = [C.POINTER(T.DOBJ), C.c_int]
+            lib.refh_set_energy.argtypes = [_f]
+            lib.refh_get_energy64.argtypes = [C.POINTER(C.c_double)]
             lib.refh_parse.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(RefProject),
                                        C.POINTER(T.WOBJ), C.c_int, C.POINTER(T.POBJ), C.c_int,
                                        C.POINTER(T.DOBJ), C.c_int]
@@ -152,6 +156,26 @@ class RefHost:
         e = np.zeros(3, np.float32)
         self.lib.refh_get_energy(_p(e, C.c_float))
         return e
+
+    def energy64(self):
+        """The same tallies summed in FP64 (GetEnergy's units)."""
+        e = np.zeros(3, np.float64)
+        self.lib.refh_get_energy64(_p(e, C.c_double))
+        return e
+
+    def reset_energy(self):
+        self.lib.refh_set_energy(None)
+
+    def set_dobj_rotation(self, about_x, about_y, rad_per_step, on=True):
+        """Turn the attached volume objects before every step, as the mill
+        driver does (restated in ref_host/refhost_kernels.cpp)."""
+        self.lib.refh_set_dobj_rotation(float(about_x), float(about_y), float(rad_per_step),
+                                        1 if on else 0)
+
+    def dobj(self, n_d):
+        d = (T.DOBJ * max(1, n_d))()
+        self.lib.refh_get_dobj(d, int(n_d))
+        return d
 
     @staticmethod
     def parse_isolated(projects_root, project, world):

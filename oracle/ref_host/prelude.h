@@ -14,7 +14,8 @@
  *     correctness; GPU_Memory_Transfer.cuh:149-158 only orders counter writes
  *     that the driver performs itself);
  *   - rsqrtf (absent on the host) is 1/sqrtf;
- *   - float/int atomicAdd use an OpenMP atomic capture;
+ *   - float/int atomicAdd use an OpenMP atomic capture (float ones are also
+ *     reported to the driver, which sums the energy tallies' values in FP64);
  *   - Thrust is pointed at its sequential C++ backend, so the reference's own
  *     thrust::stable_sort_by_key call (Collision_Detection_BroadPhase.cuh:110-117)
  *     runs on the host unchanged.
@@ -47,10 +48,14 @@ extern thread_local dim3 gridDim;
 static inline void __syncthreads() {}
 static inline float rsqrtf(float x) { return 1.0f / sqrtf(x); }
 
+/* Every float atomicAdd is also reported to the driver, which keeps an FP64
+ * sum of the same values for the energy tallies (refhost_kernels.cpp). */
+void refh_float_added(float* a, float v);
 static inline float atomicAdd(float* a, float v) {
   float o;
 #pragma omp atomic capture
   { o = *a; *a += v; }
+  refh_float_added(a, v);
   return o;
 }
 static inline int atomicAdd(int* a, int v) {

@@ -55,7 +55,52 @@ struct RefState {
   std::vector<float3> c_f_pp, c_f_pp_ang, c_f_w, c_f_w_ang, c_f_l, c_f_l_ang;
   int overflow = 0;
   double call_time = 0.0;
+  /* the mill driver's lifter turn before every step (refh_set_dobj_rotation) */
+  bool dobj_rot = false;
+  float rot_ax = 0.0f, rot_ay = 0.0f, rot_rad = 0.0f;
 } S;
+
+/* FP64 sums of the values the kernels add to the three energy tallies, in
+ * the same order as the FP32 tallies (one host thread) or any order. */
+double g_tally64[3] = {0.0, 0.0, 0.0};
+
+/* Rotate_VolObject_Inc (Processing_Mills.h:4-75), restated on the uploaded
+ * DynamicObject array (which Device_Update_DObjectPostions fills with the
+ * host's turned copy, DeviceInterface.cu:2826-2831): the attached objects'
+ * vertices and centre of mass turn by rot_rad about (rot_ax, rot_ay, 0),
+ * then every face's centroid, normal and area follow from the vertices.
+ * Single precision throughout, cos / sin of the float angle. */
+void rotate_dobj_inc() {
+  const float c = std::cos(S.rot_rad), sn = std::sin(S.rot_rad);
+  const float3 about = make_float3(S.rot_ax, S.rot_ay, 0.0f);
+  for (int k = 0; k < Num_DynamicObjects; ++k) {
+    DOBJ& D = DynamicObject[k];
+    if (!D.is_attached_DWorld) continue;
+    for (int v = 0; v < D.num_vertex; ++v) {
+      const float3 p = D.vertex[v] - about;
+      D.vertex[v].x = c * p.x + sn * p.y;
+      D.vertex[v].y = -sn * p.x + c * p.y;
+      D.vertex[v] = D.vertex[v] + about;
+    }
+    for (int j = 0; j < D.num_faces; ++j) {
+      Surface& F = D.faces[j];
+      float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+      for (int f = 0; f < F.num_vertex; ++f) sum = sum + D.vertex[F.vertex_Order[f]];
+      F.centroid = (1.0f / F.num_vertex) * sum;
+      const float3 v1 = D.vertex[F.vertex_Order[1]] - D.vertex[F.vertex_Order[0]];
+      const float3 v2 = D.vertex[F.vertex_Order[2]] - D.vertex[F.vertex_Order[1]];
+      const float3 v3 = D.vertex[F.vertex_Order[3]] - D.vertex[F.vertex_Order[2]];
+      const float3 v4 = D.vertex[F.vertex_Order[0]] - D.vertex[F.vertex_Order[3]];
+      const float3 n = cross(v2, v1);
+      F.normal = n / length(n);
+      F.area = 0.500000f * length(n) + 0.500000f * length(cross(v3, v4));
+    }
+    const float3 p = D.COM - about;
+    D.COM.x = c * p.x + sn * p.y;
+    D.COM.y = -sn * p.x + c * p.y;
+    D.COM = D.COM + about;
+  }
+}
 
 /* Run `body` once per (block, thread) of a 1-D launch over n items. */
 template <class F>
@@ -76,6 +121,16 @@ void launch(int n, F&& body) {
 }
 
 }  // namespace
+
+void refh_float_added(float* a, float v) {
+  int k = -1;
+  if (a == &Tally_EnergyDis_PP) k = 0;
+  else if (a == &Tally_EnergyDisLift) k = 1;
+  else if (a == &Tally_EnergyDisSurf) k = 2;
+  if (k < 0) return;
+#pragma omp atomic
+  g_tally64[k] += (double)v;
+}
 
 extern "C" {
 
@@ -102,6 +157,7 @@ int refh_init(const SimulationInfo* si, const WOBJ* w, int n_w, const POBJ* p,
   Num_DynamicObjects = n_d;
   Tally_EnergyDis_PP = Tally_EnergyDisLift = Tally_EnergyDisSurf = 0.0f;
   Tally_EnergyDis_Norm = Tally_EnergyDis_Shear = 0.0f;
+  for (double& t : g_tally64) t = 0.0;
   Kill_count = 0;
   S.n_w = n_w; S.n_p = n_p; S.n_d = n_d;
   const int n = si->Num_Particles;
@@ -269,6 +325,7 @@ static int step_once() {
 
 int refh_step(int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
+    if (S.dobj_rot) rotate_dobj_inc();
     int rc = step_once();
     if (rc) return rc;
   }
@@ -348,6 +405,32 @@ int refh_get_energy(float* e3) {
 int refh_update_wobj(const WOBJ* w, int n_w) {
   if (n_w < 0 || n_w > 8) return 1;
   std::memcpy(WorldObject, w, sizeof(WOBJ) * n_w);
+  return 0;
+}
+
+void refh_set_dobj_rotation(float about_x, float about_y, float rad_per_step, int on) {
+  S.dobj_rot = on != 0;
+  S.rot_ax = about_x;
+  S.rot_ay = about_y;
+  S.rot_rad = rad_per_step;
+}
+
+int refh_get_dobj(DOBJ* d, int n_d) {
+  if (n_d < 0 || n_d > 32) return 1;
+  std::memcpy(d, DynamicObject, sizeof(DOBJ) * n_d);
+  return 0;
+}
+
+void refh_set_energy(const float* raw3) {
+  Tally_EnergyDis_PP = raw3 ? raw3[0] : 0.0f;
+  Tally_EnergyDisLift = raw3 ? raw3[1] : 0.0f;
+  Tally_EnergyDisSurf = raw3 ? raw3[2] : 0.0f;
+  for (int k = 0; k < 3; ++k) g_tally64[k] = raw3 ? (double)raw3[k] : 0.0;
+}
+
+/* The FP64 sums of the same values, in GetEnergy's units (x 1e-4). */
+int refh_get_energy64(double* e3) {
+  for (int k = 0; k < 3; ++k) e3[k] = g_tally64[k] * 1E-4;
   return 0;
 }
 

@@ -54,6 +54,10 @@ def load():
     lib.blaze_destroy.argtypes = [C.c_void_p]
     lib.blaze_set_options.argtypes = [C.c_void_p, P(Options)]
     lib.blaze_set_cylinder_rotation.argtypes = [C.c_void_p, C.c_int]
+    lib.blaze_set_dobj_rotation.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int]
+    lib.blaze_get_dobj.argtypes = [C.c_void_p, C.POINTER(T.DOBJ), C.c_int]
+    lib.blaze_get_energy.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.blaze_set_energy.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.blaze_set_state.argtypes = [C.c_void_p, _f, _f, _f, _u, _i]
     lib.blaze_get_state.argtypes = [C.c_void_p, _f, _f, _f, _u, _i]
     lib.blaze_set_state_ornt.argtypes = [C.c_void_p, _f, _f, _f, _f, _u, _i]
@@ -128,6 +132,7 @@ class Simulation:
             pobj, n_p, dobj, n_d = project.pobj, project.n_p, project.dobj, project.n_d
         self.lib = lib
         self.n = sim_info.Num_Particles
+        self.n_d = int(n_d)
         self.poly = sim_info.particle_type == 1
         self.opts = default_options(**options)
         h = C.c_void_p()
@@ -156,6 +161,29 @@ class Simulation:
 
     def set_cylinder_rotation(self, on):
         _check(self.lib.blaze_set_cylinder_rotation(self.h, 1 if on else 0), "cylinder rotation")
+
+    def set_dobj_rotation(self, about_x, about_y, rad_per_step, on=True):
+        """Turn the volume objects attached to the drum by rad_per_step about
+        (about_x, about_y) before every step, on the device (the mill
+        driver's Rotate_VolObject_Inc)."""
+        _check(self.lib.blaze_set_dobj_rotation(self.h, float(about_x), float(about_y),
+                                                float(rad_per_step), 1 if on else 0),
+               "blaze_set_dobj_rotation")
+
+    def dobj(self):
+        d = (T.DOBJ * max(1, self.n_d))()
+        _check(self.lib.blaze_get_dobj(self.h, d, self.n_d), "blaze_get_dobj")
+        return d
+
+    def energy(self):
+        """Energy tallies (particle-particle, volume objects, world objects)
+        in Device_Get_Energy's units, FP64."""
+        e = np.zeros(3, np.float64)
+        _check(self.lib.blaze_get_energy(self.h, _ptr(e, C.c_double)), "blaze_get_energy")
+        return e
+
+    def reset_energy(self):
+        _check(self.lib.blaze_set_energy(self.h, None), "blaze_set_energy")
 
     def set_state(self, pos, vel=None, avel=None, ptype=None, pid=None, quat=None):
         """Positions (centres of mass), velocities, angular velocities,

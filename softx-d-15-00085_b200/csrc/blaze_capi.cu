@@ -8,6 +8,7 @@
 // and a step is a fixed sequence of kernel launches on one stream.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -79,9 +80,18 @@ struct blaze_sim {
   int stepc = 0;        // steps since the last removal check
   uint32_t status = 0;  // accumulated, reported at sync points
   int last_launches = 0;
-  // tallies kept for the reference interface (float, host side)
-  float tallies[6]{};
+  // energy tallies (SimulationInfo::EnergyCalc): particle-particle, volume
+  // objects, world objects, FP64 on the device; per-particle values of the
+  // step and per-block partial sums when the step computes them
+  double* d_tally = nullptr;
+  double* d_eb = nullptr;
+  double* d_epart = nullptr;
   float fc = 0.0f;
+  // volume objects turned with the drum on the device every step
+  // (blaze_set_dobj_rotation); the device copy is then the current one
+  bool dobj_rot = false;
+  bool dobj_on_device = false;
+  float rot_ax = 0.0f, rot_ay = 0.0f, rot_c = 1.0f, rot_s = 0.0f;
   // optional per-phase event timing (non-graph stepping only)
   bool profile = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -308,7 +318,31 @@ void build_wall_grid(blaze_sim* s, std::vector<uint32_t>& off, std::vector<uint1
   off[nt] = (uint32_t)idx.size();
 }
 
+// With the volume objects turned on the device, copy them back into the
+// host's DOBJ and parameter mirrors (vertices, faces, centre of mass) before
+// anything re-uploads the parameters from the host.
+int pull_dobj(blaze_sim* s) {
+  if (!s->dobj_on_device) return 0;
+  CK(cudaStreamSynchronize(s->stream));
+  const char* src = reinterpret_cast<const char*>(s->dp) + offsetof(SimParams, dobj);
+  CK(cudaMemcpy(s->hp.dobj, src, sizeof(DobjDev) * kMaxDobj, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < s->n_d; ++k) {
+    const DobjDev& G = s->hp.dobj[k];
+    DOBJ& D = s->d[k];
+    for (int v = 0; v < G.num_vertex; ++v) D.vertex[v] = G.vert[v];
+    for (int f = 0; f < G.num_faces; ++f) {
+      D.faces[f].centroid = G.faces[f].centroid;
+      D.faces[f].normal = G.faces[f].normal;
+      D.faces[f].area = G.faces[f].area;
+    }
+    D.COM = G.com;
+  }
+  return 0;
+}
+
 int upload_walls(blaze_sim* s) {
+  int rc = pull_dobj(s);
+  if (rc) return rc;
   drop_graphs(s);
   build_ops(s);
   CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
@@ -339,6 +373,8 @@ int upload_walls(blaze_sim* s) {
 }
 
 int upload_params(blaze_sim* s) {
+  int rc = pull_dobj(s);
+  if (rc) return rc;
   build_params(s);
   return upload_walls(s);
 }
@@ -446,9 +482,19 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
                      s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->pairs, s->ctl, link, cap, st);
     return 2 + np;
   }
+  int k = 1;
+  if (s->dobj_rot) {
+    launch_rotate_dobj(s->dp, s->rot_ax, s->rot_ay, s->rot_c, s->rot_s, s->n_d, st);
+    ++k;
+  }
+  double* eb = s->hp.energy_calc ? s->d_eb : nullptr;   // allocated when EnergyCalc
   launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
-              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, st);
-  return 1;
+              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, eb, st);
+  if (eb) {
+    launch_energy_reduce(eb, s->n_max, s->ctl, s->d_epart, s->d_tally, st);
+    k += 2;
+  }
+  return k;
 }
 
 int enqueue_step(blaze_sim* s) {
@@ -640,6 +686,7 @@ void free_sim(blaze_sim* s) {
   for (int b = 0; b < 2; ++b) { f(s->ob.pid[b]); f(s->ob.lift[b]); f(s->rs.keys[b]); f(s->rs.vals[b]); }
   f(s->rs.counts); f(s->rs.totals); f(s->cstart); f(s->cend); f(s->nl.idx); f(s->nl.cnt);
   f(s->ctl); f(s->d_rb); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
+  f(s->d_tally); f(s->d_eb); f(s->d_epart);
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   f(s->stage.pos3); f(s->stage.vel3); f(s->stage.avel3); f(s->stage.type); f(s->stage.pid);
@@ -801,6 +848,12 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->ctl, 1));
   CKF(dalloc(&s->d_rb, kGraphSteps));
   CKF(cudaMemset(s->d_rb, 0, sizeof(int) * kGraphSteps));
+  CKF(dalloc(&s->d_tally, 3));
+  CKF(cudaMemset(s->d_tally, 0, sizeof(double) * 3));
+  if (si->EnergyCalc) {
+    CKF(dalloc(&s->d_eb, (size_t)3 * n));
+    CKF(dalloc(&s->d_epart, (size_t)3 * ((n + kEnergyBlock - 1) / kEnergyBlock)));
+  }
   CKF(cudaMallocHost((void**)&s->h_ctl, sizeof(StepCtl)));
   CKF(dalloc(&s->stage.pos3, (size_t)3 * n));
   CKF(dalloc(&s->stage.vel3, (size_t)3 * n));
@@ -896,6 +949,8 @@ int blaze_set_options(blaze_sim* s, const blaze_options* opt) {
 
 int blaze_set_cylinder_rotation(blaze_sim* s, int on) {
   if (!s) return -1;
+  int rc = pull_dobj(s);
+  if (rc) return rc;
   s->cyl_rot = on ? 1 : 0;
   s->hp.cyl_rot = s->cyl_rot;
   CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
@@ -979,9 +1034,52 @@ int blaze_update_dobj(blaze_sim* s, const DOBJ* d, int n_d) {
   if (!s || !d || n_d < 0 || n_d > kMaxDobj) return -1;
   CK(cudaStreamSynchronize(s->stream));
   std::memcpy(s->d, d, sizeof(DOBJ) * n_d);
+  s->dobj_on_device = false;   // the caller's objects replace the turned ones
   build_params(s);
   CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int blaze_set_dobj_rotation(blaze_sim* s, float about_x, float about_y, float rad_per_step,
+                            int on) {
+  if (!s) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  s->dobj_rot = on != 0 && s->n_d > 0;
+  if (s->dobj_rot) s->dobj_on_device = true;
+  s->rot_ax = about_x;
+  s->rot_ay = about_y;
+  // the host's single-precision cosine and sine of the step angle, as the
+  // drum driver evaluates them once per step (Processing_Mills.h:20-21)
+  s->rot_c = std::cos(rad_per_step);
+  s->rot_s = std::sin(rad_per_step);
+  drop_graphs(s);
+  return 0;
+}
+
+int blaze_get_dobj(blaze_sim* s, DOBJ* d, int n_d) {
+  if (!s || !d || n_d < 0) return -1;
+  int rc = pull_dobj(s);
+  if (rc) return rc;
+  std::memcpy(d, s->d, sizeof(DOBJ) * std::min(n_d, s->n_d));
+  return 0;
+}
+
+int blaze_get_energy(blaze_sim* s, double* e3) {
+  if (!s || !e3) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  double t[3];
+  CK(cudaMemcpy(t, s->d_tally, sizeof(t), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 3; ++k) e3[k] = t[k] * 1E-4;
+  return 0;
+}
+
+int blaze_set_energy(blaze_sim* s, const double* raw3) {
+  if (!s) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  double t[3] = {0.0, 0.0, 0.0};
+  if (raw3) for (int k = 0; k < 3; ++k) t[k] = raw3[k];
+  CK(cudaMemcpy(s->d_tally, t, sizeof(t), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -1114,8 +1212,8 @@ int Device_Set_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, flo
 int Device_Set_Tallys(float* h_Tallys) {
   DEF_SIM();
   if (!h_Tallys) return -1;
-  for (int k = 0; k < 3; ++k) s->tallies[k] = h_Tallys[k];
-  return 0;
+  const double t[3] = {h_Tallys[0], h_Tallys[1], h_Tallys[2]};
+  return blaze_set_energy(s, t);
 }
 
 int Device_Get_System_State(float3* h_pos, Quaterion* h_Ornt, float3* h_vel, float3* h_Avel,
@@ -1155,7 +1253,10 @@ int Device_Get_W_Forces(float3* WallForces, float3* WallContact_Point) {
 int Device_Get_Energy(float* Energy) {
   DEF_SIM();
   if (!Energy) return -1;
-  for (int k = 0; k < 3; ++k) Energy[k] = s->tallies[k] * 1E-4f;
+  double e[3];
+  int rc = blaze_get_energy(s, e);
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) Energy[k] = (float)e[k];
   return 0;
 }
 
@@ -1185,8 +1286,7 @@ int Device_Clean(void) {
 
 int Device_Reset_Energy(int num_values) {
   DEF_SIM();
-  if (num_values <= 3)
-    for (int k = 0; k < 3; ++k) s->tallies[k] = 0.0f;
+  if (num_values <= 3) return blaze_set_energy(s, nullptr);
   return 0;
 }
 

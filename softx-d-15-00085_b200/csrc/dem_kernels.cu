@@ -206,10 +206,13 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
 
 // WorldObject_InteractionParticle for spheres (DEM_Kernels_Compute.cuh:254-610):
 // one op per face / plane / cylinder / cap in world-object order.
+// es: when not null, the contact's energy-tally value is added to *es.
 template <bool kSpin>
 __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& op, float3 p,
                                               float r, float3 v, float3 w, const TypeParams& T,
-                                              float3& fw, float3& tw) {
+                                              float3& fw, float3& tw, double* es = nullptr) {
+  float e = 0.0f;
+  float* ep = es ? &e : nullptr;
   if (op.kind == kOpFace || op.kind == kOpPlane) {
     // Collision_Detection_Sphere_Surface / _Plane, Collision_Detection_Spheres.cuh:6-100
     const float3 pt = p - r * op.n;
@@ -222,11 +225,12 @@ __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& 
     }
     Forces F;
     if (P.rotating_wobj && P.cyl_rot)
-      F = law_moving_surface<kSpin>(P, op.n, dis, pt - p, w, T, v, drum_velocity(P, pt));
+      F = law_moving_surface<kSpin>(P, op.n, dis, pt - p, w, T, v, drum_velocity(P, pt), ep);
     else
-      F = law_static_surface(P, v, op.n, dis, pt - p, w, T);
+      F = law_static_surface(P, v, op.n, dis, pt - p, w, T, ep);
     fw = fw + F.trans;
     if (P.rotation) tw = tw + F.torque;
+    if (es) *es += (double)e;
   } else if (op.kind == kOpCylinder) {
     // Collision_Detection_Sphere_Cylinder, Collision_Detection_Spheres.cuh:234-265
     const float3 pv = vmul(p, op.axis) - op.cbot;
@@ -238,11 +242,12 @@ __device__ __forceinline__ void apply_wall_op(const SimParams& P, const WallOp& 
     const float dis = fabsf(pd - op.radius);
     Forces F;
     if (P.cyl_rot)
-      F = law_moving_surface<kSpin>(P, nrm, dis, cp - p, w, T, v, drum_velocity(P, cp));
+      F = law_moving_surface<kSpin>(P, nrm, dis, cp - p, w, T, v, drum_velocity(P, cp), ep);
     else
-      F = law_static_surface(P, v, nrm, dis, cp - p, w, T);
+      F = law_static_surface(P, v, nrm, dis, cp - p, w, T, ep);
     fw = F.trans;
     if (P.rotation) tw = tw + F.torque;
+    if (es) *es += (double)e;
   } else {
     // end plates: Collision_Detection_Sphere_Plane + Collision_Response_EndPlate_Particle
     const float3 pt = p - r * op.n;
@@ -303,11 +308,14 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 #ifndef BLAZE_STEP_MIN_BLOCKS
 #define BLAZE_STEP_MIN_BLOCKS 4
 #endif
-template <bool kCapture, bool kSpin>
+// kEnergy: also the energy tallies of the step's contacts, per particle in
+// contact order (particle-particle, volume objects, world objects), into
+// eb[c * n_max + i] in FP64.
+template <bool kCapture, bool kSpin, bool kEnergy>
 __global__ void __launch_bounds__(kThreads, BLAZE_STEP_MIN_BLOCKS)
 k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGrid wg,
        StateBuf in_plain, StateBuf in_sorted, StateBuf out, OrderBuf ob, int n_max,
-       NbrList nl, StepCtl* ctl, StepLink link, ForceCapture cap) {
+       NbrList nl, StepCtl* ctl, StepLink link, ForceCapture cap, double* eb) {
   __shared__ TypeParams sT[kMaxTypes];
   {
     const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
@@ -338,6 +346,8 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   // particle-particle (Kernel_ParticleInteraction_Spheres_NonSymmetry)
   float3 f = P.gravity * ma;
   float3 fl = f3(0.0f, 0.0f, 0.0f);
+  double e_pp = 0.0, e_lift = 0.0, e_surf = 0.0;
+  float ec = 0.0f;
   const int cnt = (int)nl.cnt[i];
   for (int k = 0; k < cnt; ++k) {
     const int j = (int)nl.idx[(size_t)k * nl.stride + i];
@@ -353,9 +363,11 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     const float dis = fabsf(dist - (ra + pb4.w)) + 0.000010f;
     const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
     const Forces F = law_pp<kSpin>(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
-                            pp, va, vb, ma, sT[tb & (kMaxTypes - 1)].mass);
+                            pp, va, vb, ma, sT[tb & (kMaxTypes - 1)].mass,
+                            kEnergy ? &ec : nullptr);
     f = f + F.trans;
     fl = fl + F.torque;
+    if (kEnergy) e_pp += (double)ec;
   }
   const float3 f_pp = f;
   const float3 t_pp = P.rotation ? fl : f3(0.0f, 0.0f, 0.0f);
@@ -380,9 +392,11 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
           float3 vobj = f3(0.0f, 0.0f, 0.0f);
           if (D.attached) vobj = drum_velocity(P, c.cp);
           else if (D.translating) vobj = D.velocity;
-          const Forces F = law_volume<kSpin>(P, c.n, c.dis, c.cp - pa, wa, TA, va, vobj);
+          const Forces F = law_volume<kSpin>(P, c.n, c.dis, c.cp - pa, wa, TA, va, vobj,
+                                             kEnergy ? &ec : nullptr);
           f_l = f_l + F.trans;
           if (P.rotation) t_l = t_l + F.torque;
+          if (kEnergy) e_lift += (double)ec;
           break;
         }
       }
@@ -397,12 +411,21 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     if (in_grid(P, g)) {
       const uint32_t h = grid_hash(P, g);
       const uint32_t o0 = __ldg(wg.off + h), o1 = __ldg(wg.off + h + 1);
-      for (uint32_t q = o0; q < o1; ++q) apply_wall_op<kSpin>(P, ops[__ldg(wg.ops + q)], pa, ra, va, wa, TA, f_w, t_w);
+      for (uint32_t q = o0; q < o1; ++q)
+        apply_wall_op<kSpin>(P, ops[__ldg(wg.ops + q)], pa, ra, va, wa, TA, f_w, t_w,
+                             kEnergy ? &e_surf : nullptr);
     } else {
-      for (int q = 0; q < P.n_ops; ++q) apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+      for (int q = 0; q < P.n_ops; ++q)
+        apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w, kEnergy ? &e_surf : nullptr);
     }
   } else {
-    for (int q = 0; q < P.n_ops; ++q) apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w);
+    for (int q = 0; q < P.n_ops; ++q)
+      apply_wall_op<kSpin>(P, ops[q], pa, ra, va, wa, TA, f_w, t_w, kEnergy ? &e_surf : nullptr);
+  }
+  if (kEnergy) {
+    eb[i] = e_pp;
+    eb[(size_t)n_max + i] = e_lift;
+    eb[2 * (size_t)n_max + i] = e_surf;
   }
   if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
 
@@ -454,6 +477,84 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
       dsts[q][3 * i + 2] = vals[q].z;
     }
   }
+}
+
+// ------------------------------------------------------------ energy tallies
+// Sum of eb over the current particles, category by category, added to
+// tally[3]: per block a fixed tree over its particles, then one block over
+// the block sums in block order, so the result does not depend on timing.
+__global__ void __launch_bounds__(kEnergyBlock)
+k_energy_partial(const double* __restrict__ eb, int n_max, const StepCtl* ctl,
+                 double* __restrict__ part) {
+  __shared__ double sh[3][kEnergyBlock];
+  const int n = ctl->n_cur;
+  const int i = blockIdx.x * kEnergyBlock + threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] = i < n ? eb[(size_t)c * n_max + i] : 0.0;
+  __syncthreads();
+  for (int w = kEnergyBlock / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) part[3 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(kEnergyBlock)
+k_energy_final(const double* __restrict__ part, int nb, double* tally) {
+  __shared__ double sh[3][kEnergyBlock];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nb; b += kEnergyBlock)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[c] += part[3 * b + c];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = kEnergyBlock / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) tally[threadIdx.x] += sh[threadIdx.x][0];
+}
+
+// ------------------------------------------------------- kinematic lifters
+// Rotate_VolObject_Inc (Processing_Mills.h:4-75) on the device: every
+// volume object attached to the drum turns by the step angle about `about`
+// (x, y; z = 0): vertices and centre of mass x' = c x + s y, y' = -s x + c y
+// relative to `about`, then each face's centroid, normal and area from the
+// turned vertices, all in the host function's FP32 operation order; c and s
+// are the host's cosf / sinf of the angle.
+__global__ void k_rotate_dobj(SimParams* P, float about_x, float about_y, float c, float s) {
+  const int d = threadIdx.x;
+  if (d >= P->n_dobj) return;
+  DobjDev& D = P->dobj[d];
+  if (!D.attached) return;
+  const float3 about = f3(about_x, about_y, 0.0f);
+  auto turn = [&](float3 v) {
+    const float3 p = v - about;
+    v.x = c * p.x + s * p.y;
+    v.y = (-s) * p.x + c * p.y;
+    return v + about;
+  };
+  for (int k = 0; k < D.num_vertex; ++k) D.vert[k] = turn(D.vert[k]);
+  for (int j = 0; j < D.num_faces; ++j) {
+    Surface& F = D.faces[j];
+    float3 sum = f3(0.0f, 0.0f, 0.0f);
+    for (int q = 0; q < F.num_vertex && q < 8; ++q) sum = sum + D.vert[F.vertex_Order[q] & 7];
+    F.centroid = (1.0f / (float)F.num_vertex) * sum;
+    const int* o = F.vertex_Order;
+    const float3 v1 = D.vert[o[1] & 7] - D.vert[o[0] & 7];
+    const float3 v2 = D.vert[o[2] & 7] - D.vert[o[1] & 7];
+    const float3 v3 = D.vert[o[3] & 7] - D.vert[o[2] & 7];
+    const float3 v4 = D.vert[o[0] & 7] - D.vert[o[3] & 7];
+    const float3 nrm = cross3(v2, v1);
+    F.normal = nrm / len3(nrm);
+    F.area = 0.500000f * len3(nrm) + 0.500000f * len3(cross3(v3, v4));
+  }
+  D.com = turn(D.com);
 }
 
 // ---------------------------------------------------------------------- kill
@@ -579,18 +680,40 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
                  NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
-                 const ForceCapture* cap, cudaStream_t st) {
+                 const ForceCapture* cap, double* eb, cudaStream_t st) {
   const ForceCapture c = cap ? *cap : ForceCapture{};
   const int g = blocks(n_max);
-#define BLAZE_STEP_ARGS dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl, ctl, link, c
-  if (cap) {
-    if (spin_free) k_step<true, false><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
-    else k_step<true, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+#define BLAZE_STEP_ARGS dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl, ctl, link, c, eb
+#define BLAZE_STEP(C, S, E) k_step<C, S, E><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS)
+  if (eb) {
+    if (cap) {
+      if (spin_free) BLAZE_STEP(true, false, true);
+      else BLAZE_STEP(true, true, true);
+    } else {
+      if (spin_free) BLAZE_STEP(false, false, true);
+      else BLAZE_STEP(false, true, true);
+    }
+  } else if (cap) {
+    if (spin_free) BLAZE_STEP(true, false, false);
+    else BLAZE_STEP(true, true, false);
   } else {
-    if (spin_free) k_step<false, false><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
-    else k_step<false, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS);
+    if (spin_free) BLAZE_STEP(false, false, false);
+    else BLAZE_STEP(false, true, false);
   }
+#undef BLAZE_STEP
 #undef BLAZE_STEP_ARGS
+}
+
+void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, double* part,
+                          double* tally, cudaStream_t st) {
+  const int nb = (n_max + kEnergyBlock - 1) / kEnergyBlock;
+  k_energy_partial<<<nb, kEnergyBlock, 0, st>>>(eb, n_max, ctl, part);
+  k_energy_final<<<1, kEnergyBlock, 0, st>>>(part, nb, tally);
+}
+
+void launch_rotate_dobj(SimParams* dp, float about_x, float about_y, float c, float s, int n_dobj,
+                        cudaStream_t st) {
+  if (n_dobj > 0) k_rotate_dobj<<<1, 32, 0, st>>>(dp, about_x, about_y, c, s);
 }
 
 void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,

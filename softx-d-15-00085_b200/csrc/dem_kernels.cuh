@@ -84,10 +84,22 @@ void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob
 void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
                   const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
                   cudaStream_t st);
+// eb: when not null, the step also writes each particle's energy-tally
+// values (particle-particle, volume objects, world objects; FP64) to
+// eb[c * n_max + i].
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
                  NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
-                 const ForceCapture* cap, cudaStream_t st);
+                 const ForceCapture* cap, double* eb, cudaStream_t st);
+// tally[c] += sum of eb[c * n_max + i] over the current particles, in a fixed
+// order; part holds 3 doubles per block of kEnergyBlock particles.
+constexpr int kEnergyBlock = 256;
+void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, double* part,
+                          double* tally, cudaStream_t st);
+// One step of the drum's turn for the volume objects attached to it
+// (c, s: cosine and sine of the step angle, about: the drum axis).
+void launch_rotate_dobj(SimParams* dp, float about_x, float about_y, float c, float s, int n_dobj,
+                        cudaStream_t st);
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
 

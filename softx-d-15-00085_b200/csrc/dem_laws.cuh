@@ -10,8 +10,14 @@ namespace blaze {
 
 struct Forces { float3 trans, torque; };
 
-// Collision_Response_Particle_Particle, Collision_Response.cuh:374-494
-// (energy tallies excluded).  kSpin = false is the spin-free form used when
+// Energy tallies (SimulationInfo::EnergyCalc): a law given `e` stores there
+// the value the reference adds to its tally for this contact (normal
+// dissipation |Fdiss| |Vn| dt, unless the force was attractive, plus the
+// tangential |Ft| |Vt| dt), in the reference's operation order; the caller
+// sums them.  e == nullptr (the default) computes forces only.
+
+// Collision_Response_Particle_Particle, Collision_Response.cuh:374-494.
+// kSpin = false is the spin-free form used when
 // rotation is off and every angular velocity is exactly zero: then
 // v + cross(0, R) equals v up to the sign of an exact zero, so the forces
 // are the same numbers.
@@ -26,12 +32,15 @@ template <bool kSpin>
 __device__ __forceinline__ Forces law_pp_pre(const SimParams& P, float3 rvel, float3 n, float pen,
                                              float3 ra, float3 rb, float3 wa, float3 wb,
                                              const PP_Parms& pp, float3 va, float3 vb,
-                                             float tan_pre) {
+                                             float tan_pre, float* e = nullptr) {
   Forces F;
   const float3 vn = dot3(rvel, n) * n;
   const float fn = pp.Kn * pen;
   const float3 fdiss = pp.Cn * vn;
   F.trans = fn * n - fdiss;
+  // the non-symmetric path evaluates every contact from both sides: half each
+  float en = 0.0f;
+  if (e && dot3(vn, vn) > 0.0f) en = ((0.50f * len3(fdiss)) * len3(vn)) * P.dt;
   const float3 vcpa = kSpin ? va + cross3(wa, ra) : va;
   const float3 vcpb = kSpin ? vb + cross3(wb, rb) : vb;
   const float3 vcpna = dot3(vcpa, n) * n;
@@ -46,7 +55,9 @@ __device__ __forceinline__ Forces law_pp_pre(const SimParams& P, float3 rvel, fl
     else velf = 1.0f;
     const float tan_f = tan_pre * (mag / velf);
     ft = (-1.0f * tan_f) * (vt / mag);
+    if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
+  if (e) *e = en;
   F.trans = F.trans + ft;
   F.torque = (kSpin && P.rotation) ? cross3(ra, F.trans) : f3(0.0f, 0.0f, 0.0f);
   return F;
@@ -56,22 +67,24 @@ template <bool kSpin>
 __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3 n, float pen,
                                          float3 ra, float3 rb, float3 wa, float3 wb,
                                          const PP_Parms& pp, float3 va, float3 vb, float ma,
-                                         float mb) {
+                                         float mb, float* e = nullptr) {
   return law_pp_pre<kSpin>(P, rvel, n, pen, ra, rb, wa, wb, pp, va, vb,
-                           tangential_prefactor(P, pp, ma, mb));
+                           tangential_prefactor(P, pp, ma, mb), e);
 }
 
 // Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109
 __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 pvel, float3 n,
                                                      float pen, float3 r, float3 w,
-                                                     const TypeParams& T) {
+                                                     const TypeParams& T, float* e = nullptr) {
   Forces F;
   const float3 vn = dot3(pvel, n) * n;
   const float fn = T.s_kn * pen;
   const float3 fdiss = T.s_cn * vn;
   F.trans = fn * n - fdiss;
   const float3 fdir = F.trans / len3(F.trans);
+  float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
+  else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
   float3 vt = pvel - vn;
   if (P.rotation) vt = vt + cross3(w, r);
   float mag = dot3(vt, vt);
@@ -83,7 +96,9 @@ __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 
     else velf = 1.0f;
     const float tan_f = (0.050f * (T.mass / P.dt)) * (T.s_mus * (mag / velf));
     ft = (-1.0f * tan_f) * (vt / mag);
+    if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
+  if (e) *e = en;
   F.trans = F.trans + ft;
   F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
   return F;
@@ -93,7 +108,7 @@ __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 
 template <bool kSpin>
 __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 n, float pen,
                                                      float3 r, float3 w, const TypeParams& T,
-                                                     float3 va, float3 vs) {
+                                                     float3 va, float3 vs, float* e = nullptr) {
   Forces F;
   const float3 rvel = va - vs;
   const float3 vn = dot3(rvel, n) * n;
@@ -101,7 +116,9 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
   const float3 fdiss = T.s_cn * vn;
   F.trans = fn * n - fdiss;
   const float3 fdir = F.trans / len3(F.trans);
+  float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
+  else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
   const float3 vcpa = kSpin ? va + cross3(w, r) : va;
   const float3 vcpna = dot3(vcpa, n) * n;
   const float3 vt = (vcpa - vcpna) - (vs - dot3(vs, n) * n);
@@ -114,7 +131,9 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
     else velf = 1.0f;
     const float tan_f = T.s_muk * (mag / velf);
     ft = (((-1.0f * tan_f) * (vt / mag)) * (T.mass / P.dt)) * 0.050f;
+    if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
+  if (e) *e = en;
   F.trans = F.trans + ft;
   F.torque = P.rotation ? cross3(r, F.trans) : f3(0.0f, 0.0f, 0.0f);
   return F;
@@ -126,7 +145,7 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
 template <bool kSpin>
 __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float pen, float3 r,
                                              float3 w, const TypeParams& T, float3 va,
-                                             float3 vobj) {
+                                             float3 vobj, float* e = nullptr) {
   Forces F;
   const float3 rvel = va - vobj;
   const float3 vn = dot3(rvel, n) * n;
@@ -134,7 +153,9 @@ __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float
   const float3 fdiss = T.d_cn * vn;
   F.trans = fn * n - fdiss;
   const float3 fdir = F.trans / len3(F.trans);
+  float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
+  else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
   const float3 z = f3(0.0f, 0.0f, 0.0f);
   const float3 vcpa = kSpin ? va + cross3(w, r) : va;
   const float3 vcpb = vobj + cross3(z, z);
@@ -148,7 +169,9 @@ __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float
     else velf = 1.0f;
     const float tan_f = (0.050f * (T.mass / P.dt)) * (T.d_muk * (mag / velf));
     ft = (-1.0f * tan_f) * (vt / mag);
+    if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
+  if (e) *e = en;
   F.trans = F.trans + ft;
   F.torque = P.rotation ? cross3(r, F.trans) : z;
   return F;
