@@ -348,13 +348,24 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   float3 fl = f3(0.0f, 0.0f, 0.0f);
   double e_pp = 0.0, e_lift = 0.0, e_surf = 0.0;
   float ec = 0.0f;
+  // contacts first (the slots whose spheres overlap), then the law over
+  // those alone, in slot order: the law's lanes stay busy when neighbour
+  // counts differ inside a warp
   const int cnt = (int)nl.cnt[i];
+  uint32_t cm = 0;
   for (int k = 0; k < cnt; ++k) {
     const int j = (int)nl.idx[(size_t)k * nl.stride + i];
     const float4 pb4 = __ldg(in.pos + j);
     const float3 rel = pa - xyz(pb4);
+    if (len3(rel) - (ra + pb4.w) < 0.0f) cm |= 1u << k;
+  }
+  while (cm) {
+    const int k = __ffs(cm) - 1;
+    cm &= cm - 1u;
+    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
+    const float4 pb4 = __ldg(in.pos + j);
+    const float3 rel = pa - xyz(pb4);
     const float dist = len3(rel);
-    if (!(dist - (ra + pb4.w) < 0.0f)) continue;  // skin candidate not in contact
     const float4 vb4 = __ldg(in.vel + j);
     const float4 wb4 = kSpin ? __ldg(in.angv + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const int tb = __float_as_int(vb4.w);
