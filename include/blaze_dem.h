@@ -137,8 +137,21 @@ int blaze_update_dobj(blaze_sim* s, const DOBJ* d, int n_d);
  * operation order with the host's cosf / sinf of the angle.  on = 0 stops. */
 int blaze_set_dobj_rotation(blaze_sim* s, float about_x, float about_y, float rad_per_step,
                             int on);
-/* The volume objects as they are now (turned ones included). */
+/* Move volume object `index` by its velocity times dt before every step,
+ * after any turn, on the device, as Translate_VolObject does when the
+ * reference's driver translates it (Processing_Mills.h:336-396,
+ * main.cpp:176-180).  on = 0 stops. */
+int blaze_set_dobj_translation(blaze_sim* s, int index, int on);
+/* Turn the world objects marked is_rotating by rad_per_step about the axis
+ * through (about_x, about_y) parallel to z before every step, on the
+ * device, as Rotate_WObject_inc does (Processing_Mills.h:257-334,
+ * main.cpp:151-164): face vertices turned, centroids, normals and areas
+ * recomputed.  Moving walls switch off the per-cell wall lists. */
+int blaze_set_wobj_rotation(blaze_sim* s, float about_x, float about_y, float rad_per_step,
+                            int on);
+/* The volume / world objects as they are now (moved ones included). */
 int blaze_get_dobj(blaze_sim* s, DOBJ* d, int n_d);
+int blaze_get_wobj(blaze_sim* s, WOBJ* w, int n_w);
 /* Energy tallies (SimulationInfo::EnergyCalc): energy dissipated in
  * particle-particle, volume-object and world-object contacts since the
  * last reset, in Device_Get_Energy's units (tally x 1e-4), summed in FP64 in

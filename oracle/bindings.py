@@ -82,6 +82,9 @@ class RefHost:
             lib.refh_open_hatch.argtypes = [C.POINTER(T.WOBJ), C.c_int]
             lib.refh_set_dobj_rotation.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int]
             lib.refh_get_dobj.argtypes = [C.POINTER(T.DOBJ), C.c_int]
+            lib.refh_set_wobj_rotation.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int]
+            lib.refh_set_dobj_translation.argtypes = [C.c_int, C.c_int]
+            lib.refh_get_wobj.argtypes = [C.POINTER(T.WOBJ), C.c_int]
             lib.refh_set_energy.argtypes = [_f]
             lib.refh_get_energy64.argtypes = [C.POINTER(C.c_double)]
             lib.refh_parse.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(RefProject),
@@ -171,6 +174,18 @@ class RefHost:
         driver does (restated in ref_host/refhost_kernels.cpp)."""
         self.lib.refh_set_dobj_rotation(float(about_x), float(about_y), float(rad_per_step),
                                         1 if on else 0)
+
+    def set_wobj_rotation(self, about_x, about_y, rad_per_step, on=True):
+        self.lib.refh_set_wobj_rotation(float(about_x), float(about_y), float(rad_per_step),
+                                        1 if on else 0)
+
+    def set_dobj_translation(self, index, on=True):
+        self.lib.refh_set_dobj_translation(int(index), 1 if on else 0)
+
+    def wobj(self, n_w):
+        w = (T.WOBJ * 8)()
+        self.lib.refh_get_wobj(w, int(n_w))
+        return w
 
     def dobj(self, n_d):
         d = (T.DOBJ * max(1, n_d))()

@@ -58,7 +58,72 @@ struct RefState {
   /* the mill driver's lifter turn before every step (refh_set_dobj_rotation) */
   bool dobj_rot = false;
   float rot_ax = 0.0f, rot_ay = 0.0f, rot_rad = 0.0f;
+  bool wobj_rot = false;
+  float wrot_ax = 0.0f, wrot_ay = 0.0f, wrot_rad = 0.0f;
+  int dobj_tr = -1;
 } S;
+
+/* A volume object's faces from its vertices (Processing_Mills.h:27-58). */
+void dobj_faces(DOBJ& D) {
+  for (int j = 0; j < D.num_faces; ++j) {
+    Surface& F = D.faces[j];
+    float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+    for (int f = 0; f < F.num_vertex; ++f) sum = sum + D.vertex[F.vertex_Order[f]];
+    F.centroid = (1.0f / F.num_vertex) * sum;
+    const float3 v1 = D.vertex[F.vertex_Order[1]] - D.vertex[F.vertex_Order[0]];
+    const float3 v2 = D.vertex[F.vertex_Order[2]] - D.vertex[F.vertex_Order[1]];
+    const float3 v3 = D.vertex[F.vertex_Order[3]] - D.vertex[F.vertex_Order[2]];
+    const float3 v4 = D.vertex[F.vertex_Order[0]] - D.vertex[F.vertex_Order[3]];
+    const float3 n = cross(v2, v1);
+    F.normal = n / length(n);
+    F.area = 0.500000f * length(n) + 0.500000f * length(cross(v3, v4));
+  }
+}
+
+/* Rotate_WObject_inc (Processing_Mills.h:257-334), restated on the
+ * WorldObject array: the rotating objects' vertices turn by wrot_rad about
+ * (wrot_ax, wrot_ay, 0), then every surface's centroid, normal and area. */
+void rotate_wobj_inc() {
+  const float c = std::cos(S.wrot_rad), sn = std::sin(S.wrot_rad);
+  const float3 about = make_float3(S.wrot_ax, S.wrot_ay, 0.0f);
+  for (int k = 0; k < Num_WorldObjects; ++k) {
+    WOBJ& W = WorldObject[k];
+    if (!W.is_rotating) continue;
+    for (int v = 0; v < W.num_vertex; ++v) {
+      const float3 p = W.vertex[v] - about;
+      W.vertex[v].x = c * p.x + sn * p.y;
+      W.vertex[v].y = -sn * p.x + c * p.y;
+      W.vertex[v] = W.vertex[v] + about;
+    }
+    for (int j = 0; j < W.num_surfaces; ++j) {
+      Surface& F = W.surfaces[j];
+      float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+      for (int f = 0; f < F.num_vertex; ++f) sum = sum + W.vertex[F.vertex_Order[f]];
+      F.centroid = (1.0f / F.num_vertex) * sum;
+      const float3 v1 = W.vertex[F.vertex_Order[1]] - W.vertex[F.vertex_Order[0]];
+      const float3 v2 = W.vertex[F.vertex_Order[2]] - W.vertex[F.vertex_Order[1]];
+      const float3 n = cross(v2, v1);
+      F.normal = n / length(n);
+      if (F.num_vertex > 3) {
+        const float3 v3 = W.vertex[F.vertex_Order[3]] - W.vertex[F.vertex_Order[2]];
+        const float3 v4 = W.vertex[F.vertex_Order[0]] - W.vertex[F.vertex_Order[3]];
+        F.area = 0.500000f * length(n) + 0.500000f * length(cross(v3, v4));
+      } else {
+        F.area = 0.500000f * length(n);
+      }
+    }
+  }
+}
+
+/* Translate_VolObject (Processing_Mills.h:336-396), restated: object k moves
+ * by its velocity times dt (main.cpp:176-180). */
+void translate_dobj(int k) {
+  DOBJ& D = DynamicObject[k];
+  const float3 disp = D.velocity * SimParms.InitalDelta_t;
+  for (int v = 0; v < D.num_vertex; ++v) D.vertex[v] += disp;
+  dobj_faces(D);
+  D.COM = D.COM + disp;
+}
 
 /* FP64 sums of the values the kernels add to the three energy tallies, in
  * the same order as the FP32 tallies (one host thread) or any order. */
@@ -325,7 +390,9 @@ static int step_once() {
 
 int refh_step(int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
+    if (S.wobj_rot) rotate_wobj_inc();
     if (S.dobj_rot) rotate_dobj_inc();
+    if (S.dobj_tr >= 0) translate_dobj(S.dobj_tr);
     int rc = step_once();
     if (rc) return rc;
   }
@@ -413,6 +480,21 @@ void refh_set_dobj_rotation(float about_x, float about_y, float rad_per_step, in
   S.rot_ax = about_x;
   S.rot_ay = about_y;
   S.rot_rad = rad_per_step;
+}
+
+void refh_set_wobj_rotation(float about_x, float about_y, float rad_per_step, int on) {
+  S.wobj_rot = on != 0;
+  S.wrot_ax = about_x;
+  S.wrot_ay = about_y;
+  S.wrot_rad = rad_per_step;
+}
+
+void refh_set_dobj_translation(int index, int on) { S.dobj_tr = on ? index : -1; }
+
+int refh_get_wobj(WOBJ* w, int n_w) {
+  if (n_w < 0 || n_w > 8) return 1;
+  std::memcpy(w, WorldObject, sizeof(WOBJ) * n_w);
+  return 0;
 }
 
 int refh_get_dobj(DOBJ* d, int n_d) {

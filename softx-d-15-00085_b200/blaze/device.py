@@ -56,6 +56,9 @@ def load():
     lib.blaze_set_cylinder_rotation.argtypes = [C.c_void_p, C.c_int]
     lib.blaze_set_dobj_rotation.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int]
     lib.blaze_get_dobj.argtypes = [C.c_void_p, C.POINTER(T.DOBJ), C.c_int]
+    lib.blaze_set_dobj_translation.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.blaze_set_wobj_rotation.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int]
+    lib.blaze_get_wobj.argtypes = [C.c_void_p, C.POINTER(T.WOBJ), C.c_int]
     lib.blaze_get_energy.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.blaze_set_energy.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.blaze_set_state.argtypes = [C.c_void_p, _f, _f, _f, _u, _i]
@@ -133,6 +136,7 @@ class Simulation:
         self.lib = lib
         self.n = sim_info.Num_Particles
         self.n_d = int(n_d)
+        self.n_w = int(n_w)
         self.poly = sim_info.particle_type == 1
         self.opts = default_options(**options)
         h = C.c_void_p()
@@ -169,6 +173,24 @@ class Simulation:
         _check(self.lib.blaze_set_dobj_rotation(self.h, float(about_x), float(about_y),
                                                 float(rad_per_step), 1 if on else 0),
                "blaze_set_dobj_rotation")
+
+    def set_dobj_translation(self, index, on=True):
+        """Move volume object `index` by its velocity times dt before every
+        step, on the device (the driver's Translate_VolObject)."""
+        _check(self.lib.blaze_set_dobj_translation(self.h, int(index), 1 if on else 0),
+               "blaze_set_dobj_translation")
+
+    def set_wobj_rotation(self, about_x, about_y, rad_per_step, on=True):
+        """Turn the world objects marked is_rotating before every step, on the
+        device (the driver's Rotate_WObject_inc)."""
+        _check(self.lib.blaze_set_wobj_rotation(self.h, float(about_x), float(about_y),
+                                                float(rad_per_step), 1 if on else 0),
+               "blaze_set_wobj_rotation")
+
+    def wobj(self):
+        w = (T.WOBJ * 8)()
+        _check(self.lib.blaze_get_wobj(self.h, w, self.n_w), "blaze_get_wobj")
+        return w
 
     def dobj(self):
         d = (T.DOBJ * max(1, self.n_d))()

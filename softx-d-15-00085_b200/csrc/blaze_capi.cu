@@ -87,11 +87,17 @@ struct blaze_sim {
   double* d_eb = nullptr;
   double* d_epart = nullptr;
   float fc = 0.0f;
-  // volume objects turned with the drum on the device every step
-  // (blaze_set_dobj_rotation); the device copy is then the current one
+  // the mill driver's per-step moves on the device (blaze_set_dobj_rotation,
+  // blaze_set_dobj_translation, blaze_set_wobj_rotation); the device copies
+  // of the objects are then the current ones
   bool dobj_rot = false;
+  int dobj_tr = -1;
   bool dobj_on_device = false;
   float rot_ax = 0.0f, rot_ay = 0.0f, rot_c = 1.0f, rot_s = 0.0f;
+  bool wobj_rot = false;
+  bool wobj_on_device = false;
+  uint32_t wrot_mask = 0;
+  float wrot_ax = 0.0f, wrot_ay = 0.0f, wrot_c = 1.0f, wrot_s = 0.0f;
   // optional per-phase event timing (non-graph stepping only)
   bool profile = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -190,6 +196,7 @@ void build_ops(blaze_sim* s) {
         WallOp op;
         std::memset(&op, 0, sizeof(op));
         op.kind = S.area == -1.0f ? kOpPlane : kOpFace;
+        op.wobj = k;
         op.nv = std::min(std::max(S.num_vertex, 0), 8);
         op.area = S.area;
         op.tol = S.Tol;
@@ -203,6 +210,7 @@ void build_ops(blaze_sim* s) {
       WallOp op;
       std::memset(&op, 0, sizeof(op));
       op.kind = kOpCylinder;
+      op.wobj = k;
       op.radius = cg.radius;
       op.axis = cg.AXIS;
       op.cbot = cg.center_bot_cap;
@@ -340,8 +348,37 @@ int pull_dobj(blaze_sim* s) {
   return 0;
 }
 
+// With the world objects turned on the device, copy the wall program back
+// and write its faces into the host's WOBJ mirror (vertices through
+// vertex_Order, normal, centroid, area), walking the objects in build_ops'
+// order.
+int pull_wobj(blaze_sim* s) {
+  if (!s->wobj_on_device || s->ops.empty()) return 0;
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(s->ops.data(), s->d_ops, sizeof(WallOp) * s->ops.size(), cudaMemcpyDeviceToHost));
+  size_t q = 0;
+  for (int k = 0; k < s->num_wobj && k < s->n_w; ++k) {
+    WOBJ& W = s->w[k];
+    if (W.surface_type == plane) {
+      for (int f = 0; f < W.num_surfaces && f < 16 && q < s->ops.size(); ++f, ++q) {
+        const WallOp& op = s->ops[q];
+        if (!W.is_rotating) continue;
+        Surface& S = W.surfaces[f];
+        for (int v = 0; v < op.nv; ++v) W.vertex[S.vertex_Order[v] & 15] = op.v[v];
+        S.normal = op.n;
+        S.centroid = op.c;
+        S.area = op.area;
+      }
+    } else if (W.surface_type == cylinder) {
+      q += 1 + (W.cyl_geo.has_top_cap ? 1 : 0) + (W.cyl_geo.has_bot_cap ? 1 : 0);
+    }
+  }
+  return 0;
+}
+
 int upload_walls(blaze_sim* s) {
   int rc = pull_dobj(s);
+  if (!rc) rc = pull_wobj(s);
   if (rc) return rc;
   drop_graphs(s);
   build_ops(s);
@@ -374,6 +411,7 @@ int upload_walls(blaze_sim* s) {
 
 int upload_params(blaze_sim* s) {
   int rc = pull_dobj(s);
+  if (!rc) rc = pull_wobj(s);
   if (rc) return rc;
   build_params(s);
   return upload_walls(s);
@@ -483,8 +521,14 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
     return 2 + np;
   }
   int k = 1;
-  if (s->dobj_rot) {
-    launch_rotate_dobj(s->dp, s->rot_ax, s->rot_ay, s->rot_c, s->rot_s, s->n_d, st);
+  if (s->dobj_rot || s->dobj_tr >= 0) {
+    launch_move_dobj(s->dp, s->dobj_rot ? 1 : 0, s->rot_ax, s->rot_ay, s->rot_c, s->rot_s,
+                     s->dobj_tr, s->n_d, st);
+    ++k;
+  }
+  if (s->wobj_rot) {
+    launch_rotate_wobj(s->d_ops, (int)s->ops.size(), s->wrot_mask, s->wrot_ax, s->wrot_ay,
+                       s->wrot_c, s->wrot_s, st);
     ++k;
   }
   double* eb = s->hp.energy_calc ? s->d_eb : nullptr;   // allocated when EnergyCalc
@@ -1025,6 +1069,7 @@ int blaze_update_wobj(blaze_sim* s, const WOBJ* w, int n_w) {
   if (!s || !w || n_w < 0 || n_w > 8) return -1;
   CK(cudaStreamSynchronize(s->stream));
   std::memcpy(s->w, w, sizeof(WOBJ) * n_w);
+  s->wobj_on_device = false;   // the caller's objects replace the turned ones
   // moving geometry: the per-cell culling lists would go stale
   s->walls_static = false;
   return upload_params(s);
@@ -1054,6 +1099,43 @@ int blaze_set_dobj_rotation(blaze_sim* s, float about_x, float about_y, float ra
   s->rot_c = std::cos(rad_per_step);
   s->rot_s = std::sin(rad_per_step);
   drop_graphs(s);
+  return 0;
+}
+
+int blaze_set_dobj_translation(blaze_sim* s, int index, int on) {
+  if (!s || (on && (index < 0 || index >= s->n_d))) return -1;
+  CK(cudaStreamSynchronize(s->stream));
+  s->dobj_tr = on ? index : -1;
+  if (on) s->dobj_on_device = true;
+  drop_graphs(s);
+  return 0;
+}
+
+int blaze_set_wobj_rotation(blaze_sim* s, float about_x, float about_y, float rad_per_step,
+                            int on) {
+  if (!s) return -1;
+  int rc = pull_wobj(s);
+  if (rc) return rc;
+  s->wrot_mask = 0;
+  for (int k = 0; k < s->n_w && k < 32; ++k)
+    if (s->w[k].is_rotating) s->wrot_mask |= 1u << k;
+  s->wobj_rot = on != 0 && s->wrot_mask != 0;
+  s->wrot_ax = about_x;
+  s->wrot_ay = about_y;
+  s->wrot_c = std::cos(rad_per_step);   // the host's single-precision cosine and sine
+  s->wrot_s = std::sin(rad_per_step);   // (Processing_Mills.h:269-270)
+  // moving walls: no per-cell candidate lists
+  if (s->wobj_rot) s->walls_static = false;
+  rc = upload_walls(s);
+  if (s->wobj_rot) s->wobj_on_device = true;
+  return rc;
+}
+
+int blaze_get_wobj(blaze_sim* s, WOBJ* w, int n_w) {
+  if (!s || !w || n_w < 0) return -1;
+  int rc = pull_wobj(s);
+  if (rc) return rc;
+  std::memcpy(w, s->w, sizeof(WOBJ) * std::min(n_w, s->n_w));
   return 0;
 }
 

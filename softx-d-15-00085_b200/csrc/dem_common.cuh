@@ -53,6 +53,7 @@ enum WallOpKind : int {
 
 struct WallOp {
   int kind;
+  int wobj;      // the world object it came from
   int nv;        // polygon vertex count
   float area;
   float tol;

@@ -531,26 +531,22 @@ k_energy_final(const double* __restrict__ part, int nb, double* tally) {
   if (threadIdx.x < 3) tally[threadIdx.x] += sh[threadIdx.x][0];
 }
 
-// ------------------------------------------------------- kinematic lifters
-// Rotate_VolObject_Inc (Processing_Mills.h:4-75) on the device: every
-// volume object attached to the drum turns by the step angle about `about`
-// (x, y; z = 0): vertices and centre of mass x' = c x + s y, y' = -s x + c y
-// relative to `about`, then each face's centroid, normal and area from the
-// turned vertices, all in the host function's FP32 operation order; c and s
-// are the host's cosf / sinf of the angle.
-__global__ void k_rotate_dobj(SimParams* P, float about_x, float about_y, float c, float s) {
-  const int d = threadIdx.x;
-  if (d >= P->n_dobj) return;
-  DobjDev& D = P->dobj[d];
-  if (!D.attached) return;
-  const float3 about = f3(about_x, about_y, 0.0f);
-  auto turn = [&](float3 v) {
-    const float3 p = v - about;
-    v.x = c * p.x + s * p.y;
-    v.y = (-s) * p.x + c * p.y;
-    return v + about;
-  };
-  for (int k = 0; k < D.num_vertex; ++k) D.vert[k] = turn(D.vert[k]);
+// ------------------------------------------------------- kinematic world
+// The mill driver's per-step moves of volume and world objects
+// (Processing_Mills.h), on the device, in the host functions' FP32 operation
+// order; c and s are the host's cosf / sinf of the step angle.
+
+// x' = c x + s y, y' = -s x + c y about `about` (z unchanged).
+__device__ __forceinline__ float3 turn_about(float3 v, float3 about, float c, float s) {
+  const float3 p = v - about;
+  v.x = c * p.x + s * p.y;
+  v.y = (-s) * p.x + c * p.y;
+  return v + about;
+}
+
+// A volume object's faces from its vertices: centroid, normal cross(V2, V1)
+// normalised, area of the quad (Processing_Mills.h:27-58).
+__device__ void dobj_faces(DobjDev& D) {
   for (int j = 0; j < D.num_faces; ++j) {
     Surface& F = D.faces[j];
     float3 sum = f3(0.0f, 0.0f, 0.0f);
@@ -565,7 +561,61 @@ __global__ void k_rotate_dobj(SimParams* P, float about_x, float about_y, float 
     F.normal = nrm / len3(nrm);
     F.area = 0.500000f * len3(nrm) + 0.500000f * len3(cross3(v3, v4));
   }
-  D.com = turn(D.com);
+}
+
+// Rotate_VolObject_Inc (Processing_Mills.h:4-75): every volume object
+// attached to the drum turns about `about` (x, y; z = 0): vertices and
+// centre of mass, then its faces.  Translate_VolObject
+// (Processing_Mills.h:336-396), after the turn: object `tr` (or none, -1)
+// moves by its velocity times dt.
+__global__ void k_move_dobj(SimParams* P, int turn, float about_x, float about_y, float c,
+                            float s, int tr) {
+  const int d = threadIdx.x;
+  if (d >= P->n_dobj) return;
+  DobjDev& D = P->dobj[d];
+  if (turn && D.attached) {
+    const float3 about = f3(about_x, about_y, 0.0f);
+    for (int k = 0; k < D.num_vertex; ++k) D.vert[k] = turn_about(D.vert[k], about, c, s);
+    dobj_faces(D);
+    D.com = turn_about(D.com, about, c, s);
+  }
+  if (d == tr) {
+    const float3 disp = D.velocity * P->dt;
+    for (int k = 0; k < D.num_vertex; ++k) D.vert[k] = D.vert[k] + disp;
+    dobj_faces(D);
+    D.com = D.com + disp;
+  }
+}
+
+// Rotate_WObject_inc (Processing_Mills.h:257-334) on the wall program: each
+// face (or plane) of a rotating world object (bit `wobj` of rot_mask) has
+// its vertices turned, then centroid, normal cross(V2, V1) normalised and
+// area (quad: both triangles; triangle: one); every face copy of a shared
+// vertex turns the same number to the same result.
+__global__ void k_rotate_wobj(WallOp* ops, int n_ops, uint32_t rot_mask, float about_x,
+                              float about_y, float c, float s) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n_ops) return;
+  WallOp& op = ops[q];
+  if (op.kind != kOpFace && op.kind != kOpPlane) return;
+  if (op.wobj < 0 || op.wobj > 31 || !((rot_mask >> op.wobj) & 1u)) return;
+  const float3 about = f3(about_x, about_y, 0.0f);
+  for (int k = 0; k < op.nv; ++k) op.v[k] = turn_about(op.v[k], about, c, s);
+  float3 sum = f3(0.0f, 0.0f, 0.0f);
+  for (int k = 0; k < op.nv; ++k) sum = sum + op.v[k];
+  op.c = (1.0f / (float)op.nv) * sum;
+  const float3 v1 = op.v[1] - op.v[0];
+  const float3 v2 = op.v[2] - op.v[1];
+  const float3 nrm = cross3(v2, v1);
+  op.n = nrm / len3(nrm);
+  if (op.nv > 3) {
+    const float3 v3 = op.v[3] - op.v[2];
+    const float3 v4 = op.v[0] - op.v[3];
+    op.area = 0.500000f * len3(nrm) + 0.500000f * len3(cross3(v3, v4));
+  } else {
+    op.area = 0.500000f * len3(nrm);
+  }
+  op.kind = op.area == -1.0f ? kOpPlane : kOpFace;
 }
 
 // ---------------------------------------------------------------------- kill
@@ -722,9 +772,16 @@ void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, doubl
   k_energy_final<<<1, kEnergyBlock, 0, st>>>(part, nb, tally);
 }
 
-void launch_rotate_dobj(SimParams* dp, float about_x, float about_y, float c, float s, int n_dobj,
-                        cudaStream_t st) {
-  if (n_dobj > 0) k_rotate_dobj<<<1, 32, 0, st>>>(dp, about_x, about_y, c, s);
+void launch_move_dobj(SimParams* dp, int turn, float about_x, float about_y, float c, float s,
+                      int translate, int n_dobj, cudaStream_t st) {
+  if (n_dobj > 0) k_move_dobj<<<1, 32, 0, st>>>(dp, turn, about_x, about_y, c, s, translate);
+}
+
+void launch_rotate_wobj(WallOp* ops, int n_ops, uint32_t rot_mask, float about_x, float about_y,
+                        float c, float s, cudaStream_t st) {
+  if (n_ops > 0)
+    k_rotate_wobj<<<(n_ops + 127) / 128, 128, 0, st>>>(ops, n_ops, rot_mask, about_x, about_y, c,
+                                                        s);
 }
 
 void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, bool has_avel,

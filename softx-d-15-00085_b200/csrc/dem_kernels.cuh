@@ -96,10 +96,16 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
 constexpr int kEnergyBlock = 256;
 void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, double* part,
                           double* tally, cudaStream_t st);
-// One step of the drum's turn for the volume objects attached to it
-// (c, s: cosine and sine of the step angle, about: the drum axis).
-void launch_rotate_dobj(SimParams* dp, float about_x, float about_y, float c, float s, int n_dobj,
-                        cudaStream_t st);
+// One step of the mill driver's moves of volume objects: with `turn`, the
+// drum's turn of the attached ones (c, s: cosine and sine of the step
+// angle, about: the drum axis); then object `translate` (-1: none) moves by
+// its velocity times dt.
+void launch_move_dobj(SimParams* dp, int turn, float about_x, float about_y, float c, float s,
+                      int translate, int n_dobj, cudaStream_t st);
+// One step of the turn of the rotating world objects (bit k of rot_mask:
+// world object k) on the wall program.
+void launch_rotate_wobj(WallOp* ops, int n_ops, uint32_t rot_mask, float about_x, float about_y,
+                        float c, float s, cudaStream_t st);
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
 
