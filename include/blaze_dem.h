@@ -155,8 +155,8 @@ int blaze_get_wobj(blaze_sim* s, WOBJ* w, int n_w);
 /* Energy tallies (SimulationInfo::EnergyCalc): energy dissipated in
  * particle-particle, volume-object and world-object contacts since the
  * last reset, in Device_Get_Energy's units (tally x 1e-4), summed in FP64 in
- * a fixed order (the reference adds FP32 values with float atomics).
- * Spheres only: polyhedral runs leave them at zero. */
+ * a fixed order (the reference adds FP32 values with float atomics);
+ * spheres and polyhedra. */
 int blaze_get_energy(blaze_sim* s, double* e3);
 /* Set the raw tallies (Device_Set_Tallys); NULL zeroes them. */
 int blaze_set_energy(blaze_sim* s, const double* raw3);

@@ -511,15 +511,6 @@ cudaEvent_t prof_event(blaze_sim* s, int phase) {
 // number of launches.
 int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
   const ForceCapture* cap = s->opt.capture_forces ? &s->cap : nullptr;
-  if (s->poly) {
-    launch_poly_geom(s->d_shapes, s->geom, s->S[s->cur], s->S[2], s->ob, s->n_max,
-                     s->si.Rotation ? 1 : 0, s->ctl, link.rebuilt, st);
-    const int np = launch_poly_pairs(s->dp, s->d_shapes, s->geom, s->S[s->cur], s->S[2],
-                                     s->n_max, s->nl, s->ctl, link.rebuilt, s->pairs, st);
-    launch_poly_step(s->dp, s->d_shapes, s->geom, s->d_ops, s->S[s->cur], s->S[2],
-                     s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->pairs, s->ctl, link, cap, st);
-    return 2 + np;
-  }
   int k = 1;
   if (s->dobj_rot || s->dobj_tr >= 0) {
     launch_move_dobj(s->dp, s->dobj_rot ? 1 : 0, s->rot_ax, s->rot_ay, s->rot_c, s->rot_s,
@@ -532,8 +523,20 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
     ++k;
   }
   double* eb = s->hp.energy_calc ? s->d_eb : nullptr;   // allocated when EnergyCalc
-  launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
-              s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, eb, st);
+  if (s->poly) {
+    launch_poly_geom(s->d_shapes, s->geom, s->S[s->cur], s->S[2], s->ob, s->n_max,
+                     s->si.Rotation ? 1 : 0, s->ctl, link.rebuilt, st);
+    const int np = launch_poly_pairs(s->dp, s->d_shapes, s->geom, s->S[s->cur], s->S[2],
+                                     s->n_max, s->nl, s->ctl, link.rebuilt, s->pairs, st);
+    launch_poly_step(s->dp, s->d_shapes, s->geom, s->d_ops, s->S[s->cur], s->S[2],
+                     s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->pairs, s->ctl, link, cap, eb,
+                     st);
+    k += 1 + np;
+  } else {
+    launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
+                s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, eb,
+                st);
+  }
   if (eb) {
     launch_energy_reduce(eb, s->n_max, s->ctl, s->d_epart, s->d_tally, st);
     k += 2;

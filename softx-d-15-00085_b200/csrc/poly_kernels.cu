@@ -746,7 +746,7 @@ __device__ Hit dobject_edges(const DobjDev& D, const PolyRef& b, float3 relpos, 
 // contact type (1 vertex-face, 2 edge-edge, 0 none) is kept per particle.
 __device__ void poly_dobjects(const SimParams& P, const PolyRef& A, const TypeParams& T,
                               float3 va, float3 wa, int& colltype, float3& fl, float3& tl,
-                              uint32_t& st) {
+                              uint32_t& st, double* el = nullptr) {
   bool outer = P.dobj[0].translating || !P.is_mill || P.rotating_wobj;
   if (!outer) outer = len3(f3(A.pos.x, A.pos.y, 0.0f) - P.cent) > (P.dobj_cyl_bound_r - 2.0f * T.radius);
   if (!outer) return;
@@ -769,9 +769,12 @@ __device__ void poly_dobjects(const SimParams& P, const PolyRef& A, const TypePa
     float3 vobj = f3(0.0f, 0.0f, 0.0f);
     if (D.attached) vobj = drum_velocity(P, h.cp);
     else if (D.translating) vobj = D.velocity;
-    const Forces F = law_volume<true>(P, h.n, h.dis, h.cp - A.pos, wa, T, va, vobj);
+    float e = 0.0f;
+    const Forces F = law_volume<true>(P, h.n, h.dis, h.cp - A.pos, wa, T, va, vobj,
+                                      el ? &e : nullptr);
     fl = fl + F.trans;
     if (P.rotation) tl = tl + F.torque;
+    if (el) *el += (double)e;
     break;
   }
 }
@@ -888,8 +891,11 @@ __device__ Hit vertices_plane(const PolyRef& a, float3 n, float3 c) {
 // assigns nothing for an infinite plane (it has no polyhedron method), so a
 // plane applies the record the previous world-object step left behind.
 __device__ void poly_walls(const SimParams& P, const WallOp* __restrict__ ops, const PolyRef& A,
-                           const TypeParams& T, float3 va, float3 wa, float3& fw, float3& tw) {
+                           const TypeParams& T, float3 va, float3 wa, float3& fw, float3& tw,
+                           double* es = nullptr) {
   Hit last = no_hit();
+  float e = 0.0f;
+  float* ep = es ? &e : nullptr;
   for (int q = 0; q < P.n_ops; ++q) {
     const WallOp& op = ops[q];
     if (op.kind == kOpFace || op.kind == kOpPlane) {
@@ -898,22 +904,24 @@ __device__ void poly_walls(const SimParams& P, const WallOp* __restrict__ ops, c
       Forces F;
       if (P.rotating_wobj && P.cyl_rot)
         F = law_moving_surface<true>(P, last.n, last.dis, last.cp - A.pos, wa, T, va,
-                                     drum_velocity(P, last.cp));
+                                     drum_velocity(P, last.cp), ep);
       else
-        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T);
+        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T, ep);
       fw = fw + F.trans;
       if (P.rotation && last.cls != kFaceFace) tw = tw + F.torque;
+      if (es) *es += (double)e;
     } else if (op.kind == kOpCylinder) {
       last = poly_cylinder(op, A, T.radius);
       if (!last.hit) continue;
       Forces F;
       if (P.cyl_rot)
         F = law_moving_surface<true>(P, last.n, last.dis, last.cp - A.pos, wa, T, va,
-                                     drum_velocity(P, last.cp));
+                                     drum_velocity(P, last.cp), ep);
       else
-        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T);
+        F = law_static_surface(P, va, last.n, last.dis, last.cp - A.pos, wa, T, ep);
       fw = F.trans;
       if (P.rotation && last.cls != kFaceFace) tw = tw + F.torque;
+      if (es) *es += (double)e;
     } else {  // end plates (Collision_Response_EndPlate_Particle: no torque)
       last = vertices_plane(A, op.n, op.c);
       if (!last.hit) continue;
@@ -1195,12 +1203,12 @@ k_poly_ee(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes
 // reference's depth limits; VolumeObject_InteractionParticle,
 // WorldObject_InteractionParticle and Integrate_Euler_NonSymmetry with the
 // quaternion update.  One thread per particle.
-template <bool kCapture>
+template <bool kCapture, bool kEnergy>
 __global__ void __launch_bounds__(kThreads)
 k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shapes, PolyGeom g,
             const WallOp* __restrict__ ops, StateBuf in_plain, StateBuf in_sorted, StateBuf out,
             OrderBuf ob, int n_max, NbrList nl, PolyPairs pp, StepCtl* ctl, StepLink link,
-            ForceCapture cap) {
+            ForceCapture cap, double* eb) {
   __shared__ TypeParams sT[kMaxTypes];
   {
     const int words = (int)(sizeof(TypeParams) * kMaxTypes / 4);
@@ -1234,6 +1242,8 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
   // particle-particle
   float3 f = P.gravity * ma;
   float3 fl = f3(0.0f, 0.0f, 0.0f);
+  double e_pp = 0.0, e_lift = 0.0, e_surf = 0.0;
+  float ec = 0.0f;
   const int cnt = (int)nl.cnt[i];
   for (int k = 0; k < cnt; ++k) {
     const size_t slot = (size_t)k * nl.stride + i;
@@ -1263,9 +1273,10 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
     }
     const PP_Parms& ppar = TA.pp[tb < kMaxPP ? tb : 0];
     const Forces F = law_pp<true>(P, rvel, n, dis, cp - pa, cp - pb, wa, wb, ppar, va, vb, ma,
-                                  sT[tb & (kMaxTypes - 1)].mass);
+                                  sT[tb & (kMaxTypes - 1)].mass, kEnergy ? &ec : nullptr);
     f = f + F.trans;
     fl = fl + F.torque;
+    if (kEnergy) e_pp += (double)ec;
   }
   const float3 f_pp = f;
   const float3 t_pp = P.rotation ? fl : f3(0.0f, 0.0f, 0.0f);
@@ -1275,14 +1286,19 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
   if (P.n_dobj > 0) {
     int* lift = (ctl->epoch & 1) ? ob.lift[1] : ob.lift[0];
     int colltype = 0;
-    poly_dobjects(P, A, TA, va, wa, colltype, f_l, t_l, st);
+    poly_dobjects(P, A, TA, va, wa, colltype, f_l, t_l, st, kEnergy ? &e_lift : nullptr);
     lift[i] = colltype;
   }
 
   // world objects
   float3 f_w = f3(0.0f, 0.0f, 0.0f), t_w = f3(0.0f, 0.0f, 0.0f);
-  poly_walls(P, ops, A, TA, va, wa, f_w, t_w);
+  poly_walls(P, ops, A, TA, va, wa, f_w, t_w, kEnergy ? &e_surf : nullptr);
   if (!P.rotation) t_w = f3(0.0f, 0.0f, 0.0f);
+  if (kEnergy) {
+    eb[i] = e_pp;
+    eb[(size_t)n_max + i] = e_lift;
+    eb[2 * (size_t)n_max + i] = e_surf;
+  }
 
   // Integrate_Euler_NonSymmetry (Integration.cuh:6-184), polyhedra
   float3 acc = f_w + f_pp;
@@ -1365,15 +1381,20 @@ void launch_poly_step(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const WallOp* ops, const StateBuf& in_plain, const StateBuf& in_sorted,
                       const StateBuf& out, const OrderBuf& ob, int n_max, NbrList nl,
                       PolyPairs pp, StepCtl* ctl, StepLink link, const ForceCapture* cap,
-                      cudaStream_t st) {
+                      double* eb, cudaStream_t st) {
   const ForceCapture c = cap ? *cap : ForceCapture{};
   const int gr = blocks_for(n_max);
-  if (cap)
-    k_poly_step<true><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
-                                               n_max, nl, pp, ctl, link, c);
-  else
-    k_poly_step<false><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob,
-                                                n_max, nl, pp, ctl, link, c);
+#define POLY_STEP(C, E)                                                                      \
+  k_poly_step<C, E><<<gr, kThreads, 0, st>>>(dp, shapes, g, ops, in_plain, in_sorted, out, ob, \
+                                             n_max, nl, pp, ctl, link, c, eb)
+  if (eb) {
+    if (cap) POLY_STEP(true, true);
+    else POLY_STEP(false, true);
+  } else {
+    if (cap) POLY_STEP(true, false);
+    else POLY_STEP(false, false);
+  }
+#undef POLY_STEP
 }
 
 }  // namespace blaze

@@ -77,10 +77,12 @@ int launch_poly_pairs(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const StateBuf& in_plain, const StateBuf& in_sorted, int n_max, NbrList nl,
                       StepCtl* ctl, const int* rebuilt, PolyPairs pp, cudaStream_t st);
 
+// eb: when not null, also the energy-tally values per particle (as
+// launch_step).
 void launch_poly_step(const SimParams* dp, const PolyShape* shapes, PolyGeom g,
                       const WallOp* ops, const StateBuf& in_plain, const StateBuf& in_sorted,
                       const StateBuf& out, const OrderBuf& ob, int n_max, NbrList nl,
                       PolyPairs pp, StepCtl* ctl, StepLink link, const ForceCapture* cap,
-                      cudaStream_t st);
+                      double* eb, cudaStream_t st);
 
 }  // namespace blaze
