@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--no-poly", action="store_true",
                     help="skip the convex-polyhedra leg (100,000 polyhedra in a box)")
     ap.add_argument("--poly-steps", type=int, default=500)
+    ap.add_argument("--no-mill", action="store_true", help="skip the ball-mill leg")
+    ap.add_argument("--mill-steps", type=int, default=5000)
+    ap.add_argument("--mill-only", action="store_true",
+                    help="print only the ball-mill leg's JSON line")
     ap.add_argument("--poly-only", action="store_true",
                     help="run only the convex-polyhedra leg and print its object")
     return ap.parse_args()
@@ -397,6 +401,67 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
     return out
 
 
+def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=True):
+    """Ball mill, the sphere charge of the mill configuration on the
+    reference path: drum r = 50 cm, L = 30 cm with end plates, 30 rpm, eight
+    4 x 4 cm lifters turned with the drum on the device every step
+    (blaze_set_dobj_rotation), n steel spheres r ~ U[0.3, 0.6] cm in 6
+    radius bins (the drum holds about 1.5e5 at lattice fill; the
+    configuration's 2,000,000 such spheres would take three times the
+    drum's volume), linear law kn = 1e6, e = 0.4, mu = 0.6, dt = 2e-6 s,
+    rotation on, power tallies on (FP64).  GPU: CUDA graphs, `skin` Verlet
+    list, `steps` steps from the packed charge after `warmup`; the
+    dissipated power over the timed steps is reported.  CPU: the
+    reference's kernels (oracle/_ref) with the lifter turn, all host
+    threads, reference mode, a bounded sample."""
+    import torch
+    from blaze import device, synth
+    with tempfile.TemporaryDirectory() as d:
+        P, st = synth.mill_project(d, n=n)
+    R = float(P.wobj[0].cyl_geo.radius)
+    rad = float(P.mill.RadPerStep)
+    sim = device.Simulation(P, skin=skin, use_graph=1)
+    sim.set_cylinder_rotation(True)
+    sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    sim.set_dobj_rotation(R, R, rad)
+    sim.step(max(3, warmup))
+    status = sim.sync()
+    sim.reset_energy()
+    stream = torch.cuda.ExternalStream(sim.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = sim.num_rebuilds()
+    a.record(stream)
+    sim.step(steps)
+    b.record(stream)
+    fixed = sim.last_launches()
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = sim.num_rebuilds() - rb0
+    status |= sim.sync()
+    launches = fixed + rebuilds * sim.rebuild_kernels()
+    e = sim.energy()
+    T = steps * float(np.float32(P.sim_info.InitalDelta_t))
+    sim.close()
+    out = {"workload": "ball mill: drum r 50 cm L 30 cm, 30 rpm, 8 lifters turned on the device, "
+                       "%d steel spheres r 0.3-0.6 cm (6 bins), kn 1e6 e 0.4 mu 0.6, dt 2e-6 s, "
+                       "rotation and power tallies on" % n,
+           "particles": n, "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "steps": steps, "skin_cm": skin, "rebuilds": rebuilds,
+           "gpu_launches": launches,
+           # the charge starts packed above the lifter ring: over the timed
+           # steps it settles onto itself before it reaches lifters and drum
+           "power_w_timed_steps": {"particle": e[0] / T, "lifter": e[1] / T, "drum": e[2] / T,
+                                   "total": float(e.sum()) / T},
+           "status": device.decode_status(status)}
+    if want_cpu:
+        cb = cpu_reference_rate(P, st, cpu_seconds, hatch=False, mill=(R, R, rad))
+        out["cpu_baseline"] = cb
+        if cb:
+            out["vs_cpu_reference"] = out["value"] / cb["value"]
+    return out
+
+
 class _StdoutToStderr:
     """Send file descriptor 1 to stderr while the reference's kernels run:
     their printf warnings would otherwise mix with the JSON line."""
@@ -464,14 +529,16 @@ def silo_full_leg(steps, warmup, skin=0.04, block=256):
                                  "rolling friction or triangle walls"}
 
 
-def cpu_reference_rate(P, st, seconds, max_steps=None, hatch=True):
+def cpu_reference_rate(P, st, seconds, max_steps=None, hatch=True, mill=None):
     """The reference's own kernels compiled as host C++ (oracle/_ref), all
-    host threads, reference mode, on this workload: particle-steps/s."""
+    host threads, reference mode, on this workload: particle-steps/s.
+    mill = (about_x, about_y, rad_per_step): drum rotating and the mill
+    driver's lifter turn before every step."""
     with _StdoutToStderr():
-        return _cpu_reference_rate(P, st, seconds, max_steps, hatch)
+        return _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill)
 
 
-def _cpu_reference_rate(P, st, seconds, max_steps, hatch):
+def _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill=None):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from bindings import RefHost, ref_available
     if not ref_available():
@@ -483,6 +550,9 @@ def _cpu_reference_rate(P, st, seconds, max_steps, hatch):
     R = RefHost().init(si, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d, threads=threads,
                        capture=False)
     R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st.get("quat"))
+    if mill is not None:
+        R.set_cylinder_rotation(True)
+        R.set_dobj_rotation(*mill)
     R.step(1)  # first step outside the clock (page-in)
     steps = 0
     t0 = time.perf_counter()
@@ -534,6 +604,10 @@ def main():
     torch.cuda.set_device(local)
     if args.silo_full_only:
         print(json.dumps(silo_full_leg(args.silo_full_steps, args.warmup)))
+        return 0
+    if args.mill_only:
+        print(json.dumps(mill_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                                  want_cpu=not args.no_cpu_baseline)))
         return 0
     if args.poly_only:
         print(json.dumps(poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
@@ -651,6 +725,10 @@ def main():
     if not args.no_poly:
         poly = poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                         want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+    mill = None
+    if not args.no_mill:
+        mill = mill_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                        want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
     batched = None
     if not args.no_batched:
         batched = batched_leg(args.batched_steps, args.warmup)
@@ -685,6 +763,7 @@ def main():
             "reference_mode_value": ref_mode_value,
             "silo_full": silo_full,
             "polyhedra": poly,
+            "mill": mill,
             "batched": batched,
             "adjoint": adjoint,
             "status": device.decode_status(status),

@@ -921,6 +921,9 @@ def write_state_file(path, state, time=0.0, spec_type=3, sim_type=0,
         fh.write("Specfication_Detail: %d\n" % spec_type)
         if sim_type == 2:
             fh.write("  Time: %r NumRem: %d\n" % (float(time), n))
+        elif sim_type == 1:
+            fh.write(" RevNum: 0  Time: %r RevComplete: 0  RotAngle: 0.0  EParticle: 0 ELift 0 "
+                     "EDrum: 0 ENorm: 0 EShear: 0\n" % float(time))
         else:
             fh.write("  Time: %r\n" % float(time))
         ints = np.stack([np.asarray(pid, np.int64), np.asarray(ptype, np.int64)], 1)

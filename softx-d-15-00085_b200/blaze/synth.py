@@ -17,6 +17,9 @@ SI and in these units).  All randomness is numpy default_rng(seed).
   silo_full_ensemble
                  the silo discharge in its full form (Hertz-Mindlin, rolling
                  friction, a 4,096-triangle hopper) as a one-system ensemble
+  mill_project   polydisperse steel spheres in a ball-mill drum with end
+                 plates and lifters turned with it (the ball-mill
+                 configuration's sphere charge, reference path)
 """
 import math
 import os
@@ -45,7 +48,7 @@ Number: {n_p}
 ---------------------------------------
  1.3_Dynamic_Objects_(index__name)
 ---------------------------------------
-Number: 0 Repeat: 0
+{dobj_lines}
 _________________________________________________
 _________________________________________________
              2_Simulation_Setup
@@ -145,7 +148,8 @@ def _write_cylinder_wobj(path, title, radius, height, offset, axis_normal=(0.0, 
 
 
 def _write_project(root, name, world_name, *, title, sim_type, dt, wobjs, pobjs, counts, n, g,
-                   rotation, roll_res, origin, world, cell, state, specific="", particle_type=0):
+                   rotation, roll_res, origin, world, cell, state, specific="", particle_type=0,
+                   dobj_lines="Number: 0 Repeat: 0"):
     base = os.path.join(root, name)
     for sub in ("World", "SurfaceObjects", "ParticleObjects", "VolumeObjects"):
         os.makedirs(os.path.join(base, sub), exist_ok=True)
@@ -156,7 +160,7 @@ def _write_project(root, name, world_name, *, title, sim_type, dt, wobjs, pobjs,
                                n_w=len(wobjs), wobj_lines=wl,
                                n_p=len(pobjs), pobj_lines=pl, n=n, g=g, rotation=rotation,
                                roll_res=roll_res, origin=origin, world=world, cell=cell,
-                               state=state, specific=specific))
+                               state=state, specific=specific, dobj_lines=dobj_lines))
     return base
 
 
@@ -493,6 +497,110 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
                    counts=[int(c_) for c_ in counts], n=n, g=gravity, rotation=rotation, roll_res=0.0,
                    origin=origin, world=tuple(float(v) for v in worldsz), cell=float(cell), state="Start_" + world,
                    specific=specific)
+    proj = Project.load(root, name, world)
+    return proj, proj.read_state()
+
+
+def mill_project(root, n=100_000, r_min=0.3, r_max=0.6, n_bins=6, rho=7800.0, drum_r=50.0,
+                 drum_l=30.0, rpm=30.0, n_lifters=8, lifter_w=4.0, lifter_h=4.0, kn=1.0e6,
+                 cor=0.4, mu=0.6, dt=2e-6, seed=2, overlap=1e-5, name="Mill", world="Mill_C3"):
+    """Ball mill on the reference path: a drum of radius drum_r and length
+    drum_l along z (macro cylinder with both end plates, centre line
+    (drum_r, drum_r)), n_lifters box lifters of lifter_w x lifter_h along
+    it (one lifter file, copied around the drum by the reference's Repeat,
+    KSimulationData.cpp:1885-2028), mill speed rpm with power tallies on
+    (Power(Revs) 1).  Spheres: radii uniform in [r_min, r_max] in n_bins
+    particle objects, steel, linear law kn, e, mu; packed from the bottom of
+    the drum on a simple-cubic lattice of pitch 2 r (1 - overlap), largest
+    bin lowest, inside the circle the lifters leave free (drum_r - lifter_h
+    - 1 cm), clear of the end plates.  The drum holds about 1.5e5 of these
+    spheres at that lattice fill.  Returns (Project, state dict)."""
+    base = os.path.join(root, name)
+    for sub in ("SurfaceObjects", "ParticleObjects", "LifterObjects"):
+        os.makedirs(os.path.join(base, sub), exist_ok=True)
+    R, L = float(drum_r), float(drum_l)
+    with open(os.path.join(base, "SurfaceObjects", "Drum.WOBJ"), "w") as fh:
+        fh.write('Title: "DRUM_MILL"\nDescp: "synthetic"\nGeometry-Specfications\n'
+                 "NUM_VERTEX: 0\nNUM_SURFACES: 1\n")
+        fh.write('-1 "DRUM"\nDiameter: %r\nHeight: %r\nTop: true\nBot: true\n'
+                 % (2.0 * R, L + 0.1))
+        fh.write("normalT: 0.0 0.0 -1.0\nnormalB: 0.0 0.0 1.0\nOffset: 0.0 0.0 0.0\n")
+    x0, x1 = R - 0.5 * lifter_w, R + 0.5 * lifter_w
+    h = float(lifter_h)
+    lv = [(x0, 0.0, 0.0), (x0, 0.0, L), (x1, 0.0, L), (x1, 0.0, 0.0),
+          (x0, h, 0.0), (x0, h, L), (x1, h, L), (x1, h, 0.0)]
+    with open(os.path.join(base, "LifterObjects", "Lifter.DOBJ"), "w") as fh:
+        fh.write('Title: "Lifter"\nDescp: "Lifter"\nGeometry_Specfications: 1\n')
+        fh.write("AXIS: 1.0 1.0 0.0\nCOM: %r %r %r\nB_R: %r\n" % (R, 0.5 * h, 0.5 * L,
+                                                                  float(max(lifter_w, h))))
+        fh.write("NUM_VERTEX: 8\n")
+        for k, v in enumerate(lv):
+            fh.write("%d %r %r %r\n" % (k + 1, v[0], v[1], v[2]))
+        # the two side faces and the top, normals out of the lifter; the top's
+        # two long edges
+        fh.write('NUM_FACES: 3\n1 "Left" AreaTol: 0.10\nNUM_VERTEX: 4\n1 5 6 2\n'
+                 '3 "Right" AreaTol: 0.10\nNUM_VERTEX: 4\n3 7 8 4\n'
+                 '5 "Top" AreaTol: 0.10\nNUM_VERTEX: 4\n7 6 5 8\n'
+                 "NUM_EDGES: 2\n5 6\n7 8\n")
+    edges = np.linspace(r_min, r_max, n_bins + 1)
+    radii = 0.5 * (edges[:-1] + edges[1:])
+    rng = np.random.default_rng(seed)
+    rs = rng.uniform(r_min, r_max, size=n)
+    types = np.clip(np.searchsorted(edges, rs, side="right") - 1, 0, n_bins - 1).astype(np.uint32)
+    counts = np.bincount(types, minlength=n_bins)
+    pobjs = []
+    for b in range(n_bins):
+        nm = "Ball%d" % b
+        with open(os.path.join(base, "ParticleObjects", nm + ".POBJ"), "w") as fh:
+            fh.write(_POBJ.format(title=nm, diam=float(2.0 * radii[b]), rho=float(rho),
+                                  cor=float(cor), kn=float(kn), mu=float(mu)))
+        pobjs.append(nm)
+    r_in = R - h - 1.0
+    pos = np.zeros((n, 3), np.float64)
+    types_out = np.zeros(n, np.uint32)
+    k = 0
+    y = R - r_in
+    for b in range(n_bins - 1, -1, -1):
+        r = float(radii[b])
+        pitch = 2.0 * r * (1.0 - overlap)
+        need = int(counts[b])
+        y += r
+        zs_all = np.arange(r + 0.05, L - r - 0.05 + 1e-9, pitch)
+        while need > 0:
+            if y > R + r_in - r:
+                raise ValueError("mill_project: %d spheres do not fit the drum" % n)
+            half = math.sqrt(max(r_in * r_in - (y - R) ** 2, 0.0)) - r - 0.002
+            if half > 0:
+                m = int(half / pitch)
+                xs = R + np.arange(-m, m + 1) * pitch
+                xx, zz = np.meshgrid(xs, zs_all, indexing="ij")
+                xx, zz = xx.ravel()[:need], zz.ravel()[:need]
+                cnt = len(xx)
+                pos[k:k + cnt, 0] = xx
+                pos[k:k + cnt, 1] = y
+                pos[k:k + cnt, 2] = zz
+                types_out[k:k + cnt] = b
+                k += cnt
+                need -= cnt
+            y += pitch
+        y += r * 0.002
+    state = dict(pos=pos.astype(np.float32), vel=np.zeros((n, 3), np.float32),
+                 avel=np.zeros((n, 3), np.float32), pid=np.arange(n, dtype=np.int32),
+                 type=types_out)
+    write_state_file(os.path.join(base, "Start_" + world), state, sim_type=1)
+    cell = 2.0 * r_max
+    origin = (-cell, -cell, -cell)
+    worldsz = (2 * R + 2 * cell, 2 * R + 2 * cell, L + 2 * cell)
+    specific = ("_________________________________________________\n"
+                "          6_Simulation_Specfic_Options\n"
+                "Power(Revs):   1\nTotal(Revs):   5\nSpeed(RPM):    %r\n"
+                "_________________________________________________\n" % float(rpm))
+    _write_project(root, name, world, title="Mill", sim_type=1, dt=dt, wobjs=["Drum"],
+                   pobjs=pobjs, counts=[int(c_) for c_ in counts], n=n, g=(0.0, -981.0, 0.0),
+                   rotation=1, roll_res=0.0, origin=origin,
+                   world=tuple(float(v) for v in worldsz), cell=float(cell),
+                   state="Start_" + world, specific=specific,
+                   dobj_lines="Number: 1 Repeat: %d\n1 Lifter" % n_lifters)
     proj = Project.load(root, name, world)
     return proj, proj.read_state()
 
