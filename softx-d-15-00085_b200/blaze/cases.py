@@ -5,7 +5,7 @@ run these).
     python softx-d-15-00085_b200/blaze/cases.py ens_step [STEPS]
         96 systems of the batched workload (1,442,352 spheres), skin 0.01 cm,
         blocks of 128, a 1,500-step pre-roll, then STEPS plain steps (30).
-    python softx-d-15-00085_b200/blaze/cases.py adjoint [NSYS] [STEPS] [SEGMENT]
+    python softx-d-15-00085_b200/blaze/cases.py adjoint [NSYS] [STEPS] [SEGMENT] [TAPE_BYTES]
         calibration ensemble of NSYS x 20,000 spheres (64), seeded initial
         velocities, reverse mode over STEPS steps (60) with checkpoints every
         SEGMENT (30), random cotangents of the final state.
@@ -58,11 +58,14 @@ def poly(n=20000, steps=10):
     return status
 
 
-def adjoint(nsys=64, steps=60, segment=30):
+def adjoint(nsys=64, steps=60, segment=30, tape_bytes=0):
+    """The calibration ensemble (nsys x 20,000 spheres), `steps` steps with
+    checkpoints every `segment`, the tape budget `tape_bytes` (0: one
+    segment; -1: 90 % of the free device memory), forward and backward."""
     S, W, p, r = calibrate.calibration_ensemble(nsys=nsys, n=20000, seed=4)
     ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, use_graph=0)
     ens.set_state(p, r, calibrate.initial_velocity(len(p)))
-    adj = E.Adjoint(ens, steps, segment)
+    adj = E.Adjoint(ens, steps, segment, tape_bytes)
     status = adj.forward()
     st = ens.state()
     g = np.random.default_rng(0).normal(size=st["pos"].shape).astype(np.float32)
