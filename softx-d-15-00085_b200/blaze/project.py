@@ -776,6 +776,12 @@ class Project:
         si.Rotating_WObject = bool(self.wobj[0].is_rotating)
         si.Mode2D = bool(sim_2d)
         self.init.threads_perBlock = 1024
+        if self.particle_type != 1:
+            # sphere lattice step: the diameter (main.cpp:534-541); polyhedra
+            # keep the largest vertex coordinates the parser found
+            for i in range(self.n_p):
+                d = float(F(F(self.pobj[i].radius) * F(2.0)))
+                setf3(self.init.p_size[i], (d, d, d))
         setf3(si.cellSize, self.grid_size)
         setf3(si.worldOrigin, self.grid_origin)
         total = vsub(self.world_size, self.grid_origin)

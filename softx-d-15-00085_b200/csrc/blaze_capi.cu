@@ -1252,26 +1252,130 @@ int blaze_profile(blaze_sim* s, float* ms_rebuild, float* ms_step, int* n_steps)
 blaze_sim* blaze_default_sim(void) { return g_default; }
 
 // --------------------------------------------- reference interface (Part 1)
+namespace {
+
+// The initial lattice Device_Set_SimulationData lays out for a world that
+// reads no state file (DeviceInterface.cu:192-707), restated:
+//   grid_type 0 (Set_Position_DefaultGrid): num.x x num.y x num.z sites,
+//     x fastest then z then y, stepped by p_size[0] + space in FP32 from
+//     `start`; types in object order by Num_ParticlesPerObject, P_ID = index;
+//     orientations (0, 0, 0, 0) (polyhedra);
+//   grid_type 1 (Set_Position_Random_Grid): the same sites; polyhedra get
+//     the orientation (30 r1, r2, r3, r4) from four rand() / RAND_MAX each,
+//     site by site; types round robin over the objects (an object already
+//     at its count gives the site to the first one with room); then N swaps
+//     of (type, P_ID) between sites rand() % (N - 1) and rand() % (N - 1).
+//     The reference writes the positions of this grid only when particles
+//     carry orientations; here every particle gets its site.
+// Velocities are InitConfig::velocity[0], spins zero
+// (Set_Init_Config_Device, GPU_Memory_Transfer.cuh:214-271).
+void initial_lattice(const SimulationInfo& si, const InitConfig& c, int n,
+                     std::vector<float3>& pos, std::vector<Quaterion>& q,
+                     std::vector<uint>& type, std::vector<int>& pid) {
+  pos.assign(n, make_float3(0.0f, 0.0f, 0.0f));
+  q.assign(n, Quaterion{0.0f, 0.0f, 0.0f, 0.0f});
+  type.assign(n, 0u);
+  pid.assign(n, 0);
+  const int NX = c.num.x, NY = c.num.y, NZ = c.num.z;
+  const float xs = c.p_size[0].x, ys = c.p_size[0].y, zs = c.p_size[0].z;
+  const bool orient = si.particle_type == 1 || si.sphere_orient;
+  const bool random = c.grid_type == 1;
+  const int nobj = std::max(0, std::min(si.Num_ParticleObjects, 6));
+  int selectcount[6] = {0, 0, 0, 0, 0, 0};
+  int selectT = -1;
+  float x = c.start.x, y = c.start.y, z = c.start.z;
+  for (int yd = 0; yd < NY; ++yd) {
+    for (int zd = 0; zd < NZ; ++zd) {
+      for (int xd = 0; xd < NX; ++xd) {
+        const int k = yd * NZ * NX + zd * NX + xd;
+        if (k < n) {
+          pos[k] = make_float3(x, y, z);
+          if (random) {
+            if (orient) {
+              const float rw = ((float)rand() / RAND_MAX) * 30.0;
+              const float rx = (float)rand() / RAND_MAX;
+              const float ry = (float)rand() / RAND_MAX;
+              const float rz = (float)rand() / RAND_MAX;
+              q[k] = Quaterion{rw, rx, ry, rz};
+            }
+            if (++selectT >= nobj) selectT = 0;
+            int pty = selectT;
+            const int* per = si.Num_ParticlesPerObject;
+            if (per && selectcount[pty] >= per[pty]) {
+              for (int i = 0; i < nobj; ++i)
+                if (selectcount[i] <= per[i] - 1) { pty = i; break; }
+            }
+            selectcount[pty]++;
+            type[k] = (uint)pty;
+            pid[k] = k;
+          }
+        }
+        x = x + xs + c.space.x;
+      }
+      x = c.start.x;
+      z = z + zs + c.space.z;
+    }
+    z = c.start.z;
+    y = y + ys + c.space.y;
+  }
+  if (!random) {
+    int idx = 0;
+    for (int i = 0; i < si.Num_ParticleObjects && si.Num_ParticlesPerObject; ++i)
+      for (int j = 0; j < si.Num_ParticlesPerObject[i] && idx < n; ++j, ++idx) {
+        type[idx] = (uint)i;
+        pid[idx] = idx;
+      }
+  } else if (n > 1) {
+    for (int i = 0; i < n; ++i) {
+      const int src = rand() % (n - 1);
+      const int dst = rand() % (n - 1);
+      std::swap(type[src], type[dst]);
+      std::swap(pid[src], pid[dst]);
+    }
+  }
+}
+
+}  // namespace
+
 int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_DynamicOBJ,
                               SimulationInfo* h_SimInfo, int h_Num_WorldOBJ,
                               int h_Num_ParticleOBJ, int h_Num_DynamicOBJ,
                               InitConfig* h_PosConfig) {
-  (void)h_PosConfig;  // initial lattices / fill waves are produced by the caller
   if (g_default) {
     blaze_destroy(g_default);
     g_default = nullptr;
+  }
+  if (h_PosConfig && !h_PosConfig->use_file && h_PosConfig->grid_type == 2) {
+    std::fprintf(stderr, "blaze: mill fill waves (InitConfig grid_type 2) are not built; "
+                         "start from a state file\n");
+    return -1;
   }
   blaze_sim* s = nullptr;
   int rc = create_impl(&s, h_WorldOBJ, h_Num_WorldOBJ, h_ParticleOBJ, h_Num_ParticleOBJ,
                        h_DynamicOBJ, h_Num_DynamicOBJ, h_SimInfo, nullptr);
   if (rc) return rc;
   g_default = s;
+  if (h_PosConfig && !h_PosConfig->use_file) {
+    const int n = s->n_max;
+    std::vector<float3> pos;
+    std::vector<Quaterion> q;
+    std::vector<uint> type;
+    std::vector<int> pid;
+    initial_lattice(*h_SimInfo, *h_PosConfig, n, pos, q, type, pid);
+    std::vector<float3> vel(n, h_PosConfig->velocity[0]), avel(n, make_float3(0.0f, 0.0f, 0.0f));
+    const bool orient = h_SimInfo->particle_type == 1;
+    rc = set_state_impl(s, (const float*)pos.data(), orient ? (const float*)q.data() : nullptr,
+                        (const float*)vel.data(), (const float*)avel.data(), type.data(),
+                        pid.data());
+    if (rc < 0) return rc;
+  }
   return 0;
 }
 
 #define DEF_SIM()             \
   blaze_sim* s = g_default;   \
   if (!s) return -2
+
 
 int Device_Set_Pos(float3* h_pos, Quaterion* h_Ornt, uint* h_ptype, int* h_pid) {
   DEF_SIM();

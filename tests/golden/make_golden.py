@@ -321,9 +321,27 @@ def _unscaled(mine, ref):
     return c
 
 
+def make_grid(ref_root, name, project, world):
+    """A world that reads no state file: the boundary structs, its
+    InitConfig and the particle count per object (the initial lattice is
+    laid out by Device_Set_SimulationData, DeviceInterface.cu:1772-1786)."""
+    P = Project.load(os.path.join(ref_root, "Projects"), project, world)
+    assert not P.init.use_file
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        wobj=np.frombuffer(bytes(P.wobj), np.uint8), pobj=np.frombuffer(bytes(P.pobj), np.uint8),
+        dobj=np.frombuffer(bytes(P.dobj), np.uint8),
+        sim_info=np.frombuffer(bytes(P.sim_info), np.uint8),
+        init=np.frombuffer(bytes(P.init), np.uint8), n_w=P.n_w, n_p=P.n_p, n_d=P.n_d,
+        per_object=np.array([P.per_object[i] for i in range(P.n_p)], np.int32),
+        source="%s/World/%s.World" % (project, world))
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     which = sys.argv[2:] or None
+    if which is None or "box_grid" in which:
+        make_grid(ref_root, "box_grid", "1.Particles_Box", "Spheres_128cm")
     for name, project, world, rot in FIXTURES:
         if which is None or name in which:
             make(ref_root, name, project, world, rot)
