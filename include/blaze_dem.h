@@ -183,6 +183,34 @@ int blaze_profile(blaze_sim* s, float* ms_rebuild, float* ms_step, int* n_steps)
 /* Drop the last world object (the silo hatch), as Device_OpenHatch does
  * without re-uploading the objects. */
 int blaze_open_hatch(blaze_sim* s);
+/* State files in the reference's format (Output_SystemState,
+ * FileIO.h:12-315): what the writer takes from the driver's globals. */
+typedef struct blaze_state_header {
+  int detail;          /* Specfication_Detail 1..5 */
+  int sim_type;        /* 0 general, 1 ball mill, 2 silo */
+  int rotating_wobj;   /* general run with a rotating world object */
+  int particle_type;   /* 0 spheres, 1 polyhedra */
+  int fill_start;      /* the start file a mill fill writes (zeroed mill line) */
+  int revflag;         /* mill: 1 at the end of a revolution */
+  int rev_number;      /* mill: the revolution counter */
+  int num_rem;         /* silo: particles left */
+  int rot_steps;       /* rotating world object: steps turned */
+  int steps_per_rev;   /* mill: steps per revolution (power line) */
+  double time;         /* simulated time, s */
+  double rot_angle;    /* mill / rotating world object: angle turned */
+  float energy[5];     /* mill: particle, lifter, drum, normal, shear */
+  float hatch_height;  /* silo: the speed statistics count particles above it */
+  float dt;            /* time step (power line) */
+} blaze_state_header;
+/* Write host arrays (memory order, n = particles in the run; quat4 w first;
+ * pobj for detail 5) as the reference's writer does.  No GPU needed. */
+int blaze_write_state_arrays(const char* path, const blaze_state_header* h, int n,
+                             const float* pos3, const float* quat4, const float* vel3,
+                             const float* avel3, const float* acc3, const uint* type,
+                             const int* pid, const POBJ* pobj, int n_p);
+/* The simulation's current state to `path` (accelerations are not kept:
+ * detail 4's acceleration column is 0). */
+int blaze_write_state(blaze_sim* s, const char* path, const blaze_state_header* h);
 /* The simulation behind Part 1 (NULL before Device_Set_SimulationData). */
 blaze_sim* blaze_default_sim(void);
 

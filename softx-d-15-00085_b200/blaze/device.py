@@ -36,6 +36,43 @@ class Options(C.Structure):
                 ("use_graph", C.c_int), ("capture_forces", C.c_int), ("sync_each_step", C.c_int)]
 
 
+class StateHeader(C.Structure):
+    """blaze_state_header (include/blaze_dem.h): the values the reference's
+    state writer takes from its driver (FileIO.h:12-315)."""
+    _fields_ = [("detail", C.c_int), ("sim_type", C.c_int), ("rotating_wobj", C.c_int),
+                ("particle_type", C.c_int), ("fill_start", C.c_int), ("revflag", C.c_int),
+                ("rev_number", C.c_int), ("num_rem", C.c_int), ("rot_steps", C.c_int),
+                ("steps_per_rev", C.c_int), ("time", C.c_double), ("rot_angle", C.c_double),
+                ("energy", C.c_float * 5), ("hatch_height", C.c_float), ("dt", C.c_float)]
+
+
+def state_header(**kw):
+    h = StateHeader()
+    h.detail = 3
+    for k, v in kw.items():
+        if k == "energy":
+            for q, e in enumerate(v):
+                h.energy[q] = float(e)
+        else:
+            setattr(h, k, v)
+    return h
+
+
+def write_state_arrays(path, header, pos, vel=None, avel=None, acc=None, ptype=None, pid=None,
+                       quat=None, pobj=None, n_p=0):
+    """Write host arrays (memory order) in the reference's state-file format."""
+    lib = load()
+    c = np.ascontiguousarray
+    n = len(pos)
+    arrs = [c(pos, np.float32), None if quat is None else c(quat, np.float32),
+            None if vel is None else c(vel, np.float32), None if avel is None else c(avel, np.float32),
+            None if acc is None else c(acc, np.float32), c(ptype, np.uint32), c(pid, np.int32)]
+    return _check(lib.blaze_write_state_arrays(
+        path.encode(), C.byref(header), n, _ptr(arrs[0], C.c_float), _ptr(arrs[1], C.c_float),
+        _ptr(arrs[2], C.c_float), _ptr(arrs[3], C.c_float), _ptr(arrs[4], C.c_float),
+        _ptr(arrs[5], C.c_uint), _ptr(arrs[6], C.c_int), pobj, int(n_p)), "blaze_write_state_arrays")
+
+
 _lib = None
 
 
@@ -55,6 +92,9 @@ def load():
     lib.blaze_set_options.argtypes = [C.c_void_p, P(Options)]
     lib.blaze_set_cylinder_rotation.argtypes = [C.c_void_p, C.c_int]
     lib.blaze_set_dobj_rotation.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int]
+    lib.blaze_write_state_arrays.argtypes = [C.c_char_p, P(StateHeader), C.c_int] + \
+        [P(C.c_float)] * 5 + [P(C.c_uint), P(C.c_int), P(T.POBJ), C.c_int]
+    lib.blaze_write_state.argtypes = [C.c_void_p, C.c_char_p, P(StateHeader)]
     lib.blaze_get_dobj.argtypes = [C.c_void_p, C.POINTER(T.DOBJ), C.c_int]
     lib.blaze_set_dobj_translation.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.blaze_set_wobj_rotation.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int]
@@ -196,6 +236,13 @@ class Simulation:
         d = (T.DOBJ * max(1, self.n_d))()
         _check(self.lib.blaze_get_dobj(self.h, d, self.n_d), "blaze_get_dobj")
         return d
+
+    def write_state(self, path, **header):
+        """The current state in the reference's state-file format
+        (blaze_state_header fields as keywords)."""
+        h = state_header(**header)
+        return _check(self.lib.blaze_write_state(self.h, path.encode(), C.byref(h)),
+                      "blaze_write_state")
 
     def energy(self):
         """Energy tallies (particle-particle, volume objects, world objects)

@@ -1168,6 +1168,21 @@ int blaze_set_energy(blaze_sim* s, const double* raw3) {
   return 0;
 }
 
+int blaze_write_state(blaze_sim* s, const char* path, const blaze_state_header* h) {
+  if (!s || !path || !h) return -1;
+  const int n = s->n_max;
+  std::vector<float> pos(3 * n), q(4 * n), vel(3 * n), avel(3 * n), acc(3 * n, 0.0f);
+  std::vector<uint> type(n);
+  std::vector<int> pid(n);
+  int rc = get_state_impl(s, pos.data(), s->poly ? q.data() : nullptr, vel.data(), avel.data(),
+                          type.data(), pid.data());
+  if (rc < 0) return rc;
+  // the removed particles sit after the ones in the run
+  const int cur = s->h_ctl->n_cur - s->h_ctl->pending_dead;
+  return blaze_write_state_arrays(path, h, cur, pos.data(), q.data(), vel.data(), avel.data(),
+                                  acc.data(), type.data(), pid.data(), s->p, s->n_p);
+}
+
 int blaze_get_forces(blaze_sim* s, float* f_pp, float* t_pp, float* f_w, float* t_w, float* f_l,
                      float* t_l) {
   if (!s || !s->cap_alloc) return -1;

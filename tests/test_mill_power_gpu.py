@@ -99,3 +99,26 @@ def test_reference_energy_interface(mill):
     s.step(100)
     np.testing.assert_array_equal(s.energy().astype(np.float32), e)
     s.close()
+
+
+def test_state_file_round_trip(mill, tmp_path):
+    """blaze_write_state on the GPU simulation: the file reads back (the
+    reference's reader layout) to the state within the format's 6
+    significant digits."""
+    from blaze.project import read_state_file
+    g = mill
+    s = device.Simulation(sim_info=g.sim_info, wobj=g.wobj, n_w=g.n_w, pobj=g.pobj, n_p=g.n_p,
+                          dobj=g.dobj, n_d=g.n_d)
+    st = g.init()
+    s.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    s.step(50)
+    a = s.state()
+    path = str(tmp_path / "state.dat")
+    s.write_state(path, detail=3, sim_type=1, rev_number=1, revflag=0, time=50 * 1e-5,
+                  steps_per_rev=272727, dt=1e-5)
+    s.close()
+    b = read_state_file(path, g.n, sim_type=1)
+    np.testing.assert_array_equal(b["pid"], a["pid"])
+    np.testing.assert_array_equal(b["type"], a["type"])
+    for key in ("pos", "vel", "avel"):
+        np.testing.assert_allclose(b[key], a[key], rtol=1e-5, atol=1e-30, err_msg=key)
