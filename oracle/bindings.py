@@ -84,6 +84,7 @@ class RefHost:
             lib.refh_get_dobj.argtypes = [C.POINTER(T.DOBJ), C.c_int]
             lib.refh_set_wobj_rotation.argtypes = [C.c_float, C.c_float, C.c_float, C.c_int]
             lib.refh_set_dobj_translation.argtypes = [C.c_int, C.c_int]
+            lib.refh_set_fill.argtypes = [C.c_int, C.c_int]
             lib.refh_get_wobj.argtypes = [C.POINTER(T.WOBJ), C.c_int]
             lib.refh_set_energy.argtypes = [_f]
             lib.refh_get_energy64.argtypes = [C.POINTER(C.c_double)]
@@ -178,6 +179,10 @@ class RefHost:
     def set_wobj_rotation(self, about_x, about_y, rad_per_step, on=True):
         self.lib.refh_set_wobj_rotation(float(about_x), float(about_y), float(rad_per_step),
                                         1 if on else 0)
+
+    def set_fill(self, pack, clear):
+        """Fill waves: `pack` particles join every clear + 1 steps."""
+        self.lib.refh_set_fill(int(pack), int(clear))
 
     def set_dobj_translation(self, index, on=True):
         self.lib.refh_set_dobj_translation(int(index), 1 if on else 0)

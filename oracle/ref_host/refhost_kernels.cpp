@@ -61,6 +61,9 @@ struct RefState {
   bool wobj_rot = false;
   float wrot_ax = 0.0f, wrot_ay = 0.0f, wrot_rad = 0.0f;
   int dobj_tr = -1;
+  /* the mill's fill waves (refh_set_fill) */
+  bool filling = false;
+  int fill_pack = 0, fill_clear = 0, fill_counter = 0;
 } S;
 
 /* A volume object's faces from its vertices (Processing_Mills.h:27-58). */
@@ -390,6 +393,20 @@ static int step_once() {
 
 int refh_step(int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
+    /* Device_DEM_UpdateSim's wave control and Fill_State
+       (DeviceInterface.cu:1055-1110, 1840-1866), restated */
+    if (S.filling) {
+      if (S.fill_counter > S.fill_clear || S.n_cur == 0) {
+        S.fill_counter = 0;
+        if (S.n_cur < S.n_max) {
+          S.n_cur += std::min(S.fill_pack, S.n_max - S.n_cur);
+          SimParms.Num_Particles = S.n_cur;
+        }
+        if (S.n_cur >= S.n_max) S.filling = false;
+      } else {
+        S.fill_counter++;
+      }
+    }
     if (S.wobj_rot) rotate_wobj_inc();
     if (S.dobj_rot) rotate_dobj_inc();
     if (S.dobj_tr >= 0) translate_dobj(S.dobj_tr);
@@ -490,6 +507,17 @@ void refh_set_wobj_rotation(float about_x, float about_y, float rad_per_step, in
 }
 
 void refh_set_dobj_translation(int index, int on) { S.dobj_tr = on ? index : -1; }
+
+/* A fill run: nothing in the run until the first step's wave, then `pack`
+ * particles (the next ones in memory order) every clear + 1 steps. */
+void refh_set_fill(int pack, int clear) {
+  S.filling = pack > 0;
+  S.fill_pack = pack;
+  S.fill_clear = clear;
+  S.fill_counter = 0;
+  S.n_cur = 0;
+  SimParms.Num_Particles = 0;
+}
 
 int refh_get_wobj(WOBJ* w, int n_w) {
   if (n_w < 0 || n_w > 8) return 1;

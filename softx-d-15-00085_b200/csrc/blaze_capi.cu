@@ -94,6 +94,10 @@ struct blaze_sim {
   int dobj_tr = -1;
   bool dobj_on_device = false;
   float rot_ax = 0.0f, rot_ay = 0.0f, rot_c = 1.0f, rot_s = 0.0f;
+  // the mill's fill waves (InitConfig grid_type 2): fill_pack particles join
+  // the run every fill_clear + 1 steps until all are in
+  bool filling = false;
+  int fill_n = 0, fill_pack = 0, fill_clear = 0, fill_counter = 0;
   bool wobj_rot = false;
   bool wobj_on_device = false;
   uint32_t wrot_mask = 0;
@@ -544,7 +548,36 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
   return k;
 }
 
+// Fill_State and the wave control of Device_DEM_UpdateSim
+// (DeviceInterface.cu:1055-1110, 1840-1866): before a step, either the next
+// wave joins (the counter passed the clearing time, or nothing is in the
+// run yet) or the counter advances.  A wave is the next fill_pack particles
+// at the end of the run, in memory order.
+int fill_wave(blaze_sim* s) {
+  if (s->fill_counter > s->fill_clear || s->fill_n == 0) {
+    s->fill_counter = 0;
+    if (s->fill_n < s->n_max) {
+      s->fill_n += std::min(s->fill_pack, s->n_max - s->fill_n);
+      CK(cudaStreamSynchronize(s->stream));
+      CK(cudaMemcpy(&s->h_ctl->n_cur, &s->ctl->n_cur, sizeof(int), cudaMemcpyDeviceToHost));
+      s->h_ctl->n_cur = s->fill_n;
+      s->h_ctl->rebuild_req = 1;
+      CK(cudaMemcpy(&s->ctl->n_cur, &s->h_ctl->n_cur, sizeof(int), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(&s->ctl->rebuild_req, &s->h_ctl->rebuild_req, sizeof(int),
+                    cudaMemcpyHostToDevice));
+    }
+    if (s->fill_n >= s->n_max) s->filling = false;
+  } else {
+    s->fill_counter++;
+  }
+  return 0;
+}
+
 int enqueue_step(blaze_sim* s) {
+  if (s->filling) {
+    int rc = fill_wave(s);
+    if (rc) return rc;
+  }
   if (s->profile) prof_event(s, 0);
   launch_gate(s->ctl, s->stream);
   int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
@@ -1031,7 +1064,7 @@ int blaze_get_state_ornt(blaze_sim* s, float* pos3, float* quat4, float* vel3, f
 int blaze_step(blaze_sim* s, int nsteps) {
   if (!s || nsteps < 0) return -1;
   s->last_launches = 0;
-  if (s->opt.use_graph && !s->opt.sync_each_step && !s->profile) {
+  if (s->opt.use_graph && !s->opt.sync_each_step && !s->profile && !s->filling) {
     int rc = graph_steps(s, nsteps);
     if (rc) return rc;
     CK(cudaGetLastError());
@@ -1350,6 +1383,88 @@ void initial_lattice(const SimulationInfo& si, const InitConfig& c, int n,
   }
 }
 
+// Set_Position_Fill_Mill (DeviceInterface.cu:708-1054), restated: the
+// whole charge on a lattice of the largest particle's diameter with gaps
+// (0.001, 0.001, 0) -- for a ball mill across the drum from its centre
+// height upwards (inside the lifters' bound when there are any), else over
+// the fill plane -- waves of NX x NZ sites one diameter apart in height;
+// types round robin with room, P_ID = site, then the rand() shuffle of
+// (type, P_ID); polyhedra get rand() orientations site by site.  Returns
+// the wave size; clear = the steps a wave needs to fall two diameters at
+// the launch speed.
+int fill_lattice(const SimulationInfo& si, const InitConfig& c, const POBJ* po, const WOBJ* w,
+                 int n_d, int n, std::vector<float3>& pos, std::vector<Quaterion>& q,
+                 std::vector<uint>& type, std::vector<int>& pid, int& clear) {
+  pos.assign(n, make_float3(0.0f, 0.0f, 0.0f));
+  q.assign(n, Quaterion{0.0f, 0.0f, 0.0f, 0.0f});
+  type.assign(n, 0u);
+  pid.assign(n, 0);
+  const float3 space = make_float3(0.00100f, 0.0010f, 0.0000f);
+  const float xs = 2.0 * po[0].radius, ys = 2.0 * po[0].radius, zs = 2.0 * po[0].radius;
+  const float radius = n_d > 0 ? si.DObject_CylinderBoundR : w[0].cyl_geo.radius;
+  float x, y, z;
+  int NX, NY, NZ;
+  if (si.Simulation_Type == ballmill && !si.Rotating_WObject) {
+    x = n_d > 0 ? xs + (w[0].cyl_geo.radius - si.DObject_CylinderBoundR) : xs + space.x;
+    y = w[0].cyl_geo.radius;
+    z = w[0].cyl_geo.center_bot_cap.z + zs / 2.0f + space.z;
+    NX = (int)floor((radius * 2 - xs) / (xs + space.x));
+    NZ = (int)floor((w[0].cyl_geo.height) / (zs + space.z));
+    NY = (int)ceil(n / (float)(NX * NZ));
+  } else {
+    x = c.fill_plane_start.x + xs;
+    y = c.fill_plane_start.y;
+    z = c.fill_plane_start.z + zs;
+    NX = (int)floor((c.fill_plane_end.x - c.fill_plane_start.x) / (xs + space.x));
+    NZ = (int)floor((c.fill_plane_end.z - c.fill_plane_start.z) / (zs + space.z));
+    NY = (int)ceilf(n / (float)(NX * NZ));
+  }
+  const float3 start = make_float3(x, y, z);
+  clear = (int)fabs((int)ceil((2.0f * ys / (si.InitalDelta_t * c.launch_Vel.y))));
+  const bool orient = si.particle_type == 1 || si.sphere_orient;
+  const int nobj = std::max(0, std::min(si.Num_ParticleObjects, 6));
+  int selectcount[6] = {0, 0, 0, 0, 0, 0};
+  int selectT = -1;
+  for (int yd = 0; yd < NY; ++yd) {
+    for (int zd = 0; zd < NZ; ++zd) {
+      for (int xd = 0; xd < NX; ++xd) {
+        const int k = yd * NZ * NX + zd * NX + xd;
+        if (k >= n) break;
+        pos[k] = make_float3(x, y, z);
+        if (orient) {
+          const float rw = ((float)rand() / RAND_MAX) * 30.0;
+          const float rx = (float)rand() / RAND_MAX;
+          const float ry = (float)rand() / RAND_MAX;
+          const float rz = (float)rand() / RAND_MAX;
+          q[k] = Quaterion{rw, rx, ry, rz};
+        }
+        if (++selectT >= nobj) selectT = 0;
+        int pty = selectT;
+        const int* per = si.Num_ParticlesPerObject;
+        if (per && selectcount[pty] >= per[pty]) {
+          for (int i = 0; i < nobj; ++i)
+            if (selectcount[i] <= per[i] - 1) { pty = i; break; }
+        }
+        selectcount[pty]++;
+        type[k] = (uint)pty;
+        pid[k] = k;
+        x = x + xs + space.x;
+      }
+      x = start.x;
+      z = z + zs + space.z;
+    }
+    z = start.z;
+    y = y + ys + space.y;
+  }
+  for (int i = 0; i < n && n > 1; ++i) {
+    const int src = rand() % (n - 1);
+    const int dst = rand() % (n - 1);
+    std::swap(type[src], type[dst]);
+    std::swap(pid[src], pid[dst]);
+  }
+  return NX * NZ;
+}
+
 }  // namespace
 
 int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_DynamicOBJ,
@@ -1359,11 +1474,6 @@ int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_Dyn
   if (g_default) {
     blaze_destroy(g_default);
     g_default = nullptr;
-  }
-  if (h_PosConfig && !h_PosConfig->use_file && h_PosConfig->grid_type == 2) {
-    std::fprintf(stderr, "blaze: mill fill waves (InitConfig grid_type 2) are not built; "
-                         "start from a state file\n");
-    return -1;
   }
   blaze_sim* s = nullptr;
   int rc = create_impl(&s, h_WorldOBJ, h_Num_WorldOBJ, h_ParticleOBJ, h_Num_ParticleOBJ,
@@ -1376,13 +1486,29 @@ int Device_Set_SimulationData(WOBJ* h_WorldOBJ, POBJ* h_ParticleOBJ, DOBJ* h_Dyn
     std::vector<Quaterion> q;
     std::vector<uint> type;
     std::vector<int> pid;
-    initial_lattice(*h_SimInfo, *h_PosConfig, n, pos, q, type, pid);
+    const bool fill = h_PosConfig->grid_type == 2;
+    int clear = 0, pack = 0;
+    if (fill)
+      pack = fill_lattice(*h_SimInfo, *h_PosConfig, h_ParticleOBJ, h_WorldOBJ, h_Num_DynamicOBJ,
+                          n, pos, q, type, pid, clear);
+    else
+      initial_lattice(*h_SimInfo, *h_PosConfig, n, pos, q, type, pid);
     std::vector<float3> vel(n, h_PosConfig->velocity[0]), avel(n, make_float3(0.0f, 0.0f, 0.0f));
     const bool orient = h_SimInfo->particle_type == 1;
     rc = set_state_impl(s, (const float*)pos.data(), orient ? (const float*)q.data() : nullptr,
                         (const float*)vel.data(), (const float*)avel.data(), type.data(),
                         pid.data());
     if (rc < 0) return rc;
+    if (fill && pack > 0) {
+      // nothing in the run until the first step's wave (NUMPARTICLES_Current = 0)
+      s->filling = true;
+      s->fill_n = 0;
+      s->fill_pack = pack;
+      s->fill_clear = clear;
+      s->fill_counter = 0;
+      s->h_ctl->n_cur = 0;
+      CK(cudaMemcpy(&s->ctl->n_cur, &s->h_ctl->n_cur, sizeof(int), cudaMemcpyHostToDevice));
+    }
   }
   return 0;
 }

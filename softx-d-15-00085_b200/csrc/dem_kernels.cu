@@ -76,7 +76,8 @@ k_hash(const SimParams* __restrict__ P, const float4* __restrict__ pos, OrderBuf
   const int* pid = (ctl->epoch & 1) ? ob.pid[1] : ob.pid[0];
   uint32_t key;
   uint32_t st = 0;
-  if (pid[i] < 0) {
+  // removed particles and those a fill has not reached yet stay at the end
+  if (pid[i] < 0 || i >= ctl->n_cur) {
     key = P->ncell_tab + 1u;
   } else {
     const float4 p = pos[i];

@@ -321,11 +321,11 @@ def _unscaled(mine, ref):
     return c
 
 
-def make_grid(ref_root, name, project, world):
+def make_grid(ref_root, name, project, world, projects_dir=None):
     """A world that reads no state file: the boundary structs, its
     InitConfig and the particle count per object (the initial lattice is
     laid out by Device_Set_SimulationData, DeviceInterface.cu:1772-1786)."""
-    P = Project.load(os.path.join(ref_root, "Projects"), project, world)
+    P = Project.load(projects_dir or os.path.join(ref_root, "Projects"), project, world)
     assert not P.init.use_file
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
@@ -337,11 +337,32 @@ def make_grid(ref_root, name, project, world):
         source="%s/World/%s.World" % (project, world))
 
 
+def make_mill_fill(ref_root, name):
+    """The ball mill filled by waves: Mill_SPH30 with its initial setup
+    switched to the fill the reference's Mill_SPH30_Fill world asks for
+    (Read_FromFile 0, SetpUp 2, launch_Vel 10 -200 10; that world file
+    itself lacks its Delta_t line, which its parser then misreads)."""
+    with tempfile.TemporaryDirectory() as tmp:
+        proj = os.path.join(tmp, "3.BallMill")
+        shutil.copytree(os.path.join(ref_root, "Projects", "3.BallMill"), proj)
+        wf = os.path.join(proj, "World", "Mill_SPH30.World")
+        text = open(wf).read()
+        text, k = re.subn(r"Read_FromFile:\s+1\s+File_Name:\s+\S+",
+                          "Read_FromFile:  0\nSetpUp(0=grid,2=fill): 2\nlaunch_Vel: 10.0 -200.0 10.0",
+                          text)
+        assert k == 1
+        with open(os.path.join(proj, "World", "Mill_Fill.World"), "w") as fh:
+            fh.write(text)
+        make_grid(tmp, name, "3.BallMill", "Mill_Fill", projects_dir=tmp)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     which = sys.argv[2:] or None
     if which is None or "box_grid" in which:
         make_grid(ref_root, "box_grid", "1.Particles_Box", "Spheres_128cm")
+    if which is None or "mill_fill" in which:
+        make_mill_fill(ref_root, "mill_fill")
     for name, project, world, rot in FIXTURES:
         if which is None or name in which:
             make(ref_root, name, project, world, rot)

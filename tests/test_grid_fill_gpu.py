@@ -126,3 +126,97 @@ def test_random_grid():
     ref = restated(g, random=True)
     for key in ("pos", "vel", "type", "pid"):
         np.testing.assert_array_equal(got[key], ref[key], err_msg=key)
+
+
+class Fill(Grid):
+    def __init__(self):
+        z = np.load(os.path.join(HERE, "golden", "mill_fill.npz"))
+        self.n_w, self.n_p, self.n_d = int(z["n_w"]), int(z["n_p"]), int(z["n_d"])
+        self.wobj = (T.WOBJ * 8).from_buffer_copy(z["wobj"].tobytes())
+        self.pobj = (T.POBJ * 8).from_buffer_copy(z["pobj"].tobytes())
+        self.dobj = (T.DOBJ * 32).from_buffer_copy(z["dobj"].tobytes())
+        self.sim_info = T.SimulationInfo.from_buffer_copy(z["sim_info"].tobytes())
+        self.init = T.InitConfig.from_buffer_copy(z["init"].tobytes())
+        self.per = (ctypes.c_int * 8)(*[int(v) for v in z["per_object"]])
+        self.sim_info.Num_ParticlesPerObject = ctypes.cast(self.per, ctypes.POINTER(ctypes.c_int))
+        self.n = self.sim_info.Num_Particles
+
+
+def restated_fill(g):
+    """Set_Position_Fill_Mill (DeviceInterface.cu:708-1054) for a ball mill
+    with lifters, float32 throughout, glibc rand() for the shuffle."""
+    f = np.float32
+    si, c, w = g.sim_info, g.init, g.wobj[0]
+    xs = f(2.0 * g.pobj[0].radius)
+    sx, sy, sz = f(0.001), f(0.001), f(0.0)
+    radius = f(si.DObject_CylinderBoundR)
+    x0 = f(xs + f(f(w.cyl_geo.radius) - radius))
+    y = f(w.cyl_geo.radius)
+    z0 = f(f(f(w.cyl_geo.center_bot_cap.z) + f(xs / f(2.0))) + sz)
+    NX = int(np.floor(f(f(f(radius * f(2)) - xs) / f(xs + sx))))
+    NZ = int(np.floor(f(f(w.cyl_geo.height) / f(xs + sz))))
+    NY = int(np.ceil(f(g.n / f(NX * NZ))))
+    pos = np.zeros((g.n, 3), np.float32)
+    typ = np.zeros(g.n, np.uint32)
+    pid = np.arange(g.n, dtype=np.int32)
+    per = [g.per[i] for i in range(g.n_p)]
+    count, sel = [0] * g.n_p, -1
+    z = z0
+    for yd in range(NY):
+        for zd in range(NZ):
+            x = x0
+            for xd in range(NX):
+                k = yd * NZ * NX + zd * NX + xd
+                if k >= g.n:
+                    break
+                pos[k] = (x, y, z)
+                sel = sel + 1 if sel + 1 < g.n_p else 0
+                pty = sel
+                if count[pty] >= per[pty]:
+                    pty = next(i for i in range(g.n_p) if count[i] <= per[i] - 1)
+                count[pty] += 1
+                typ[k] = pty
+                x = f(f(x + xs) + sx)
+            z = f(f(z + xs) + sz)
+        z = z0
+        y = f(f(y + xs) + sy)
+    for _ in range(g.n):
+        a = LIBC.rand() % (g.n - 1)
+        b = LIBC.rand() % (g.n - 1)
+        typ[a], typ[b] = typ[b], typ[a]
+        pid[a], pid[b] = pid[b], pid[a]
+    clear = int(abs(int(np.ceil(f(f(f(2.0) * xs) / f(f(si.InitalDelta_t) * f(c.launch_Vel.y)))))))
+    return dict(pos=pos, type=typ, pid=pid), NX * NZ, clear
+
+
+def test_mill_fill_waves():
+    """The mill filled by waves (grid type 2): the lattice, then three waves
+    (10,100 steps) on oracle A's trajectory with the same wave control."""
+    g = Fill()
+    LIBC.srand(1)
+    kd, got = device_state(g, g.init)
+    LIBC.srand(1)
+    ref, pack, clear = restated_fill(g)
+    for key in ("pos", "type", "pid"):
+        np.testing.assert_array_equal(got[key], ref[key], err_msg=key)
+    assert pack == 45 and clear == 5000
+    if bindings.ref_available():
+        zero = np.zeros((g.n, 3), np.float32)
+        R = bindings.RefHost()
+        R.init(g.sim_info, g.wobj, g.n_w, g.pobj, g.n_p, g.dobj, g.n_d, threads=4, capture=False)
+        R.set_state(ref["pos"], zero, zero, ref["type"], ref["pid"])
+        R.set_fill(pack, clear)
+        steps = 2 * (clear + 1) + 99
+        assert R.step(steps) == 0
+        for _ in range(steps):
+            kd.IDevice_DEM_UpdateSim()
+        after = {k: np.zeros((g.n, 3), np.float32) for k in ("pos", "vel", "avel", "acc")}
+        after["type"] = np.zeros(g.n, np.uint32)
+        after["pid"] = np.zeros(g.n, np.int32)
+        kd.IDevice_Get_System_State(after["pos"], None, after["vel"], after["avel"], after["acc"],
+                                    after["type"], after["pid"])
+        b = R.state()
+        assert R.lib.refh_num_current() == 3 * pack
+        for key in ("pos", "vel", "pid"):
+            np.testing.assert_array_equal(after[key], b[key], err_msg=key)
+    kd.clean()
