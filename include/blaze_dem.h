@@ -211,6 +211,10 @@ int blaze_write_state_arrays(const char* path, const blaze_state_header* h, int 
 /* The simulation's current state to `path` (accelerations are not kept:
  * detail 4's acceleration column is 0). */
 int blaze_write_state(blaze_sim* s, const char* path, const blaze_state_header* h);
+/* Self-check of the step's shared-reciprocal division against IEEE
+ * division on the GPU: components that differ over n random triples
+ * (0 expected), -1 on error. */
+long long blaze_check_division(long long n, unsigned long long seed);
 /* The simulation behind Part 1 (NULL before Device_Set_SimulationData). */
 blaze_sim* blaze_default_sim(void);
 

@@ -1201,6 +1201,18 @@ int blaze_set_energy(blaze_sim* s, const double* raw3) {
   return 0;
 }
 
+long long blaze_check_division(long long n, unsigned long long seed) {
+  if (n < 0) return -1;
+  unsigned long long* d = nullptr;
+  if (cudaMalloc((void**)&d, sizeof(*d)) != cudaSuccess) return -1;
+  unsigned long long h = 0;
+  cudaMemset(d, 0, sizeof(*d));
+  launch_check_div(n, seed, d, 0);
+  const cudaError_t e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? (long long)h : -1;
+}
+
 int blaze_write_state(blaze_sim* s, const char* path, const blaze_state_header* h) {
   if (!s || !path || !h) return -1;
   const int n = s->n_max;

@@ -122,4 +122,32 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 }
 __device__ __forceinline__ float3 xyz(float4 a) { return f3(a.x, a.y, a.z); }
 
+// a / b for the three components of a by one positive, normal b, correctly
+// rounded (the same numbers as three IEEE divisions), from one correctly
+// rounded reciprocal y = RN(1/b) and correction steps with exact remainders
+// (one fused multiply-add each): q0 = RN(a y) is within 1.5 ulp of a/b;
+// q1 = RN(q0 + (a - b q0) y) is then within one ulp, and the final
+// q = RN(q1 + (a - b q1) y) is a/b rounded to nearest by Markstein's theorem
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990; J.-M. Muller et al.,
+// Handbook of Floating-Point Arithmetic: with y within half an ulp of 1/b
+// and q1 within an ulp of a/b, the corrected quotient is correctly rounded,
+// barring underflow or overflow of the intermediate values).  A zero
+// numerator keeps its sign.  Outside the range where every intermediate is
+// normal and finite (b in [1e-15, 1e15], |a| in [1e-20, 1e15]: quotients
+// between 1e-35 and 1e30) the IEEE division is used.  blaze_check_division
+// compares it with IEEE division on the GPU.
+__device__ __forceinline__ float div_rn(float a, float y, float b) {
+  if (a == 0.0f) return a * y;
+  if (!(fabsf(a) >= 1e-20f && fabsf(a) <= 1e15f)) return a / b;
+  const float q0 = a * y;
+  const float q1 = fmaf(fmaf(-q0, b, a), y, q0);
+  const float r1 = fmaf(-q1, b, a);
+  return r1 == 0.0f ? q1 : fmaf(r1, y, q1);
+}
+__device__ __forceinline__ float3 div3_rn(float3 a, float b) {
+  if (!(b >= 1e-15f && b <= 1e15f)) return f3(a.x / b, a.y / b, a.z / b);
+  const float y = __frcp_rn(b);
+  return f3(div_rn(a.x, y, b), div_rn(a.y, y, b), div_rn(a.z, y, b));
+}
+
 }  // namespace blaze

@@ -371,7 +371,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     const float4 wb4 = kSpin ? __ldg(in.angv + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const int tb = __float_as_int(vb4.w);
     const float3 vb = xyz(vb4);
-    const float3 nrm = rel / dist;
+    const float3 nrm = div3_rn(rel, dist);   // = rel / dist, three correctly rounded quotients
     const float dis = fabsf(dist - (ra + pb4.w)) + 0.000010f;
     const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
     const Forces F = law_pp<kSpin>(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
@@ -619,6 +619,43 @@ __global__ void k_rotate_wobj(WallOp* ops, int n_ops, uint32_t rot_mask, float a
   op.kind = op.area == -1.0f ? kOpPlane : kOpFace;
 }
 
+// --------------------------------------------------------- division check
+// div3_rn against three IEEE divisions on n pseudo-random triples (a
+// SplitMix64 stream per index: numerators over 1e-25..1e25 and both signs,
+// denominators over 1e-18..1e18, one in 64 numerators zero or a signed
+// power of two), counting the components that differ in any bit.
+__device__ __forceinline__ unsigned long long splitmix(unsigned long long& x) {
+  unsigned long long z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ float log_uniform(unsigned long long u, float lo_exp, float hi_exp) {
+  const float t = (float)(u >> 40) * (1.0f / 16777216.0f);
+  return exp10f(lo_exp + t * (hi_exp - lo_exp));
+}
+__global__ void k_check_div(long long n, unsigned long long seed, unsigned long long* bad) {
+  unsigned long long local = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long x = seed ^ (unsigned long long)i * 0xD1B54A32D192ED03ull;
+    float a[3];
+    for (int c = 0; c < 3; ++c) {
+      const unsigned long long u = splitmix(x);
+      float v = log_uniform(u, -25.0f, 25.0f);
+      if ((u & 63ull) == 0) v = 0.0f;
+      else if ((u & 63ull) == 1) v = ldexpf(1.0f, (int)((u >> 8) % 120) - 60);
+      a[c] = (u >> 7) & 1ull ? -v : v;
+    }
+    const float b = log_uniform(splitmix(x), -18.0f, 18.0f);
+    const float3 q = div3_rn(f3(a[0], a[1], a[2]), b);
+    const float r[3] = {q.x, q.y, q.z};
+    for (int c = 0; c < 3; ++c)
+      if (__float_as_uint(r[c]) != __float_as_uint(__fdiv_rn(a[c], b))) ++local;
+  }
+  if (local) atomicAdd(bad, local);
+}
+
 // ---------------------------------------------------------------------- kill
 // Remove_Silo_Discharged_Particles / Remove_PL_Discharged_Particles
 // (GPU_Memory_Transfer.cuh:646-682): park at max_size, pid -1, count.  The
@@ -764,6 +801,11 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
   }
 #undef BLAZE_STEP
 #undef BLAZE_STEP_ARGS
+}
+
+void launch_check_div(long long n, unsigned long long seed, unsigned long long* bad,
+                      cudaStream_t st) {
+  k_check_div<<<148 * 8, 256, 0, st>>>(n, seed, bad);
 }
 
 void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, double* part,

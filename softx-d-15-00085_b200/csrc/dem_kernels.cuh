@@ -94,6 +94,10 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
 // tally[c] += sum of eb[c * n_max + i] over the current particles, in a fixed
 // order; part holds 3 doubles per block of kEnergyBlock particles.
 constexpr int kEnergyBlock = 256;
+// Self-check of div3_rn against IEEE division on n random triples:
+// *bad += the components that differ.
+void launch_check_div(long long n, unsigned long long seed, unsigned long long* bad,
+                      cudaStream_t st);
 void launch_energy_reduce(const double* eb, int n_max, const StepCtl* ctl, double* part,
                           double* tally, cudaStream_t st);
 // One step of the mill driver's moves of volume objects: with `turn`, the

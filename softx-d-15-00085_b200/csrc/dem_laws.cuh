@@ -1,7 +1,9 @@
 // dem_laws.cuh -- the reference's contact laws and point-in-polygon test as
 // FP32 device functions, shared by the sphere and polyhedron step kernels.
 // Every expression keeps the reference's operation order (the translation
-// units that include this file are compiled with -fmad=false).
+// units that include this file are compiled with -fmad=false); a vector
+// divided by a scalar goes through div3_rn (dem_common.cuh), which gives
+// the IEEE quotients bit for bit.
 #pragma once
 
 #include "dem_common.cuh"
@@ -54,7 +56,7 @@ __device__ __forceinline__ Forces law_pp_pre(const SimParams& P, float3 rvel, fl
     if (velf > 0) velf = sqrtf(velf);
     else velf = 1.0f;
     const float tan_f = tan_pre * (mag / velf);
-    ft = (-1.0f * tan_f) * (vt / mag);
+    ft = (-1.0f * tan_f) * div3_rn(vt, mag);
     if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
   if (e) *e = en;
@@ -81,7 +83,7 @@ __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 
   const float fn = T.s_kn * pen;
   const float3 fdiss = T.s_cn * vn;
   F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
+  const float3 fdir = div3_rn(F.trans, len3(F.trans));
   float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
   else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
@@ -95,7 +97,7 @@ __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 
     if (velf > 0) velf = sqrtf(velf);
     else velf = 1.0f;
     const float tan_f = (0.050f * (T.mass / P.dt)) * (T.s_mus * (mag / velf));
-    ft = (-1.0f * tan_f) * (vt / mag);
+    ft = (-1.0f * tan_f) * div3_rn(vt, mag);
     if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
   if (e) *e = en;
@@ -115,7 +117,7 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
   const float fn = T.s_kn * pen;
   const float3 fdiss = T.s_cn * vn;
   F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
+  const float3 fdir = div3_rn(F.trans, len3(F.trans));
   float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
   else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
@@ -130,7 +132,7 @@ __device__ __forceinline__ Forces law_moving_surface(const SimParams& P, float3 
     if (velf > 0) velf = sqrtf(velf);
     else velf = 1.0f;
     const float tan_f = T.s_muk * (mag / velf);
-    ft = (((-1.0f * tan_f) * (vt / mag)) * (T.mass / P.dt)) * 0.050f;
+    ft = (((-1.0f * tan_f) * div3_rn(vt, mag)) * (T.mass / P.dt)) * 0.050f;
     if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
   if (e) *e = en;
@@ -152,7 +154,7 @@ __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float
   const float fn = T.d_kn * pen;
   const float3 fdiss = T.d_cn * vn;
   F.trans = fn * n - fdiss;
-  const float3 fdir = F.trans / len3(F.trans);
+  const float3 fdir = div3_rn(F.trans, len3(F.trans));
   float en = 0.0f;
   if (dot3(fdir, n) < 0) F.trans = fn * n;
   else if (e && dot3(vn, vn) > 0.0f) en = (len3(fdiss) * len3(vn)) * P.dt;
@@ -168,7 +170,7 @@ __device__ __forceinline__ Forces law_volume(const SimParams& P, float3 n, float
     if (velf > 0) velf = sqrtf(velf);
     else velf = 1.0f;
     const float tan_f = (0.050f * (T.mass / P.dt)) * (T.d_muk * (mag / velf));
-    ft = (-1.0f * tan_f) * (vt / mag);
+    ft = (-1.0f * tan_f) * div3_rn(vt, mag);
     if (e) en = en + ((len3(ft) * mag) * P.dt);
   }
   if (e) *e = en;

@@ -1,6 +1,8 @@
 """GPU parity through the C ABI: the sm_100a kernels against the reference's
 own kernels (golden fixtures) and against the FP32 restatement, bit for bit
 in the reference mode (skin 0); within stated tolerance with a Verlet skin."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -165,3 +167,15 @@ def test_graph_stepping_is_exact(silo_small, skin):
     b = run_steps(P, st, 301, skin=skin, use_graph=1)
     for key in ("pos", "vel", "avel", "pid"):
         np.testing.assert_array_equal(a[key], b[key])
+
+
+@pytest.mark.gpu
+def test_shared_reciprocal_division_is_ieee():
+    """div3_rn (one correctly rounded reciprocal + two corrections per
+    quotient, dem_common.cuh) equals IEEE division bit for bit on 3 x 2^30
+    random quotients over 1e-25..1e25 / 1e-18..1e18 (including the ranges
+    it hands to the IEEE division), zero and power-of-two numerators."""
+    lib = device.load()
+    lib.blaze_check_division.restype = ctypes.c_longlong
+    lib.blaze_check_division.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong]
+    assert lib.blaze_check_division(1 << 30, 12345) == 0
