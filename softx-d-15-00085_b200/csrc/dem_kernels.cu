@@ -309,6 +309,8 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 #ifndef BLAZE_STEP_MIN_BLOCKS
 #define BLAZE_STEP_MIN_BLOCKS 4
 #endif
+// candidate slots tested per batch of independent loads in the contact pass
+constexpr int kMaskBatch = 8;
 // kEnergy: also the energy tallies of the step's contacts, per particle in
 // contact order (particle-particle, volume objects, world objects), into
 // eb[c * n_max + i] in FP64.
@@ -349,26 +351,36 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   float3 fl = f3(0.0f, 0.0f, 0.0f);
   double e_pp = 0.0, e_lift = 0.0, e_surf = 0.0;
   float ec = 0.0f;
-  // contacts first (the slots whose spheres overlap), then the law over
-  // those alone, in slot order: the law's lanes stay busy when neighbour
-  // counts differ inside a warp
+  // contacts first (the slots whose spheres overlap), candidates in batches:
+  // all index loads of a batch, then all position gathers, then the tests,
+  // so a batch costs one round trip per level
   const int cnt = (int)nl.cnt[i];
+  const uint32_t* __restrict__ li = nl.idx + i;
   uint32_t cm = 0;
-  for (int k = 0; k < cnt; ++k) {
-    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
-    const float4 pb4 = __ldg(in.pos + j);
-    const float3 rel = pa - xyz(pb4);
-    if (len3(rel) - (ra + pb4.w) < 0.0f) cm |= 1u << k;
+  for (int k0 = 0; k0 < cnt; k0 += kMaskBatch) {
+    uint32_t jj[kMaskBatch];
+#pragma unroll
+    for (int u = 0; u < kMaskBatch; ++u)
+      jj[u] = k0 + u < cnt ? __ldg(li + (size_t)(k0 + u) * nl.stride) : 0u;
+    float4 pb[kMaskBatch];
+#pragma unroll
+    for (int u = 0; u < kMaskBatch; ++u)
+      pb[u] = k0 + u < cnt ? __ldg(in.pos + jj[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int u = 0; u < kMaskBatch; ++u) {
+      const float3 rel = pa - xyz(pb[u]);
+      if (k0 + u < cnt && len3(rel) - (ra + pb[u].w) < 0.0f) cm |= 1u << (k0 + u);
+    }
   }
   while (cm) {
     const int k = __ffs(cm) - 1;
     cm &= cm - 1u;
-    const int j = (int)nl.idx[(size_t)k * nl.stride + i];
+    const int j = (int)li[(size_t)k * nl.stride];
     const float4 pb4 = __ldg(in.pos + j);
-    const float3 rel = pa - xyz(pb4);
-    const float dist = len3(rel);
     const float4 vb4 = __ldg(in.vel + j);
     const float4 wb4 = kSpin ? __ldg(in.angv + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float3 rel = pa - xyz(pb4);
+    const float dist = len3(rel);
     const int tb = __float_as_int(vb4.w);
     const float3 vb = xyz(vb4);
     const float3 nrm = div3_rn(rel, dist);   // = rel / dist, three correctly rounded quotients

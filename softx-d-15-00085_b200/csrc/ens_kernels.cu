@@ -305,6 +305,8 @@ __global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
 }
 
 // ------------------------------------------------------------------- step
+// candidate slots tested per batch of independent loads in the contact pass
+constexpr uint32_t kEnsMaskBatch = 4;
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
 // history words are reserved first, by every thread of the block).
 template <int kLaw, bool kCapture, bool kRecord>
@@ -357,7 +359,30 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     tv.mask[i] = mask_o;
   }
   uint32_t mask = 0;
-  for (uint32_t k = 0; k < cnt; ++k) {
+  // contacts first, candidates in batches (all index loads of a batch, then
+  // all position gathers, then the tests); then the law over the contacts
+  // alone, in list order
+  uint32_t cmask = 0;
+  for (uint32_t k0 = 0; k0 < cnt; k0 += kEnsMaskBatch) {
+    uint32_t jj[kEnsMaskBatch];
+#pragma unroll
+    for (uint32_t u = 0; u < kEnsMaskBatch; ++u)
+      jj[u] = k0 + u < cnt ? __ldg(L.idx + (size_t)(k0 + u) * stride + i) : 0u;
+    float4 pb[kEnsMaskBatch];
+#pragma unroll
+    for (uint32_t u = 0; u < kEnsMaskBatch; ++u)
+      pb[u] = k0 + u < cnt ? __ldg(in.pos + jj[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (uint32_t u = 0; u < kEnsMaskBatch; ++u) {
+      const float3 rel = pa - xyz(pb[u]);
+      const float sr = ra + pb[u].w;
+      const float d2 = dot3(rel, rel);
+      if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f) cmask |= 1u << (k0 + u);
+    }
+  }
+  while (cmask) {
+    const uint32_t k = (uint32_t)(__ffs(cmask) - 1);
+    cmask &= cmask - 1u;
     const size_t sk = (size_t)k * stride + i;
     const uint32_t j = L.idx[sk];
     const float4 pb4 = __ldg(in.pos + j);
