@@ -73,10 +73,17 @@ struct blaze_sim {
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;          // captures the IF-node bodies
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // kGraphSteps steps, starting at cur = 0 / 1
+  // with a skin: one block of kGraphSteps steps per kind (BlockKind), per start
+  cudaGraphExec_t block[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int* h_dec = nullptr;                // pinned: the gate's (exact, gate_r) of a block start
   int* d_rb = nullptr;                 // per graph step: nonzero when that step re-sorted
+  uint32_t* d_chk = nullptr;           // list-check maxima slots (StepCtl::chk)
   bool spin_free = false;              // rotation off and every angular velocity zero
   int key_bits = 1;
   long long steps = 0;
+  // with a skin, steps below this index each end with a list check (from a
+  // forced re-sort to the next multiple of kListCheckEvery; see force_check)
+  long long check_until = 0;
   int stepc = 0;        // steps since the last removal check
   uint32_t status = 0;  // accumulated, reported at sync points
   int last_launches = 0;
@@ -121,7 +128,7 @@ struct blaze_sim {
 
 namespace {
 
-constexpr int kGraphSteps = 8;
+constexpr int kGraphSteps = kListCheckEvery;
 blaze_sim* g_default = nullptr;
 
 void drop_graphs(blaze_sim* s);
@@ -548,6 +555,18 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
   return k;
 }
 
+// the list check's look-ahead distance per unit speed (list_needs_rebuild)
+float list_look(const blaze_sim* s) { return 2.0f * kListCheckEvery * s->si.InitalDelta_t; }
+
+// After a forced re-sort (new state, fill wave, removal, new options) the
+// next regular check may be up to kListCheckEvery steps away and nothing has
+// looked ahead from the new state: every step up to the next multiple of
+// kListCheckEvery ends with a check, and those steps run as plain steps in
+// both stepping modes, so graph and plain stepping re-sort at the same steps.
+void force_check(blaze_sim* s) {
+  s->check_until = (s->steps / kListCheckEvery + 1) * kListCheckEvery;
+}
+
 // Fill_State and the wave control of Device_DEM_UpdateSim
 // (DeviceInterface.cu:1055-1110, 1840-1866): before a step, either the next
 // wave joins (the counter passed the clearing time, or nothing is in the
@@ -562,6 +581,7 @@ int fill_wave(blaze_sim* s) {
       CK(cudaMemcpy(&s->h_ctl->n_cur, &s->ctl->n_cur, sizeof(int), cudaMemcpyDeviceToHost));
       s->h_ctl->n_cur = s->fill_n;
       s->h_ctl->rebuild_req = 1;
+      force_check(s);
       CK(cudaMemcpy(&s->ctl->n_cur, &s->h_ctl->n_cur, sizeof(int), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(&s->ctl->rebuild_req, &s->h_ctl->rebuild_req, sizeof(int),
                     cudaMemcpyHostToDevice));
@@ -579,11 +599,16 @@ int enqueue_step(blaze_sim* s) {
     if (rc) return rc;
   }
   if (s->profile) prof_event(s, 0);
-  launch_gate(s->ctl, s->stream);
+  const int block_start = (int)(s->opt.skin > 0.0f && s->steps % kListCheckEvery == 0 &&
+                                s->steps >= s->check_until);
+  launch_gate(s->ctl, s->stream, s->opt.skin, list_look(s), block_start);
   int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
   if (rc) return rc;
   if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
-  s->last_launches += 1 + enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0}, s->stream);
+  const int check_next =
+      (int)((s->steps + 1) % kListCheckEvery == 0 || s->steps < s->check_until);
+  s->last_launches +=
+      1 + enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0, check_next}, s->stream);
   if (s->profile) prof_event(s, 1);
   s->cur ^= 1;
   s->steps++;
@@ -593,6 +618,7 @@ int enqueue_step(blaze_sim* s) {
     if (s->stepc >= 1000) {
       launch_kill(s->S[s->cur], s->ob, s->n_max, s->si.Silo_Kill_Height,
                   s->si.Rotating_WObject ? 1 : 0, s->si.max_size, s->ctl, s->stream);
+      force_check(s);
       s->last_launches += 1;
       s->stepc = 0;
     }
@@ -604,15 +630,58 @@ void drop_graphs(blaze_sim* s) {
   for (int c = 0; c < 2; ++c) {
     if (s->graph[c]) cudaGraphExecDestroy(s->graph[c]);
     s->graph[c] = nullptr;
+    for (int k = 0; k < 3; ++k) {
+      if (s->block[c][k]) cudaGraphExecDestroy(s->block[c][k]);
+      s->block[c][k] = nullptr;
+    }
   }
 }
 
-// kGraphSteps steps as one CUDA graph, starting from S[c].  A one-thread
-// gate kernel carries the rebuild request of the previous launch into the
-// first step's IF node; every later step's IF condition is set by the step
-// kernel before it (any particle past half the skin sets it).  An IF body
-// marks its step in d_rb, then re-sorts and rebuilds the neighbour list.
-// Steps that keep the list launch only the fused step kernel.
+// Adds to the graph being captured on `cs` a conditional node of `nbody`
+// bodies (1: IF, 2: IF/ELSE) on handle h; returns the bodies.
+int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, int nbody,
+                    cudaGraph_t* bodies) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t capg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  CK(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capg, &deps, &ndeps));
+  alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
+  std::memset(cp_raw, 0, sizeof(cp_raw));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = (unsigned)nbody;
+  cudaGraphNode_t cnode;
+  CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+  for (int b = 0; b < nbody; ++b) bodies[b] = cp.conditional.phGraph_out[b];
+  CK(cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies));
+  return 0;
+}
+
+// An IF node on h (captured on `cs`) whose body, captured on `bs`, marks
+// step k in d_rb, then re-sorts and rebuilds the neighbour list.
+int add_rebuild_if(blaze_sim* s, cudaStream_t cs, cudaStream_t bs, cudaGraphConditionalHandle h,
+                   int k) {
+  cudaGraph_t body = nullptr;
+  int rc = add_conditional(cs, h, 1, &body);
+  if (rc) return rc;
+  CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  CK(cudaMemsetAsync(s->d_rb + k, 0x01, sizeof(int), bs));
+  rc = enqueue_rebuild(s, nullptr, bs);
+  cudaGraph_t tmp = nullptr;
+  CK(cudaStreamEndCapture(bs, &tmp));
+  return rc;
+}
+
+// kGraphSteps steps as one CUDA graph, starting from S[c], without a skin
+// (the reference re-sorts every step): a one-thread gate kernel carries the
+// re-sort request of the previous launch into the first step's IF node, and
+// every later step's IF condition is set by the step kernel before it.  An
+// IF body marks its step in d_rb, then re-sorts and rebuilds the neighbour
+// list.  Steps that keep the list launch only the fused step kernel.
 int build_graph(blaze_sim* s, int c) {
   const int saved = s->cur;
   s->cur = c;
@@ -624,41 +693,56 @@ int build_graph(blaze_sim* s, int c) {
   CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
   launch_gate_graph(s->ctl, h[0], s->d_rb, kGraphSteps, s->stream);
-  for (int k = 0; k < kGraphSteps; ++k) {
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t capg = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    CK(cudaStreamGetCaptureInfo(s->stream, &cs, nullptr, &capg, &deps, &ndeps));
-    alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
-    std::memset(cp_raw, 0, sizeof(cp_raw));
-    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h[k];
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cnode;
-    CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    CK(cudaStreamUpdateCaptureDependencies(s->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
-    CK(cudaStreamBeginCaptureToGraph(s->aux, body, nullptr, nullptr, 0,
-                                     cudaStreamCaptureModeThreadLocal));
-    CK(cudaMemsetAsync(s->d_rb + k, 0x01, sizeof(int), s->aux));
-    int rc = enqueue_rebuild(s, nullptr, s->aux);
-    cudaGraph_t tmp = nullptr;
-    CK(cudaStreamEndCapture(s->aux, &tmp));
-    if (rc) return rc;
-    const StepLink link = k + 1 < kGraphSteps ? StepLink{s->d_rb + k, h[k + 1], 1}
-                                               : StepLink{s->d_rb + k, 0, 0};
+  int rc = 0;
+  for (int k = 0; k < kGraphSteps && !rc; ++k) {
+    rc = add_rebuild_if(s, s->stream, s->aux, h[k], k);
+    const StepLink link = k + 1 < kGraphSteps ? StepLink{s->d_rb + k, h[k + 1], 1, 1}
+                                               : StepLink{s->d_rb + k, 0, 0, 1};
     enqueue_step_kernels(s, link, s->stream);
     s->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
   CK(cudaStreamEndCapture(s->stream, &out));
-  CK(cudaGraphInstantiate(&s->graph[c], out, 0));
+  if (!rc) CK(cudaGraphInstantiate(&s->graph[c], out, 0));
   CK(cudaGraphDestroy(out));
   s->cur = saved;
-  return 0;
+  return rc;
+}
+
+// With a skin, graph stepping runs one block of kListCheckEvery steps per
+// launch (list_needs_rebuild).  The block-start gate runs on its own and the
+// host reads its decision, then launches the graph of that kind: conditional
+// nodes cost more than a host round trip per block, so the blocks that keep
+// the list hold nothing but the step kernels.
+enum BlockKind { kBlockKeep = 0, kBlockResort = 1, kBlockExact = 2 };
+
+int build_block(blaze_sim* s, int c, int kind) {
+  const int saved = s->cur;
+  s->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  const int n_if = kind == kBlockExact ? kGraphSteps : 0;
+  cudaGraphConditionalHandle h[kGraphSteps];
+  for (int k = 0; k < n_if; ++k)
+    CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  if (kind == kBlockResort) rc = enqueue_rebuild(s, nullptr, s->stream);
+  if (kind == kBlockExact) launch_gate_body(s->ctl, h[0], s->stream);
+  for (int k = 0; k < kGraphSteps && !rc; ++k) {
+    if (k < n_if) rc = add_rebuild_if(s, s->stream, s->aux, h[k], k);
+    const StepLink link = k + 1 < n_if ? StepLink{s->d_rb + k, h[k + 1], 1, 0}
+                                        : StepLink{s->d_rb + k, 0, 0, (int)(k + 1 == kGraphSteps)};
+    enqueue_step_kernels(s, link, s->stream);
+    s->cur ^= 1;
+  }
+  cudaGraph_t out = nullptr;
+  CK(cudaStreamEndCapture(s->stream, &out));
+  if (!rc) CK(cudaGraphInstantiate(&s->block[c][kind], out, 0));
+  CK(cudaGraphDestroy(out));
+  s->cur = saved;
+  return rc;
 }
 
 int graph_steps(blaze_sim* s, int nsteps) {
@@ -666,21 +750,39 @@ int graph_steps(blaze_sim* s, int nsteps) {
   while (done < nsteps) {
     // removal checks and odd tails run as plain steps
     const bool kill_soon = s->si.Kill_Particles && s->stepc + kGraphSteps >= 1000;
-    if (nsteps - done < kGraphSteps || kill_soon) {
+    // with a skin a graph starts on a list check (a multiple of kListCheckEvery)
+    const bool off_cadence =
+        s->opt.skin > 0.0f && (s->steps % kListCheckEvery != 0 || s->steps < s->check_until);
+    if (nsteps - done < kGraphSteps || kill_soon || off_cadence) {
       int rc = enqueue_step(s);
       if (rc) return rc;
       done += 1;
       continue;
     }
     const int c = s->cur;
-    if (!s->graph[c]) {
-      int rc = build_graph(s, c);
-      if (rc) return rc;
+    if (s->opt.skin > 0.0f) {
+      // the block-start gate (the decision of plain stepping's gate), read back
+      launch_gate_decide(s->ctl, s->d_rb, kGraphSteps, s->opt.skin, list_look(s), s->stream);
+      CK(cudaMemcpyAsync(s->h_dec, &s->ctl->exact, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                         s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      const int kind = s->h_dec[0] ? kBlockExact : (s->h_dec[1] ? kBlockResort : kBlockKeep);
+      if (!s->block[c][kind]) {
+        int rc = build_block(s, c, kind);
+        if (rc) return rc;
+      }
+      CK(cudaGraphLaunch(s->block[c][kind], s->stream));
+      s->last_launches += 1 + (kind == kBlockExact ? 1 : 0) + kGraphSteps * (s->poly ? 5 : 1);
+    } else {
+      if (!s->graph[c]) {
+        int rc = build_graph(s, c);
+        if (rc) return rc;
+      }
+      CK(cudaGraphLaunch(s->graph[c], s->stream));
+      // launches that always run: the gate and the step kernels of each step
+      // (re-sort bodies run only when a step asks for them)
+      s->last_launches += 1 + kGraphSteps * (s->poly ? 5 : 1);
     }
-    CK(cudaGraphLaunch(s->graph[c], s->stream));
-    // launches that always run: the gate and the step kernels of each step
-    // (re-sort bodies run only when a step asks for them)
-    s->last_launches += 1 + kGraphSteps * (s->poly ? 5 : 1);
     s->steps += kGraphSteps;
     if (s->si.Kill_Particles) s->stepc += kGraphSteps;
     if (kGraphSteps & 1) s->cur ^= 1;
@@ -733,6 +835,8 @@ int set_state_impl(blaze_sim* s, const float* pos3, const float* quat4, const fl
   c.n_cur = n;
   c.pending_dead = dead;
   *s->h_ctl = c;
+  CK(cudaMemsetAsync(s->d_chk, 0, sizeof(uint32_t) * 2 * kChkSlots * kChkStride, s->stream));
+  force_check(s);
   CK(cudaMemcpyAsync(s->ctl, s->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
@@ -765,10 +869,11 @@ void free_sim(blaze_sim* s) {
   for (int b = 0; b < 3; ++b) { f(s->S[b].pos); f(s->S[b].vel); f(s->S[b].angv); }
   for (int b = 0; b < 2; ++b) { f(s->ob.pid[b]); f(s->ob.lift[b]); f(s->rs.keys[b]); f(s->rs.vals[b]); }
   f(s->rs.counts); f(s->rs.totals); f(s->cstart); f(s->cend); f(s->nl.idx); f(s->nl.cnt);
-  f(s->ctl); f(s->d_rb); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
+  f(s->ctl); f(s->d_rb); f(s->d_chk); f(s->dp); f(s->d_ops); f(s->d_wall_off); f(s->d_wall_idx);
   f(s->d_tally); f(s->d_eb); f(s->d_epart);
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_dec) cudaFreeHost(s->h_dec);
   f(s->stage.pos3); f(s->stage.vel3); f(s->stage.avel3); f(s->stage.type); f(s->stage.pid);
   f(s->stage.flags); f(s->stage.quat4);
   f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
@@ -778,6 +883,7 @@ void free_sim(blaze_sim* s) {
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->aux) cudaStreamDestroy(s->aux);
   delete s;
 }
 
@@ -942,9 +1048,14 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->stage.pid, n));
   CKF(dalloc(&s->stage.flags, 2));
   CKF(cudaMallocHost((void**)&s->h_flags, 2 * sizeof(int)));
+  CKF(cudaMallocHost((void**)&s->h_dec, 2 * sizeof(int)));
   std::memset(s->h_ctl, 0, sizeof(StepCtl));
+  CKF(dalloc(&s->d_chk, (size_t)2 * kChkSlots * kChkStride));
+  CKF(cudaMemset(s->d_chk, 0, sizeof(uint32_t) * 2 * kChkSlots * kChkStride));
+  s->h_ctl->chk = s->d_chk;
   s->h_ctl->n_cur = n;
   s->h_ctl->rebuild_req = 1;
+  force_check(s);
   CKF(cudaMemcpy(s->ctl, s->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice));
   int rc = upload_params(s);
   if (rc) return fail(rc);
@@ -1023,6 +1134,7 @@ int blaze_set_options(blaze_sim* s, const blaze_options* opt) {
   if (!rc) rc = upload_params(s);
   // a new skin or capacity invalidates the current list
   s->h_ctl->rebuild_req = 1;
+  force_check(s);
   CK(cudaMemcpy(&s->ctl->rebuild_req, &s->h_ctl->rebuild_req, sizeof(int), cudaMemcpyHostToDevice));
   return rc;
 }

@@ -38,6 +38,8 @@ enum StatusBits : uint32_t {
   kStatusTimeout = 16u,       // a bounded device wait gave up
   kStatusPolyUndefined = 32u, // a polyhedron contact met a case the reference
                               // leaves undefined (see poly_kernels.cu)
+  kStatusStaleList = 64u,     // with a skin: a particle passed half the skin
+                              // between two list checks (contacts may be missed)
 };
 
 // One step of the wall program: planar faces, infinite planes, a macro

@@ -45,17 +45,75 @@ __device__ __forceinline__ void flag_status(StepCtl* ctl, uint32_t bits) {
 }
 
 // --------------------------------------------------------------------- gate
-__global__ void k_gate(StepCtl* ctl) {
-  const int r = ctl->rebuild_req;
+// A list check prepared by the step before (maxima nonzero) re-sorts when a
+// particle might pass half the skin before the next check.
+// The gate of a step, run by kChkSlots threads (thread 0 decides): the
+// re-sort request, and with a skin the maxima recorded by the step before it
+// (nonzero only then), which ask for a re-sort when a particle might pass
+// half the skin before the next check; at a block start also the block's
+// mode (list_needs_rebuild).  Returns the decision in thread 0.
+__device__ __forceinline__ int gate_request(StepCtl* ctl, float skin, float look,
+                                            int block_start) {
+  __shared__ uint32_t sp[kChkSlots / 32], sv[kChkSlots / 32];
+  const int t = threadIdx.x;
+  uint32_t p = 0u, v = 0u;
+  if (skin > 0.0f && ctl->chk) {
+    uint32_t* cp = ctl->chk + t * kChkStride;
+    uint32_t* cv = ctl->chk + (kChkSlots + t) * kChkStride;
+    p = *cp;
+    v = *cv;
+    if (p) *cp = 0u;
+    if (v) *cv = 0u;
+  }
+  p = __reduce_max_sync(0xffffffffu, p);
+  v = __reduce_max_sync(0xffffffffu, v);
+  if ((t & 31) == 0) {
+    sp[t >> 5] = p;
+    sv[t >> 5] = v;
+  }
+  __syncthreads();
+  if (t != 0) return 0;
+  for (int w = 1; w < kChkSlots / 32; ++w) {
+    p = max(p, sp[w]);
+    v = max(v, sv[w]);
+  }
+  int r = ctl->rebuild_req;
+  float vm = 0.0f;
+  if (p | v) {
+    const float pm = __uint_as_float(p);
+    vm = __uint_as_float(v);
+    if (!(pm + look * vm <= 0.5f * skin)) r = 1;
+  }
+  if (block_start) ctl->exact = (skin > 0.0f && !(look * vm <= 0.25f * skin)) ? 1 : 0;
+  return r;
+}
+
+__global__ void k_gate(StepCtl* ctl, float skin, float look, int block_start) {
+  const int r = gate_request(ctl, skin, look, block_start);
+  if (threadIdx.x != 0) return;
   ctl->rebuilt = r;
   ctl->rebuild_req = 0;
+}
+
+__global__ void k_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look) {
+  const int r = gate_request(ctl, skin, look, 1);
+  if (threadIdx.x != 0) return;
+  ctl->rebuild_req = 0;
+  ctl->gate_r = r;
+  for (int k = 0; k < nrb; ++k) rb[k] = k == 0 ? r : 0;
+}
+
+__global__ void k_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0) {
+  cudaGraphSetConditional(h0, ctl->gate_r ? 1u : 0u);
 }
 
 // First node of a step graph: latch the request carried over from the last
 // launch into the first step's IF condition and clear the per-step
 // "re-sorted" flags (an IF body marks its own step).
-__global__ void k_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb) {
-  const int r = ctl->rebuild_req;
+__global__ void k_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
+                             float skin, float look) {
+  const int r = gate_request(ctl, skin, look, 0);
+  if (threadIdx.x != 0) return;
   ctl->rebuild_req = 0;
   for (int k = 0; k < nrb; ++k) rb[k] = 0;
   cudaGraphSetConditional(h0, r ? 1u : 0u);
@@ -331,6 +389,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   const bool rebuilt = *link.rebuilt != 0;
   const StateBuf in = rebuilt ? in_sorted : in_plain;
   const int n = ctl->n_cur;
+  const int exact = ctl->exact;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_max) return;
   if (i >= n) {  // removed particles keep their parked state
@@ -478,11 +537,11 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
   out.angv[i] = make_float4(w.x, w.y, w.z, path);
   if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
 
-  // Verlet-list validity: rebuild before any particle has moved half the
-  // skin; with no skin the contact list is rebuilt every step (reference).
+  // Verlet-list validity (list_needs_rebuild); with no skin the contact list
+  // is rebuilt every step (reference).
   {
     const unsigned m = __activemask();
-    const bool need = P.skin <= 0.0f || path > 0.5f * P.skin;
+    const bool need = list_needs_rebuild(P.skin, link, exact, path, len3(v), ctl, st);
     const unsigned b = __ballot_sync(m, need);
     if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) {
       if (link.has_next_h) cudaGraphSetConditional(link.next_h, 1u);
@@ -760,11 +819,21 @@ inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
 
-void launch_gate(StepCtl* ctl, cudaStream_t st) { k_gate<<<1, 1, 0, st>>>(ctl); }
+void launch_gate(StepCtl* ctl, cudaStream_t st, float skin, float look, int block_start) {
+  k_gate<<<1, kChkSlots, 0, st>>>(ctl, skin, look, block_start);
+}
+
+void launch_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look, cudaStream_t st) {
+  k_gate_decide<<<1, kChkSlots, 0, st>>>(ctl, rb, nrb, skin, look);
+}
+
+void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st) {
+  k_gate_body<<<1, 1, 0, st>>>(ctl, h0);
+}
 
 void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
-                       cudaStream_t st) {
-  k_gate_graph<<<1, 1, 0, st>>>(ctl, h0, rb, nrb);
+                       cudaStream_t st, float skin, float look) {
+  k_gate_graph<<<1, kChkSlots, 0, st>>>(ctl, h0, rb, nrb, skin, look);
 }
 
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,

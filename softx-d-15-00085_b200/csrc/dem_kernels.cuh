@@ -32,6 +32,10 @@ struct StepCtl {        // device words the step pipeline communicates through
   int pending_dead;     // removed since the last re-sort
   int killed_total;
   int pad;
+  uint32_t* chk;        // with a skin: kChkSlots maxima of path, then of speed (float
+                        // bits, one per 128-byte line), recorded at the step before a check
+  int exact;            // with a skin: 1 = this block of steps checks before every step
+  int gate_r;           // the gate's re-sort decision, for the first IF of a graph body
 };
 
 struct NbrList {
@@ -50,7 +54,55 @@ struct StepLink {
   const int* rebuilt;                  // nonzero: read the sorted buffer
   cudaGraphConditionalHandle next_h;   // next step's IF condition (graph)
   int has_next_h;                      // 0: request through StepCtl::rebuild_req
+  int check_next;                      // with a skin: the next step starts with a list check
 };
+
+// With a Verlet skin the sphere and polyhedron paths run in blocks of
+// kListCheckEvery steps, blocks starting on multiples of it (counted from the
+// simulation's first step).  The step before a block start records the
+// largest path since the last re-sort and the largest speed; the gate of the
+// block start re-sorts when path_max + look speed_max exceeds half the skin
+// (look = 2 kListCheckEvery dt: a particle at rest struck by the fastest one
+// reaches at most about twice its speed), and picks the block's mode:
+//   fast   (look speed_max <= skin / 4: a fresh list outlasts the block with
+//          a factor of two to spare): no check inside the block; every step
+//          verifies that no particle has passed half the skin (the bound
+//          under which the list holds every contact) and raises
+//          kStatusStaleList if one has;
+//   exact  (otherwise): a check before every step, re-sorting when a
+//          particle has passed half the skin, as without blocks.
+// From a forced re-sort (new state, fill wave, removal, new options) to the
+// next block start every step ends with a recorded check, so a state that
+// starts fast is looked at before its first unchecked step.
+constexpr int kListCheckEvery = 8;
+// The maxima are spread over kChkSlots words (warp w adds to slot
+// w % kChkSlots), so that the atomics of a million particles do not queue on
+// one address; the gate reduces the slots with kChkSlots threads.
+constexpr int kChkSlots = 128;
+constexpr int kChkStride = 32;   // words between slots (one 128-byte line each)
+// Returns whether this particle asks for a re-sort before the next step
+// (always without a skin); with a skin and check_next, adds its path and
+// speed to the maxima instead (one atomic per warp; the gate decides).
+__device__ __forceinline__ bool list_needs_rebuild(float skin, const StepLink& link, int exact,
+                                                   float path, float speed, StepCtl* ctl,
+                                                   uint32_t& st) {
+  if (skin <= 0.0f) return true;
+  if (link.check_next) {
+    const unsigned m = __activemask();
+    const uint32_t pm = __reduce_max_sync(m, __float_as_uint(fmaxf(path, 0.0f)));
+    const uint32_t vm = __reduce_max_sync(m, __float_as_uint(fmaxf(speed, 0.0f)));
+    if ((threadIdx.x & 31) == (__ffs(m) - 1) && ctl->chk) {
+      const uint32_t slot =
+          ((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % kChkSlots) * kChkStride;
+      atomicMax(ctl->chk + slot, pm);
+      atomicMax(ctl->chk + kChkSlots * kChkStride + slot, vm);
+    }
+    return false;
+  }
+  if (exact) return path > 0.5f * skin;
+  if (path > 0.5f * skin) st |= kStatusStaleList;
+  return false;
+}
 
 struct WallGrid {       // per-cell candidate wall ops (CSR), optional
   const uint32_t* off;  // ncell_tab + 1 entries, or null = test every op
@@ -71,9 +123,19 @@ struct HostStage {
   int* flags;
 };
 
-void launch_gate(StepCtl* ctl, cudaStream_t st);
+// skin > 0: the gate also re-sorts when the maxima recorded by the step
+// before it say so, and at a block start picks the block's mode
+// (list_needs_rebuild); look = 2 kListCheckEvery dt.
+void launch_gate(StepCtl* ctl, cudaStream_t st, float skin = 0.0f, float look = 0.0f,
+                 int block_start = 0);
 void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
-                       cudaStream_t st);
+                       cudaStream_t st, float skin = 0.0f, float look = 0.0f);
+// Block-start gate of skin > 0 graph stepping, launched on its own: the
+// decision goes to ctl->gate_r (and rb[0]; rb[1..nrb) are cleared), the
+// block's mode to ctl->exact; an exact block's first IF takes ctl->gate_r
+// through launch_gate_body.
+void launch_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look, cudaStream_t st);
+void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
 // (flat_n, when given, is reset for the contact-list kernel's flat list)

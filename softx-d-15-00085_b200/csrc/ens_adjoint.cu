@@ -268,6 +268,32 @@ __global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
   c->lsnap = c->cur;
 }
 
+// Slots k < cnt of a particle's list whose spheres overlap (the forward's
+// test, d2 < (ra + rb)^2 and |rel| > 0), as a bit mask; the candidates in
+// batches of four: the entries, then the position gathers, then the tests.
+__device__ __forceinline__ uint32_t contact_mask(const uint2* ent, uint32_t cnt,
+                                                 const float4* pos, float3 xa, float ra) {
+  constexpr uint32_t kB = 4;
+  uint32_t cm = 0;
+  for (uint32_t k0 = 0; k0 < cnt; k0 += kB) {
+    uint32_t jj[kB];
+#pragma unroll
+    for (uint32_t u = 0; u < kB; ++u) jj[u] = k0 + u < cnt ? ent[k0 + u].x : 0u;
+    float4 pb[kB];
+#pragma unroll
+    for (uint32_t u = 0; u < kB; ++u)
+      pb[u] = k0 + u < cnt ? pos[jj[u]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (uint32_t u = 0; u < kB; ++u) {
+      const float3 rel = xa - xyz4(pb[u]);
+      const float sr = ra + pb[u].w;
+      const float d2 = dot3(rel, rel);
+      if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f) cm |= 1u << (k0 + u);
+    }
+  }
+  return cm;
+}
+
 // --------------------------------------------------------------- reverse
 // The step backwards, per particle: symplectic Euler (v' = v + (f/m + g) dt,
 // x' = x + v' dt, w' = w + t/I dt) gives the cotangents of the particle's
@@ -296,16 +322,18 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   LawBar th = {0.0f, 0.0f, 0.0f, 0.0f};
   float mu_wb = 0.0f;
   const uint32_t cnt = lv.cnt[i], mask = tv.mask[i];
-  for (uint32_t k = 0; k < cnt; ++k) {
+  // the slots in contact first (batched loads, as in the forward), then the
+  // contacts and the slots that held a history, in slot order
+  const uint32_t cm = contact_mask(ent, cnt, tv.pos, A.x, A.r);
+  for (uint32_t todo = cm | (mask & ((cnt >= 32u ? 0u : (1u << cnt)) - 1u)); todo;
+       todo &= todo - 1u) {
+    const uint32_t k = (uint32_t)(__ffs(todo) - 1);
     const size_t sl = (size_t)k * n + i;          // cotangent slot (one step)
-    const uint32_t j = ent[k].x;
-    const float4 pb = tv.pos[j];
-    const float3 rel = A.x - xyz4(pb);
-    const float sr = A.r + pb.w;
-    const float d2 = dot3(rel, rel);
     const bool had = (mask >> k) & 1u;
     float4 hout = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (d2 < sr * sr && sqrtf(d2) > 0.0f) {
+    if ((cm >> k) & 1u) {
+      const uint32_t j = ent[k].x;
+      const float4 pb = tv.pos[j];
       const float4 vb = tv.vel[j], wb = tv.angv[j];
       Body B;
       B.x = xyz4(pb);
@@ -394,14 +422,10 @@ k_adj_gather(EnsTape tp, int t, int n, AdjBufs a) {
   const float3 xa = xyz4(pa);
   float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
   const uint32_t cnt = lv.cnt[i];
-  for (uint32_t k = 0; k < cnt; ++k) {
+  for (uint32_t cm = contact_mask(ent, cnt, tv.pos, xa, pa.w); cm; cm &= cm - 1u) {
+    const uint32_t k = (uint32_t)(__ffs(cm) - 1);
     const uint2 e = ent[k];
     const uint32_t j = e.x;
-    const float4 pb = tv.pos[j];
-    const float3 rel = xa - xyz4(pb);
-    const float sr = pa.w + pb.w;
-    const float d2 = dot3(rel, rel);
-    if (!(d2 < sr * sr && sqrtf(d2) > 0.0f)) continue;
     const uint32_t q = e.y & 0xffu;
     if (q == 0xffu) continue;
     const size_t sj = (size_t)q * n + j;

@@ -1333,7 +1333,7 @@ k_poly_step(const SimParams* __restrict__ Pg, const PolyShape* __restrict__ shap
   // Verlet-list validity on the bounding spheres, as for spheres
   {
     const unsigned m = __activemask();
-    const bool need = P.skin <= 0.0f || path > 0.5f * P.skin;
+    const bool need = list_needs_rebuild(P.skin, link, ctl->exact, path, len3(v), ctl, st);
     const unsigned b = __ballot_sync(m, need);
     if (b && (threadIdx.x & 31) == (__ffs(m) - 1)) {
       if (link.has_next_h) cudaGraphSetConditional(link.next_h, 1u);
