@@ -169,6 +169,28 @@ def test_graph_stepping_is_exact(silo_small, skin):
         np.testing.assert_array_equal(a[key], b[key])
 
 
+def test_graph_stepping_exact_blocks_fast_state(box):
+    """A state too fast for an 8-step block without list checks (speeds
+    N(0, 300 cm/s) against a 0.02 cm skin at dt 1e-5 s): the blocks run
+    exact, with a check before every step.  Graph and plain stepping re-sort
+    at the same steps and agree bit for bit, and no stale-list status is
+    raised."""
+    P, st0 = box
+    vel = np.random.default_rng(7).normal(scale=300.0, size=st0["vel"].shape).astype(np.float32)
+    out = []
+    for g in (0, 1):
+        s = device.Simulation(P, skin=0.02, use_graph=g)
+        s.set_state(st0["pos"], vel, st0["avel"], st0["type"], st0["pid"])
+        s.step(67)
+        out.append((s.state(), s.num_rebuilds()))
+        s.close()
+    (a, ra), (b, rb) = out
+    assert a["status"] == 0 and b["status"] == 0, device.decode_status(a["status"] | b["status"])
+    assert ra == rb and ra > 67 // 8
+    for key in ("pos", "vel", "avel", "pid"):
+        np.testing.assert_array_equal(a[key], b[key])
+
+
 @pytest.mark.gpu
 def test_shared_reciprocal_division_is_ieee():
     """div3_rn (one correctly rounded reciprocal + two corrections per
