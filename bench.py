@@ -353,7 +353,8 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
         P, st = synth.poly_box_project(d, n=n)
     sim = device.Simulation(P, skin=skin, use_graph=1)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
-    sim.step(max(3, warmup))
+    sim.prepare_graphs()
+    sim.step(max(16, -(-warmup // 8) * 8))
     status = sim.sync()
     stream = torch.cuda.ExternalStream(sim.device_state()[3])
     a = torch.cuda.Event(enable_timing=True)
@@ -424,7 +425,8 @@ def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=Tru
     sim.set_cylinder_rotation(True)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     sim.set_dobj_rotation(R, R, rad)
-    sim.step(max(3, warmup))
+    sim.prepare_graphs()
+    sim.step(max(16, -(-warmup // 8) * 8))
     status = sim.sync()
     sim.reset_energy()
     stream = torch.cuda.ExternalStream(sim.device_state()[3])
@@ -630,7 +632,13 @@ def main():
         st = dict(pos=settled["pos"], vel=settled["vel"], avel=settled["avel"],
                   type=settled["type"], pid=settled["pid"])
     sim.open_hatch()  # the discharge: the last world object (hatch) is dropped
-    sim.step(args.warmup)
+    # every graph is instantiated before the timed region; the warm-up runs
+    # at least W steps and ends on a block start (a multiple of 8 steps past
+    # the 8 checked steps that follow setting a state), so the timed region
+    # opens with a whole block
+    sim.prepare_graphs()
+    warm = max(16, -(-args.warmup // 8) * 8)
+    sim.step(warm)
     status = sim.sync()
     stream = torch.cuda.ExternalStream(sim.device_state()[3])
 
@@ -644,6 +652,7 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     rb0 = sim.num_rebuilds()
+    x0 = sim.num_exact_blocks()
     e0.record(stream)
     sim.step(args.steps)
     e1.record(stream)
@@ -653,7 +662,9 @@ def main():
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     rebuilds = sim.num_rebuilds() - rb0
-    launches = fixed_launches + rebuilds * sim.rebuild_kernels()
+    exact_blocks = sim.num_exact_blocks() - x0
+    # unconditional launches + re-sort bodies + the exact mode's extra gate
+    launches = fixed_launches + rebuilds * sim.rebuild_kernels() + exact_blocks
     status |= sim.sync()
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -759,6 +770,8 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "rebuilds_in_timed_region": rebuilds,
+            "exact_blocks_in_timed_region": exact_blocks,
+            "warmup_steps_run": warm,
             "rebuild_ms_per_step": ms_rebuild / max(nsteps, 1),
             "reference_mode_value": ref_mode_value,
             "silo_full": silo_full,

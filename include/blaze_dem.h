@@ -13,7 +13,9 @@
  *          4 non-finite state, 8 particle type outside the table,
  *          16 bounded device wait gave up, 32 a polyhedron contact met a
  *          case the reference leaves undefined and got the library's
- *          defined result)
+ *          defined result, 64 with a neighbour-list skin: a particle passed
+ *          half the skin inside a block of steps with no list check, so
+ *          contacts may have been missed)
  *       <0 -(1000 + cudaError_t) for a CUDA error, -1 bad argument,
  *          -2 no simulation set up
  *   - Device_DEM_UpdateSim only enqueues the step on the library's stream;
@@ -31,6 +33,10 @@
 #define BLAZE_DEM_H_
 
 #include "blaze_types.h"
+
+#ifndef __cplusplus
+#include <stdbool.h> /* drum_rotation(bool) */
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -120,8 +126,20 @@ int blaze_set_state_ornt(blaze_sim* s, const float* pos3, const float* quat4, co
                          const float* avel3, const uint* type, const int* pid);
 int blaze_get_state_ornt(blaze_sim* s, float* pos3, float* quat4, float* vel3, float* avel3,
                          uint* type, int* pid);
-/* Enqueue nsteps steps (asynchronous unless sync_each_step). */
+/* Enqueue nsteps steps (asynchronous unless sync_each_step; with
+ * use_graph = 1 no step waits for the host: the list checks of a skin are
+ * decided on the device).  With use_graph = 1 the graphs are built on first
+ * use; blaze_prepare_graphs builds them ahead. */
 int blaze_step(blaze_sim* s, int nsteps);
+/* Instantiate every CUDA graph that graph stepping with the current options
+ * launches (both buffer parities; with a skin the block graph and the
+ * one-step graphs), so that no stream capture or instantiation happens
+ * inside a later blaze_step.  Changing options or moves drops them. */
+int blaze_prepare_graphs(blaze_sim* s);
+/* With a skin: blocks of steps that ran in the exact mode (a list check
+ * before every step, chosen on the device when particles are fast for the
+ * skin) since the simulation was created. */
+int blaze_num_exact_blocks(blaze_sim* s);
 /* Wait for the stream; returns the accumulated status (see Part 1). */
 int blaze_sync(blaze_sim* s);
 int blaze_num_current(blaze_sim* s);

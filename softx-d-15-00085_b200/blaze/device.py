@@ -109,6 +109,8 @@ def load():
     lib.blaze_sync.argtypes = [C.c_void_p]
     lib.blaze_num_current.argtypes = [C.c_void_p]
     lib.blaze_num_rebuilds.argtypes = [C.c_void_p]
+    lib.blaze_prepare_graphs.argtypes = [C.c_void_p]
+    lib.blaze_num_exact_blocks.argtypes = [C.c_void_p]
     lib.blaze_update_wobj.argtypes = [C.c_void_p, P(T.WOBJ), C.c_int]
     lib.blaze_update_dobj.argtypes = [C.c_void_p, P(T.DOBJ), C.c_int]
     lib.blaze_get_forces.argtypes = [C.c_void_p] + [_f] * 6
@@ -313,6 +315,14 @@ class Simulation:
 
     def num_rebuilds(self):
         return _check(self.lib.blaze_num_rebuilds(self.h), "blaze_num_rebuilds")
+
+    def prepare_graphs(self):
+        """Instantiate the CUDA graphs graph stepping will launch (no capture
+        then happens inside later steps)."""
+        _check(self.lib.blaze_prepare_graphs(self.h), "blaze_prepare_graphs")
+
+    def num_exact_blocks(self):
+        return _check(self.lib.blaze_num_exact_blocks(self.h), "blaze_num_exact_blocks")
 
     def update_wobj(self, wobj, n_w):
         _check(self.lib.blaze_update_wobj(self.h, wobj, n_w), "blaze_update_wobj")

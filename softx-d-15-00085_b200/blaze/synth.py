@@ -456,12 +456,14 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
     pos = np.zeros((n, 3), np.float64)
     types_out = np.zeros(n, np.uint32)
     k = 0
-    y = y_out + 0.05
+    y_last, r_last = None, None   # centre height and radius of the last layer laid
     for b in range(n_bins - 1, -1, -1):
         r = float(radii[b])
         pitch = 2.0 * r * (1.0 - overlap)
         need = int(counts[b])
-        y += r
+        # the first layer of a bin rests on the last layer of the bin below
+        # (the same relative overlap), so no bin starts in free fall
+        y = y_out + 0.05 + r if y_last is None else y_last + (r_last + r) * (1.0 - overlap)
         while need > 0:
             ra = (r_out + (y - y_out) * tan_a) * math.cos(math.pi / n_seg) if y < y_top else silo_r
             ra -= r / cos_a + 0.002
@@ -478,8 +480,9 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
                 types_out[k:k + cnt] = b
                 k += cnt
                 need -= cnt
+                y_last = y
             y += pitch
-        y += r * 0.002
+        r_last = r
     types = types_out
     pos = pos.astype(np.float32)
     state = dict(pos=pos, vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),

@@ -71,11 +71,15 @@ struct blaze_sim {
   ForceCapture cap{};
   bool cap_alloc = false;
   cudaStream_t stream = nullptr;
-  cudaStream_t aux = nullptr;          // captures the IF-node bodies
+  cudaStream_t aux = nullptr;          // captures conditional bodies
+  cudaStream_t aux2 = nullptr;         // captures the IF bodies nested in a SWITCH body
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // kGraphSteps steps, starting at cur = 0 / 1
-  // with a skin: one block of kGraphSteps steps per kind (BlockKind), per start
-  cudaGraphExec_t block[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
-  int* h_dec = nullptr;                // pinned: the gate's (exact, gate_r) of a block start
+  // with a skin: a block of kGraphSteps steps whose kind the device picks
+  // (build_block), per start; and one step as a graph, per start, per
+  // (block start, check after the step) (build_single)
+  cudaGraphExec_t block[2] = {nullptr, nullptr};
+  cudaGraphExec_t single[2][2][2] = {};
+  int step_launches = 0;               // kernels of one step, counted when a graph is built
   int* d_rb = nullptr;                 // per graph step: nonzero when that step re-sorted
   uint32_t* d_chk = nullptr;           // list-check maxima slots (StepCtl::chk)
   bool spin_free = false;              // rotation off and every angular velocity zero
@@ -593,26 +597,21 @@ int fill_wave(blaze_sim* s) {
   return 0;
 }
 
-int enqueue_step(blaze_sim* s) {
-  if (s->filling) {
-    int rc = fill_wave(s);
-    if (rc) return rc;
-  }
-  if (s->profile) prof_event(s, 0);
-  const int block_start = (int)(s->opt.skin > 0.0f && s->steps % kListCheckEvery == 0 &&
-                                s->steps >= s->check_until);
-  launch_gate(s->ctl, s->stream, s->opt.skin, list_look(s), block_start);
-  int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
-  if (rc) return rc;
-  if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
-  const int check_next =
-      (int)((s->steps + 1) % kListCheckEvery == 0 || s->steps < s->check_until);
-  s->last_launches +=
-      1 + enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0, check_next}, s->stream);
-  if (s->profile) prof_event(s, 1);
+// Whether the step about to run starts a block of list checks, and whether
+// it ends with a recorded check (list_needs_rebuild).
+int block_start_here(const blaze_sim* s) {
+  return (int)(s->opt.skin > 0.0f && s->steps % kListCheckEvery == 0 &&
+               s->steps >= s->check_until);
+}
+int check_after_here(const blaze_sim* s) {
+  return (int)((s->steps + 1) % kListCheckEvery == 0 || s->steps < s->check_until);
+}
+
+// After the kernels of one step: the next state is current; the removal
+// check of a silo or plant every 1000 steps (DeviceInterface.cu:2463-2498).
+void finish_step(blaze_sim* s) {
   s->cur ^= 1;
   s->steps++;
-  // silo / plant removal check every 1000 steps (DeviceInterface.cu:2463-2498)
   if (s->si.Kill_Particles) {
     s->stepc++;
     if (s->stepc >= 1000) {
@@ -623,6 +622,22 @@ int enqueue_step(blaze_sim* s) {
       s->stepc = 0;
     }
   }
+}
+
+int enqueue_step(blaze_sim* s) {
+  if (s->filling) {
+    int rc = fill_wave(s);
+    if (rc) return rc;
+  }
+  if (s->profile) prof_event(s, 0);
+  launch_gate(s->ctl, s->stream, s->opt.skin, list_look(s), block_start_here(s));
+  int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
+  if (rc) return rc;
+  if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
+  s->last_launches += 1 + enqueue_step_kernels(
+                              s, StepLink{&s->ctl->rebuilt, 0, 0, check_after_here(s)}, s->stream);
+  if (s->profile) prof_event(s, 1);
+  finish_step(s);
   return 0;
 }
 
@@ -630,17 +645,21 @@ void drop_graphs(blaze_sim* s) {
   for (int c = 0; c < 2; ++c) {
     if (s->graph[c]) cudaGraphExecDestroy(s->graph[c]);
     s->graph[c] = nullptr;
-    for (int k = 0; k < 3; ++k) {
-      if (s->block[c][k]) cudaGraphExecDestroy(s->block[c][k]);
-      s->block[c][k] = nullptr;
-    }
+    if (s->block[c]) cudaGraphExecDestroy(s->block[c]);
+    s->block[c] = nullptr;
+    for (int b = 0; b < 2; ++b)
+      for (int k = 0; k < 2; ++k) {
+        if (s->single[c][b][k]) cudaGraphExecDestroy(s->single[c][b][k]);
+        s->single[c][b][k] = nullptr;
+      }
   }
 }
 
-// Adds to the graph being captured on `cs` a conditional node of `nbody`
-// bodies (1: IF, 2: IF/ELSE) on handle h; returns the bodies.
-int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, int nbody,
-                    cudaGraph_t* bodies) {
+// Adds to the graph being captured on `cs` a conditional node of `type`
+// with `nbody` bodies (IF: 1, or 2 for IF/ELSE; SWITCH: any) on handle h;
+// returns the bodies.
+int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    int nbody, cudaGraph_t* bodies) {
   cudaStreamCaptureStatus cst;
   cudaGraph_t capg = nullptr;
   const cudaGraphNode_t* deps = nullptr;
@@ -651,7 +670,7 @@ int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, int nbody,
   cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
   cp.type = cudaGraphNodeTypeConditional;
   cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.type = type;
   cp.conditional.size = (unsigned)nbody;
   cudaGraphNode_t cnode;
   CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
@@ -661,15 +680,15 @@ int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, int nbody,
 }
 
 // An IF node on h (captured on `cs`) whose body, captured on `bs`, marks
-// step k in d_rb, then re-sorts and rebuilds the neighbour list.
+// step k in d_rb (k >= 0), then re-sorts and rebuilds the neighbour list.
 int add_rebuild_if(blaze_sim* s, cudaStream_t cs, cudaStream_t bs, cudaGraphConditionalHandle h,
                    int k) {
   cudaGraph_t body = nullptr;
-  int rc = add_conditional(cs, h, 1, &body);
+  int rc = add_conditional(cs, h, cudaGraphCondTypeIf, 1, &body);
   if (rc) return rc;
   CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
-  CK(cudaMemsetAsync(s->d_rb + k, 0x01, sizeof(int), bs));
+  if (k >= 0) CK(cudaMemsetAsync(s->d_rb + k, 0x01, sizeof(int), bs));
   rc = enqueue_rebuild(s, nullptr, bs);
   cudaGraph_t tmp = nullptr;
   CK(cudaStreamEndCapture(bs, &tmp));
@@ -698,7 +717,7 @@ int build_graph(blaze_sim* s, int c) {
     rc = add_rebuild_if(s, s->stream, s->aux, h[k], k);
     const StepLink link = k + 1 < kGraphSteps ? StepLink{s->d_rb + k, h[k + 1], 1, 1}
                                                : StepLink{s->d_rb + k, 0, 0, 1};
-    enqueue_step_kernels(s, link, s->stream);
+    s->step_launches = enqueue_step_kernels(s, link, s->stream);
     s->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
@@ -709,80 +728,148 @@ int build_graph(blaze_sim* s, int c) {
   return rc;
 }
 
-// With a skin, graph stepping runs one block of kListCheckEvery steps per
-// launch (list_needs_rebuild).  The block-start gate runs on its own and the
-// host reads its decision, then launches the graph of that kind: conditional
-// nodes cost more than a host round trip per block, so the blocks that keep
-// the list hold nothing but the step kernels.
+// With a skin, graph stepping runs blocks of kListCheckEvery steps
+// (list_needs_rebuild).  A block is one graph: the block-start gate, then a
+// SWITCH node whose body the gate picks on the device, so no block waits
+// for the host:
+//   0 keep   the kGraphSteps step kernels;
+//   1 re-sort, then the step kernels (the first reads the sorted copy);
+//   2 exact  an IF node (re-sort) before every step, set by the step before.
 enum BlockKind { kBlockKeep = 0, kBlockResort = 1, kBlockExact = 2 };
 
-int build_block(blaze_sim* s, int c, int kind) {
-  const int saved = s->cur;
+// Captures into `body` (on stream bs; nested IF bodies on bs2) the steps of
+// one block kind starting from S[c].
+int capture_block_body(blaze_sim* s, cudaGraph_t body, cudaStream_t bs, cudaStream_t bs2, int c,
+                       int kind) {
   s->cur = c;
-  cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
   const int n_if = kind == kBlockExact ? kGraphSteps : 0;
   cudaGraphConditionalHandle h[kGraphSteps];
   for (int k = 0; k < n_if; ++k)
-    CK(cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault));
-  CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
+    CK(cudaGraphConditionalHandleCreate(&h[k], body, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
   int rc = 0;
-  if (kind == kBlockResort) rc = enqueue_rebuild(s, nullptr, s->stream);
-  if (kind == kBlockExact) launch_gate_body(s->ctl, h[0], s->stream);
+  if (kind == kBlockResort) rc = enqueue_rebuild(s, nullptr, bs);
+  if (kind == kBlockExact) launch_gate_body(s->ctl, h[0], bs);
   for (int k = 0; k < kGraphSteps && !rc; ++k) {
-    if (k < n_if) rc = add_rebuild_if(s, s->stream, s->aux, h[k], k);
+    if (k < n_if) rc = add_rebuild_if(s, bs, bs2, h[k], k);
     const StepLink link = k + 1 < n_if ? StepLink{s->d_rb + k, h[k + 1], 1, 0}
                                         : StepLink{s->d_rb + k, 0, 0, (int)(k + 1 == kGraphSteps)};
-    enqueue_step_kernels(s, link, s->stream);
+    s->step_launches = enqueue_step_kernels(s, link, bs);
     s->cur ^= 1;
   }
+  cudaGraph_t tmp = nullptr;
+  CK(cudaStreamEndCapture(bs, &tmp));
+  return rc;
+}
+
+int build_block(blaze_sim* s, int c) {
+  const int saved = s->cur;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hs;
+  CK(cudaGraphConditionalHandleCreate(&hs, g, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  launch_gate_switch(s->ctl, hs, s->d_rb, kGraphSteps, s->opt.skin, list_look(s), s->stream);
+  cudaGraph_t bodies[3] = {nullptr, nullptr, nullptr};
+  int rc = add_conditional(s->stream, hs, cudaGraphCondTypeSwitch, 3, bodies);
+  for (int kind = 0; kind < 3 && !rc; ++kind)
+    rc = capture_block_body(s, bodies[kind], s->aux, s->aux2, c, kind);
   cudaGraph_t out = nullptr;
   CK(cudaStreamEndCapture(s->stream, &out));
-  if (!rc) CK(cudaGraphInstantiate(&s->block[c][kind], out, 0));
+  if (!rc) CK(cudaGraphInstantiate(&s->block[c], out, 0));
   CK(cudaGraphDestroy(out));
   s->cur = saved;
   return rc;
 }
 
+// One step with a skin as a graph, starting from S[c]: the gate of plain
+// stepping (block start or not), an IF node re-sorting when it says so, and
+// the step kernels (recording a list check after the step or not).  Steps
+// outside whole blocks (a tail shorter than a block, the steps after a
+// forced re-sort, those around a removal check) run this way; they make the
+// decisions plain stepping makes, with an IF node instead of gated kernels.
+int build_single(blaze_sim* s, int c, int bstart, int chk) {
+  const int saved = s->cur;
+  s->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  launch_gate_if(s->ctl, h, s->opt.skin, list_look(s), bstart, s->stream);
+  int rc = add_rebuild_if(s, s->stream, s->aux, h, -1);
+  if (!rc) s->step_launches = enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0, chk},
+                                                   s->stream);
+  cudaGraph_t out = nullptr;
+  CK(cudaStreamEndCapture(s->stream, &out));
+  if (!rc) CK(cudaGraphInstantiate(&s->single[c][bstart][chk], out, 0));
+  CK(cudaGraphDestroy(out));
+  s->cur = saved;
+  return rc;
+}
+
+// Instantiates every graph the current options can launch, so that no
+// stream capture or instantiation happens inside a later blaze_step.
+int prepare_graphs(blaze_sim* s) {
+  for (int c = 0; c < 2; ++c) {
+    if (s->opt.skin > 0.0f) {
+      if (!s->block[c]) {
+        int rc = build_block(s, c);
+        if (rc) return rc;
+      }
+      for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 2; ++k)
+          if (!s->single[c][b][k]) {
+            int rc = build_single(s, c, b, k);
+            if (rc) return rc;
+          }
+    } else if (!s->graph[c]) {
+      int rc = build_graph(s, c);
+      if (rc) return rc;
+    }
+  }
+  return 0;
+}
+
 int graph_steps(blaze_sim* s, int nsteps) {
+  int rc = prepare_graphs(s);
+  if (rc) return rc;
   int done = 0;
   while (done < nsteps) {
-    // removal checks and odd tails run as plain steps
+    // a removal check every 1000 steps ends a step outside a block
     const bool kill_soon = s->si.Kill_Particles && s->stepc + kGraphSteps >= 1000;
-    // with a skin a graph starts on a list check (a multiple of kListCheckEvery)
-    const bool off_cadence =
-        s->opt.skin > 0.0f && (s->steps % kListCheckEvery != 0 || s->steps < s->check_until);
-    if (nsteps - done < kGraphSteps || kill_soon || off_cadence) {
-      int rc = enqueue_step(s);
+    const int c = s->cur;
+    if (s->opt.skin > 0.0f) {
+      if (nsteps - done >= kGraphSteps && !kill_soon && block_start_here(s)) {
+        CK(cudaGraphLaunch(s->block[c], s->stream));
+        // the gate and the step kernels (re-sorts and the exact mode's
+        // extra gate are counted on the device)
+        s->last_launches += 1 + kGraphSteps * s->step_launches;
+        s->steps += kGraphSteps;
+        if (s->si.Kill_Particles) s->stepc += kGraphSteps;
+        if (kGraphSteps & 1) s->cur ^= 1;
+        done += kGraphSteps;
+      } else {
+        CK(cudaGraphLaunch(s->single[c][block_start_here(s)][check_after_here(s)], s->stream));
+        s->last_launches += 1 + s->step_launches;
+        finish_step(s);
+        done += 1;
+      }
+      continue;
+    }
+    if (nsteps - done < kGraphSteps || kill_soon) {
+      rc = enqueue_step(s);
       if (rc) return rc;
       done += 1;
       continue;
     }
-    const int c = s->cur;
-    if (s->opt.skin > 0.0f) {
-      // the block-start gate (the decision of plain stepping's gate), read back
-      launch_gate_decide(s->ctl, s->d_rb, kGraphSteps, s->opt.skin, list_look(s), s->stream);
-      CK(cudaMemcpyAsync(s->h_dec, &s->ctl->exact, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                         s->stream));
-      CK(cudaStreamSynchronize(s->stream));
-      const int kind = s->h_dec[0] ? kBlockExact : (s->h_dec[1] ? kBlockResort : kBlockKeep);
-      if (!s->block[c][kind]) {
-        int rc = build_block(s, c, kind);
-        if (rc) return rc;
-      }
-      CK(cudaGraphLaunch(s->block[c][kind], s->stream));
-      s->last_launches += 1 + (kind == kBlockExact ? 1 : 0) + kGraphSteps * (s->poly ? 5 : 1);
-    } else {
-      if (!s->graph[c]) {
-        int rc = build_graph(s, c);
-        if (rc) return rc;
-      }
-      CK(cudaGraphLaunch(s->graph[c], s->stream));
-      // launches that always run: the gate and the step kernels of each step
-      // (re-sort bodies run only when a step asks for them)
-      s->last_launches += 1 + kGraphSteps * (s->poly ? 5 : 1);
-    }
+    CK(cudaGraphLaunch(s->graph[c], s->stream));
+    // launches that always run: the gate and the step kernels of each step
+    // (re-sort bodies run only when a step asks for them)
+    s->last_launches += 1 + kGraphSteps * s->step_launches;
     s->steps += kGraphSteps;
     if (s->si.Kill_Particles) s->stepc += kGraphSteps;
     if (kGraphSteps & 1) s->cur ^= 1;
@@ -873,7 +960,6 @@ void free_sim(blaze_sim* s) {
   f(s->d_tally); f(s->d_eb); f(s->d_epart);
   f(s->cap.f_pp); f(s->cap.t_pp); f(s->cap.f_w); f(s->cap.t_w); f(s->cap.f_l); f(s->cap.t_l);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
-  if (s->h_dec) cudaFreeHost(s->h_dec);
   f(s->stage.pos3); f(s->stage.vel3); f(s->stage.avel3); f(s->stage.type); f(s->stage.pid);
   f(s->stage.flags); f(s->stage.quat4);
   f(s->ob.ornt[0]); f(s->ob.ornt[1]); f(s->d_shapes);
@@ -882,8 +968,10 @@ void free_sim(blaze_sim* s) {
   f(s->nl.flat);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+  drop_graphs(s);
   if (s->stream) cudaStreamDestroy(s->stream);
   if (s->aux) cudaStreamDestroy(s->aux);
+  if (s->aux2) cudaStreamDestroy(s->aux2);
   delete s;
 }
 
@@ -1015,6 +1103,8 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   if (e != cudaSuccess) return fail(cuda_fail(e));
   e = cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking);
   if (e != cudaSuccess) return fail(cuda_fail(e));
+  e = cudaStreamCreateWithFlags(&s->aux2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_fail(e));
 #define CKF(x) do { cudaError_t e2 = (x); if (e2 != cudaSuccess) return fail(cuda_fail(e2)); } while (0)
   for (int b = 0; b < 3; ++b) {
     CKF(dalloc(&s->S[b].pos, n)); CKF(dalloc(&s->S[b].vel, n)); CKF(dalloc(&s->S[b].angv, n));
@@ -1048,7 +1138,6 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->stage.pid, n));
   CKF(dalloc(&s->stage.flags, 2));
   CKF(cudaMallocHost((void**)&s->h_flags, 2 * sizeof(int)));
-  CKF(cudaMallocHost((void**)&s->h_dec, 2 * sizeof(int)));
   std::memset(s->h_ctl, 0, sizeof(StepCtl));
   CKF(dalloc(&s->d_chk, (size_t)2 * kChkSlots * kChkStride));
   CKF(cudaMemset(s->d_chk, 0, sizeof(uint32_t) * 2 * kChkSlots * kChkStride));
@@ -1197,6 +1286,21 @@ int blaze_step(blaze_sim* s, int nsteps) {
 int blaze_sync(blaze_sim* s) {
   if (!s) return -1;
   return sync_status(s);
+}
+
+int blaze_prepare_graphs(blaze_sim* s) {
+  if (!s) return -1;
+  int rc = prepare_graphs(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int blaze_num_exact_blocks(blaze_sim* s) {
+  if (!s) return -1;
+  int rc = sync_status(s);
+  if (rc < 0) return rc;
+  return s->h_ctl->exact_blocks;
 }
 
 int blaze_num_current(blaze_sim* s) {

@@ -84,7 +84,10 @@ __device__ __forceinline__ int gate_request(StepCtl* ctl, float skin, float look
     vm = __uint_as_float(v);
     if (!(pm + look * vm <= 0.5f * skin)) r = 1;
   }
-  if (block_start) ctl->exact = (skin > 0.0f && !(look * vm <= 0.25f * skin)) ? 1 : 0;
+  if (block_start) {
+    ctl->exact = (skin > 0.0f && !(look * vm <= 0.25f * skin)) ? 1 : 0;
+    ctl->exact_blocks += ctl->exact;
+  }
   return r;
 }
 
@@ -95,12 +98,23 @@ __global__ void k_gate(StepCtl* ctl, float skin, float look, int block_start) {
   ctl->rebuild_req = 0;
 }
 
-__global__ void k_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look) {
+__global__ void k_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb,
+                              float skin, float look) {
   const int r = gate_request(ctl, skin, look, 1);
   if (threadIdx.x != 0) return;
   ctl->rebuild_req = 0;
   ctl->gate_r = r;
   for (int k = 0; k < nrb; ++k) rb[k] = k == 0 ? r : 0;
+  cudaGraphSetConditional(hs, ctl->exact ? 2u : (r ? 1u : 0u));
+}
+
+__global__ void k_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
+                          int block_start) {
+  const int r = gate_request(ctl, skin, look, block_start);
+  if (threadIdx.x != 0) return;
+  ctl->rebuilt = r;
+  ctl->rebuild_req = 0;
+  cudaGraphSetConditional(h, r ? 1u : 0u);
 }
 
 __global__ void k_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0) {
@@ -823,8 +837,14 @@ void launch_gate(StepCtl* ctl, cudaStream_t st, float skin, float look, int bloc
   k_gate<<<1, kChkSlots, 0, st>>>(ctl, skin, look, block_start);
 }
 
-void launch_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look, cudaStream_t st) {
-  k_gate_decide<<<1, kChkSlots, 0, st>>>(ctl, rb, nrb, skin, look);
+void launch_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb, float skin,
+                        float look, cudaStream_t st) {
+  k_gate_switch<<<1, kChkSlots, 0, st>>>(ctl, hs, rb, nrb, skin, look);
+}
+
+void launch_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
+                    int block_start, cudaStream_t st) {
+  k_gate_if<<<1, kChkSlots, 0, st>>>(ctl, h, skin, look, block_start);
 }
 
 void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st) {

@@ -31,7 +31,7 @@ struct StepCtl {        // device words the step pipeline communicates through
   int n_cur;            // live particles (removed ones sit at the end)
   int pending_dead;     // removed since the last re-sort
   int killed_total;
-  int pad;
+  int exact_blocks;     // with a skin: blocks of steps run in the exact mode so far
   uint32_t* chk;        // with a skin: kChkSlots maxima of path, then of speed (float
                         // bits, one per 128-byte line), recorded at the step before a check
   int exact;            // with a skin: 1 = this block of steps checks before every step
@@ -130,12 +130,19 @@ void launch_gate(StepCtl* ctl, cudaStream_t st, float skin = 0.0f, float look = 
                  int block_start = 0);
 void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
                        cudaStream_t st, float skin = 0.0f, float look = 0.0f);
-// Block-start gate of skin > 0 graph stepping, launched on its own: the
-// decision goes to ctl->gate_r (and rb[0]; rb[1..nrb) are cleared), the
-// block's mode to ctl->exact; an exact block's first IF takes ctl->gate_r
-// through launch_gate_body.
-void launch_gate_decide(StepCtl* ctl, int* rb, int nrb, float skin, float look, cudaStream_t st);
+// Block-start gate of skin > 0 graph stepping: the first node of a block
+// graph, followed by a SWITCH node on `hs` whose body it picks on the
+// device: 0 keep the list, 1 re-sort then step, 2 exact (a check before
+// every step).  The re-sort decision also goes to ctl->gate_r and rb[0]
+// (rb[1..nrb) are cleared), the mode to ctl->exact; an exact block's first
+// IF takes ctl->gate_r through launch_gate_body.
+void launch_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb, float skin,
+                        float look, cudaStream_t st);
 void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st);
+// The gate of plain stepping (launch_gate) as the first node of a one-step
+// graph: its decision also sets the IF node `h` of the step's re-sort.
+void launch_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
+                    int block_start, cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
 // (flat_n, when given, is reset for the contact-list kernel's flat list)

@@ -169,6 +169,27 @@ def test_graph_stepping_is_exact(silo_small, skin):
         np.testing.assert_array_equal(a[key], b[key])
 
 
+def test_graph_stepping_uneven_calls(silo_small):
+    """Graph stepping with a skin cut into calls of uneven length (tails
+    shorter than a block run as one-step graphs, blocks start mid-call)
+    equals plain stepping bit for bit, and neither runs an exact block on
+    this slow state."""
+    P, st = silo_small
+    a = run_steps(P, st, 203, skin=0.04, use_graph=0)
+    s = device.Simulation(P, skin=0.04, use_graph=1)
+    s.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    s.open_hatch()
+    s.prepare_graphs()
+    for k in (5, 3, 13, 1, 8, 20, 7, 9, 16, 2, 40, 79):
+        s.step(k)
+    b = s.state()
+    assert s.num_exact_blocks() == 0
+    s.close()
+    assert a["status"] == 0 and b["status"] == 0
+    for key in ("pos", "vel", "avel", "pid"):
+        np.testing.assert_array_equal(a[key], b[key])
+
+
 def test_graph_stepping_exact_blocks_fast_state(box):
     """A state too fast for an 8-step block without list checks (speeds
     N(0, 300 cm/s) against a 0.02 cm skin at dt 1e-5 s): the blocks run
@@ -182,10 +203,13 @@ def test_graph_stepping_exact_blocks_fast_state(box):
         s = device.Simulation(P, skin=0.02, use_graph=g)
         s.set_state(st0["pos"], vel, st0["avel"], st0["type"], st0["pid"])
         s.step(67)
-        out.append((s.state(), s.num_rebuilds()))
+        out.append((s.state(), s.num_rebuilds(), s.num_exact_blocks()))
         s.close()
-    (a, ra), (b, rb) = out
+    (a, ra, xa), (b, rb, xb) = out
     assert a["status"] == 0 and b["status"] == 0, device.decode_status(a["status"] | b["status"])
+    # steps 0-7 check after every step (forced re-sort at set_state); the
+    # block starts 8, 16, ..., 64 all run exact, in both stepping modes
+    assert xa == xb == 8, (xa, xb)
     assert ra == rb and ra > 67 // 8
     for key in ("pos", "vel", "avel", "pid"):
         np.testing.assert_array_equal(a[key], b[key])
