@@ -102,10 +102,16 @@ typedef struct blaze_options {
   int use_graph;       /* 1 = step through a captured CUDA graph */
   int capture_forces;  /* 1 = keep the last step's per-particle forces (parity hooks) */
   int sync_each_step;  /* 1 = every step blocks and returns its status */
+  int fast_law;        /* 1 = the sphere particle-particle law in contracted form
+                        * (fused multiply-adds, approximate reciprocals): contact
+                        * sets unchanged, forces within 1e-5 relative of the
+                        * reference's arithmetic instead of bit for bit; steps
+                        * with energy tallies keep the reference's arithmetic */
 } blaze_options;
 
 /* Library defaults: skin 0, max_nbr 32, wall_grid 1, use_graph 0,
- * capture_forces 0, sync_each_step 0 (the reference's semantics). */
+ * capture_forces 0, sync_each_step 0, fast_law 0 (the reference's
+ * semantics). */
 void blaze_default_options(blaze_options* o);
 
 int blaze_create(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
@@ -187,6 +193,16 @@ int blaze_get_nlist(blaze_sim* s, uint* nn, uint* list);
 /* Device pointers of the current state (SoA float4: pos+radius, vel+type,
  * angular velocity) and the CUDA stream the simulation runs on. */
 int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, void** stream);
+/* Headless replacement of the reference's OpenGL view (Graphics.h draws
+ * positions and, for polyhedra, orientations every frame): waits for the
+ * stream, then returns device pointers to the current step's positions as
+ * float4 (x, y, z, radius; polyhedra: centre of mass) and orientations as
+ * float4 (w, x, y, z; NULL for spheres), in memory order, and the number of
+ * entries n (particles removed since the last re-sort are parked far
+ * outside the world).  The pointers stay valid until the next step or
+ * state change; read them on `stream` or after this call.  Returns the
+ * status like blaze_sync. */
+int blaze_device_view(blaze_sim* s, const void** pos4, const void** ornt4, int* n, void** stream);
 /* Kernel launches the last blaze_step enqueued unconditionally (gate and
  * step kernels; graph re-sort bodies are counted by blaze_rebuild_kernels
  * per re-sort). */

@@ -63,7 +63,86 @@ typedef struct {
   int kind;
   real r;
   v3 a, b, c;
+  v3 nh, nl, eh[3], el[3];   /* triangle: unit normal, unit edges ab, ac, bc as hi + lo */
 } wallc;
+
+/* Accurate overlaps (csrc/ens_kernels.cuh, "accurate overlaps"): the same
+ * error-free transformations in the same order.  In the FP64 build the
+ * same code runs in double (the lo parts of the triangle's unit vectors
+ * are then zero). */
+typedef struct { real hi, lo; } ffr;
+static real FMA(real a, real b, real c) {
+  return IS_FLOAT ? (real)fmaf((float)a, (float)b, (float)c) : (real)fma((double)a, (double)b, (double)c);
+}
+static real two_sum(real a, real b, real* e) {
+  const real s = a + b;
+  const real bb = s - a;
+  *e = (a - (s - bb)) + (b - bb);
+  return s;
+}
+static real two_prod(real a, real b, real* e) {
+  const real p = a * b;
+  *e = FMA(a, b, -p);
+  return p;
+}
+static void acc_add(real* s, real* c, real x) {
+  real e;
+  *s = two_sum(*s, x, &e);
+  *c = *c + e;
+}
+static ffr ff_diff(real a, real b) {
+  ffr r;
+  r.hi = two_sum(a, -b, &r.lo);
+  return r;
+}
+static ffr ffv(real hi, real lo) { ffr r = {hi, lo}; return r; }
+static void acc_sq(real* s, real* c, ffr x) {
+  real e;
+  const real p = two_prod(x.hi, x.hi, &e);
+  acc_add(s, c, p);
+  *c = *c + (e + (real)2.0 * (x.hi * x.lo));
+}
+static void acc_prod(real* s, real* c, ffr x, ffr y) {
+  real e;
+  const real p = two_prod(x.hi, y.hi, &e);
+  acc_add(s, c, p);
+  *c = *c + (e + (x.hi * y.lo + x.lo * y.hi));
+}
+static real overlap_pair(real ra, real rb, v3 pa, v3 pb, real dist) {
+  ffr sr;
+  sr.hi = two_sum(ra, rb, &sr.lo);
+  real s = 0, c = 0;
+  acc_sq(&s, &c, sr);
+  real t = 0, u = 0;
+  acc_sq(&t, &u, ff_diff(pa.x, pb.x));
+  acc_sq(&t, &u, ff_diff(pa.y, pb.y));
+  acc_sq(&t, &u, ff_diff(pa.z, pb.z));
+  acc_add(&s, &c, -t);
+  c = c - u;
+  return (s + c) / (sr.hi + dist);
+}
+static real overlap_plane(real r, v3 n, real d, v3 p) {
+  real e0, e1, e2, c;
+  const real q0 = two_prod(n.x, p.x, &e0), q1 = two_prod(n.y, p.y, &e1), q2 = two_prod(n.z, p.z, &e2);
+  real s = two_sum(r, d, &c);
+  acc_add(&s, &c, -q0);
+  acc_add(&s, &c, -q1);
+  acc_add(&s, &c, -q2);
+  c = c - ((e0 + e1) + e2);
+  return s + c;
+}
+/* a unit vector computed in double from float components, as hi + lo */
+static void unit_split(double x, double y, double z, v3* hi, v3* lo) {
+  const double l = sqrt(x * x + y * y + z * z);
+  const double u[3] = {l > 0 ? x / l : 0.0, l > 0 ? y / l : 0.0, l > 0 ? z / l : 0.0};
+  real h[3], o[3];
+  for (int k = 0; k < 3; ++k) {
+    h[k] = IN(u[k]);
+    o[k] = IN(u[k] - (double)h[k]);
+  }
+  *hi = mk(h[0], h[1], h[2]);
+  *lo = mk(o[0], o[1], o[2]);
+}
 
 typedef struct {
   v3 pos, vel, w;
@@ -147,6 +226,14 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
     if (d->kind == BLAZE_WALL_PLANE) { d->a = mk(p[0], p[1], p[2]); d->r = p[3]; }
     else if (d->kind == BLAZE_WALL_TRIANGLE) {
       d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->c = mk(p[6], p[7], p[8]);
+      const double ab[3] = {(double)p[3] - p[0], (double)p[4] - p[1], (double)p[5] - p[2]};
+      const double ac[3] = {(double)p[6] - p[0], (double)p[7] - p[1], (double)p[8] - p[2]};
+      const double bc[3] = {(double)p[6] - p[3], (double)p[7] - p[4], (double)p[8] - p[5]};
+      unit_split(ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2],
+                 ab[0] * ac[1] - ab[1] * ac[0], &d->nh, &d->nl);
+      unit_split(ab[0], ab[1], ab[2], &d->eh[0], &d->el[0]);
+      unit_split(ac[0], ac[1], ac[2], &d->eh[1], &d->el[1]);
+      unit_split(bc[0], bc[1], bc[2], &d->eh[2], &d->el[2]);
     } else { d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->r = p[6]; }
   }
   o->p = (part*)calloc(n, sizeof(part));
@@ -372,56 +459,114 @@ static void contact_law(const ens_oracle* o, const sysc* S, real mu, v3 n, real 
   }
 }
 
-static v3 closest_tri(v3 p, v3 a, v3 b, v3 c, int* region) {
+static v3 closest_tri(v3 p, v3 a, v3 b, v3 c, int* region, int* feat) {
   const v3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
   const real d1 = dot(ab, ap), d2 = dot(ac, ap);
-  if (d1 <= 0 && d2 <= 0) { *region = 2; return a; }
+  if (d1 <= 0 && d2 <= 0) { *region = 2; *feat = 0; return a; }
   const v3 bp = sub(p, b);
   const real d3 = dot(ab, bp), d4 = dot(ac, bp);
-  if (d3 >= 0 && d4 <= d3) { *region = 2; return b; }
+  if (d3 >= 0 && d4 <= d3) { *region = 2; *feat = 1; return b; }
   const real vc = d1 * d4 - d3 * d2;
-  if (vc <= 0 && d1 >= 0 && d3 <= 0) { *region = 1; return add(a, mul(ab, d1 / (d1 - d3))); }
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+    *region = 1; *feat = 0;
+    return add(a, mul(ab, d1 / (d1 - d3)));
+  }
   const v3 cp = sub(p, c);
   const real d5 = dot(ab, cp), d6 = dot(ac, cp);
-  if (d6 >= 0 && d5 <= d6) { *region = 2; return c; }
+  if (d6 >= 0 && d5 <= d6) { *region = 2; *feat = 2; return c; }
   const real vb = d5 * d2 - d1 * d6;
-  if (vb <= 0 && d2 >= 0 && d6 <= 0) { *region = 1; return add(a, mul(ac, d2 / (d2 - d6))); }
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+    *region = 1; *feat = 1;
+    return add(a, mul(ac, d2 / (d2 - d6)));
+  }
   const real va = d3 * d6 - d5 * d4;
   if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
-    *region = 1;
+    *region = 1; *feat = 2;
     return add(b, mul(sub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
   }
   const real den = (real)1.0 / ((va + vb) + vc);
-  *region = 0;
+  *region = 0; *feat = 0;
   return add(add(a, mul(ab, vb * den)), mul(ac, vc * den));
 }
 
 static int wall_touch(const wallc* W, v3 p, real r, v3* n, real* delta, int* region) {
   *region = 0;
   if (W->kind == BLAZE_WALL_PLANE) {
-    const real s = dot(W->a, p) - W->r;
-    if (!(s < r)) return 0;
+    *delta = overlap_plane(r, W->a, W->r, p);
+    if (!(*delta > 0)) return 0;
     *n = W->a;
-    *delta = r - s;
     return 1;
   }
   if (W->kind == BLAZE_WALL_CYLINDER) {
-    const v3 v = sub(p, W->a);
-    const v3 rad = sub(v, smul(dot(v, W->b), W->b));
-    const real rho = len(rad);
-    if (!(rho + r > W->r) || !(rho > 0)) return 0;
-    *n = mul(rad, (real)-1.0 / rho);
-    *delta = (rho + r) - W->r;
+    const ffr v[3] = {ff_diff(p.x, W->a.x), ff_diff(p.y, W->a.y), ff_diff(p.z, W->a.z)};
+    const real b[3] = {W->b.x, W->b.y, W->b.z};
+    real vb = 0, vbc = 0;
+    for (int k = 0; k < 3; ++k) acc_prod(&vb, &vbc, v[k], ffv(b[k], 0));
+    ffr rad[3];
+    real t = 0, u = 0;
+    for (int k = 0; k < 3; ++k) {
+      real e, e2;
+      const real q = two_prod(vb, b[k], &e);
+      rad[k].hi = two_sum(v[k].hi, -q, &e2);
+      rad[k].lo = ((v[k].lo + e2) - e) - vbc * b[k];
+      acc_sq(&t, &u, rad[k]);
+    }
+    const real rho = SQRT(t + u);
+    ffr rr;
+    rr.hi = two_sum(W->r, -r, &rr.lo);
+    real t2 = 0, u2 = 0;
+    acc_sq(&t2, &u2, rr);
+    acc_add(&t, &u, -t2);
+    u = u - u2;
+    *delta = (t + u) / (rho + rr.hi);
+    if (!(*delta > 0) || !(rho > 0)) return 0;
+    *n = mul(mk(rad[0].hi, rad[1].hi, rad[2].hi), (real)-1.0 / rho);
     return 1;
   }
-  const v3 q = closest_tri(p, W->a, W->b, W->c, region);
+  int feat;
+  const v3 q = closest_tri(p, W->a, W->b, W->c, region, &feat);
   const v3 d = sub(p, q);
   const real d2 = dot(d, d);
   if (!(d2 < r * r)) return 0;
-  const real dist = SQRT(d2);
+  if (*region == 0) {
+    const ffr pa[3] = {ff_diff(p.x, W->a.x), ff_diff(p.y, W->a.y), ff_diff(p.z, W->a.z)};
+    real s = 0, c = 0;
+    acc_prod(&s, &c, pa[0], ffv(W->nh.x, W->nl.x));
+    acc_prod(&s, &c, pa[1], ffv(W->nh.y, W->nl.y));
+    acc_prod(&s, &c, pa[2], ffv(W->nh.z, W->nl.z));
+    const real sg = s < 0 ? (real)-1.0 : (real)1.0;
+    *delta = (r - sg * s) - sg * c;
+    if (!(*delta > 0) || !(sg * s > 0)) return 0;
+    *n = mul(W->nh, sg);
+    return 1;
+  }
+  const v3 v0 = *region == 2 ? (feat == 0 ? W->a : (feat == 1 ? W->b : W->c))
+                             : (feat == 2 ? W->b : W->a);
+  const ffr pv[3] = {ff_diff(p.x, v0.x), ff_diff(p.y, v0.y), ff_diff(p.z, v0.z)};
+  real t = 0, u = 0;
+  for (int k = 0; k < 3; ++k) acc_sq(&t, &u, pv[k]);
+  v3 dir = mk(pv[0].hi, pv[1].hi, pv[2].hi);
+  if (*region == 1) {
+    const v3 eh = W->eh[feat], el = W->el[feat];
+    real s = 0, c = 0;
+    acc_prod(&s, &c, pv[0], ffv(eh.x, el.x));
+    acc_prod(&s, &c, pv[1], ffv(eh.y, el.y));
+    acc_prod(&s, &c, pv[2], ffv(eh.z, el.z));
+    real s2 = 0, c2 = 0;
+    acc_sq(&s2, &c2, ffv(s, c));
+    acc_add(&t, &u, -s2);
+    u = u - c2;
+    dir = sub(dir, mul(eh, s));
+  }
+  const real dist = SQRT(t + u);
   if (!(dist > 0)) return 0;
-  *n = mul(d, (real)1.0 / dist);
-  *delta = r - dist;
+  real er;
+  real S = two_prod(r, r, &er), C = er;
+  acc_add(&S, &C, -t);
+  C = C - u;
+  *delta = (S + C) / (r + dist);
+  if (!(*delta > 0)) return 0;
+  *n = mul(dir, (real)1.0 / len(dir));
   return 1;
 }
 
@@ -510,7 +655,7 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
       const real dist = SQRT(d2);
       if (!(dist > 0)) continue;
       const v3 nrm = mul(rel, (real)1.0 / dist);
-      const real delta = sr - dist;
+      const real delta = overlap_pair(ra, rb, a->pos, b->pos, dist);
       const real mb = S->dens43pi * ((rb * rb) * rb);
       v3 xi = mk(0, 0, 0);
       if ((M[i] >> k) & 1u) xi = mk(H[3 * sk], H[3 * sk + 1], H[3 * sk + 2]);
@@ -745,7 +890,7 @@ static v3 pair_vjp(const ens_oracle* o, const sysc* S, const part* a, const part
   const real dist = SQRT(dot(rel, rel));
   const real inv = (real)1.0 / dist;
   const v3 n = mul(rel, inv);
-  const real delta = (ra + rb) - dist;
+  const real delta = overlap_pair(ra, rb, a->pos, b->pos, dist);
   const real ma = S->dens43pi * ((ra * ra) * ra), mb = S->dens43pi * ((rb * rb) * rb);
   const real ms = (ma * mb) / (ma + mb);
   const v3 ua = mul(n, -ra), ub = mul(n, rb);
@@ -780,7 +925,7 @@ static v3 plane_vjp(const ens_oracle* o, const sysc* S, const wallc* W, const pa
                     v3 Fb, v3 Tb, v3 Xb, sbar* ab, lawbar* th, real* mu_wb) {
   const real r = a->r;
   const v3 n = W->a;
-  const real delta = r - (dot(W->a, a->pos) - W->r);
+  const real delta = overlap_plane(r, W->a, W->r, a->pos);
   const real ma = S->dens43pi * ((r * r) * r);
   const v3 ua = mul(n, -r);
   const v3 vca = add(a->vel, cross(a->w, ua));

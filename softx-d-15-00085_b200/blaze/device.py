@@ -33,7 +33,8 @@ class BlazeError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("skin", C.c_float), ("max_nbr", C.c_int), ("wall_grid", C.c_int),
-                ("use_graph", C.c_int), ("capture_forces", C.c_int), ("sync_each_step", C.c_int)]
+                ("use_graph", C.c_int), ("capture_forces", C.c_int), ("sync_each_step", C.c_int),
+                ("fast_law", C.c_int)]
 
 
 class StateHeader(C.Structure):
@@ -110,6 +111,8 @@ def load():
     lib.blaze_num_current.argtypes = [C.c_void_p]
     lib.blaze_num_rebuilds.argtypes = [C.c_void_p]
     lib.blaze_prepare_graphs.argtypes = [C.c_void_p]
+    lib.blaze_device_view.argtypes = [C.c_void_p] + [P(C.c_void_p), P(C.c_void_p), P(C.c_int),
+                                                     P(C.c_void_p)]
     lib.blaze_num_exact_blocks.argtypes = [C.c_void_p]
     lib.blaze_update_wobj.argtypes = [C.c_void_p, P(T.WOBJ), C.c_int]
     lib.blaze_update_dobj.argtypes = [C.c_void_p, P(T.DOBJ), C.c_int]
@@ -164,6 +167,19 @@ def default_options(**kw):
     for k, v in kw.items():
         setattr(o, k, v)
     return o
+
+
+class _DeviceArray:
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
+                                         "version": 2}
+
+
+def device_array(ptr, n, width, typestr="<f4"):
+    """A torch view (no copy) of n x width device values at `ptr` (e.g. a
+    pointer from Simulation.device_state or device_view)."""
+    import torch
+    return torch.as_tensor(_DeviceArray(int(ptr), (int(n), int(width)), typestr), device="cuda")
 
 
 class Simulation:
@@ -335,6 +351,15 @@ class Simulation:
         ptrs = [C.c_void_p() for _ in range(4)]
         _check(self.lib.blaze_device_state(self.h, *[C.byref(p) for p in ptrs]), "device_state")
         return tuple(p.value for p in ptrs)
+
+    def device_view(self):
+        """(pos4, ornt4 or None, n, stream): the headless view buffer, device
+        pointers as ints (blaze_device_view)."""
+        pos, orn, st = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        n = C.c_int()
+        _check(self.lib.blaze_device_view(self.h, C.byref(pos), C.byref(orn), C.byref(n),
+                                          C.byref(st)), "blaze_device_view")
+        return pos.value, orn.value, n.value, st.value
 
     def last_launches(self):
         return self.lib.blaze_last_launches(self.h)

@@ -104,7 +104,7 @@ struct blaze_sim {
   bool dobj_rot = false;
   int dobj_tr = -1;
   bool dobj_on_device = false;
-  float rot_ax = 0.0f, rot_ay = 0.0f, rot_c = 1.0f, rot_s = 0.0f;
+  float rot_ax = 0.0f, rot_ay = 0.0f, rot_c = 1.0f, rot_s = 0.0f, rot_rad = 0.0f;
   // the mill's fill waves (InitConfig grid_type 2): fill_pack particles join
   // the run every fill_clear + 1 steps until all are in
   bool filling = false;
@@ -112,7 +112,7 @@ struct blaze_sim {
   bool wobj_rot = false;
   bool wobj_on_device = false;
   uint32_t wrot_mask = 0;
-  float wrot_ax = 0.0f, wrot_ay = 0.0f, wrot_c = 1.0f, wrot_s = 0.0f;
+  float wrot_ax = 0.0f, wrot_ay = 0.0f, wrot_c = 1.0f, wrot_s = 0.0f, wrot_rad = 0.0f;
   // optional per-phase event timing (non-graph stepping only)
   bool profile = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -151,6 +151,7 @@ void build_params(blaze_sim* s) {
   P.ncell_tab = (uint32_t)std::max(hmax, prod);
   P.gravity = si.Force_Field;
   P.dt = si.InitalDelta_t;
+  P.tan_k = si.InitalDelta_t > 0.0f ? 0.025f / si.InitalDelta_t : 0.0f;
   P.roll_res = si.Roll_Res;
   P.mill_rot_vel = si.MillRotVel;
   P.drum_r = s->n_w > 0 ? s->w[0].cyl_geo.radius : 0.0f;
@@ -550,7 +551,7 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
   } else {
     launch_step(s->dp, s->d_ops, WallGrid{s->d_wall_off, s->d_wall_idx}, s->S[s->cur], s->S[2],
                 s->S[s->cur ^ 1], s->ob, s->n_max, s->nl, s->ctl, link, s->spin_free, cap, eb,
-                st);
+                s->opt.fast_law != 0, st);
   }
   if (eb) {
     launch_energy_reduce(eb, s->n_max, s->ctl, s->d_epart, s->d_tally, st);
@@ -561,6 +562,48 @@ int enqueue_step_kernels(blaze_sim* s, StepLink link, cudaStream_t st) {
 
 // the list check's look-ahead distance per unit speed (list_needs_rebuild)
 float list_look(const blaze_sim* s) { return 2.0f * kListCheckEvery * s->si.InitalDelta_t; }
+
+// The largest surface speed of a moving wall or volume object, cm/s (0 when
+// all are at rest): the drum wall turning at MillRotVel (cylinder rotation,
+// and the faces of a rotating world object under it), volume objects
+// attached to a mill drum (they meet particles at the drum's wall velocity,
+// DEM_Kernels_Compute.cuh:206-216), lifters turned on the device, a
+// translating volume object, world objects turned on the device.  The list
+// check counts it as a particle speed at every block start: a moving wall
+// can set a particle at rest in motion within the block.
+float wall_speed(const blaze_sim* s) {
+  const float dt = s->si.InitalDelta_t;
+  auto rxy = [](float3 p, float ax, float ay) {
+    return std::sqrt((p.x - ax) * (p.x - ax) + (p.y - ay) * (p.y - ay));
+  };
+  const float om_drum = std::fabs(s->hp.mill_rot_vel);
+  const float om_dobj = dt > 0.0f ? std::fabs(s->rot_rad) / dt : 0.0f;
+  const float om_wobj = dt > 0.0f ? std::fabs(s->wrot_rad) / dt : 0.0f;
+  const float R = s->hp.drum_r;
+  float v = 0.0f;
+  if (s->cyl_rot) v = std::max(v, om_drum * R);
+  for (int k = 0; k < s->n_d; ++k) {
+    const DOBJ& D = s->d[k];
+    for (int q = 0; q < D.num_vertex && q < 8; ++q) {
+      if (s->hp.is_mill && D.is_attached_DWorld) v = std::max(v, om_drum * rxy(D.vertex[q], R, R));
+      if (s->dobj_rot && D.is_attached_DWorld)
+        v = std::max(v, om_dobj * rxy(D.vertex[q], s->rot_ax, s->rot_ay));
+    }
+    if (k == s->dobj_tr)
+      v = std::max(v, std::sqrt(D.velocity.x * D.velocity.x + D.velocity.y * D.velocity.y +
+                                D.velocity.z * D.velocity.z));
+  }
+  for (int k = 0; k < s->n_w; ++k) {
+    const WOBJ& W = s->w[k];
+    const bool turned = s->wobj_rot && k < 32 && ((s->wrot_mask >> k) & 1u);
+    const bool drum_faces = s->hp.rotating_wobj && s->cyl_rot;
+    for (int q = 0; q < W.num_vertex && q < 16; ++q) {
+      if (turned) v = std::max(v, om_wobj * rxy(W.vertex[q], s->wrot_ax, s->wrot_ay));
+      if (drum_faces) v = std::max(v, om_drum * rxy(W.vertex[q], R, R));
+    }
+  }
+  return v;
+}
 
 // After a forced re-sort (new state, fill wave, removal, new options) the
 // next regular check may be up to kListCheckEvery steps away and nothing has
@@ -630,7 +673,7 @@ int enqueue_step(blaze_sim* s) {
     if (rc) return rc;
   }
   if (s->profile) prof_event(s, 0);
-  launch_gate(s->ctl, s->stream, s->opt.skin, list_look(s), block_start_here(s));
+  launch_gate(s->ctl, s->stream, s->opt.skin, list_look(s), block_start_here(s), wall_speed(s));
   int rc = enqueue_rebuild(s, &s->ctl->rebuilt, s->stream);
   if (rc) return rc;
   if (s->profile) { prof_event(s, 0); prof_event(s, 1); }
@@ -771,7 +814,8 @@ int build_block(blaze_sim* s, int c) {
   CK(cudaGraphConditionalHandleCreate(&hs, g, 0, cudaGraphCondAssignDefault));
   CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
-  launch_gate_switch(s->ctl, hs, s->d_rb, kGraphSteps, s->opt.skin, list_look(s), s->stream);
+  launch_gate_switch(s->ctl, hs, s->d_rb, kGraphSteps, s->opt.skin, list_look(s), wall_speed(s),
+                     s->stream);
   cudaGraph_t bodies[3] = {nullptr, nullptr, nullptr};
   int rc = add_conditional(s->stream, hs, cudaGraphCondTypeSwitch, 3, bodies);
   for (int kind = 0; kind < 3 && !rc; ++kind)
@@ -799,7 +843,7 @@ int build_single(blaze_sim* s, int c, int bstart, int chk) {
   CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
   CK(cudaStreamBeginCaptureToGraph(s->stream, g, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeThreadLocal));
-  launch_gate_if(s->ctl, h, s->opt.skin, list_look(s), bstart, s->stream);
+  launch_gate_if(s->ctl, h, s->opt.skin, list_look(s), bstart, wall_speed(s), s->stream);
   int rc = add_rebuild_if(s, s->stream, s->aux, h, -1);
   if (!rc) s->step_launches = enqueue_step_kernels(s, StepLink{&s->ctl->rebuilt, 0, 0, chk},
                                                    s->stream);
@@ -1192,6 +1236,7 @@ void blaze_default_options(blaze_options* o) {
   o->use_graph = 0;
   o->capture_forces = 0;
   o->sync_each_step = 0;
+  o->fast_law = 0;
 }
 
 int blaze_create(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p, const DOBJ* d,
@@ -1234,6 +1279,7 @@ int blaze_set_cylinder_rotation(blaze_sim* s, int on) {
   if (rc) return rc;
   s->cyl_rot = on ? 1 : 0;
   s->hp.cyl_rot = s->cyl_rot;
+  drop_graphs(s);   // the list check's wall speed changes
   CK(cudaMemcpyAsync(s->dp, &s->hp, sizeof(SimParams), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
@@ -1350,6 +1396,7 @@ int blaze_set_dobj_rotation(blaze_sim* s, float about_x, float about_y, float ra
   // drum driver evaluates them once per step (Processing_Mills.h:20-21)
   s->rot_c = std::cos(rad_per_step);
   s->rot_s = std::sin(rad_per_step);
+  s->rot_rad = rad_per_step;
   drop_graphs(s);
   return 0;
 }
@@ -1376,6 +1423,7 @@ int blaze_set_wobj_rotation(blaze_sim* s, float about_x, float about_y, float ra
   s->wrot_ay = about_y;
   s->wrot_c = std::cos(rad_per_step);   // the host's single-precision cosine and sine
   s->wrot_s = std::sin(rad_per_step);   // (Processing_Mills.h:269-270)
+  s->wrot_rad = rad_per_step;
   // moving walls: no per-cell candidate lists
   if (s->wobj_rot) s->walls_static = false;
   rc = upload_walls(s);
@@ -1480,6 +1528,19 @@ int blaze_device_state(blaze_sim* s, void** pos4, void** vel4, void** angv4, voi
   if (angv4) *angv4 = s->S[s->cur].angv;
   if (stream) *stream = (void*)s->stream;
   return 0;
+}
+
+int blaze_device_view(blaze_sim* s, const void** pos4, const void** ornt4, int* n, void** stream) {
+  if (!s) return -1;
+  const int rc = sync_status(s);
+  if (rc < 0) return rc;
+  if (pos4) *pos4 = s->S[s->cur].pos;
+  // orientations follow the particles' memory order, which changes at a
+  // re-sort: the copy the step wrote is selected by the re-sort count
+  if (ornt4) *ornt4 = s->poly ? s->ob.ornt[s->h_ctl->epoch & 1] : nullptr;
+  if (n) *n = s->h_ctl->n_cur;
+  if (stream) *stream = (void*)s->stream;
+  return rc;
 }
 
 int blaze_last_launches(blaze_sim* s) { return s ? s->last_launches : -1; }

@@ -96,6 +96,7 @@ struct SimParams {
   // dynamics
   float3 gravity;
   float dt, roll_res, mill_rot_vel, drum_r;
+  float tan_k;          // 0.025 / dt: the contracted law's tangential factor per (mu (ma + mb))
   int rotation, mode2d, energy_calc, is_mill, rotating_wobj, cyl_rot;
   float3 cent;
   float dobj_cyl_bound_r;

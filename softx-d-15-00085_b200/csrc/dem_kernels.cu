@@ -53,7 +53,7 @@ __device__ __forceinline__ void flag_status(StepCtl* ctl, uint32_t bits) {
 // half the skin before the next check; at a block start also the block's
 // mode (list_needs_rebuild).  Returns the decision in thread 0.
 __device__ __forceinline__ int gate_request(StepCtl* ctl, float skin, float look,
-                                            int block_start) {
+                                            int block_start, float vwall) {
   __shared__ uint32_t sp[kChkSlots / 32], sv[kChkSlots / 32];
   const int t = threadIdx.x;
   uint32_t p = 0u, v = 0u;
@@ -79,9 +79,12 @@ __device__ __forceinline__ int gate_request(StepCtl* ctl, float skin, float look
   }
   int r = ctl->rebuild_req;
   float vm = 0.0f;
-  if (p | v) {
+  // at a block start the step before recorded the maxima (all zero for a
+  // bed at rest), and a moving wall may set a particle in motion within the
+  // block: its surface speed counts as a particle speed
+  if ((p | v) || (block_start && vwall > 0.0f)) {
     const float pm = __uint_as_float(p);
-    vm = __uint_as_float(v);
+    vm = fmaxf(__uint_as_float(v), block_start ? vwall : 0.0f);
     if (!(pm + look * vm <= 0.5f * skin)) r = 1;
   }
   if (block_start) {
@@ -91,16 +94,16 @@ __device__ __forceinline__ int gate_request(StepCtl* ctl, float skin, float look
   return r;
 }
 
-__global__ void k_gate(StepCtl* ctl, float skin, float look, int block_start) {
-  const int r = gate_request(ctl, skin, look, block_start);
+__global__ void k_gate(StepCtl* ctl, float skin, float look, int block_start, float vwall) {
+  const int r = gate_request(ctl, skin, look, block_start, vwall);
   if (threadIdx.x != 0) return;
   ctl->rebuilt = r;
   ctl->rebuild_req = 0;
 }
 
 __global__ void k_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb,
-                              float skin, float look) {
-  const int r = gate_request(ctl, skin, look, 1);
+                              float skin, float look, float vwall) {
+  const int r = gate_request(ctl, skin, look, 1, vwall);
   if (threadIdx.x != 0) return;
   ctl->rebuild_req = 0;
   ctl->gate_r = r;
@@ -109,8 +112,8 @@ __global__ void k_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* 
 }
 
 __global__ void k_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
-                          int block_start) {
-  const int r = gate_request(ctl, skin, look, block_start);
+                          int block_start, float vwall) {
+  const int r = gate_request(ctl, skin, look, block_start, vwall);
   if (threadIdx.x != 0) return;
   ctl->rebuilt = r;
   ctl->rebuild_req = 0;
@@ -126,7 +129,7 @@ __global__ void k_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0) {
 // "re-sorted" flags (an IF body marks its own step).
 __global__ void k_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
                              float skin, float look) {
-  const int r = gate_request(ctl, skin, look, 0);
+  const int r = gate_request(ctl, skin, look, 0, 0.0f);
   if (threadIdx.x != 0) return;
   ctl->rebuild_req = 0;
   for (int k = 0; k < nrb; ++k) rb[k] = 0;
@@ -383,10 +386,33 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 #endif
 // candidate slots tested per batch of independent loads in the contact pass
 constexpr int kMaskBatch = 8;
+
+// The reference's contact test |xa - xb| - (ra + rb) < 0
+// (Collision_Detection_BroadPhase.cuh:376, len3 then a subtraction), decided
+// without the square root wherever that is exact.  With d2 formed as len3
+// forms it, the test is RN(sqrt(d2)) < sr (the difference of two distinct
+// floats never rounds to zero).  With s2 = RN(sr^2): d2 < RN(s2 (1 - 2^-20))
+// implies sqrt(d2) < sr (1 - 2^-22), so RN(sqrt(d2)) < sr; d2 > RN(s2 (1 +
+// 2^-20)) implies sqrt(d2) > sr (1 + 2^-23), so RN(sqrt(d2)) > sr (each
+// rounding moves a value by at most 2^-24 of itself while s2 is normal).
+// In between, and for NaN or tiny radii, the IEEE square root decides.
+__device__ __forceinline__ bool touches(float3 rel, float sr) {
+  const float d2 = dot3(rel, rel);
+  const float s2 = sr * sr;
+  if (s2 >= 1e-30f) {
+    if (d2 < s2 * (1.0f - 0x1p-20f)) return true;
+    if (d2 > s2 * (1.0f + 0x1p-20f)) return false;
+  }
+  return sqrtf(d2) - sr < 0.0f;
+}
+
 // kEnergy: also the energy tallies of the step's contacts, per particle in
 // contact order (particle-particle, volume objects, world objects), into
 // eb[c * n_max + i] in FP64.
-template <bool kCapture, bool kSpin, bool kEnergy>
+// kFast: the particle-particle law in contracted form (law_pp_fast) and the
+// contact normal from an approximate reciprocal; contact tests, walls, volume
+// objects and the integrator are unchanged.  Not with kEnergy.
+template <bool kCapture, bool kSpin, bool kEnergy, bool kFast>
 __global__ void __launch_bounds__(kThreads, BLAZE_STEP_MIN_BLOCKS)
 k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGrid wg,
        StateBuf in_plain, StateBuf in_sorted, StateBuf out, OrderBuf ob, int n_max,
@@ -441,8 +467,7 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
       pb[u] = k0 + u < cnt ? __ldg(in.pos + jj[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
     for (int u = 0; u < kMaskBatch; ++u) {
-      const float3 rel = pa - xyz(pb[u]);
-      if (k0 + u < cnt && len3(rel) - (ra + pb[u].w) < 0.0f) cm |= 1u << (k0 + u);
+      if (k0 + u < cnt && touches(pa - xyz(pb[u]), ra + pb[u].w)) cm |= 1u << (k0 + u);
     }
   }
   while (cm) {
@@ -456,12 +481,18 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
     const float dist = len3(rel);
     const int tb = __float_as_int(vb4.w);
     const float3 vb = xyz(vb4);
-    const float3 nrm = div3_rn(rel, dist);   // = rel / dist, three correctly rounded quotients
     const float dis = fabsf(dist - (ra + pb4.w)) + 0.000010f;
     const PP_Parms& pp = TA.pp[tb < kMaxPP ? tb : 0];
-    const Forces F = law_pp<kSpin>(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4),
-                            pp, va, vb, ma, sT[tb & (kMaxTypes - 1)].mass,
-                            kEnergy ? &ec : nullptr);
+    Forces F;
+    if constexpr (kFast) {
+      const float3 nrm = rel * __fdividef(1.0f, dist);
+      F = law_pp_fast<kSpin>(P, va - vb, nrm, dis, nrm * (-ra), nrm * pb4.w, wa, xyz(wb4), pp, va,
+                             vb, (P.tan_k * pp.Fric_kinetic) * (ma + sT[tb & (kMaxTypes - 1)].mass));
+    } else {
+      const float3 nrm = div3_rn(rel, dist);   // = rel / dist, three correctly rounded quotients
+      F = law_pp<kSpin>(P, va - vb, nrm, dis, (-1.0f * nrm) * ra, nrm * pb4.w, wa, xyz(wb4), pp,
+                        va, vb, ma, sT[tb & (kMaxTypes - 1)].mass, kEnergy ? &ec : nullptr);
+    }
     f = f + F.trans;
     fl = fl + F.torque;
     if (kEnergy) e_pp += (double)ec;
@@ -833,18 +864,19 @@ inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
 
-void launch_gate(StepCtl* ctl, cudaStream_t st, float skin, float look, int block_start) {
-  k_gate<<<1, kChkSlots, 0, st>>>(ctl, skin, look, block_start);
+void launch_gate(StepCtl* ctl, cudaStream_t st, float skin, float look, int block_start,
+                 float vwall) {
+  k_gate<<<1, kChkSlots, 0, st>>>(ctl, skin, look, block_start, vwall);
 }
 
 void launch_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb, float skin,
-                        float look, cudaStream_t st) {
-  k_gate_switch<<<1, kChkSlots, 0, st>>>(ctl, hs, rb, nrb, skin, look);
+                        float look, float vwall, cudaStream_t st) {
+  k_gate_switch<<<1, kChkSlots, 0, st>>>(ctl, hs, rb, nrb, skin, look, vwall);
 }
 
 void launch_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
-                    int block_start, cudaStream_t st) {
-  k_gate_if<<<1, kChkSlots, 0, st>>>(ctl, h, skin, look, block_start);
+                    int block_start, float vwall, cudaStream_t st) {
+  k_gate_if<<<1, kChkSlots, 0, st>>>(ctl, h, skin, look, block_start, vwall);
 }
 
 void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st) {
@@ -880,12 +912,21 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
                  NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
-                 const ForceCapture* cap, double* eb, cudaStream_t st) {
+                 const ForceCapture* cap, double* eb, bool fast, cudaStream_t st) {
   const ForceCapture c = cap ? *cap : ForceCapture{};
   const int g = blocks(n_max);
 #define BLAZE_STEP_ARGS dp, ops, wg, in_plain, in_sorted, out, ob, n_max, nl, ctl, link, c, eb
-#define BLAZE_STEP(C, S, E) k_step<C, S, E><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS)
-  if (eb) {
+#define BLAZE_STEP(C, S, E) k_step<C, S, E, false><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS)
+#define BLAZE_STEP_FAST(C, S) k_step<C, S, false, true><<<g, kThreads, 0, st>>>(BLAZE_STEP_ARGS)
+  if (fast && !eb) {
+    if (cap) {
+      if (spin_free) BLAZE_STEP_FAST(true, false);
+      else BLAZE_STEP_FAST(true, true);
+    } else {
+      if (spin_free) BLAZE_STEP_FAST(false, false);
+      else BLAZE_STEP_FAST(false, true);
+    }
+  } else if (eb) {
     if (cap) {
       if (spin_free) BLAZE_STEP(true, false, true);
       else BLAZE_STEP(true, true, true);
@@ -901,6 +942,7 @@ void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const Stat
     else BLAZE_STEP(false, true, false);
   }
 #undef BLAZE_STEP
+#undef BLAZE_STEP_FAST
 #undef BLAZE_STEP_ARGS
 }
 

@@ -125,9 +125,11 @@ struct HostStage {
 
 // skin > 0: the gate also re-sorts when the maxima recorded by the step
 // before it say so, and at a block start picks the block's mode
-// (list_needs_rebuild); look = 2 kListCheckEvery dt.
+// (list_needs_rebuild); look = 2 kListCheckEvery dt; vwall = the largest
+// surface speed of a moving wall or volume object, counted at a block start
+// as a particle speed (a wall can set a resting particle in motion).
 void launch_gate(StepCtl* ctl, cudaStream_t st, float skin = 0.0f, float look = 0.0f,
-                 int block_start = 0);
+                 int block_start = 0, float vwall = 0.0f);
 void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int nrb,
                        cudaStream_t st, float skin = 0.0f, float look = 0.0f);
 // Block-start gate of skin > 0 graph stepping: the first node of a block
@@ -137,12 +139,12 @@ void launch_gate_graph(StepCtl* ctl, cudaGraphConditionalHandle h0, int* rb, int
 // (rb[1..nrb) are cleared), the mode to ctl->exact; an exact block's first
 // IF takes ctl->gate_r through launch_gate_body.
 void launch_gate_switch(StepCtl* ctl, cudaGraphConditionalHandle hs, int* rb, int nrb, float skin,
-                        float look, cudaStream_t st);
+                        float look, float vwall, cudaStream_t st);
 void launch_gate_body(StepCtl* ctl, cudaGraphConditionalHandle h0, cudaStream_t st);
 // The gate of plain stepping (launch_gate) as the first node of a one-step
 // graph: its decision also sets the IF node `h` of the step's re-sort.
 void launch_gate_if(StepCtl* ctl, cudaGraphConditionalHandle h, float skin, float look,
-                    int block_start, cudaStream_t st);
+                    int block_start, float vwall, cudaStream_t st);
 void launch_hash(const SimParams* dp, const StateBuf& s, const OrderBuf& ob, int n_max,
                  uint32_t* keys, StepCtl* ctl, const int* gate, cudaStream_t st);
 // (flat_n, when given, is reset for the contact-list kernel's flat list)
@@ -155,11 +157,12 @@ void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint3
                   cudaStream_t st);
 // eb: when not null, the step also writes each particle's energy-tally
 // values (particle-particle, volume objects, world objects; FP64) to
-// eb[c * n_max + i].
+// eb[c * n_max + i].  fast: the contracted particle-particle law (ignored
+// when eb is given: tallies use the reference's arithmetic).
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,
                  const StateBuf& in_sorted, const StateBuf& out, const OrderBuf& ob, int n_max,
                  NbrList nl, StepCtl* ctl, StepLink link, bool spin_free,
-                 const ForceCapture* cap, double* eb, cudaStream_t st);
+                 const ForceCapture* cap, double* eb, bool fast, cudaStream_t st);
 // tally[c] += sum of eb[c * n_max + i] over the current particles, in a fixed
 // order; part holds 3 doubles per block of kEnergyBlock particles.
 constexpr int kEnergyBlock = 256;

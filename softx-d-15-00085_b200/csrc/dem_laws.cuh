@@ -74,6 +74,48 @@ __device__ __forceinline__ Forces law_pp(const SimParams& P, float3 rvel, float3
                            tangential_prefactor(P, pp, ma, mb), e);
 }
 
+// The reference's particle-particle law (law_pp_pre) in contracted form,
+// for runs that ask for agreement within a tolerance instead of bit for bit:
+// fused multiply-adds, an approximate reciprocal square root, and the
+// tangential force as -(tan_pre / |v_rel|) v_t, which is the reference's
+// -(tan_pre |v_t| / |v_rel|) (v_t / |v_t|) without forming |v_t|.  The
+// normal force uses the caller's penetration unchanged (it carries the
+// cancellation of |xa - xb| - (ra + rb), so it is formed as the reference
+// forms it).  Differs from law_pp_pre by a few ulp of the force's terms.
+template <bool kSpin>
+__device__ __forceinline__ Forces law_pp_fast(const SimParams& P, float3 rvel, float3 n,
+                                              float pen, float3 ra, float3 rb, float3 wa,
+                                              float3 wb, const PP_Parms& pp, float3 va,
+                                              float3 vb, float tan_pre) {
+  Forces F;
+  const float vrn = fmaf(rvel.x, n.x, fmaf(rvel.y, n.y, rvel.z * n.z));
+  // Kn pen n - Cn (v_rel . n) n
+  const float fnt = fmaf(-pp.Cn, vrn, pp.Kn * pen);
+  float3 dv = rvel;
+  float dvn = vrn;
+  if (kSpin) {
+    // (va + wa x ra) - (vb + wb x rb)
+    dv = f3(rvel.x + fmaf(wa.y, ra.z, -wa.z * ra.y) - fmaf(wb.y, rb.z, -wb.z * rb.y),
+            rvel.y + fmaf(wa.z, ra.x, -wa.x * ra.z) - fmaf(wb.z, rb.x, -wb.x * rb.z),
+            rvel.z + fmaf(wa.x, ra.y, -wa.y * ra.x) - fmaf(wb.x, rb.y, -wb.y * rb.x));
+    dvn = fmaf(dv.x, n.x, fmaf(dv.y, n.y, dv.z * n.z));
+  }
+  // v_t = dv - (dv . n) n
+  const float3 vt = f3(fmaf(-dvn, n.x, dv.x), fmaf(-dvn, n.y, dv.y), fmaf(-dvn, n.z, dv.z));
+  const float vt2 = fmaf(vt.x, vt.x, fmaf(vt.y, vt.y, vt.z * vt.z));
+  float3 f = n * fnt;
+  if (vt2 > 0.0f) {
+    const float v2 = fmaf(rvel.x, rvel.x, fmaf(rvel.y, rvel.y, rvel.z * rvel.z));
+    const float k = -tan_pre * (v2 > 0.0f ? rsqrtf(v2) : 1.0f);
+    f = f3(fmaf(k, vt.x, f.x), fmaf(k, vt.y, f.y), fmaf(k, vt.z, f.z));
+  }
+  F.trans = f;
+  F.torque = (kSpin && P.rotation) ? f3(fmaf(ra.y, f.z, -ra.z * f.y), fmaf(ra.z, f.x, -ra.x * f.z),
+                                        fmaf(ra.x, f.y, -ra.y * f.x))
+                                   : f3(0.0f, 0.0f, 0.0f);
+  return F;
+}
+
 // Collision_Response_Particle_StaticSurface, Collision_Response.cuh:4-109
 __device__ __forceinline__ Forces law_static_surface(const SimParams& P, float3 pvel, float3 n,
                                                      float pen, float3 r, float3 w,

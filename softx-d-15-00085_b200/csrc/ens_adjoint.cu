@@ -138,7 +138,8 @@ __device__ float3 pair_vjp(const EnsSysDev& S, const Body& a, const Body& b, flo
   const float dist = sqrtf(dot3(rel, rel));
   const float inv = 1.0f / dist;
   const float3 n = rel * inv;
-  const float delta = (a.r + b.r) - dist;
+  const float delta = overlap_pair(a.r, b.r, ff_diff(a.x.x, b.x.x), ff_diff(a.x.y, b.x.y),
+                                   ff_diff(a.x.z, b.x.z), dist);
   const float ms = (a.m * b.m) / (a.m + b.m);
   const float3 ua = n * (-a.r), ub = n * b.r;
   const float3 vca = a.v + cross3(a.w, ua);
@@ -170,7 +171,7 @@ __device__ float3 plane_vjp(const EnsSysDev& S, const EnsWallDev& W, const Body&
                             float dt, float3 Fb, float3 Tb, float3 Xb, SBar& ab, LawBar& th,
                             float& mu_wb) {
   const float3 n = W.a;
-  const float delta = a.r - (dot3(W.a, a.x) - W.r);
+  const float delta = overlap_plane(a.r, W.a, W.r, a.x);
   const float3 ua = n * (-a.r);
   const float3 vca = a.v + cross3(a.w, ua);
   float3 nb, vrelb, vctb, xib;
@@ -379,8 +380,7 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   int nw = 0;
   for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
     const EnsWallDev W = g.walls[w];
-    const float s = dot3(W.a, A.x) - W.r;
-    if (!(s < A.r)) continue;
+    if (!(overlap_plane(A.r, W.a, W.r, A.x) > 0.0f)) continue;   // as wall_touch decides
     float3 xi = f3(0.0f, 0.0f, 0.0f);
     int qo = -1;
 #pragma unroll

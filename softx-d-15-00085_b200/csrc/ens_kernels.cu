@@ -102,35 +102,40 @@ __device__ __forceinline__ void contact_law(const EnsSysDev& S, float mu, float3
 
 // Closest point of triangle (a, b, c) to p by Voronoi regions of the
 // vertices, edges and face (Ericson, Real-Time Collision Detection, 5.1.5).
-// region: 0 face interior, 1 edge, 2 vertex.
+// region: 0 face interior, 1 edge, 2 vertex; feat: the vertex (0 a, 1 b,
+// 2 c) or edge (0 ab, 1 ac, 2 bc) it lies on.
 __device__ __forceinline__ float3 closest_on_triangle(float3 p, float3 a, float3 b, float3 c,
-                                                      int& region) {
+                                                      int& region, int& feat) {
   const float3 ab = b - a, ac = c - a, ap = p - a;
   const float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
-  if (d1 <= 0.0f && d2 <= 0.0f) { region = 2; return a; }
+  if (d1 <= 0.0f && d2 <= 0.0f) { region = 2; feat = 0; return a; }
   const float3 bp = p - b;
   const float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
-  if (d3 >= 0.0f && d4 <= d3) { region = 2; return b; }
+  if (d3 >= 0.0f && d4 <= d3) { region = 2; feat = 1; return b; }
   const float vc = d1 * d4 - d3 * d2;
   if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
     region = 1;
+    feat = 0;
     return a + ab * (d1 / (d1 - d3));
   }
   const float3 cp = p - c;
   const float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
-  if (d6 >= 0.0f && d5 <= d6) { region = 2; return c; }
+  if (d6 >= 0.0f && d5 <= d6) { region = 2; feat = 2; return c; }
   const float vb = d5 * d2 - d1 * d6;
   if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
     region = 1;
+    feat = 1;
     return a + ac * (d2 / (d2 - d6));
   }
   const float va = d3 * d6 - d5 * d4;
   if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
     region = 1;
+    feat = 2;
     return b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
   }
   const float den = 1.0f / ((va + vb) + vc);
   region = 0;
+  feat = 0;
   return a + ab * (vb * den) + ac * (vc * den);
 }
 
@@ -140,29 +145,86 @@ __device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float 
                                            float& delta, int& region) {
   region = 0;
   if (W.kind == kWallPlane) {
-    const float s = dot3(W.a, p) - W.r;
-    if (!(s < r)) return false;
+    delta = overlap_plane(r, W.a, W.r, p);
+    if (!(delta > 0.0f)) return false;
     n = W.a;
-    delta = r - s;
     return true;
   }
   if (W.kind == kWallCylinder) {
-    const float3 v = p - W.a;
-    const float3 rad = v - dot3(v, W.b) * W.b;
-    const float rho = len3(rad);
-    if (!(rho + r > W.r) || !(rho > 0.0f)) return false;
-    n = rad * (-1.0f / rho);
-    delta = (rho + r) - W.r;
+    // v = p - a exactly, then rad = v - (v . b) b and |rad|^2 in double-float
+    const ff v[3] = {ff_diff(p.x, W.a.x), ff_diff(p.y, W.a.y), ff_diff(p.z, W.a.z)};
+    const float b[3] = {W.b.x, W.b.y, W.b.z};
+    float vb = 0.0f, vbc = 0.0f;
+    for (int k = 0; k < 3; ++k) acc_prod(vb, vbc, v[k], ff{b[k], 0.0f});
+    ff rad[3];
+    float t = 0.0f, u = 0.0f;
+    for (int k = 0; k < 3; ++k) {
+      float e, e2;
+      const float q = two_prod(vb, b[k], e);   // (vb + vbc) b = q + e + vbc b
+      rad[k].hi = two_sum(v[k].hi, -q, e2);
+      rad[k].lo = ((v[k].lo + e2) - e) - vbc * b[k];
+      acc_sq(t, u, rad[k]);
+    }
+    const float rho = sqrtf(t + u);
+    // (rho + r) - R = (rho^2 - (R - r)^2) / (rho + (R - r)), R - r exact
+    ff rr;
+    rr.hi = two_sum(W.r, -r, rr.lo);
+    float t2 = 0.0f, u2 = 0.0f;
+    acc_sq(t2, u2, rr);
+    acc_add(t, u, -t2);
+    u = u - u2;
+    delta = (t + u) / (rho + rr.hi);
+    if (!(delta > 0.0f) || !(rho > 0.0f)) return false;
+    n = f3(rad[0].hi, rad[1].hi, rad[2].hi) * (-1.0f / rho);
     return true;
   }
-  const float3 q = closest_on_triangle(p, W.a, W.b, W.c, region);
+  int feat;
+  const float3 q = closest_on_triangle(p, W.a, W.b, W.c, region, feat);
   const float3 d = p - q;
   const float d2 = dot3(d, d);
   if (!(d2 < r * r)) return false;
-  const float dist = sqrtf(d2);
+  if (region == 0) {
+    // face: the signed distance (p - a) . n, n the unit normal in double-float
+    const ff pa[3] = {ff_diff(p.x, W.a.x), ff_diff(p.y, W.a.y), ff_diff(p.z, W.a.z)};
+    float s = 0.0f, c = 0.0f;
+    acc_prod(s, c, pa[0], ff{W.nh.x, W.nl.x});
+    acc_prod(s, c, pa[1], ff{W.nh.y, W.nl.y});
+    acc_prod(s, c, pa[2], ff{W.nh.z, W.nl.z});
+    const float sg = s < 0.0f ? -1.0f : 1.0f;
+    delta = (r - sg * s) - sg * c;
+    if (!(delta > 0.0f) || !(sg * s > 0.0f)) return false;
+    n = W.nh * sg;
+    return true;
+  }
+  // vertex: p - v exactly; edge: p - v0 less its part along the unit edge
+  const float3 v0 = region == 2 ? (feat == 0 ? W.a : (feat == 1 ? W.b : W.c))
+                                : (feat == 2 ? W.b : W.a);
+  const ff pv[3] = {ff_diff(p.x, v0.x), ff_diff(p.y, v0.y), ff_diff(p.z, v0.z)};
+  float t = 0.0f, u = 0.0f;
+  for (int k = 0; k < 3; ++k) acc_sq(t, u, pv[k]);
+  float3 dir = f3(pv[0].hi, pv[1].hi, pv[2].hi);
+  if (region == 1) {
+    const float3 eh = W.eh[feat], el = W.el[feat];
+    float s = 0.0f, c = 0.0f;
+    acc_prod(s, c, pv[0], ff{eh.x, el.x});
+    acc_prod(s, c, pv[1], ff{eh.y, el.y});
+    acc_prod(s, c, pv[2], ff{eh.z, el.z});
+    float s2 = 0.0f, c2 = 0.0f;
+    acc_sq(s2, c2, ff{s, c});
+    acc_add(t, u, -s2);   // |p - v0|^2 - ((p - v0) . e)^2
+    u = u - c2;
+    dir = dir - eh * s;
+  }
+  const float dist = sqrtf(t + u);
   if (!(dist > 0.0f)) return false;
-  n = d * (1.0f / dist);
-  delta = r - dist;
+  // r - dist = (r^2 - dist^2) / (r + dist)
+  float er;
+  float S = two_prod(r, r, er), C = er;
+  acc_add(S, C, -t);
+  C = C - u;
+  delta = (S + C) / (r + dist);
+  if (!(delta > 0.0f)) return false;
+  n = dir * (1.0f / len3(dir));
   return true;
 }
 
@@ -394,7 +456,8 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     const float dist = sqrtf(d2);
     if (!(dist > 0.0f)) continue;
     const float3 nrm = rel * (1.0f / dist);
-    const float delta = sr - dist;
+    const float delta = overlap_pair(ra, rb, ff_diff(pa.x, pb4.x), ff_diff(pa.y, pb4.y),
+                                     ff_diff(pa.z, pb4.z), dist);
     const float4 vb4 = __ldg(in.vel + j), wb4 = __ldg(in.angv + j);
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);

@@ -65,6 +65,38 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 std::mutex g_mu;
 unsigned char* g_base[kMaxDevices] = {};
 
+// What the broad-phase kernels read from SimParams, passed by value to the
+// kernel that writes the call's parameters and control words into the
+// scratch array (no copy from host memory).
+struct StaticParams {
+  float3 origin, cell;
+  int3 ncells;
+  uint32_t ncell_tab;
+  float skin;
+  int max_nbr;
+  int n;
+};
+
+static_assert(sizeof(SimParams) % 4 == 0 && sizeof(StepCtl) % 4 == 0, "zeroed as 32-bit words");
+
+// One block: zeroes the SimParams and StepCtl slots, then sets the fields
+// the hash, reorder and contact-list kernels read.
+__global__ void k_static_init(StaticParams sp, SimParams* dp, StepCtl* ctl) {
+  uint32_t* pw = reinterpret_cast<uint32_t*>(dp);
+  uint32_t* cw = reinterpret_cast<uint32_t*>(ctl);
+  for (size_t k = threadIdx.x; k < sizeof(SimParams) / 4; k += blockDim.x) pw[k] = 0u;
+  for (size_t k = threadIdx.x; k < sizeof(StepCtl) / 4; k += blockDim.x) cw[k] = 0u;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  dp->origin = sp.origin;
+  dp->cell = sp.cell;
+  dp->ncells = sp.ncells;
+  dp->ncell_tab = sp.ncell_tab;
+  dp->skin = sp.skin;
+  dp->max_nbr = sp.max_nbr;
+  ctl->n_cur = sp.n;
+}
+
 int cuda_fail(cudaError_t e) {
   std::fprintf(stderr, "blaze: CUDA error %d (%s)\n", (int)e, cudaGetErrorString(e));
   return -(1000 + (int)e);
@@ -113,17 +145,14 @@ extern "C" int blaze_contact_list_static(const float* pos4, int n, const Simulat
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  SimParams hp;
-  std::memset(&hp, 0, sizeof(hp));
-  hp.origin = si->worldOrigin;
-  hp.cell = si->cellSize;
-  hp.ncells = si->num_NNCells;
-  hp.ncell_tab = (uint32_t)ntab;
-  hp.skin = skin;
-  hp.max_nbr = max_nbr;
-  StepCtl hc;
-  std::memset(&hc, 0, sizeof(hc));
-  hc.n_cur = n;
+  StaticParams sp;
+  sp.origin = si->worldOrigin;
+  sp.cell = si->cellSize;
+  sp.ncells = si->num_NNCells;
+  sp.ncell_tab = (uint32_t)ntab;
+  sp.skin = skin;
+  sp.max_nbr = max_nbr;
+  sp.n = n;
 
   SimParams* dp = reinterpret_cast<SimParams*>(base + kOffParams);
   StepCtl* ctl = reinterpret_cast<StepCtl*>(base + kOffCtl);
@@ -159,8 +188,7 @@ extern "C" int blaze_contact_list_static(const float* pos4, int n, const Simulat
     if (e_ != cudaSuccess) return cuda_fail(e_);  \
   } while (0)
   // what this call relies on starting from a known value
-  CKS(cudaMemcpyAsync(dp, &hp, sizeof(hp), cudaMemcpyHostToDevice, st));
-  CKS(cudaMemcpyAsync(ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st));
+  k_static_init<<<1, 256, 0, st>>>(sp, dp, ctl);
   CKS(cudaMemsetAsync(ob.pid[0], 0, sizeof(int) * n, st));  // every particle live
   CKS(cudaMemsetAsync(cstart, 0xff, sizeof(uint32_t) * ntab, st));
   launch_hash(dp, src, ob, n, rs.keys[0], ctl, nullptr, st);

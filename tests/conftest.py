@@ -15,7 +15,9 @@ for p in (PKG, os.path.join(REPO, "oracle")):
 from blaze import types as T  # noqa: E402
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
-REFERENCE = "/root/reference"
+# the reference tree (only the CPU tests that compile or parse it read it):
+# $BLAZE_REFERENCE, else a directory "reference" beside the repository
+REFERENCE = os.environ.get("BLAZE_REFERENCE", os.path.join(os.path.dirname(REPO), "reference"))
 
 
 def pytest_configure(config):

@@ -3,7 +3,8 @@ project files and the reference's own kernels (oracle A: the reference's
 DEM kernels compiled as host C++, oracle/_ref/libblaze_refhost.so).
 
 Run in a container that has the reference tree (its path is the first
-argument, default /root/reference) after `make -C oracle ref`:
+argument, default $BLAZE_REFERENCE, else a directory "reference" beside the
+repository) after `make -C oracle ref`:
 
     python tests/golden/make_golden.py [/path/to/reference] [fixture ...]
 
@@ -357,7 +358,8 @@ def make_mill_fill(ref_root, name):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "BLAZE_REFERENCE", os.path.join(os.path.dirname(REPO), "reference"))
     which = sys.argv[2:] or None
     if which is None or "box_grid" in which:
         make_grid(ref_root, "box_grid", "1.Particles_Box", "Spheres_128cm")

@@ -1,0 +1,103 @@
+"""The contracted particle-particle law (blaze_options.fast_law = 1) against
+the reference's own kernels on its own projects (oracle-A golden fixtures:
+Projects/2.Silo world SPH_90, 1,950 spheres with the silo hatch;
+Projects/3.BallMill world Mill_SPH30, 242 spheres, rotating drum and
+lifters), and against the FP64 restatement of the reference law on the
+synthetic 10,000-sphere box.
+
+Bar: the contact lists are the reference's bit for bit (the contact test is
+not contracted); the forces of the first step agree within 1e-5 relative,
+per particle, where the scale of a particle is the larger of its net force
+and its weight (a particle whose contact forces nearly cancel carries their
+rounding, not its net force's); the state after the step agrees within the
+same relative bound on the velocity change.  The error of the bit-exact law
+against FP64 is printed beside the contracted one's."""
+import numpy as np
+import pytest
+
+from bindings import Restated
+from blaze import device, synth
+from conftest import Golden
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def gpu_sim(g, **opts):
+    s = device.Simulation(sim_info=g.sim_info, wobj=g.wobj, n_w=g.n_w, pobj=g.pobj, n_p=g.n_p,
+                          dobj=g.dobj, n_d=g.n_d, **opts)
+    s.set_cylinder_rotation(g.cyl_rot)
+    st = g.init()
+    s.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    return s
+
+
+def rel_err(f, ref, weight):
+    scale = np.maximum(np.linalg.norm(ref, axis=1), weight)
+    return float((np.linalg.norm(f.astype(np.float64) - ref, axis=1) / scale).max())
+
+
+@pytest.mark.parametrize("name", ["silo_sph90", "mill_sph30"])
+def test_fast_law_vs_reference_kernels(name):
+    g = Golden(name)
+    s = gpu_sim(g, capture_forces=1, fast_law=1)
+    s.step(1)
+    ref = g.at(1)
+    st = s.state()
+    assert st["status"] == 0, device.decode_status(st["status"])
+    nn, lst = s.nlist()
+    np.testing.assert_array_equal(nn, ref["nn"])
+    w = ref["list"].shape[1]
+    np.testing.assert_array_equal(lst[:, :w], ref["list"])
+    np.testing.assert_array_equal(st["pid"], ref["pid"])
+    f = s.forces()
+    gmag = float(np.linalg.norm([g.sim_info.Force_Field.x, g.sim_info.Force_Field.y,
+                                 g.sim_info.Force_Field.z]))
+    mass = np.array([g.pobj[t].mass for t in st["type"]], np.float64)
+    weight = mass * gmag
+    e_pp = rel_err(f["f_pp"], ref["f_pp"].astype(np.float64), weight)
+    # walls and lifters keep the reference's arithmetic
+    for key in ("f_wall", "t_wall", "f_lift", "t_lift"):
+        np.testing.assert_array_equal(f[key], ref[key], err_msg=key)
+    dt = float(np.float32(g.sim_info.InitalDelta_t))
+    vel_scale = np.maximum(np.linalg.norm(ref["vel"], axis=1), gmag * dt)
+    e_v = float((np.linalg.norm(st["vel"].astype(np.float64) - ref["vel"], axis=1) / vel_scale).max())
+    print("%s: contracted law, step 1: force %.2e, velocity %.2e (relative, per particle)"
+          % (name, e_pp, e_v))
+    s.close()
+    assert e_pp < TOL, e_pp
+    assert e_v < TOL, e_v
+
+
+def test_fast_law_vs_fp64_box(tmp_path):
+    """10,000 spheres of the box configuration after 400 steps of settling:
+    one step's particle-particle forces, contracted and bit-exact, against
+    the FP64 restatement of the reference law from the same state."""
+    P, st0 = synth.box_project(str(tmp_path))
+    s = device.Simulation(P, skin=0.02, use_graph=1)
+    s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
+    s.step(400)
+    st = s.state()
+    s.close()
+    assert st["status"] == 0
+    out = {}
+    for fast in (0, 1):
+        g = device.Simulation(P, capture_forces=1, fast_law=fast)
+        g.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+        g.step(1)
+        f = g.forces()["f_pp"]
+        pid = g.state()["pid"]
+        g.close()
+        out[fast] = f[np.argsort(pid)]
+    o = Restated("f64").init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d)
+    o.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    o.step(1)
+    f64 = o.forces()["f_pp"][np.argsort(o.state()["pid"])]
+    weight = float(P.pobj[0].mass) * 981.0
+    e_exact = rel_err(out[0], f64, weight)
+    e_fast = rel_err(out[1], f64, weight)
+    e_pair = rel_err(out[1], out[0].astype(np.float64), weight)
+    print("box, 10,000 spheres: vs FP64 bit-exact %.2e contracted %.2e; contracted vs bit-exact "
+          "%.2e" % (e_exact, e_fast, e_pair))
+    assert e_pair < TOL, e_pair

@@ -225,3 +225,54 @@ def test_shared_reciprocal_division_is_ieee():
     lib.blaze_check_division.restype = ctypes.c_longlong
     lib.blaze_check_division.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong]
     assert lib.blaze_check_division(1 << 30, 12345) == 0
+
+
+def test_moving_walls_enter_the_list_check(tmp_path):
+    """A drum turning at 30 rpm (wall and lifter surface speed up to 157
+    cm/s) with a 0.015 cm skin at dt 2e-6 s: from the first block start the
+    list check counts that surface speed as a particle speed, so every block
+    runs exact although the charge starts at rest (a lifter can set a resting
+    sphere in motion within a block).  Graph and plain stepping agree bit for
+    bit, and no stale-list status is raised."""
+    P, st = synth.mill_project(str(tmp_path), n=3000)
+    R = float(P.wobj[0].cyl_geo.radius)
+    rad = float(P.mill.RadPerStep)
+    out = []
+    for g in (0, 1):
+        s = device.Simulation(P, skin=0.015, use_graph=g)
+        s.set_cylinder_rotation(True)
+        s.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+        s.set_dobj_rotation(R, R, rad)
+        s.step(64)
+        out.append((s.state(), s.num_exact_blocks()))
+        s.close()
+    (a, xa), (b, xb) = out
+    assert a["status"] == 0 and b["status"] == 0, device.decode_status(a["status"] | b["status"])
+    assert xa == xb == 7, (xa, xb)   # block starts 8, 16, ..., 56
+    for key in ("pos", "vel", "avel", "pid"):
+        np.testing.assert_array_equal(a[key], b[key])
+
+
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_stale_list_status_raised(box, use_graph):
+    """A box of resting spheres keeps its list through a block (no check
+    inside it); then the whole box is moved 0.21 cm up between two calls,
+    into the bottom layer.  The spheres it strikes leave at thousands of cm/s
+    within the block, past half the 0.02 cm skin before the next check, and
+    the step reports it as status bit 64 (stale list) instead of silently
+    missing contacts."""
+    P, st0 = box
+    s = device.Simulation(P, skin=0.02, use_graph=use_graph)
+    s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
+    s.step(16)
+    assert s.sync() == 0
+    w = s.wobj()
+    for k in range(w[0].num_vertex):
+        w[0].vertex[k].z += 0.21
+    for f in range(w[0].num_surfaces):
+        w[0].surfaces[f].centroid.z += 0.21
+    s.update_wobj(w, P.n_w)
+    s.step(8)
+    st = s.sync()
+    s.close()
+    assert st & 64, device.decode_status(st)

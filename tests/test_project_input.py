@@ -11,7 +11,9 @@ import canon
 from blaze import types as T
 from blaze.project import Project, read_state_file
 
-REF_PROJECTS = "/root/reference/Projects"
+from conftest import REFERENCE
+
+REF_PROJECTS = os.path.join(REFERENCE, "Projects")
 need_ref_tree = pytest.mark.skipif(not os.path.isdir(REF_PROJECTS),
                                    reason="reference project tree not present")
 need_ref_lib = pytest.mark.skipif(not bindings.ref_available(), reason="oracle/_ref not built")
