@@ -63,85 +63,27 @@ typedef struct {
   int kind;
   real r;
   v3 a, b, c;
-  v3 nh, nl, eh[3], el[3];   /* triangle: unit normal, unit edges ab, ac, bc as hi + lo */
+  double n64[3], e64[3][3];   /* triangle: unit normal, unit edges ab, ac, bc (double) */
 } wallc;
 
-/* Accurate overlaps (csrc/ens_kernels.cuh, "accurate overlaps"): the same
- * error-free transformations in the same order.  In the FP64 build the
- * same code runs in double (the lo parts of the triangle's unit vectors
- * are then zero). */
-typedef struct { real hi, lo; } ffr;
-static real FMA(real a, real b, real c) {
-  return IS_FLOAT ? (real)fmaf((float)a, (float)b, (float)c) : (real)fma((double)a, (double)b, (double)c);
-}
-static real two_sum(real a, real b, real* e) {
-  const real s = a + b;
-  const real bb = s - a;
-  *e = (a - (s - bb)) + (b - bb);
-  return s;
-}
-static real two_prod(real a, real b, real* e) {
-  const real p = a * b;
-  *e = FMA(a, b, -p);
-  return p;
-}
-static void acc_add(real* s, real* c, real x) {
-  real e;
-  *s = two_sum(*s, x, &e);
-  *c = *c + e;
-}
-static ffr ff_diff(real a, real b) {
-  ffr r;
-  r.hi = two_sum(a, -b, &r.lo);
-  return r;
-}
-static ffr ffv(real hi, real lo) { ffr r = {hi, lo}; return r; }
-static void acc_sq(real* s, real* c, ffr x) {
-  real e;
-  const real p = two_prod(x.hi, x.hi, &e);
-  acc_add(s, c, p);
-  *c = *c + (e + (real)2.0 * (x.hi * x.lo));
-}
-static void acc_prod(real* s, real* c, ffr x, ffr y) {
-  real e;
-  const real p = two_prod(x.hi, y.hi, &e);
-  acc_add(s, c, p);
-  *c = *c + (e + (x.hi * y.lo + x.lo * y.hi));
-}
-static real overlap_pair(real ra, real rb, v3 pa, v3 pb, real dist) {
-  ffr sr;
-  sr.hi = two_sum(ra, rb, &sr.lo);
-  real s = 0, c = 0;
-  acc_sq(&s, &c, sr);
-  real t = 0, u = 0;
-  acc_sq(&t, &u, ff_diff(pa.x, pb.x));
-  acc_sq(&t, &u, ff_diff(pa.y, pb.y));
-  acc_sq(&t, &u, ff_diff(pa.z, pb.z));
-  acc_add(&s, &c, -t);
-  c = c - u;
-  return (s + c) / (sr.hi + dist);
+/* Accurate overlaps (csrc/ens_kernels.cuh, "accurate overlaps"): formed in
+ * double from the working-precision state, as the kernels do, then rounded
+ * to the working precision once. */
+static double dotd(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static real overlap_pair(real ra, real rb, v3 pa, v3 pb) {
+  const double d[3] = {(double)pa.x - (double)pb.x, (double)pa.y - (double)pb.y,
+                       (double)pa.z - (double)pb.z};
+  return (real)(((double)ra + (double)rb) - sqrt(dotd(d, d)));
 }
 static real overlap_plane(real r, v3 n, real d, v3 p) {
-  real e0, e1, e2, c;
-  const real q0 = two_prod(n.x, p.x, &e0), q1 = two_prod(n.y, p.y, &e1), q2 = two_prod(n.z, p.z, &e2);
-  real s = two_sum(r, d, &c);
-  acc_add(&s, &c, -q0);
-  acc_add(&s, &c, -q1);
-  acc_add(&s, &c, -q2);
-  c = c - ((e0 + e1) + e2);
-  return s + c;
+  const double nn[3] = {n.x, n.y, n.z}, pp[3] = {p.x, p.y, p.z};
+  return (real)(((double)r + (double)d) - dotd(nn, pp));
 }
-/* a unit vector computed in double from float components, as hi + lo */
-static void unit_split(double x, double y, double z, v3* hi, v3* lo) {
+static void unit64(double x, double y, double z, double* u) {
   const double l = sqrt(x * x + y * y + z * z);
-  const double u[3] = {l > 0 ? x / l : 0.0, l > 0 ? y / l : 0.0, l > 0 ? z / l : 0.0};
-  real h[3], o[3];
-  for (int k = 0; k < 3; ++k) {
-    h[k] = IN(u[k]);
-    o[k] = IN(u[k] - (double)h[k]);
-  }
-  *hi = mk(h[0], h[1], h[2]);
-  *lo = mk(o[0], o[1], o[2]);
+  u[0] = l > 0 ? x / l : 0.0;
+  u[1] = l > 0 ? y / l : 0.0;
+  u[2] = l > 0 ? z / l : 0.0;
 }
 
 typedef struct {
@@ -229,11 +171,11 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
       const double ab[3] = {(double)p[3] - p[0], (double)p[4] - p[1], (double)p[5] - p[2]};
       const double ac[3] = {(double)p[6] - p[0], (double)p[7] - p[1], (double)p[8] - p[2]};
       const double bc[3] = {(double)p[6] - p[3], (double)p[7] - p[4], (double)p[8] - p[5]};
-      unit_split(ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2],
-                 ab[0] * ac[1] - ab[1] * ac[0], &d->nh, &d->nl);
-      unit_split(ab[0], ab[1], ab[2], &d->eh[0], &d->el[0]);
-      unit_split(ac[0], ac[1], ac[2], &d->eh[1], &d->el[1]);
-      unit_split(bc[0], bc[1], bc[2], &d->eh[2], &d->el[2]);
+      unit64(ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2],
+             ab[0] * ac[1] - ab[1] * ac[0], d->n64);
+      unit64(ab[0], ab[1], ab[2], d->e64[0]);
+      unit64(ac[0], ac[1], ac[2], d->e64[1]);
+      unit64(bc[0], bc[1], bc[2], d->e64[2]);
     } else { d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->r = p[6]; }
   }
   o->p = (part*)calloc(n, sizeof(part));
@@ -498,29 +440,16 @@ static int wall_touch(const wallc* W, v3 p, real r, v3* n, real* delta, int* reg
     return 1;
   }
   if (W->kind == BLAZE_WALL_CYLINDER) {
-    const ffr v[3] = {ff_diff(p.x, W->a.x), ff_diff(p.y, W->a.y), ff_diff(p.z, W->a.z)};
-    const real b[3] = {W->b.x, W->b.y, W->b.z};
-    real vb = 0, vbc = 0;
-    for (int k = 0; k < 3; ++k) acc_prod(&vb, &vbc, v[k], ffv(b[k], 0));
-    ffr rad[3];
-    real t = 0, u = 0;
-    for (int k = 0; k < 3; ++k) {
-      real e, e2;
-      const real q = two_prod(vb, b[k], &e);
-      rad[k].hi = two_sum(v[k].hi, -q, &e2);
-      rad[k].lo = ((v[k].lo + e2) - e) - vbc * b[k];
-      acc_sq(&t, &u, rad[k]);
-    }
-    const real rho = SQRT(t + u);
-    ffr rr;
-    rr.hi = two_sum(W->r, -r, &rr.lo);
-    real t2 = 0, u2 = 0;
-    acc_sq(&t2, &u2, rr);
-    acc_add(&t, &u, -t2);
-    u = u - u2;
-    *delta = (t + u) / (rho + rr.hi);
+    const double v[3] = {(double)p.x - (double)W->a.x, (double)p.y - (double)W->a.y,
+                         (double)p.z - (double)W->a.z};
+    const double b[3] = {W->b.x, W->b.y, W->b.z};
+    const double vb = dotd(v, b);
+    const double rad[3] = {v[0] - vb * b[0], v[1] - vb * b[1], v[2] - vb * b[2]};
+    const double rho = sqrt(dotd(rad, rad));
+    *delta = (real)(((double)r + rho) - (double)W->r);
     if (!(*delta > 0) || !(rho > 0)) return 0;
-    *n = mul(mk(rad[0].hi, rad[1].hi, rad[2].hi), (real)-1.0 / rho);
+    const real rinv = (real)(-1.0 / rho);
+    *n = mk((real)rad[0] * rinv, (real)rad[1] * rinv, (real)rad[2] * rinv);
     return 1;
   }
   int feat;
@@ -529,44 +458,31 @@ static int wall_touch(const wallc* W, v3 p, real r, v3* n, real* delta, int* reg
   const real d2 = dot(d, d);
   if (!(d2 < r * r)) return 0;
   if (*region == 0) {
-    const ffr pa[3] = {ff_diff(p.x, W->a.x), ff_diff(p.y, W->a.y), ff_diff(p.z, W->a.z)};
-    real s = 0, c = 0;
-    acc_prod(&s, &c, pa[0], ffv(W->nh.x, W->nl.x));
-    acc_prod(&s, &c, pa[1], ffv(W->nh.y, W->nl.y));
-    acc_prod(&s, &c, pa[2], ffv(W->nh.z, W->nl.z));
-    const real sg = s < 0 ? (real)-1.0 : (real)1.0;
-    *delta = (r - sg * s) - sg * c;
-    if (!(*delta > 0) || !(sg * s > 0)) return 0;
-    *n = mul(W->nh, sg);
+    const double pa[3] = {(double)p.x - (double)W->a.x, (double)p.y - (double)W->a.y,
+                          (double)p.z - (double)W->a.z};
+    const double s = dotd(pa, W->n64);
+    *delta = (real)((double)r - fabs(s));
+    if (!(*delta > 0) || !(s != 0.0)) return 0;
+    const real sg = s < 0.0 ? (real)-1.0 : (real)1.0;
+    *n = mk((real)W->n64[0] * sg, (real)W->n64[1] * sg, (real)W->n64[2] * sg);
     return 1;
   }
   const v3 v0 = *region == 2 ? (feat == 0 ? W->a : (feat == 1 ? W->b : W->c))
                              : (feat == 2 ? W->b : W->a);
-  const ffr pv[3] = {ff_diff(p.x, v0.x), ff_diff(p.y, v0.y), ff_diff(p.z, v0.z)};
-  real t = 0, u = 0;
-  for (int k = 0; k < 3; ++k) acc_sq(&t, &u, pv[k]);
-  v3 dir = mk(pv[0].hi, pv[1].hi, pv[2].hi);
+  double pv[3] = {(double)p.x - (double)v0.x, (double)p.y - (double)v0.y,
+                  (double)p.z - (double)v0.z};
   if (*region == 1) {
-    const v3 eh = W->eh[feat], el = W->el[feat];
-    real s = 0, c = 0;
-    acc_prod(&s, &c, pv[0], ffv(eh.x, el.x));
-    acc_prod(&s, &c, pv[1], ffv(eh.y, el.y));
-    acc_prod(&s, &c, pv[2], ffv(eh.z, el.z));
-    real s2 = 0, c2 = 0;
-    acc_sq(&s2, &c2, ffv(s, c));
-    acc_add(&t, &u, -s2);
-    u = u - c2;
-    dir = sub(dir, mul(eh, s));
+    const double* e = W->e64[feat];
+    const double t = dotd(pv, e);
+    pv[0] = pv[0] - t * e[0];
+    pv[1] = pv[1] - t * e[1];
+    pv[2] = pv[2] - t * e[2];
   }
-  const real dist = SQRT(t + u);
-  if (!(dist > 0)) return 0;
-  real er;
-  real S = two_prod(r, r, &er), C = er;
-  acc_add(&S, &C, -t);
-  C = C - u;
-  *delta = (S + C) / (r + dist);
-  if (!(*delta > 0)) return 0;
-  *n = mul(dir, (real)1.0 / len(dir));
+  const double dist = sqrt(dotd(pv, pv));
+  *delta = (real)((double)r - dist);
+  if (!(*delta > 0) || !(dist > 0)) return 0;
+  const real dinv = (real)(1.0 / dist);
+  *n = mk((real)pv[0] * dinv, (real)pv[1] * dinv, (real)pv[2] * dinv);
   return 1;
 }
 
@@ -655,7 +571,7 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
       const real dist = SQRT(d2);
       if (!(dist > 0)) continue;
       const v3 nrm = mul(rel, (real)1.0 / dist);
-      const real delta = overlap_pair(ra, rb, a->pos, b->pos, dist);
+      const real delta = overlap_pair(ra, rb, a->pos, b->pos);
       const real mb = S->dens43pi * ((rb * rb) * rb);
       v3 xi = mk(0, 0, 0);
       if ((M[i] >> k) & 1u) xi = mk(H[3 * sk], H[3 * sk + 1], H[3 * sk + 2]);
@@ -890,7 +806,7 @@ static v3 pair_vjp(const ens_oracle* o, const sysc* S, const part* a, const part
   const real dist = SQRT(dot(rel, rel));
   const real inv = (real)1.0 / dist;
   const v3 n = mul(rel, inv);
-  const real delta = overlap_pair(ra, rb, a->pos, b->pos, dist);
+  const real delta = overlap_pair(ra, rb, a->pos, b->pos);
   const real ma = S->dens43pi * ((ra * ra) * ra), mb = S->dens43pi * ((rb * rb) * rb);
   const real ms = (ma * mb) / (ma + mb);
   const v3 ua = mul(n, -ra), ub = mul(n, rb);

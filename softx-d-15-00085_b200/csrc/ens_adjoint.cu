@@ -138,8 +138,7 @@ __device__ float3 pair_vjp(const EnsSysDev& S, const Body& a, const Body& b, flo
   const float dist = sqrtf(dot3(rel, rel));
   const float inv = 1.0f / dist;
   const float3 n = rel * inv;
-  const float delta = overlap_pair(a.r, b.r, ff_diff(a.x.x, b.x.x), ff_diff(a.x.y, b.x.y),
-                                   ff_diff(a.x.z, b.x.z), dist);
+  const float delta = overlap_pair(a.r, b.r, a.x, b.x);
   const float ms = (a.m * b.m) / (a.m + b.m);
   const float3 ua = n * (-a.r), ub = n * b.r;
   const float3 vca = a.v + cross3(a.w, ua);

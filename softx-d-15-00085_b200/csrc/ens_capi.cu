@@ -119,6 +119,12 @@ EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off) {
   return d;
 }
 
+// A unit vector computed in double from float components.
+double3 unit64(double x, double y, double z) {
+  const double l = std::sqrt(x * x + y * y + z * z);
+  return l > 0 ? make_double3(x / l, y / l, z / l) : make_double3(0.0, 0.0, 0.0);
+}
+
 EnsWallDev wall_dev(const blaze_wall& w) {
   EnsWallDev d;
   std::memset(&d, 0, sizeof(d));
@@ -127,9 +133,18 @@ EnsWallDev wall_dev(const blaze_wall& w) {
     d.a = make_float3(w.p[0], w.p[1], w.p[2]);
     d.r = w.p[3];
   } else if (w.kind == BLAZE_WALL_TRIANGLE) {
-    d.a = make_float3(w.p[0], w.p[1], w.p[2]);
-    d.b = make_float3(w.p[3], w.p[4], w.p[5]);
-    d.c = make_float3(w.p[6], w.p[7], w.p[8]);
+    const float* p = w.p;
+    d.a = make_float3(p[0], p[1], p[2]);
+    d.b = make_float3(p[3], p[4], p[5]);
+    d.c = make_float3(p[6], p[7], p[8]);
+    const double ab[3] = {(double)p[3] - p[0], (double)p[4] - p[1], (double)p[5] - p[2]};
+    const double ac[3] = {(double)p[6] - p[0], (double)p[7] - p[1], (double)p[8] - p[2]};
+    const double bc[3] = {(double)p[6] - p[3], (double)p[7] - p[4], (double)p[8] - p[5]};
+    d.n64 = unit64(ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2],
+                   ab[0] * ac[1] - ab[1] * ac[0]);
+    d.e64[0] = unit64(ab[0], ab[1], ab[2]);
+    d.e64[1] = unit64(ac[0], ac[1], ac[2]);
+    d.e64[2] = unit64(bc[0], bc[1], bc[2]);
   } else {
     d.a = make_float3(w.p[0], w.p[1], w.p[2]);
     d.b = make_float3(w.p[3], w.p[4], w.p[5]);

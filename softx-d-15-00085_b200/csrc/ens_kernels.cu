@@ -151,31 +151,15 @@ __device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float 
     return true;
   }
   if (W.kind == kWallCylinder) {
-    // v = p - a exactly, then rad = v - (v . b) b and |rad|^2 in double-float
-    const ff v[3] = {ff_diff(p.x, W.a.x), ff_diff(p.y, W.a.y), ff_diff(p.z, W.a.z)};
-    const float b[3] = {W.b.x, W.b.y, W.b.z};
-    float vb = 0.0f, vbc = 0.0f;
-    for (int k = 0; k < 3; ++k) acc_prod(vb, vbc, v[k], ff{b[k], 0.0f});
-    ff rad[3];
-    float t = 0.0f, u = 0.0f;
-    for (int k = 0; k < 3; ++k) {
-      float e, e2;
-      const float q = two_prod(vb, b[k], e);   // (vb + vbc) b = q + e + vbc b
-      rad[k].hi = two_sum(v[k].hi, -q, e2);
-      rad[k].lo = ((v[k].lo + e2) - e) - vbc * b[k];
-      acc_sq(t, u, rad[k]);
-    }
-    const float rho = sqrtf(t + u);
-    // (rho + r) - R = (rho^2 - (R - r)^2) / (rho + (R - r)), R - r exact
-    ff rr;
-    rr.hi = two_sum(W.r, -r, rr.lo);
-    float t2 = 0.0f, u2 = 0.0f;
-    acc_sq(t2, u2, rr);
-    acc_add(t, u, -t2);
-    u = u - u2;
-    delta = (t + u) / (rho + rr.hi);
-    if (!(delta > 0.0f) || !(rho > 0.0f)) return false;
-    n = f3(rad[0].hi, rad[1].hi, rad[2].hi) * (-1.0f / rho);
+    // rad = v - (v . b) b with v = p - a, in double
+    const double3 v = dsub(d3(p), d3(W.a)), b = d3(W.b);
+    const double vb = ddot(v, b);
+    const double3 rad = make_double3(v.x - vb * b.x, v.y - vb * b.y, v.z - vb * b.z);
+    const double rho = sqrt(ddot(rad, rad));
+    delta = (float)(((double)r + rho) - (double)W.r);
+    if (!(delta > 0.0f) || !(rho > 0.0)) return false;
+    const float rinv = (float)(-1.0 / rho);
+    n = f3((float)rad.x * rinv, (float)rad.y * rinv, (float)rad.z * rinv);
     return true;
   }
   int feat;
@@ -184,47 +168,28 @@ __device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float 
   const float d2 = dot3(d, d);
   if (!(d2 < r * r)) return false;
   if (region == 0) {
-    // face: the signed distance (p - a) . n, n the unit normal in double-float
-    const ff pa[3] = {ff_diff(p.x, W.a.x), ff_diff(p.y, W.a.y), ff_diff(p.z, W.a.z)};
-    float s = 0.0f, c = 0.0f;
-    acc_prod(s, c, pa[0], ff{W.nh.x, W.nl.x});
-    acc_prod(s, c, pa[1], ff{W.nh.y, W.nl.y});
-    acc_prod(s, c, pa[2], ff{W.nh.z, W.nl.z});
-    const float sg = s < 0.0f ? -1.0f : 1.0f;
-    delta = (r - sg * s) - sg * c;
-    if (!(delta > 0.0f) || !(sg * s > 0.0f)) return false;
-    n = W.nh * sg;
+    // face: the signed distance (p - a) . n, n the unit normal in double
+    const double s = ddot(dsub(d3(p), d3(W.a)), W.n64);
+    delta = (float)((double)r - fabs(s));
+    if (!(delta > 0.0f) || !(s != 0.0)) return false;
+    const float sg = s < 0.0 ? -1.0f : 1.0f;
+    n = f3((float)W.n64.x * sg, (float)W.n64.y * sg, (float)W.n64.z * sg);
     return true;
   }
-  // vertex: p - v exactly; edge: p - v0 less its part along the unit edge
+  // vertex: p - v; edge: p - v0 less its part along the unit edge e
   const float3 v0 = region == 2 ? (feat == 0 ? W.a : (feat == 1 ? W.b : W.c))
                                 : (feat == 2 ? W.b : W.a);
-  const ff pv[3] = {ff_diff(p.x, v0.x), ff_diff(p.y, v0.y), ff_diff(p.z, v0.z)};
-  float t = 0.0f, u = 0.0f;
-  for (int k = 0; k < 3; ++k) acc_sq(t, u, pv[k]);
-  float3 dir = f3(pv[0].hi, pv[1].hi, pv[2].hi);
+  double3 pv = dsub(d3(p), d3(v0));
   if (region == 1) {
-    const float3 eh = W.eh[feat], el = W.el[feat];
-    float s = 0.0f, c = 0.0f;
-    acc_prod(s, c, pv[0], ff{eh.x, el.x});
-    acc_prod(s, c, pv[1], ff{eh.y, el.y});
-    acc_prod(s, c, pv[2], ff{eh.z, el.z});
-    float s2 = 0.0f, c2 = 0.0f;
-    acc_sq(s2, c2, ff{s, c});
-    acc_add(t, u, -s2);   // |p - v0|^2 - ((p - v0) . e)^2
-    u = u - c2;
-    dir = dir - eh * s;
+    const double3 e = W.e64[feat];
+    const double t = ddot(pv, e);
+    pv = make_double3(pv.x - t * e.x, pv.y - t * e.y, pv.z - t * e.z);
   }
-  const float dist = sqrtf(t + u);
-  if (!(dist > 0.0f)) return false;
-  // r - dist = (r^2 - dist^2) / (r + dist)
-  float er;
-  float S = two_prod(r, r, er), C = er;
-  acc_add(S, C, -t);
-  C = C - u;
-  delta = (S + C) / (r + dist);
-  if (!(delta > 0.0f)) return false;
-  n = dir * (1.0f / len3(dir));
+  const double dist = sqrt(ddot(pv, pv));
+  delta = (float)((double)r - dist);
+  if (!(delta > 0.0f) || !(dist > 0.0)) return false;
+  const float dinv = (float)(1.0 / dist);
+  n = f3((float)pv.x * dinv, (float)pv.y * dinv, (float)pv.z * dinv);
   return true;
 }
 
@@ -456,8 +421,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     const float dist = sqrtf(d2);
     if (!(dist > 0.0f)) continue;
     const float3 nrm = rel * (1.0f / dist);
-    const float delta = overlap_pair(ra, rb, ff_diff(pa.x, pb4.x), ff_diff(pa.y, pb4.y),
-                                     ff_diff(pa.z, pb4.z), dist);
+    const float delta = overlap_pair(ra, rb, pa, xyz(pb4));
     const float4 vb4 = __ldg(in.vel + j), wb4 = __ldg(in.angv + j);
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);

@@ -56,94 +56,42 @@ struct EnsWallDev {
   float3 a, b, c;      // plane: a = unit normal into the domain; triangle: vertices;
                        // cylinder: a = point on the axis, b = unit axis
   // triangle: the unit face normal and the unit edge directions (ab, ac,
-  // bc), each as an unevaluated sum hi + lo of two floats (computed in
-  // double on the host from the float vertices), for the overlaps below
-  float3 nh, nl;
-  float3 eh[3], el[3];
+  // bc), computed in double on the host from the float vertices
+  double3 n64;
+  double3 e64[3];
 };
 
 // ------------------------------------------------------ accurate overlaps
 // The overlap of a contact is a small difference of lengths of the size of
 // the particles or of the world (|xa - xb| against ra + rb, n . x against a
 // plane's offset, a distance to an axis against the cylinder radius).
-// Formed directly in FP32 it carries ~1e-7 of the large terms, which is
-// ~1e-3 of an overlap of 1e-4 r.  Here the large terms cancel exactly: the
-// overlaps are formed from error-free transformations, Knuth's TwoSum
-// (a + b = s + e exactly) and the FMA product (a b = p + e exactly), with
-// the errors summed separately (Ogita, Rump and Oishi, "Accurate sum and dot
-// product", SIAM J. Sci. Comput. 26 (2005)); the result carries a few ulp of
-// itself.  These translation units are compiled with -fmad=false, so every
-// addition keeps the rounding TwoSum relies on.  Every function is odd under
-// exchanging the two particles, so the pair law keeps its exact symmetry.
-struct ff { float hi, lo; };   // the unevaluated sum hi + lo
-
-__device__ __forceinline__ float two_sum(float a, float b, float& e) {
-  const float s = a + b;
-  const float bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
-  return s;
+// Formed in FP32 it carries ~1e-7 of the large terms, which is ~1e-3 of an
+// overlap of 1e-4 r.  The overlaps are therefore formed in FP64 from the
+// FP32 state: differences and products of FP32 values are exact there, and
+// what rounding is left is ~1e-16 of the large terms; the result is rounded
+// to FP32 once.  FP64 runs at half the FP32 rate on this GPU.  The
+// translation units are compiled with -fmad=false, so the FP64 expressions
+// are evaluated as written (the restatement does the same on the host).
+__device__ __forceinline__ double3 d3(float3 a) {
+  return make_double3((double)a.x, (double)a.y, (double)a.z);
 }
-__device__ __forceinline__ float two_prod(float a, float b, float& e) {
-  const float p = a * b;
-  e = fmaf(a, b, -p);
-  return p;
+__device__ __forceinline__ double3 dsub(double3 a, double3 b) {
+  return make_double3(a.x - b.x, a.y - b.y, a.z - b.z);
 }
-// s + c += x, c collecting the rounding errors
-__device__ __forceinline__ void acc_add(float& s, float& c, float x) {
-  float e;
-  s = two_sum(s, x, e);
-  c = c + e;
-}
-__device__ __forceinline__ ff ff_diff(float a, float b) {   // a - b exactly
-  ff r;
-  r.hi = two_sum(a, -b, r.lo);
-  return r;
-}
-// s + c += x^2 for x = x.hi + x.lo (the lo^2 term is below the result's ulp)
-__device__ __forceinline__ void acc_sq(float& s, float& c, ff x) {
-  float e;
-  const float p = two_prod(x.hi, x.hi, e);
-  acc_add(s, c, p);
-  c = c + (e + 2.0f * (x.hi * x.lo));
-}
-// s + c += x y for x = x.hi + x.lo, y = y.hi + y.lo
-__device__ __forceinline__ void acc_prod(float& s, float& c, ff x, ff y) {
-  float e;
-  const float p = two_prod(x.hi, y.hi, e);
-  acc_add(s, c, p);
-  c = c + (e + (x.hi * y.lo + x.lo * y.hi));
+__device__ __forceinline__ double ddot(double3 a, double3 b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
 }
 
-// (ra + rb) - |xa - xb| = ((ra + rb)^2 - |xa - xb|^2) / (ra + rb + |xa - xb|);
-// d = xa - xb componentwise exact, dist its FP32 length.  The radius sum
-// enters exactly too (its FP32 rounding alone is ~1e-8 cm).
-__device__ __forceinline__ float overlap_pair(float ra, float rb, ff dx, ff dy, ff dz,
-                                              float dist) {
-  ff sr;
-  sr.hi = two_sum(ra, rb, sr.lo);
-  float s = 0.0f, c = 0.0f;
-  acc_sq(s, c, sr);
-  float t = 0.0f, u = 0.0f;
-  acc_sq(t, u, dx);
-  acc_sq(t, u, dy);
-  acc_sq(t, u, dz);
-  acc_add(s, c, -t);
-  c = c - u;
-  return (s + c) / (sr.hi + dist);
+// (ra + rb) - |xa - xb|
+__device__ __forceinline__ float overlap_pair(float ra, float rb, float3 xa, float3 xb) {
+  const double3 d = dsub(d3(xa), d3(xb));
+  return (float)(((double)ra + (double)rb) - sqrt(ddot(d, d)));
 }
 
 // r - (n . p - d) for a plane n . x = d
 __device__ __forceinline__ float overlap_plane(float r, float3 n, float d, float3 p) {
-  float e0, e1, e2, c;
-  const float q0 = two_prod(n.x, p.x, e0), q1 = two_prod(n.y, p.y, e1), q2 = two_prod(n.z, p.z, e2);
-  float s = two_sum(r, d, c);
-  acc_add(s, c, -q0);
-  acc_add(s, c, -q1);
-  acc_add(s, c, -q2);
-  c = c - ((e0 + e1) + e2);
-  return s + c;
+  return (float)(((double)r + (double)d) - ddot(d3(n), d3(p)));
 }
-
 struct EnsList {        // one copy of the neighbour list + tangential history
   uint32_t* idx;
   uint32_t* cnt;

@@ -6,11 +6,17 @@ Case: two box systems (40 and 60 spheres) thrown at random velocities,
 200 steps of dt = 1e-5 s, checkpoints every 64 steps (the backward
 recomputes four segments).  The GPU's forward equals the FP32 restatement's
 bit for bit, and its reverse sweep equals the FP32 restatement's reverse
-sweep within 1e-4 (the summation order of the reverse differs).  Against the
-FP64 reverse sweep the FP32 gradients differ by ~1e-3 to 3e-3 of the largest
-component (1e-4 to 3e-3 relative for the law constants): the FP32 and FP64
-trajectories separate over 200 steps of contacts; the FP32 restatement shows
-the same differences, so they are precision, stated and bounded at 1e-2.
+sweep within 1e-4 (the summation order of the reverse differs).
+
+Against the FP64 reverse sweep the comparison runs over 120 steps, bound
+1e-3: the gradients are pathwise (the derivative along the contact onsets
+and stick/slip states the trajectory took), and somewhere between 120 and
+160 steps of this case one such decision comes out differently in FP32 and
+FP64 (a contact whose overlap crosses zero within the rounding); from there
+the two precisions differentiate different branches and their gradients
+part by O(1) (measured: 1.6e-4 of the largest component at 120 steps, 0.6
+at 160; with the previous overlap arithmetic the flip came at 240).  That is
+the active-branch nature of the derivative, not an arithmetic error.
 """
 import numpy as np
 import pytest
@@ -39,10 +45,17 @@ def case():
 
 @pytest.fixture(scope="module")
 def gpu_grads(case):
+    return _gpu_grads(case, T)
+
+
+T_F64 = 120   # steps of the FP64 comparison (before the first branch flip of this case)
+
+
+def _gpu_grads(case, steps):
     S, W, p, r, v0, wx, wv = case
     ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=1e-5, skin=0.02, max_nbr=32, use_graph=0)
     ens.set_state(p, r, v0)
-    adj = E.Adjoint(ens, T, SEG)
+    adj = E.Adjoint(ens, steps, SEG)
     assert adj.forward() == 0
     st = ens.state()
     gx, gv0, gw0, gc = adj.backward(wx[st["pid"]], wv[st["pid"]], None)
@@ -54,15 +67,29 @@ def gpu_grads(case):
 @pytest.fixture(scope="module", params=["f32", "f64"])
 def oracle_grads(case, request):
     S, W, p, r, v0, wx, wv = case
+    steps = T if request.param == "f32" else T_F64
     o = EnsRestated(S, W, 1, 1e-5, 0.02, 32, precision=request.param)
     o.set_state(p, r, v0)
-    assert o.adj_record(T) == 0
+    assert o.adj_record(steps) == 0
     st = o.state()
     dx0, dv0, dw0, th = o.adj_reverse(wx[st["pid"]], wv[st["pid"]], np.zeros(p.shape))
     return dx0, dv0, dw0, th, request.param
 
 
-TOL = {"f32": 1e-4, "f64": 1e-2}
+@pytest.fixture(scope="module")
+def gpu_grads_f64_horizon(case):
+    return _gpu_grads(case, T_F64)
+
+
+def grads_for(oracle_grads, gpu_grads, gpu_grads_f64_horizon):
+    return gpu_grads if oracle_grads[4] == "f32" else gpu_grads_f64_horizon
+
+
+TOL = {"f32": 1e-4, "f64": 1e-3}
+# the law-constant gradients are sums over every contact of every step with
+# cancellation between them (measured against FP64 at 120 steps: up to
+# 5e-3 relative, for kt of the 60-sphere system)
+TOL_LAW = {"f32": 1e-4, "f64": 1e-2}
 
 
 def test_forward_equals_fp32_restatement(case, gpu_grads):
@@ -77,8 +104,8 @@ def test_forward_equals_fp32_restatement(case, gpu_grads):
 
 
 @pytest.mark.parametrize("k,name", [(0, "position"), (1, "velocity"), (2, "angular velocity")])
-def test_initial_state_gradient(gpu_grads, oracle_grads, k, name):
-    g = gpu_grads[1 + k].astype(np.float64)
+def test_initial_state_gradient(gpu_grads, gpu_grads_f64_horizon, oracle_grads, k, name):
+    g = grads_for(oracle_grads, gpu_grads, gpu_grads_f64_horizon)[1 + k].astype(np.float64)
     o = oracle_grads[k]
     scale = np.abs(o).max()
     assert scale > 0
@@ -89,13 +116,13 @@ def test_initial_state_gradient(gpu_grads, oracle_grads, k, name):
     assert err < TOL[prec]
 
 
-def test_law_constant_gradient(gpu_grads, oracle_grads):
-    g = gpu_grads[4]
+def test_law_constant_gradient(gpu_grads, gpu_grads_f64_horizon, oracle_grads):
+    g = grads_for(oracle_grads, gpu_grads, gpu_grads_f64_horizon)[4]
     o = oracle_grads[3]
     rel = np.abs(g - o) / np.maximum(np.abs(o), 1e-30)
     prec = oracle_grads[4]
     print("law-constant gradients vs %s, relative error per (system, constant):\n" % prec, rel)
-    assert np.all(rel < TOL[prec]), rel
+    assert np.all(rel < TOL_LAW[prec]), rel
 
 
 def run_with_tape(case, **kw):

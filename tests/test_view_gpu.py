@@ -16,7 +16,7 @@ class _DeviceArray:
     """A float32 (n, 4) device array at a raw pointer, for torch.as_tensor."""
 
     def __init__(self, ptr, n):
-        self.__cuda_array_interface__ = {"shape": (n, 4), "typestr": "<f4", "data": (ptr, True),
+        self.__cuda_array_interface__ = {"shape": (n, 4), "typestr": "<f4", "data": (ptr, False),
                                          "version": 2}
 
 
