@@ -433,13 +433,22 @@ static v3 closest_tri(v3 p, v3 a, v3 b, v3 c, int* region, int* feat) {
 
 static int wall_touch(const wallc* W, v3 p, real r, v3* n, real* delta, int* region) {
   *region = 0;
+  /* the kernels' conservative pre-test (a contact is never rejected by it) */
+  const real mag = (real)fabs((double)p.x) + (real)fabs((double)p.y) + (real)fabs((double)p.z) +
+                   (real)fabs((double)W->r);
   if (W->kind == BLAZE_WALL_PLANE) {
+    if (!(dot(W->a, p) - W->r < r + (real)1e-6 * mag)) return 0;
     *delta = overlap_plane(r, W->a, W->r, p);
     if (!(*delta > 0)) return 0;
     *n = W->a;
     return 1;
   }
   if (W->kind == BLAZE_WALL_CYLINDER) {
+    {
+      const v3 v = sub(p, W->a);
+      if (!(len(sub(v, smul(dot(v, W->b), W->b))) + r > W->r - (real)1e-6 * (mag + 2 * W->r)))
+        return 0;
+    }
     const double v[3] = {(double)p.x - (double)W->a.x, (double)p.y - (double)W->a.y,
                          (double)p.z - (double)W->a.z};
     const double b[3] = {W->b.x, W->b.y, W->b.z};
@@ -572,6 +581,7 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
       if (!(dist > 0)) continue;
       const v3 nrm = mul(rel, (real)1.0 / dist);
       const real delta = overlap_pair(ra, rb, a->pos, b->pos);
+      if (!(delta > 0)) continue;
       const real mb = S->dens43pi * ((rb * rb) * rb);
       v3 xi = mk(0, 0, 0);
       if ((M[i] >> k) & 1u) xi = mk(H[3 * sk], H[3 * sk + 1], H[3 * sk + 2]);
@@ -957,6 +967,7 @@ int ens_adj_reverse(ens_oracle* o, const double* gx_f, const double* gv_f, const
         const real sr = ra + b->r;
         const real d2 = dot(rel, rel);
         if (!(d2 < sr * sr) || !(SQRT(d2) > 0)) continue;
+        if (!(overlap_pair(ra, b->r, a->pos, b->pos) > 0)) continue;
         const int had = (t->mask[i] >> k) & 1u;
         const v3 xi = had ? mk(t->hist[3 * sk], t->hist[3 * sk + 1], t->hist[3 * sk + 2]) : mk(0, 0, 0);
         const v3 xib = pair_vjp(o, S, a, b, xi, Fb[i], Tb[i], gH[sk], &gin[i], &gin[t->idx[sk]], tb);

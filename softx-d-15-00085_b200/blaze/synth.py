@@ -379,15 +379,23 @@ def cone_hopper_faces(r_top, r_out, y_top, y_out, n_seg):
 
 
 def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, silo_r=25.0,
-                 silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, seg_per_obj=7, n_hopper_objs=6,
+                 silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, seg_per_obj=4, n_sectors=7,
                  kn=1.0e5, cor=0.6, mu=0.5, dt=5e-6, seed=1, overlap=1e-5, rotation=0,
                  name="Silo", world="Silo_discharge", gravity=(0.0, -981.0, 0.0)):
     """Silo discharge, reference-law variant (y vertical, as the reference's
-    silo logic assumes, main.cpp:271 and GPU_Memory_Transfer.cuh:656):
-    cylinder r=silo_r over a conical hopper of half-angle half_angle_deg down
-    to an outlet of outlet_d, made of n_hopper_objs world objects of
-    seg_per_obj planar quads each; radii uniform in [r_min, r_max] quantised
-    to n_bins particle objects (the reference's 6-entry pair table).
+    silo logic assumes, main.cpp:271 and GPU_Memory_Transfer.cuh:656): a
+    barrel of radius silo_r over a conical hopper of half-angle
+    half_angle_deg down to an outlet of outlet_d, both faceted into
+    n_sectors * seg_per_obj planar quads around, one world object per sector
+    holding its hopper and barrel quads (the reference's limits: 8 world
+    objects of at most 16 vertices and 16 faces), then the hatch.  Planar
+    faces only, as the reference's own silo project (Projects/2.Silo: Tank,
+    Container, Floor and Hatch objects): a macro cylinder would overwrite the
+    forces of the hopper faces it meets at the junction (the reference's
+    cylinder force replaces, DEM_Kernels_Compute.cuh:493), and the particles
+    there sink through the hopper.  The barrel reaches 2 cm above the
+    initial packing.  Radii uniform in [r_min, r_max] quantised to n_bins
+    particle objects (the reference's 6-entry pair table).
     Rotation is off by default: the reference's tangential force scales with
     |v_t| / |v_rel| where v_t carries the spin term and v_rel does not
     (Collision_Response.cuh:430-466), which diverges for spinning particles
@@ -401,35 +409,7 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
     h_hop = (silo_r - r_out) / math.tan(math.radians(half_angle_deg))
     y_out = 10.0
     y_top = y_out + h_hop
-    n_seg = seg_per_obj * n_hopper_objs
-    quads = cone_hopper_faces(silo_r, r_out, y_top, y_out, n_seg)
-    wobjs = []
-    for o in range(n_hopper_objs):
-        vs, fs = [], []
-        for k in range(seg_per_obj):
-            q = quads[o * seg_per_obj + k]
-            if k == 0:
-                vs += [q[0], q[3]]
-            vs += [q[1], q[2]]
-            a = 2 * k
-            # vertices: top0 bot0 top1 bot1 ... ; quad (top_k, top_k+1, bot_k+1, bot_k)
-            fs.append((a, a + 2, a + 3, a + 1))
-        nm = "Hopper%d" % o
-        # normals point into the hopper: towards the axis, up the cone
-        fs = _orient(vs, fs, lambda c: (silo_r, c[1] + 10.0, silo_r))
-        _write_wobj(os.path.join(base, "SurfaceObjects", nm + ".WOBJ"), nm, vs, fs)
-        wobjs.append(nm)
-    _write_cylinder_wobj(os.path.join(base, "SurfaceObjects", "Barrel.WOBJ"), "Barrel", silo_r,
-                         silo_h + h_hop, (0.0, 0.0, 0.0))
-    wobjs.append("Barrel")
-    # last world object: the hatch under the outlet (the removal height is
-    # its first vertex's y - 5, main.cpp:771-773); opening it drops it
-    yh = y_out - 1.0
-    hv = [(silo_r - 2 * r_out, yh, silo_r - 2 * r_out), (silo_r + 2 * r_out, yh, silo_r - 2 * r_out),
-          (silo_r + 2 * r_out, yh, silo_r + 2 * r_out), (silo_r - 2 * r_out, yh, silo_r + 2 * r_out)]
-    _write_wobj(os.path.join(base, "SurfaceObjects", "Hatch.WOBJ"), "Hatch", hv,
-                _orient(hv, [(0, 1, 2, 3)], lambda c: (c[0], c[1] + 1.0, c[2])))
-    wobjs.append("Hatch")
+    n_seg = seg_per_obj * n_sectors
     edges = np.linspace(r_min, r_max, n_bins + 1)
     radii = 0.5 * (edges[:-1] + edges[1:])
     rng = np.random.default_rng(seed)
@@ -465,8 +445,13 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
         # (the same relative overlap), so no bin starts in free fall
         y = y_out + 0.05 + r if y_last is None else y_last + (r_last + r) * (1.0 - overlap)
         while need > 0:
-            ra = (r_out + (y - y_out) * tan_a) * math.cos(math.pi / n_seg) if y < y_top else silo_r
-            ra -= r / cos_a + 0.002
+            # inscribed radius of the faceted hopper / barrel at this height,
+            # less the sphere's reach to the wall (slanted in the hopper)
+            inscribed = math.cos(math.pi / n_seg)
+            if y < y_top:
+                ra = (r_out + (y - y_out) * tan_a) * inscribed - (r / cos_a + 0.002)
+            else:
+                ra = silo_r * inscribed - (r + 0.002)
             if ra > 0:
                 m = int(ra / pitch)
                 g = np.arange(-m, m + 1) * pitch
@@ -485,6 +470,35 @@ def silo_project(root, n=1_000_000, r_min=0.2, r_max=0.4, n_bins=6, rho=2600.0, 
         r_last = r
     types = types_out
     pos = pos.astype(np.float32)
+    # world objects: per sector the hopper quads (outlet ring to hopper top)
+    # and the barrel quads (hopper top to the barrel top), vertex rings
+    # outlet / hopper top / barrel top
+    y_bar = float(pos[:, 1].max()) + 2.0
+    wobjs = []
+    for o in range(n_sectors):
+        vs, fs = [], []
+        for k in range(seg_per_obj + 1):
+            a = 2 * math.pi * (o * seg_per_obj + k) / n_seg
+            ca, sa = math.cos(a), math.sin(a)
+            vs += [(c + r_out * ca, y_out, c + r_out * sa), (c + silo_r * ca, y_top, c + silo_r * sa),
+                   (c + silo_r * ca, y_bar, c + silo_r * sa)]
+        for k in range(seg_per_obj):
+            b0, b1 = 3 * k, 3 * (k + 1)
+            fs.append((b0 + 1, b1 + 1, b1, b0))          # hopper quad
+            fs.append((b0 + 2, b1 + 2, b1 + 1, b0 + 1))  # barrel quad
+        nm = "Sector%d" % o
+        # normals point into the silo: towards the axis (and up the cone)
+        fs = _orient(vs, fs, lambda cc: (silo_r, cc[1] + 10.0, silo_r))
+        _write_wobj(os.path.join(base, "SurfaceObjects", nm + ".WOBJ"), nm, vs, fs)
+        wobjs.append(nm)
+    # last world object: the hatch under the outlet (the removal height is
+    # its first vertex's y - 5, main.cpp:771-773); opening it drops it
+    yh = y_out - 1.0
+    hv = [(silo_r - 2 * r_out, yh, silo_r - 2 * r_out), (silo_r + 2 * r_out, yh, silo_r - 2 * r_out),
+          (silo_r + 2 * r_out, yh, silo_r + 2 * r_out), (silo_r - 2 * r_out, yh, silo_r + 2 * r_out)]
+    _write_wobj(os.path.join(base, "SurfaceObjects", "Hatch.WOBJ"), "Hatch", hv,
+                _orient(hv, [(0, 1, 2, 3)], lambda cc: (cc[0], cc[1] + 1.0, cc[2])))
+    wobjs.append("Hatch")
     state = dict(pos=pos, vel=np.zeros((n, 3), np.float32), avel=np.zeros((n, 3), np.float32),
                  pid=np.arange(n, dtype=np.int32), type=types)
     write_state_file(os.path.join(base, "Start_" + world), state, sim_type=2)

@@ -269,8 +269,9 @@ __global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
 }
 
 // Slots k < cnt of a particle's list whose spheres overlap (the forward's
-// test, d2 < (ra + rb)^2 and |rel| > 0), as a bit mask; the candidates in
-// batches of four: the entries, then the position gathers, then the tests.
+// test: d2 < (ra + rb)^2, |rel| > 0 and a positive overlap), as a bit mask;
+// the candidates in batches of four: the entries, then the position gathers,
+// then the tests.
 __device__ __forceinline__ uint32_t contact_mask(const uint2* ent, uint32_t cnt,
                                                  const float4* pos, float3 xa, float ra) {
   constexpr uint32_t kB = 4;
@@ -288,7 +289,9 @@ __device__ __forceinline__ uint32_t contact_mask(const uint2* ent, uint32_t cnt,
       const float3 rel = xa - xyz4(pb[u]);
       const float sr = ra + pb[u].w;
       const float d2 = dot3(rel, rel);
-      if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f) cm |= 1u << (k0 + u);
+      if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f &&
+          overlap_pair(ra, pb[u].w, xa, xyz4(pb[u])) > 0.0f)
+        cm |= 1u << (k0 + u);
     }
   }
   return cm;
@@ -378,7 +381,7 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   for (int q = 0; q < kWallSlots; ++q) win[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   int nw = 0;
   for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
-    const EnsWallDev W = g.walls[w];
+    const EnsWallDev& W = g.walls[w];
     if (!(overlap_plane(A.r, W.a, W.r, A.x) > 0.0f)) continue;   // as wall_touch decides
     float3 xi = f3(0.0f, 0.0f, 0.0f);
     int qo = -1;

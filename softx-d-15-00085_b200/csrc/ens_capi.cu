@@ -87,6 +87,9 @@ EnsGeom geom(const blaze_ens* e) {
   g.law = e->opt.law;
   g.dt = e->opt.dt;
   g.skin = e->opt.skin;
+  g.curved = 0;
+  for (const EnsWallDev& w : e->hwalls)
+    if (w.kind != kWallPlane) g.curved = 1;
   return g;
 }
 

@@ -140,17 +140,28 @@ __device__ __forceinline__ float3 closest_on_triangle(float3 p, float3 a, float3
 }
 
 // Contact of a sphere (centre p, radius r) with one wall: normal from the
-// wall to the centre, overlap; false when not touching.
+// wall to the centre, overlap; false when not touching.  kCurved = false
+// compiles the plane test only (ensembles whose walls are all planes).
+template <bool kCurved>
 __device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float r, float3& n,
                                            float& delta, int& region) {
   region = 0;
+  // Walls first take a conservative FP32 test (its margin is ten times the
+  // FP32 rounding of the distance), so the FP64 overlap runs only near them.
+  const float mag = fabsf(p.x) + fabsf(p.y) + fabsf(p.z) + fabsf(W.r);
   if (W.kind == kWallPlane) {
+    if (!(dot3(W.a, p) - W.r < r + 1e-6f * mag)) return false;
     delta = overlap_plane(r, W.a, W.r, p);
     if (!(delta > 0.0f)) return false;
     n = W.a;
     return true;
   }
+  if constexpr (!kCurved) return false;
   if (W.kind == kWallCylinder) {
+    {
+      const float3 v = p - W.a;
+      if (!(len3(v - dot3(v, W.b) * W.b) + r > W.r - 1e-6f * (mag + 2.0f * W.r))) return false;
+    }
     // rad = v - (v . b) b with v = p - a, in double
     const double3 v = dsub(d3(p), d3(W.a)), b = d3(W.b);
     const double vb = ddot(v, b);
@@ -336,7 +347,7 @@ __global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
 constexpr uint32_t kEnsMaskBatch = 4;
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
 // history words are reserved first, by every thread of the block).
-template <int kLaw, bool kCapture, bool kRecord>
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved>
 __global__ void __launch_bounds__(kMaxStepBlock)
 k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
            StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
@@ -421,7 +432,10 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     const float dist = sqrtf(d2);
     if (!(dist > 0.0f)) continue;
     const float3 nrm = rel * (1.0f / dist);
+    // the contact is decided by the overlap itself: the FP32 test above can
+    // pass a pair whose FP64-formed overlap is not positive
     const float delta = overlap_pair(ra, rb, pa, xyz(pb4));
+    if (!(delta > 0.0f)) continue;
     const float4 vb4 = __ldg(in.vel + j), wb4 = __ldg(in.angv + j);
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);
@@ -496,13 +510,13 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     }
   };
   for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
-    const EnsWallDev W = g.walls[w];
+    const EnsWallDev& W = g.walls[w];
     float3 nrm;
     float delta;
     int region;
-    if (wall_touch(W, pa, ra, nrm, delta, region)) wall_contact(w, nrm, delta);
+    if (wall_touch<kCurved>(W, pa, ra, nrm, delta, region)) wall_contact(w, nrm, delta);
   }
-  if (g.tri_off) {
+  if (kCurved && g.tri_off) {
     const int3 c = ens_cell(S, pa);
     if (ens_in(S, c)) {
       const uint32_t h = ens_key(S, c);
@@ -516,7 +530,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
         float3 nrm;
         float delta;
         int region;
-        if (!wall_touch(g.walls[id], pa, ra, nrm, delta, region)) continue;
+        if (!wall_touch<kCurved>(g.walls[id], pa, ra, nrm, delta, region)) continue;
         if (region == 0) ++nface;
         else if (best < 0 || delta > best_d) { best = id; best_d = delta; }
       }
@@ -525,7 +539,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
         float3 nrm;
         float delta;
         int region;
-        if (!wall_touch(g.walls[id], pa, ra, nrm, delta, region)) continue;
+        if (!wall_touch<kCurved>(g.walls[id], pa, ra, nrm, delta, region)) continue;
         if ((nface > 0 && region == 0) || (nface == 0 && id == best)) wall_contact(id, nrm, delta);
       }
     }
@@ -627,13 +641,25 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
   const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
   const int gs = (n + bs - 1) / bs;
 #define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c, EnsTape{}
-  if (g.law == kLawHertz) {
-    if (cap) k_ens_step<kLawHertz, true, false><<<gs, bs, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawHertz, false, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+#define ENS_STEP(L, C, K) k_ens_step<L, C, false, K><<<gs, bs, 0, st>>>(ENS_ARGS)
+  if (g.curved) {
+    if (g.law == kLawHertz) {
+      if (cap) ENS_STEP(kLawHertz, true, true);
+      else ENS_STEP(kLawHertz, false, true);
+    } else {
+      if (cap) ENS_STEP(kLawLinear, true, true);
+      else ENS_STEP(kLawLinear, false, true);
+    }
   } else {
-    if (cap) k_ens_step<kLawLinear, true, false><<<gs, bs, 0, st>>>(ENS_ARGS);
-    else k_ens_step<kLawLinear, false, false><<<gs, bs, 0, st>>>(ENS_ARGS);
+    if (g.law == kLawHertz) {
+      if (cap) ENS_STEP(kLawHertz, true, false);
+      else ENS_STEP(kLawHertz, false, false);
+    } else {
+      if (cap) ENS_STEP(kLawLinear, true, false);
+      else ENS_STEP(kLawLinear, false, false);
+    }
   }
+#undef ENS_STEP
 #undef ENS_ARGS
 }
 
@@ -641,7 +667,8 @@ void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, 
                             StepLink link, const EnsTape& tape, int block, cudaStream_t st) {
   const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
   const int gs = (n + bs - 1) / bs;
-  k_ens_step<kLawLinear, false, true><<<gs, bs, 0, st>>>(
+  // reverse mode accepts plane walls only (blaze_ens_adj_create)
+  k_ens_step<kLawLinear, false, true, false><<<gs, bs, 0, st>>>(
       g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, EnsCapture{nullptr, nullptr}, tape);
 }
 

@@ -119,6 +119,7 @@ struct EnsGeom {
   uint32_t ncell_tab;        // total hash-table entries
   int law;
   float dt, skin;
+  int curved;                // 1: some wall is a cylinder or a triangle (not only planes)
 };
 
 struct EnsCapture { float4* f; float4* t; };
