@@ -143,6 +143,19 @@ int blaze_ens_adj_forward(blaze_ens_adj* a);
 int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
                            const float* gavel, float* gpos0, float* gvel0, float* gavel0,
                            double* gconst);
+/* The reverse sweep over the last `window` steps only (truncated
+ * backpropagation): the law-constant cotangents of those steps, and the
+ * cotangents of the state at step nsteps - window (that step's memory
+ * order; NULL skips), the earlier state held fixed.  Over long horizons
+ * the full discrete adjoint of dense granular flow grows exponentially
+ * with the horizon (the dynamics is chaotic: the derivative along the
+ * contact onsets and stick/slip states taken, measured about 5 % per step
+ * at dt = 1e-5 s), so the full backward of a 3,000-step run overflows FP32;
+ * a window keeps the gradient bounded and local.  window = nsteps is
+ * blaze_ens_adj_backward. */
+int blaze_ens_adj_backward_window(blaze_ens_adj* a, int window, const float* gpos,
+                                  const float* gvel, const float* gavel, float* gpos_w,
+                                  float* gvel_w, float* gavel_w, double* gconst);
 /* Device time of the last backward call by phase, ms: restoring the
  * checkpoints, recomputing the segments into the tape, the reverse sweep. */
 int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,

@@ -66,6 +66,8 @@ def load():
         lib.blaze_ens_adj_forward.argtypes = [C.c_void_p]
         lib.blaze_ens_adj_backward.argtypes = [C.c_void_p, _f, _f, _f, _f, _f, _f,
                                                P(C.c_double)]
+        lib.blaze_ens_adj_backward_window.argtypes = [C.c_void_p, C.c_int, _f, _f, _f, _f, _f,
+                                                      _f, P(C.c_double)]
         lib.blaze_ens_adj_destroy.argtypes = [C.c_void_p]
         lib.blaze_ens_adj_profile.argtypes = [C.c_void_p, _f, _f, _f]
         lib.blaze_ens_adj_create_ex.argtypes = [P(C.c_void_p), C.c_void_p, C.c_int, C.c_int,
@@ -219,6 +221,7 @@ class Adjoint:
         """arena_bytes: the tape's arena size exactly, instead of tape_bytes."""
         self.ens = ens
         self.lib = ens.lib
+        self.nsteps = int(nsteps)
         h = C.c_void_p()
         if arena_bytes is not None:
             _check(self.lib.blaze_ens_adj_create_tape(C.byref(h), ens.h, int(nsteps),
@@ -253,16 +256,24 @@ class Adjoint:
     def forward(self):
         return _check(self.lib.blaze_ens_adj_forward(self.h), "blaze_ens_adj_forward")
 
-    def backward(self, gpos=None, gvel=None, gavel=None):
+    def backward(self, gpos=None, gvel=None, gavel=None, window=None):
+        """Cotangents of the final state -> (gx, gv, gw) of the initial
+        state and the law constants (nsys x 5).  With `window`, only the
+        last `window` steps are reversed (blaze_ens_adj_backward_window):
+        the state cotangents are then those of the state `window` steps
+        before the end."""
         n = self.ens.n
         c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(n, 3)
         gpos, gvel, gavel = c(gpos), c(gvel), c(gavel)
         out = [np.zeros((n, 3), np.float32) for _ in range(3)]
         gc = np.zeros((self.ens.nsys, 5), np.float64)
-        _check(self.lib.blaze_ens_adj_backward(
-            self.h, _ptr(gpos, C.c_float), _ptr(gvel, C.c_float), _ptr(gavel, C.c_float),
-            *[_ptr(a, C.c_float) for a in out], gc.ctypes.data_as(C.POINTER(C.c_double))),
-            "blaze_ens_adj_backward")
+        ptrs = [_ptr(gpos, C.c_float), _ptr(gvel, C.c_float), _ptr(gavel, C.c_float)] + \
+            [_ptr(a, C.c_float) for a in out] + [gc.ctypes.data_as(C.POINTER(C.c_double))]
+        if window is None:
+            _check(self.lib.blaze_ens_adj_backward(self.h, *ptrs), "blaze_ens_adj_backward")
+        else:
+            _check(self.lib.blaze_ens_adj_backward_window(self.h, int(window), *ptrs),
+                   "blaze_ens_adj_backward_window")
         return out[0], out[1], out[2], gc
 
     def profile(self):

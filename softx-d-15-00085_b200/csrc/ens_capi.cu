@@ -1042,10 +1042,14 @@ int blaze_ens_adj_forward(blaze_ens_adj* a) {
   return st;
 }
 
-int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
-                           const float* gavel, float* gpos0, float* gvel0, float* gavel0,
-                           double* gconst) {
-  if (!a || !a->forward_done) return -1;
+namespace {
+
+// The reverse sweep over steps [first, nsteps): first = 0 is the whole run;
+// first > 0 the window of the last nsteps - first steps.
+int backward_impl(blaze_ens_adj* a, int first, const float* gpos, const float* gvel,
+                  const float* gavel, float* gpos0, float* gvel0, float* gavel0,
+                  double* gconst) {
+  if (!a || !a->forward_done || first < 0 || first >= a->nsteps) return -1;
   blaze_ens* e = a->e;
   const size_t n = e->n, cap = e->opt.max_nbr;
   cudaStream_t st = e->stream;
@@ -1069,8 +1073,9 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
   for (cudaEvent_t& ev : a->ev)
     if (!ev) CK(cudaEventCreate(&ev));
   for (float& m : a->ms_phase) m = 0.0f;
-  for (int s = a->nseg - 1; s >= 0; --s) {
+  for (int s = a->nseg - 1; s >= 0 && (s + 1) * a->K > first; --s) {
     const int len = std::min(a->K, a->nsteps - s * a->K);
+    const int q0 = std::max(0, first - s * a->K);   // first step of the segment to reverse
     TapeSeg& sg = a->seg[s];
     CK(cudaEventRecord(a->ev[0], st));
     if (!sg.valid) {
@@ -1085,7 +1090,7 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
       for (int r = 0; r < s; ++r) a->seg[r].valid = false;
     }
     CK(cudaEventRecord(a->ev[2], st));
-    for (int q = len - 1; q >= 0; --q) {
+    for (int q = len - 1; q >= q0; --q) {
       const int t = s * a->K + q;
       adj_launch_step(g, a->tape, t, (int)n, A, st);
       if (sg.rb[q]) {
@@ -1124,6 +1129,22 @@ int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gve
   }
   CK(cudaStreamSynchronize(st));
   return sync_status(e);
+}
+
+}  // namespace
+
+int blaze_ens_adj_backward(blaze_ens_adj* a, const float* gpos, const float* gvel,
+                           const float* gavel, float* gpos0, float* gvel0, float* gavel0,
+                           double* gconst) {
+  return backward_impl(a, 0, gpos, gvel, gavel, gpos0, gvel0, gavel0, gconst);
+}
+
+int blaze_ens_adj_backward_window(blaze_ens_adj* a, int window, const float* gpos,
+                                  const float* gvel, const float* gavel, float* gpos_w,
+                                  float* gvel_w, float* gavel_w, double* gconst) {
+  if (!a || window < 1 || window > a->nsteps) return -1;
+  return backward_impl(a, a->nsteps - window, gpos, gvel, gavel, gpos_w, gvel_w, gavel_w,
+                       gconst);
 }
 
 int blaze_ens_adj_profile(blaze_ens_adj* a, float* ms_restore, float* ms_record,
