@@ -89,7 +89,7 @@ def parse():
     ap.add_argument("--case", nargs="+", metavar=("NAME", "ARG"),
                     help="run one named workload case for profiling (no timing line): "
                          "ens_step [STEPS], adjoint [NSYS STEPS SEGMENT TAPE_BYTES], "
-                         "poly [N STEPS]; see case_*")
+                         "poly [N STEPS], silo_settled [N SETTLE STEPS FAST SKIN_UM]; see case_*")
     return ap.parse_args()
 
 
@@ -150,7 +150,37 @@ def case_adjoint(nsys=64, steps=60, segment=30, tape_bytes=0):
     return status
 
 
-CASES = {"ens_step": case_ens_step, "adjoint": case_adjoint, "poly": case_poly}
+def case_silo_settled(n=1_000_000, settle=48000, steps=8, fast=1, skin_um=1600):
+    """The headline silo workload from its settled bed: n spheres settled
+    `settle` steps with the hatch closed (cached under /tmp on the first run:
+    the same command line run again loads the cache, so a profiler sees only
+    `steps` plain steps of the discharge), hatch open, contracted law when
+    `fast`, skin skin_um / 1e4 cm."""
+    from blaze import device, synth
+    skin = skin_um * 1e-4
+    cache = os.path.join(tempfile.gettempdir(), "blaze_silo_settled_%d_%d.npz" % (n, settle))
+    with tempfile.TemporaryDirectory() as d:
+        P, st0 = synth.silo_project(d, n=n)
+    sim = device.Simulation(P, skin=skin, max_nbr=32, use_graph=1)
+    if os.path.isfile(cache):
+        z = np.load(cache)
+        sim.set_state(z["pos"], z["vel"], z["avel"], z["type"], z["pid"])
+    else:
+        sim.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
+        sim.step(settle)
+        s = sim.state()
+        np.savez(cache, **{k: s[k] for k in ("pos", "vel", "avel", "type", "pid")})
+    sim.open_hatch()
+    sim.set_options(skin=skin, max_nbr=32, use_graph=1, fast_law=int(fast))
+    sim.step(steps)
+    status = sim.sync()
+    print("silo_settled: n %d status %d" % (n, status))
+    sim.close()
+    return status
+
+
+CASES = {"ens_step": case_ens_step, "adjoint": case_adjoint, "poly": case_poly,
+         "silo_settled": case_silo_settled}
 
 
 def contacts_per_particle(sim):
