@@ -1,9 +1,9 @@
 """The contracted particle-particle law (blaze_options.fast_law = 1) against
-the reference's own kernels on its own projects (oracle-A golden fixtures:
-Projects/2.Silo world SPH_90, 1,950 spheres with the silo hatch;
-Projects/3.BallMill world Mill_SPH30, 242 spheres, rotating drum and
-lifters), and against the FP64 restatement of the reference law on the
-synthetic 10,000-sphere box.
+the reference's own kernels on its own project (oracle-A golden fixture:
+Projects/2.Silo world SPH_90, 1,950 spheres with the silo hatch), and
+against the FP64 restatement of the reference law on the synthetic
+10,000-sphere box settled into contact.  (A run with energy tallies, such as
+the ball-mill fixture, keeps the reference's arithmetic in the law.)
 
 Bar: the contact lists are the reference's bit for bit (the contact test is
 not contracted); the forces of the first step agree within 1e-5 relative,
@@ -38,7 +38,7 @@ def rel_err(f, ref, weight):
     return float((np.linalg.norm(f.astype(np.float64) - ref, axis=1) / scale).max())
 
 
-@pytest.mark.parametrize("name", ["silo_sph90", "mill_sph30"])
+@pytest.mark.parametrize("name", ["silo_sph90"])
 def test_fast_law_vs_reference_kernels(name):
     g = Golden(name)
     s = gpu_sim(g, capture_forces=1, fast_law=1)
@@ -71,16 +71,23 @@ def test_fast_law_vs_reference_kernels(name):
 
 
 def test_fast_law_vs_fp64_box(tmp_path):
-    """10,000 spheres of the box configuration after 400 steps of settling:
-    one step's particle-particle forces, contracted and bit-exact, against
-    the FP64 restatement of the reference law from the same state."""
+    """10,000 spheres of the box configuration after 16,000 steps of settling
+    (a bed in contact): one step's particle-particle forces, contracted and
+    bit-exact, against the FP64 restatement of the reference law from the
+    same state."""
     P, st0 = synth.box_project(str(tmp_path))
     s = device.Simulation(P, skin=0.02, use_graph=1)
     s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
-    s.step(400)
+    s.step(16000)
     st = s.state()
+    nn, lst = s.nlist()
     s.close()
     assert st["status"] == 0
+    # contacts per particle in the settled bed (the list of the last re-sort)
+    r = 0.1
+    d = np.linalg.norm(st["pos"][:, None, :] - st["pos"][lst.astype(np.int64)], axis=2)
+    touching = (d < 2 * r) & (np.arange(lst.shape[1])[None, :] < nn[:, None])
+    assert touching.sum() / len(nn) > 2.0, touching.sum() / len(nn)
     out = {}
     for fast in (0, 1):
         g = device.Simulation(P, capture_forces=1, fast_law=fast)
