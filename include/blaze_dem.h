@@ -245,6 +245,21 @@ int blaze_write_state_arrays(const char* path, const blaze_state_header* h, int 
 /* The simulation's current state to `path` (accelerations are not kept:
  * detail 4's acceleration column is 0). */
 int blaze_write_state(blaze_sim* s, const char* path, const blaze_state_header* h);
+/* Silo_Stats (main.cpp:253-280), on the device: *count = the particles of
+ * the current run (memory positions [0, n_cur)) above `height`, the hatch
+ * height; particles removed since the last re-sort still sit in that range
+ * at the parking position and count, as in the reference.  Waits for the
+ * stream; returns the status like blaze_sync. */
+int blaze_count_above(blaze_sim* s, float height, int* count);
+/* The driver's result files, one line appended per call, as main.cpp
+ * writes them (ostream defaults).  FlowRate.dat (main.cpp:142): time and
+ * the percentage discharged, (n0 - remaining) / (float) n0 * 100.
+ * Results.dat (main.cpp:74-82): per revolution the total, particle, lifter
+ * and drum power from Device_Get_Energy's three values over
+ * steps_per_rev * dt.  No GPU needed.  0 ok, -1 bad argument, -3 I/O. */
+int blaze_write_flow_line(const char* path, double time, int n0, int remaining);
+int blaze_write_power_line(const char* path, double time, const float* energy3, int steps_per_rev,
+                           float dt);
 /* Self-check of the step's shared-reciprocal division against IEEE
  * division on the GPU: components that differ over n random triples
  * (0 expected), -1 on error. */

@@ -124,6 +124,9 @@ def load():
     lib.blaze_open_hatch.argtypes = [C.c_void_p]
     lib.blaze_rebuild_kernels.argtypes = [C.c_void_p]
     lib.blaze_profile.argtypes = [C.c_void_p, _f, _f, _i]
+    lib.blaze_count_above.argtypes = [C.c_void_p, C.c_float, _i]
+    lib.blaze_write_flow_line.argtypes = [C.c_char_p, C.c_double, C.c_int, C.c_int]
+    lib.blaze_write_power_line.argtypes = [C.c_char_p, C.c_double, _f, C.c_int, C.c_float]
     lib.blaze_default_sim.restype = C.c_void_p
     lib.Device_Set_SimulationData.argtypes = [P(T.WOBJ), P(T.POBJ), P(T.DOBJ), P(T.SimulationInfo),
                                               C.c_int, C.c_int, C.c_int, P(T.InitConfig)]
@@ -336,6 +339,13 @@ class Simulation:
         """Instantiate the CUDA graphs graph stepping will launch (no capture
         then happens inside later steps)."""
         _check(self.lib.blaze_prepare_graphs(self.h), "blaze_prepare_graphs")
+
+    def count_above(self, height):
+        """Particles of the current run whose centre is above `height`
+        (the silo's remaining count, main.cpp:253-276), counted on the device."""
+        n = C.c_int()
+        _check(self.lib.blaze_count_above(self.h, float(height), C.byref(n)), "blaze_count_above")
+        return n.value
 
     def num_exact_blocks(self):
         return _check(self.lib.blaze_num_exact_blocks(self.h), "blaze_num_exact_blocks")

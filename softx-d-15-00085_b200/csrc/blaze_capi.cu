@@ -122,6 +122,7 @@ struct blaze_sim {
   // each), packed / unpacked by a kernel, and its two result words (pinned)
   HostStage stage{};
   int* h_flags = nullptr;
+  unsigned int* d_count = nullptr;     // blaze_count_above's device word
   // convex polyhedra (particle_type 1): body-frame objects and the
   // world-frame geometry the step rebuilds
   bool poly = false;
@@ -1010,6 +1011,7 @@ void free_sim(blaze_sim* s) {
   f(s->geom.vert); f(s->geom.fnorm); f(s->geom.fcent);
   f(s->pairs.status); f(s->pairs.hint); f(s->pairs.con); f(s->pairs.qv); f(s->pairs.qe); f(s->pairs.counts);
   f(s->nl.flat);
+  f(s->d_count);
   if (s->h_flags) cudaFreeHost(s->h_flags);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   drop_graphs(s);
@@ -1182,6 +1184,7 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(dalloc(&s->stage.pid, n));
   CKF(dalloc(&s->stage.flags, 2));
   CKF(cudaMallocHost((void**)&s->h_flags, 2 * sizeof(int)));
+  CKF(dalloc(&s->d_count, 1));
   std::memset(s->h_ctl, 0, sizeof(StepCtl));
   CKF(dalloc(&s->d_chk, (size_t)2 * kChkSlots * kChkStride));
   CKF(cudaMemset(s->d_chk, 0, sizeof(uint32_t) * 2 * kChkSlots * kChkStride));
@@ -1540,6 +1543,17 @@ int blaze_device_view(blaze_sim* s, const void** pos4, const void** ornt4, int* 
   if (ornt4) *ornt4 = s->poly ? s->ob.ornt[s->h_ctl->epoch & 1] : nullptr;
   if (n) *n = s->h_ctl->n_cur;
   if (stream) *stream = (void*)s->stream;
+  return rc;
+}
+
+int blaze_count_above(blaze_sim* s, float height, int* count) {
+  if (!s || !count) return -1;
+  CK(cudaMemsetAsync(s->d_count, 0, sizeof(unsigned int), s->stream));
+  launch_count_above(s->S[s->cur].pos, s->ctl, s->n_max, height, s->d_count, s->stream);
+  CK(cudaMemcpyAsync(s->h_flags, s->d_count, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                     s->stream));
+  const int rc = sync_status(s);
+  *count = s->h_flags[0];
   return rc;
 }
 

@@ -799,6 +799,20 @@ __global__ void k_kill(StateBuf s, OrderBuf ob, int n_max, float kill_height, in
   }
 }
 
+// Silo_Stats (main.cpp:253-280): how many particles of the current run
+// (memory positions [0, n_cur)) lie above `height`.  Particles removed since
+// the last re-sort are still in that range at the parking position, as the
+// reference counts them.  Integer sums: the count does not depend on order.
+__global__ void __launch_bounds__(kThreads)
+k_count_above(const float4* __restrict__ pos, const StepCtl* ctl, int n_max, float height,
+              unsigned int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = min(ctl->n_cur, n_max);
+  const unsigned int above = (i < n && pos[i].y > height) ? 1u : 0u;
+  const unsigned int w = __reduce_add_sync(0xffffffffu, above);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(out, w);
+}
+
 // ------------------------------------------------------------ state staging
 // Set_PSystem_State / Get_SystemState (GPU_Memory_Transfer.cuh:377-418,
 // 486-520) as one pass each over the staged host arrays.
@@ -980,6 +994,11 @@ void launch_pack_state(const SimParams* dp, const HostStage& hs, bool has_vel, b
 void launch_unpack_state(const SimParams* dp, const HostStage& hs, const StateBuf& s,
                          const int* pid_src, const float4* ornt_src, int n, cudaStream_t st) {
   k_unpack_state<<<blocks(n), kThreads, 0, st>>>(dp, hs, s, pid_src, ornt_src, n);
+}
+
+void launch_count_above(const float4* pos, const StepCtl* ctl, int n_max, float height,
+                        unsigned int* out, cudaStream_t st) {
+  k_count_above<<<blocks(n_max), kThreads, 0, st>>>(pos, ctl, n_max, height, out);
 }
 
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,

@@ -182,6 +182,10 @@ void launch_move_dobj(SimParams* dp, int turn, float about_x, float about_y, flo
 // world object k) on the wall program.
 void launch_rotate_wobj(WallOp* ops, int n_ops, uint32_t rot_mask, float about_x, float about_y,
                         float c, float s, cudaStream_t st);
+// *out += the particles of the current run whose y exceeds height
+// (Silo_Stats, main.cpp:253-280; removed ones parked in range count).
+void launch_count_above(const float4* pos, const StepCtl* ctl, int n_max, float height,
+                        unsigned int* out, cudaStream_t st);
 void launch_kill(const StateBuf& s, const OrderBuf& ob, int n_max, float kill_height,
                  int rotating, float3 max_size, StepCtl* ctl, cudaStream_t st);
 

@@ -155,3 +155,34 @@ extern "C" int blaze_write_state_arrays(const char* path, const blaze_state_head
   }
   return out.good() ? 0 : -3;
 }
+
+// The driver's result files, one line per call, appended, with the
+// reference's expressions and ostream's default formatting.
+//
+// FlowRate.dat of a silo run (main.cpp:133-147): every flow_steps steps
+// after the hatch opens, the time and the percentage discharged,
+// (n0 - remaining) / (float) n0 * 100, remaining counted as Silo_Stats
+// counts it (blaze_count_above).
+extern "C" int blaze_write_flow_line(const char* path, double time, int n0, int remaining) {
+  if (!path || n0 <= 0) return -1;
+  std::ofstream out(path, std::ios::app);
+  if (!out) return -3;
+  out << time << " " << ((n0 - remaining) / (float)n0) * 100.0 << std::endl;
+  return out.good() ? 0 : -3;
+}
+
+// Results.dat of a ball-mill run (main.cpp:53-82): at the end of every
+// revolution the power from the energy tallies of that revolution
+// (Device_Get_Energy's three values: particle, lifter, drum).
+extern "C" int blaze_write_power_line(const char* path, double time, const float* energy3,
+                                      int steps_per_rev, float dt) {
+  if (!path || !energy3) return -1;
+  std::ofstream out(path, std::ios::app);
+  if (!out) return -3;
+  const float* e = energy3;
+  out << "time: " << time << " Power:   Total = " << ((e[0] + e[1] + e[2]) / (steps_per_rev * dt))
+      << "  Particle: " << (e[0]) / (steps_per_rev * dt)
+      << "  Lifter: " << e[1] / (steps_per_rev * dt) << " Drum " << e[2] / (steps_per_rev * dt)
+      << std::endl;
+  return out.good() ? 0 : -3;
+}
