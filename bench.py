@@ -119,7 +119,7 @@ def case_poly(n=20000, steps=10):
     mode (contact list rebuilt every step), `steps` plain steps."""
     from blaze import device, synth
     with tempfile.TemporaryDirectory() as d:
-        P, st = synth.poly_box_project(d, n=n)
+        P, st = synth.poly_box_project(d, n=n, spacing=POLY_SPACING, jitter=POLY_JITTER)
     sim = device.Simulation(P)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
     sim.step(steps)
@@ -285,6 +285,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+SEQ_SAMPLE = 64   # systems timed one at a time for the sequential comparator
+
+
 def batched_leg(steps, warmup):
     """The batched ensemble: 512 independent box-settling systems, particle
     counts log-uniform in [2,000, 50,000] (seed 3), radii uniform in
@@ -294,10 +297,11 @@ def batched_leg(steps, warmup):
     sequence per step (CUDA graph), skin and block size from the autotuner.
     The timed region is the whole settling run from rest (2,000 steps by
     default), re-sorts included.  Compared with plain solves of single
-    systems (same kernels and settings, one system per launch sequence) of
-    16 sizes spread over the range, each timed over the same steps; the
-    sequential time of all 512 is their linear fit in N summed over the 512
-    counts."""
+    systems (same kernels and settings, one system per launch sequence): a
+    seeded random sample of SEQ_SAMPLE of the 512 systems, each timed over
+    the same steps from the same start; the sequential time of all 512 is
+    512 x the sample's mean (the sum's unbiased estimate), with the
+    sample's standard error scaled alike."""
     import torch
     from blaze import autotune, synth
     from blaze import ensemble as E
@@ -326,9 +330,9 @@ def batched_leg(steps, warmup):
     status = ens.sync()
     n = ens.n
     ens.close()
-    # single systems, one after another
+    # single systems, one after another: a seeded random sample
     off = np.concatenate([[0], np.cumsum(counts)])
-    pick = np.argsort(counts)[np.linspace(0, len(counts) - 1, 16).astype(int)]
+    pick = np.sort(np.random.default_rng(11).choice(len(counts), SEQ_SAMPLE, replace=False))
     single = []
     for s_ in pick:
         Ss = E.System.from_buffer_copy(bytes(best["systems"][s_]))
@@ -344,10 +348,9 @@ def batched_leg(steps, warmup):
         b.synchronize()
         single.append((int(counts[s_]), a.elapsed_time(b) / steps))
         e1.close()
-    ns = np.array([x[0] for x in single], float)
     ts = np.array([x[1] for x in single])
-    coef = np.linalg.lstsq(np.stack([np.ones_like(ns), ns], 1), ts, rcond=None)[0]
-    seq_ms = float(np.sum(coef[0] + coef[1] * counts))
+    seq_ms = float(len(counts) * ts.mean())
+    seq_se = float(len(counts) * ts.std(ddof=1) / np.sqrt(len(ts)))
     return {"workload": "512 box-settling systems, N log-uniform in [2000, 50000], "
                         "linear spring-dashpot + tangential history, dt 1e-5 s",
             "particles": int(n), "systems": len(counts), "value": n / (ms * 1e-3),
@@ -357,6 +360,9 @@ def batched_leg(steps, warmup):
                           "block": best["block"],
                           "trials": [[t[0], t[1], round(t[2], 4), t[3]] for t in trials]},
             "sequential_plain_ms_per_step": seq_ms, "vs_sequential_plain": seq_ms / ms,
+            "sequential_plain_stderr_ms": seq_se,
+            "sequential_sample": "%d of %d systems (seeded random), each timed over %d steps"
+                                 % (len(single), len(counts), steps),
             "single_samples": [[n_, round(t_, 5)] for n_, t_ in single]}
 
 
@@ -474,22 +480,30 @@ def adjoint_leg(steps, segment=100):
                               "backward_ms": win_ms}}
 
 
+POLY_SPACING, POLY_JITTER = 0.99, 0.005   # cm
+
+
 def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=True):
     """Convex polyhedra on the reference path: 100,000 particles (the
     polyhedron count of the mill configuration) in a closed box, a third
     each dodecahedra, cubes and hexagonal prisms of circumradius 0.5 cm on a
-    0.93 cm jittered lattice (every bounding sphere overlaps its lattice
-    neighbours', so contacts exist from the first step), random orientations,
+    0.99 cm lattice jittered by +-0.005 cm (bounding spheres of lattice
+    neighbours overlap, so vertex contacts exist from the first step, while
+    no initial penetration reaches the 0.05 r at which the reference's
+    polyhedron kernel starts to clamp, DEM_Kernels_Compute.cuh:917-950),
+    random orientations,
     velocities N(0, 10 cm/s), spins N(0, 20 rad/s), linear law kn = 1e5,
     e = 0.5, mu = 0.4, dt = 1e-5 s, rotation on.  GPU: CUDA graphs with a
     `skin` Verlet list on the bounding spheres (value) and the reference's
     rebuild-every-step mode (reference_mode_value).  CPU: the reference's own
     polyhedron kernels (oracle/_ref) on all host threads, reference mode, a
-    bounded sample of whole steps of the same workload."""
+    bounded sample of whole steps from the state the GPU reached after its
+    timed steps (the same contacts), with the count of the kernel's
+    penetration-clamp warnings."""
     import torch
     from blaze import device, synth
     with tempfile.TemporaryDirectory() as d:
-        P, st = synth.poly_box_project(d, n=n)
+        P, st = synth.poly_box_project(d, n=n, spacing=POLY_SPACING, jitter=POLY_JITTER)
     sim = device.Simulation(P, skin=skin, use_graph=1)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"], quat=st["quat"])
     sim.prepare_graphs()
@@ -508,6 +522,7 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
     rebuilds = sim.num_rebuilds() - rb0
     launches = fixed + rebuilds * sim.rebuild_kernels()
     status |= sim.sync()
+    st_timed = sim.state()
     sim.set_profile(True)
     sim.step(min(steps, 100))
     ms_rebuild, ms_step, nprof = sim.profile()
@@ -533,15 +548,17 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
            "reference_mode_value": n / (ref_ms * 1e-3), "reference_mode_ms_per_step": ref_ms,
            "status": device.decode_status(status)}
     if want_cpu:
-        cb = cpu_reference_rate(P, st, cpu_seconds, hatch=False)
+        cb = cpu_reference_rate(P, st_timed, cpu_seconds, hatch=False)
         out["cpu_baseline"] = cb
         if cb:
+            cb["sample"] += ", from the state after the GPU's timed steps"
             out["vs_cpu_reference"] = out["value"] / cb["value"]
             out["reference_mode_vs_cpu_reference"] = out["reference_mode_value"] / cb["value"]
     return out
 
 
-def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=True):
+def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=True,
+             settle=60000):
     """Ball mill, the sphere charge of the mill configuration on the
     reference path: drum r = 50 cm, L = 30 cm with end plates, 30 rpm, eight
     4 x 4 cm lifters turned with the drum on the device every step
@@ -549,11 +566,14 @@ def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=Tru
     radius bins (the drum holds about 1.5e5 at lattice fill; the
     configuration's 2,000,000 such spheres would take three times the
     drum's volume), linear law kn = 1e6, e = 0.4, mu = 0.6, dt = 2e-6 s,
-    rotation on, power tallies on (FP64).  GPU: CUDA graphs, `skin` Verlet
-    list, `steps` steps from the packed charge after `warmup`; the
-    dissipated power over the timed steps is reported.  CPU: the
-    reference's kernels (oracle/_ref) with the lifter turn, all host
-    threads, reference mode, a bounded sample."""
+    rotation on, power tallies on (FP64).  The charge, packed inside the
+    lifter ring, first runs `settle` untimed steps with the drum turning
+    (0.12 s: it drops onto the drum and lifters and starts to tumble).
+    GPU: CUDA graphs, `skin` Verlet list, `steps` timed steps after
+    `warmup`; the dissipated power over the timed steps is reported.  CPU:
+    the reference's kernels (oracle/_ref) with the lifter turn, all host
+    threads, reference mode, a bounded sample of whole steps from the
+    GPU's state and lifter positions after its timed steps."""
     import torch
     from blaze import device, synth
     with tempfile.TemporaryDirectory() as d:
@@ -565,7 +585,7 @@ def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=Tru
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     sim.set_dobj_rotation(R, R, rad)
     sim.prepare_graphs()
-    sim.step(max(16, -(-warmup // 8) * 8))
+    sim.step(settle + max(16, -(-warmup // 8) * 8))
     status = sim.sync()
     sim.reset_energy()
     stream = torch.cuda.ExternalStream(sim.device_state()[3])
@@ -583,40 +603,55 @@ def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=Tru
     launches = fixed + rebuilds * sim.rebuild_kernels()
     e = sim.energy()
     T = steps * float(np.float32(P.sim_info.InitalDelta_t))
+    st_timed = sim.state()
+    dobj_timed = sim.dobj()
     sim.close()
     out = {"workload": "ball mill: drum r 50 cm L 30 cm, 30 rpm, 8 lifters turned on the device, "
                        "%d steel spheres r 0.3-0.6 cm (6 bins), kn 1e6 e 0.4 mu 0.6, dt 2e-6 s, "
                        "rotation and power tallies on" % n,
            "particles": n, "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-           "steps": steps, "skin_cm": skin, "rebuilds": rebuilds,
+           "steps": steps, "skin_cm": skin, "rebuilds": rebuilds, "settle_steps": settle,
            "gpu_launches": launches,
-           # the charge starts packed above the lifter ring: over the timed
-           # steps it settles onto itself before it reaches lifters and drum
            "power_w_timed_steps": {"particle": e[0] / T, "lifter": e[1] / T, "drum": e[2] / T,
                                    "total": float(e.sum()) / T},
            "status": device.decode_status(status)}
     if want_cpu:
-        cb = cpu_reference_rate(P, st, cpu_seconds, hatch=False, mill=(R, R, rad))
+        for k in range(P.n_d):
+            P.dobj[k] = dobj_timed[k]
+        cb = cpu_reference_rate(P, st_timed, cpu_seconds, hatch=False, mill=(R, R, rad))
         out["cpu_baseline"] = cb
         if cb:
+            cb["sample"] += ", from the state after the GPU's timed steps"
             out["vs_cpu_reference"] = out["value"] / cb["value"]
     return out
 
 
 class _StdoutToStderr:
-    """Send file descriptor 1 to stderr while the reference's kernels run:
-    their printf warnings would otherwise mix with the JSON line."""
+    """Catch file descriptor 1 while the reference's kernels run (their
+    printf warnings would otherwise mix with the JSON line), count the
+    polyhedron kernel's penetration-clamp warnings ("large dis",
+    DEM_Kernels_Compute.cuh:917-924) and pass the first lines to stderr."""
 
     def __enter__(self):
         sys.stdout.flush()
         self.saved = os.dup(1)
-        os.dup2(2, 1)
+        self.tmp = tempfile.TemporaryFile("w+b")
+        os.dup2(self.tmp.fileno(), 1)
+        self.large_dis = 0
         return self
 
     def __exit__(self, *exc):
         sys.stdout.flush()
+        import ctypes
+        ctypes.CDLL(None).fflush(None)
         os.dup2(self.saved, 1)
         os.close(self.saved)
+        self.tmp.seek(0)
+        text = self.tmp.read().decode("utf-8", "replace")
+        self.tmp.close()
+        self.large_dis = text.count("large dis")
+        if text:
+            sys.stderr.write(text[:4000])
         return False
 
 
@@ -675,8 +710,11 @@ def cpu_reference_rate(P, st, seconds, max_steps=None, hatch=True, mill=None):
     host threads, reference mode, on this workload: particle-steps/s.
     mill = (about_x, about_y, rad_per_step): drum rotating and the mill
     driver's lifter turn before every step."""
-    with _StdoutToStderr():
-        return _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill)
+    with _StdoutToStderr() as cap:
+        out = _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill)
+    if out is not None:
+        out["large_dis_warnings"] = cap.large_dis
+    return out
 
 
 def _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill=None):

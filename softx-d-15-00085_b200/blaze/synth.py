@@ -281,13 +281,14 @@ def random_quaternions(rng, n):
 
 
 def poly_box_project(root, n=100_000, r=0.5, spacing=0.93, rho=2700.0, kn=1.0e5, cor=0.5,
-                     mu=0.4, dt=1e-5, seed=2, name="PolyBox", world="Poly_box"):
+                     mu=0.4, dt=1e-5, seed=2, name="PolyBox", world="Poly_box", jitter=0.02):
     """Convex polyhedra in a closed box: dodecahedra, cubes and hexagonal
     prisms of circumradius r (types 0, 1, 2 in turn) on a jittered cubic
     lattice of the given spacing, so that bounding spheres of lattice
     neighbours overlap and every particle starts with contacts (the first
     layer touches the three lower walls); random
-    orientations, velocities N(0, 10 cm/s), spins N(0, 20 rad/s); y vertical.
+    orientations, velocities N(0, 10 cm/s), spins N(0, 20 rad/s); y vertical;
+    lattice positions jittered by U(-jitter, jitter) cm per coordinate.
     Returns (Project, state dict with a `quat` entry)."""
     base = os.path.join(root, name)
     for sub in ("SurfaceObjects", "ParticleObjects"):
@@ -308,7 +309,7 @@ def poly_box_project(root, n=100_000, r=0.5, spacing=0.93, rho=2700.0, kn=1.0e5,
                  axis=-1).reshape(-1, 3)[:n]
     # the first lattice layer 0.94 r from the three lower walls: vertices
     # that point at a wall touch it
-    pos = (g * spacing + 0.94 * r + rng.uniform(-0.02, 0.02, size=(n, 3)))
+    pos = (g * spacing + 0.94 * r + rng.uniform(-jitter, jitter, size=(n, 3)))
     # the parser's objects carry their centre of mass in the file frame
     # (here the origin up to rounding); positions are centres of mass
     ptype = np.arange(n, dtype=np.uint32) % len(shapes)
