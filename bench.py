@@ -330,6 +330,22 @@ def batched_leg(steps, warmup):
     status = ens.sync()
     n = ens.n
     ens.close()
+    # the same run with persistent stepping (one cooperative kernel between
+    # re-sorts, a grid barrier per step) instead of a graph node per step
+    ep = E.Ensemble(best["systems"], W, **dict(opts, use_graph=2))
+    ep.set_state(p, r)
+    ep.step(max(3, warmup))
+    ep.sync()
+    sp = torch.cuda.ExternalStream(ep.device_state()[3])
+    rbp0 = ep.num_rebuilds()
+    a.record(sp)
+    ep.step(steps)
+    b.record(sp)
+    b.synchronize()
+    persist_ms = a.elapsed_time(b) / steps
+    persist = {"ms_per_step": persist_ms, "rebuilds": ep.num_rebuilds() - rbp0,
+               "status": ep.sync(), "value": n / (persist_ms * 1e-3)}
+    ep.close()
     # single systems, one after another: a seeded random sample
     off = np.concatenate([[0], np.cumsum(counts)])
     pick = np.sort(np.random.default_rng(11).choice(len(counts), SEQ_SAMPLE, replace=False))
@@ -359,6 +375,7 @@ def batched_leg(steps, warmup):
             "autotuned": {"skin_cm": best["skin"], "cell_cm": best["cell"],
                           "block": best["block"],
                           "trials": [[t[0], t[1], round(t[2], 4), t[3]] for t in trials]},
+            "persistent_step": persist,
             "sequential_plain_ms_per_step": seq_ms, "vs_sequential_plain": seq_ms / ms,
             "sequential_plain_stderr_ms": seq_se,
             "sequential_sample": "%d of %d systems (seeded random), each timed over %d steps"

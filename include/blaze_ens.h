@@ -65,7 +65,13 @@ typedef struct blaze_ens_options {
   float dt;            /* s */
   float skin;          /* Verlet skin, cm, > 0 */
   int max_nbr;         /* neighbour / history slots per particle, 1..32 */
-  int use_graph;       /* 1: steps run as CUDA graphs (re-sort in a conditional node) */
+  int use_graph;       /* 1: steps run as CUDA graphs (re-sort in a conditional node);
+                        * 2: persistent stepping: one graph per call whose WHILE
+                        *    node runs rounds of (re-sort if asked, then one
+                        *    cooperative kernel that runs the steps up to the
+                        *    next re-sort with a grid barrier between steps;
+                        *    a barrier wait that gives up after 2 s raises
+                        *    status 16); not with capture_forces */
   int capture_forces;  /* 1: keep each step's contact force and torque per particle */
   int block;           /* threads per block of the step kernel: 64, 128, 256 or 512 */
 } blaze_ens_options;

@@ -67,8 +67,11 @@ struct blaze_ens {
   int* d_flags = nullptr;
   int* h_flags = nullptr;
   EnsCapture cap{};
-  cudaStream_t stream = nullptr, aux = nullptr;
+  cudaStream_t stream = nullptr, aux = nullptr, aux2 = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t pgraph[2] = {nullptr, nullptr};   // persistent stepping, home S[c]
+  int* d_pw = nullptr;        // persistent stepping: left, done, req_step, barrier x3
+  int persist_grid = 0;
   int* d_rb = nullptr;
   uint32_t status = 0;
   int last_launches = 0;
@@ -205,6 +208,8 @@ void drop_graphs(blaze_ens* e) {
   for (int c = 0; c < 2; ++c) {
     if (e->graph[c]) cudaGraphExecDestroy(e->graph[c]);
     e->graph[c] = nullptr;
+    if (e->pgraph[c]) cudaGraphExecDestroy(e->pgraph[c]);
+    e->pgraph[c] = nullptr;
   }
 }
 
@@ -222,9 +227,10 @@ void free_ens(blaze_ens* e) {
   f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
   f(e->d_sys); f(e->d_walls); f(e->d_tri_off); f(e->d_tri_ids); f(e->d_sys_of);
   f(e->st_pos3); f(e->st_rad); f(e->st_vel3); f(e->st_avel3); f(e->st_sys); f(e->st_pid);
-  f(e->d_flags); f(e->cap.f); f(e->cap.t);
+  f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->h_flags) cudaFreeHost(e->h_flags);
+  if (e->aux2) cudaStreamDestroy(e->aux2);
   if (e->aux) cudaStreamDestroy(e->aux);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -334,6 +340,118 @@ int build_graph(blaze_ens* e, int c) {
   return 0;
 }
 
+EnsPersist persist_words(const blaze_ens* e, cudaGraphConditionalHandle loop_h) {
+  EnsPersist p;
+  p.left = e->d_pw;
+  p.done = e->d_pw + 1;
+  p.req_step = e->d_pw + 2;
+  p.bar = reinterpret_cast<unsigned int*>(e->d_pw + 4);
+  p.loop_h = loop_h;
+  return p;
+}
+
+// Persistent stepping from and back to S[c]: one graph whose WHILE node runs
+// rounds until the step budget (*left, set before each launch) is spent.  A
+// round is a gate kernel (pending re-sort request into the IF node), the IF
+// node with the re-sort, and the persistent step kernel, which runs steps
+// until one asks for a re-sort or the budget is spent.
+int build_persist_graph_as(blaze_ens* e, int c, bool coop) {
+  if (e->persist_grid <= 0) {
+    e->persist_grid = ens_persist_grid(geom(e), e->opt.block, e->n);
+    if (e->persist_grid <= 0) return -2;
+  }
+  const int saved = e->cur;
+  e->cur = c;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hw;
+  CK(cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault));
+  const EnsPersist p = persist_words(e, hw);
+  CK(cudaStreamBeginCaptureToGraph(e->stream, g, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(e->stream, &cs, nullptr, &capg, &deps, &ndeps));
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    std::memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hw;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, capg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(e->stream, &wnode, 1, cudaStreamSetCaptureDependencies));
+    // the round, captured into the loop body on aux
+    cudaGraphConditionalHandle hi;
+    CK(cudaGraphConditionalHandleCreate(&hi, body, 0, 0));
+    CK(cudaStreamBeginCaptureToGraph(e->aux, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    ens_launch_persist_gate(e->ctl, p, e->d_rb, hi, e->aux);
+    {
+      cudaStreamCaptureStatus cs2;
+      cudaGraph_t capb = nullptr;
+      const cudaGraphNode_t* deps2 = nullptr;
+      size_t ndeps2 = 0;
+      CK(cudaStreamGetCaptureInfo(e->aux, &cs2, nullptr, &capb, &deps2, &ndeps2));
+      alignas(cudaGraphNodeParams) unsigned char raw2[sizeof(cudaGraphNodeParams)];
+      std::memset(raw2, 0, sizeof(raw2));
+      cudaGraphNodeParams& ip = *reinterpret_cast<cudaGraphNodeParams*>(raw2);
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hi;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      CK(cudaGraphAddNode(&inode, capb, deps2, ndeps2, &ip));
+      cudaGraph_t ibody = ip.conditional.phGraph_out[0];
+      CK(cudaStreamUpdateCaptureDependencies(e->aux, &inode, 1, cudaStreamSetCaptureDependencies));
+      CK(cudaStreamBeginCaptureToGraph(e->aux2, ibody, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal));
+      CK(cudaMemsetAsync(e->d_rb, 0x01, sizeof(int), e->aux2));
+      rc = enqueue_rebuild(e, nullptr, e->aux2);
+      cudaGraph_t tmp = nullptr;
+      CK(cudaStreamEndCapture(e->aux2, &tmp));
+    }
+    cudaError_t le = cudaSuccess;
+    if (!rc)
+      le = ens_launch_persist(geom(e), e->b, c, e->n, e->ctl, e->d_rb, p, e->opt.block,
+                              e->persist_grid, coop, e->aux);
+    cudaGraph_t tmp = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(e->aux, &tmp);
+    if (!rc && (le != cudaSuccess || ee != cudaSuccess)) rc = -3;
+  }
+  cudaGraph_t out = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(e->stream, &out);
+  if (!rc && ee != cudaSuccess) rc = -3;
+  if (!rc && cudaGraphInstantiate(&e->pgraph[c], out, 0) != cudaSuccess) rc = -3;
+  if (out) cudaGraphDestroy(out);
+  e->cur = saved;
+  return rc;
+}
+
+// A cooperative kernel node guarantees that every block of the persistent
+// kernel is resident; where a conditional body does not take one, the
+// kernel node is a plain one with the same occupancy-sized grid (the
+// barrier's bounded wait turns a block that could not start into
+// kStatusTimeout, not a hang).
+int build_persist_graph(blaze_ens* e, int c) {
+  int rc = build_persist_graph_as(e, c, true);
+  if (rc == -3) {
+    cudaGetLastError();
+    rc = build_persist_graph_as(e, c, false);
+  }
+  if (rc == -3) {
+    cudaGetLastError();
+    return -1;
+  }
+  return rc;
+}
+
 int sync_status(blaze_ens* e) {
   CK(cudaMemcpyAsync(e->h_ctl, e->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
@@ -354,6 +472,7 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
     return -1;
   if (o.block == 0) o.block = 256;
   if (o.block < 64 || o.block > kMaxStepBlock || o.block % 32 != 0) return -1;
+  if (o.use_graph < 0 || o.use_graph > 2) return -1;
   long long ntot = 0, cells = 0;
   for (int s = 0; s < nsys; ++s) {
     if (!valid_system(systems[s], nwalls, o.skin)) return -1;
@@ -386,6 +505,7 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   while (e->key_bits < 32 && (top >> e->key_bits) != 0) e->key_bits++;
   CKF(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   CKF(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
+  CKF(cudaStreamCreateWithFlags(&e->aux2, cudaStreamNonBlocking));
   const int n = e->n;
   const int cap = o.max_nbr;
   e->b.stride = n;
@@ -418,6 +538,8 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   CKF(dalloc(&e->ctl, 1));
   CKF(dalloc(&e->d_rb, kGraphSteps));
   CKF(cudaMemset(e->d_rb, 0, sizeof(int) * kGraphSteps));
+  CKF(dalloc(&e->d_pw, 8));
+  CKF(cudaMemset(e->d_pw, 0, sizeof(int) * 8));
   CKF(dalloc(&e->d_sys, nsys));
   CKF(dalloc(&e->d_walls, nwalls));
   CKF(dalloc(&e->d_sys_of, n));
@@ -571,6 +693,17 @@ namespace {
 // nsteps steps, as kGraphSteps-step CUDA graphs where `graphs` allows (the
 // remainder as plain steps).
 int advance(blaze_ens* e, int nsteps, bool graphs) {
+  if (graphs && e->opt.use_graph == 2 && !e->opt.capture_forces && nsteps > 0) {
+    const int c = e->cur;
+    if (!e->pgraph[c]) {
+      int rc = build_persist_graph(e, c);
+      if (rc) return rc;
+    }
+    ens_launch_persist_init(persist_words(e, 0), nsteps, e->stream);
+    CK(cudaGraphLaunch(e->pgraph[c], e->stream));
+    e->last_launches += 3;   // the budget, then one round's gate and step kernels
+    return 0;
+  }
   int done = 0;
   while (done < nsteps) {
     if (!graphs || nsteps - done < kGraphSteps) {
@@ -657,7 +790,11 @@ int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4,
 
 int blaze_ens_last_launches(blaze_ens* e) { return e ? e->last_launches : -1; }
 
-int blaze_ens_rebuild_kernels(blaze_ens* e) { return e ? rebuild_kernel_count(e) : -1; }
+int blaze_ens_rebuild_kernels(blaze_ens* e) {
+  if (!e) return -1;
+  // persistent stepping: a re-sort also starts another round (gate + step)
+  return rebuild_kernel_count(e) + (e->opt.use_graph == 2 ? 2 : 0);
+}
 
 }  // extern "C"
 

@@ -24,6 +24,8 @@
 //   Walls use the same law with R* = r, m* = m.
 #include "ens_kernels.cuh"
 
+#include <algorithm>
+
 namespace blaze {
 namespace {
 
@@ -345,35 +347,26 @@ __global__ void k_ens_epoch(StepCtl* ctl, const int* gate) {
 // ------------------------------------------------------------------- step
 // candidate slots tested per batch of independent loads in the contact pass
 constexpr uint32_t kEnsMaskBatch = 4;
-// kRecord: also write what the step reads into tape slot tp.ctl->slot (the
-// history words are reserved first, by every thread of the block).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved>
-__global__ void __launch_bounds__(kMaxStepBlock)
-k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
-           StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
-  const bool rebuilt = *link.rebuilt != 0;
-  const StateBuf in = rebuilt ? in_sorted : in_plain;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = ctl->epoch & 1;
-  const EnsList L = b.L[e];
-  TapeView tv{};
-  float* hrec = nullptr;
-  if constexpr (kRecord) {
-    const TapeStep ts = tp.steps[tp.ctl->slot];
-    tv = tape_view(tp, ts.block, n);
-    uint32_t words = 0;
-    if (i < n)
-      words = 3u * (uint32_t)__popc(L.mask[i]) +
-              4u * (uint32_t)__popc(__float_as_uint(in.vel[i].w) >> kSysBits);
-    bool ok;
-    const uint32_t off =
-        tape_reserve(words, &tp.ctl->cur, tp.ctl->lim, ts.hbase, &tp.ctl->overflow, ok);
-    if (i < n) {
-      tv.hoff[i] = off;
-      if (ok) hrec = reinterpret_cast<float*>(tp.arena + ts.hbase + off);
-    }
-  }
-  if (i >= n) return;
+// A neighbour's state: through the read-only cache (kNc) when the state
+// cannot change during the kernel, else a plain load (the persistent kernel
+// reads, after a grid barrier, what other blocks wrote in the same launch).
+template <bool kNc>
+__device__ __forceinline__ float4 ld_state(const float4* p) {
+  if constexpr (kNc) return __ldg(p);
+  else return *p;
+}
+
+// The step of particle i: its contacts in list order (tangential histories
+// updated in place, the particle's own slots only), its walls, symplectic
+// Euler from `in` into `out`.  Raises status bits in st; returns the path
+// the particle has moved since the last re-sort.  kRecord: also writes what
+// the step reads into the tape view (histories to hrec when it is not null).
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true>
+__device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBufs& b,
+                                                   const StateBuf& in, const StateBuf& out,
+                                                   int i, int e, const EnsList& L, TapeView tv,
+                                                   float* hrec, const EnsCapture& cap,
+                                                   uint32_t& st) {
   const size_t stride = (size_t)b.stride;
   const float dt = g.dt;
   const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
@@ -384,7 +377,6 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   const uint32_t wmask_o = bits >> kSysBits;
   const EnsSysDev& S = g.sys[sys];
   const float ma = sphere_mass(S, ra);
-  uint32_t st = 0;
 
   // particle-particle contacts, in list order
   float3 f = f3(0.0f, 0.0f, 0.0f), t = f3(0.0f, 0.0f, 0.0f);
@@ -409,7 +401,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     float4 pb[kEnsMaskBatch];
 #pragma unroll
     for (uint32_t u = 0; u < kEnsMaskBatch; ++u)
-      pb[u] = k0 + u < cnt ? __ldg(in.pos + jj[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      pb[u] = k0 + u < cnt ? ld_state<kNc>(in.pos + jj[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
     for (uint32_t u = 0; u < kEnsMaskBatch; ++u) {
       const float3 rel = pa - xyz(pb[u]);
@@ -423,7 +415,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     cmask &= cmask - 1u;
     const size_t sk = (size_t)k * stride + i;
     const uint32_t j = L.idx[sk];
-    const float4 pb4 = __ldg(in.pos + j);
+    const float4 pb4 = ld_state<kNc>(in.pos + j);
     const float3 rel = pa - xyz(pb4);
     const float rb = pb4.w;
     const float sr = ra + rb;
@@ -436,7 +428,7 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     // pass a pair whose FP64-formed overlap is not positive
     const float delta = overlap_pair(ra, rb, pa, xyz(pb4));
     if (!(delta > 0.0f)) continue;
-    const float4 vb4 = __ldg(in.vel + j), wb4 = __ldg(in.angv + j);
+    const float4 vb4 = ld_state<kNc>(in.vel + j), wb4 = ld_state<kNc>(in.angv + j);
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);
     float3 xi = f3(0.0f, 0.0f, 0.0f);
@@ -558,6 +550,45 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   out.vel[i] = make_float4(v.x, v.y, v.z, __uint_as_float(sys | (wmask << kSysBits)));
   out.angv[i] = make_float4(w.x, w.y, w.z, path);
   if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
+  if (kCapture) {
+    cap.f[i] = make_float4(f.x, f.y, f.z, 0.0f);
+    cap.t[i] = make_float4(t.x, t.y, t.z, 0.0f);
+  }
+  return path;
+}
+
+// kRecord: also write what the step reads into tape slot tp.ctl->slot (the
+// history words are reserved first, by every thread of the block).
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved>
+__global__ void __launch_bounds__(kMaxStepBlock)
+k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
+           StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
+  const bool rebuilt = *link.rebuilt != 0;
+  const StateBuf in = rebuilt ? in_sorted : in_plain;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = ctl->epoch & 1;
+  const EnsList L = b.L[e];
+  TapeView tv{};
+  float* hrec = nullptr;
+  if constexpr (kRecord) {
+    const TapeStep ts = tp.steps[tp.ctl->slot];
+    tv = tape_view(tp, ts.block, n);
+    uint32_t words = 0;
+    if (i < n)
+      words = 3u * (uint32_t)__popc(L.mask[i]) +
+              4u * (uint32_t)__popc(__float_as_uint(in.vel[i].w) >> kSysBits);
+    bool ok;
+    const uint32_t off =
+        tape_reserve(words, &tp.ctl->cur, tp.ctl->lim, ts.hbase, &tp.ctl->overflow, ok);
+    if (i < n) {
+      tv.hoff[i] = off;
+      if (ok) hrec = reinterpret_cast<float*>(tp.arena + ts.hbase + off);
+    }
+  }
+  if (i >= n) return;
+  uint32_t st = 0;
+  const float path =
+      ens_particle_step<kLaw, kCapture, kRecord, kCurved>(g, b, in, out, i, e, L, tv, hrec, cap, st);
   {
     const unsigned m = __activemask();
     const unsigned req = __ballot_sync(m, path > 0.5f * g.skin);
@@ -567,10 +598,127 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     }
   }
   ens_flag(ctl, st);
-  if (kCapture) {
-    cap.f[i] = make_float4(f.x, f.y, f.z, 0.0f);
-    cap.t[i] = make_float4(t.x, t.y, t.z, 0.0f);
+}
+
+// ------------------------------------------------------- persistent steps
+// One launch runs up to *left steps with a grid barrier between them, so a
+// stretch of steps without a re-sort costs one launch instead of one launch
+// and one conditional node per step.  Every block is resident (cooperative
+// launch, grid from the occupancy), the particles are strided over the grid.
+// Buffers: step 0 reads the sorted copy after a re-sort, else `home`; steps
+// then alternate home -> other -> home, and an odd count ends with a copy
+// back, so each launch leaves the state in `home`.  A step whose particles
+// ask for a re-sort is the launch's last: requests record the step index
+// (atomicMin), and after barrier k every block reads the same answer to
+// "was one made at step <= k" (a block already in step k + 1 can only write
+// k + 1).  Barrier waits are bounded by the global timer; a block that gives
+// up raises kStatusTimeout and the abort word, and every block returns.
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;   // 2 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Arrival counter bar[0], generation bar[1], abort word bar[2].  Returns
+// false when the barrier was aborted (by this block or another).
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks,
+                                             StepCtl* ctl) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vb = bar;
+    int ok = vb[2] == 0u;
+    if (ok) {
+      const unsigned int gen = vb[1];
+      __threadfence();
+      if (atomicAdd(bar, 1u) == nblocks - 1u) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        const unsigned long long t0 = global_ns();
+        while (vb[1] == gen) {
+          if (vb[2] != 0u) { ok = 0; break; }
+          if (global_ns() - t0 > kBarrierLimitNs) {
+            atomicExch(bar + 2, 1u);
+            atomicOr(&ctl->status, kStatusTimeout);
+            ok = 0;
+            break;
+          }
+          __nanosleep(100);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
   }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int kLaw, bool kCurved>
+__global__ void __launch_bounds__(kMaxStepBlock)
+k_ens_persist(EnsGeom g, EnsBufs b, StateBuf home, StateBuf other, StateBuf sorted, int n,
+              StepCtl* ctl, const int* rebuilt, EnsPersist p) {
+  const int e = ctl->epoch & 1;
+  const EnsList L = b.L[e];
+  const int budget = *p.left;
+  const bool rb = *rebuilt != 0;
+  const int gstride = gridDim.x * blockDim.x;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  int done = 0;
+  bool stop = false, aborted = false;
+  for (int k = 0; k < budget && !stop; ++k) {
+    const StateBuf in = k == 0 ? (rb ? sorted : home) : ((k & 1) ? other : home);
+    const StateBuf out = (k & 1) ? home : other;
+    uint32_t st = 0;
+    bool req = false;
+    for (int i = i0; i < n; i += gstride) {
+      const float path = ens_particle_step<kLaw, false, false, kCurved, false>(
+          g, b, in, out, i, e, L, TapeView{}, nullptr, EnsCapture{nullptr, nullptr}, st);
+      req |= path > 0.5f * g.skin;
+    }
+    if (__syncthreads_or(req ? 1 : 0) && threadIdx.x == 0) atomicMin(p.req_step, k);
+    if (st) atomicOr(&ctl->status, st);
+    if (!grid_barrier(p.bar, gridDim.x, ctl)) { aborted = true; break; }
+    done = k + 1;
+    stop = *(volatile int*)p.req_step <= k;
+  }
+  if (!aborted && (done & 1)) {
+    for (int i = i0; i < n; i += gstride) {
+      home.pos[i] = other.pos[i];
+      home.vel[i] = other.vel[i];
+      home.angv[i] = other.angv[i];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int left = aborted ? 0 : budget - done;
+    if (stop) ctl->rebuild_req = 1;
+    if (aborted) left = 0;
+    *p.left = left;
+    *p.done += done;
+    cudaGraphSetConditional(p.loop_h, left > 0 ? 1u : 0u);
+  }
+}
+
+// Start of a round of the WHILE loop: take the pending re-sort request into
+// the IF node, clear the round's words.
+__global__ void k_ens_persist_gate(StepCtl* ctl, EnsPersist p, int* rb,
+                                   cudaGraphConditionalHandle if_h) {
+  const int r = ctl->rebuild_req;
+  ctl->rebuild_req = 0;
+  *rb = 0;
+  *p.req_step = 0x7fffffff;
+  p.bar[0] = 0u;
+  p.bar[1] = 0u;
+  p.bar[2] = 0u;
+  cudaGraphSetConditional(if_h, r ? 1u : 0u);
+}
+
+__global__ void k_ens_persist_init(EnsPersist p, int steps) {
+  *p.left = steps;
 }
 
 // ---------------------------------------------------------------- staging
@@ -670,6 +818,56 @@ void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, 
   // reverse mode accepts plane walls only (blaze_ens_adj_create)
   k_ens_step<kLawLinear, false, true, false><<<gs, bs, 0, st>>>(
       g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, EnsCapture{nullptr, nullptr}, tape);
+}
+
+int ens_persist_grid(const EnsGeom& g, int block, int n) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  cudaError_t err;
+  if (g.curved)
+    err = g.law == kLawHertz
+              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawHertz, true>, block, 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawLinear, true>, block, 0);
+  else
+    err = g.law == kLawHertz
+              ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawHertz, false>, block, 0)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawLinear, false>, block, 0);
+  if (err != cudaSuccess || per_sm < 1) return 0;
+  const int need = (n + block - 1) / block;
+  return std::max(1, std::min(need, per_sm * sms));
+}
+
+cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int n, StepCtl* ctl,
+                               const int* rebuilt, const EnsPersist& p, int block, int grid,
+                               bool coop, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = coop ? 1 : 0;
+  const StateBuf sh = b.S[home], so = b.S[home ^ 1], ss = b.S[2];
+  if (g.curved) {
+    if (g.law == kLawHertz)
+      return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawHertz, true>, g, b, sh, so, ss, n, ctl, rebuilt, p);
+    return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawLinear, true>, g, b, sh, so, ss, n, ctl, rebuilt, p);
+  }
+  if (g.law == kLawHertz)
+    return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawHertz, false>, g, b, sh, so, ss, n, ctl, rebuilt, p);
+  return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawLinear, false>, g, b, sh, so, ss, n, ctl, rebuilt, p);
+}
+
+void ens_launch_persist_gate(StepCtl* ctl, const EnsPersist& p, int* rb,
+                             cudaGraphConditionalHandle if_h, cudaStream_t st) {
+  k_ens_persist_gate<<<1, 1, 0, st>>>(ctl, p, rb, if_h);
+}
+
+void ens_launch_persist_init(const EnsPersist& p, int steps, cudaStream_t st) {
+  k_ens_persist_init<<<1, 1, 0, st>>>(p, steps);
 }
 
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,

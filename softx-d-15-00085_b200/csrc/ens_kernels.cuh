@@ -250,6 +250,29 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
 // tape.ctl->slot: input state, history mask, active and wall histories.
 void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
                             StepLink link, const EnsTape& tape, int block, cudaStream_t st);
+// Persistent stepping: one cooperative launch runs up to *left steps with a
+// grid barrier between steps and returns at the first step that asks for a
+// re-sort (ctl->rebuild_req set) or when the budget is spent, with the state
+// back in S[home]; it subtracts the steps run from *left, adds them to
+// *done and sets loop_h (a WHILE node's handle) to *left > 0.
+struct EnsPersist {
+  int* left;                           // steps still to run in this graph launch
+  int* done;                           // steps run (a running count)
+  int* req_step;                       // first step of the launch that asked for a re-sort
+  unsigned int* bar;                   // grid barrier: arrivals, generation, abort
+  cudaGraphConditionalHandle loop_h;
+};
+// The grid of the persistent step: every block resident (0: no fit).
+int ens_persist_grid(const EnsGeom& g, int block, int n);
+// coop: launch as a cooperative kernel (every block resident or no launch).
+cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int n, StepCtl* ctl,
+                               const int* rebuilt, const EnsPersist& p, int block, int grid,
+                               bool coop, cudaStream_t st);
+// One thread: the pending re-sort request into if_h, *rb = 0, the round's
+// request word and barrier cleared.
+void ens_launch_persist_gate(StepCtl* ctl, const EnsPersist& p, int* rb,
+                             cudaGraphConditionalHandle if_h, cudaStream_t st);
+void ens_launch_persist_init(const EnsPersist& p, int steps, cudaStream_t st);
 // Staged caller arrays -> state S[cur], pid = index, both list copies and
 // every history cleared; flags[0] |= 1 for a radius that is not positive.
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,

@@ -11,9 +11,11 @@ tests compare the library's Verlet-skin path with.
   box_c1      the Particles_Box plain configuration (10,000 spheres,
               r = 0.1 cm, in a 10 cm cube, falling from a jittered lattice):
               kinetic energy (translational + rotational) every 100 steps to
-              12,000 steps, the dissipated-energy tallies at the same steps,
-              and the vertical solid-fraction profile at 2,000 and 12,000
-              steps.
+              12,000 steps, the dissipated-energy tallies at the same steps
+              (the per-contact values summed in FP64, as the library sums
+              them; box_edis_float_tally: the reference's own FP32
+              accumulators, which lose the small late contributions), and
+              the vertical solid-fraction profile at 2,000 and 12,000 steps.
 
 Each case runs R_RUNS times: run 0 from the given state, the others with
 every position coordinate moved by one unit in the last place, up or down at
@@ -83,15 +85,16 @@ def _box(run, threads):
                        capture=False)
     R.set_state(perturb(st["pos"], run), st["vel"], st["avel"], st["type"], st["pid"])
     m, r = float(P.pobj[0].mass), float(P.pobj[0].radius)
-    ke, edis, prof = [], [], []
+    ke, edis, edis32, prof = [], [], [], []
     for k in range(BOX_EVERY, BOX_STEPS + 1, BOX_EVERY):
         assert R.step(BOX_EVERY) == 0
         s = R.state()
         ke.append(S.kinetic_energy(s["vel"], s["avel"], m, r))
-        edis.append(np.asarray(R.energy(), np.float64)[[0, 2]])
+        edis.append(R.energy64()[[0, 2]])
+        edis32.append(np.asarray(R.energy(), np.float64)[[0, 2]])
         if k in BOX_PROFILE_AT:
             prof.append(S.solid_fraction_profile(s["pos"], r))
-    return np.array(ke), np.array(edis), np.array(prof)
+    return np.array(ke), np.array(edis), np.array(prof), np.array(edis32)
 
 
 def _job(args):
@@ -110,7 +113,8 @@ def main():
                box_every=BOX_EVERY, box_steps=BOX_STEPS,
                box_profile_at=np.array(BOX_PROFILE_AT),
                box_ke=np.stack([b[0] for b in box]), box_edis=np.stack([b[1] for b in box]),
-               box_profile=np.stack([b[2] for b in box]), runs=R_RUNS)
+               box_profile=np.stack([b[2] for b in box]),
+               box_edis_float_tally=np.stack([b[3] for b in box]), runs=R_RUNS)
     path = os.path.join(HERE, "long_run.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -128,6 +128,30 @@ def test_graph_stepping_equals_plain(boxes):
     assert out[0]["status"] == 0 and out[1]["status"] == 0
 
 
+@pytest.mark.parametrize("law", [E.LAW_LINEAR, E.LAW_HERTZ_MINDLIN])
+def test_persistent_stepping_equals_plain(boxes, law):
+    """use_graph = 2: one persistent kernel runs the steps between re-sorts
+    with a grid barrier per step.  Same states, order and re-sort count as
+    plain stepping, over uneven calls (budgets that end on and off a
+    re-sort); planes, and the triangle-mesh silo with its cylinder."""
+    S, W, p, r = boxes
+    S2, W2, p2, r2, v2 = mesh_silo()
+    for (sy, wa, pos, rad, vel) in ((S, W, p, r, None), (S2, W2, p2, r2, v2)):
+        out, rb = [], []
+        for g in (0, 2):
+            e = E.Ensemble(sy, wa, law=law, dt=DT, skin=SKIN, use_graph=g)
+            e.set_state(pos, rad, vel)
+            for k in (1, 7, 150, 245):
+                e.step(k)
+            out.append(e.state())
+            rb.append(e.num_rebuilds())
+            e.close()
+        for key in ("pos", "vel", "avel", "pid"):
+            np.testing.assert_array_equal(out[0][key], out[1][key], err_msg=key)
+        assert out[0]["status"] == 0 and out[1]["status"] == 0, (out[0]["status"], out[1]["status"])
+        assert rb[0] == rb[1] and rb[0] > 1, rb
+
+
 def test_out_of_grid_is_reported_not_faulted(boxes):
     S, W, p, r = boxes
     p = p.copy()

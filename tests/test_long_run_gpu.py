@@ -15,8 +15,9 @@ must lie within max(SPREAD_FACTOR x that spread, a stated floor) of run 0.
         percent discharged (main.cpp:142), 20 counts; written to
         FlowRate.dat by the driver loop of blaze.results.
   box   the Particles_Box plain configuration, 10,000 spheres: kinetic
-        energy every 100 steps to 12,000, the dissipated-energy tallies,
-        and the solid-fraction profile at 2,000 and 12,000 steps.
+        energy every 100 steps to 12,000, the dissipated-energy tallies
+        (bit-exact law; energy tallies keep the reference's arithmetic), and
+        the solid-fraction profile at 2,000 and 12,000 steps.
 """
 import os
 import types
@@ -96,7 +97,9 @@ def test_box_energy_and_packing_statistics(tmp_path, fast_law):
     from blaze import device, synth
     z = _fixture()
     P, st = synth.box_project(str(tmp_path))
-    P.sim_info.EnergyCalc = True
+    # energy tallies keep the reference's arithmetic in the law, so the
+    # contracted law runs without them
+    P.sim_info.EnergyCalc = not fast_law
     sim = device.Simulation(P, skin=0.02, use_graph=1, fast_law=fast_law)
     sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     m, r = float(P.pobj[0].mass), float(P.pobj[0].radius)
@@ -119,9 +122,14 @@ def test_box_energy_and_packing_statistics(tmp_path, fast_law):
         "contracted" if fast_law else "bit-exact law", np.round(ke[9::10], 2).tolist(),
         np.round(ref_ke[0][9::10], 2).tolist(), (d_ke / b_ke).max()))
     assert np.all(d_ke <= b_ke), (d_ke / b_ke).max()
-    # dissipated energy (particle-particle, particle-world), final values
-    b_ed = _band(ref_ed[:, -1, :], EDIS_REL * ref_ed[0, -1, :])
-    assert np.all(np.abs(edis[-1] - ref_ed[0, -1]) <= b_ed), (edis[-1], ref_ed[:, -1])
+    if not fast_law:
+        # dissipated energy (particle-particle, particle-world) at every
+        # sample, FP64 sums of the per-contact values on both sides
+        b_ed = _band(ref_ed, EDIS_REL * ref_ed[0, -1, :])
+        d_ed = np.abs(edis - ref_ed[0])
+        print("  dissipated energy at 12,000 steps GPU %s oracle A %s, worst deviation / band %.2f"
+              % (edis[-1], ref_ed[0, -1], (d_ed / b_ed).max()))
+        assert np.all(d_ed <= b_ed), (d_ed / b_ed).max()
     b_phi = _band(ref_prof, PHI_ABS)
     d_phi = np.abs(prof - ref_prof[0])
     print("  solid fraction profile at %s steps, worst deviation / band %.2f" % (
