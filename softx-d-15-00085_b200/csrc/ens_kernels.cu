@@ -658,8 +658,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
   return s_ok != 0;
 }
 
+// Registers capped at the step kernel's count, so as many blocks stay
+// resident as the per-step launches have.
+constexpr int kPersistRegs = 80;
+
 template <int kLaw, bool kCurved>
-__global__ void __launch_bounds__(kMaxStepBlock)
+__global__ void __maxnreg__(kPersistRegs)
 k_ens_persist(EnsGeom g, EnsBufs b, StateBuf home, StateBuf other, StateBuf sorted, int n,
               StepCtl* ctl, const int* rebuilt, EnsPersist p) {
   const int e = ctl->epoch & 1;

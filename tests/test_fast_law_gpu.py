@@ -1,8 +1,8 @@
 """The contracted particle-particle law (blaze_options.fast_law = 1) against
 the reference's own kernels on its own project (oracle-A golden fixture:
 Projects/2.Silo world SPH_90, 1,950 spheres with the silo hatch), and
-against the FP64 restatement of the reference law on the synthetic
-10,000-sphere box brought to rest in contact.  (A run with energy tallies, such as
+against the FP64 restatement of the reference law on 20,000 spheres of
+the synthetic silo workload settled into contact.  (A run with energy tallies, such as
 the ball-mill fixture, keeps the reference's arithmetic in the law.)
 
 Bar: the contact lists are the reference's bit for bit (the contact test is
@@ -70,31 +70,27 @@ def test_fast_law_vs_reference_kernels(name):
     assert e_v < TOL, e_v
 
 
-def test_fast_law_vs_fp64_box(tmp_path):
-    """10,000 spheres of the box configuration brought to rest in contact:
-    a simple-cubic stack of pitch 0.2005 cm (r = 0.1 cm) just above the
-    floor, settled under gravity by 20 rounds of 200 steps with the
-    velocities zeroed before each round (the box's own dynamics, e = 0.5 at
-    ~2.3 steps per contact, keep it bouncing for tens of thousands of
-    steps).  Every particle then rests on the one below.  One step's
+def test_fast_law_vs_fp64_settled_silo(tmp_path):
+    """20,000 spheres (r in [0.2, 0.4] cm) of the silo workload settled for
+    20,000 steps with the hatch closed: a bed in contact, several contacts
+    per particle with overlaps set by the weight above.  One step's
     particle-particle forces, contracted and bit-exact, against the FP64
     restatement of the reference law from that state."""
-    P, st0 = synth.box_project(str(tmp_path), pitch=0.2005, start=0.1005, jitter=0.0)
-    s = device.Simulation(P, skin=0.02, use_graph=1)
-    st = st0
-    zero = np.zeros_like(st0["vel"])
-    for _ in range(20):
-        s.set_state(st["pos"], zero, zero, st["type"], st["pid"])
-        s.step(200)
-        st = s.state()
-        assert st["status"] == 0, device.decode_status(st["status"])
+    P, st0 = synth.silo_project(str(tmp_path), n=20000)
+    s = device.Simulation(P, skin=0.1, use_graph=1)
+    s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
+    s.step(20000)
+    st = s.state()
     s.close()
-    st["vel"][:] = 0.0
-    st["avel"][:] = 0.0
+    assert st["status"] == 0, device.decode_status(st["status"])
     # contacts per particle
     from scipy.spatial import cKDTree
-    pairs = cKDTree(st["pos"].astype(np.float64)).query_pairs(0.2)
-    assert 2 * len(pairs) / len(st["pos"]) > 1.5, 2 * len(pairs) / len(st["pos"])
+    rad = np.array([P.pobj[t].radius for t in range(P.n_p)], np.float64)[st["type"]]
+    pos = st["pos"].astype(np.float64)
+    pairs = np.array(sorted(cKDTree(pos).query_pairs(2.0 * rad.max())))
+    dist = np.linalg.norm(pos[pairs[:, 0]] - pos[pairs[:, 1]], axis=1)
+    contacts = int((dist < rad[pairs[:, 0]] + rad[pairs[:, 1]]).sum())
+    assert 2 * contacts / len(pos) > 2.0, 2 * contacts / len(pos)
     out = {}
     for fast in (0, 1):
         g = device.Simulation(P, capture_forces=1, fast_law=fast)
@@ -108,10 +104,12 @@ def test_fast_law_vs_fp64_box(tmp_path):
     o.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
     o.step(1)
     f64 = o.forces()["f_pp"][np.argsort(o.state()["pid"])]
-    weight = float(P.pobj[0].mass) * 981.0
+    mass = np.array([P.pobj[t].mass for t in range(P.n_p)], np.float64)
+    weight = mass[st["type"][np.argsort(st["pid"])]] * 981.0
     e_exact = rel_err(out[0], f64, weight)
     e_fast = rel_err(out[1], f64, weight)
     e_pair = rel_err(out[1], out[0].astype(np.float64), weight)
-    print("box, 10,000 spheres: vs FP64 bit-exact %.2e contracted %.2e; contracted vs bit-exact "
-          "%.2e" % (e_exact, e_fast, e_pair))
+    print("settled silo, 20,000 spheres, %.1f contacts per particle: vs FP64 bit-exact %.2e "
+          "contracted %.2e; contracted vs bit-exact %.2e"
+          % (2 * contacts / len(pos), e_exact, e_fast, e_pair))
     assert e_pair < TOL, e_pair
