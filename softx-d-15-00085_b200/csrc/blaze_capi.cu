@@ -84,6 +84,7 @@ struct blaze_sim {
   uint32_t* d_chk = nullptr;           // list-check maxima slots (StepCtl::chk)
   bool spin_free = false;              // rotation off and every angular velocity zero
   int key_bits = 1;
+  uint32_t cells_cap = 0;   // entries allocated in cstart / cend
   long long steps = 0;
   // with a skin, steps below this index each end with a list check (from a
   // forced re-sort to the next multiple of kListCheckEvery; see force_check)
@@ -146,7 +147,25 @@ void build_params(blaze_sim* s) {
   P.origin = si.worldOrigin;
   P.cell = si.cellSize;
   P.ncells = si.num_NNCells;
-  const long long nx = si.num_NNCells.x, ny = si.num_NNCells.y, nz = si.num_NNCells.z;
+  if (s->opt.skin > 0.0f) {
+    // A Verlet list keeps pairs up to ra + rb + skin apart, and the 27-cell
+    // search finds a pair only when it lies within one cell edge: the list
+    // grid's cells are at least 2 r_max + skin, over the project grid's
+    // extent (the project's cells, 2 r_max in the shipped worlds, serve the
+    // contacts-only search of reference mode).
+    float rmax = 0.0f;
+    for (int t = 0; t < s->n_p; ++t) rmax = std::max(rmax, s->p[t].radius);
+    const float need = 2.0f * rmax + s->opt.skin;
+    float* c[3] = {&P.cell.x, &P.cell.y, &P.cell.z};
+    int* nc[3] = {&P.ncells.x, &P.ncells.y, &P.ncells.z};
+    for (int a = 0; a < 3; ++a) {
+      if (*c[a] >= need) continue;
+      const double extent = (double)*nc[a] * (double)*c[a];
+      *c[a] = need;
+      *nc[a] = std::max(1, (int)std::ceil(extent / (double)need));
+    }
+  }
+  const long long nx = P.ncells.x, ny = P.ncells.y, nz = P.ncells.z;
   const long long hmax = (nx - 1) + (nz - 1) * nz + (ny - 1) * nx * nz + 1;
   const long long prod = nx * ny * nz;
   P.ncell_tab = (uint32_t)std::max(hmax, prod);
@@ -432,6 +451,27 @@ int upload_params(blaze_sim* s) {
   if (rc) return rc;
   build_params(s);
   return upload_walls(s);
+}
+
+// The cell table and the sort's key width for the current grid (the list
+// grid with a skin, the project's without); reallocated when the grid grows.
+int alloc_cells(blaze_sim* s) {
+  const uint32_t nt = s->hp.ncell_tab;
+  const uint32_t top = nt + 1u;
+  s->key_bits = 1;
+  while (s->key_bits < 32 && (top >> s->key_bits) != 0) s->key_bits++;
+  if (nt > s->cells_cap) {
+    if (s->cstart) CK(cudaFree(s->cstart));
+    if (s->cend) CK(cudaFree(s->cend));
+    s->cstart = s->cend = nullptr;
+    s->cells_cap = 0;
+    CK(dalloc(&s->cstart, nt));
+    CK(dalloc(&s->cend, nt));
+    s->cells_cap = nt;
+  }
+  CK(cudaMemset(s->cstart, 0xff, sizeof(uint32_t) * nt));
+  CK(cudaMemset(s->cend, 0xff, sizeof(uint32_t) * nt));
+  return 0;
 }
 
 // Per-slot narrow-phase buffers of the polyhedron passes, sized by the
@@ -1195,13 +1235,8 @@ int create_impl(blaze_sim** out, const WOBJ* w, int n_w, const POBJ* p, int n_p,
   CKF(cudaMemcpy(s->ctl, s->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice));
   int rc = upload_params(s);
   if (rc) return fail(rc);
-  uint32_t top = s->hp.ncell_tab + 1u;
-  s->key_bits = 1;
-  while (s->key_bits < 32 && (top >> s->key_bits) != 0) s->key_bits++;
-  CKF(dalloc(&s->cstart, s->hp.ncell_tab));
-  CKF(dalloc(&s->cend, s->hp.ncell_tab));
-  CKF(cudaMemset(s->cstart, 0xff, sizeof(uint32_t) * s->hp.ncell_tab));
-  CKF(cudaMemset(s->cend, 0xff, sizeof(uint32_t) * s->hp.ncell_tab));
+  rc = alloc_cells(s);
+  if (rc) return fail(rc);
   rc = alloc_nlist(s);
   if (rc) return fail(rc);
   rc = alloc_capture(s);
@@ -1269,6 +1304,8 @@ int blaze_set_options(blaze_sim* s, const blaze_options* opt) {
   if (s->opt.max_nbr != old.max_nbr) rc = alloc_nlist(s);
   if (!rc) rc = alloc_capture(s);
   if (!rc) rc = upload_params(s);
+  // a skin turned on or off changes the list grid
+  if (!rc) rc = alloc_cells(s);
   // a new skin or capacity invalidates the current list
   s->h_ctl->rebuild_req = 1;
   force_check(s);
