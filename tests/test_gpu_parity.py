@@ -121,6 +121,57 @@ def test_skin_mode_matches_reference_mode(box):
     fast.close()
 
 
+def _skin_vs_reference_each_step(P, st, skin, pre, count, hatch=False):
+    """Step the skin path `pre` steps, then for `count` steps compare each
+    step's particle-particle forces with the reference mode's from the same
+    state: equal up to the order of summation (a pair the list missed
+    would show as a whole contact force)."""
+    sk = device.Simulation(P, skin=skin, capture_forces=1)
+    rf = device.Simulation(P, capture_forces=1)
+    for s in (sk, rf):
+        if hatch:
+            s.open_hatch()
+    sk.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+    sk.step(pre)
+    mass = np.array([P.pobj[t].mass for t in range(P.n_p)], np.float64)
+    worst = 0.0
+    for _ in range(count):
+        a = sk.state()
+        rf.set_state(a["pos"], a["vel"], a["avel"], a["type"], a["pid"])
+        rf.step(1)
+        fr, pr = rf.forces()["f_pp"], rf.state()["pid"]
+        sk.step(1)
+        fs, ps = sk.forces()["f_pp"], sk.state()["pid"]
+        x = fr[np.argsort(pr)].astype(np.float64)
+        y = fs[np.argsort(ps)].astype(np.float64)
+        w = mass[a["type"][np.argsort(a["pid"])]] * 981.0
+        e = np.linalg.norm(x - y, axis=1) / np.maximum(np.linalg.norm(x, axis=1), w)
+        worst = max(worst, float(e.max()))
+    status = sk.sync()
+    sk.close()
+    rf.close()
+    return worst, status
+
+
+def test_skin_list_finds_every_contact_box(box):
+    """The box (r = 0.1 cm, project cells 0.2 cm = 2 r) with a 0.02 cm skin,
+    in its bouncing phase (steps 6,000-6,200): the list grid's cells are
+    2 r + skin, so no pair within the skin lies beyond the 27 cells."""
+    P, st0 = box
+    worst, status = _skin_vs_reference_each_step(P, st0, 0.02, 6000, 200)
+    assert status == 0, device.decode_status(status)
+    assert worst < 1e-4, worst
+
+
+def test_skin_list_finds_every_contact_silo(silo_small):
+    """The silo workload (r in [0.2, 0.4] cm, project cells 0.8 cm = 2 r_max)
+    with the headline's 0.16 cm skin, hatch open, steps 3,000-3,100."""
+    P, st = silo_small
+    worst, status = _skin_vs_reference_each_step(P, st, 0.16, 3000, 100, hatch=True)
+    assert status == 0, device.decode_status(status)
+    assert worst < 1e-4, worst
+
+
 def test_status_out_of_grid_and_overflow(box):
     P, st0 = box
     pos = st0["pos"].copy()
