@@ -15,7 +15,11 @@
  *          case the reference leaves undefined and got the library's
  *          defined result, 64 with a neighbour-list skin: a particle passed
  *          half the skin inside a block of steps with no list check, so
- *          contacts may have been missed)
+ *          contacts may have been missed, 128 with a skin: 2 r + skin of
+ *          some sphere exceeds a cell edge of the grid the list is searched
+ *          on (only blaze_contact_list_static can raise it: with a skin the
+ *          handle API searches a grid of cells at least 2 r_max + skin over
+ *          the project grid's extent))
  *       <0 -(1000 + cudaError_t) for a CUDA error, -1 bad argument,
  *          -2 no simulation set up
  *   - Device_DEM_UpdateSim only enqueues the step on the library's stream;
@@ -280,14 +284,17 @@ blaze_sim* blaze_default_sim(void);
  *
  * Same broad phase as the step: cell keys from si->worldOrigin, cellSize and
  * num_NNCells, stable sort by cell, and every pair with
- * |xi - xj| - (ri + rj) < skin from the 27 surrounding cells.
+ * |xi - xj| - (ri + rj) < skin from the 27 surrounding cells.  The list
+ * holds every such pair only when each cell edge is at least 2 r_max + skin
+ * (a pair further apart than one cell edge is not searched); a sphere with
+ * 2 r + skin above the smallest edge raises status 128.
  *   pos4    device, n x (x, y, z, radius) floats, every particle live
  *   perm    device, n: sorted slot k holds input particle perm[k]
  *   nn      device, n: neighbour count of sorted particle i (<= max_nbr)
  *   list    device, max_nbr * n, slot-major: list[k * n + i] is the k-th
  *           neighbour of sorted particle i, as a sorted slot
  *   status  device, 1 word (may be NULL): status bits (1 overflow, 2 outside
- *           the grid)
+ *           the grid, 128 cells too small for the skin)
  *   stream  cudaStream_t the work is enqueued on (NULL: default stream)
  * Returns 0 once the work is enqueued, -1 for a bad argument, -3 beyond the
  * size limit, -(1000 + cudaError_t) for a CUDA error.  The first call on

@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("BLAZE_LIB") or os.path.join(os.path.dirname(os.path.a
                                                        "libblaze_b200.so")
 
 STATUS_BITS = {1: "list_overflow", 2: "out_of_grid", 4: "non_finite", 8: "type_range",
-               16: "timeout", 32: "poly_undefined", 64: "stale_list"}
+               16: "timeout", 32: "poly_undefined", 64: "stale_list", 128: "cell_too_small"}
 
 _f = C.POINTER(C.c_float)
 _u = C.POINTER(C.c_uint)

@@ -40,6 +40,8 @@ enum StatusBits : uint32_t {
                               // leaves undefined (see poly_kernels.cu)
   kStatusStaleList = 64u,     // with a skin: a particle passed half the skin
                               // between two list checks (contacts may be missed)
+  kStatusCellTooSmall = 128u, // with a skin: 2 r + skin exceeds a cell edge, so the
+                              // 27-cell search may miss pairs within the skin
 };
 
 // One step of the wall program: planar faces, infinite planes, a macro

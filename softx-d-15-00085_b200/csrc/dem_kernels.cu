@@ -235,6 +235,10 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
   const int3 g = grid_pos(*P, pa);
   uint32_t cnt = 0;
   uint32_t st = 0;
+  // a pair within the skin is at most 2 max(ra, rb) + skin apart: the
+  // larger sphere of every pair checks that this fits in one cell edge
+  if (skin > 0.0f && 2.0f * ra + skin > fminf(P->cell.x, fminf(P->cell.y, P->cell.z)))
+    st |= kStatusCellTooSmall;
   if (in_grid(*P, g)) {
     const int xs = g.x == 0 ? 0 : -1, xe = g.x == P->ncells.x - 1 ? 0 : 1;
     const int ys = g.y == 0 ? 0 : -1, ye = g.y == P->ncells.y - 1 ? 0 : 1;

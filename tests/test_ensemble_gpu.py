@@ -136,7 +136,7 @@ def test_persistent_stepping_equals_plain(boxes, law):
     re-sort); planes, and the triangle-mesh silo with its cylinder."""
     S, W, p, r = boxes
     # velocities that make the boxes re-sort every few tens of steps
-    v = np.random.default_rng(9).normal(scale=40.0, size=p.shape).astype(np.float32)
+    v = np.random.default_rng(9).normal(scale=10.0, size=p.shape).astype(np.float32)
     S2, W2, p2, r2, v2 = mesh_silo()
     for (sy, wa, pos, rad, vel) in ((S, W, p, r, v), (S2, W2, p2, r2, v2)):
         out, rb = [], []

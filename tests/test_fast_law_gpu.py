@@ -72,10 +72,13 @@ def test_fast_law_vs_reference_kernels(name):
 
 def test_fast_law_vs_fp64_settled_silo(tmp_path):
     """20,000 spheres (r in [0.2, 0.4] cm) of the silo workload settled for
-    20,000 steps with the hatch closed: a bed in contact, several contacts
-    per particle with overlaps set by the weight above.  One step's
-    particle-particle forces, contracted and bit-exact, against the FP64
-    restatement of the reference law from that state."""
+    20,000 steps with the hatch closed: a bed in contact, its overlaps set
+    by the weight above.  One step's particle-particle forces, contracted
+    and bit-exact, against the FP64 restatement of the reference law from
+    that state.  Deep in a bed a particle's contact forces are many times
+    its net force and its weight, and each carries its own rounding, so the
+    scale of a particle here is the largest of its net force, its weight
+    and its largest normal contact force (kn times the FP64 overlap)."""
     P, st0 = synth.silo_project(str(tmp_path), n=20000)
     s = device.Simulation(P, skin=0.1, use_graph=1)
     s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
@@ -89,8 +92,18 @@ def test_fast_law_vs_fp64_settled_silo(tmp_path):
     pos = st["pos"].astype(np.float64)
     pairs = np.array(sorted(cKDTree(pos).query_pairs(2.0 * rad.max())))
     dist = np.linalg.norm(pos[pairs[:, 0]] - pos[pairs[:, 1]], axis=1)
-    contacts = int((dist < rad[pairs[:, 0]] + rad[pairs[:, 1]]).sum())
+    touch = dist < rad[pairs[:, 0]] + rad[pairs[:, 1]]
+    contacts = int(touch.sum())
     assert 2 * contacts / len(pos) > 2.0, 2 * contacts / len(pos)
+    # largest normal contact force per particle, in pid order
+    kn = np.array([[P.pobj[a].PP[b].Kn for b in range(P.n_p)] for a in range(P.n_p)], np.float64)
+    tp = st["type"].astype(np.int64)
+    cp = pairs[touch]
+    fc = kn[tp[cp[:, 0]], tp[cp[:, 1]]] * (rad[cp[:, 0]] + rad[cp[:, 1]] - dist[touch])
+    fmax = np.zeros(len(pos))
+    np.maximum.at(fmax, cp[:, 0], fc)
+    np.maximum.at(fmax, cp[:, 1], fc)
+    fmax = fmax[np.argsort(st["pid"])]
     out = {}
     for fast in (0, 1):
         g = device.Simulation(P, capture_forces=1, fast_law=fast)
@@ -105,7 +118,7 @@ def test_fast_law_vs_fp64_settled_silo(tmp_path):
     o.step(1)
     f64 = o.forces()["f_pp"][np.argsort(o.state()["pid"])]
     mass = np.array([P.pobj[t].mass for t in range(P.n_p)], np.float64)
-    weight = mass[st["type"][np.argsort(st["pid"])]] * 981.0
+    weight = np.maximum(mass[st["type"][np.argsort(st["pid"])]] * 981.0, fmax)
     e_exact = rel_err(out[0], f64, weight)
     e_fast = rel_err(out[1], f64, weight)
     e_pair = rel_err(out[1], out[0].astype(np.float64), weight)

@@ -86,8 +86,10 @@ def test_poly_checkpoints_bit_exact(golden_poly):
 
 def test_poly_graph_and_skin_modes(golden_poly):
     """CUDA-graph stepping reproduces plain stepping bit for bit; a Verlet
-    skin on the bounding spheres keeps the first step's forces bit for bit
-    and the trajectory within 1e-5 of the reference mode."""
+    skin on the bounding spheres (searched on cells of 2 r + skin, so the
+    contacts are summed in another order) keeps the first step's forces
+    within 1e-6 of the largest and the trajectory within 1e-5 of the
+    reference mode."""
     g = golden_poly
     plain = gpu_sim(g)
     graph = gpu_sim(g, use_graph=1)
@@ -101,8 +103,11 @@ def test_poly_graph_and_skin_modes(golden_poly):
     ref.step(1)
     skin.step(1)
     fr, fs = ref.forces(), skin.forces()
+    ir, is_ = np.argsort(ref.state()["pid"]), np.argsort(skin.state()["pid"])
     for key in FORCE_KEYS:
-        np.testing.assert_array_equal(fr[key], fs[key], err_msg=key)
+        x, y = fr[key][ir].astype(np.float64), fs[key][is_].astype(np.float64)
+        scale = max(float(np.abs(x).max()), 1e-30)
+        np.testing.assert_allclose(y, x, rtol=0, atol=1e-6 * scale, err_msg=key)
     ref.step(49)
     skin.step(49)
     a, b = ref.state(), skin.state()

@@ -69,7 +69,9 @@ def static_list(f, P, st):
 
 
 def test_static_scratch_matches_handle_api(tmp_path):
-    P, st0 = synth.box_project(str(tmp_path), n_side=(16, 16, 20))  # 5,120 spheres
+    # 5,120 spheres; cells of 2 r + skin, so that every pair within the skin
+    # is searched and the handle API keeps the project's grid
+    P, st0 = synth.box_project(str(tmp_path), n_side=(16, 16, 20), cell=0.32)
     f = static_entry()
     # a second, different state: the packing after 150 steps of settling,
     # stored in that run's (cell-sorted) order
@@ -97,3 +99,13 @@ def test_static_scratch_rejects_sizes_beyond_its_limit(tmp_path):
     si = T.SimulationInfo.from_buffer_copy(bytes(P.sim_info))
     si.num_NNCells = T.int3(100, 100, 100)   # 1,000,000 hash cells > 262,144
     assert f(dummy, 64, C.byref(si), SKIN, CAP, dummy, dummy, dummy, None, None) == -3
+
+
+def test_static_cells_too_small_for_the_skin(tmp_path):
+    """The box's own 0.2 cm cells with a 0.12 cm skin (2 r + skin = 0.32):
+    pairs more than one cell edge apart are not searched, and the call says
+    so with status 128."""
+    P, st0 = synth.box_project(str(tmp_path), n_side=(16, 16, 20))
+    f = static_entry()
+    perm, nn, lst, status = static_list(f, P, st0)
+    assert status & 128, device.decode_status(status)
