@@ -70,6 +70,47 @@ def test_fast_law_vs_reference_kernels(name):
     assert e_v < TOL, e_v
 
 
+def contact_force_scale(P, st):
+    """Per particle (pid order) the largest force of its sphere contacts,
+    normal spring-dashpot or the reference's tangential force
+    tan_pre |v_t| / |v_rel|, in FP64; and the number of contacts."""
+    from scipy.spatial import cKDTree
+    rad = np.array([P.pobj[t].radius for t in range(P.n_p)], np.float64)[st["type"]]
+    pos = st["pos"].astype(np.float64)
+    pairs = np.array(sorted(cKDTree(pos).query_pairs(2.0 * rad.max())))
+    dist = np.linalg.norm(pos[pairs[:, 0]] - pos[pairs[:, 1]], axis=1)
+    touch = dist < rad[pairs[:, 0]] + rad[pairs[:, 1]]
+    contacts = int(touch.sum())
+    # largest contact force per particle (normal spring-dashpot or the
+    # reference's tangential force, tan_pre |v_t| / |v_rel|, in FP64), in pid order
+    pp = [[P.pobj[a].PP[b] for b in range(P.n_p)] for a in range(P.n_p)]
+    tp = st["type"].astype(np.int64)
+    cp = pairs[touch]
+    ta, tb = tp[cp[:, 0]], tp[cp[:, 1]]
+    kn = np.array([pp[a][b].Kn for a, b in zip(ta, tb)])
+    cn = np.array([pp[a][b].Cn for a, b in zip(ta, tb)])
+    muk = np.array([pp[a][b].Fric_kinetic for a, b in zip(ta, tb)])
+    m_all = np.array([P.pobj[t].mass for t in range(P.n_p)], np.float64)
+    dt = float(np.float32(P.sim_info.InitalDelta_t))
+    nrm = (pos[cp[:, 0]] - pos[cp[:, 1]]) / dist[touch][:, None]
+    vel, avel = st["vel"].astype(np.float64), st["avel"].astype(np.float64)
+    rvel = vel[cp[:, 0]] - vel[cp[:, 1]]
+    vcpa = vel[cp[:, 0]] + np.cross(avel[cp[:, 0]], -nrm * rad[cp[:, 0]][:, None])
+    vcpb = vel[cp[:, 1]] + np.cross(avel[cp[:, 1]], nrm * rad[cp[:, 1]][:, None])
+    dv = vcpa - vcpb
+    vt = dv - (dv * nrm).sum(1)[:, None] * nrm
+    vr = np.linalg.norm(rvel, axis=1)
+    tan_pre = 0.5 * (m_all[ta] + m_all[tb]) / dt * 0.05 * muk
+    f_t = tan_pre * np.linalg.norm(vt, axis=1) / np.where(vr > 0, vr, 1.0)
+    f_n = np.abs(kn * (rad[cp[:, 0]] + rad[cp[:, 1]] - dist[touch]) - cn * (rvel * nrm).sum(1))
+    fc = np.maximum(f_n, f_t)
+    fmax = np.zeros(len(pos))
+    np.maximum.at(fmax, cp[:, 0], fc)
+    np.maximum.at(fmax, cp[:, 1], fc)
+    fmax = fmax[np.argsort(st["pid"])]
+    return fmax, contacts
+
+
 def test_fast_law_vs_fp64_settled_silo(tmp_path):
     """20,000 spheres (r in [0.2, 0.4] cm) of the silo workload settled for
     20,000 steps with the hatch closed: a bed in contact, its overlaps set
@@ -78,7 +119,9 @@ def test_fast_law_vs_fp64_settled_silo(tmp_path):
     that state.  Deep in a bed a particle's contact forces are many times
     its net force and its weight, and each carries its own rounding, so the
     scale of a particle here is the largest of its net force, its weight
-    and its largest normal contact force (kn times the FP64 overlap)."""
+    and its largest contact force, normal or tangential (FP64; the
+    reference's tangential force tan_pre |v_t| / |v_rel| is large where a
+    contact spins against a slow relative motion)."""
     P, st0 = synth.silo_project(str(tmp_path), n=20000)
     s = device.Simulation(P, skin=0.1, use_graph=1)
     s.set_state(st0["pos"], st0["vel"], st0["avel"], st0["type"], st0["pid"])
@@ -86,24 +129,8 @@ def test_fast_law_vs_fp64_settled_silo(tmp_path):
     st = s.state()
     s.close()
     assert st["status"] == 0, device.decode_status(st["status"])
-    # contacts per particle
-    from scipy.spatial import cKDTree
-    rad = np.array([P.pobj[t].radius for t in range(P.n_p)], np.float64)[st["type"]]
-    pos = st["pos"].astype(np.float64)
-    pairs = np.array(sorted(cKDTree(pos).query_pairs(2.0 * rad.max())))
-    dist = np.linalg.norm(pos[pairs[:, 0]] - pos[pairs[:, 1]], axis=1)
-    touch = dist < rad[pairs[:, 0]] + rad[pairs[:, 1]]
-    contacts = int(touch.sum())
-    assert 2 * contacts / len(pos) > 2.0, 2 * contacts / len(pos)
-    # largest normal contact force per particle, in pid order
-    kn = np.array([[P.pobj[a].PP[b].Kn for b in range(P.n_p)] for a in range(P.n_p)], np.float64)
-    tp = st["type"].astype(np.int64)
-    cp = pairs[touch]
-    fc = kn[tp[cp[:, 0]], tp[cp[:, 1]]] * (rad[cp[:, 0]] + rad[cp[:, 1]] - dist[touch])
-    fmax = np.zeros(len(pos))
-    np.maximum.at(fmax, cp[:, 0], fc)
-    np.maximum.at(fmax, cp[:, 1], fc)
-    fmax = fmax[np.argsort(st["pid"])]
+    fmax, contacts = contact_force_scale(P, st)
+    assert 2 * contacts / len(st["pos"]) > 2.0, 2 * contacts / len(st["pos"])
     out = {}
     for fast in (0, 1):
         g = device.Simulation(P, capture_forces=1, fast_law=fast)
@@ -124,5 +151,5 @@ def test_fast_law_vs_fp64_settled_silo(tmp_path):
     e_pair = rel_err(out[1], out[0].astype(np.float64), weight)
     print("settled silo, 20,000 spheres, %.1f contacts per particle: vs FP64 bit-exact %.2e "
           "contracted %.2e; contracted vs bit-exact %.2e"
-          % (2 * contacts / len(pos), e_exact, e_fast, e_pair))
+          % (2 * contacts / len(st["pos"]), e_exact, e_fast, e_pair))
     assert e_pair < TOL, e_pair
