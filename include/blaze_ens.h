@@ -29,7 +29,17 @@ extern "C" {
 
 typedef struct blaze_ens blaze_ens;
 
-enum { BLAZE_LAW_LINEAR = 1, BLAZE_LAW_HERTZ_MINDLIN = 2 };
+/* BLAZE_LAW_REFERENCE: the reference's own sphere law and step
+ * (Collision_Response.cuh:374-494 and 4-109, Integration.cuh:6-184): linear
+ * spring-dashpot without history, the tangential force
+ * mu_k (m_a + m_b) / (40 dt) |v_t| / |v_rel| against v_t, plane walls as the
+ * reference's faces, its contact test and penetration (+1e-5 cm), with the
+ * parameters its parser derives for a particle object (KSimulationData.cpp:
+ * 955-1047, 1096) formed per particle from the radius: kn, the damping from
+ * the restitution and the (reduced) mass, mu (pairs, kinetic), mu_wall
+ * (walls, static), mu_roll as the reference's rolling resistance (RollRes).
+ * Plane walls only; kt_ratio, youngs and poisson are not read. */
+enum { BLAZE_LAW_LINEAR = 1, BLAZE_LAW_HERTZ_MINDLIN = 2, BLAZE_LAW_REFERENCE = 3 };
 enum { BLAZE_WALL_PLANE = 0, BLAZE_WALL_TRIANGLE = 1, BLAZE_WALL_CYLINDER = 2 };
 
 typedef struct blaze_wall {
@@ -61,7 +71,7 @@ typedef struct blaze_system {
 } blaze_system;
 
 typedef struct blaze_ens_options {
-  int law;             /* BLAZE_LAW_LINEAR or BLAZE_LAW_HERTZ_MINDLIN */
+  int law;             /* BLAZE_LAW_LINEAR, BLAZE_LAW_HERTZ_MINDLIN or BLAZE_LAW_REFERENCE */
   float dt;            /* s */
   float skin;          /* Verlet skin, cm, > 0 */
   int max_nbr;         /* neighbour / history slots per particle, 1..32 */

@@ -13,6 +13,7 @@ from .device import _check, _ptr, load as _load_lib
 
 LAW_LINEAR = 1
 LAW_HERTZ_MINDLIN = 2
+LAW_REFERENCE = 3
 WALL_PLANE = 0
 WALL_TRIANGLE = 1
 WALL_CYLINDER = 2

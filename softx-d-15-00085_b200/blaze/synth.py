@@ -722,6 +722,45 @@ def box_ensemble(counts, *, r_min=0.1, r_max=0.2, solid_fraction=0.55, height_fa
     return systems, walls, np.concatenate(pos), np.concatenate(rad)
 
 
+def box_system_project(root, name, system, L, H, radii, rho, dt=1e-5):
+    """The reference project of one box system of an ensemble: the box
+    [0, L]^2 x [0, H] as six quads, one particle object per distinct radius
+    in `radii` (diameter 2 r, density rho kg/m^3, the system's kn,
+    restitution and friction for pairs, surfaces and lifters), the system's
+    grid and gravity, rotation on.  With BLAZE_LAW_REFERENCE the ensemble
+    steps the same system with the same laws.  Returns (Project, types),
+    types[k] the particle object of radius radii[k]."""
+    base = os.path.join(root, name)
+    for sub in ("SurfaceObjects", "ParticleObjects"):
+        os.makedirs(os.path.join(base, sub), exist_ok=True)
+    L, H = float(L), float(H)
+    verts = [(0, 0, 0), (L, 0, 0), (L, L, 0), (0, L, 0), (0, 0, H), (L, 0, H), (L, L, H), (0, L, H)]
+    faces = [(0, 1, 2, 3), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (3, 7, 4, 0), (4, 7, 6, 5)]
+    faces = _orient(verts, faces, lambda c: (0.5 * L, 0.5 * L, 0.5 * H))
+    _write_wobj(os.path.join(base, "SurfaceObjects", "Box.WOBJ"), "Box", verts, faces)
+    rs = np.asarray(radii, np.float32)
+    bins = np.unique(rs)
+    types = np.searchsorted(bins, rs).astype(np.uint32)
+    pobjs = []
+    f32 = lambda v: float(np.float32(v))  # noqa: E731  (the ensemble's float values)
+    for b, r in enumerate(bins):
+        nm = "Ball%d" % b
+        with open(os.path.join(base, "ParticleObjects", nm + ".POBJ"), "w") as fh:
+            fh.write(_POBJ.format(title=nm, diam=2.0 * float(r), rho=float(rho),
+                                  cor=f32(system.restitution), kn=f32(system.kn),
+                                  mu=f32(system.mu)))
+        pobjs.append(nm)
+    counts = [int(c) for c in np.bincount(types, minlength=len(bins))]
+    cell = f32(system.cell)
+    origin = tuple(f32(system.origin[k]) for k in range(3))
+    world = tuple(float(np.float32(origin[k] + system.ncells[k] * cell)) for k in range(3))
+    _write_project(root, name, "Box", title=name, sim_type=0, dt=dt, wobjs=["Box"], pobjs=pobjs,
+                   counts=counts, n=len(rs), g=tuple(f32(system.gravity[k]) for k in range(3)),
+                   rotation=1, roll_res=f32(system.mu_roll), origin=origin, world=world,
+                   cell=cell, state="none")
+    return Project.load(root, name, "Box"), types
+
+
 def cone_hopper_triangles(silo_r, r_out, y_top, y_out, n_seg=64, n_ring=32, centre=None):
     """A cone (axis +y) from radius r_out at y_out to silo_r at y_top as
     n_seg x n_ring quads, each split into two triangles (2 n_seg n_ring

@@ -391,24 +391,6 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 // candidate slots tested per batch of independent loads in the contact pass
 constexpr int kMaskBatch = 8;
 
-// The reference's contact test |xa - xb| - (ra + rb) < 0
-// (Collision_Detection_BroadPhase.cuh:376, len3 then a subtraction), decided
-// without the square root wherever that is exact.  With d2 formed as len3
-// forms it, the test is RN(sqrt(d2)) < sr (the difference of two distinct
-// floats never rounds to zero).  With s2 = RN(sr^2): d2 < RN(s2 (1 - 2^-20))
-// implies sqrt(d2) < sr (1 - 2^-22), so RN(sqrt(d2)) < sr; d2 > RN(s2 (1 +
-// 2^-20)) implies sqrt(d2) > sr (1 + 2^-23), so RN(sqrt(d2)) > sr (each
-// rounding moves a value by at most 2^-24 of itself while s2 is normal).
-// In between, and for NaN or tiny radii, the IEEE square root decides.
-__device__ __forceinline__ bool touches(float3 rel, float sr) {
-  const float d2 = dot3(rel, rel);
-  const float s2 = sr * sr;
-  if (s2 >= 1e-30f) {
-    if (d2 < s2 * (1.0f - 0x1p-20f)) return true;
-    if (d2 > s2 * (1.0f + 0x1p-20f)) return false;
-  }
-  return sqrtf(d2) - sr < 0.0f;
-}
 
 // kEnergy: also the energy tallies of the step's contacts, per particle in
 // contact order (particle-particle, volume objects, world objects), into

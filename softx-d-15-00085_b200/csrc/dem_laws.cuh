@@ -12,6 +12,26 @@ namespace blaze {
 
 struct Forces { float3 trans, torque; };
 
+// The reference's contact test |xa - xb| - (ra + rb) < 0
+// (Collision_Detection_BroadPhase.cuh:376, len3 then a subtraction), decided
+// without the square root wherever that is exact.  With d2 formed as len3
+// forms it, the test is RN(sqrt(d2)) < sr (the difference of two distinct
+// floats never rounds to zero).  With s2 = RN(sr^2): d2 < RN(s2 (1 - 2^-20))
+// implies sqrt(d2) < sr (1 - 2^-22), so RN(sqrt(d2)) < sr; d2 > RN(s2 (1 +
+// 2^-20)) implies sqrt(d2) > sr (1 + 2^-23), so RN(sqrt(d2)) > sr (each
+// rounding moves a value by at most 2^-24 of itself while s2 is normal).
+// In between, and for NaN or tiny radii, the IEEE square root decides.
+__device__ __forceinline__ bool touches(float3 rel, float sr) {
+  const float d2 = dot3(rel, rel);
+  const float s2 = sr * sr;
+  if (s2 >= 1e-30f) {
+    if (d2 < s2 * (1.0f - 0x1p-20f)) return true;
+    if (d2 > s2 * (1.0f + 0x1p-20f)) return false;
+  }
+  return sqrtf(d2) - sr < 0.0f;
+}
+
+
 // Energy tallies (SimulationInfo::EnergyCalc): a law given `e` stores there
 // the value the reference adds to its tally for this contact (normal
 // dissipation |Fdiss| |Vn| dt, unless the force was attractive, plus the

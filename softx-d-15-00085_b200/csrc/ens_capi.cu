@@ -122,6 +122,22 @@ EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off) {
   d.mu_r = s.mu_roll;
   d.wall0 = s.wall0;
   d.nwall = s.nwalls;
+  // reference law: Set_SpringConstantsParticleKN / Set_SpringConstantsSurface_KN
+  // (KSimulationData.cpp:955-1047): the restitution less 0.03808 inside
+  // [0.3, 0.9], Cn = -2 ln(e) sqrt(Kn m) / sqrt(ln(e)^2 + pi^2), none at e = 1
+  {
+    const double rpi = 2.0 * std::asin(1.0);
+    double cor = (double)s.restitution;
+    if (cor < 1.0) {
+      if (cor >= 0.30 && cor <= 0.90) cor -= 0.038080;
+      d.ref_a = -2.0 * std::log(cor);
+      d.ref_b = std::sqrt(std::log(cor) * std::log(cor) + rpi * rpi);
+    } else {
+      d.ref_a = 0.0;
+      d.ref_b = 0.0;
+    }
+    d.ref_m = ((4.0 / 3.0) * rpi) * (double)s.density;
+  }
   return d;
 }
 
@@ -467,7 +483,8 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   blaze_ens_options o;
   if (opt) o = *opt;
   else blaze_ens_default_options(&o);
-  if ((o.law != BLAZE_LAW_LINEAR && o.law != BLAZE_LAW_HERTZ_MINDLIN) || !(o.dt > 0.0f) ||
+  if ((o.law != BLAZE_LAW_LINEAR && o.law != BLAZE_LAW_HERTZ_MINDLIN &&
+       o.law != BLAZE_LAW_REFERENCE) || !(o.dt > 0.0f) ||
       !(o.skin > 0.0f) || o.max_nbr < 1 || o.max_nbr > 32)
     return -1;
   if (o.block == 0) o.block = 256;
@@ -482,8 +499,12 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   for (int w = 0; w < nwalls; ++w)
     if (walls[w].kind < BLAZE_WALL_PLANE || walls[w].kind > BLAZE_WALL_CYLINDER) return -1;
   for (int s = 0; s < nsys; ++s) {
-    for (int w = systems[s].wall0; w < systems[s].wall0 + systems[s].nwalls; ++w)
+    // the reference law meets plane walls only
+    if (o.law == BLAZE_LAW_REFERENCE && systems[s].ntris > 0) return -1;
+    for (int w = systems[s].wall0; w < systems[s].wall0 + systems[s].nwalls; ++w) {
       if (walls[w].kind == BLAZE_WALL_TRIANGLE) return -1;
+      if (o.law == BLAZE_LAW_REFERENCE && walls[w].kind != BLAZE_WALL_PLANE) return -1;
+    }
     for (int w = systems[s].tri0; w < systems[s].tri0 + systems[s].ntris; ++w)
       if (walls[w].kind != BLAZE_WALL_TRIANGLE) return -1;
   }

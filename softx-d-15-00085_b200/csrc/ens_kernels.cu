@@ -23,6 +23,7 @@
 //   capped force).  Rolling friction: a torque -mu_r max(f_n, 0) R* w_rel / |w_rel|.
 //   Walls use the same law with R* = r, m* = m.
 #include "ens_kernels.cuh"
+#include "dem_laws.cuh"
 
 #include <algorithm>
 
@@ -356,6 +357,123 @@ __device__ __forceinline__ float4 ld_state(const float4* p) {
   else return *p;
 }
 
+// ----------------------------------------------------- reference law (3)
+// The reference's sphere step, per particle, with the parameters its
+// parser derives for a particle object formed here from the particle's own
+// radius and the system's constants:
+//   mass     m = (4/3 pi density) r^3 in double, rounded once
+//            (KSimulationData.cpp:1096); 1/I = 1 / (0.4 r r m) in float
+//            (main.cpp:622-626)
+//   pairs    Kn = kn, Cn = (ref_a sqrt(Kn m*)) / ref_b in double with
+//            m* = 1 / (1/ma + 1/mb) (KSimulationData.cpp:955-1016), kinetic
+//            friction mu
+//   planes   Kn = kn, Cn the same with m* = m (KSimulationData.cpp:1019-1047),
+//            static friction mu_wall
+// The contact test and penetration (|d| - (ra + rb), plus 1e-5), the laws
+// (Collision_Response.cuh:374-494 and 4-109) and the integration
+// (Integrate_Euler_NonSymmetry, Integration.cuh:6-184, rolling resistance
+// mu_roll) are the sphere path's own functions; a plane is tested as the
+// reference tests a face (Collision_Detection_Spheres.cuh:6-100) against
+// its point d n.  The law keeps no history.
+__device__ __forceinline__ float ref_mass(const EnsSysDev& S, float r) {
+  const double r3 = ((double)r * (double)r) * (double)r;
+  return (float)(S.ref_m * r3);
+}
+
+__device__ __forceinline__ float ref_damping(const EnsSysDev& S, double m) {
+  return S.ref_b > 0.0 ? (float)((S.ref_a * sqrt((double)S.kn * m)) / S.ref_b) : 0.0f;
+}
+
+template <bool kCapture, bool kNc>
+__device__ __forceinline__ float ens_particle_step_ref(const EnsGeom& g, const EnsBufs& b,
+                                                       const StateBuf& in, const StateBuf& out,
+                                                       int i, const EnsList& L,
+                                                       const EnsCapture& cap, uint32_t& st) {
+  const size_t stride = (size_t)b.stride;
+  const float dt = g.dt;
+  const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
+  const float3 pa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
+  const float ra = pa4.w;
+  const uint32_t sys = __float_as_uint(va4.w) & kSysMask;
+  const EnsSysDev& S = g.sys[sys];
+  const float ma = ref_mass(S, ra);
+  SimParams P;   // the two fields the reference's laws read
+  P.dt = dt;
+  P.rotation = 1;
+
+  // particle-particle (Kernel_ParticleInteraction_Spheres_NonSymmetry)
+  float3 f = S.gravity * ma;
+  float3 tl = f3(0.0f, 0.0f, 0.0f);
+  const uint32_t cnt = L.cnt[i];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t j = L.idx[(size_t)k * stride + i];
+    const float4 pb4 = ld_state<kNc>(in.pos + j);
+    const float3 rel = pa - xyz(pb4);
+    const float rb = pb4.w;
+    if (!touches(rel, ra + rb)) continue;
+    const float dist = len3(rel);
+    const float dis = fabsf(dist - (ra + rb)) + 0.000010f;
+    const float3 nrm = div3_rn(rel, dist);
+    const float4 vb4 = ld_state<kNc>(in.vel + j), wb4 = ld_state<kNc>(in.angv + j);
+    const float mb = ref_mass(S, rb);
+    PP_Parms pp;
+    pp.Kn = S.kn;
+    pp.Cn = ref_damping(S, 1.0 / ((1.0 / (double)ma) + (1.0 / (double)mb)));
+    pp.Fric_static = S.mu;
+    pp.Fric_kinetic = S.mu;
+    const Forces F = law_pp<true>(P, va - xyz(vb4), nrm, dis, (-1.0f * nrm) * ra, nrm * rb, wa,
+                                  xyz(wb4), pp, va, xyz(vb4), ma, mb);
+    f = f + F.trans;
+    tl = tl + F.torque;
+  }
+
+  // plane walls (WorldObject_InteractionParticle, face and plane contacts)
+  float3 fw = f3(0.0f, 0.0f, 0.0f), tw = f3(0.0f, 0.0f, 0.0f);
+  TypeParams T;
+  T.mass = ma;
+  T.s_kn = S.kn;
+  T.s_cn = ref_damping(S, (double)ma);
+  T.s_mus = S.mu_w;
+  for (int w = S.wall0; w < S.wall0 + S.nwall; ++w) {
+    const EnsWallDev& W = g.walls[w];
+    const float3 n = W.a;
+    const float3 c = n * W.r;
+    const float3 pt = pa - ra * n;
+    float dis = dot3(n, pt - c);
+    if (!(dis < 0.000000f && dis > -ra)) continue;
+    dis = fabsf(dis);
+    const Forces F = law_static_surface(P, va, n, dis, pt - pa, wa, T);
+    fw = fw + F.trans;
+    tw = tw + F.torque;
+  }
+
+  // Integrate_Euler_NonSymmetry (Integration.cuh:6-184), spheres
+  float3 acc = fw + f;
+  acc = acc * (1.0f / ma);
+  const float3 v = va + acc * dt;
+  const float3 p = pa + v * dt;
+  const float3 tq = tl + tw;
+  float3 w = wa;
+  if (dot3(tq, tq) > 0.0f) {
+    const float iinv = 1.0f / (((0.4f * ra) * ra) * ma);
+    const float3 aa = iinv * tq;
+    w = w + aa * dt;
+    w = w - w * S.mu_r;
+  }
+  const float path = wa4.w + len3(v) * dt;
+  out.pos[i] = make_float4(p.x, p.y, p.z, ra);
+  out.vel[i] = make_float4(v.x, v.y, v.z, __uint_as_float(sys));
+  out.angv[i] = make_float4(w.x, w.y, w.z, path);
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st |= kStatusNonFinite;
+  if (kCapture) {
+    const float3 fc = (f - S.gravity * ma) + fw;
+    cap.f[i] = make_float4(fc.x, fc.y, fc.z, 0.0f);
+    cap.t[i] = make_float4(tq.x, tq.y, tq.z, 0.0f);
+  }
+  return path;
+}
+
+
 // The step of particle i: its contacts in list order (tangential histories
 // updated in place, the particle's own slots only), its walls, symplectic
 // Euler from `in` into `out`.  Raises status bits in st; returns the path
@@ -367,6 +485,9 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
                                                    int i, int e, const EnsList& L, TapeView tv,
                                                    float* hrec, const EnsCapture& cap,
                                                    uint32_t& st) {
+  if constexpr (kLaw == kLawReference) {
+    return ens_particle_step_ref<kCapture, kNc>(g, b, in, out, i, L, cap, st);
+  } else {
   const size_t stride = (size_t)b.stride;
   const float dt = g.dt;
   const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
@@ -555,6 +676,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     cap.t[i] = make_float4(t.x, t.y, t.z, 0.0f);
   }
   return path;
+  }
 }
 
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
@@ -803,7 +925,10 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
       else ENS_STEP(kLawLinear, false, true);
     }
   } else {
-    if (g.law == kLawHertz) {
+    if (g.law == kLawReference) {   // plane walls only
+      if (cap) ENS_STEP(kLawReference, true, false);
+      else ENS_STEP(kLawReference, false, false);
+    } else if (g.law == kLawHertz) {
       if (cap) ENS_STEP(kLawHertz, true, false);
       else ENS_STEP(kLawHertz, false, false);
     } else {
@@ -829,7 +954,9 @@ int ens_persist_grid(const EnsGeom& g, int block, int n) {
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
   cudaError_t err;
-  if (g.curved)
+  if (g.law == kLawReference)
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawReference, false>, block, 0);
+  else if (g.curved)
     err = g.law == kLawHertz
               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawHertz, true>, block, 0)
               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_persist<kLawLinear, true>, block, 0);
@@ -855,6 +982,8 @@ cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int
   cfg.attrs = attr;
   cfg.numAttrs = coop ? 1 : 0;
   const StateBuf sh = b.S[home], so = b.S[home ^ 1], ss = b.S[2];
+  if (g.law == kLawReference)
+    return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawReference, false>, g, b, sh, so, ss, n, ctl, rebuilt, p);
   if (g.curved) {
     if (g.law == kLawHertz)
       return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawHertz, true>, g, b, sh, so, ss, n, ctl, rebuilt, p);

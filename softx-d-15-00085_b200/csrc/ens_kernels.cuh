@@ -32,7 +32,7 @@ constexpr int kWallSlots = 4;
 constexpr uint32_t kSysBits = 24;
 constexpr uint32_t kSysMask = (1u << kSysBits) - 1u;
 
-enum EnsLaw : int { kLawLinear = 1, kLawHertz = 2 };
+enum EnsLaw : int { kLawLinear = 1, kLawHertz = 2, kLawReference = 3 };
 enum EnsWallKind : int { kWallPlane = 0, kWallTriangle = 1, kWallCylinder = 2 };
 
 struct EnsSysDev {
@@ -48,6 +48,12 @@ struct EnsSysDev {
   float beta2h;        // Hertz-Mindlin: 2 sqrt(5/6) beta
   float mu, mu_w, mu_r;
   int wall0, nwall;    // planes and cylinders, tested for every particle
+  // reference law: the damping coefficient of a contact with (reduced) mass
+  // m is (ref_a sqrt(kn m)) / ref_b in double, rounded to float, as the
+  // reference's parser forms it (KSimulationData.cpp:955-1047); ref_b = 0:
+  // no damping (restitution 1)
+  double ref_a, ref_b;
+  double ref_m;        // (4/3) pi density: m = ref_m r^3 in double, rounded once
 };
 
 struct EnsWallDev {
