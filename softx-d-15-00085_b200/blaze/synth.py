@@ -727,7 +727,8 @@ def box_system_project(root, name, system, L, H, radii, rho, dt=1e-5):
     [0, L]^2 x [0, H] as six quads, one particle object per distinct radius
     in `radii` (diameter 2 r, density rho kg/m^3, the system's kn,
     restitution and friction for pairs, surfaces and lifters), the system's
-    grid and gravity, rotation on.  With BLAZE_LAW_REFERENCE the ensemble
+    cell size and gravity (as many cells on every axis as the longest one
+    needs), rotation on.  With BLAZE_LAW_REFERENCE the ensemble
     steps the same system with the same laws.  Returns (Project, types),
     types[k] the particle object of radius radii[k]."""
     base = os.path.join(root, name)
@@ -753,7 +754,11 @@ def box_system_project(root, name, system, L, H, radii, rho, dt=1e-5):
     counts = [int(c) for c in np.bincount(types, minlength=len(bins))]
     cell = f32(system.cell)
     origin = tuple(f32(system.origin[k]) for k in range(3))
-    world = tuple(float(np.float32(origin[k] + system.ncells[k] * cell)) for k in range(3))
+    # the same cell count on every axis: the reference's hash
+    # x + z nz + y nx nz (BroadPhase.cuh:42-50) indexes past its cell table
+    # when nx < nz, and the grid only has to cover the box
+    nc = max(int(system.ncells[k]) for k in range(3))
+    world = tuple(float(np.float32(origin[k] + nc * cell)) for k in range(3))
     _write_project(root, name, "Box", title=name, sim_type=0, dt=dt, wobjs=["Box"], pobjs=pobjs,
                    counts=counts, n=len(rs), g=tuple(f32(system.gravity[k]) for k in range(3)),
                    rotation=1, roll_res=f32(system.mu_roll), origin=origin, world=world,
