@@ -216,8 +216,9 @@ k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
 // Kernel_BroadCollisionDetection_NonSymmetry (BroadPhase.cuh:402-513) with
 // CollisionDetection_Filter_SphereNNCell (BroadPhase.cuh:335-392): the
 // clamped 3x3x3 block scanned in y, z, x order, j ascending inside a cell,
-// pairs kept when |xi - xj| - (ri + rj) < skin (skin 0: the reference's
-// contacts-only list).  Slots beyond the capacity are dropped and flagged
+// pairs kept when |xi - xj| - (ri + rj) < 0 (skin 0: the reference's
+// contacts-only list, bit for bit), or with a skin every pair with
+// |xi - xj| < ri + rj + skin (up to a relative 2^-20 more).  Slots beyond the capacity are dropped and flagged
 // (the reference writes past its 32-slot row).
 __global__ void __launch_bounds__(kThreads)
 k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_max,
@@ -253,8 +254,19 @@ k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_m
           for (uint32_t j = s; j < e; ++j) {
             if ((int)j == i) continue;
             const float4 pb = __ldg(pos + j);
-            const float sep = len3(pa - xyz(pb)) - (ra + pb.w);
-            if (sep < skin) {
+            const float3 rel = pa - xyz(pb);
+            const float sr = ra + pb.w;
+            // skin 0: the reference's test, decided without the square root
+            // where that is exact (touches); with a skin the list need only
+            // hold every pair within it, so a bound a hair wider serves
+            bool keep;
+            if (skin > 0.0f) {
+              const float reach = sr + skin;
+              keep = dot3(rel, rel) < (reach * reach) * (1.0f + 0x1p-20f);
+            } else {
+              keep = touches(rel, sr);
+            }
+            if (keep) {
               if (cnt < (uint32_t)nl.cap) nl.idx[(size_t)cnt * nl.stride + i] = j;
               else st |= kStatusListOverflow;
               ++cnt;
