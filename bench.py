@@ -152,16 +152,17 @@ def case_adjoint(nsys=64, steps=60, segment=30, tape_bytes=0):
 
 def case_silo_settled(n=1_000_000, settle=48000, steps=8, fast=1, skin_um=1600):
     """The headline silo workload from its settled bed: n spheres settled
-    `settle` steps with the hatch closed (cached under /tmp on the first run:
-    the same command line run again loads the cache, so a profiler sees only
-    `steps` plain steps of the discharge), hatch open, contracted law when
-    `fast`, skin skin_um / 1e4 cm."""
+    `settle` steps with the hatch closed and the headline's 0.16 cm skin
+    (cached under /tmp on the first run: the same command line run again
+    loads the cache, so a profiler sees only `steps` plain steps of the
+    discharge), hatch open, contracted law when `fast`, then skin
+    skin_um / 1e4 cm (0: the reference mode, a re-sort every step)."""
     from blaze import device, synth
     skin = skin_um * 1e-4
     cache = os.path.join(tempfile.gettempdir(), "blaze_silo_settled_%d_%d.npz" % (n, settle))
     with tempfile.TemporaryDirectory() as d:
         P, st0 = synth.silo_project(d, n=n)
-    sim = device.Simulation(P, skin=skin, max_nbr=32, use_graph=1)
+    sim = device.Simulation(P, skin=0.16, max_nbr=32, use_graph=1)
     if os.path.isfile(cache):
         z = np.load(cache)
         sim.set_state(z["pos"], z["vel"], z["avel"], z["type"], z["pid"])
