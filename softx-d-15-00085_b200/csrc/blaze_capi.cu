@@ -545,7 +545,7 @@ int enqueue_rebuild(blaze_sim* s, const int* gate, cudaStream_t st) {
   CK(cudaMemsetAsync(s->cstart, 0xff, cbytes, st));
   launch_reorder(s->S[s->cur], s->S[2], s->ob, n, s->rs.keys[res], s->rs.vals[res], s->cstart,
                  s->cend, s->hp.ncell_tab, s->n_d > 0, s->nl.flat_n, s->ctl, gate, st);
-  launch_nlist(s->dp, s->S[2], n, s->hp.ncell_tab, s->cstart, s->cend, s->nl, s->ctl, gate, st);
+  launch_nlist(s->dp, s->S[2], n, s->cstart, s->cend, s->nl, s->ctl, gate, st);
   s->last_launches += 3 + 3 * std::max(1, (s->key_bits + kRadixBits - 1) / kRadixBits);
   return 0;
 }

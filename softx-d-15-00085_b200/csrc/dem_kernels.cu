@@ -214,47 +214,59 @@ k_reorder(StateBuf src, StateBuf dst, OrderBuf ob, int n_max,
 
 // -------------------------------------------------------------------- nlist
 // Kernel_BroadCollisionDetection_NonSymmetry (BroadPhase.cuh:402-513) with
-// CollisionDetection_Filter_SphereNNCell (BroadPhase.cuh:335-392): for
-// particle i the clamped 3x3x3 block of cells around its own, scanned in
-// y, z, x order, j ascending inside a cell; pairs kept when
-// |xi - xj| - (ri + rj) < 0 (skin 0: the reference's contacts-only list,
-// bit for bit, decided without the square root where that is exact), or
-// with a skin every pair with |xi - xj| < ri + rj + skin (up to a relative
-// 2^-20 more).  Slots beyond the capacity are dropped and flagged (the
-// reference writes past its 32-slot row).
-__device__ __forceinline__ bool pair_kept(float3 pa, float ra, float4 pb, float skin) {
-  const float3 rel = pa - xyz(pb);
-  const float sr = ra + pb.w;
-  if (skin > 0.0f) {
-    const float reach = sr + skin;
-    return dot3(rel, rel) < (reach * reach) * (1.0f + 0x1p-20f);
-  }
-  return touches(rel, sr);
-}
-
-// Particle i scans its own 27 cells (the reference's structure).
-__device__ __forceinline__ uint32_t nlist_particle(const SimParams& P, const float4* pos,
-                                                   const uint32_t* cstart, const uint32_t* cend,
-                                                   const NbrList& nl, int i, uint32_t& st) {
+// CollisionDetection_Filter_SphereNNCell (BroadPhase.cuh:335-392): the
+// clamped 3x3x3 block scanned in y, z, x order, j ascending inside a cell,
+// pairs kept when |xi - xj| - (ri + rj) < 0 (skin 0: the reference's
+// contacts-only list, bit for bit), or with a skin every pair with
+// |xi - xj| < ri + rj + skin (up to a relative 2^-20 more).  Slots beyond the capacity are dropped and flagged
+// (the reference writes past its 32-slot row).
+__global__ void __launch_bounds__(kThreads)
+k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos, int n_max,
+        const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, NbrList nl,
+        StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ctl->epoch += 1;
+  const int n = ctl->n_cur;
+  if (i >= n) return;
   const float4 pa4 = pos[i];
   const float3 pa = xyz(pa4);
   const float ra = pa4.w;
-  const int3 g = grid_pos(P, pa);
+  const float skin = P->skin;
+  const int3 g = grid_pos(*P, pa);
   uint32_t cnt = 0;
-  if (in_grid(P, g)) {
-    const int xs = g.x == 0 ? 0 : -1, xe = g.x == P.ncells.x - 1 ? 0 : 1;
-    const int ys = g.y == 0 ? 0 : -1, ye = g.y == P.ncells.y - 1 ? 0 : 1;
-    const int zs = g.z == 0 ? 0 : -1, ze = g.z == P.ncells.z - 1 ? 0 : 1;
+  uint32_t st = 0;
+  // a pair within the skin is at most 2 max(ra, rb) + skin apart: the
+  // larger sphere of every pair checks that this fits in one cell edge
+  if (skin > 0.0f && 2.0f * ra + skin > fminf(P->cell.x, fminf(P->cell.y, P->cell.z)))
+    st |= kStatusCellTooSmall;
+  if (in_grid(*P, g)) {
+    const int xs = g.x == 0 ? 0 : -1, xe = g.x == P->ncells.x - 1 ? 0 : 1;
+    const int ys = g.y == 0 ? 0 : -1, ye = g.y == P->ncells.y - 1 ? 0 : 1;
+    const int zs = g.z == 0 ? 0 : -1, ze = g.z == P->ncells.z - 1 ? 0 : 1;
     for (int y = ys; y <= ye; ++y)
       for (int z = zs; z <= ze; ++z)
         for (int x = xs; x <= xe; ++x) {
-          const uint32_t h = grid_hash(P, make_int3(g.x + x, g.y + y, g.z + z));
+          const uint32_t h = grid_hash(*P, make_int3(g.x + x, g.y + y, g.z + z));
           const uint32_t s = __ldg(cstart + h);
           if (s == 0xffffffffu) continue;
           const uint32_t e = __ldg(cend + h);
           for (uint32_t j = s; j < e; ++j) {
             if ((int)j == i) continue;
-            if (pair_kept(pa, ra, __ldg(pos + j), P.skin)) {
+            const float4 pb = __ldg(pos + j);
+            const float3 rel = pa - xyz(pb);
+            const float sr = ra + pb.w;
+            // skin 0: the reference's test, decided without the square root
+            // where that is exact (touches); with a skin the list need only
+            // hold every pair within it, so a bound a hair wider serves
+            bool keep;
+            if (skin > 0.0f) {
+              const float reach = sr + skin;
+              keep = dot3(rel, rel) < (reach * reach) * (1.0f + 0x1p-20f);
+            } else {
+              keep = touches(rel, sr);
+            }
+            if (keep) {
               if (cnt < (uint32_t)nl.cap) nl.idx[(size_t)cnt * nl.stride + i] = j;
               else st |= kStatusListOverflow;
               ++cnt;
@@ -262,136 +274,23 @@ __device__ __forceinline__ uint32_t nlist_particle(const SimParams& P, const flo
           }
         }
   }
-  return cnt < (uint32_t)nl.cap ? cnt : (uint32_t)nl.cap;
-}
-
-// One warp per cell-table bucket.  The particles of a bucket share their 27
-// cells, so the warp enumerates the candidates once, in the reference's
-// order, 32 at a time (lane l takes candidate base + l, found among the
-// cells by a binary search over the cells' offsets held one per lane), and
-// tests each against every particle of the bucket in turn; a ballot orders
-// the kept candidates, so particle i's slots come out in the same order as
-// its own scan would give them.  A bucket whose particles lie in different
-// cells (the hash aliases when nx != nz) falls back to a lane per particle.
-// The pass before the buckets empties the lists of particles outside the
-// grid (they own no bucket).
-__global__ void __launch_bounds__(kThreads)
-k_nlist(const SimParams* __restrict__ P, const float4* __restrict__ pos,
-        const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, NbrList nl,
-        StepCtl* ctl, const int* gate) {
-  if (gate && *gate == 0) return;
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid == 0) ctl->epoch += 1;
-  const int n = ctl->n_cur;
-  const float skin = P->skin;
-  const float cmin = fminf(P->cell.x, fminf(P->cell.y, P->cell.z));
-  uint32_t st = 0;
-  for (size_t i = gid; i < (size_t)n; i += (size_t)gridDim.x * blockDim.x) {
-    const float4 p4 = pos[i];
-    if (!in_grid(*P, grid_pos(*P, xyz(p4)))) nl.cnt[i] = 0u;
-    // a pair within the skin is at most 2 max(ra, rb) + skin apart: the
-    // larger sphere of every pair checks that this fits in one cell edge
-    if (skin > 0.0f && 2.0f * p4.w + skin > cmin) st |= kStatusCellTooSmall;
-  }
-  const uint32_t h = (uint32_t)(gid >> 5);
-  const uint32_t s0 = h < P->ncell_tab ? __ldg(cstart + h) : 0xffffffffu;
-  if (s0 != 0xffffffffu) {
-    const uint32_t e0 = __ldg(cend + h);
-    const uint32_t cap = (uint32_t)nl.cap;
-    const size_t stride = (size_t)nl.stride;
-    const int3 g = grid_pos(*P, xyz(__ldg(pos + s0)));
-    bool same = true;
-    for (uint32_t k = s0 + lane; k < e0; k += 32) {
-      const int3 gk = grid_pos(*P, xyz(__ldg(pos + k)));
-      same = same && gk.x == g.x && gk.y == g.y && gk.z == g.z;
+  const uint32_t kept = cnt < (uint32_t)nl.cap ? cnt : (uint32_t)nl.cap;
+  nl.cnt[i] = kept;
+  if (nl.flat) {
+    // append this particle's slots to the flat list: one atomic per warp;
+    // the lanes still here (i < n) are a prefix of the warp
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31;
+    uint32_t x = kept;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(m, x, d);
+      if (lane >= d) x += y;
     }
-    same = __all_sync(full, same);
-    for (uint32_t g0 = s0; g0 < e0; g0 += 32) {
-      const uint32_t ng = min(32u, e0 - g0);
-      uint32_t kept = 0;   // lane l: the list length of particle g0 + l
-      if (!same) {
-        const int i = (int)(g0 + lane);
-        if ((uint32_t)lane < ng && i < n) kept = nlist_particle(*P, pos, cstart, cend, nl, i, st);
-      } else {
-        const int xs = g.x == 0 ? 0 : -1, xe = g.x == P->ncells.x - 1 ? 0 : 1;
-        const int ys = g.y == 0 ? 0 : -1, ye = g.y == P->ncells.y - 1 ? 0 : 1;
-        const int zs = g.z == 0 ? 0 : -1, ze = g.z == P->ncells.z - 1 ? 0 : 1;
-        const int nxr = xe - xs + 1, nzr = ze - zs + 1;
-        const int nq = nxr * nzr * (ye - ys + 1);
-        // lane q < nq: the q-th cell in y, z, x order
-        uint32_t q_start = 0, q_cnt = 0;
-        if (lane < nq) {
-          const int dx = lane % nxr, rest = lane / nxr;
-          const int dz = rest % nzr, dy = rest / nzr;
-          const uint32_t hq = grid_hash(*P, make_int3(g.x + xs + dx, g.y + ys + dy, g.z + zs + dz));
-          const uint32_t sq = __ldg(cstart + hq);
-          if (sq != 0xffffffffu) {
-            q_start = sq;
-            q_cnt = __ldg(cend + hq) - sq;
-          }
-        }
-        uint32_t incl = q_cnt;
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t y = __shfl_up_sync(full, incl, d);
-          if (lane >= d) incl += y;
-        }
-        const uint32_t q_off = incl - q_cnt;
-        const uint32_t total = __shfl_sync(full, incl, 31);
-        uint32_t cnt = 0;
-        for (uint32_t base = 0; base < total; base += 32) {
-          const uint32_t t = base + (uint32_t)lane;
-          // the last cell whose offset is <= t (empty cells share the next one's)
-          int lo = 0, hi = nq;
-          for (int it = 0; it < 5; ++it) {
-            const int mid = (lo + hi) >> 1;
-            const uint32_t om = __shfl_sync(full, q_off, mid);
-            if (hi - lo > 1) {
-              if (om <= t) lo = mid;
-              else hi = mid;
-            }
-          }
-          const uint32_t qs = __shfl_sync(full, q_start, lo);
-          const uint32_t qo = __shfl_sync(full, q_off, lo);
-          const bool live = t < total;
-          const uint32_t j = live ? qs + (t - qo) : 0u;
-          const float4 pb = live ? __ldg(pos + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          for (uint32_t kk = 0; kk < ng; ++kk) {
-            const uint32_t i = g0 + kk;
-            const float4 pa4 = __ldg(pos + i);
-            const bool hit = live && j != i && pair_kept(xyz(pa4), pa4.w, pb, skin);
-            const unsigned bits = __ballot_sync(full, hit);
-            const uint32_t c = __shfl_sync(full, cnt, (int)kk);
-            if (hit) {
-              const uint32_t slot = c + (uint32_t)__popc(bits & ((1u << lane) - 1u));
-              if (slot < cap) nl.idx[(size_t)slot * stride + i] = j;
-              else st |= kStatusListOverflow;
-            }
-            if ((uint32_t)lane == kk) cnt = c + (uint32_t)__popc(bits);
-          }
-        }
-        if ((uint32_t)lane < ng && (int)(g0 + lane) < n) kept = min(cnt, cap);
-      }
-      if ((uint32_t)lane < ng && (int)(g0 + lane) < n) nl.cnt[g0 + lane] = kept;
-      if (nl.flat) {
-        // this group's slots, particle by particle: one atomic per group
-        uint32_t x = kept;
-        for (int d = 1; d < 32; d <<= 1) {
-          const uint32_t y = __shfl_up_sync(full, x, d);
-          if (lane >= d) x += y;
-        }
-        uint32_t fb = 0;
-        if (lane == 31 && x) fb = (uint32_t)atomicAdd(nl.flat_n, (int)x);
-        fb = __shfl_sync(full, fb, 31) + (x - kept);
-        for (uint32_t kk = 0; kk < ng; ++kk) {
-          const uint32_t kc = __shfl_sync(full, kept, (int)kk);
-          const uint32_t kb = __shfl_sync(full, fb, (int)kk);
-          for (uint32_t k = lane; k < kc; k += 32)
-            nl.flat[kb + k] = k * (uint32_t)nl.stride + (g0 + kk);
-        }
-      }
-    }
+    const int last = 31 - __clz((int)m);
+    uint32_t base = 0;
+    if (lane == last) base = (uint32_t)atomicAdd(nl.flat_n, (int)x);
+    base = __shfl_sync(m, base, last) + (x - kept);
+    for (uint32_t k = 0; k < kept; ++k) nl.flat[base + k] = k * (uint32_t)nl.stride + (uint32_t)i;
   }
   flag_status(ctl, st);
 }
@@ -1015,14 +914,11 @@ void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob
                                                 ctl, gate);
 }
 
-void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, uint32_t ncell_tab,
-                  const uint32_t* cell_start, const uint32_t* cell_end, NbrList nl, StepCtl* ctl,
-                  const int* gate, cudaStream_t st) {
-  // a warp per bucket, and at least a thread per particle for the pass
-  // over particles outside the grid
-  const size_t threads = std::max((size_t)ncell_tab * 32, (size_t)std::max(n_max, 1));
-  const unsigned g = (unsigned)((threads + kThreads - 1) / kThreads);
-  k_nlist<<<g, kThreads, 0, st>>>(dp, s.pos, cell_start, cell_end, nl, ctl, gate);
+void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
+                  const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
+                  cudaStream_t st) {
+  k_nlist<<<blocks(n_max), kThreads, 0, st>>>(dp, s.pos, n_max, cell_start, cell_end, nl, ctl,
+                                              gate);
 }
 
 void launch_step(const SimParams* dp, const WallOp* ops, WallGrid wg, const StateBuf& in_plain,

@@ -152,9 +152,9 @@ void launch_reorder(const StateBuf& src, const StateBuf& dst, const OrderBuf& ob
                     const uint32_t* sorted_keys, const int32_t* perm, uint32_t* cell_start,
                     uint32_t* cell_end, uint32_t ncell_tab, bool has_lift, int* flat_n,
                     StepCtl* ctl, const int* gate, cudaStream_t st);
-void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, uint32_t ncell_tab,
-                  const uint32_t* cell_start, const uint32_t* cell_end, NbrList nl, StepCtl* ctl,
-                  const int* gate, cudaStream_t st);
+void launch_nlist(const SimParams* dp, const StateBuf& s, int n_max, const uint32_t* cell_start,
+                  const uint32_t* cell_end, NbrList nl, StepCtl* ctl, const int* gate,
+                  cudaStream_t st);
 // eb: when not null, the step also writes each particle's energy-tally
 // values (particle-particle, volume objects, world objects; FP64) to
 // eb[c * n_max + i].  fast: the contracted particle-particle law (ignored

@@ -202,7 +202,7 @@ extern "C" int blaze_contact_list_static(const float* pos4, int n, const Simulat
   nl.cap = max_nbr;
   nl.flat = nullptr;
   nl.flat_n = nullptr;
-  launch_nlist(dp, dst, n, (uint32_t)ntab, cstart, cend, nl, ctl, nullptr, st);
+  launch_nlist(dp, dst, n, cstart, cend, nl, ctl, nullptr, st);
   CKS(cudaMemcpyAsync(perm, rs.vals[res], sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
   if (status)
     CKS(cudaMemcpyAsync(status, &ctl->status, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
