@@ -9,11 +9,16 @@ data-path collective); the barrier and the max-over-ranks time reduction use
 the process group only.
 
 Workload: the silo discharge configuration in its reference-law form (the
-form the reference's own code can run): cylinder r = 25 cm over a 30 degree
-conical hopper of 42 planar faces to a 6 cm outlet, 1,000,000 spheres with
+form the reference's own code can run): a 25 cm barrel over a 30 degree
+hopper to a 6 cm outlet as 7 sector world objects of planar quads (the
+reference's own silo is built of planar faces), 1,000,000 spheres with
 radius uniform in [0.2, 0.4] cm quantised to 6 particle objects, density
 2600 kg/m^3, linear spring-dashpot kn = 1e5 kg/s^2, restitution 0.6,
-mu 0.5, dt = 5e-6 s, FP32; synthetic seeded packing (no dataset exists).
+mu 0.5, dt = 5e-6 s, FP32; synthetic seeded packing (no dataset exists),
+settled with the hatch closed before the hatch opens and the timing starts.
+The full form (Hertz-Mindlin, 4,096-triangle hopper, which the reference
+cannot run) is the line's `silo_full` entry, and `--silo-full-only` prints
+it alone.
 
 Timed region (value): K steps enqueued through the handle API on device-
 resident state, bracketed by CUDA events on the library's stream.
