@@ -86,6 +86,7 @@ def parse():
                     help="skip the convex-polyhedra leg (100,000 polyhedra in a box)")
     ap.add_argument("--poly-steps", type=int, default=500)
     ap.add_argument("--no-mill", action="store_true", help="skip the ball-mill leg")
+    ap.add_argument("--no-c1", action="store_true", help="skip the C1 box leg")
     ap.add_argument("--mill-steps", type=int, default=5000)
     ap.add_argument("--mill-only", action="store_true",
                     help="print only the ball-mill leg's JSON line")
@@ -576,6 +577,71 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
     return out
 
 
+def c1_leg(steps=2000, warmup=20, want_cpu=True):
+    """The Particles_Box plain configuration (C1): 10,000 spheres r = 0.1 cm
+    falling from a jittered 20 x 20 x 25 lattice (pitch 0.3 cm) in a 10 cm
+    cube of six quads, linear law kn = 1e5, e = 0.5, mu = 0.4, dt = 1e-5 s,
+    gravity -981 cm/s^2 along z, the full `steps` steps from rest.  GPU: the
+    reference mode (contacts-only list rebuilt every step, the reference's
+    arithmetic, graph stepping) and a 0.02 cm Verlet skin, each timed with
+    CUDA events over the whole run.  CPU: oracle A (the reference's kernels
+    on the host) over the same full run on all host threads; its final
+    state is compared with the GPU reference mode's bit for bit."""
+    import torch
+    from blaze import device, synth
+    with tempfile.TemporaryDirectory() as d:
+        P, st = synth.box_project(d)
+    n = P.num_particles
+    out = {"workload": "C1 Particles_Box plain: 10,000 spheres r 0.1 cm falling in a 10 cm box, "
+                       "linear law kn 1e5 e 0.5 mu 0.4, dt 1e-5 s, the full run from rest",
+           "particles": n, "steps": steps}
+    final = {}
+    for name, opts in (("reference_mode", dict(use_graph=1)),
+                       ("skin", dict(skin=0.02, use_graph=1))):
+        sim = device.Simulation(P, **opts)
+        sim.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+        sim.prepare_graphs()
+        stream = torch.cuda.ExternalStream(sim.device_state()[3])
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(steps)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b) / steps
+        s_ = sim.state()
+        final[name] = s_
+        out[name] = {"value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "rebuilds": sim.num_rebuilds(), "status": device.decode_status(s_["status"])}
+        sim.close()
+    out["value"] = out["skin"]["value"]
+    out["unit"] = UNIT
+    if want_cpu:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from bindings import RefHost, ref_available
+        if ref_available():
+            threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+            with _StdoutToStderr():
+                R = RefHost().init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d,
+                                   threads=threads, capture=False)
+                R.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+                t0 = time.perf_counter()
+                rc = R.step(steps)
+                el = time.perf_counter() - t0
+                r = R.state()
+            g = final["reference_mode"]
+            ig, ir = np.argsort(g["pid"]), np.argsort(r["pid"])
+            same = bool(rc == 0 and all(np.array_equal(g[k][ig], r[k][ir])
+                                        for k in ("pos", "vel", "avel")))
+            out["cpu_baseline"] = {"value": n * steps / el, "unit": UNIT, "cores": threads,
+                                   "kind": "reference",
+                                   "sample": "the full %d-step run (%.1f s), reference mode"
+                                             % (steps, el)}
+            out["reference_mode_bit_exact_vs_cpu"] = same
+            out["vs_cpu_reference"] = out["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
 def mill_leg(steps, warmup, n=100_000, skin=0.05, cpu_seconds=15.0, want_cpu=True,
              settle=60000):
     """Ball mill, the sphere charge of the mill configuration on the
@@ -962,6 +1028,9 @@ def main():
     if not args.no_mill:
         mill = mill_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                         want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+    c1 = None
+    if not args.no_c1:
+        c1 = c1_leg(2000, args.warmup, want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
     batched = None
     if not args.no_batched:
         batched = batched_leg(args.batched_steps, args.warmup)
@@ -1005,6 +1074,7 @@ def main():
             "silo_full": silo_full,
             "polyhedra": poly,
             "mill": mill,
+            "c1_box": c1,
             "batched": batched,
             "adjoint": adjoint,
             "status": device.decode_status(status),
