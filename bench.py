@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--poly-steps", type=int, default=500)
     ap.add_argument("--no-mill", action="store_true", help="skip the ball-mill leg")
     ap.add_argument("--no-c1", action="store_true", help="skip the C1 box leg")
+    ap.add_argument("--no-mill-mesh", action="store_true",
+                    help="skip the turning-mesh ball-mill leg (ensemble path)")
     ap.add_argument("--mill-steps", type=int, default=5000)
     ap.add_argument("--mill-only", action="store_true",
                     help="print only the ball-mill leg's JSON line")
@@ -577,6 +579,47 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
     return out
 
 
+def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
+    """The ball mill with its drum and lifters as a turning mesh of 16,192
+    triangles (ensemble path; the reference has no triangle walls): drum
+    r = 50 cm, L = 30 cm, 8 lifters 4 x 4 cm, 30 rpm, n steel spheres
+    r ~ U[0.3, 0.6] cm, linear law with tangential history kn = 1e6,
+    e = 0.4, mu = 0.6, dt = 2e-6 s.  The charge, packed inside the lifter
+    ring, runs `settle` untimed steps with the drum turning (0.12 s), then
+    `steps` graph steps are timed with CUDA events."""
+    import torch
+    from blaze import synth
+    from blaze import ensemble as E
+    S, W, p, r = synth.drum_mesh_ensemble(n=n, skin=skin)
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=skin, use_graph=1)
+    ens.set_state(p, r)
+    ens.step(settle + max(3, warmup))
+    ens.sync()
+    stream = torch.cuda.ExternalStream(ens.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = ens.num_rebuilds()
+    a.record(stream)
+    ens.step(steps)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = ens.num_rebuilds() - rb0
+    launches = ens.last_launches() + rebuilds * ens.rebuild_kernels()
+    st = ens.state()
+    ens.close()
+    x, y = st["pos"][:, 0].astype(np.float64), st["pos"][:, 1].astype(np.float64)
+    # tangential velocity in the drum's sense of turn (clockwise seen from +z)
+    vt = -(x * st["vel"][:, 1] - y * st["vel"][:, 0]) / np.maximum(np.hypot(x, y), 1e-9)
+    return {"workload": "ball mill, drum and lifters as a turning mesh of %d triangles, 30 rpm, "
+                        "%d steel spheres r 0.3-0.6 cm, linear law + tangential history kn 1e6 "
+                        "e 0.4 mu 0.6, dt 2e-6 s" % (len(W), n),
+            "particles": n, "triangles": len(W), "value": n / (ms * 1e-3), "unit": UNIT,
+            "ms_per_step": ms, "steps": steps, "settle_steps": settle, "skin_cm": skin,
+            "rebuilds": rebuilds, "gpu_launches": launches, "status": st["status"],
+            "charge_mean_tangential_velocity_cm_s": float(vt.mean())}
+
+
 def c1_leg(steps=2000, warmup=20, want_cpu=True):
     """The Particles_Box plain configuration (C1): 10,000 spheres r = 0.1 cm
     falling from a jittered 20 x 20 x 25 lattice (pitch 0.3 cm) in a 10 cm
@@ -1028,6 +1071,9 @@ def main():
     if not args.no_mill:
         mill = mill_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                         want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+    mill_mesh = None
+    if not args.no_mill_mesh:
+        mill_mesh = mill_mesh_leg(args.mill_steps, args.warmup)
     c1 = None
     if not args.no_c1:
         c1 = c1_leg(2000, args.warmup, want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
@@ -1074,6 +1120,7 @@ def main():
             "silo_full": silo_full,
             "polyhedra": poly,
             "mill": mill,
+            "mill_mesh": mill_mesh,
             "c1_box": c1,
             "batched": batched,
             "adjoint": adjoint,

@@ -68,6 +68,17 @@ typedef struct blaze_system {
   float mu_roll;      /* rolling friction coefficient (0: none) */
   int wall0, nwalls;  /* planes and cylinders of this system: walls[wall0 .. +nwalls) */
   int tri0, ntris;    /* triangles of this system: walls[tri0 .. +ntris) */
+  /* A turning drum: the system's triangles and cylinders turn at rot_omega
+   * (rad/s, right-handed about rot_axis, a unit vector, through rot_point),
+   * from their given positions at the last blaze_ens_set_state.  Their
+   * surfaces move with the turn (the contact laws see the relative
+   * velocity, and the drum's spin in the rolling friction); planes stay.
+   * The turn is advanced on the device after every step by the constant
+   * increment (cos, sin of rot_omega dt in float) and renormalised.
+   * rot_omega 0: nothing turns. */
+  float rot_point[3];
+  float rot_axis[3];
+  float rot_omega;
 } blaze_system;
 
 typedef struct blaze_ens_options {

@@ -57,6 +57,10 @@ typedef struct {
   v3 g;
   real dens43pi, kn, kt, beta2, estar, gstar, beta2h, mu, mu_w, mu_r;
   int wall0, nwall, tri0, ntri;
+  /* turning drum (blaze_system.rot_*), csrc/ens_kernels.cu "drum turn" */
+  v3 rot_o, rot_a;
+  real rot_w, rot_cd, rot_sd;
+  int rot;
 } sysc;
 
 typedef struct {
@@ -117,11 +121,13 @@ struct ens_oracle {
   v3* cap_f;
   v3* cap_t;
   int* sys_of;      /* system of each entry of the caller's arrays */
+  real* rot_c;      /* per system: cosine and sine of the drum's turn so far */
+  real* rot_s;
   struct tstep_* tape; /* recorded steps of the reverse sweep */
   int ntape;
 };
 
-static void constants(sysc* d, const blaze_system* s, uint32_t off) {
+static void constants(sysc* d, const blaze_system* s, uint32_t off, float dt) {
   const double pi = 3.14159265358979323846;
   const double e = s->restitution;
   const double le = log(e);
@@ -142,6 +148,23 @@ static void constants(sysc* d, const blaze_system* s, uint32_t off) {
   d->beta2h = (real)(2.0 * sqrt(5.0 / 6.0) * beta);
   d->mu = s->mu; d->mu_w = s->mu_wall; d->mu_r = s->mu_roll;
   d->wall0 = s->wall0; d->nwall = s->nwalls; d->tri0 = s->tri0; d->ntri = s->ntris;
+  d->rot_o = mk(s->rot_point[0], s->rot_point[1], s->rot_point[2]);
+  d->rot_a = mk(s->rot_axis[0], s->rot_axis[1], s->rot_axis[2]);
+  d->rot_w = s->rot_omega;
+  d->rot = s->rot_omega != 0.0f;
+  {
+    const float ang = s->rot_omega * dt;   /* single-precision cosine and sine, as the host */
+    d->rot_cd = (real)cosf(ang);
+    d->rot_sd = (real)sinf(ang);
+  }
+}
+
+/* v turned by the angle with cosine c and sine s about the unit axis a:
+ * v c + (a x v) s + a (a . v) (1 - c), in the kernels' order */
+static v3 rot_about(v3 a, real c, real s, v3 v) {
+  const v3 axv = cross(a, v);
+  const real av = dot(a, v);
+  return add(add(mul(v, c), mul(axv, s)), mul(a, av * ((real)1.0 - c)));
 }
 
 ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* walls, int nwalls,
@@ -154,7 +177,7 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
   uint32_t off = 0;
   int n = 0;
   for (int s = 0; s < nsys; ++s) {
-    constants(&o->S[s], &sys[s], off);
+    constants(&o->S[s], &sys[s], off, (float)dt);
     off += (uint32_t)sys[s].ncells[0] * sys[s].ncells[1] * sys[s].ncells[2];
     n += sys[s].n;
   }
@@ -191,6 +214,9 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
   o->cap_f = (v3*)calloc(n, sizeof(v3));
   o->cap_t = (v3*)calloc(n, sizeof(v3));
   o->sys_of = (int*)calloc(n, sizeof(int));
+  o->rot_c = (real*)calloc(nsys, sizeof(real));
+  o->rot_s = (real*)calloc(nsys, sizeof(real));
+  for (int s = 0; s < nsys; ++s) o->rot_c[s] = 1;
   int k = 0;
   for (int s = 0; s < nsys; ++s)
     for (int m = 0; m < sys[s].n; ++m) o->sys_of[k++] = s;
@@ -204,6 +230,7 @@ void ens_destroy(ens_oracle* o) {
   free(o->S); free(o->W); free(o->p); free(o->q);
   for (int c = 0; c < 2; ++c) { free(o->idx[c]); free(o->cnt[c]); free(o->mask[c]); free(o->hist[c]); }
   free(o->cstart); free(o->cend); free(o->cap_f); free(o->cap_t); free(o->sys_of);
+  free(o->rot_c); free(o->rot_s);
   free(o);
 }
 
@@ -221,7 +248,7 @@ void ens_set_constants(ens_oracle* o, int s, const double* c5) {
 }
 
 int ens_set_params(ens_oracle* o, const blaze_system* sys) {
-  for (int s = 0; s < o->nsys; ++s) constants(&o->S[s], &sys[s], o->S[s].cell_off);
+  for (int s = 0; s < o->nsys; ++s) constants(&o->S[s], &sys[s], o->S[s].cell_off, (float)o->dt);
   return 0;
 }
 
@@ -247,6 +274,7 @@ void ens_set_state(ens_oracle* o, const double* pos3, const double* rad, const d
   }
   o->rebuild_req = 1;
   o->status = 0;
+  for (int s = 0; s < o->nsys; ++s) { o->rot_c[s] = 1; o->rot_s[s] = 0; }
 }
 
 static int cell_of(const sysc* S, v3 p, int c[3]) {
@@ -507,14 +535,23 @@ typedef struct {
   uint32_t st;
 } wctx;
 
-static void wall_contact(wctx* c, int id, v3 n, real delta) {
+static void wall_contact(wctx* c, int id, v3 n, real delta, int moving) {
   const part* a = c->a;
+  const sysc* S = c->S;
   v3 xi = mk(0, 0, 0);
   for (int q = 0; q < WSLOTS; ++q)
     if (((a->wmask >> q) & 1u) && a->wid[q] == id) xi = mk(a->wh[q][0], a->wh[q][1], a->wh[q][2]);
   const v3 vcpa = add(a->vel, cross(a->w, mul(n, -a->r)));
+  v3 vr = a->vel, vc = vcpa, wr = a->w;
+  if (moving) {
+    /* the wall's velocity at the contact point, and its spin */
+    const v3 vw = mul(cross(S->rot_a, sub(sub(a->pos, mul(n, a->r)), S->rot_o)), S->rot_w);
+    vr = sub(a->vel, vw);
+    vc = sub(vcpa, vw);
+    wr = sub(a->w, mul(S->rot_a, S->rot_w));
+  }
   v3 F, T;
-  contact_law(c->o, c->S, c->S->mu_w, n, delta, a->r, c->ma, a->vel, vcpa, a->w, a->r, &xi, &F, &T);
+  contact_law(c->o, c->S, c->S->mu_w, n, delta, a->r, c->ma, vr, vc, wr, a->r, &xi, &F, &T);
   c->f = add(c->f, F);
   c->t = add(c->t, T);
   if (c->nw < WSLOTS) {
@@ -603,22 +640,28 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
     c.o = o; c.S = S; c.a = a; c.ma = ma; c.f = f; c.t = t;
     for (int w = S->wall0; w < S->wall0 + S->nwall; ++w) {
       v3 nn; real d; int reg;
-      if (wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) wall_contact(&c, w, nn, d);
+      if (wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg))
+        wall_contact(&c, w, nn, d, S->rot && o->W[w].kind == BLAZE_WALL_CYLINDER);
     }
     int cc[3];
-    if (S->ntri > 0 && cell_of(S, a->pos, cc)) {
+    /* a turning drum: its triangles are tested in the drum's frame */
+    const real rc = o->rot_c[a->sys], rsn = o->rot_s[a->sys];
+    const v3 pd = S->rot ? add(S->rot_o, rot_about(S->rot_a, rc, -rsn, sub(a->pos, S->rot_o)))
+                         : a->pos;
+    if (S->ntri > 0 && cell_of(S, pd, cc)) {
       int nface = 0, best = -1;
       real best_d = 0;
       for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
         v3 nn; real d; int reg;
-        if (!wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) continue;
+        if (!wall_touch(&o->W[w], pd, ra, &nn, &d, &reg)) continue;
         if (reg == 0) ++nface;
         else if (best < 0 || d > best_d) { best = w; best_d = d; }
       }
       for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
         v3 nn; real d; int reg;
-        if (!wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg)) continue;
-        if ((nface > 0 && reg == 0) || (nface == 0 && w == best)) wall_contact(&c, w, nn, d);
+        if (!wall_touch(&o->W[w], pd, ra, &nn, &d, &reg)) continue;
+        if ((nface > 0 && reg == 0) || (nface == 0 && w == best))
+          wall_contact(&c, w, S->rot ? rot_about(S->rot_a, rc, rsn, nn) : nn, d, S->rot);
       }
     }
     f = c.f; t = c.t;
@@ -648,6 +691,16 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
   }
   part* tmp = o->p; o->p = o->q; o->q = tmp;
   if (req) o->rebuild_req = 1;
+  /* the drums' turn advances after the step (k_ens_rot_tick) */
+  for (int s = 0; s < o->nsys; ++s) {
+    if (!o->S[s].rot) continue;
+    const real c0 = o->rot_c[s], s0 = o->rot_s[s];
+    const real c1 = c0 * o->S[s].rot_cd - s0 * o->S[s].rot_sd;
+    const real s1 = s0 * o->S[s].rot_cd + c0 * o->S[s].rot_sd;
+    const real m = SQRT(c1 * c1 + s1 * s1);
+    o->rot_c[s] = c1 / m;
+    o->rot_s[s] = s1 / m;
+  }
 }
 
 int ens_step(ens_oracle* o, int nsteps) {

@@ -30,7 +30,8 @@ class System(C.Structure):
         ("kt_ratio", C.c_float), ("youngs", C.c_float), ("poisson", C.c_float),
         ("restitution", C.c_float), ("mu", C.c_float), ("mu_wall", C.c_float),
         ("mu_roll", C.c_float), ("wall0", C.c_int), ("nwalls", C.c_int), ("tri0", C.c_int),
-        ("ntris", C.c_int),
+        ("ntris", C.c_int), ("rot_point", C.c_float * 3), ("rot_axis", C.c_float * 3),
+        ("rot_omega", C.c_float),
     ]
 
 

@@ -789,6 +789,92 @@ def cone_hopper_triangles(silo_r, r_out, y_top, y_out, n_seg=64, n_ring=32, cent
     return tris
 
 
+def drum_mesh_triangles(R, L, n_seg, n_len, n_lifters=8, lifter_w=4.0, lifter_h=4.0):
+    """A ball-mill drum as triangles: the barrel (radius R, axis z, from z = 0
+    to L) as n_seg x n_len quads, the two end plates as fans of n_seg
+    triangles about the axis, and n_lifters box lifters (lifter_w wide,
+    lifter_h high, the drum's length) on the barrel, each as its two sides
+    and top, each face split along its length into n_len quads; every quad is
+    two triangles.  The axis passes through (0, 0).  Returns a list of
+    triangles ((x, y, z) x 3)."""
+    tris = []
+    zs = np.linspace(0.0, L, n_len + 1)
+    for m in range(n_seg):
+        a0, a1 = 2 * math.pi * m / n_seg, 2 * math.pi * (m + 1) / n_seg
+        for k in range(n_len):
+            p00 = (R * math.cos(a0), R * math.sin(a0), zs[k])
+            p01 = (R * math.cos(a1), R * math.sin(a1), zs[k])
+            p10 = (R * math.cos(a0), R * math.sin(a0), zs[k + 1])
+            p11 = (R * math.cos(a1), R * math.sin(a1), zs[k + 1])
+            tris += [(p00, p01, p11), (p00, p11, p10)]
+        for z in (0.0, L):
+            tris.append(((0.0, 0.0, z), (R * math.cos(a0), R * math.sin(a0), z),
+                         (R * math.cos(a1), R * math.sin(a1), z)))
+    for q in range(n_lifters):
+        ang = 2 * math.pi * q / n_lifters
+        er = np.array([math.cos(ang), math.sin(ang), 0.0])    # outward
+        et = np.array([-math.sin(ang), math.cos(ang), 0.0])   # along the barrel
+        # the lifter's foot sits on the chord at R cos(half angle) so its
+        # corners touch the barrel
+        half = 0.5 * lifter_w
+        base = math.sqrt(R * R - half * half)
+        top = base - lifter_h
+        corners = {"bl": base * er - half * et, "br": base * er + half * et,
+                   "tl": top * er - half * et, "tr": top * er + half * et}
+        faces = [("bl", "tl"), ("tl", "tr"), ("tr", "br")]   # side, top, side
+        for u, v in faces:
+            for k in range(n_len):
+                a = tuple(corners[u][:2]) + (zs[k],)
+                b = tuple(corners[v][:2]) + (zs[k],)
+                c = tuple(corners[v][:2]) + (zs[k + 1],)
+                d = tuple(corners[u][:2]) + (zs[k + 1],)
+                tris += [(a, b, c), (a, c, d)]
+    return tris
+
+
+def drum_mesh_ensemble(n=100_000, R=50.0, L=30.0, n_seg=256, n_len=28, n_lifters=8,
+                       lifter_w=4.0, lifter_h=4.0, r_min=0.3, r_max=0.6, rho=7800.0, kn=1e6,
+                       restitution=0.4, mu=0.6, rpm=30.0, law_youngs=0.0, skin=0.04, seed=2,
+                       gravity=(0.0, -981.0, 0.0)):
+    """The ball mill with its drum and lifters as a turning triangle mesh
+    (drum_mesh_triangles: 256 x 28 barrel quads, two 256-triangle end plates,
+    8 lifters of 3 faces x 28 quads: 16,192 triangles), as a one-system
+    ensemble turning at rpm about the z axis: n spheres r ~ U[r_min, r_max]
+    on a lattice in the lower part of the drum inside the lifter ring, at
+    rest; linear law kn (kt = 2/7 kn), restitution, mu; y vertical.
+    Returns (systems, walls, pos, radius)."""
+    from . import ensemble as E
+    tris = drum_mesh_triangles(R, L, n_seg, n_len, n_lifters, lifter_w, lifter_h)
+    walls = [E.triangle(*t) for t in tris]
+    s = E.System()
+    s.n = int(n)
+    cell = 2.0 * r_max + skin
+    for k, (o, ext) in enumerate(zip((-R - cell, -R - cell, -cell),
+                                     (2 * R + 2 * cell, 2 * R + 2 * cell, L + 2 * cell))):
+        s.origin[k] = o
+        s.ncells[k] = int(math.ceil(ext / cell))
+    s.cell = cell
+    for k in range(3):
+        s.gravity[k] = gravity[k]
+    s.density = rho * 1e-6
+    s.kn, s.kt_ratio, s.youngs, s.poisson = kn, 2.0 / 7.0, law_youngs, 0.3
+    s.restitution, s.mu, s.mu_wall, s.mu_roll = restitution, mu, mu, 0.0
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 0, 0, len(walls)
+    s.rot_axis[2] = 1.0
+    s.rot_omega = -rpm * 2.0 * math.pi / 60.0
+    rng = np.random.default_rng(seed)
+    r_in = R - lifter_h - 1.0
+    pitch = 2.0 * r_max + 0.5 * skin
+    pts = lattice_fill(int(4 * n), (-r_in, -r_in, r_max + 0.05), (r_in, r_in, L - r_max - 0.05),
+                       pitch, rng, jitter=0.1 * (pitch - 2.0 * r_max))
+    pts = pts[np.hypot(pts[:, 0], pts[:, 1]) < r_in - r_max]
+    pts = pts[np.argsort(pts[:, 1], kind="stable")][:n]   # lowest first
+    if len(pts) < n:
+        raise ValueError("drum_mesh_ensemble: %d spheres do not fit the drum" % n)
+    rad = rng.uniform(r_min, r_max, n)
+    return [s], walls, pts.astype(np.float32), rad.astype(np.float32)
+
+
 def silo_full_ensemble(n=1_000_000, r_min=0.2, r_max=0.4, rho=2600.0, silo_r=25.0,
                        silo_h=100.0, half_angle_deg=30.0, outlet_d=6.0, n_seg=64, n_ring=32,
                        youngs_pa=1e7, poisson=0.3, restitution=0.6, mu=0.5, mu_roll=0.01,

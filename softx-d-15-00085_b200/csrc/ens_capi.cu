@@ -71,6 +71,8 @@ struct blaze_ens {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t pgraph[2] = {nullptr, nullptr};   // persistent stepping, home S[c]
   int* d_pw = nullptr;        // persistent stepping: left, done, req_step, barrier x3
+  float2* d_rot = nullptr;    // per system: (cos, sin) of the drum's turn so far
+  bool any_rot = false;
   int persist_grid = 0;
   int* d_rb = nullptr;
   uint32_t status = 0;
@@ -93,11 +95,12 @@ EnsGeom geom(const blaze_ens* e) {
   g.curved = 0;
   for (const EnsWallDev& w : e->hwalls)
     if (w.kind != kWallPlane) g.curved = 1;
+  g.rot = e->d_rot;
   return g;
 }
 
 // Per-system constants of the contact law, in double, rounded once to float.
-EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off) {
+EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off, float dt) {
   EnsSysDev d;
   std::memset(&d, 0, sizeof(d));
   d.origin = make_float3(s.origin[0], s.origin[1], s.origin[2]);
@@ -137,6 +140,15 @@ EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off) {
       d.ref_b = 0.0;
     }
     d.ref_m = ((4.0 / 3.0) * rpi) * (double)s.density;
+  }
+  d.rot_o = make_float3(s.rot_point[0], s.rot_point[1], s.rot_point[2]);
+  d.rot_a = make_float3(s.rot_axis[0], s.rot_axis[1], s.rot_axis[2]);
+  d.rot_w = s.rot_omega;
+  d.rot = s.rot_omega != 0.0f ? 1 : 0;
+  {
+    const float ang = s.rot_omega * dt;   // the host's single-precision cosine and sine
+    d.rot_cd = std::cos(ang);
+    d.rot_sd = std::sin(ang);
   }
   return d;
 }
@@ -243,7 +255,7 @@ void free_ens(blaze_ens* e) {
   f(e->rs.counts); f(e->rs.totals); f(e->cstart); f(e->cend); f(e->ctl); f(e->d_rb);
   f(e->d_sys); f(e->d_walls); f(e->d_tri_off); f(e->d_tri_ids); f(e->d_sys_of);
   f(e->st_pos3); f(e->st_rad); f(e->st_vel3); f(e->st_avel3); f(e->st_sys); f(e->st_pid);
-  f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw);
+  f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw); f(e->d_rot);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->h_flags) cudaFreeHost(e->h_flags);
   if (e->aux2) cudaStreamDestroy(e->aux2);
@@ -259,6 +271,11 @@ bool valid_system(const blaze_system& s, int nwalls, float skin) {
   if (!(s.density > 0.0f) || !(s.restitution > 0.0f) || !(s.restitution <= 1.0f)) return false;
   if (s.wall0 < 0 || s.nwalls < 0 || s.wall0 + s.nwalls > nwalls) return false;
   if (s.tri0 < 0 || s.ntris < 0 || s.tri0 + s.ntris > nwalls) return false;
+  if (!std::isfinite(s.rot_omega)) return false;
+  if (s.rot_omega != 0.0f) {
+    const double ax = s.rot_axis[0], ay = s.rot_axis[1], az = s.rot_axis[2];
+    if (!(std::fabs(std::sqrt(ax * ax + ay * ay + az * az) - 1.0) < 1e-5)) return false;
+  }
   return true;
 }
 
@@ -266,7 +283,7 @@ int upload_params(blaze_ens* e) {
   uint32_t off = 0;
   e->hsys.resize(e->nsys);
   for (int s = 0; s < e->nsys; ++s) {
-    e->hsys[s] = system_constants(e->sys[s], off);
+    e->hsys[s] = system_constants(e->sys[s], off, e->opt.dt);
     off += (uint32_t)e->sys[s].ncells[0] * (uint32_t)e->sys[s].ncells[1] *
            (uint32_t)e->sys[s].ncells[2];
   }
@@ -300,6 +317,10 @@ int enqueue_step(blaze_ens* e) {
   ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0},
                   e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
   e->last_launches += 2 + rebuild_kernel_count(e);
+  if (e->any_rot) {
+    ens_launch_rot_tick(geom(e), e->nsys, e->stream);
+    e->last_launches += 1;
+  }
   e->cur ^= 1;
   return 0;
 }
@@ -346,6 +367,7 @@ int build_graph(blaze_ens* e, int c) {
                                                : StepLink{e->d_rb + k, 0, 0};
     ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link,
                     e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
+    if (e->any_rot) ens_launch_rot_tick(geom(e), e->nsys, e->stream);
     e->cur ^= 1;
   }
   cudaGraph_t out = nullptr;
@@ -500,7 +522,8 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
     if (walls[w].kind < BLAZE_WALL_PLANE || walls[w].kind > BLAZE_WALL_CYLINDER) return -1;
   for (int s = 0; s < nsys; ++s) {
     // the reference law meets plane walls only
-    if (o.law == BLAZE_LAW_REFERENCE && systems[s].ntris > 0) return -1;
+    if (o.law == BLAZE_LAW_REFERENCE && (systems[s].ntris > 0 || systems[s].rot_omega != 0.0f))
+      return -1;
     for (int w = systems[s].wall0; w < systems[s].wall0 + systems[s].nwalls; ++w) {
       if (walls[w].kind == BLAZE_WALL_TRIANGLE) return -1;
       if (o.law == BLAZE_LAW_REFERENCE && walls[w].kind != BLAZE_WALL_PLANE) return -1;
@@ -561,6 +584,12 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   CKF(cudaMemset(e->d_rb, 0, sizeof(int) * kGraphSteps));
   CKF(dalloc(&e->d_pw, 8));
   CKF(cudaMemset(e->d_pw, 0, sizeof(int) * 8));
+  CKF(dalloc(&e->d_rot, nsys));
+  for (int s = 0; s < nsys; ++s) e->any_rot = e->any_rot || systems[s].rot_omega != 0.0f;
+  {
+    const std::vector<float2> id((size_t)nsys, make_float2(1.0f, 0.0f));
+    CKF(cudaMemcpy(e->d_rot, id.data(), sizeof(float2) * nsys, cudaMemcpyHostToDevice));
+  }
   CKF(dalloc(&e->d_sys, nsys));
   CKF(dalloc(&e->d_walls, nwalls));
   CKF(dalloc(&e->d_sys_of, n));
@@ -669,6 +698,11 @@ int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, co
   const int ep = e->h_ctl->epoch & 1;
   ens_launch_pack(e->st_pos3, e->st_rad, vel3 ? e->st_vel3 : nullptr, avel3 ? e->st_avel3 : nullptr,
                   e->d_sys_of, e->b, e->cur, e->b.pid[ep], n, e->d_flags, e->stream);
+  if (e->any_rot) {   // the drums start from the walls' given positions
+    const std::vector<float2> id((size_t)e->nsys, make_float2(1.0f, 0.0f));
+    CK(cudaMemcpyAsync(e->d_rot, id.data(), sizeof(float2) * e->nsys, cudaMemcpyHostToDevice,
+                       e->stream));
+  }
   CK(cudaMemcpyAsync(e->h_flags, e->d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   CK(cudaGetLastError());
@@ -714,7 +748,8 @@ namespace {
 // nsteps steps, as kGraphSteps-step CUDA graphs where `graphs` allows (the
 // remainder as plain steps).
 int advance(blaze_ens* e, int nsteps, bool graphs) {
-  if (graphs && e->opt.use_graph == 2 && !e->opt.capture_forces && nsteps > 0) {
+  // persistent stepping (no drum turns: those advance between steps)
+  if (graphs && e->opt.use_graph == 2 && !e->opt.capture_forces && !e->any_rot && nsteps > 0) {
     const int c = e->cur;
     if (!e->pgraph[c]) {
       int rc = build_persist_graph(e, c);
@@ -739,7 +774,7 @@ int advance(blaze_ens* e, int nsteps, bool graphs) {
       if (rc) return rc;
     }
     CK(cudaGraphLaunch(e->graph[c], e->stream));
-    e->last_launches += 1 + kGraphSteps;
+    e->last_launches += 1 + kGraphSteps * (e->any_rot ? 2 : 1);
     if (kGraphSteps & 1) e->cur ^= 1;
     done += kGraphSteps;
   }
@@ -1068,7 +1103,7 @@ int blaze_ens_adj_create_tape(blaze_ens_adj** out, blaze_ens* e, int nsteps, int
   if (!out || !e || nsteps < 1 || segment < 1) return -1;
   const unsigned long long aw = arena_bytes / 4 & ~3ull;
   if (aw < (unsigned long long)std::min(segment, nsteps) * tape_block_words(e->n)) return -2;
-  if (e->opt.law != BLAZE_LAW_LINEAR) return -1;
+  if (e->opt.law != BLAZE_LAW_LINEAR || e->any_rot) return -1;
   for (const blaze_system& s : e->sys)
     if (s.mu_roll > 0.0f || s.ntris > 0) return -1;
   for (const EnsWallDev& w : e->hwalls)

@@ -51,6 +51,14 @@ __device__ __forceinline__ bool ens_in(const EnsSysDev& S, int3 c) {
 __device__ __forceinline__ uint32_t ens_key(const EnsSysDev& S, int3 c) {
   return S.cell_off + (uint32_t)(c.x + S.nc.x * (c.y + S.nc.y * c.z));
 }
+// v turned by the angle with cosine c and sine s about the unit axis a
+// (Rodrigues): v c + (a x v) s + a (a . v) (1 - c)
+__device__ __forceinline__ float3 rot_about(float3 a, float c, float s, float3 v) {
+  const float3 axv = cross3(a, v);
+  const float av = dot3(a, v);
+  return (v * c + axv * s) + a * (av * (1.0f - c));
+}
+
 __device__ __forceinline__ float sphere_mass(const EnsSysDev& S, float r) {
   return S.dens43pi * ((r * r) * r);
 }
@@ -605,14 +613,35 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     }
   }
   int nw = 0;
-  auto wall_contact = [&](int id, float3 nrm, float delta) {
+  // a turning drum (kCurved only): its triangles are tested in the drum's
+  // frame, where they stand still, and the normals turned back; triangles
+  // and cylinders move with the turn
+  bool rot = false;
+  float rc = 1.0f, rsn = 0.0f;
+  if constexpr (kCurved) {
+    if (S.rot) {
+      rot = true;
+      const float2 cs = g.rot[sys];
+      rc = cs.x;
+      rsn = cs.y;
+    }
+  }
+  auto wall_contact = [&](int id, float3 nrm, float delta, bool moving) {
     float3 xi = f3(0.0f, 0.0f, 0.0f);
 #pragma unroll
     for (int q = 0; q < kWallSlots; ++q)
       if (__float_as_int(oh[q].w) == id) xi = f3(oh[q].x, oh[q].y, oh[q].z);
     const float3 vcpa = va + cross3(wa, nrm * (-ra));
+    float3 vr = va, vc = vcpa, wr = wa;
+    if (moving) {
+      // the wall's velocity at the contact point, and its spin
+      const float3 vw = cross3(S.rot_a, (pa - nrm * ra) - S.rot_o) * S.rot_w;
+      vr = va - vw;
+      vc = vcpa - vw;
+      wr = wa - S.rot_a * S.rot_w;
+    }
     float3 F, T;
-    contact_law<kLaw>(S, S.mu_w, nrm, delta, ra, ma, va, vcpa, wa, ra, dt, xi, F, T);
+    contact_law<kLaw>(S, S.mu_w, nrm, delta, ra, ma, vr, vc, wr, ra, dt, xi, F, T);
     f = f + F;
     t = t + T;
     if (nw < kWallSlots) {
@@ -627,10 +656,12 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     float3 nrm;
     float delta;
     int region;
-    if (wall_touch<kCurved>(W, pa, ra, nrm, delta, region)) wall_contact(w, nrm, delta);
+    if (wall_touch<kCurved>(W, pa, ra, nrm, delta, region))
+      wall_contact(w, nrm, delta, rot && W.kind == kWallCylinder);
   }
   if (kCurved && g.tri_off) {
-    const int3 c = ens_cell(S, pa);
+    const float3 pd = rot ? S.rot_o + rot_about(S.rot_a, rc, -rsn, pa - S.rot_o) : pa;
+    const int3 c = ens_cell(S, pd);
     if (ens_in(S, c)) {
       const uint32_t h = ens_key(S, c);
       const uint32_t o0 = __ldg(g.tri_off + h), o1 = __ldg(g.tri_off + h + 1);
@@ -643,7 +674,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
         float3 nrm;
         float delta;
         int region;
-        if (!wall_touch<kCurved>(g.walls[id], pa, ra, nrm, delta, region)) continue;
+        if (!wall_touch<kCurved>(g.walls[id], pd, ra, nrm, delta, region)) continue;
         if (region == 0) ++nface;
         else if (best < 0 || delta > best_d) { best = id; best_d = delta; }
       }
@@ -652,8 +683,9 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
         float3 nrm;
         float delta;
         int region;
-        if (!wall_touch<kCurved>(g.walls[id], pa, ra, nrm, delta, region)) continue;
-        if ((nface > 0 && region == 0) || (nface == 0 && id == best)) wall_contact(id, nrm, delta);
+        if (!wall_touch<kCurved>(g.walls[id], pd, ra, nrm, delta, region)) continue;
+        if ((nface > 0 && region == 0) || (nface == 0 && id == best))
+          wall_contact(id, rot ? rot_about(S.rot_a, rc, rsn, nrm) : nrm, delta, rot);
       }
     }
   }
@@ -720,6 +752,17 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     }
   }
   ens_flag(ctl, st);
+}
+
+// ------------------------------------------------------------ drum turn
+__global__ void k_ens_rot_tick(const EnsSysDev* __restrict__ sys, float2* rot, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || !sys[s].rot) return;
+  const float2 r = rot[s];
+  const float c1 = r.x * sys[s].rot_cd - r.y * sys[s].rot_sd;
+  const float s1 = r.y * sys[s].rot_cd + r.x * sys[s].rot_sd;
+  const float m = sqrtf(c1 * c1 + s1 * s1);
+  rot[s] = make_float2(c1 / m, s1 / m);
 }
 
 // ------------------------------------------------------- persistent steps
@@ -992,6 +1035,10 @@ cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int
   if (g.law == kLawHertz)
     return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawHertz, false>, g, b, sh, so, ss, n, ctl, rebuilt, p);
   return cudaLaunchKernelEx(&cfg, k_ens_persist<kLawLinear, false>, g, b, sh, so, ss, n, ctl, rebuilt, p);
+}
+
+void ens_launch_rot_tick(const EnsGeom& g, int nsys, cudaStream_t st) {
+  k_ens_rot_tick<<<(nsys + kThreads - 1) / kThreads, kThreads, 0, st>>>(g.sys, g.rot, nsys);
 }
 
 void ens_launch_persist_gate(StepCtl* ctl, const EnsPersist& p, int* rb,

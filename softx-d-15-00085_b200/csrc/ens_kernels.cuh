@@ -54,6 +54,11 @@ struct EnsSysDev {
   // no damping (restitution 1)
   double ref_a, ref_b;
   double ref_m;        // (4/3) pi density: m = ref_m r^3 in double, rounded once
+  // turning drum (blaze_system.rot_*): triangles and cylinders turn about
+  // rot_a through rot_o at rot_w rad/s; the increment per step is (rot_cd, rot_sd)
+  float3 rot_o, rot_a;
+  float rot_w, rot_cd, rot_sd;
+  int rot;
 };
 
 struct EnsWallDev {
@@ -126,6 +131,7 @@ struct EnsGeom {
   int law;
   float dt, skin;
   int curved;                // 1: some wall is a cylinder or a triangle (not only planes)
+  float2* rot;               // per system: (cos, sin) of the drum's turn so far
 };
 
 struct EnsCapture { float4* f; float4* t; };
@@ -256,6 +262,9 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
 // tape.ctl->slot: input state, history mask, active and wall histories.
 void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl* ctl,
                             StepLink link, const EnsTape& tape, int block, cudaStream_t st);
+// After a step: every turning system's (cos, sin) advanced by its increment
+// and renormalised.
+void ens_launch_rot_tick(const EnsGeom& g, int nsys, cudaStream_t st);
 // Persistent stepping: one cooperative launch runs up to *left steps with a
 // grid barrier between steps and returns at the first step that asks for a
 // re-sort (ctl->rebuild_req set) or when the budget is spent, with the state

@@ -128,6 +128,61 @@ def test_graph_stepping_equals_plain(boxes):
     assert out[0]["status"] == 0 and out[1]["status"] == 0
 
 
+def turning_drum(n=1500, seed=3):
+    """A small ball mill as a turning triangle mesh: drum R = 8 cm, L = 4 cm
+    (48 x 4 barrel quads, end plates as fans, 4 lifters 1.5 x 1.2 cm: 576
+    triangles) turning at 60 rpm about z, spheres r in [0.15, 0.3] cm
+    packed against the lower barrel, thrown down at 50 cm/s; y vertical."""
+    R, L = 8.0, 4.0
+    tris = synth.drum_mesh_triangles(R, L, 48, 4, n_lifters=4, lifter_w=1.5, lifter_h=1.2)
+    walls = [E.triangle(*t) for t in tris]
+    s = E.System()
+    s.n = n
+    cell = 0.64
+    for k, (o, ext) in enumerate(zip((-R - cell, -R - cell, -cell),
+                                     (2 * R + 2 * cell, 2 * R + 2 * cell, L + 2 * cell))):
+        s.origin[k] = o
+        s.ncells[k] = int(np.ceil(ext / cell))
+    s.cell = cell
+    s.gravity[1] = -981.0
+    s.density = 7800e-6
+    s.kn, s.kt_ratio, s.youngs, s.poisson = 1e5, 2.0 / 7.0, 1e6, 0.3
+    s.restitution, s.mu, s.mu_wall, s.mu_roll = 0.4, 0.6, 0.6, 0.01
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 0, 0, len(walls)
+    s.rot_axis[2] = 1.0
+    s.rot_omega = 2.0 * np.pi
+    rng = np.random.default_rng(seed)
+    pts = synth.lattice_fill(2400, (-R + 0.35, -R + 0.35, 0.35), (R - 0.35, 0.0, L - 0.35), 0.62,
+                             rng, jitter=0.01)
+    pts = pts[np.hypot(pts[:, 0], pts[:, 1]) < R - 0.35]
+    pts = pts[np.argsort(pts[:, 1], kind="stable")][:n]
+    assert len(pts) == n
+    rad = rng.uniform(0.15, 0.3, n)
+    vel = np.zeros((n, 3))
+    vel[:, 1] = -50.0
+    return [s], walls, pts.astype(np.float32), rad.astype(np.float32), vel.astype(np.float32)
+
+
+@pytest.mark.parametrize("law", [E.LAW_LINEAR, E.LAW_HERTZ_MINDLIN])
+def test_turning_drum_mesh_bit_exact(law):
+    """Triangles turning with the drum (tested in its frame, surfaces moving):
+    GPU = FP32 restatement bit for bit, graph stepping included; and the
+    turn is felt (the mean tangential velocity of the charge follows the
+    drum)."""
+    S, W, p, r, v = turning_drum()
+    run_pair(S, W, p, r, law, (1, 50, 400), vel=v)
+    run_pair(S, W, p, r, law, (8, 64), vel=v, use_graph=1)
+    e = E.Ensemble(S, W, law=law, dt=DT, skin=SKIN, use_graph=1)
+    e.set_state(p, r, v)
+    e.step(2000)
+    st = e.state()
+    e.close()
+    assert st["status"] == 0, st["status"]
+    x, y = st["pos"][:, 0].astype(np.float64), st["pos"][:, 1].astype(np.float64)
+    vt = (x * st["vel"][:, 1] - y * st["vel"][:, 0]) / np.hypot(x, y)   # counter-clockwise
+    assert vt.mean() > 1.0, vt.mean()
+
+
 @pytest.mark.parametrize("law", [E.LAW_LINEAR, E.LAW_HERTZ_MINDLIN])
 def test_persistent_stepping_equals_plain(boxes, law):
     """use_graph = 2: one persistent kernel runs the steps between re-sorts
