@@ -626,8 +626,8 @@ def mill_project(root, n=100_000, r_min=0.3, r_max=0.6, n_bins=6, rho=7800.0, dr
 # ---------------------------------------------------------------- ensembles
 def lattice_fill(n, lo, hi, pitch, rng, jitter=0.0):
     """First n sites of a face-centred cubic lattice of nearest-neighbour
-    distance `pitch` inside the box [lo, hi] (filled bottom up, z last), each
-    moved by a uniform jitter in [-jitter, jitter]."""
+    distance `pitch` inside the box [lo, hi] (filled bottom up, z last; n
+    None: all of them), each moved by a uniform jitter in [-jitter, jitter]."""
     a = pitch * math.sqrt(2.0)
     lo = np.asarray(lo, np.float64)
     hi = np.asarray(hi, np.float64)
@@ -642,9 +642,11 @@ def lattice_fill(n, lo, hi, pitch, rng, jitter=0.0):
         layer = np.concatenate(layer)
         layer = layer[np.all((layer >= lo) & (layer <= hi), axis=1)]
         pts.append(layer[np.lexsort((layer[:, 0], layer[:, 1], layer[:, 2]))])
-        if sum(len(p) for p in pts) >= n:
+        if n is not None and sum(len(p) for p in pts) >= n:
             break
     pts = np.concatenate(pts)
+    if n is None:
+        n = len(pts)
     if len(pts) < n:
         raise ValueError("box holds %d lattice sites, %d requested" % (len(pts), n))
     pts = pts[:n]
@@ -865,7 +867,7 @@ def drum_mesh_ensemble(n=100_000, R=50.0, L=30.0, n_seg=256, n_len=28, n_lifters
     rng = np.random.default_rng(seed)
     r_in = R - lifter_h - 1.0
     pitch = 2.0 * r_max + 0.5 * skin
-    pts = lattice_fill(int(4 * n), (-r_in, -r_in, r_max + 0.05), (r_in, r_in, L - r_max - 0.05),
+    pts = lattice_fill(None, (-r_in, -r_in, r_max + 0.05), (r_in, r_in, L - r_max - 0.05),
                        pitch, rng, jitter=0.1 * (pitch - 2.0 * r_max))
     pts = pts[np.hypot(pts[:, 0], pts[:, 1]) < r_in - r_max]
     pts = pts[np.argsort(pts[:, 1], kind="stable")][:n]   # lowest first
