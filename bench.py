@@ -580,8 +580,9 @@ def poly_leg(steps, warmup, n=100_000, cpu_seconds=15.0, skin=0.05, want_cpu=Tru
 
 
 def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
-    """The ball mill with its drum and lifters as a turning mesh of 16,192
-    triangles (ensemble path; the reference has no triangle walls): drum
+    """The ball mill with its drum and lifters as a turning mesh of 16,384
+    triangles and two end plates turning in place (ensemble path; the
+    reference has no triangle walls): drum
     r = 50 cm, L = 30 cm, 8 lifters 4 x 4 cm, 30 rpm, n steel spheres
     r ~ U[0.3, 0.6] cm, linear law with tangential history kn = 1e6,
     e = 0.4, mu = 0.6, dt = 2e-6 s.  The charge, packed inside the lifter
@@ -613,8 +614,8 @@ def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
     vt = -(x * st["vel"][:, 1] - y * st["vel"][:, 0]) / np.maximum(np.hypot(x, y), 1e-9)
     return {"workload": "ball mill, drum and lifters as a turning mesh of %d triangles, 30 rpm, "
                         "%d steel spheres r 0.3-0.6 cm, linear law + tangential history kn 1e6 "
-                        "e 0.4 mu 0.6, dt 2e-6 s" % (len(W), n),
-            "particles": n, "triangles": len(W), "value": n / (ms * 1e-3), "unit": UNIT,
+                        "e 0.4 mu 0.6, dt 2e-6 s" % (int(S[0].ntris), n),
+            "particles": n, "triangles": int(S[0].ntris), "value": n / (ms * 1e-3), "unit": UNIT,
             "ms_per_step": ms, "steps": steps, "settle_steps": settle, "skin_cm": skin,
             "rebuilds": rebuilds, "gpu_launches": launches, "status": st["status"],
             "charge_mean_tangential_velocity_cm_s": float(vt.mean())}

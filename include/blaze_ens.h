@@ -72,7 +72,10 @@ typedef struct blaze_system {
    * (rad/s, right-handed about rot_axis, a unit vector, through rot_point),
    * from their given positions at the last blaze_ens_set_state.  Their
    * surfaces move with the turn (the contact laws see the relative
-   * velocity, and the drum's spin in the rolling friction); planes stay.
+   * velocity, and the drum's spin in the rolling friction).  Cylinders must
+   * be coaxial with the turn (they stay in place); planes normal to the
+   * axis (end plates) stay in place and their surfaces move; other planes
+   * stand still.
    * The turn is advanced on the device after every step by the constant
    * increment (cos, sin of rot_omega dt in float) and renormalised.
    * rot_omega 0: nothing turns. */

@@ -65,6 +65,7 @@ typedef struct {
 
 typedef struct {
   int kind;
+  int turning;   /* turns in place with its system's drum: its surface moves */
   real r;
   v3 a, b, c;
   double n64[3], e64[3][3];   /* triangle: unit normal, unit edges ab, ac, bc (double) */
@@ -200,6 +201,26 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
       unit64(ac[0], ac[1], ac[2], d->e64[1]);
       unit64(bc[0], bc[1], bc[2], d->e64[2]);
     } else { d->a = mk(p[0], p[1], p[2]); d->b = mk(p[3], p[4], p[5]); d->r = p[6]; }
+  }
+  /* walls that turn in place with a drum (csrc/ens_capi.cu, create_impl) */
+  for (int s = 0; s < nsys; ++s) {
+    const blaze_system* y = &sys[s];
+    if (y->rot_omega == 0.0f) continue;
+    const double ax = y->rot_axis[0], ay = y->rot_axis[1], az = y->rot_axis[2];
+    for (int w = y->wall0; w < y->wall0 + y->nwalls; ++w) {
+      wallc* W = &o->W[w];
+      const double a[3] = {(float)W->a.x, (float)W->a.y, (float)W->a.z};
+      const double b[3] = {(float)W->b.x, (float)W->b.y, (float)W->b.z};
+      if (W->kind == BLAZE_WALL_PLANE) {
+        W->turning = fabs(fabs(a[0] * ax + a[1] * ay + a[2] * az) - 1.0) < 1e-6;
+      } else if (W->kind == BLAZE_WALL_CYLINDER) {
+        const double par = fabs(b[0] * ax + b[1] * ay + b[2] * az);
+        const double d[3] = {a[0] - y->rot_point[0], a[1] - y->rot_point[1], a[2] - y->rot_point[2]};
+        const double dd = d[0] * ax + d[1] * ay + d[2] * az;
+        const double q = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] - dd * dd;
+        W->turning = fabs(par - 1.0) < 1e-6 && sqrt(q > 0 ? q : 0) < 1e-4;
+      }
+    }
   }
   o->p = (part*)calloc(n, sizeof(part));
   o->q = (part*)calloc(n, sizeof(part));
@@ -641,7 +662,7 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
     for (int w = S->wall0; w < S->wall0 + S->nwall; ++w) {
       v3 nn; real d; int reg;
       if (wall_touch(&o->W[w], a->pos, ra, &nn, &d, &reg))
-        wall_contact(&c, w, nn, d, S->rot && o->W[w].kind == BLAZE_WALL_CYLINDER);
+        wall_contact(&c, w, nn, d, S->rot && o->W[w].turning);
     }
     int cc[3];
     /* a turning drum: its triangles are tested in the drum's frame */

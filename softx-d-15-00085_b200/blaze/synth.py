@@ -791,14 +791,15 @@ def cone_hopper_triangles(silo_r, r_out, y_top, y_out, n_seg=64, n_ring=32, cent
     return tris
 
 
-def drum_mesh_triangles(R, L, n_seg, n_len, n_lifters=8, lifter_w=4.0, lifter_h=4.0):
+def drum_mesh_triangles(R, L, n_seg, n_len, n_lifters=8, lifter_w=4.0, lifter_h=4.0,
+                        end_fans=True):
     """A ball-mill drum as triangles: the barrel (radius R, axis z, from z = 0
     to L) as n_seg x n_len quads, the two end plates as fans of n_seg
-    triangles about the axis, and n_lifters box lifters (lifter_w wide,
-    lifter_h high, the drum's length) on the barrel, each as its two sides
-    and top, each face split along its length into n_len quads; every quad is
-    two triangles.  The axis passes through (0, 0).  Returns a list of
-    triangles ((x, y, z) x 3)."""
+    triangles about the axis (end_fans), and n_lifters box lifters
+    (lifter_w wide, lifter_h high, the drum's length) on the barrel, each as
+    its two sides and top, each face split along its length into n_len
+    quads; every quad is two triangles.  The axis passes through (0, 0).
+    Returns a list of triangles ((x, y, z) x 3)."""
     tris = []
     zs = np.linspace(0.0, L, n_len + 1)
     for m in range(n_seg):
@@ -809,7 +810,7 @@ def drum_mesh_triangles(R, L, n_seg, n_len, n_lifters=8, lifter_w=4.0, lifter_h=
             p10 = (R * math.cos(a0), R * math.sin(a0), zs[k + 1])
             p11 = (R * math.cos(a1), R * math.sin(a1), zs[k + 1])
             tris += [(p00, p01, p11), (p00, p11, p10)]
-        for z in (0.0, L):
+        for z in ((0.0, L) if end_fans else ()):
             tris.append(((0.0, 0.0, z), (R * math.cos(a0), R * math.sin(a0), z),
                          (R * math.cos(a1), R * math.sin(a1), z)))
     for q in range(n_lifters):
@@ -834,20 +835,20 @@ def drum_mesh_triangles(R, L, n_seg, n_len, n_lifters=8, lifter_w=4.0, lifter_h=
     return tris
 
 
-def drum_mesh_ensemble(n=100_000, R=50.0, L=30.0, n_seg=256, n_len=28, n_lifters=8,
+def drum_mesh_ensemble(n=100_000, R=50.0, L=30.0, n_seg=232, n_len=32, n_lifters=8,
                        lifter_w=4.0, lifter_h=4.0, r_min=0.3, r_max=0.6, rho=7800.0, kn=1e6,
                        restitution=0.4, mu=0.6, rpm=30.0, law_youngs=0.0, skin=0.04, seed=2,
                        gravity=(0.0, -981.0, 0.0)):
     """The ball mill with its drum and lifters as a turning triangle mesh
-    (drum_mesh_triangles: 256 x 28 barrel quads, two 256-triangle end plates,
-    8 lifters of 3 faces x 28 quads: 16,192 triangles), as a one-system
-    ensemble turning at rpm about the z axis: n spheres r ~ U[r_min, r_max]
+    (drum_mesh_triangles: 232 x 32 barrel quads and 8 lifters of 3 faces x
+    32 quads, 16,384 triangles; the end plates are planes turning in place)
+    as a one-system ensemble turning at rpm about the z axis: n spheres r ~ U[r_min, r_max]
     on a lattice in the lower part of the drum inside the lifter ring, at
     rest; linear law kn (kt = 2/7 kn), restitution, mu; y vertical.
     Returns (systems, walls, pos, radius)."""
     from . import ensemble as E
-    tris = drum_mesh_triangles(R, L, n_seg, n_len, n_lifters, lifter_w, lifter_h)
-    walls = [E.triangle(*t) for t in tris]
+    tris = drum_mesh_triangles(R, L, n_seg, n_len, n_lifters, lifter_w, lifter_h, end_fans=False)
+    walls = [E.plane((0, 0, 1), 0.0), E.plane((0, 0, -1), -L)] + [E.triangle(*t) for t in tris]
     s = E.System()
     s.n = int(n)
     cell = 2.0 * r_max + skin
@@ -861,7 +862,7 @@ def drum_mesh_ensemble(n=100_000, R=50.0, L=30.0, n_seg=256, n_len=28, n_lifters
     s.density = rho * 1e-6
     s.kn, s.kt_ratio, s.youngs, s.poisson = kn, 2.0 / 7.0, law_youngs, 0.3
     s.restitution, s.mu, s.mu_wall, s.mu_roll = restitution, mu, mu, 0.0
-    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 0, 0, len(walls)
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 2, 2, len(tris)
     s.rot_axis[2] = 1.0
     s.rot_omega = -rpm * 2.0 * math.pi / 60.0
     rng = np.random.default_rng(seed)

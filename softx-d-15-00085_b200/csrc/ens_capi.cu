@@ -544,6 +544,27 @@ int create_impl(blaze_ens** out, const blaze_system* systems, int nsys, const bl
   e->sys.assign(systems, systems + nsys);
   e->ncell_tab = (uint32_t)cells;
   for (int w = 0; w < nwalls; ++w) e->hwalls.push_back(wall_dev(walls[w]));
+  // walls that turn in place with a drum: cylinders coaxial with it, planes
+  // normal to its axis (their surfaces move; their positions do not)
+  for (int s = 0; s < nsys; ++s) {
+    const blaze_system& y = systems[s];
+    if (y.rot_omega == 0.0f) continue;
+    const double ax = y.rot_axis[0], ay = y.rot_axis[1], az = y.rot_axis[2];
+    for (int w = y.wall0; w < y.wall0 + y.nwalls; ++w) {
+      EnsWallDev& W = e->hwalls[w];
+      const double a[3] = {W.a.x, W.a.y, W.a.z}, b[3] = {W.b.x, W.b.y, W.b.z};
+      if (W.kind == kWallPlane) {
+        W.turning = std::fabs(std::fabs(a[0] * ax + a[1] * ay + a[2] * az) - 1.0) < 1e-6 ? 1 : 0;
+      } else if (W.kind == kWallCylinder) {
+        // axis parallel, and the axis point on the turn's axis
+        const double par = std::fabs(b[0] * ax + b[1] * ay + b[2] * az);
+        const double d[3] = {a[0] - y.rot_point[0], a[1] - y.rot_point[1], a[2] - y.rot_point[2]};
+        const double dd = d[0] * ax + d[1] * ay + d[2] * az;
+        const double off = std::sqrt(std::max(0.0, d[0] * d[0] + d[1] * d[1] + d[2] * d[2] - dd * dd));
+        W.turning = (std::fabs(par - 1.0) < 1e-6 && off < 1e-4) ? 1 : 0;
+      }
+    }
+  }
   const uint32_t top = e->ncell_tab + 1u;
   e->key_bits = 1;
   while (e->key_bits < 32 && (top >> e->key_bits) != 0) e->key_bits++;

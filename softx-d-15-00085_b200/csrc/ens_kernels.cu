@@ -657,7 +657,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     float delta;
     int region;
     if (wall_touch<kCurved>(W, pa, ra, nrm, delta, region))
-      wall_contact(w, nrm, delta, rot && W.kind == kWallCylinder);
+      wall_contact(w, nrm, delta, rot && W.turning);
   }
   if (kCurved && g.tri_off) {
     const float3 pd = rot ? S.rot_o + rot_about(S.rot_a, rc, -rsn, pa - S.rot_o) : pa;

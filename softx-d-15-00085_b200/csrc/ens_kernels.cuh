@@ -63,6 +63,8 @@ struct EnsSysDev {
 
 struct EnsWallDev {
   int kind;
+  int turning;         // a cylinder or a plane that turns in place with its system's drum
+                       // (coaxial cylinder, plane normal to the axis): its surface moves
   float r;             // plane: offset d (n . x = d on the plane); cylinder: radius
   float3 a, b, c;      // plane: a = unit normal into the domain; triangle: vertices;
                        // cylinder: a = point on the axis, b = unit axis

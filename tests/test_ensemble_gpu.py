@@ -130,12 +130,14 @@ def test_graph_stepping_equals_plain(boxes):
 
 def turning_drum(n=1500, seed=3):
     """A small ball mill as a turning triangle mesh: drum R = 8 cm, L = 4 cm
-    (48 x 4 barrel quads, end plates as fans, 4 lifters 1.5 x 1.2 cm: 576
-    triangles) turning at 60 rpm about z, spheres r in [0.15, 0.3] cm
-    packed against the lower barrel, thrown down at 50 cm/s; y vertical."""
+    (48 x 4 barrel quads and 4 lifters 1.5 x 1.2 cm: 480 triangles; the end
+    plates are planes turning in place) turning at 60 rpm about z, spheres
+    r in [0.15, 0.3] cm packed against the lower barrel, thrown down at
+    50 cm/s; y vertical."""
     R, L = 8.0, 4.0
-    tris = synth.drum_mesh_triangles(R, L, 48, 4, n_lifters=4, lifter_w=1.5, lifter_h=1.2)
-    walls = [E.triangle(*t) for t in tris]
+    tris = synth.drum_mesh_triangles(R, L, 48, 4, n_lifters=4, lifter_w=1.5, lifter_h=1.2,
+                                     end_fans=False)
+    walls = [E.plane((0, 0, 1), 0.0), E.plane((0, 0, -1), -L)] + [E.triangle(*t) for t in tris]
     s = E.System()
     s.n = n
     cell = 0.64
@@ -148,7 +150,7 @@ def turning_drum(n=1500, seed=3):
     s.density = 7800e-6
     s.kn, s.kt_ratio, s.youngs, s.poisson = 1e5, 2.0 / 7.0, 1e6, 0.3
     s.restitution, s.mu, s.mu_wall, s.mu_roll = 0.4, 0.6, 0.6, 0.01
-    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 0, 0, len(walls)
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 2, 2, len(tris)
     s.rot_axis[2] = 1.0
     s.rot_omega = 2.0 * np.pi
     rng = np.random.default_rng(seed)
