@@ -96,6 +96,7 @@ EnsGeom geom(const blaze_ens* e) {
   for (const EnsWallDev& w : e->hwalls)
     if (w.kind != kWallPlane) g.curved = 1;
   g.rot = e->d_rot;
+  g.any_rot = e->any_rot ? 1 : 0;
   return g;
 }
 

@@ -487,7 +487,7 @@ __device__ __forceinline__ float ens_particle_step_ref(const EnsGeom& g, const E
 // Euler from `in` into `out`.  Raises status bits in st; returns the path
 // the particle has moved since the last re-sort.  kRecord: also writes what
 // the step reads into the tape view (histories to hrec when it is not null).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true>
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true, bool kRot = false>
 __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBufs& b,
                                                    const StateBuf& in, const StateBuf& out,
                                                    int i, int e, const EnsList& L, TapeView tv,
@@ -618,7 +618,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
   // and cylinders move with the turn
   bool rot = false;
   float rc = 1.0f, rsn = 0.0f;
-  if constexpr (kCurved) {
+  if constexpr (kCurved && kRot) {
     if (S.rot) {
       rot = true;
       const float2 cs = g.rot[sys];
@@ -713,7 +713,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
 
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
 // history words are reserved first, by every thread of the block).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved>
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot = false>
 __global__ void __launch_bounds__(kMaxStepBlock)
 k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
            StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
@@ -742,7 +742,8 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   if (i >= n) return;
   uint32_t st = 0;
   const float path =
-      ens_particle_step<kLaw, kCapture, kRecord, kCurved>(g, b, in, out, i, e, L, tv, hrec, cap, st);
+      ens_particle_step<kLaw, kCapture, kRecord, kCurved, true, kRot>(g, b, in, out, i, e, L, tv,
+                                                                       hrec, cap, st);
   {
     const unsigned m = __activemask();
     const unsigned req = __ballot_sync(m, path > 0.5f * g.skin);
@@ -959,7 +960,16 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
   const int gs = (n + bs - 1) / bs;
 #define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c, EnsTape{}
 #define ENS_STEP(L, C, K) k_ens_step<L, C, false, K><<<gs, bs, 0, st>>>(ENS_ARGS)
-  if (g.curved) {
+#define ENS_STEP_ROT(L, C) k_ens_step<L, C, false, true, true><<<gs, bs, 0, st>>>(ENS_ARGS)
+  if (g.curved && g.any_rot) {   // a turning drum
+    if (g.law == kLawHertz) {
+      if (cap) ENS_STEP_ROT(kLawHertz, true);
+      else ENS_STEP_ROT(kLawHertz, false);
+    } else {
+      if (cap) ENS_STEP_ROT(kLawLinear, true);
+      else ENS_STEP_ROT(kLawLinear, false);
+    }
+  } else if (g.curved) {
     if (g.law == kLawHertz) {
       if (cap) ENS_STEP(kLawHertz, true, true);
       else ENS_STEP(kLawHertz, false, true);
@@ -979,6 +989,7 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
       else ENS_STEP(kLawLinear, false, false);
     }
   }
+#undef ENS_STEP_ROT
 #undef ENS_STEP
 #undef ENS_ARGS
 }

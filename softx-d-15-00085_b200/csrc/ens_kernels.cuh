@@ -134,6 +134,7 @@ struct EnsGeom {
   float dt, skin;
   int curved;                // 1: some wall is a cylinder or a triangle (not only planes)
   float2* rot;               // per system: (cos, sin) of the drum's turn so far
+  int any_rot;               // 1: some system turns (the step compiled with the turn)
 };
 
 struct EnsCapture { float4* f; float4* t; };
