@@ -268,35 +268,6 @@ __global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
   c->lsnap = c->cur;
 }
 
-// Slots k < cnt of a particle's list whose spheres overlap (the forward's
-// test: d2 < (ra + rb)^2, |rel| > 0 and a positive overlap), as a bit mask;
-// the candidates in batches of four: the entries, then the position gathers,
-// then the tests.
-__device__ __forceinline__ uint32_t contact_mask(const uint2* ent, uint32_t cnt,
-                                                 const float4* pos, float3 xa, float ra) {
-  constexpr uint32_t kB = 4;
-  uint32_t cm = 0;
-  for (uint32_t k0 = 0; k0 < cnt; k0 += kB) {
-    uint32_t jj[kB];
-#pragma unroll
-    for (uint32_t u = 0; u < kB; ++u) jj[u] = k0 + u < cnt ? ent[k0 + u].x : 0u;
-    float4 pb[kB];
-#pragma unroll
-    for (uint32_t u = 0; u < kB; ++u)
-      pb[u] = k0 + u < cnt ? pos[jj[u]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-#pragma unroll
-    for (uint32_t u = 0; u < kB; ++u) {
-      const float3 rel = xa - xyz4(pb[u]);
-      const float sr = ra + pb[u].w;
-      const float d2 = dot3(rel, rel);
-      if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f &&
-          overlap_pair(ra, pb[u].w, xa, xyz4(pb[u])) > 0.0f)
-        cm |= 1u << (k0 + u);
-    }
-  }
-  return cm;
-}
-
 // --------------------------------------------------------------- reverse
 // The step backwards, per particle: symplectic Euler (v' = v + (f/m + g) dt,
 // x' = x + v' dt, w' = w + t/I dt) gives the cotangents of the particle's
@@ -327,7 +298,7 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   const uint32_t cnt = lv.cnt[i], mask = tv.mask[i];
   // the slots in contact first (batched loads, as in the forward), then the
   // contacts and the slots that held a history, in slot order
-  const uint32_t cm = contact_mask(ent, cnt, tv.pos, A.x, A.r);
+  const uint32_t cm = tv.cmask[i];   // the contacts the forward step applied its law to
   for (uint32_t todo = cm | (mask & ((cnt >= 32u ? 0u : (1u << cnt)) - 1u)); todo;
        todo &= todo - 1u) {
     const uint32_t k = (uint32_t)(__ffs(todo) - 1);
@@ -420,11 +391,8 @@ k_adj_gather(EnsTape tp, int t, int n, AdjBufs a) {
   const TapeView tv = tape_view(tp, ts.block, n);
   const TapeView lv = tape_view(tp, tl.block, n);
   const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + tl.lbase + lv.loff[i]);
-  const float4 pa = tv.pos[i];
-  const float3 xa = xyz4(pa);
   float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
-  const uint32_t cnt = lv.cnt[i];
-  for (uint32_t cm = contact_mask(ent, cnt, tv.pos, xa, pa.w); cm; cm &= cm - 1u) {
+  for (uint32_t cm = tv.cmask[i]; cm; cm &= cm - 1u) {
     const uint32_t k = (uint32_t)(__ffs(cm) - 1);
     const uint2 e = ent[k];
     const uint32_t j = e.x;

@@ -587,6 +587,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     t = t + T;
   }
   if (mask != mask_o) L.mask[i] = mask;
+  if constexpr (kRecord) tv.cmask[i] = mask;
 
   // walls: old history slots (by wall id) held in registers; new slots are
   // written in processing order straight over the old ones

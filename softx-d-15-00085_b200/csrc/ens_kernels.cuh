@@ -147,7 +147,8 @@ struct EnsCapture { float4* f; float4* t; };
 //   words, from TapeStep::hbase), and at a list step (a re-sort, or the
 //   first step of a segment) cnt 14n, loff 15n (the particle's list entries,
 //   from TapeStep::lbase), perm 16n (a re-sort: old index of each new
-//   position); 17n words rounded up to a multiple of 4.
+//   position), cmask 17n (the slots the step applied its law to: its
+//   contacts); 18n words rounded up to a multiple of 4.
 // Pool space, reserved a thread block at a time: per particle and step, 3
 // words per active history (slot order) then 4 per wall history (xi, wall
 // id); per particle and list, 2 words per list slot: (neighbour,
@@ -180,7 +181,7 @@ struct EnsTape {
 };
 
 __host__ __device__ constexpr unsigned long long tape_block_words(int n) {
-  return ((unsigned long long)n * 17ull + 3ull) & ~3ull;
+  return ((unsigned long long)n * 18ull + 3ull) & ~3ull;
 }
 
 struct TapeView {
@@ -192,6 +193,7 @@ struct TapeView {
   uint32_t* cnt;
   uint32_t* loff;
   int32_t* perm;
+  uint32_t* cmask;
 };
 
 __device__ __forceinline__ TapeView tape_view(const EnsTape& tp, unsigned long long block, int n) {
@@ -206,6 +208,7 @@ __device__ __forceinline__ TapeView tape_view(const EnsTape& tp, unsigned long l
   v.cnt = b + 14 * m;
   v.loff = b + 15 * m;
   v.perm = reinterpret_cast<int32_t*>(b + 16 * m);
+  v.cmask = b + 17 * m;
   return v;
 }
 
