@@ -229,7 +229,7 @@ k_adj_list(EnsBufs b, EnsTape tp, int n, const StepCtl* ctl, const int* gate, in
   TapeCtl* tc = tp.ctl;
   const int t = tc->slot + 1;
   const unsigned long long base = tc->lsnap;
-  const TapeView tv = tape_view(tp, tp.steps[t].block, n);
+  const unsigned long long lblock = tp.steps[t].lblock;
   const EnsList L = b.L[ctl->epoch & 1];
   const size_t stride = (size_t)b.stride;
   const uint32_t cnt = i < n ? L.cnt[i] : 0u;
@@ -240,9 +240,12 @@ k_adj_list(EnsBufs b, EnsTape tp, int n, const StepCtl* ctl, const int* gate, in
     tc->lslot = t;
   }
   if (i >= n) return;
-  tv.cnt[i] = cnt;
-  tv.loff[i] = off;
-  if (resorted) tv.perm[i] = perm[i];
+  if (lblock != ~0ull) {
+    const TapeList tl = tape_list(tp, lblock, n);
+    tl.cnt[i] = cnt;
+    tl.loff[i] = off;
+    if (resorted) tl.perm[i] = perm[i];
+  }
   if (!ok) return;
   uint2* ent = reinterpret_cast<uint2*>(tp.arena + base + off);
   for (uint32_t k = 0; k < cnt; ++k) {
@@ -254,6 +257,22 @@ k_adj_list(EnsBufs b, EnsTape tp, int n, const StepCtl* ctl, const int* gate, in
       if (L.idx[(size_t)q * stride + j] == (uint32_t)i) { tw = q; break; }
     const uint32_t src = resorted ? (uint32_t)L.src[sk] : 0xffu;
     ent[k] = make_uint2(j, tw | (src << 8));
+  }
+}
+
+// Before k_adj_list: the list step's dense arrays (cnt, loff, perm) from the
+// pool, ~0 when they do not fit (the overflow flag then fails the backward).
+__global__ void k_adj_list_block(EnsTape tp, int n, const int* gate) {
+  if (gate && *gate == 0) return;
+  TapeCtl* c = tp.ctl;
+  const int t = c->slot + 1;
+  const unsigned long long w = tape_list_words(n);
+  if (c->cur + w <= c->lim) {
+    tp.steps[t].lblock = c->cur;
+    c->cur += w;
+  } else {
+    tp.steps[t].lblock = ~0ull;
+    c->overflow = 1;
   }
 }
 
@@ -281,7 +300,7 @@ k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   const TapeStep ts = tp.steps[t];
   const TapeStep tl = tp.steps[ts.lat];
   const TapeView tv = tape_view(tp, ts.block, n);
-  const TapeView lv = tape_view(tp, tl.block, n);
+  const TapeList lv = tape_list(tp, tl.lblock, n);
   const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + tl.lbase + lv.loff[i]);
   const float* hp = reinterpret_cast<const float*>(tp.arena + ts.hbase + tv.hoff[i]);
   const uint32_t bits = __float_as_uint(tv.vel[i].w);
@@ -389,7 +408,7 @@ k_adj_gather(EnsTape tp, int t, int n, AdjBufs a) {
   const TapeStep ts = tp.steps[t];
   const TapeStep tl = tp.steps[ts.lat];
   const TapeView tv = tape_view(tp, ts.block, n);
-  const TapeView lv = tape_view(tp, tl.block, n);
+  const TapeList lv = tape_list(tp, tl.lblock, n);
   const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + tl.lbase + lv.loff[i]);
   float3 gx = f3(0.0f, 0.0f, 0.0f), gv = gx, gw = gx;
   for (uint32_t cm = tv.cmask[i]; cm; cm &= cm - 1u) {
@@ -416,7 +435,8 @@ k_adj_unsort(EnsTape tp, int t, int n, AdjBufs a) {
   if (i >= n) return;
   const TapeStep ts = tp.steps[t];
   const TapeView tv = tape_view(tp, ts.block, n);
-  const int io = tv.perm[i];
+  const TapeList tl = tape_list(tp, ts.lblock, n);
+  const int io = tl.perm[i];
   a.gx[io] = a.ix[i];
   a.gv[io] = a.iv[i];
   a.gw[io] = a.iw[i];
@@ -424,8 +444,8 @@ k_adj_unsort(EnsTape tp, int t, int n, AdjBufs a) {
 #pragma unroll
   for (int q = 0; q < kWallSlots; ++q)
     if ((wmask >> q) & 1u) a.gW[(size_t)q * n + io] = a.iW[(size_t)q * n + i];
-  const uint32_t cnt = tv.cnt[i];
-  const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + ts.lbase + tv.loff[i]);
+  const uint32_t cnt = tl.cnt[i];
+  const uint2* ent = reinterpret_cast<const uint2*>(tp.arena + ts.lbase + tl.loff[i]);
   for (uint32_t k = 0; k < cnt; ++k) {
     const uint32_t s = (ent[k].y >> 8) & 0xffu;
     if (s != 0xffu) a.gH[(size_t)s * n + io] = a.iH[(size_t)k * n + i];
@@ -490,6 +510,7 @@ void adj_launch_seg_start(const EnsTape& tp, int slot0, int len, unsigned long l
 
 void adj_launch_list(const EnsBufs& b, const EnsTape& tp, int n, const StepCtl* ctl,
                      const int* gate, int resorted, const int32_t* perm, cudaStream_t st) {
+  k_adj_list_block<<<1, 1, 0, st>>>(tp, n, gate);
   k_adj_list<<<nblk(n), kThreads, 0, st>>>(b, tp, n, ctl, gate, resorted, perm);
 }
 

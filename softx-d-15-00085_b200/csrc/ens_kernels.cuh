@@ -144,11 +144,12 @@ struct EnsCapture { float4* f; float4* t; };
 // steps reserved.  The dense block of a step (n particles; word offsets):
 //   pos 0, vel 4n, angv 8n (float4: the step's input state), mask 12n
 //   (active histories before the step), hoff 13n (the particle's history
-//   words, from TapeStep::hbase), and at a list step (a re-sort, or the
-//   first step of a segment) cnt 14n, loff 15n (the particle's list entries,
-//   from TapeStep::lbase), perm 16n (a re-sort: old index of each new
-//   position), cmask 17n (the slots the step applied its law to: its
-//   contacts); 18n words rounded up to a multiple of 4.
+//   words, from TapeStep::hbase), cmask 14n (the slots the step applied its
+//   law to: its contacts); 15n words rounded up to a multiple of 4.  A list
+//   step (a re-sort, or the first step of a segment) also reserves, in the
+//   pool at TapeStep::lblock, the list's dense arrays: cnt 0, loff n (the
+//   particle's list entries, from TapeStep::lbase), perm 2n (a re-sort: old
+//   index of each new position); 3n words rounded up to an even count.
 // Pool space, reserved a thread block at a time: per particle and step, 3
 // words per active history (slot order) then 4 per wall history (xi, wall
 // id); per particle and list, 2 words per list slot: (neighbour,
@@ -160,6 +161,7 @@ struct TapeStep {
   unsigned long long block;   // arena word of the step's dense block
   unsigned long long hbase;   // the step's history words count from here
   unsigned long long lbase;   // the list recorded for the step counts from here
+  unsigned long long lblock;  // a list step: its cnt / loff / perm arrays (~0: no room)
   int rb;                     // 1 when the step re-sorted
   int lat;                    // step whose list this step used
 };
@@ -181,7 +183,11 @@ struct EnsTape {
 };
 
 __host__ __device__ constexpr unsigned long long tape_block_words(int n) {
-  return ((unsigned long long)n * 18ull + 3ull) & ~3ull;
+  return ((unsigned long long)n * 15ull + 3ull) & ~3ull;
+}
+
+__host__ __device__ constexpr unsigned long long tape_list_words(int n) {
+  return ((unsigned long long)n * 3ull + 1ull) & ~1ull;
 }
 
 struct TapeView {
@@ -190,11 +196,24 @@ struct TapeView {
   float4* angv;
   uint32_t* mask;
   uint32_t* hoff;
+  uint32_t* cmask;
+};
+
+struct TapeList {
   uint32_t* cnt;
   uint32_t* loff;
   int32_t* perm;
-  uint32_t* cmask;
 };
+
+__device__ __forceinline__ TapeList tape_list(const EnsTape& tp, unsigned long long lblock, int n) {
+  uint32_t* b = tp.arena + lblock;
+  const size_t m = (size_t)n;
+  TapeList v;
+  v.cnt = b;
+  v.loff = b + m;
+  v.perm = reinterpret_cast<int32_t*>(b + 2 * m);
+  return v;
+}
 
 __device__ __forceinline__ TapeView tape_view(const EnsTape& tp, unsigned long long block, int n) {
   uint32_t* b = tp.arena + block;
@@ -205,10 +224,7 @@ __device__ __forceinline__ TapeView tape_view(const EnsTape& tp, unsigned long l
   v.angv = reinterpret_cast<float4*>(b + 8 * m);
   v.mask = b + 12 * m;
   v.hoff = b + 13 * m;
-  v.cnt = b + 14 * m;
-  v.loff = b + 15 * m;
-  v.perm = reinterpret_cast<int32_t*>(b + 16 * m);
-  v.cmask = b + 17 * m;
+  v.cmask = b + 14 * m;
   return v;
 }
 

@@ -156,9 +156,9 @@ def test_tape_holding_every_segment(case, gpu_grads):
 
 
 def state_bytes(n, steps):
-    """Arena bytes of `steps` recorded steps' dense blocks (17 words per
+    """Arena bytes of `steps` recorded steps' dense blocks (15 words per
     particle, rounded up to 4 words)."""
-    return 4 * ((17 * n + 3) // 4 * 4) * steps
+    return 4 * ((15 * n + 3) // 4 * 4) * steps
 
 
 def test_tape_ring(case, gpu_grads):
