@@ -293,7 +293,10 @@ __global__ void k_adj_tick(EnsTape tp, const int* rebuilt) {
 // force and torque; then the reverse of each of its own contacts, once: its
 // state, history and law-constant cotangents are kept, the share that goes
 // to the neighbour is left in the slot (px, pv, pw) for k_adj_gather.
-__global__ void __launch_bounds__(kThreads, 5)
+#ifndef BLAZE_ADJ_MIN_BLOCKS
+#define BLAZE_ADJ_MIN_BLOCKS 5
+#endif
+__global__ void __launch_bounds__(kThreads, BLAZE_ADJ_MIN_BLOCKS)
 k_adj_pair(EnsGeom g, EnsTape tp, int t, int n, AdjBufs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
