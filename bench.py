@@ -140,7 +140,7 @@ def case_poly(n=20000, steps=10):
 def case_adjoint(nsys=64, steps=60, segment=30, tape_bytes=0):
     """The calibration ensemble (nsys x 20,000 spheres), `steps` steps with
     checkpoints every `segment`, the tape budget `tape_bytes` (0: one
-    segment; -1: 90 % of the free device memory), forward and backward with
+    segment; -1: 96 % of the free device memory), forward and backward with
     random cotangents of the final state."""
     from blaze import calibrate
     from blaze import ensemble as E
@@ -399,7 +399,7 @@ def adjoint_leg(steps, segment=100):
     Timed with CUDA events on the ensemble's stream over `steps` steps: the
     plain forward (CUDA graphs, no tape), the checkpointing forward
     (blaze_ens_adj_forward: a checkpoint per segment, and the trailing
-    segments that fit recorded into a tape of 90 % of the free HBM) and the
+    segments that fit recorded into a tape of 96 % of the free HBM) and the
     backward (blaze_ens_adj_backward: recomputation of the segments the tape
     does not hold + reverse kernels), with the
     cotangents of the calibration loss (bed height + 32-bin side-wall force

@@ -153,7 +153,7 @@ int blaze_ens_adj_create(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segm
  *   tape_bytes == 0: one segment, with room for the most it can take (every
  *                    list slot an active history, a re-sort every step);
  *   tape_bytes  > 0: an arena of that many bytes;
- *   tape_bytes  < 0: 90 % of the device memory the reverse mode's other
+ *   tape_bytes  < 0: 96 % of the device memory the reverse mode's other
  *                    buffers leave free, less 4 GiB.
  * Returns -2 when the arena cannot hold one segment's states; a backward
  * whose recomputed segment does not fit the arena also returns -2. */

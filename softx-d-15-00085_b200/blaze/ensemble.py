@@ -215,7 +215,7 @@ class Adjoint:
 
     tape_bytes: 0 keeps one segment on the tape (the forward records the
     last one; the backward recomputes the others from their checkpoints);
-    a positive value is a budget in bytes; -1 takes 90 % of the free device
+    a positive value is a budget in bytes; -1 takes 96 % of the free device
     memory less 4 GiB.  The trailing segments that fit are recorded by the
     forward and not recomputed."""
 

@@ -1195,7 +1195,7 @@ int blaze_ens_adj_create_ex(blaze_ens_adj** out, blaze_ens* e, int nsteps, int s
     budget = (size_t)tape_bytes;
   } else {
     // what the other buffers of the reverse mode leave free: all device
-    // memory but 4 GiB, less 10 %
+    // memory but 4 GiB, less 4 %
     const int nseg = (nsteps + (int)K - 1) / (int)K;
     const size_t ckpt = n * (3 * sizeof(float4) + 3 * sizeof(uint32_t) + sizeof(int) +
                              kWallSlots * sizeof(float4)) + cap * n * 4 * sizeof(float);
@@ -1204,7 +1204,7 @@ int blaze_ens_adj_create_ex(blaze_ens_adj** out, blaze_ens* e, int nsteps, int s
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
     const size_t other = ckpt * (size_t)nseg + bufs + ((size_t)4 << 30);
-    budget = fr > other ? (fr - other) / 10 * 9 : 0;
+    budget = fr > other ? (fr - other) / 100 * 96 : 0;
   }
   return blaze_ens_adj_create_tape(out, e, nsteps, segment, (unsigned long long)budget);
 }
