@@ -683,6 +683,17 @@ def c1_leg(steps=2000, warmup=20, want_cpu=True):
                                              % (steps, el)}
             out["reference_mode_bit_exact_vs_cpu"] = same
             out["vs_cpu_reference"] = out["value"] / out["cpu_baseline"]["value"]
+            if threads > 1:
+                with _StdoutToStderr():
+                    R1 = RefHost().init(P.sim_info, P.wobj, P.n_w, P.pobj, P.n_p, P.dobj, P.n_d,
+                                        threads=1, capture=False)
+                    R1.set_state(st["pos"], st["vel"], st["avel"], st["type"], st["pid"])
+                    t0 = time.perf_counter()
+                    R1.step(steps)
+                    e1 = time.perf_counter() - t0
+                out["cpu_baseline"]["single_thread_value"] = n * steps / e1
+                out["cpu_baseline"]["single_thread_sample"] = ("the full %d-step run on 1 thread "
+                                                               "(%.1f s)" % (steps, e1))
     return out
 
 
@@ -870,10 +881,24 @@ def _cpu_reference_rate(P, st, seconds, max_steps, hatch, mill=None):
         el = time.perf_counter() - t0
         if el >= seconds or (max_steps and steps >= max_steps):
             break
-    return {"value": P.num_particles * steps / el, "unit": UNIT, "cores": threads,
-            "kind": "reference",
-            "sample": "%d full steps of the %d-particle workload (%.1f s), reference mode"
-                      % (steps, P.num_particles, el)}
+    out = {"value": P.num_particles * steps / el, "unit": UNIT, "cores": threads,
+           "kind": "reference",
+           "sample": "%d full steps of the %d-particle workload (%.1f s), reference mode"
+                     % (steps, P.num_particles, el)}
+    if threads > 1:
+        # the same kernels on one host thread, a third of the time budget (20 s at most)
+        R.lib.refh_set_threads(1)
+        s1 = 0
+        t0 = time.perf_counter()
+        while True:
+            R.step(1)
+            s1 += 1
+            e1 = time.perf_counter() - t0
+            if e1 >= min(seconds / 3.0, 20.0) or (max_steps and s1 >= max_steps):
+                break
+        out["single_thread_value"] = P.num_particles * s1 / e1
+        out["single_thread_sample"] = "%d further full steps on 1 thread (%.1f s)" % (s1, e1)
+    return out
 
 
 def run_reference_arm(args, rank):
