@@ -115,6 +115,12 @@ int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, co
  * entry i and pid[i] its index in the set_state arrays.  NULL skips an array. */
 int blaze_ens_get_state(blaze_ens* e, float* pos3, float* radius, float* vel3, float* avel3,
                         int* sys, int* pid);
+/* Self-check of persistent stepping's bounded barrier wait: two blocks wait
+ * at a barrier counted for three, which nothing completes; after the 2 s
+ * limit every block gives up and returns.  Returns the status words raised
+ * (16 expected: a bounded device wait gave up), <0 on a CUDA error; the
+ * context stays usable. */
+int blaze_ens_check_barrier_timeout(void);
 /* Enqueue nsteps steps on the ensemble's stream. */
 int blaze_ens_step(blaze_ens* e, int nsteps);
 /* Wait for the stream; the status bits raised since the state was set. */

@@ -808,6 +808,24 @@ int advance(blaze_ens* e, int nsteps, bool graphs) {
 
 extern "C" {
 
+int blaze_ens_check_barrier_timeout(void) {
+  unsigned int* bar = nullptr;
+  StepCtl* ctl = nullptr;
+  if (cudaMalloc((void**)&bar, 4 * sizeof(unsigned int)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&ctl, sizeof(StepCtl)) != cudaSuccess) {
+    cudaFree(bar);
+    return -1;
+  }
+  cudaMemset(bar, 0, 4 * sizeof(unsigned int));
+  cudaMemset(ctl, 0, sizeof(StepCtl));
+  ens_launch_barrier_check(bar, ctl, 0);
+  StepCtl h;
+  const cudaError_t e = cudaMemcpy(&h, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost);
+  cudaFree(bar);
+  cudaFree(ctl);
+  return e == cudaSuccess ? (int)h.status : -(1000 + (int)e);
+}
+
 int blaze_ens_step(blaze_ens* e, int nsteps) {
   if (!e || nsteps < 0 || !e->state_set) return -1;
   e->last_launches = 0;

@@ -829,6 +829,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
 // resident as the per-step launches have.
 constexpr int kPersistRegs = 80;
 
+// Self-check of the barrier's bounded wait: the barrier is told of one
+// block more than the launch has, so nothing completes it; every block must
+// give up after the limit, raise kStatusTimeout and return.
+__global__ void k_barrier_check(unsigned int* bar, StepCtl* ctl) {
+  grid_barrier(bar, gridDim.x + 1u, ctl);
+}
+
 template <int kLaw, bool kCurved>
 __global__ void __maxnreg__(kPersistRegs)
 k_ens_persist(EnsGeom g, EnsBufs b, StateBuf home, StateBuf other, StateBuf sorted, int n,
@@ -1051,6 +1058,10 @@ cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int
 
 void ens_launch_rot_tick(const EnsGeom& g, int nsys, cudaStream_t st) {
   k_ens_rot_tick<<<(nsys + kThreads - 1) / kThreads, kThreads, 0, st>>>(g.sys, g.rot, nsys);
+}
+
+void ens_launch_barrier_check(unsigned int* bar, StepCtl* ctl, cudaStream_t st) {
+  k_barrier_check<<<2, 64, 0, st>>>(bar, ctl);
 }
 
 void ens_launch_persist_gate(StepCtl* ctl, const EnsPersist& p, int* rb,

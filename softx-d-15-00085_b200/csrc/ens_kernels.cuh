@@ -310,6 +310,8 @@ cudaError_t ens_launch_persist(const EnsGeom& g, const EnsBufs& b, int home, int
 void ens_launch_persist_gate(StepCtl* ctl, const EnsPersist& p, int* rb,
                              cudaGraphConditionalHandle if_h, cudaStream_t st);
 void ens_launch_persist_init(const EnsPersist& p, int steps, cudaStream_t st);
+// Two blocks wait at a barrier counted for three (bar: 3 zeroed words).
+void ens_launch_barrier_check(unsigned int* bar, StepCtl* ctl, cudaStream_t st);
 // Staged caller arrays -> state S[cur], pid = index, both list copies and
 // every history cleared; flags[0] |= 1 for a radius that is not positive.
 void ens_launch_pack(const float* pos3, const float* rad, const float* vel3, const float* avel3,

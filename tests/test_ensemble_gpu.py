@@ -220,3 +220,18 @@ def test_out_of_grid_is_reported_not_faulted(boxes):
     e.step(2)
     assert e.sync() & 2
     e.close()
+
+
+def test_barrier_wait_gives_up_and_the_context_stays_usable(boxes):
+    """Persistent stepping's grid barrier waits at most 2 s: two blocks at a
+    barrier counted for three (nothing completes it) give up, raise status
+    16 and return; the next ensemble runs normally on the same context."""
+    lib = E.load()
+    lib.blaze_ens_check_barrier_timeout.argtypes = []
+    assert lib.blaze_ens_check_barrier_timeout() == 16
+    S, W, p, r = boxes
+    e = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=DT, skin=SKIN, use_graph=2)
+    e.set_state(p, r)
+    e.step(20)
+    assert e.sync() == 0
+    e.close()
