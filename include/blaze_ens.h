@@ -139,6 +139,60 @@ int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4,
 int blaze_ens_last_launches(blaze_ens* e);
 int blaze_ens_rebuild_kernels(blaze_ens* e);
 
+/* ------------------------------------------------------------- polyhedra
+ * Convex polyhedra among the spheres of a system (the mixed charge of the
+ * ball mill: steel balls and rocks).  The reference runs either spheres or
+ * polyhedra, never both (KSimulationData.cpp:129-141).
+ *
+ * A shape is a closed convex hull of 4..16 vertices and 2 V - 4 triangular
+ * faces in its body frame, centre of mass at the origin, faces
+ * counter-clockwise seen from outside, with its density.  A polyhedron
+ * meets
+ *   spheres     at the closest point of its hull to the sphere's centre,
+ *   polyhedra   along the axis of least penetration of the separating-axis
+ *               test (face normals of both hulls, cross products of the edge
+ *               pairs that form a face of the Minkowski difference), a face
+ *               preferred unless an edge pair is clearly shallower,
+ *   triangles   the same test with the triangle as a flat hull (coplanar
+ *               triangles touched together count once, the deepest),
+ *   planes      at its deepest vertex,
+ * all formed in FP64 from the FP32 state; the contact point is the mean of
+ * the penetrating vertices, or the midpoint of two crossing edges.  The law
+ * is the linear law with tangential history and Coulomb cap on the contact
+ * point's relative velocity, without rolling friction; a polyhedron
+ * integrates Euler's equations in its body frame and its orientation as a
+ * unit quaternion.  Systems holding polyhedra: linear law, plane and
+ * triangle walls (no cylinders), 2 r_bound + skin <= cell, at most 64
+ * neighbours per polyhedron; not with persistent stepping (use_graph 2
+ * steps as 1) nor reverse mode. */
+typedef struct blaze_shape {
+  int nverts;            /* 4 .. 16 */
+  int nfaces;            /* 2 nverts - 4 */
+  float density;         /* kg/cm^3 */
+  float verts[16 * 3];   /* body frame, cm, centre of mass at the origin */
+  int faces[28 * 3];     /* vertex indices per face, counter-clockwise seen from outside */
+} blaze_shape;
+
+/* Mass (kg), centre of mass (cm), inertia tensor about the centre of mass
+ * (kg cm^2, row-major) and bounding radius about the origin (cm, rounded
+ * up) of a shape, in FP64 from its faces; no device needed.  Returns -1 for
+ * a shape that is not a closed, outward-oriented convex hull of the sizes
+ * above. */
+int blaze_shape_mass_properties(const blaze_shape* s, double* mass, double* com3,
+                                double* inertia9, float* rbound);
+
+/* Right after blaze_ens_set_state (before any step): the particles with
+ * shape_of[i] >= 0 (caller order) are polyhedra of shapes[shape_of[i]] with
+ * orientation quat4[4 i ..] = (w, x, y, z) (normalised here); their radius
+ * in the state becomes the shape's bounding radius.  A later set_state
+ * leaves only spheres.  Returns -1 on a shape or system the rules above
+ * exclude. */
+int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes,
+                            const int* shape_of, const float* quat4);
+/* Orientations in the current memory order (4 floats per particle, w x y z;
+ * spheres 1 0 0 0). */
+int blaze_ens_get_orientations(blaze_ens* e, float* quat4);
+
 /* ------------------------------------------------------------ reverse mode
  * Gradients of a loss of the final state with respect to the initial state
  * and the law constants, by the discrete adjoint of the step (linear law

@@ -35,6 +35,17 @@ class System(C.Structure):
     ]
 
 
+MAX_VERTS = 16
+MAX_FACES = 28
+
+
+class Shape(C.Structure):
+    """blaze_shape: a convex hull in its body frame (centre of mass at the
+    origin), triangular faces counter-clockwise seen from outside."""
+    _fields_ = [("nverts", C.c_int), ("nfaces", C.c_int), ("density", C.c_float),
+                ("verts", C.c_float * (3 * MAX_VERTS)), ("faces", C.c_int * (3 * MAX_FACES))]
+
+
 class EnsOptions(C.Structure):
     _fields_ = [("law", C.c_int), ("dt", C.c_float), ("skin", C.c_float), ("max_nbr", C.c_int),
                 ("use_graph", C.c_int), ("capture_forces", C.c_int), ("block", C.c_int)]
@@ -78,6 +89,10 @@ def load():
                                                 P(C.c_ulonglong)]
         lib.blaze_ens_adj_create_tape.argtypes = [P(C.c_void_p), C.c_void_p, C.c_int, C.c_int,
                                                   C.c_ulonglong]
+        lib.blaze_shape_mass_properties.argtypes = [P(Shape), P(C.c_double), P(C.c_double),
+                                                    P(C.c_double), _f]
+        lib.blaze_ens_set_polyhedra.argtypes = [C.c_void_p, P(Shape), C.c_int, _i, _f]
+        lib.blaze_ens_get_orientations.argtypes = [C.c_void_p, _f]
         _bound = True
     return lib
 
@@ -119,6 +134,37 @@ def cylinder(point, axis, radius):
     return w
 
 
+def shape(verts, faces, density):
+    """A Shape from (V, 3) vertices (cm, about the centre of mass) and (F, 3)
+    outward triangles; density in kg/cm^3."""
+    v = np.asarray(verts, np.float32).reshape(-1, 3)
+    f = np.asarray(faces, np.int32).reshape(-1, 3)
+    if len(v) > MAX_VERTS or len(f) > MAX_FACES:
+        raise ValueError("shape: at most %d vertices and %d faces" % (MAX_VERTS, MAX_FACES))
+    s = Shape()
+    s.nverts, s.nfaces, s.density = len(v), len(f), float(density)
+    for k, x in enumerate(v.reshape(-1)):
+        s.verts[k] = float(x)
+    for k, x in enumerate(f.reshape(-1)):
+        s.faces[k] = int(x)
+    return s
+
+
+def mass_properties(s):
+    """(mass kg, centre of mass (3,), inertia about it (3, 3) kg cm^2,
+    bounding radius cm) of a Shape, from the library (FP64, no device)."""
+    lib = load()
+    m = C.c_double()
+    com = np.zeros(3, np.float64)
+    J = np.zeros(9, np.float64)
+    rb = C.c_float()
+    _check(lib.blaze_shape_mass_properties(C.byref(s), C.byref(m),
+                                           com.ctypes.data_as(C.POINTER(C.c_double)),
+                                           J.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rb)),
+           "blaze_shape_mass_properties")
+    return m.value, com, J.reshape(3, 3), rb.value
+
+
 class Ensemble:
     """Systems + walls on the GPU.  State arrays are (N, 3) float32 for all
     systems concatenated in system order."""
@@ -158,6 +204,23 @@ class Ensemble:
         _check(self.lib.blaze_ens_set_state(self.h, _ptr(pos, C.c_float), _ptr(radius, C.c_float),
                                             _ptr(vel, C.c_float), _ptr(avel, C.c_float)),
                "blaze_ens_set_state")
+
+    def set_polyhedra(self, shapes, shape_of, quat):
+        """After set_state: particle i (caller order) with shape_of[i] >= 0 is a
+        polyhedron of shapes[shape_of[i]] oriented by quat[i] = (w, x, y, z)."""
+        n = self.n
+        arr = (Shape * len(shapes))(*shapes)
+        so = np.ascontiguousarray(shape_of, np.int32).reshape(n)
+        q = np.ascontiguousarray(quat, np.float32).reshape(n, 4)
+        _check(self.lib.blaze_ens_set_polyhedra(self.h, arr, len(shapes), _ptr(so, C.c_int),
+                                                _ptr(q, C.c_float)), "blaze_ens_set_polyhedra")
+
+    def orientations(self):
+        """(N, 4) orientations (w, x, y, z) in the current memory order."""
+        q = np.zeros((self.n, 4), np.float32)
+        _check(self.lib.blaze_ens_get_orientations(self.h, _ptr(q, C.c_float)),
+               "blaze_ens_get_orientations")
+        return q
 
     def step(self, n=1):
         return _check(self.lib.blaze_ens_step(self.h, int(n)), "blaze_ens_step")

@@ -986,3 +986,181 @@ def box_c1(n_side=(20, 20, 25), radius=0.1, rho=2500.0, box=10.0, kn=1.0e5, cor=
     S = box_system(n, box, box, cell, 0, density=rho * 1e-6, kn=kn, kt_ratio=kt_ratio,
                    restitution=cor, mu=mu)
     return [S], box_walls(box, box), pos, np.full(n, radius, np.float32)
+
+
+# ------------------------------------------------------- mixed charges
+def hull_mass_centre(v, f):
+    """Volume and centre of mass of the closed outward triangle mesh (v, f),
+    FP64 (tetrahedra of the faces with the origin)."""
+    a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    det = np.einsum("ij,ij->i", a, np.cross(b, c))
+    vol = det.sum() / 6.0
+    return vol, (det[:, None] * (a + b + c)).sum(axis=0) / 24.0 / vol
+
+
+def rock_hull(rng, n_min=8, n_max=16, r_min=0.5, r_max=1.0):
+    """A rock: the convex hull of n ~ U{n_min .. n_max} points uniform on a
+    sphere of radius R ~ U[r_min, r_max] (cm), moved so that its centre of
+    mass is the origin.  Returns (vertices (n, 3) float32, outward triangles
+    (2 n - 4, 3) int32)."""
+    from scipy.spatial import ConvexHull
+    while True:
+        n = int(rng.integers(n_min, n_max + 1))
+        R = float(rng.uniform(r_min, r_max))
+        p = rng.normal(size=(n, 3))
+        p = p / np.linalg.norm(p, axis=1, keepdims=True) * R
+        h = ConvexHull(p)
+        if len(h.vertices) != n or len(h.simplices) != 2 * n - 4:
+            continue
+        f = h.simplices.copy()
+        cen = p.mean(axis=0)
+        for k in range(len(f)):
+            a, b, c = p[f[k]]
+            if np.dot(np.cross(b - a, c - a), a - cen) < 0:
+                f[k] = f[k][[0, 2, 1]]
+        _, com = hull_mass_centre(p, f)
+        return (p - com).astype(np.float32), f.astype(np.int32)
+
+
+def rock_shapes(n, seed=2, n_pts=(8, 16), radius=(0.5, 1.0), rho=2700.0):
+    """n distinct rocks (rock_hull, seed) as ensemble Shapes of density rho
+    (kg/m^3)."""
+    from . import ensemble as E
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        v, f = rock_hull(rng, n_pts[0], n_pts[1], radius[0], radius[1])
+        out.append(E.shape(v, f, rho * 1e-6))
+    return out
+
+
+def _mixed_placement(rng, sphere_sites, rock_sites, n_spheres, n_rocks, r_min, r_max, rock_rb,
+                     height_axis, gap=0.02):
+    """Rocks at n_rocks random sites of the rock lattice below a level h
+    (rock k gets bounding radius rock_rb[k]), spheres (radii drawn per
+    sphere site, U[r_min, r_max]) at the lowest n_spheres sites below h whose
+    sphere keeps `gap` from every rock's bounding sphere: the lowest level
+    (in steps of 0.5 cm) where both fit.  Returns (sphere centres, their
+    radii, rock centres)."""
+    from scipy.spatial import cKDTree
+    rs = rng.uniform(r_min, r_max, len(sphere_sites))
+    ys = sphere_sites[:, height_axis]
+    yr = rock_sites[:, height_axis]
+    rb = np.asarray(rock_rb, np.float64)
+    reach = r_max + (rb.max() if len(rb) else 0.0) + gap
+    h = min(ys.min(), yr.min())
+    top = max(ys.max(), yr.max()) + 1.0
+    while h <= top:
+        cand = np.nonzero(yr < h)[0]
+        if len(cand) >= n_rocks:
+            sub = np.random.default_rng(int(rng.integers(1 << 31)))
+            pick = np.sort(sub.choice(cand, n_rocks, replace=False))
+            rocks = rock_sites[pick]
+            ok = ys < h
+            if n_rocks:
+                kq = min(16, n_rocks)
+                d, k = cKDTree(rocks).query(sphere_sites, k=kq, distance_upper_bound=reach)
+                d, k = d.reshape(len(rs), kq), k.reshape(len(rs), kq)
+                hit = k < n_rocks
+                lim = rs[:, None] + rb[np.minimum(k, n_rocks - 1)] + gap
+                ok &= ~np.any(hit & (d <= lim), axis=1)
+            idx = np.nonzero(ok)[0]
+            if len(idx) >= n_spheres:
+                idx = idx[np.argsort(ys[idx], kind="stable")][:n_spheres]
+                return sphere_sites[idx], rs[idx], rocks
+        h += 0.5
+    raise ValueError("the charge of %d spheres and %d rocks does not fit" % (n_spheres, n_rocks))
+
+
+def _bounding_radius(s):
+    return float(np.linalg.norm(np.asarray(s.verts).reshape(-1, 3)[:s.nverts], axis=1).max())
+
+
+def mixed_charge_state(sph, sph_r, rocks, shapes, rng):
+    """Caller arrays of a mixed charge: spheres first, then rocks (shape k
+    for rock k, random orientations).  Returns (pos, radius, shape_of, quat)."""
+    ns, nr = len(sph), len(rocks)
+    pos = np.concatenate([sph, rocks]).astype(np.float32)
+    rad = np.concatenate([sph_r, [_bounding_radius(s) for s in shapes[:nr]]])
+    shape_of = np.concatenate([np.full(ns, -1), np.arange(nr)]).astype(np.int32)
+    quat = np.zeros((ns + nr, 4), np.float32)
+    quat[:ns, 0] = 1.0
+    quat[ns:] = random_quaternions(rng, nr)
+    return pos, rad.astype(np.float32), shape_of, quat
+
+
+def mixed_box_ensemble(n_spheres=300, n_rocks=24, L=10.0, H=20.0, r_min=0.3, r_max=0.6,
+                       rock_radius=(0.5, 1.0), rho=7800.0, rock_rho=2700.0, kn=1e6,
+                       restitution=0.4, mu=0.6, skin=0.04, seed=2, gravity=(0.0, 0.0, -981.0)):
+    """Steel balls and rocks in a closed box [0, L]^2 x [0, H] (six planes):
+    rocks (rock_shapes, seed) at random sites of a lattice of pitch 2 R_max,
+    balls r ~ U[r_min, r_max] on a lattice of pitch 2 r_max + skin / 2 clear
+    of the rocks, at rest; linear law kn (kt = 2/7 kn), restitution, mu.
+    Returns (systems, walls, pos, radius, shapes, shape_of, quat)."""
+    rng = np.random.default_rng(seed)
+    shapes = rock_shapes(n_rocks, seed=seed, radius=rock_radius, rho=rock_rho)
+    rbs = [_bounding_radius(x) for x in shapes]
+    rb = max([0.0] + rbs)
+    cell = 2.0 * max(r_max, rb) + skin + 1e-3
+    walls = box_walls(L, H)
+    s = box_system(n_spheres + n_rocks, L, H, cell, 0, density=rho * 1e-6, kn=kn,
+                   restitution=restitution, mu=mu, gravity=gravity)
+    m = 0.05
+    sph = lattice_fill(None, (r_max + m,) * 2 + (r_max + m,), (L - r_max - m,) * 2 + (H - r_max - m,),
+                       2.0 * r_max + 0.5 * skin, rng)
+    rk = lattice_fill(None, (rock_radius[1] + m,) * 2 + (rock_radius[1] + m,),
+                      (L - rock_radius[1] - m,) * 2 + (H - rock_radius[1] - m,),
+                      2.0 * rock_radius[1] + 0.1, rng)
+    sph, sph_r, rocks = _mixed_placement(rng, sph, rk, n_spheres, n_rocks, r_min, r_max, rbs, 2)
+    pos, rad, shape_of, quat = mixed_charge_state(sph, sph_r, rocks, shapes, rng)
+    return [s], walls, pos, rad, shapes, shape_of, quat
+
+
+def mill_mixed_ensemble(n_spheres=100_000, n_rocks=5_000, R=50.0, L=30.0, n_seg=232, n_len=32,
+                        n_lifters=8, lifter_w=4.0, lifter_h=4.0, r_min=0.3, r_max=0.6,
+                        rho=7800.0, rock_radius=(0.5, 1.0), rock_rho=2700.0, kn=1e6,
+                        restitution=0.4, mu=0.6, rpm=30.0, skin=0.04, seed=2,
+                        gravity=(0.0, -981.0, 0.0)):
+    """The ball mill's mixed charge: the drum and lifters as a turning mesh
+    (drum_mesh_triangles, end plates as planes turning in place) with steel
+    balls r ~ U[r_min, r_max] (density rho) and rocks (rock_shapes: hulls of
+    8-16 points on spheres of radius rock_radius, seed, density rock_rho),
+    the count ratio of the configuration's 2,000,000 : 100,000; rocks at
+    random sites of a lattice of pitch 2 R_max + 0.1, balls on a lattice of
+    pitch 2 r_max + skin / 2 clear of them, inside the lifter ring from the
+    bottom up, at rest; linear law kn (kt = 2/7 kn), restitution, mu, rpm
+    about z.  Returns (systems, walls, pos, radius, shapes, shape_of, quat)."""
+    from . import ensemble as E
+    rng = np.random.default_rng(seed)
+    shapes = rock_shapes(n_rocks, seed=seed, radius=rock_radius, rho=rock_rho)
+    rbs = [_bounding_radius(x) for x in shapes]
+    rb = max([0.0] + rbs)
+    tris = drum_mesh_triangles(R, L, n_seg, n_len, n_lifters, lifter_w, lifter_h, end_fans=False)
+    walls = [E.plane((0, 0, 1), 0.0), E.plane((0, 0, -1), -L)] + [E.triangle(*t) for t in tris]
+    s = E.System()
+    s.n = int(n_spheres + n_rocks)
+    cell = 2.0 * max(r_max, rb) + skin + 1e-3
+    for k, (o, ext) in enumerate(zip((-R - cell, -R - cell, -cell),
+                                     (2 * R + 2 * cell, 2 * R + 2 * cell, L + 2 * cell))):
+        s.origin[k] = o
+        s.ncells[k] = int(math.ceil(ext / cell))
+    s.cell = cell
+    for k in range(3):
+        s.gravity[k] = gravity[k]
+    s.density = rho * 1e-6
+    s.kn, s.kt_ratio, s.youngs, s.poisson = kn, 2.0 / 7.0, 0.0, 0.3
+    s.restitution, s.mu, s.mu_wall, s.mu_roll = restitution, mu, mu, 0.0
+    s.wall0, s.nwalls, s.tri0, s.ntris = 0, 2, 2, len(tris)
+    s.rot_axis[2] = 1.0
+    s.rot_omega = -rpm * 2.0 * math.pi / 60.0
+    r_in = R - lifter_h - 1.0
+    m = 0.05
+    sph = lattice_fill(None, (-r_in, -r_in, r_max + m), (r_in, r_in, L - r_max - m),
+                       2.0 * r_max + 0.5 * skin, rng)
+    sph = sph[np.hypot(sph[:, 0], sph[:, 1]) < r_in - r_max]
+    rk = lattice_fill(None, (-r_in, -r_in, rock_radius[1] + m),
+                      (r_in, r_in, L - rock_radius[1] - m), 2.0 * rock_radius[1] + 0.1, rng)
+    rk = rk[np.hypot(rk[:, 0], rk[:, 1]) < r_in - rock_radius[1]]
+    sph, sph_r, rocks = _mixed_placement(rng, sph, rk, n_spheres, n_rocks, r_min, r_max, rbs, 1)
+    pos, rad, shape_of, quat = mixed_charge_state(sph, sph_r, rocks, shapes, rng)
+    return [s], walls, pos, rad, shapes, shape_of, quat

@@ -5,13 +5,16 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "blaze_dem.h"
 #include "blaze_ens.h"
 #include "ens_adjoint.cuh"
 #include "ens_kernels.cuh"
+#include "mix_kernels.cuh"
 #include "radix_sort.cuh"
 
 using namespace blaze;
@@ -78,6 +81,23 @@ struct blaze_ens {
   uint32_t status = 0;
   int last_launches = 0;
   bool state_set = false;
+  bool stepped = false;       // a step since the last set_state
+  // polyhedra (blaze_ens_set_polyhedra); npoly 0: spheres only
+  int npoly = 0, poly_cap = 0, shape_cap = 0;
+  MixShapeDev* d_shapes = nullptr;
+  float4* d_bv = nullptr;
+  double4* d_bn = nullptr;
+  uchar4* d_faces = nullptr;
+  uchar4* d_edges = nullptr;
+  int* d_shape_of = nullptr;
+  int* d_pidx = nullptr;
+  float4* d_quat = nullptr;
+  float4* d_quat0 = nullptr;
+  int* d_pat = nullptr;
+  float* d_ppath = nullptr;
+  double4* d_gv = nullptr;
+  double4* d_gf = nullptr;
+  MixList ml[2] = {};
 };
 
 namespace {
@@ -97,7 +117,35 @@ EnsGeom geom(const blaze_ens* e) {
     if (w.kind != kWallPlane) g.curved = 1;
   g.rot = e->d_rot;
   g.any_rot = e->any_rot ? 1 : 0;
+  g.mix = MixView{};
+  if (e->npoly > 0) {
+    g.mix.shapes = e->d_shapes;
+    g.mix.shape_of = e->d_shape_of;
+    g.mix.gv = e->d_gv;
+    g.mix.gf = e->d_gf;
+    g.mix.faces = e->d_faces;
+    g.mix.npoly = e->npoly;
+  }
   return g;
+}
+
+MixBufs mix_bufs(const blaze_ens* e) {
+  MixBufs m;
+  m.shapes = e->d_shapes;
+  m.bv = e->d_bv;
+  m.bn = e->d_bn;
+  m.faces = e->d_faces;
+  m.edges = e->d_edges;
+  m.shape_of = e->d_shape_of;
+  m.quat = e->d_quat;
+  m.pat = e->d_pat;
+  m.ppath = e->d_ppath;
+  m.gv = e->d_gv;
+  m.gf = e->d_gf;
+  m.L[0] = e->ml[0];
+  m.L[1] = e->ml[1];
+  m.npoly = e->npoly;
+  return m;
 }
 
 // Per-system constants of the contact law, in double, rounded once to float.
@@ -257,6 +305,12 @@ void free_ens(blaze_ens* e) {
   f(e->d_sys); f(e->d_walls); f(e->d_tri_off); f(e->d_tri_ids); f(e->d_sys_of);
   f(e->st_pos3); f(e->st_rad); f(e->st_vel3); f(e->st_avel3); f(e->st_sys); f(e->st_pid);
   f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw); f(e->d_rot);
+  f(e->d_shapes); f(e->d_bv); f(e->d_bn); f(e->d_faces); f(e->d_edges); f(e->d_shape_of);
+  f(e->d_pidx); f(e->d_quat); f(e->d_quat0); f(e->d_pat); f(e->d_ppath); f(e->d_gv); f(e->d_gf);
+  for (int k = 0; k < 2; ++k) {
+    f(e->ml[k].idx); f(e->ml[k].cnt); f(e->ml[k].mlo); f(e->ml[k].mhi);
+    f(e->ml[k].hx); f(e->ml[k].hy); f(e->ml[k].hz);
+  }
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->h_flags) cudaFreeHost(e->h_flags);
   if (e->aux2) cudaStreamDestroy(e->aux2);
@@ -303,25 +357,35 @@ int enqueue_rebuild(blaze_ens* e, const int* gate, cudaStream_t st) {
   ens_launch_reorder(e->b, e->cur, n, e->rs.keys[res], e->rs.vals[res], e->cstart, e->cend,
                      e->ncell_tab, e->ctl, gate, st);
   ens_launch_nlist(g, e->b, n, e->rs.vals[res], e->cstart, e->cend, e->ctl, gate, st);
+  if (e->npoly > 0) mix_launch_plist(g, e->b, mix_bufs(e), e->cstart, e->cend, e->ctl, gate, st);
   ens_launch_epoch(e->ctl, gate, st);
   return 0;
 }
 
 int rebuild_kernel_count(const blaze_ens* e) {
-  return 4 + 3 * std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits);
+  return 4 + 3 * std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits) + (e->npoly > 0 ? 1 : 0);
+}
+
+// The step's kernels: polyhedron geometry, the sphere step, the polyhedron
+// step (the last two read the same input state and write disjoint entries).
+void launch_step_kernels(blaze_ens* e, StepLink link, cudaStream_t st) {
+  const EnsCapture* cap = e->opt.capture_forces ? &e->cap : nullptr;
+  if (e->npoly > 0) mix_launch_geom(mix_bufs(e), st);
+  ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, cap, e->opt.block, st);
+  if (e->npoly > 0) mix_launch_poly_step(geom(e), e->b, mix_bufs(e), e->cur, e->ctl, link, cap, st);
+}
+
+int step_kernel_count(const blaze_ens* e) {
+  return 1 + (e->npoly > 0 ? 2 : 0) + (e->any_rot ? 1 : 0);
 }
 
 int enqueue_step(blaze_ens* e) {
   launch_gate(e->ctl, e->stream);
   int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
   if (rc) return rc;
-  ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, StepLink{&e->ctl->rebuilt, 0, 0},
-                  e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
-  e->last_launches += 2 + rebuild_kernel_count(e);
-  if (e->any_rot) {
-    ens_launch_rot_tick(geom(e), e->nsys, e->stream);
-    e->last_launches += 1;
-  }
+  launch_step_kernels(e, StepLink{&e->ctl->rebuilt, 0, 0}, e->stream);
+  if (e->any_rot) ens_launch_rot_tick(geom(e), e->nsys, e->stream);
+  e->last_launches += 1 + step_kernel_count(e) + rebuild_kernel_count(e);
   e->cur ^= 1;
   return 0;
 }
@@ -366,8 +430,7 @@ int build_graph(blaze_ens* e, int c) {
     if (rc) return rc;
     const StepLink link = k + 1 < kGraphSteps ? StepLink{e->d_rb + k, h[k + 1], 1}
                                                : StepLink{e->d_rb + k, 0, 0};
-    ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link,
-                    e->opt.capture_forces ? &e->cap : nullptr, e->opt.block, e->stream);
+    launch_step_kernels(e, link, e->stream);
     if (e->any_rot) ens_launch_rot_tick(geom(e), e->nsys, e->stream);
     e->cur ^= 1;
   }
@@ -740,6 +803,13 @@ int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, co
   CK(cudaMemcpyAsync(e->ctl, e->h_ctl, sizeof(StepCtl), cudaMemcpyHostToDevice, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   e->state_set = true;
+  e->stepped = false;
+  if (e->npoly > 0) {   // spheres only again: the graphs hold the polyhedron kernels
+    e->npoly = 0;
+    e->b.pat = nullptr;
+    e->b.ppath = nullptr;
+    drop_graphs(e);
+  }
   return 0;
 }
 
@@ -771,7 +841,8 @@ namespace {
 // remainder as plain steps).
 int advance(blaze_ens* e, int nsteps, bool graphs) {
   // persistent stepping (no drum turns: those advance between steps)
-  if (graphs && e->opt.use_graph == 2 && !e->opt.capture_forces && !e->any_rot && nsteps > 0) {
+  if (graphs && e->opt.use_graph == 2 && !e->opt.capture_forces && !e->any_rot && e->npoly == 0 &&
+      nsteps > 0) {
     const int c = e->cur;
     if (!e->pgraph[c]) {
       int rc = build_persist_graph(e, c);
@@ -796,7 +867,7 @@ int advance(blaze_ens* e, int nsteps, bool graphs) {
       if (rc) return rc;
     }
     CK(cudaGraphLaunch(e->graph[c], e->stream));
-    e->last_launches += 1 + kGraphSteps * (e->any_rot ? 2 : 1);
+    e->last_launches += 1 + kGraphSteps * step_kernel_count(e);
     if (kGraphSteps & 1) e->cur ^= 1;
     done += kGraphSteps;
   }
@@ -829,6 +900,7 @@ int blaze_ens_check_barrier_timeout(void) {
 int blaze_ens_step(blaze_ens* e, int nsteps) {
   if (!e || nsteps < 0 || !e->state_set) return -1;
   e->last_launches = 0;
+  if (nsteps > 0) e->stepped = true;
   return advance(e, nsteps, e->opt.use_graph != 0);
 }
 
@@ -890,6 +962,284 @@ int blaze_ens_rebuild_kernels(blaze_ens* e) {
   if (!e) return -1;
   // persistent stepping: a re-sort also starts another round (gate + step)
   return rebuild_kernel_count(e) + (e->opt.use_graph == 2 ? 2 : 0);
+}
+
+}  // extern "C"
+
+// ============================================================== polyhedra
+namespace {
+
+struct ShapeHost {
+  MixShapeDev dev;
+  float4 bv[kMixMaxV];
+  double4 bn[kMixMaxF];
+  uchar4 faces[kMixMaxF];
+  uchar4 edges[kMixMaxE];
+  double mass, com[3], J[9], rb;
+};
+
+// A closed, outward-oriented convex hull of triangles (every directed edge
+// once, its reverse once; V - E + F = 2; every vertex on or below every face
+// plane), its unit face normals, its edges (vertex i < j, in (i, j) order,
+// faces f1 < f2) and its mass properties, in FP64: volume, centre of mass
+// and inertia from the tetrahedra of the faces with the origin
+// (covariance of a tetrahedron (0, a, b, c): det / 120 (a a^T + b b^T +
+// c c^T + s s^T), s = a + b + c; inertia = tr(C) 1 - C, moved to the centre
+// of mass).
+bool shape_setup(const blaze_shape& s, ShapeHost& o) {
+  std::memset(&o, 0, sizeof(o));
+  const int nv = s.nverts, nf = s.nfaces;
+  if (nv < 4 || nv > kMixMaxV || nf != 2 * nv - 4 || !(s.density > 0.0f) ||
+      !std::isfinite(s.density))
+    return false;
+  double v[kMixMaxV][3];
+  for (int k = 0; k < nv; ++k)
+    for (int c = 0; c < 3; ++c) {
+      if (!std::isfinite(s.verts[3 * k + c])) return false;
+      v[k][c] = (double)s.verts[3 * k + c];
+    }
+  std::map<std::pair<int, int>, int> dir;
+  for (int f = 0; f < nf; ++f) {
+    const int a = s.faces[3 * f], b = s.faces[3 * f + 1], c = s.faces[3 * f + 2];
+    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv || a == b || b == c || a == c)
+      return false;
+    const int ed[3][2] = {{a, b}, {b, c}, {c, a}};
+    for (int k = 0; k < 3; ++k) {
+      const std::pair<int, int> key(ed[k][0], ed[k][1]);
+      if (dir.count(key)) return false;
+      dir[key] = f;
+    }
+    o.faces[f] = make_uchar4((unsigned char)a, (unsigned char)b, (unsigned char)c, 0);
+    const double e1[3] = {v[b][0] - v[a][0], v[b][1] - v[a][1], v[b][2] - v[a][2]};
+    const double e2[3] = {v[c][0] - v[a][0], v[c][1] - v[a][1], v[c][2] - v[a][2]};
+    const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                          e1[0] * e2[1] - e1[1] * e2[0]};
+    const double l = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    if (!(l > 0.0)) return false;
+    o.bn[f] = make_double4(cr[0] / l, cr[1] / l, cr[2] / l, 0.0);
+  }
+  int ne = 0;
+  for (const auto& kv : dir) {
+    const int a = kv.first.first, b = kv.first.second;
+    const auto rev = dir.find(std::make_pair(b, a));
+    if (rev == dir.end()) return false;
+    if (a > b) continue;
+    if (ne >= kMixMaxE) return false;
+    const int f1 = std::min(kv.second, rev->second), f2 = std::max(kv.second, rev->second);
+    o.edges[ne++] = make_uchar4((unsigned char)a, (unsigned char)b, (unsigned char)f1,
+                                (unsigned char)f2);
+  }
+  if (ne != 3 * nv - 6 || nv - ne + nf != 2) return false;
+  double rb = 0.0;
+  for (int k = 0; k < nv; ++k)
+    rb = std::max(rb, std::sqrt(v[k][0] * v[k][0] + v[k][1] * v[k][1] + v[k][2] * v[k][2]));
+  for (int f = 0; f < nf; ++f) {
+    const double* n = &o.bn[f].x;
+    const double* p0 = v[o.faces[f].x];
+    const double h = n[0] * p0[0] + n[1] * p0[1] + n[2] * p0[2];
+    for (int k = 0; k < nv; ++k)
+      if (n[0] * v[k][0] + n[1] * v[k][1] + n[2] * v[k][2] - h > 1e-6 * rb) return false;
+  }
+  double vol = 0.0, cen[3] = {0.0, 0.0, 0.0}, C[9] = {0.0};
+  for (int f = 0; f < nf; ++f) {
+    const double* a = v[o.faces[f].x];
+    const double* b = v[o.faces[f].y];
+    const double* c = v[o.faces[f].z];
+    const double det = a[0] * (b[1] * c[2] - b[2] * c[1]) + a[1] * (b[2] * c[0] - b[0] * c[2]) +
+                       a[2] * (b[0] * c[1] - b[1] * c[0]);
+    vol += det / 6.0;
+    double sm[3];
+    for (int q = 0; q < 3; ++q) {
+      sm[q] = a[q] + b[q] + c[q];
+      cen[q] += det * sm[q] / 24.0;
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        C[3 * r + q] += det / 120.0 * (a[r] * a[q] + b[r] * b[q] + c[r] * c[q] + sm[r] * sm[q]);
+  }
+  if (!(vol > 0.0)) return false;
+  const double rho = (double)s.density;
+  o.mass = rho * vol;
+  for (int q = 0; q < 3; ++q) o.com[q] = cen[q] / vol;
+  const double tr = C[0] + C[4] + C[8];
+  const double c2 = o.com[0] * o.com[0] + o.com[1] * o.com[1] + o.com[2] * o.com[2];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q)
+      o.J[3 * r + q] = rho * ((r == q ? tr : 0.0) - C[3 * r + q]) -
+                       o.mass * ((r == q ? c2 : 0.0) - o.com[r] * o.com[q]);
+  const double* J = o.J;
+  const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                     J[2] * (J[3] * J[7] - J[4] * J[6]);
+  if (!(det > 0.0)) return false;
+  const double inv[9] = {(J[4] * J[8] - J[5] * J[7]) / det, (J[2] * J[7] - J[1] * J[8]) / det,
+                         (J[1] * J[5] - J[2] * J[4]) / det, (J[5] * J[6] - J[3] * J[8]) / det,
+                         (J[0] * J[8] - J[2] * J[6]) / det, (J[2] * J[3] - J[0] * J[5]) / det,
+                         (J[3] * J[7] - J[4] * J[6]) / det, (J[1] * J[6] - J[0] * J[7]) / det,
+                         (J[0] * J[4] - J[1] * J[3]) / det};
+  o.rb = rb;
+  float rbf = (float)rb;
+  if ((double)rbf < rb) rbf = std::nextafter(rbf, INFINITY);
+  o.dev.nv = nv;
+  o.dev.nf = nf;
+  o.dev.ne = ne;
+  o.dev.mass = (float)o.mass;
+  o.dev.rb = rbf;
+  for (int q = 0; q < 9; ++q) {
+    o.dev.inertia[q] = (float)J[q];
+    o.dev.iinv[q] = (float)inv[q];
+  }
+  for (int k = 0; k < nv; ++k)
+    o.bv[k] = make_float4(s.verts[3 * k], s.verts[3 * k + 1], s.verts[3 * k + 2], 0.0f);
+  return true;
+}
+
+// A device array of `count` elements in place of the old one.
+template <class T>
+int realloc_dev(T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  CK(dalloc(p, count));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int blaze_shape_mass_properties(const blaze_shape* s, double* mass, double* com3,
+                                double* inertia9, float* rbound) {
+  if (!s) return -1;
+  ShapeHost h;
+  if (!shape_setup(*s, h)) return -1;
+  if (mass) *mass = h.mass;
+  if (com3)
+    for (int q = 0; q < 3; ++q) com3[q] = h.com[q];
+  if (inertia9)
+    for (int q = 0; q < 9; ++q) inertia9[q] = h.J[q];
+  if (rbound) *rbound = h.dev.rb;
+  return 0;
+}
+
+int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes,
+                            const int* shape_of, const float* quat4) {
+  if (!e || !shapes || nshapes < 1 || !shape_of || !quat4) return -1;
+  if (!e->state_set || e->stepped || e->opt.law != BLAZE_LAW_LINEAR) return -1;
+  std::vector<ShapeHost> hs(nshapes);
+  for (int k = 0; k < nshapes; ++k) {
+    if (!shape_setup(shapes[k], hs[k])) return -1;
+    const double* c = hs[k].com;
+    if (std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) > 1e-4 * hs[k].rb) return -1;
+  }
+  std::vector<int> pidx, pshape;
+  std::vector<float4> q0;
+  int i = 0;
+  for (int sy = 0; sy < e->nsys; ++sy) {
+    const blaze_system& S = e->sys[sy];
+    for (int k = 0; k < S.n; ++k, ++i) {
+      const int sh = shape_of[i];
+      if (sh < 0) continue;
+      if (sh >= nshapes) return -1;
+      if (2.0f * hs[sh].dev.rb + e->opt.skin > S.cell) return -1;
+      for (int w = S.wall0; w < S.wall0 + S.nwalls; ++w)
+        if (e->hwalls[w].kind != kWallPlane) return -1;
+      const double qw = quat4[4 * i], qx = quat4[4 * i + 1], qy = quat4[4 * i + 2],
+                   qz = quat4[4 * i + 3];
+      const double qn = std::sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
+      if (!(qn > 0.0) || !std::isfinite(qn)) return -1;
+      pidx.push_back(i);
+      pshape.push_back(sh);
+      q0.push_back(make_float4((float)(qw / qn), (float)(qx / qn), (float)(qy / qn),
+                               (float)(qz / qn)));
+    }
+  }
+  int rc = sync_status(e);
+  if (rc < 0) return rc;
+  const int np = (int)pidx.size();
+  drop_graphs(e);
+  e->npoly = 0;
+  e->b.pat = nullptr;
+  e->b.ppath = nullptr;
+  if (np == 0) return 0;
+  if (nshapes > e->shape_cap) {
+    if ((rc = realloc_dev(&e->d_shapes, (size_t)nshapes)) || (rc = realloc_dev(&e->d_bv, (size_t)nshapes * kMixMaxV)) ||
+        (rc = realloc_dev(&e->d_bn, (size_t)nshapes * kMixMaxF)) ||
+        (rc = realloc_dev(&e->d_faces, (size_t)nshapes * kMixMaxF)) ||
+        (rc = realloc_dev(&e->d_edges, (size_t)nshapes * kMixMaxE)))
+      return rc;
+    e->shape_cap = nshapes;
+  }
+  if (np > e->poly_cap) {
+    if ((rc = realloc_dev(&e->d_shape_of, (size_t)np)) || (rc = realloc_dev(&e->d_pidx, (size_t)np)) ||
+        (rc = realloc_dev(&e->d_quat, (size_t)np)) || (rc = realloc_dev(&e->d_quat0, (size_t)np)) ||
+        (rc = realloc_dev(&e->d_pat, (size_t)np)) || (rc = realloc_dev(&e->d_ppath, (size_t)np)) ||
+        (rc = realloc_dev(&e->d_gv, (size_t)np * kMixMaxV)) || (rc = realloc_dev(&e->d_gf, (size_t)np * kMixMaxF)))
+      return rc;
+    for (int k = 0; k < 2; ++k) {
+      MixList& L = e->ml[k];
+      if ((rc = realloc_dev(&L.idx, (size_t)np * kMixSlots)) || (rc = realloc_dev(&L.cnt, (size_t)np)) ||
+          (rc = realloc_dev(&L.mlo, (size_t)np)) || (rc = realloc_dev(&L.mhi, (size_t)np)) ||
+          (rc = realloc_dev(&L.hx, (size_t)np * kMixSlots)) || (rc = realloc_dev(&L.hy, (size_t)np * kMixSlots)) ||
+          (rc = realloc_dev(&L.hz, (size_t)np * kMixSlots)))
+        return rc;
+    }
+    e->poly_cap = np;
+  }
+  {
+    std::vector<MixShapeDev> sd(nshapes);
+    std::vector<float4> bv((size_t)nshapes * kMixMaxV, make_float4(0, 0, 0, 0));
+    std::vector<double4> bn((size_t)nshapes * kMixMaxF, make_double4(0, 0, 0, 0));
+    std::vector<uchar4> fa((size_t)nshapes * kMixMaxF, make_uchar4(0, 0, 0, 0));
+    std::vector<uchar4> ed((size_t)nshapes * kMixMaxE, make_uchar4(0, 0, 0, 0));
+    for (int k = 0; k < nshapes; ++k) {
+      sd[k] = hs[k].dev;
+      std::copy(hs[k].bv, hs[k].bv + kMixMaxV, bv.begin() + (size_t)k * kMixMaxV);
+      std::copy(hs[k].bn, hs[k].bn + kMixMaxF, bn.begin() + (size_t)k * kMixMaxF);
+      std::copy(hs[k].faces, hs[k].faces + kMixMaxF, fa.begin() + (size_t)k * kMixMaxF);
+      std::copy(hs[k].edges, hs[k].edges + kMixMaxE, ed.begin() + (size_t)k * kMixMaxE);
+    }
+    CK(cudaMemcpy(e->d_shapes, sd.data(), sizeof(MixShapeDev) * nshapes, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_bv, bv.data(), sizeof(float4) * bv.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_bn, bn.data(), sizeof(double4) * bn.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_faces, fa.data(), sizeof(uchar4) * fa.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_edges, ed.data(), sizeof(uchar4) * ed.size(), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(e->d_shape_of, pshape.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->d_pidx, pidx.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->d_quat0, q0.data(), sizeof(float4) * np, cudaMemcpyHostToDevice));
+  CK(cudaMemset(e->d_gv, 0, sizeof(double4) * (size_t)np * kMixMaxV));
+  CK(cudaMemset(e->d_gf, 0, sizeof(double4) * (size_t)np * kMixMaxF));
+  e->npoly = np;
+  e->b.pat = e->d_pat;
+  e->b.ppath = e->d_ppath;
+  mix_launch_mark(e->b, e->cur, mix_bufs(e), e->d_pidx, e->d_quat0, e->stream);
+  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int blaze_ens_get_orientations(blaze_ens* e, float* quat4) {
+  if (!e || !quat4) return -1;
+  int st = sync_status(e);
+  if (st < 0) return st;
+  const int n = e->n;
+  std::vector<float4> pos(n), angv(n), q(std::max(e->npoly, 1));
+  CK(cudaMemcpy(pos.data(), e->b.S[e->cur].pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(angv.data(), e->b.S[e->cur].angv, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  if (e->npoly > 0)
+    CK(cudaMemcpy(q.data(), e->d_quat, sizeof(float4) * e->npoly, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; ++i) {
+    float4 o = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+    if (e->npoly > 0 && pos[i].w < 0.0f) {
+      int p;
+      std::memcpy(&p, &angv[i].w, sizeof(int));
+      if (p >= 0 && p < e->npoly) o = q[p];
+    }
+    quat4[4 * i] = o.x;
+    quat4[4 * i + 1] = o.y;
+    quat4[4 * i + 2] = o.z;
+    quat4[4 * i + 3] = o.w;
+  }
+  return st;
 }
 
 }  // extern "C"
@@ -1140,7 +1490,7 @@ extern "C" {
 
 int blaze_ens_adj_create_tape(blaze_ens_adj** out, blaze_ens* e, int nsteps, int segment,
                               unsigned long long arena_bytes) {
-  if (!out || !e || nsteps < 1 || segment < 1) return -1;
+  if (!out || !e || nsteps < 1 || segment < 1 || e->npoly > 0) return -1;
   const unsigned long long aw = arena_bytes / 4 & ~3ull;
   if (aw < (unsigned long long)std::min(segment, nsteps) * tape_block_words(e->n)) return -2;
   if (e->opt.law != BLAZE_LAW_LINEAR || e->any_rot) return -1;

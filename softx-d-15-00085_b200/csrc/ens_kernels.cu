@@ -23,6 +23,8 @@
 //   capped force).  Rolling friction: a torque -mu_r max(f_n, 0) R* w_rel / |w_rel|.
 //   Walls use the same law with R* = r, m* = m.
 #include "ens_kernels.cuh"
+#include "ens_device.cuh"
+#include "mix_device.cuh"
 #include "dem_laws.cuh"
 
 #include <algorithm>
@@ -31,189 +33,6 @@ namespace blaze {
 namespace {
 
 constexpr int kThreads = 256;
-
-__device__ __forceinline__ void ens_flag(StepCtl* ctl, uint32_t bits) {
-  const unsigned m = __activemask();
-  const uint32_t all = __reduce_or_sync(m, bits);
-  if (all && (threadIdx.x & 31) == (__ffs(m) - 1)) atomicOr(&ctl->status, all);
-}
-
-__device__ __forceinline__ int3 ens_cell(const EnsSysDev& S, float3 p) {
-  int3 c;
-  c.x = (int)floorf((p.x - S.origin.x) / S.cell);
-  c.y = (int)floorf((p.y - S.origin.y) / S.cell);
-  c.z = (int)floorf((p.z - S.origin.z) / S.cell);
-  return c;
-}
-__device__ __forceinline__ bool ens_in(const EnsSysDev& S, int3 c) {
-  return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < S.nc.x && c.y < S.nc.y && c.z < S.nc.z;
-}
-__device__ __forceinline__ uint32_t ens_key(const EnsSysDev& S, int3 c) {
-  return S.cell_off + (uint32_t)(c.x + S.nc.x * (c.y + S.nc.y * c.z));
-}
-// v turned by the angle with cosine c and sine s about the unit axis a
-// (Rodrigues): v c + (a x v) s + a (a . v) (1 - c)
-__device__ __forceinline__ float3 rot_about(float3 a, float c, float s, float3 v) {
-  const float3 axv = cross3(a, v);
-  const float av = dot3(a, v);
-  return (v * c + axv * s) + a * (av * (1.0f - c));
-}
-
-__device__ __forceinline__ float sphere_mass(const EnsSysDev& S, float r) {
-  return S.dens43pi * ((r * r) * r);
-}
-
-// ------------------------------------------------------------- contact law
-template <int kLaw>
-__device__ __forceinline__ void contact_law(const EnsSysDev& S, float mu, float3 n, float delta,
-                                            float rs, float ms, float3 vrel, float3 vct,
-                                            float3 wrel, float arm, float dt, float3& xi,
-                                            float3& F, float3& T) {
-  const float vn = dot3(vrel, n);
-  float kn_e, cn, kt_e, ct;
-  if (kLaw == kLawLinear) {
-    kn_e = S.kn;
-    kt_e = S.kt;
-    cn = S.beta2 * sqrtf(ms * S.kn);
-    ct = S.beta2 * sqrtf(ms * S.kt);
-  } else {
-    const float sq = sqrtf(rs * delta);
-    const float sn = (2.0f * S.estar) * sq;
-    kn_e = 0.6666667f * sn;
-    kt_e = (8.0f * S.gstar) * sq;
-    cn = S.beta2h * sqrtf(sn * ms);
-    ct = S.beta2h * sqrtf(kt_e * ms);
-  }
-  const float fn = kn_e * delta - cn * vn;
-  const float fc = fn > 0.0f ? fn : 0.0f;  // compressive part: friction bound
-  const float3 vt = vct - dot3(vct, n) * n;
-  const float xn = dot3(xi, n);
-  if (xn != 0.0f) {
-    const float m0 = dot3(xi, xi);
-    xi = xi - xn * n;
-    const float m1 = dot3(xi, xi);
-    if (m1 > 0.0f) xi = xi * sqrtf(m0 / m1);
-  }
-  xi = xi + vt * dt;
-  float3 ft = xi * (-kt_e) - vt * ct;
-  const float cap = mu * fc;
-  const float f2 = dot3(ft, ft);
-  if (f2 > cap * cap) {
-    const float s = cap / sqrtf(f2);
-    ft = ft * s;
-    xi = (ft + vt * ct) * (-1.0f / kt_e);
-  }
-  F = n * fn + ft;
-  T = cross3(n * (-arm), F);
-  if (S.mu_r > 0.0f) {
-    const float w2 = dot3(wrel, wrel);
-    if (w2 > 0.0f) T = T + wrel * (-((S.mu_r * fc) * rs) / sqrtf(w2));
-  }
-}
-
-// Closest point of triangle (a, b, c) to p by Voronoi regions of the
-// vertices, edges and face (Ericson, Real-Time Collision Detection, 5.1.5).
-// region: 0 face interior, 1 edge, 2 vertex; feat: the vertex (0 a, 1 b,
-// 2 c) or edge (0 ab, 1 ac, 2 bc) it lies on.
-__device__ __forceinline__ float3 closest_on_triangle(float3 p, float3 a, float3 b, float3 c,
-                                                      int& region, int& feat) {
-  const float3 ab = b - a, ac = c - a, ap = p - a;
-  const float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
-  if (d1 <= 0.0f && d2 <= 0.0f) { region = 2; feat = 0; return a; }
-  const float3 bp = p - b;
-  const float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
-  if (d3 >= 0.0f && d4 <= d3) { region = 2; feat = 1; return b; }
-  const float vc = d1 * d4 - d3 * d2;
-  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-    region = 1;
-    feat = 0;
-    return a + ab * (d1 / (d1 - d3));
-  }
-  const float3 cp = p - c;
-  const float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
-  if (d6 >= 0.0f && d5 <= d6) { region = 2; feat = 2; return c; }
-  const float vb = d5 * d2 - d1 * d6;
-  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-    region = 1;
-    feat = 1;
-    return a + ac * (d2 / (d2 - d6));
-  }
-  const float va = d3 * d6 - d5 * d4;
-  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
-    region = 1;
-    feat = 2;
-    return b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
-  }
-  const float den = 1.0f / ((va + vb) + vc);
-  region = 0;
-  feat = 0;
-  return a + ab * (vb * den) + ac * (vc * den);
-}
-
-// Contact of a sphere (centre p, radius r) with one wall: normal from the
-// wall to the centre, overlap; false when not touching.  kCurved = false
-// compiles the plane test only (ensembles whose walls are all planes).
-template <bool kCurved>
-__device__ __forceinline__ bool wall_touch(const EnsWallDev& W, float3 p, float r, float3& n,
-                                           float& delta, int& region) {
-  region = 0;
-  // Walls first take a conservative FP32 test (its margin is ten times the
-  // FP32 rounding of the distance), so the FP64 overlap runs only near them.
-  const float mag = fabsf(p.x) + fabsf(p.y) + fabsf(p.z) + fabsf(W.r);
-  if (W.kind == kWallPlane) {
-    if (!(dot3(W.a, p) - W.r < r + 1e-6f * mag)) return false;
-    delta = overlap_plane(r, W.a, W.r, p);
-    if (!(delta > 0.0f)) return false;
-    n = W.a;
-    return true;
-  }
-  if constexpr (!kCurved) return false;
-  if (W.kind == kWallCylinder) {
-    {
-      const float3 v = p - W.a;
-      if (!(len3(v - dot3(v, W.b) * W.b) + r > W.r - 1e-6f * (mag + 2.0f * W.r))) return false;
-    }
-    // rad = v - (v . b) b with v = p - a, in double
-    const double3 v = dsub(d3(p), d3(W.a)), b = d3(W.b);
-    const double vb = ddot(v, b);
-    const double3 rad = make_double3(v.x - vb * b.x, v.y - vb * b.y, v.z - vb * b.z);
-    const double rho = sqrt(ddot(rad, rad));
-    delta = (float)(((double)r + rho) - (double)W.r);
-    if (!(delta > 0.0f) || !(rho > 0.0)) return false;
-    const float rinv = (float)(-1.0 / rho);
-    n = f3((float)rad.x * rinv, (float)rad.y * rinv, (float)rad.z * rinv);
-    return true;
-  }
-  int feat;
-  const float3 q = closest_on_triangle(p, W.a, W.b, W.c, region, feat);
-  const float3 d = p - q;
-  const float d2 = dot3(d, d);
-  if (!(d2 < r * r)) return false;
-  if (region == 0) {
-    // face: the signed distance (p - a) . n, n the unit normal in double
-    const double s = ddot(dsub(d3(p), d3(W.a)), W.n64);
-    delta = (float)((double)r - fabs(s));
-    if (!(delta > 0.0f) || !(s != 0.0)) return false;
-    const float sg = s < 0.0 ? -1.0f : 1.0f;
-    n = f3((float)W.n64.x * sg, (float)W.n64.y * sg, (float)W.n64.z * sg);
-    return true;
-  }
-  // vertex: p - v; edge: p - v0 less its part along the unit edge e
-  const float3 v0 = region == 2 ? (feat == 0 ? W.a : (feat == 1 ? W.b : W.c))
-                                : (feat == 2 ? W.b : W.a);
-  double3 pv = dsub(d3(p), d3(v0));
-  if (region == 1) {
-    const double3 e = W.e64[feat];
-    const double t = ddot(pv, e);
-    pv = make_double3(pv.x - t * e.x, pv.y - t * e.y, pv.z - t * e.z);
-  }
-  const double dist = sqrt(ddot(pv, pv));
-  delta = (float)((double)r - dist);
-  if (!(delta > 0.0f) || !(dist > 0.0)) return false;
-  const float dinv = (float)(1.0 / dist);
-  n = f3((float)pv.x * dinv, (float)pv.y * dinv, (float)pv.z * dinv);
-  return true;
-}
 
 // ------------------------------------------------------------------- hash
 __global__ void __launch_bounds__(kThreads)
@@ -246,11 +65,18 @@ k_ens_reorder(StateBuf src, StateBuf dst, EnsBufs b, int n, const uint32_t* __re
   if (i >= n) return;
   const int e = ctl->epoch & 1;
   const int j = perm[i];
-  dst.pos[i] = src.pos[j];
+  const float4 x = src.pos[j];
+  dst.pos[i] = x;
   const float4 v = src.vel[j];
   dst.vel[i] = v;
   float4 w = src.angv[j];
-  w.w = 0.0f;
+  if (x.w < 0.0f) {   // a polyhedron: angv.w is its id; its path restarts per id
+    const int pq = __float_as_int(w.w);
+    b.pat[pq] = i;
+    b.ppath[pq] = 0.0f;
+  } else {
+    w.w = 0.0f;
+  }
   dst.angv[i] = w;
   b.pid[e ^ 1][i] = b.pid[e][j];
   if ((__float_as_uint(v.w) >> kSysBits) != 0u) {
@@ -283,6 +109,11 @@ k_ens_nlist(EnsGeom g, EnsBufs b, const float4* __restrict__ pos, const float4* 
   const int* pid_new = b.pid[e ^ 1];
   const size_t stride = (size_t)b.stride;
   const float4 pa4 = pos[i];
+  if (pa4.w < 0.0f) {   // a polyhedron: its neighbours are listed by k_mix_plist
+    Ln.cnt[i] = 0;
+    Ln.mask[i] = 0;
+    return;
+  }
   const float3 pa = xyz(pa4);
   const float ra = pa4.w;
   const uint32_t sys = __float_as_uint(vel[i].w) & kSysMask;
@@ -308,7 +139,7 @@ k_ens_nlist(EnsGeom g, EnsBufs b, const float4* __restrict__ pos, const float4* 
             if ((int)j == i) continue;
             const float4 pb = __ldg(pos + j);
             const float3 rel = pa - xyz(pb);
-            const float lim = (ra + pb.w) + g.skin;
+            const float lim = (ra + fabsf(pb.w)) + g.skin;   // a polyhedron: its bounding radius
             if (!(dot3(rel, rel) < lim * lim)) continue;
             if (cnt < (uint32_t)b.cap) {
               Ln.idx[cnt * stride + i] = j;
@@ -487,7 +318,11 @@ __device__ __forceinline__ float ens_particle_step_ref(const EnsGeom& g, const E
 // Euler from `in` into `out`.  Raises status bits in st; returns the path
 // the particle has moved since the last re-sort.  kRecord: also writes what
 // the step reads into the tape view (histories to hrec when it is not null).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true, bool kRot = false>
+// kMix: the system holds polyhedra (linear law): a polyhedron's own entry is
+// skipped (k_mix_poly_step steps it), a polyhedron neighbour is met by the
+// sphere-hull test and the law of mix_pair_law.
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true, bool kRot = false,
+          bool kMix = false>
 __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBufs& b,
                                                    const StateBuf& in, const StateBuf& out,
                                                    int i, int e, const EnsList& L, TapeView tv,
@@ -499,6 +334,9 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
   const size_t stride = (size_t)b.stride;
   const float dt = g.dt;
   const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
+  if constexpr (kMix) {
+    if (pa4.w < 0.0f) return 0.0f;
+  }
   const float3 pa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
   const float ra = pa4.w;
   const uint32_t bits = __float_as_uint(va4.w);
@@ -534,7 +372,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
 #pragma unroll
     for (uint32_t u = 0; u < kEnsMaskBatch; ++u) {
       const float3 rel = pa - xyz(pb[u]);
-      const float sr = ra + pb[u].w;
+      const float sr = ra + (kMix ? fabsf(pb[u].w) : pb[u].w);
       const float d2 = dot3(rel, rel);
       if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f) cmask |= 1u << (k0 + u);
     }
@@ -545,6 +383,30 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     const size_t sk = (size_t)k * stride + i;
     const uint32_t j = L.idx[sk];
     const float4 pb4 = ld_state<kNc>(in.pos + j);
+    if constexpr (kMix) {
+      if (pb4.w < 0.0f) {
+        const float4 vb4 = ld_state<kNc>(in.vel + j), wb4 = ld_state<kNc>(in.angv + j);
+        const int q = __float_as_int(wb4.w);
+        const int sq = g.mix.shape_of[q];
+        const MixShapeDev& SH = g.mix.shapes[sq];
+        MixHit h;
+        if (!sphere_hull(pa, ra, xyz(pb4), g.mix.gv + (size_t)q * kMixMaxV,
+                         g.mix.gf + (size_t)q * kMixMaxF, g.mix.faces + (size_t)sq * kMixMaxF,
+                         SH.nf, h))
+          continue;
+        float3 xi = f3(0.0f, 0.0f, 0.0f);
+        if ((mask_o >> k) & 1u) xi = f3(L.hx[sk], L.hy[sk], L.hz[sk]);
+        float3 F, Ta, Tb;
+        mix_pair_law(S, h, ma, va, wa, SH.mass, xyz(vb4), xyz(wb4), dt, xi, F, Ta, Tb);
+        L.hx[sk] = xi.x;
+        L.hy[sk] = xi.y;
+        L.hz[sk] = xi.z;
+        mask |= 1u << k;
+        f = f + F;
+        t = t + Ta;
+        continue;
+      }
+    }
     const float3 rel = pa - xyz(pb4);
     const float rb = pb4.w;
     const float sr = ra + rb;
@@ -714,7 +576,8 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
 
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
 // history words are reserved first, by every thread of the block).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot = false>
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot = false,
+          bool kMix = false>
 __global__ void __launch_bounds__(kMaxStepBlock)
 k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
            StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
@@ -743,8 +606,8 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
   if (i >= n) return;
   uint32_t st = 0;
   const float path =
-      ens_particle_step<kLaw, kCapture, kRecord, kCurved, true, kRot>(g, b, in, out, i, e, L, tv,
-                                                                       hrec, cap, st);
+      ens_particle_step<kLaw, kCapture, kRecord, kCurved, true, kRot, kMix>(g, b, in, out, i, e, L,
+                                                                             tv, hrec, cap, st);
   {
     const unsigned m = __activemask();
     const unsigned req = __ballot_sync(m, path > 0.5f * g.skin);
@@ -927,7 +790,7 @@ k_ens_unpack(StateBuf s, const int* __restrict__ pid_src, int n, float* pos3, fl
   if (i >= n) return;
   const float4 p = s.pos[i], v = s.vel[i], w = s.angv[i];
   pos3[3 * i] = p.x; pos3[3 * i + 1] = p.y; pos3[3 * i + 2] = p.z;
-  rad[i] = p.w;
+  rad[i] = fabsf(p.w);   // a polyhedron: its bounding radius
   vel3[3 * i] = v.x; vel3[3 * i + 1] = v.y; vel3[3 * i + 2] = v.z;
   avel3[3 * i] = w.x; avel3[3 * i + 1] = w.y; avel3[3 * i + 2] = w.z;
   sys[i] = (int)(__float_as_uint(v.w) & kSysMask);
@@ -969,7 +832,19 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
 #define ENS_ARGS g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, c, EnsTape{}
 #define ENS_STEP(L, C, K) k_ens_step<L, C, false, K><<<gs, bs, 0, st>>>(ENS_ARGS)
 #define ENS_STEP_ROT(L, C) k_ens_step<L, C, false, true, true><<<gs, bs, 0, st>>>(ENS_ARGS)
-  if (g.curved && g.any_rot) {   // a turning drum
+#define ENS_STEP_MIX(C, K, R) k_ens_step<kLawLinear, C, false, K, R, true><<<gs, bs, 0, st>>>(ENS_ARGS)
+  if (g.mix.npoly > 0) {   // polyhedra among the spheres (linear law)
+    if (g.curved && g.any_rot) {
+      if (cap) ENS_STEP_MIX(true, true, true);
+      else ENS_STEP_MIX(false, true, true);
+    } else if (g.curved) {
+      if (cap) ENS_STEP_MIX(true, true, false);
+      else ENS_STEP_MIX(false, true, false);
+    } else {
+      if (cap) ENS_STEP_MIX(true, false, false);
+      else ENS_STEP_MIX(false, false, false);
+    }
+  } else if (g.curved && g.any_rot) {   // a turning drum
     if (g.law == kLawHertz) {
       if (cap) ENS_STEP_ROT(kLawHertz, true);
       else ENS_STEP_ROT(kLawHertz, false);
@@ -997,6 +872,7 @@ void ens_launch_step(const EnsGeom& g, const EnsBufs& b, int cur, int n, StepCtl
       else ENS_STEP(kLawLinear, false, false);
     }
   }
+#undef ENS_STEP_MIX
 #undef ENS_STEP_ROT
 #undef ENS_STEP
 #undef ENS_ARGS

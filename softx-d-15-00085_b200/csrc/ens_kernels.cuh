@@ -122,6 +122,22 @@ struct EnsBufs {
   EnsList L[2];
   int stride;           // >= n
   int cap;              // neighbour slots
+  int* pat;             // polyhedra: memory position of each polyhedron id (or null)
+  float* ppath;         // polyhedra: path since the last re-sort, per polyhedron id
+};
+
+// Convex polyhedra among a system's spheres (mix_device.cuh): what the
+// sphere step reads about them.  A polyhedron's entry in the state carries
+// minus its bounding radius in pos4.w and its polyhedron id in angv4.w (its
+// path since the last re-sort is kept per polyhedron instead).
+struct MixShapeDev;
+struct MixView {
+  const MixShapeDev* shapes;
+  const int* shape_of;       // per polyhedron id
+  const double4* gv;         // per polyhedron: world-frame vertex offsets (kMixMaxV)
+  const double4* gf;         // per polyhedron: world-frame face planes (kMixMaxF)
+  const uchar4* faces;       // per shape: vertex triples (kMixMaxF)
+  int npoly;                 // 0: spheres only
 };
 
 struct EnsGeom {
@@ -135,6 +151,7 @@ struct EnsGeom {
   int curved;                // 1: some wall is a cylinder or a triangle (not only planes)
   float2* rot;               // per system: (cos, sin) of the drum's turn so far
   int any_rot;               // 1: some system turns (the step compiled with the turn)
+  MixView mix;
 };
 
 struct EnsCapture { float4* f; float4* t; };
