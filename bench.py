@@ -89,6 +89,10 @@ def parse():
     ap.add_argument("--no-c1", action="store_true", help="skip the C1 box leg")
     ap.add_argument("--no-mill-mesh", action="store_true",
                     help="skip the turning-mesh ball-mill leg (ensemble path)")
+    ap.add_argument("--no-mill-mixed", action="store_true",
+                    help="skip the mixed-charge ball-mill leg (spheres + polyhedral rocks)")
+    ap.add_argument("--mill-mixed-only", action="store_true",
+                    help="run only the mixed-charge ball-mill leg and print its object")
     ap.add_argument("--mill-steps", type=int, default=5000)
     ap.add_argument("--mill-only", action="store_true",
                     help="print only the ball-mill leg's JSON line")
@@ -621,6 +625,100 @@ def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
             "charge_mean_tangential_velocity_cm_s": float(vt.mean())}
 
 
+def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, settle=60000,
+                   skin=0.04):
+    """The ball mill's mixed charge (ensemble path; the reference runs
+    spheres or polyhedra, never both): the turning drum of mill_mesh_leg with
+    n_spheres steel balls r ~ U[0.3, 0.6] cm and n_rocks rocks (convex hulls
+    of 8-16 points on spheres of radius 0.5-1 cm, seed 2, density 2700
+    kg/m^3): the configuration's 2,000,000 : 100,000 count ratio at the
+    charge the drum holds.  Linear law with tangential history kn = 1e6,
+    e = 0.4, mu = 0.6, dt = 2e-6 s, 30 rpm.  `settle` untimed steps with the
+    drum turning, then `steps` graph steps timed with CUDA events.  No CPU
+    baseline: the reference cannot run the charge, and the restatement tests
+    every triangle for every particle (minutes a step at this size)."""
+    import torch
+    from blaze import synth
+    from blaze import ensemble as E
+    S, W, p, r, sh, so, q = synth.mill_mixed_ensemble(n_spheres=n_spheres, n_rocks=n_rocks,
+                                                      skin=skin)
+    n = len(p)
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=skin, use_graph=1)
+    ens.set_state(p, r)
+    ens.set_polyhedra(sh, so, q)
+    ens.step(settle + max(3, warmup))
+    ens.sync()
+    stream = torch.cuda.ExternalStream(ens.device_state()[3])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    rb0 = ens.num_rebuilds()
+    a.record(stream)
+    ens.step(steps)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    rebuilds = ens.num_rebuilds() - rb0
+    launches = ens.last_launches() + rebuilds * ens.rebuild_kernels()
+    st = ens.state()
+    # device time by phase over plain steps (each waits for the device)
+    ens.set_profile(True)
+    ens.step(50)
+    ph, nph = ens.profile()
+    ens.set_profile(False)
+    ens.close()
+    rocks = so[st["pid"]] >= 0
+    x, y = st["pos"][:, 0].astype(np.float64), st["pos"][:, 1].astype(np.float64)
+    vt = -(x * st["vel"][:, 1] - y * st["vel"][:, 0]) / np.maximum(np.hypot(x, y), 1e-9)
+    return {"workload": "ball mill mixed charge: drum and lifters as a turning mesh of %d "
+                        "triangles, 30 rpm, %d steel spheres r 0.3-0.6 cm + %d convex rocks "
+                        "(hulls of 8-16 points, r 0.5-1 cm), linear law + tangential history "
+                        "kn 1e6 e 0.4 mu 0.6, dt 2e-6 s" % (int(S[0].ntris), n_spheres, n_rocks),
+            "particles": n, "spheres": n_spheres, "polyhedra": n_rocks,
+            "triangles": int(S[0].ntris), "value": n / (ms * 1e-3), "unit": UNIT,
+            "ms_per_step": ms, "steps": steps, "settle_steps": settle, "skin_cm": skin,
+            "cell_cm": float(S[0].cell), "rebuilds": rebuilds, "gpu_launches": launches,
+            "status": st["status"],
+            "plain_step_ms_by_phase": {k: float(v) / max(nph, 1) for k, v in
+                                       zip(("resort", "polyhedron_geometry", "sphere_step",
+                                            "polyhedron_step"), ph)},
+            "mean_tangential_velocity_cm_s": {"spheres": float(vt[~rocks].mean()),
+                                              "rocks": float(vt[rocks].mean())}}
+
+
+def case_mixed(n_spheres=100_000, n_rocks=5_000, settle=60000, steps=4):
+    """The mixed charge of mill_mixed_leg: the state after `settle` graph
+    steps (kept in a file under the temporary directory, so that a second run
+    -- under a profiler -- starts from it at once), set again (histories
+    cleared), then `steps` plain steps (one launch per kernel; steps < 8)."""
+    from blaze import synth
+    from blaze import ensemble as E
+    S, W, p, r, sh, so, q = synth.mill_mixed_ensemble(n_spheres=n_spheres, n_rocks=n_rocks)
+    path = os.path.join(tempfile.gettempdir(),
+                        "blaze_mixed_%d_%d_%d.npz" % (n_spheres, n_rocks, settle))
+    if not os.path.isfile(path):
+        g = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=0.04, use_graph=1)
+        g.set_state(p, r)
+        g.set_polyhedra(sh, so, q)
+        g.step(settle)
+        st = g.state()
+        qq = g.orientations()
+        g.close()
+        o = np.argsort(st["pid"])
+        np.savez(path, pos=st["pos"][o], vel=st["vel"][o], avel=st["avel"][o], quat=qq[o])
+    z = np.load(path)
+    g = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=0.04, use_graph=1)
+    g.set_state(z["pos"], r, z["vel"], z["avel"])
+    g.set_polyhedra(sh, so, z["quat"])
+    g.step(steps)
+    status = g.sync()
+    print("mixed: n %d status %d rebuilds %d" % (g.n, status, g.num_rebuilds()))
+    g.close()
+    return status
+
+
+CASES["mixed"] = case_mixed
+
+
 def c1_leg(steps=2000, warmup=20, want_cpu=True):
     """The Particles_Box plain configuration (C1): 10,000 spheres r = 0.1 cm
     falling from a jittered 20 x 20 x 25 lattice (pitch 0.3 cm) in a 10 cm
@@ -954,6 +1052,9 @@ def main():
         print(json.dumps(mill_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                                   want_cpu=not args.no_cpu_baseline)))
         return 0
+    if args.mill_mixed_only:
+        print(json.dumps(mill_mixed_leg(args.mill_steps, args.warmup)))
+        return 0
     if args.poly_only:
         print(json.dumps(poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
                                   want_cpu=not args.no_cpu_baseline)))
@@ -1100,6 +1201,9 @@ def main():
     mill_mesh = None
     if not args.no_mill_mesh:
         mill_mesh = mill_mesh_leg(args.mill_steps, args.warmup)
+    mill_mixed = None
+    if not args.no_mill_mixed:
+        mill_mixed = mill_mixed_leg(args.mill_steps, args.warmup)
     c1 = None
     if not args.no_c1:
         c1 = c1_leg(2000, args.warmup, want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
@@ -1147,6 +1251,7 @@ def main():
             "polyhedra": poly,
             "mill": mill,
             "mill_mesh": mill_mesh,
+            "mill_mixed": mill_mixed,
             "c1_box": c1,
             "batched": batched,
             "adjoint": adjoint,

@@ -138,6 +138,13 @@ int blaze_ens_device_state(blaze_ens* e, void** pos4, void** vel4, void** angv4,
  * counted by blaze_ens_rebuild_kernels each). */
 int blaze_ens_last_launches(blaze_ens* e);
 int blaze_ens_rebuild_kernels(blaze_ens* e);
+/* Profiling: while on, blaze_ens_step runs plain steps, each waiting for the
+ * device, and adds their device time by phase: the re-sort (with the gate;
+ * zero-work launches when no re-sort is due), the polyhedron geometry, the
+ * sphere step, the polyhedron step.  Turning it on clears the sums. */
+int blaze_ens_set_profile(blaze_ens* e, int on);
+/* ms4: the four sums in ms; steps: the plain steps they cover. */
+int blaze_ens_profile(blaze_ens* e, float* ms4, int* steps);
 
 /* ------------------------------------------------------------- polyhedra
  * Convex polyhedra among the spheres of a system (the mixed charge of the

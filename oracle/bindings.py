@@ -392,6 +392,8 @@ class EnsRestated:
             lib.ens_set_constants.argtypes = [C.c_void_p, C.c_int, _d]
             lib.ens_adj_record.argtypes = [C.c_void_p, C.c_int]
             lib.ens_adj_reverse.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _d, _d]
+            lib.ens_set_polyhedra.argtypes = [C.c_void_p, C.POINTER(E.Shape), C.c_int, _i, _d]
+            lib.ens_get_orientations.argtypes = [C.c_void_p, _d]
             EnsRestated._libs[path] = lib
         self.lib = EnsRestated._libs[path]
         self.nsys = len(systems)
@@ -421,6 +423,24 @@ class EnsRestated:
         c = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
         self._keep = [c(pos), c(radius), c(vel), c(avel)]
         self.lib.ens_set_state(self.h, *[_p(a, C.c_double) for a in self._keep])
+
+    def set_polyhedra(self, shapes, shape_of, quat):
+        """After set_state, as blaze_ens_set_polyhedra: particle i with
+        shape_of[i] >= 0 is a polyhedron of shapes[shape_of[i]] (ensemble
+        Shape structs) oriented by quat[i] = (w, x, y, z)."""
+        from blaze import ensemble as E
+        arr = (E.Shape * len(shapes))(*shapes)
+        so = np.ascontiguousarray(shape_of, np.int32)
+        q = np.ascontiguousarray(quat, np.float64)
+        self._keep_poly = [arr, so, q]
+        rc = self.lib.ens_set_polyhedra(self.h, arr, len(shapes), _p(so, C.c_int), _p(q, C.c_double))
+        if rc != 0:
+            raise ValueError("ens_set_polyhedra: %d" % rc)
+
+    def orientations(self):
+        q = np.zeros((self.n, 4))
+        self.lib.ens_get_orientations(self.h, _p(q, C.c_double))
+        return q
 
     def step(self, n=1):
         return self.lib.ens_step(self.h, int(n))

@@ -93,8 +93,9 @@ static void unit64(double x, double y, double z, double* u) {
 
 typedef struct {
   v3 pos, vel, w;
-  real r, path;
+  real r, path;       /* a polyhedron: r = its bounding radius; path kept per polyhedron */
   int sys, pid;
+  int poly;           /* polyhedron id, -1 for a sphere */
   uint32_t wmask;
   real wh[WSLOTS][3];
   int wid[WSLOTS];
@@ -126,6 +127,7 @@ struct ens_oracle {
   real* rot_s;
   struct tstep_* tape; /* recorded steps of the reverse sweep */
   int ntape;
+  struct mixc_* mix;   /* polyhedra among the spheres (NULL: spheres only) */
 };
 
 static void constants(sysc* d, const blaze_system* s, uint32_t off, float dt) {
@@ -245,9 +247,11 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
 }
 
 static void free_tape(ens_oracle* o);
+static void free_mix(ens_oracle* o);
 void ens_destroy(ens_oracle* o) {
   if (!o) return;
   free_tape(o);
+  free_mix(o);
   free(o->S); free(o->W); free(o->p); free(o->q);
   for (int c = 0; c < 2; ++c) { free(o->idx[c]); free(o->cnt[c]); free(o->mask[c]); free(o->hist[c]); }
   free(o->cstart); free(o->cend); free(o->cap_f); free(o->cap_t); free(o->sys_of);
@@ -287,8 +291,10 @@ void ens_set_state(ens_oracle* o, const double* pos3, const double* rad, const d
     if (vel3) a->vel = mk(IN(vel3[3 * i]), IN(vel3[3 * i + 1]), IN(vel3[3 * i + 2]));
     if (avel3) a->w = mk(IN(avel3[3 * i]), IN(avel3[3 * i + 1]), IN(avel3[3 * i + 2]));
     a->pid = i;
+    a->poly = -1;
     for (int q = 0; q < WSLOTS; ++q) a->wid[q] = -1;
   }
+  free_mix(o);   /* spheres only again */
   for (int c = 0; c < 2; ++c) {
     memset(o->cnt[c], 0, sizeof(uint32_t) * o->n);
     memset(o->mask[c], 0, sizeof(uint32_t) * o->n);
@@ -321,6 +327,7 @@ static int kv_cmp(const void* a, const void* b) {
  * the old slot each new slot's history came from (-1: none). */
 static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out);
 static void rebuild(ens_oracle* o) { rebuild_rec(o, NULL, NULL); }
+static void mix_rebuild_lists(ens_oracle* o);
 static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out) {
   const int n = o->n, cap = o->cap;
   const int e = o->epoch & 1;
@@ -350,6 +357,11 @@ static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out) {
   real *Ho = o->hist[e], *Hn = o->hist[e ^ 1];
   for (int i = 0; i < n; ++i) {
     const part* a = &o->q[i];
+    if (a->poly >= 0) {   /* a polyhedron: its own list (mix_rebuild_lists) */
+      Cn[i] = 0;
+      Mn[i] = 0;
+      continue;
+    }
     const sysc* S = &o->S[a->sys];
     const int io = ks[i].idx;
     const uint32_t cnt_o = Co[io], mask_o = Mo[io];
@@ -399,6 +411,7 @@ static void rebuild_rec(ens_oracle* o, int* perm_out, int* src_out) {
   }
   if (perm_out)
     for (int i = 0; i < n; ++i) perm_out[i] = ks[i].idx;
+  if (o->mix) mix_rebuild_lists(o);
   part* t = o->p; o->p = o->q; o->q = t;
   o->epoch += 1;
   free(ks);
@@ -584,6 +597,967 @@ static void wall_contact(wctx* c, int id, v3 n, real delta, int moving) {
   }
 }
 
+/* ============================================================ polyhedra
+ * Convex polyhedra among the spheres of a system (csrc/mix_device.cuh,
+ * csrc/mix_kernels.cu): the same shapes, narrow phases (FP64 from the
+ * working-precision state), laws and integration, stepped one particle at a
+ * time.  The polyhedron's own force sums its list slots in slot order, then
+ * the planes in order, then the kept triangles in ascending order. */
+enum { MIX_V = 16, MIX_F = 28, MIX_E = 42, MIX_SLOTS = 64, MIX_WSLOTS = 8 };
+
+typedef struct {
+  int nv, nf, ne;
+  real mass, inertia[9], iinv[9];
+  float rb;                  /* bounding radius, rounded up to float */
+  double bv[MIX_V][3];       /* body vertices (the float inputs) */
+  double bn[MIX_F][3];       /* body unit normals */
+  int faces[MIX_F][3];
+  int edges[MIX_E][4];       /* vertex i < j, faces f1 < f2 */
+} mshape;
+
+typedef struct mixc_ {
+  int npoly, nshape;
+  mshape* shapes;
+  int* shape_of;             /* per polyhedron */
+  real* quat;                /* per polyhedron: w x y z */
+  real* path;
+  int* pat;                  /* memory position */
+  double* gv;                /* per polyhedron: MIX_V x 4 (offset from the centre) */
+  double* gf;                /* per polyhedron: MIX_F x 4 (unit normal, offset h) */
+  real* wh;                  /* per polyhedron: MIX_WSLOTS wall histories (xi) */
+  int* wid;                  /* their wall ids */
+  int* wn;                   /* slots in use */
+  uint32_t* idx[2];          /* slot k of polyhedron p at k * npoly + p */
+  uint32_t* cnt[2];
+  uint64_t* mask[2];
+  real* hist[2];
+} mixc;
+
+static void free_mix(ens_oracle* o) {
+  mixc* m = o->mix;
+  if (!m) return;
+  free(m->shapes); free(m->shape_of); free(m->quat); free(m->path); free(m->pat);
+  free(m->gv); free(m->gf); free(m->wh); free(m->wid); free(m->wn);
+  for (int c = 0; c < 2; ++c) { free(m->idx[c]); free(m->cnt[c]); free(m->mask[c]); free(m->hist[c]); }
+  free(m);
+  o->mix = NULL;
+}
+
+static int edge_cmp(const void* a, const void* b) {
+  const int* x = (const int*)a;
+  const int* y = (const int*)b;
+  if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+  return x[1] < y[1] ? -1 : (x[1] > y[1]);
+}
+
+/* Shape of a blaze_shape (csrc/ens_capi.cu, shape_setup): unit normals,
+ * edges, and mass properties from the tetrahedra of the faces with the
+ * origin, in FP64 in the same order of operations. */
+static int mix_shape(const blaze_shape* s, mshape* o) {
+  memset(o, 0, sizeof(*o));
+  const int nv = s->nverts, nf = s->nfaces;
+  if (nv < 4 || nv > MIX_V || nf != 2 * nv - 4 || !(s->density > 0.0f)) return -1;
+  o->nv = nv;
+  o->nf = nf;
+  for (int k = 0; k < nv; ++k)
+    for (int c = 0; c < 3; ++c) o->bv[k][c] = (double)s->verts[3 * k + c];
+  for (int f = 0; f < nf; ++f) {
+    const int a = s->faces[3 * f], b = s->faces[3 * f + 1], c = s->faces[3 * f + 2];
+    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) return -1;
+    o->faces[f][0] = a; o->faces[f][1] = b; o->faces[f][2] = c;
+    const double* va = o->bv[a];
+    const double* vb = o->bv[b];
+    const double* vc = o->bv[c];
+    const double e1[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
+    const double e2[3] = {vc[0] - va[0], vc[1] - va[1], vc[2] - va[2]};
+    const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                          e1[0] * e2[1] - e1[1] * e2[0]};
+    const double l = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    if (!(l > 0.0)) return -1;
+    o->bn[f][0] = cr[0] / l; o->bn[f][1] = cr[1] / l; o->bn[f][2] = cr[2] / l;
+  }
+  /* edges: every directed edge (a, b) of a face; (a < b) with both faces */
+  int ne = 0;
+  for (int f = 0; f < nf; ++f)
+    for (int k = 0; k < 3; ++k) {
+      const int a = o->faces[f][k], b = o->faces[f][(k + 1) % 3];
+      if (a > b) continue;
+      int g = -1;
+      for (int h = 0; h < nf; ++h)
+        for (int q = 0; q < 3; ++q)
+          if (o->faces[h][q] == b && o->faces[h][(q + 1) % 3] == a) g = h;
+      if (g < 0 || ne >= MIX_E) return -1;
+      o->edges[ne][0] = a; o->edges[ne][1] = b;
+      o->edges[ne][2] = f < g ? f : g; o->edges[ne][3] = f < g ? g : f;
+      ++ne;
+    }
+  if (ne != 3 * nv - 6) return -1;
+  qsort(o->edges, ne, sizeof(o->edges[0]), edge_cmp);
+  o->ne = ne;
+  double rb = 0.0;
+  for (int k = 0; k < nv; ++k) {
+    const double r = sqrt(o->bv[k][0] * o->bv[k][0] + o->bv[k][1] * o->bv[k][1] +
+                          o->bv[k][2] * o->bv[k][2]);
+    if (r > rb) rb = r;
+  }
+  float rbf = (float)rb;
+  if ((double)rbf < rb) rbf = nextafterf(rbf, INFINITY);
+  o->rb = rbf;
+  double vol = 0.0, cen[3] = {0.0, 0.0, 0.0}, C[9] = {0.0};
+  for (int f = 0; f < nf; ++f) {
+    const double* a = o->bv[o->faces[f][0]];
+    const double* b = o->bv[o->faces[f][1]];
+    const double* c = o->bv[o->faces[f][2]];
+    const double det = a[0] * (b[1] * c[2] - b[2] * c[1]) + a[1] * (b[2] * c[0] - b[0] * c[2]) +
+                       a[2] * (b[0] * c[1] - b[1] * c[0]);
+    vol += det / 6.0;
+    double sm[3];
+    for (int q = 0; q < 3; ++q) {
+      sm[q] = a[q] + b[q] + c[q];
+      cen[q] += det * sm[q] / 24.0;
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        C[3 * r + q] += det / 120.0 * (a[r] * a[q] + b[r] * b[q] + c[r] * c[q] + sm[r] * sm[q]);
+  }
+  if (!(vol > 0.0)) return -1;
+  const double rho = (double)s->density;
+  const double mass = rho * vol;
+  double com[3];
+  for (int q = 0; q < 3; ++q) com[q] = cen[q] / vol;
+  const double tr = C[0] + C[4] + C[8];
+  const double c2 = com[0] * com[0] + com[1] * com[1] + com[2] * com[2];
+  double J[9];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q)
+      J[3 * r + q] = rho * ((r == q ? tr : 0.0) - C[3 * r + q]) -
+                     mass * ((r == q ? c2 : 0.0) - com[r] * com[q]);
+  const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                     J[2] * (J[3] * J[7] - J[4] * J[6]);
+  if (!(det > 0.0)) return -1;
+  const double inv[9] = {(J[4] * J[8] - J[5] * J[7]) / det, (J[2] * J[7] - J[1] * J[8]) / det,
+                         (J[1] * J[5] - J[2] * J[4]) / det, (J[5] * J[6] - J[3] * J[8]) / det,
+                         (J[0] * J[8] - J[2] * J[6]) / det, (J[2] * J[3] - J[0] * J[5]) / det,
+                         (J[3] * J[7] - J[4] * J[6]) / det, (J[1] * J[6] - J[0] * J[7]) / det,
+                         (J[0] * J[4] - J[1] * J[3]) / det};
+  o->mass = (real)mass;
+  for (int q = 0; q < 9; ++q) {
+    o->inertia[q] = (real)J[q];
+    o->iinv[q] = (real)inv[q];
+  }
+  return 0;
+}
+
+/* After ens_set_state: particle i (caller order) with shape_of[i] >= 0 is a
+ * polyhedron of shapes[shape_of[i]] oriented by quat4[4 i ..] (normalised in
+ * double, then rounded to float). */
+int ens_set_polyhedra(ens_oracle* o, const blaze_shape* shapes, int nshapes, const int* shape_of,
+                      const double* quat4) {
+  free_mix(o);
+  int np = 0;
+  for (int i = 0; i < o->n; ++i) np += shape_of[i] >= 0;
+  if (np == 0) return 0;
+  mixc* m = (mixc*)calloc(1, sizeof(mixc));
+  m->nshape = nshapes;
+  m->shapes = (mshape*)calloc(nshapes, sizeof(mshape));
+  for (int k = 0; k < nshapes; ++k)
+    if (mix_shape(&shapes[k], &m->shapes[k])) { free(m->shapes); free(m); return -1; }
+  m->npoly = np;
+  m->shape_of = (int*)calloc(np, sizeof(int));
+  m->quat = (real*)calloc((size_t)4 * np, sizeof(real));
+  m->path = (real*)calloc(np, sizeof(real));
+  m->pat = (int*)calloc(np, sizeof(int));
+  m->gv = (double*)calloc((size_t)np * MIX_V * 4, sizeof(double));
+  m->gf = (double*)calloc((size_t)np * MIX_F * 4, sizeof(double));
+  m->wh = (real*)calloc((size_t)np * MIX_WSLOTS * 3, sizeof(real));
+  m->wid = (int*)calloc((size_t)np * MIX_WSLOTS, sizeof(int));
+  m->wn = (int*)calloc(np, sizeof(int));
+  for (int c = 0; c < 2; ++c) {
+    m->idx[c] = (uint32_t*)calloc((size_t)np * MIX_SLOTS, sizeof(uint32_t));
+    m->cnt[c] = (uint32_t*)calloc(np, sizeof(uint32_t));
+    m->mask[c] = (uint64_t*)calloc(np, sizeof(uint64_t));
+    m->hist[c] = (real*)calloc((size_t)np * MIX_SLOTS * 3, sizeof(real));
+  }
+  int p = 0;
+  for (int i = 0; i < o->n; ++i) {
+    if (shape_of[i] < 0) continue;
+    const mshape* sh = &m->shapes[shape_of[i]];
+    m->shape_of[p] = shape_of[i];
+    const double* q = quat4 + 4 * i;
+    const double qn = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    /* as the product takes it, in both builds: normalised in double, rounded
+       to float (a 1-ulp turn moves a vertex by ~1e-7 cm, a few 1e-3 of a
+       resting overlap) */
+    for (int c = 0; c < 4; ++c) m->quat[4 * p + c] = (real)(float)(q[c] / qn);
+    m->pat[p] = i;
+    o->p[i].poly = p;
+    o->p[i].r = (real)sh->rb;
+    ++p;
+  }
+  o->mix = m;
+  return 0;
+}
+
+/* Orientations in the current memory order (w x y z; spheres 1 0 0 0). */
+void ens_get_orientations(const ens_oracle* o, double* quat4) {
+  for (int i = 0; i < o->n; ++i) {
+    const int p = o->p[i].poly;
+    for (int c = 0; c < 4; ++c)
+      quat4[4 * i + c] = p >= 0 ? (double)o->mix->quat[4 * p + c] : (c == 0 ? 1.0 : 0.0);
+  }
+}
+
+/* FP64 vectors, evaluated as csrc/mix_device.cuh writes them */
+typedef struct { double x, y, z; } dv3;
+static dv3 dv(double x, double y, double z) { dv3 r = {x, y, z}; return r; }
+static dv3 dof(v3 a) { return dv((double)a.x, (double)a.y, (double)a.z); }
+static dv3 d4v(const double* p) { return dv(p[0], p[1], p[2]); }
+static dv3 dadd(dv3 a, dv3 b) { return dv(a.x + b.x, a.y + b.y, a.z + b.z); }
+static dv3 dsub(dv3 a, dv3 b) { return dv(a.x - b.x, a.y - b.y, a.z - b.z); }
+static dv3 dscale(dv3 a, double s) { return dv(a.x * s, a.y * s, a.z * s); }
+static dv3 dneg(dv3 a) { return dv(-a.x, -a.y, -a.z); }
+static double ddot(dv3 a, dv3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static dv3 dcross(dv3 a, dv3 b) {
+  return dv(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static v3 tov(dv3 a) { return mk((real)a.x, (real)a.y, (real)a.z); }
+
+static void mix_rotation(const real* q4, double* R) {
+  const double w = q4[0], x = q4[1], y = q4[2], z = q4[3];
+  const double s = 2.0 / (((w * w + x * x) + y * y) + z * z);
+  R[0] = 1.0 - s * (y * y + z * z);
+  R[1] = s * (x * y - w * z);
+  R[2] = s * (x * z + w * y);
+  R[3] = s * (x * y + w * z);
+  R[4] = 1.0 - s * (x * x + z * z);
+  R[5] = s * (y * z - w * x);
+  R[6] = s * (x * z - w * y);
+  R[7] = s * (y * z + w * x);
+  R[8] = 1.0 - s * (x * x + y * y);
+}
+static dv3 mat_vec(const double* R, dv3 v) {
+  return dv((R[0] * v.x + R[1] * v.y) + R[2] * v.z, (R[3] * v.x + R[4] * v.y) + R[5] * v.z,
+            (R[6] * v.x + R[7] * v.y) + R[8] * v.z);
+}
+static dv3 rot_about_d(dv3 a, double c, double s, dv3 v) {
+  const dv3 axv = dcross(a, v);
+  const double av = ddot(a, v);
+  return dadd(dadd(dscale(v, c), dscale(axv, s)), dscale(a, av * (1.0 - c)));
+}
+
+static dv3 closest_on_triangle_d(dv3 p, dv3 a, dv3 b, dv3 c) {
+  const dv3 ab = dsub(b, a), ac = dsub(c, a), ap = dsub(p, a);
+  const double d1 = ddot(ab, ap), d2 = ddot(ac, ap);
+  if (d1 <= 0.0 && d2 <= 0.0) return a;
+  const dv3 bp = dsub(p, b);
+  const double d3_ = ddot(ab, bp), d4 = ddot(ac, bp);
+  if (d3_ >= 0.0 && d4 <= d3_) return b;
+  const double vc = d1 * d4 - d3_ * d2;
+  if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0) return dadd(a, dscale(ab, d1 / (d1 - d3_)));
+  const dv3 cp = dsub(p, c);
+  const double d5 = ddot(ab, cp), d6 = ddot(ac, cp);
+  if (d6 >= 0.0 && d5 <= d6) return c;
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return dadd(a, dscale(ac, d2 / (d2 - d6)));
+  const double va = d3_ * d6 - d5 * d4;
+  if (va <= 0.0 && (d4 - d3_) >= 0.0 && (d5 - d6) >= 0.0)
+    return dadd(b, dscale(dsub(c, b), (d4 - d3_) / ((d4 - d3_) + (d5 - d6))));
+  const double den = 1.0 / ((va + vb) + vc);
+  return dadd(dadd(a, dscale(ab, vb * den)), dscale(ac, vc * den));
+}
+
+typedef struct { v3 n; real delta; v3 ca, cb; } mhit;
+
+/* a world-frame hull: vertex offsets V[k * 4], planes F[f * 4] (normal, h) */
+typedef struct {
+  const double* V;
+  const double* F;
+  const int (*E)[4];
+  const int (*T)[3];
+  int nv, nf, ne;
+} hullr;
+
+static int sphere_hull(v3 c, real r, v3 x, const hullr* H, mhit* h) {
+  const dv3 d = dsub(dof(c), dof(x));
+  const double rr = (double)r;
+  double smax = -1e300;
+  int fb = 0;
+  for (int f = 0; f < H->nf; ++f) {
+    const double* P = H->F + 4 * f;
+    const double s = ((P[0] * d.x + P[1] * d.y) + P[2] * d.z) - P[3];
+    if (s > smax) { smax = s; fb = f; }
+  }
+  if (!(smax < rr)) return 0;
+  dv3 q, nn;
+  double delta;
+  if (smax <= 0.0) {
+    nn = d4v(H->F + 4 * fb);
+    delta = rr - smax;
+    q = dsub(d, dscale(nn, smax));
+  } else {
+    double best = 1e300;
+    q = d;
+    for (int f = 0; f < H->nf; ++f) {
+      const double* P = H->F + 4 * f;
+      const double s = ((P[0] * d.x + P[1] * d.y) + P[2] * d.z) - P[3];
+      if (!(s > 0.0 && s < rr)) continue;
+      const int* t = H->T[f];
+      const dv3 qf = closest_on_triangle_d(d, d4v(H->V + 4 * t[0]), d4v(H->V + 4 * t[1]),
+                                           d4v(H->V + 4 * t[2]));
+      const dv3 e = dsub(d, qf);
+      const double e2 = ddot(e, e);
+      if (e2 < best) { best = e2; q = qf; }
+    }
+    if (!(best < rr * rr)) return 0;
+    const double dist = sqrt(best);
+    if (!(dist > 0.0)) return 0;
+    nn = dv((d.x - q.x) / dist, (d.y - q.y) / dist, (d.z - q.z) / dist);
+    delta = rr - dist;
+  }
+  const real df = (real)delta;
+  if (!(df > 0)) return 0;
+  h->n = tov(nn);
+  h->delta = df;
+  h->ca = mul(h->n, -r);
+  h->cb = tov(q);
+  return 1;
+}
+
+static double face_sep(const double* P, dv3 d, const double* VB, int nvB) {
+  double m = 1e300;
+  for (int k = 0; k < nvB; ++k) {
+    const double* v = VB + 4 * k;
+    const double t = (P[0] * (d.x + v[0]) + P[1] * (d.y + v[1])) + P[2] * (d.z + v[2]);
+    if (t < m) m = t;
+  }
+  return m - P[3];
+}
+
+#define NO_AXIS (-1e300)
+
+static double edge_sep(dv3 a, dv3 b, dv3 c, dv3 dn, dv3 PA, dv3 QA, dv3 PB, dv3 QB) {
+  c = dneg(c);
+  dn = dneg(dn);
+  const dv3 bxa = dcross(b, a), dxc = dcross(dn, c);
+  const double cba = ddot(c, bxa), dba = ddot(dn, bxa), adc = ddot(a, dxc), bdc = ddot(b, dxc);
+  if (!(cba * dba < 0.0 && adc * bdc < 0.0 && cba * bdc > 0.0)) return NO_AXIS;
+  const dv3 ea = dsub(QA, PA), eb = dsub(QB, PB);
+  dv3 ax = dcross(ea, eb);
+  const double l2 = ddot(ax, ax);
+  if (!(l2 > 1e-10 * (ddot(ea, ea) * ddot(eb, eb)))) return NO_AXIS;
+  const double l = sqrt(l2);
+  ax = dv(ax.x / l, ax.y / l, ax.z / l);
+  if (ddot(ax, PA) < 0.0) ax = dneg(ax);
+  return ddot(ax, dsub(PB, PA));
+}
+
+static dv3 edge_axis(dv3 PA, dv3 QA, dv3 PB, dv3 QB) {
+  const dv3 ea = dsub(QA, PA), eb = dsub(QB, PB);
+  dv3 ax = dcross(ea, eb);
+  const double l = sqrt(ddot(ax, ax));
+  ax = dv(ax.x / l, ax.y / l, ax.z / l);
+  if (ddot(ax, PA) < 0.0) ax = dneg(ax);
+  return ax;
+}
+
+static double clamp01(double s) { return s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s); }
+
+static dv3 segments_midpoint(dv3 P1, dv3 Q1, dv3 P2, dv3 Q2) {
+  const dv3 d1 = dsub(Q1, P1), d2 = dsub(Q2, P2), r = dsub(P1, P2);
+  const double a = ddot(d1, d1), e = ddot(d2, d2), f = ddot(d2, r);
+  const double c = ddot(d1, r), b = ddot(d1, d2);
+  const double den = a * e - b * b;
+  double s = den > 0.0 ? (b * f - c * e) / den : 0.0;
+  s = clamp01(s);
+  double t = (b * s + f) / e;
+  if (t < 0.0) {
+    t = 0.0;
+    s = clamp01(-c / a);
+  } else if (t > 1.0) {
+    t = 1.0;
+    s = clamp01((b - c) / a);
+  }
+  const dv3 c1 = dadd(P1, dscale(d1, s)), c2 = dadd(P2, dscale(d2, t));
+  return dscale(dadd(c1, c2), 0.5);
+}
+
+#define REL_FACE 0.98
+#define REL_EDGE 0.90
+
+typedef struct { double sA, sB, sE; int fA, fB, eE; } satpick;
+
+static int sat_kind(const satpick* q) {
+  const double sf = q->sA > q->sB ? q->sA : q->sB;
+  if (q->sE > REL_EDGE * sf) return 2;
+  if (q->sB > REL_FACE * q->sA) return 1;
+  return 0;
+}
+
+/* the separating-axis queries of A and B (B's centre at d from A's) */
+static int hull_hull_queries(dv3 d, const hullr* A, const hullr* B, satpick* q) {
+  double s = -1e300;
+  int k = 0;
+  for (int f = 0; f < A->nf; ++f) {
+    const double t = face_sep(A->F + 4 * f, d, B->V, B->nv);
+    if (t > s) { s = t; k = f; }
+  }
+  if (s > 0.0) return 0;
+  q->sA = s; q->fA = k;
+  const dv3 md = dneg(d);
+  s = -1e300;
+  k = 0;
+  for (int f = 0; f < B->nf; ++f) {
+    const double t = face_sep(B->F + 4 * f, md, A->V, A->nv);
+    if (t > s) { s = t; k = f; }
+  }
+  if (s > 0.0) return 0;
+  q->sB = s; q->fB = k;
+  s = NO_AXIS;
+  k = 0;
+  for (int ea = 0; ea < A->ne; ++ea)
+    for (int eb = 0; eb < B->ne; ++eb) {
+      const int* EA = A->E[ea];
+      const int* EB = B->E[eb];
+      const double t = edge_sep(d4v(A->F + 4 * EA[2]), d4v(A->F + 4 * EA[3]), d4v(B->F + 4 * EB[2]),
+                                d4v(B->F + 4 * EB[3]), d4v(A->V + 4 * EA[0]), d4v(A->V + 4 * EA[1]),
+                                dadd(d, d4v(B->V + 4 * EB[0])), dadd(d, d4v(B->V + 4 * EB[1])));
+      if (t > s) { s = t; k = ea * B->ne + eb; }
+    }
+  if (s > 0.0) return 0;
+  q->sE = s; q->eE = k;
+  return 1;
+}
+
+static int hull_hull_finish(const satpick* q, dv3 d, const hullr* A, const hullr* B, mhit* h) {
+  const int kind = sat_kind(q);
+  dv3 nAB, cp;
+  double s;
+  if (kind == 0) {
+    const double* P = A->F + 4 * q->fA;
+    nAB = d4v(P);
+    s = q->sA;
+    dv3 acc = dv(0.0, 0.0, 0.0);
+    double wsum = 0.0;
+    for (int k = 0; k < B->nv; ++k) {
+      const dv3 v = dadd(d, d4v(B->V + 4 * k));
+      const double t = ((P[0] * v.x + P[1] * v.y) + P[2] * v.z) - P[3];
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
+    }
+    cp = dscale(acc, 1.0 / wsum);
+  } else if (kind == 1) {
+    const double* P = B->F + 4 * q->fB;
+    nAB = dneg(d4v(P));
+    s = q->sB;
+    dv3 acc = dv(0.0, 0.0, 0.0);
+    double wsum = 0.0;
+    for (int k = 0; k < A->nv; ++k) {
+      const dv3 v = d4v(A->V + 4 * k);
+      const dv3 w = dsub(v, d);
+      const double t = ((P[0] * w.x + P[1] * w.y) + P[2] * w.z) - P[3];
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
+    }
+    cp = dscale(acc, 1.0 / wsum);
+  } else {
+    const int* ea = A->E[q->eE / B->ne];
+    const int* eb = B->E[q->eE % B->ne];
+    const dv3 PA = d4v(A->V + 4 * ea[0]), QA = d4v(A->V + 4 * ea[1]);
+    const dv3 PB = dadd(d, d4v(B->V + 4 * eb[0])), QB = dadd(d, d4v(B->V + 4 * eb[1]));
+    nAB = edge_axis(PA, QA, PB, QB);
+    s = q->sE;
+    cp = segments_midpoint(PA, QA, PB, QB);
+  }
+  const real df = (real)(-s);
+  if (!(df > 0)) return 0;
+  h->n = tov(dneg(nAB));
+  h->delta = df;
+  h->ca = tov(cp);
+  h->cb = tov(dsub(cp, d));
+  return 1;
+}
+
+static int tri_e0(int t) { return t == 2 ? 1 : 0; }
+static int tri_e1(int t) { return t == 0 ? 1 : 2; }
+
+static int hull_tri(const hullr* H, const dv3* T, dv3 nt, mhit* h, dv3* nd) {
+  double sP = -1e300;
+  int fP = 0;
+  for (int f = 0; f < H->nf; ++f) {
+    const double* P = H->F + 4 * f;
+    double m = 1e300;
+    for (int k = 0; k < 3; ++k) {
+      const double t = (P[0] * T[k].x + P[1] * T[k].y) + P[2] * T[k].z;
+      if (t < m) m = t;
+    }
+    const double s = m - P[3];
+    if (s > sP) { sP = s; fP = f; }
+  }
+  if (sP > 0.0) return 0;
+  double lo = 1e300, hi = -1e300;
+  for (int k = 0; k < H->nv; ++k) {
+    const double t = ddot(nt, d4v(H->V + 4 * k));
+    if (t < lo) lo = t;
+    if (t > hi) hi = t;
+  }
+  const double h0 = ddot(nt, T[0]);
+  const double sTp = lo - h0, sTm = h0 - hi;
+  const int tplus = sTp >= sTm;
+  const double sT = tplus ? sTp : sTm;
+  if (sT > 0.0) return 0;
+  double sE = -1e300;
+  int eE = -1, eplus = 1;
+  for (int e = 0; e < H->ne; ++e) {
+    const int* ed = H->E[e];
+    const dv3 P0 = d4v(H->V + 4 * ed[0]), ep = dsub(d4v(H->V + 4 * ed[1]), P0);
+    for (int t = 0; t < 3; ++t) {
+      const dv3 et = dsub(T[tri_e1(t)], T[tri_e0(t)]);
+      dv3 ax = dcross(ep, et);
+      const double l2 = ddot(ax, ax);
+      if (!(l2 > 1e-10 * (ddot(ep, ep) * ddot(et, et)))) continue;
+      const double l = sqrt(l2);
+      ax = dv(ax.x / l, ax.y / l, ax.z / l);
+      double pmin = 1e300, pmax = -1e300;
+      for (int k = 0; k < H->nv; ++k) {
+        const double u = ddot(ax, d4v(H->V + 4 * k));
+        if (u < pmin) pmin = u;
+        if (u > pmax) pmax = u;
+      }
+      double tmin = 1e300, tmax = -1e300;
+      for (int k = 0; k < 3; ++k) {
+        const double u = ddot(ax, T[k]);
+        if (u < tmin) tmin = u;
+        if (u > tmax) tmax = u;
+      }
+      const double s1 = tmin - pmax, s2 = pmin - tmax;
+      const double s = s1 >= s2 ? s1 : s2;
+      if (s > 0.0) return 0;
+      if (s > sE) { sE = s; eE = 3 * e + t; eplus = s1 >= s2; }
+    }
+  }
+  satpick q;
+  q.sA = sT;
+  q.sB = sP;
+  q.sE = eE >= 0 ? sE : NO_AXIS;
+  const int kind = sat_kind(&q);
+  dv3 n_in, cp;
+  double s;
+  if (kind == 0) {
+    n_in = tplus ? nt : dneg(nt);
+    s = sT;
+    dv3 acc = dv(0.0, 0.0, 0.0);
+    double wsum = 0.0;
+    for (int k = 0; k < H->nv; ++k) {
+      const dv3 v = d4v(H->V + 4 * k);
+      const double t = ddot(n_in, v) - ddot(n_in, T[0]);
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
+    }
+    cp = dscale(acc, 1.0 / wsum);
+  } else if (kind == 1) {
+    const double* P = H->F + 4 * fP;
+    n_in = dneg(d4v(P));
+    s = sP;
+    dv3 acc = dv(0.0, 0.0, 0.0);
+    double wsum = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double t = ((P[0] * T[k].x + P[1] * T[k].y) + P[2] * T[k].z) - P[3];
+      if (t < 0.0) { acc = dadd(acc, dscale(T[k], -t)); wsum = wsum - t; }
+    }
+    cp = dscale(acc, 1.0 / wsum);
+  } else {
+    const int e = eE / 3, t = eE % 3;
+    const int* ed = H->E[e];
+    const dv3 P0 = d4v(H->V + 4 * ed[0]), Q0 = d4v(H->V + 4 * ed[1]);
+    const dv3 P1 = T[tri_e0(t)], Q1 = T[tri_e1(t)];
+    dv3 ax = dcross(dsub(Q0, P0), dsub(Q1, P1));
+    const double l = sqrt(ddot(ax, ax));
+    ax = dv(ax.x / l, ax.y / l, ax.z / l);
+    n_in = eplus ? dneg(ax) : ax;
+    s = sE;
+    cp = segments_midpoint(P0, Q0, P1, Q1);
+  }
+  const real df = (real)(-s);
+  if (!(df > 0)) return 0;
+  *nd = n_in;
+  h->n = tov(n_in);
+  h->delta = df;
+  h->ca = tov(cp);
+  h->cb = h->ca;
+  return 1;
+}
+
+static int hull_plane(v3 n, real pd, v3 x, const hullr* H, mhit* h) {
+  const dv3 nn = dof(n);
+  const double base = ddot(nn, dof(x)) - (double)pd;
+  double lo = 1e300, wsum = 0.0;
+  dv3 acc = dv(0.0, 0.0, 0.0);
+  for (int k = 0; k < H->nv; ++k) {
+    const dv3 v = d4v(H->V + 4 * k);
+    const double s = base + ddot(nn, v);
+    if (s < lo) lo = s;
+    if (s < 0.0) { acc = dadd(acc, dscale(v, -s)); wsum = wsum - s; }
+  }
+  const real df = (real)(-lo);
+  if (!(df > 0) || !(wsum > 0.0)) return 0;
+  h->n = n;
+  h->delta = df;
+  h->ca = tov(dscale(acc, 1.0 / wsum));
+  h->cb = h->ca;
+  return 1;
+}
+
+#define COPLANAR (1.0 - 1e-9)
+
+static hullr hull_of(const mixc* m, int p) {
+  const mshape* sh = &m->shapes[m->shape_of[p]];
+  hullr h;
+  h.V = m->gv + (size_t)p * MIX_V * 4;
+  h.F = m->gf + (size_t)p * MIX_F * 4;
+  h.E = (const int (*)[4])sh->edges;
+  h.T = (const int (*)[3])sh->faces;
+  h.nv = sh->nv;
+  h.nf = sh->nf;
+  h.ne = sh->ne;
+  return h;
+}
+
+/* world-frame geometry of every polyhedron from its orientation (k_mix_geom) */
+static void mix_geometry(ens_oracle* o) {
+  mixc* m = o->mix;
+  for (int p = 0; p < m->npoly; ++p) {
+    const mshape* sh = &m->shapes[m->shape_of[p]];
+    double R[9];
+    mix_rotation(m->quat + 4 * p, R);
+    double* V = m->gv + (size_t)p * MIX_V * 4;
+    double* F = m->gf + (size_t)p * MIX_F * 4;
+    for (int k = 0; k < sh->nv; ++k) {
+      const dv3 v = mat_vec(R, d4v(sh->bv[k]));
+      V[4 * k] = v.x; V[4 * k + 1] = v.y; V[4 * k + 2] = v.z; V[4 * k + 3] = 0.0;
+    }
+    for (int f = 0; f < sh->nf; ++f) {
+      const dv3 n = mat_vec(R, d4v(sh->bn[f]));
+      const dv3 v = mat_vec(R, d4v(sh->bv[sh->faces[f][0]]));
+      F[4 * f] = n.x; F[4 * f + 1] = n.y; F[4 * f + 2] = n.z; F[4 * f + 3] = ddot(n, v);
+    }
+  }
+}
+
+/* The law of a contact h of particle a with particle b (mix_pair_law). */
+static void mix_pair_law(const ens_oracle* o, const sysc* S, const mhit* h, real ma, v3 va, v3 wa,
+                         real mb, v3 vb, v3 wb, v3* xi, v3* F, v3* Ta, v3* Tb) {
+  const v3 vct = sub(add(va, cross(wa, h->ca)), add(vb, cross(wb, h->cb)));
+  const real ms = (ma * mb) / (ma + mb);
+  v3 t0;
+  contact_law(o, S, S->mu, h->n, h->delta, 0, ms, vct, vct, mk(0, 0, 0), 0, xi, F, &t0);
+  *Ta = cross(h->ca, *F);
+  *Tb = cross(h->cb, mk(-F->x, -F->y, -F->z));
+}
+
+/* The polyhedra's lists of the new memory order (k_mix_plist), after the
+ * re-sort placed them: the new order is o->q, the old o->p. */
+static void mix_rebuild_lists(ens_oracle* o) {
+  mixc* m = o->mix;
+  const int n = o->n, e = o->epoch & 1;
+  const size_t P = (size_t)m->npoly;
+  for (int i = 0; i < n; ++i)
+    if (o->q[i].poly >= 0) {
+      m->pat[o->q[i].poly] = i;
+      m->path[o->q[i].poly] = 0;
+    }
+  uint32_t *Io = m->idx[e], *In = m->idx[e ^ 1];
+  uint32_t *Co = m->cnt[e], *Cn = m->cnt[e ^ 1];
+  uint64_t *Mo = m->mask[e], *Mn = m->mask[e ^ 1];
+  real *Ho = m->hist[e], *Hn = m->hist[e ^ 1];
+  for (int p = 0; p < m->npoly; ++p) {
+    const int i = m->pat[p];
+    const part* a = &o->q[i];
+    const sysc* S = &o->S[a->sys];
+    const uint32_t cnt_o = Co[p];
+    const uint64_t mask_o = Mo[p];
+    uint32_t cnt = 0;
+    uint64_t mask = 0;
+    int c[3];
+    if (cell_of(S, a->pos, c)) {
+      const int x0 = c[0] > 0 ? c[0] - 1 : 0, x1 = c[0] < S->nc[0] - 1 ? c[0] + 1 : c[0];
+      const int y0 = c[1] > 0 ? c[1] - 1 : 0, y1 = c[1] < S->nc[1] - 1 ? c[1] + 1 : c[1];
+      const int z0 = c[2] > 0 ? c[2] - 1 : 0, z1 = c[2] < S->nc[2] - 1 ? c[2] + 1 : c[2];
+      for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y)
+          for (int x = x0; x <= x1; ++x) {
+            const uint32_t h = S->cell_off + (uint32_t)(S->nc[0] * (y + S->nc[1] * z)) + (uint32_t)x;
+            const uint32_t s0 = o->cstart[h];
+            if (s0 == 0xffffffffu) continue;
+            for (uint32_t j = s0; j < o->cend[h]; ++j) {
+              if ((int)j == i) continue;
+              const part* b = &o->q[j];
+              const v3 rel = sub(a->pos, b->pos);
+              const real lim = (a->r + b->r) + o->skin;
+              if (!(dot(rel, rel) < lim * lim)) continue;
+              if (cnt < MIX_SLOTS) {
+                In[(size_t)cnt * P + p] = j;
+                for (uint32_t ko = 0; ko < cnt_o && ko < MIX_SLOTS; ++ko) {
+                  if (!((mask_o >> ko) & 1ull)) continue;
+                  const size_t so = (size_t)ko * P + p;
+                  if (o->p[Io[so]].pid == b->pid) {
+                    const size_t sn = (size_t)cnt * P + p;
+                    Hn[3 * sn] = Ho[3 * so]; Hn[3 * sn + 1] = Ho[3 * so + 1]; Hn[3 * sn + 2] = Ho[3 * so + 2];
+                    mask |= 1ull << cnt;
+                    break;
+                  }
+                }
+              } else {
+                o->status |= ST_OVERFLOW;
+              }
+              ++cnt;
+            }
+          }
+    } else {
+      o->status |= ST_OUT_OF_GRID;
+    }
+    Cn[p] = cnt < MIX_SLOTS ? cnt : MIX_SLOTS;
+    Mn[p] = mask;
+  }
+}
+
+/* One sphere's contact with polyhedron neighbour b (the sphere step's
+ * branch); 0 when they do not touch. */
+static int mix_sphere_contact(const ens_oracle* o, const sysc* S, const part* a, real ma,
+                              const part* b, v3* xi, v3* F, v3* T) {
+  const mixc* m = o->mix;
+  const hullr H = hull_of(m, b->poly);
+  mhit h;
+  if (!sphere_hull(a->pos, a->r, b->pos, &H, &h)) return 0;
+  v3 Tb;
+  mix_pair_law(o, S, &h, ma, a->vel, a->w, m->shapes[m->shape_of[b->poly]].mass, b->vel, b->w, xi,
+               F, T, &Tb);
+  return 1;
+}
+
+enum { MIX_HITS = 16 };
+
+/* One polyhedron's step (k_mix_poly_step): reads o->p, writes o->q. */
+static void mix_poly_step(ens_oracle* o, int p, int* req) {
+  mixc* m = o->mix;
+  const int e = o->epoch & 1;
+  const size_t P = (size_t)m->npoly;
+  const int i = m->pat[p];
+  const part* a = &o->p[i];
+  const sysc* S = &o->S[a->sys];
+  const mshape* SH = &m->shapes[m->shape_of[p]];
+  const hullr A = hull_of(m, p);
+  const real dt = o->dt;
+  uint32_t* I = m->idx[e];
+  real* Hs = m->hist[e];
+  const uint32_t cnt = m->cnt[e][p];
+  const uint64_t mask_o = m->mask[e][p];
+  uint64_t touch = 0;
+  v3 f = mk(0, 0, 0), t = mk(0, 0, 0);
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t sk = (size_t)k * P + p;
+    const part* b = &o->p[I[sk]];
+    v3 xi = mk(0, 0, 0);
+    if ((mask_o >> k) & 1ull) xi = mk(Hs[3 * sk], Hs[3 * sk + 1], Hs[3 * sk + 2]);
+    v3 F, Ta, Tb;
+    if (b->poly < 0) {
+      const v3 rel = sub(b->pos, a->pos);
+      const real sr = b->r + a->r;
+      const real d2 = dot(rel, rel);
+      if (!(d2 < sr * sr && SQRT(d2) > 0)) continue;
+      mhit h;
+      if (!sphere_hull(b->pos, b->r, a->pos, &A, &h)) continue;
+      const real mb = S->dens43pi * ((b->r * b->r) * b->r);
+      mix_pair_law(o, S, &h, mb, b->vel, b->w, SH->mass, a->vel, a->w, &xi, &F, &Ta, &Tb);
+      f = add(f, mk(-F.x, -F.y, -F.z));
+      t = add(t, Tb);
+    } else {
+      const int q = b->poly;
+      const int selfA = p < q;
+      const part* pA = selfA ? a : b;
+      const part* pB = selfA ? b : a;
+      const v3 rel = sub(pB->pos, pA->pos);
+      const real sr = pA->r + pB->r;
+      if (!(dot(rel, rel) < sr * sr)) continue;
+      const hullr Bq = hull_of(m, q);
+      const hullr* HA = selfA ? &A : &Bq;
+      const hullr* HB = selfA ? &Bq : &A;
+      const dv3 d = dsub(dof(pB->pos), dof(pA->pos));
+      satpick pk;
+      if (!hull_hull_queries(d, HA, HB, &pk)) continue;
+      mhit h;
+      if (!hull_hull_finish(&pk, d, HA, HB, &h)) continue;
+      const real mq = m->shapes[m->shape_of[q]].mass;
+      if (selfA) mix_pair_law(o, S, &h, SH->mass, a->vel, a->w, mq, b->vel, b->w, &xi, &F, &Ta, &Tb);
+      else mix_pair_law(o, S, &h, mq, b->vel, b->w, SH->mass, a->vel, a->w, &xi, &F, &Ta, &Tb);
+      f = add(f, selfA ? F : mk(-F.x, -F.y, -F.z));
+      t = add(t, selfA ? Ta : Tb);
+    }
+    Hs[3 * sk] = xi.x; Hs[3 * sk + 1] = xi.y; Hs[3 * sk + 2] = xi.z;
+    touch |= 1ull << k;
+  }
+  m->mask[e][p] = touch;
+
+  /* walls */
+  part* out = &o->q[i];
+  *out = *a;
+  int nw = 0;
+  uint32_t st = 0;
+  const int rot = S->rot;
+  const real rc = o->rot_c[a->sys], rsn = o->rot_s[a->sys];
+  /* the polyhedron's wall histories (by wall id), new ones in processing order */
+  real* wh = m->wh + (size_t)p * MIX_WSLOTS * 3;
+  int* wid = m->wid + (size_t)p * MIX_WSLOTS;
+  const int nw_o = m->wn[p];
+  real oh[MIX_WSLOTS][3];
+  int oid[MIX_WSLOTS];
+  for (int q_ = 0; q_ < MIX_WSLOTS; ++q_) {
+    oid[q_] = q_ < nw_o ? wid[q_] : -1;
+    for (int c_ = 0; c_ < 3; ++c_) oh[q_][c_] = q_ < nw_o ? wh[3 * q_ + c_] : 0;
+  }
+#define MIX_WALL(ID, H, MOVING)                                                               \
+  do {                                                                                        \
+    v3 xi_ = mk(0, 0, 0);                                                                     \
+    for (int q_ = 0; q_ < MIX_WSLOTS; ++q_)                                                   \
+      if (oid[q_] == (ID)) xi_ = mk(oh[q_][0], oh[q_][1], oh[q_][2]);                         \
+    const v3 vw_ = (MOVING) ? mul(cross(S->rot_a, sub(add(a->pos, (H).ca), S->rot_o)), S->rot_w) \
+                            : mk(0, 0, 0);                                                    \
+    const v3 vct_ = sub(add(a->vel, cross(a->w, (H).ca)), vw_);                               \
+    v3 F_, t0_;                                                                               \
+    contact_law(o, S, S->mu_w, (H).n, (H).delta, 0, SH->mass, vct_, vct_, mk(0, 0, 0), 0, &xi_, \
+                &F_, &t0_);                                                                   \
+    f = add(f, F_);                                                                           \
+    t = add(t, cross((H).ca, F_));                                                            \
+    if (nw < MIX_WSLOTS) {                                                                    \
+      wh[3 * nw] = xi_.x; wh[3 * nw + 1] = xi_.y; wh[3 * nw + 2] = xi_.z;                     \
+      wid[nw] = (ID);                                                                         \
+      ++nw;                                                                                   \
+    } else {                                                                                  \
+      st |= ST_OVERFLOW;                                                                      \
+    }                                                                                         \
+  } while (0)
+  for (int w = S->wall0; w < S->wall0 + S->nwall; ++w) {
+    const wallc* W = &o->W[w];
+    mhit h;
+    if (W->kind == BLAZE_WALL_PLANE && hull_plane(W->a, W->r, a->pos, &A, &h))
+      MIX_WALL(w, h, rot && W->turning);
+  }
+  int cc[3];
+  const v3 pd = rot ? add(S->rot_o, rot_about(S->rot_a, rc, -rsn, sub(a->pos, S->rot_o))) : a->pos;
+  if (S->ntri > 0 && cell_of(S, pd, cc)) {
+    /* the polyhedron in the drum's frame */
+    double Vd[MIX_V * 4], Fd[MIX_F * 4];
+    hullr D = A;
+    if (rot) {
+      const dv3 ax = dof(S->rot_a);
+      const double c = (double)rc, s = -(double)rsn;
+      for (int k = 0; k < A.nv; ++k) {
+        const dv3 v = rot_about_d(ax, c, s, d4v(A.V + 4 * k));
+        Vd[4 * k] = v.x; Vd[4 * k + 1] = v.y; Vd[4 * k + 2] = v.z; Vd[4 * k + 3] = 0.0;
+      }
+      for (int f2 = 0; f2 < A.nf; ++f2) {
+        const dv3 nn = rot_about_d(ax, c, s, d4v(A.F + 4 * f2));
+        Fd[4 * f2] = nn.x; Fd[4 * f2 + 1] = nn.y; Fd[4 * f2 + 2] = nn.z; Fd[4 * f2 + 3] = A.F[4 * f2 + 3];
+      }
+      D.V = Vd;
+      D.F = Fd;
+    }
+    const real lim = (real)SH->rb * (real)1.001f + (real)1e-3f;
+    mhit hits[MIX_HITS];
+    dv3 nds[MIX_HITS];
+    int ids[MIX_HITS], nhit = 0;
+    for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+      const wallc* W = &o->W[w];
+      int reg, feat;
+      const v3 cp = closest_tri(pd, W->a, W->b, W->c, &reg, &feat);
+      const v3 dd = sub(pd, cp);
+      if (!(dot(dd, dd) < lim * lim)) continue;
+      const dv3 o0 = dof(pd);
+      dv3 T[3];
+      T[0] = dsub(dof(W->a), o0);
+      T[1] = dsub(dof(W->b), o0);
+      T[2] = dsub(dof(W->c), o0);
+      mhit h;
+      dv3 nd;
+      if (!hull_tri(&D, T, d4v(W->n64), &h, &nd)) continue;
+      if (nhit < MIX_HITS) {
+        hits[nhit] = h;
+        nds[nhit] = nd;
+        ids[nhit] = w;
+        ++nhit;
+      } else {
+        st |= ST_OVERFLOW;
+      }
+    }
+    for (int q = 0; q < nhit; ++q) {
+      int keep = 1;
+      for (int c2 = 0; c2 < nhit && keep; ++c2) {
+        if (c2 == q || !(ddot(nds[q], nds[c2]) > COPLANAR)) continue;
+        const real da = hits[q].delta, dc = hits[c2].delta;
+        if (dc > da || (dc == da && ids[c2] < ids[q])) keep = 0;
+      }
+      if (!keep) continue;
+      mhit h = hits[q];
+      if (rot) {
+        h.n = rot_about(S->rot_a, rc, rsn, h.n);
+        h.ca = rot_about(S->rot_a, rc, rsn, h.ca);
+      }
+      MIX_WALL(ids[q], h, rot);
+    }
+  }
+#undef MIX_WALL
+  o->status |= st;
+  m->wn[p] = nw;
+  out->wmask = 0;
+
+  /* translation; Euler's equations in the body frame; the quaternion */
+  const real inv_m = (real)1.0 / SH->mass;
+  const v3 acc = add(mul(f, inv_m), S->g);
+  const v3 v = add(a->vel, mul(acc, dt));
+  const v3 x = add(a->pos, mul(v, dt));
+  real* qq = m->quat + 4 * p;
+  const real qw = qq[0], qx = qq[1], qy = qq[2], qz = qq[3];
+  real R[9];
+  {
+    const real s = (real)2.0 / (((qw * qw + qx * qx) + qy * qy) + qz * qz);
+    R[0] = (real)1.0 - s * (qy * qy + qz * qz);
+    R[1] = s * (qx * qy - qw * qz);
+    R[2] = s * (qx * qz + qw * qy);
+    R[3] = s * (qx * qy + qw * qz);
+    R[4] = (real)1.0 - s * (qx * qx + qz * qz);
+    R[5] = s * (qy * qz - qw * qx);
+    R[6] = s * (qx * qz - qw * qy);
+    R[7] = s * (qy * qz + qw * qx);
+    R[8] = (real)1.0 - s * (qx * qx + qy * qy);
+  }
+#define MV(M, u) mk(((M)[0] * (u).x + (M)[1] * (u).y) + (M)[2] * (u).z, \
+                    ((M)[3] * (u).x + (M)[4] * (u).y) + (M)[5] * (u).z, \
+                    ((M)[6] * (u).x + (M)[7] * (u).y) + (M)[8] * (u).z)
+#define MTV(M, u) mk(((M)[0] * (u).x + (M)[3] * (u).y) + (M)[6] * (u).z, \
+                     ((M)[1] * (u).x + (M)[4] * (u).y) + (M)[7] * (u).z, \
+                     ((M)[2] * (u).x + (M)[5] * (u).y) + (M)[8] * (u).z)
+  const v3 tb = MTV(R, t), wb = MTV(R, a->w);
+  const v3 lb = MV(SH->inertia, wb);
+  const v3 rhs = sub(tb, cross(wb, lb));
+  const v3 dwb = MV(SH->iinv, rhs);
+  const v3 wb2 = add(wb, mul(dwb, dt));
+  const v3 w = MV(R, wb2);
+#undef MV
+#undef MTV
+  const real hdt = (real)0.5 * dt;
+  const real nw_ = -((w.x * qx + w.y * qy) + w.z * qz);
+  const v3 nv_ = add(mk(qw * w.x, qw * w.y, qw * w.z), cross(w, mk(qx, qy, qz)));
+  real q2w = qw + hdt * nw_, q2x = qx + hdt * nv_.x, q2y = qy + hdt * nv_.y, q2z = qz + hdt * nv_.z;
+  const real qi = (real)1.0 / SQRT(((q2w * q2w + q2x * q2x) + q2y * q2y) + q2z * q2z);
+  qq[0] = q2w * qi; qq[1] = q2x * qi; qq[2] = q2y * qi; qq[3] = q2z * qi;
+  const real path = m->path[p] + len(v) * dt;
+  m->path[p] = path;
+  out->pos = x;
+  out->vel = v;
+  out->w = w;
+  if (!(isfinite((double)x.x) && isfinite((double)x.y) && isfinite((double)x.z)))
+    o->status |= ST_NONFINITE;
+  if (path > (real)0.5 * o->skin) *req = 1;
+  o->cap_f[i] = f;
+  o->cap_t[i] = t;
+}
+
 /* One recorded step of the reverse sweep's tape: the step's input state
  * (after its re-sort), the list it used with masks and histories before the
  * step, and for a re-sort step the permutation and history sources. */
@@ -620,8 +1594,10 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
   }
   const real dt = o->dt;
   int req = 0;
+  if (o->mix) mix_geometry(o);
   for (int i = 0; i < n; ++i) {
     const part* a = &o->p[i];
+    if (a->poly >= 0) continue;   /* stepped by mix_poly_step */
     const sysc* S = &o->S[a->sys];
     const real ra = a->r;
     const real ma = S->dens43pi * ((ra * ra) * ra);
@@ -637,6 +1613,17 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
       if (!(d2 < sr * sr)) continue;
       const real dist = SQRT(d2);
       if (!(dist > 0)) continue;
+      if (b->poly >= 0) {
+        v3 xi = mk(0, 0, 0);
+        if ((M[i] >> k) & 1u) xi = mk(H[3 * sk], H[3 * sk + 1], H[3 * sk + 2]);
+        v3 F, T;
+        if (!mix_sphere_contact(o, S, a, ma, b, &xi, &F, &T)) continue;
+        H[3 * sk] = xi.x; H[3 * sk + 1] = xi.y; H[3 * sk + 2] = xi.z;
+        mask |= 1u << k;
+        f = add(f, F);
+        t = add(t, T);
+        continue;
+      }
       const v3 nrm = mul(rel, (real)1.0 / dist);
       const real delta = overlap_pair(ra, rb, a->pos, b->pos);
       if (!(delta > 0)) continue;
@@ -710,6 +1697,8 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
     o->cap_f[i] = f;
     o->cap_t[i] = t;
   }
+  if (o->mix)
+    for (int p = 0; p < o->mix->npoly; ++p) mix_poly_step(o, p, &req);
   part* tmp = o->p; o->p = o->q; o->q = tmp;
   if (req) o->rebuild_req = 1;
   /* the drums' turn advances after the step (k_ens_rot_tick) */

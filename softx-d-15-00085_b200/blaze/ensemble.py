@@ -93,6 +93,8 @@ def load():
                                                     P(C.c_double), _f]
         lib.blaze_ens_set_polyhedra.argtypes = [C.c_void_p, P(Shape), C.c_int, _i, _f]
         lib.blaze_ens_get_orientations.argtypes = [C.c_void_p, _f]
+        lib.blaze_ens_set_profile.argtypes = [C.c_void_p, C.c_int]
+        lib.blaze_ens_profile.argtypes = [C.c_void_p, _f, _i]
         _bound = True
     return lib
 
@@ -266,6 +268,18 @@ class Ensemble:
 
     def rebuild_kernels(self):
         return self.lib.blaze_ens_rebuild_kernels(self.h)
+
+    def set_profile(self, on):
+        _check(self.lib.blaze_ens_set_profile(self.h, int(bool(on))), "blaze_ens_set_profile")
+
+    def profile(self):
+        """(ms of re-sorts, polyhedron geometry, sphere step, polyhedron step)
+        summed over the plain steps profiled, and their count."""
+        ms = np.zeros(4, np.float32)
+        n = C.c_int()
+        _check(self.lib.blaze_ens_profile(self.h, _ptr(ms, C.c_float), C.byref(n)),
+               "blaze_ens_profile")
+        return ms.astype(np.float64), n.value
 
 
 class Adjoint:

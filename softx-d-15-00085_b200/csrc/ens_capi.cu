@@ -97,7 +97,14 @@ struct blaze_ens {
   float* d_ppath = nullptr;
   double4* d_gv = nullptr;
   double4* d_gf = nullptr;
+  float4* d_pwh = nullptr;
+  int* d_pwn = nullptr;
   MixList ml[2] = {};
+  // blaze_ens_set_profile: plain steps timed by phase
+  bool prof = false;
+  cudaEvent_t pev[5] = {};
+  double prof_ms[4] = {0.0, 0.0, 0.0, 0.0};
+  int prof_n = 0;
 };
 
 namespace {
@@ -142,6 +149,8 @@ MixBufs mix_bufs(const blaze_ens* e) {
   m.ppath = e->d_ppath;
   m.gv = e->d_gv;
   m.gf = e->d_gf;
+  m.wh = e->d_pwh;
+  m.wn = e->d_pwn;
   m.L[0] = e->ml[0];
   m.L[1] = e->ml[1];
   m.npoly = e->npoly;
@@ -307,11 +316,14 @@ void free_ens(blaze_ens* e) {
   f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw); f(e->d_rot);
   f(e->d_shapes); f(e->d_bv); f(e->d_bn); f(e->d_faces); f(e->d_edges); f(e->d_shape_of);
   f(e->d_pidx); f(e->d_quat); f(e->d_quat0); f(e->d_pat); f(e->d_ppath); f(e->d_gv); f(e->d_gf);
+  f(e->d_pwh); f(e->d_pwn);
   for (int k = 0; k < 2; ++k) {
     f(e->ml[k].idx); f(e->ml[k].cnt); f(e->ml[k].mlo); f(e->ml[k].mhi);
     f(e->ml[k].hx); f(e->ml[k].hy); f(e->ml[k].hz);
   }
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
+  for (int k = 0; k < 5; ++k)
+    if (e->pev[k]) cudaEventDestroy(e->pev[k]);
   if (e->h_flags) cudaFreeHost(e->h_flags);
   if (e->aux2) cudaStreamDestroy(e->aux2);
   if (e->aux) cudaStreamDestroy(e->aux);
@@ -368,11 +380,17 @@ int rebuild_kernel_count(const blaze_ens* e) {
 
 // The step's kernels: polyhedron geometry, the sphere step, the polyhedron
 // step (the last two read the same input state and write disjoint entries).
-void launch_step_kernels(blaze_ens* e, StepLink link, cudaStream_t st) {
+// ev (profiling, or null): recorded after the polyhedron geometry, the
+// sphere step and the polyhedron step.
+void launch_step_kernels(blaze_ens* e, StepLink link, cudaStream_t st,
+                         const cudaEvent_t* ev = nullptr) {
   const EnsCapture* cap = e->opt.capture_forces ? &e->cap : nullptr;
   if (e->npoly > 0) mix_launch_geom(mix_bufs(e), st);
+  if (ev) cudaEventRecord(ev[0], st);
   ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, cap, e->opt.block, st);
+  if (ev) cudaEventRecord(ev[1], st);
   if (e->npoly > 0) mix_launch_poly_step(geom(e), e->b, mix_bufs(e), e->cur, e->ctl, link, cap, st);
+  if (ev) cudaEventRecord(ev[2], st);
 }
 
 int step_kernel_count(const blaze_ens* e) {
@@ -380,13 +398,24 @@ int step_kernel_count(const blaze_ens* e) {
 }
 
 int enqueue_step(blaze_ens* e) {
+  if (e->prof) CK(cudaEventRecord(e->pev[0], e->stream));
   launch_gate(e->ctl, e->stream);
   int rc = enqueue_rebuild(e, &e->ctl->rebuilt, e->stream);
   if (rc) return rc;
-  launch_step_kernels(e, StepLink{&e->ctl->rebuilt, 0, 0}, e->stream);
+  if (e->prof) CK(cudaEventRecord(e->pev[1], e->stream));
+  launch_step_kernels(e, StepLink{&e->ctl->rebuilt, 0, 0}, e->stream, e->prof ? e->pev + 2 : nullptr);
   if (e->any_rot) ens_launch_rot_tick(geom(e), e->nsys, e->stream);
   e->last_launches += 1 + step_kernel_count(e) + rebuild_kernel_count(e);
   e->cur ^= 1;
+  if (e->prof) {   // re-sort, polyhedron geometry, sphere step, polyhedron step
+    CK(cudaEventSynchronize(e->pev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, e->pev[k], e->pev[k + 1]));
+      e->prof_ms[k] += ms;
+    }
+    e->prof_n += 1;
+  }
   return 0;
 }
 
@@ -901,7 +930,24 @@ int blaze_ens_step(blaze_ens* e, int nsteps) {
   if (!e || nsteps < 0 || !e->state_set) return -1;
   e->last_launches = 0;
   if (nsteps > 0) e->stepped = true;
-  return advance(e, nsteps, e->opt.use_graph != 0);
+  return advance(e, nsteps, e->opt.use_graph != 0 && !e->prof);
+}
+
+int blaze_ens_set_profile(blaze_ens* e, int on) {
+  if (!e) return -1;
+  if (on && !e->pev[0])
+    for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&e->pev[k]));
+  e->prof = on != 0;
+  for (int k = 0; k < 4; ++k) e->prof_ms[k] = 0.0;
+  e->prof_n = 0;
+  return 0;
+}
+
+int blaze_ens_profile(blaze_ens* e, float* ms4, int* steps) {
+  if (!e || !ms4) return -1;
+  for (int k = 0; k < 4; ++k) ms4[k] = (float)e->prof_ms[k];
+  if (steps) *steps = e->prof_n;
+  return 0;
 }
 
 int blaze_ens_sync(blaze_ens* e) {
@@ -1172,7 +1218,10 @@ int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes
     if ((rc = realloc_dev(&e->d_shape_of, (size_t)np)) || (rc = realloc_dev(&e->d_pidx, (size_t)np)) ||
         (rc = realloc_dev(&e->d_quat, (size_t)np)) || (rc = realloc_dev(&e->d_quat0, (size_t)np)) ||
         (rc = realloc_dev(&e->d_pat, (size_t)np)) || (rc = realloc_dev(&e->d_ppath, (size_t)np)) ||
-        (rc = realloc_dev(&e->d_gv, (size_t)np * kMixMaxV)) || (rc = realloc_dev(&e->d_gf, (size_t)np * kMixMaxF)))
+        (rc = realloc_dev(&e->d_gv, (size_t)np * kMixMaxV)) ||
+        (rc = realloc_dev(&e->d_gf, (size_t)np * kMixMaxF)) ||
+        (rc = realloc_dev(&e->d_pwh, (size_t)np * kMixWallSlots)) ||
+        (rc = realloc_dev(&e->d_pwn, (size_t)np)))
       return rc;
     for (int k = 0; k < 2; ++k) {
       MixList& L = e->ml[k];

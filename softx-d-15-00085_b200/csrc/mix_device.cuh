@@ -23,8 +23,11 @@
 //   polyhedron - plane    the deepest vertex below the plane
 // All of it in FP64 from the FP32 state: a resting contact's overlap is
 // ~1e-6 cm against vertex offsets of ~1 cm and positions of ~50 cm.  The
-// contact point is the mean of the penetrating vertices (a face axis) or the
-// midpoint of the closest points of the two edges (an edge axis).  The law
+// contact point is the mean of the penetrating vertices weighted by their
+// depths (a face axis: it moves continuously as vertices enter and leave,
+// and shifts toward the deeper side under an off-centre load, as a pressure
+// distribution would) or the midpoint of the closest points of the two
+// edges (an edge axis).  The law
 // is the ensemble's linear law with tangential history, evaluated with the
 // contact point's relative velocity, without rolling friction.
 #pragma once
@@ -41,6 +44,7 @@ constexpr int kMixMaxV = 16;     // vertices of a shape
 constexpr int kMixMaxF = 28;     // triangular faces (2 V - 4)
 constexpr int kMixMaxE = 42;     // edges (3 V - 6)
 constexpr int kMixSlots = 64;    // neighbour slots of a polyhedron
+constexpr int kMixWallSlots = 8; // wall contacts (tangential histories) of a polyhedron
 
 struct MixShapeDev {
   int nv, nf, ne, pad;
@@ -69,7 +73,9 @@ struct MixList {
 // f1 < f2).  Per polyhedron id: its shape, orientation (w, x, y, z), memory
 // position, path since the last re-sort, and world-frame geometry rebuilt
 // every step: gv (vertex offsets from the centre) and gf (unit normal,
-// offset h: the face plane is n . x = h relative to the centre), FP64.
+// offset h: the face plane is n . x = h relative to the centre), FP64; its
+// wall histories (wh: kMixWallSlots of (xi, wall id), wn in use), kept per
+// id (a polyhedron's vel4.w carries no wall-history mask).
 struct MixBufs {
   const MixShapeDev* shapes;
   const float4* bv;
@@ -82,6 +88,8 @@ struct MixBufs {
   float* ppath;
   double4* gv;
   double4* gf;
+  float4* wh;
+  int* wn;
   MixList L[2];
   int npoly;
 };
@@ -314,24 +322,26 @@ __device__ __forceinline__ bool hull_hull_finish(const SatPick& q, double3 d, co
     nAB = dxyz(P);
     s = q.sA;
     double3 acc = dv(0.0, 0.0, 0.0);
-    int m = 0;
+    double wsum = 0.0;
     for (int k = 0; k < nvB; ++k) {
       const double3 v = dadd(d, dxyz(VB[k]));
-      if (((P.x * v.x + P.y * v.y) + P.z * v.z) - P.w < 0.0) { acc = dadd(acc, v); ++m; }
+      const double t = ((P.x * v.x + P.y * v.y) + P.z * v.z) - P.w;
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
     }
-    cp = dscale(acc, 1.0 / (double)(m > 0 ? m : 1));
+    cp = dscale(acc, 1.0 / wsum);
   } else if (kind == 1) {
     const double4 P = FB[q.fB];
     nAB = dneg(dxyz(P));
     s = q.sB;
     double3 acc = dv(0.0, 0.0, 0.0);
-    int m = 0;
+    double wsum = 0.0;
     for (int k = 0; k < nvA; ++k) {
       const double3 v = dxyz(VA[k]);
       const double3 w = dsub(v, d);
-      if (((P.x * w.x + P.y * w.y) + P.z * w.z) - P.w < 0.0) { acc = dadd(acc, v); ++m; }
+      const double t = ((P.x * w.x + P.y * w.y) + P.z * w.z) - P.w;
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
     }
-    cp = dscale(acc, 1.0 / (double)(m > 0 ? m : 1));
+    cp = dscale(acc, 1.0 / wsum);
   } else {
     const uchar4 ea = EA[q.eE / neB], eb = EB[q.eE % neB];
     const double3 PA = dxyz(VA[ea.x]), QA = dxyz(VA[ea.y]);
@@ -432,21 +442,24 @@ __device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, con
     n_in = tplus ? nt : dneg(nt);
     s = sT;
     double3 acc = dv(0.0, 0.0, 0.0);
-    int m = 0;
+    double wsum = 0.0;
     for (int k = 0; k < nv; ++k) {
       const double3 v = dxyz(V[k]);
-      if (ddot(n_in, v) - ddot(n_in, T[0]) < 0.0) { acc = dadd(acc, v); ++m; }
+      const double t = ddot(n_in, v) - ddot(n_in, T[0]);
+      if (t < 0.0) { acc = dadd(acc, dscale(v, -t)); wsum = wsum - t; }
     }
-    cp = dscale(acc, 1.0 / (double)(m > 0 ? m : 1));
+    cp = dscale(acc, 1.0 / wsum);
   } else if (kind == 1) {
     const double4 P = F[fP];
     n_in = dneg(dxyz(P));
     s = sP;
     double3 acc = dv(0.0, 0.0, 0.0);
-    int m = 0;
-    for (int k = 0; k < 3; ++k)
-      if (((P.x * T[k].x + P.y * T[k].y) + P.z * T[k].z) - P.w < 0.0) { acc = dadd(acc, T[k]); ++m; }
-    cp = dscale(acc, 1.0 / (double)(m > 0 ? m : 1));
+    double wsum = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double t = ((P.x * T[k].x + P.y * T[k].y) + P.z * T[k].z) - P.w;
+      if (t < 0.0) { acc = dadd(acc, dscale(T[k], -t)); wsum = wsum - t; }
+    }
+    cp = dscale(acc, 1.0 / wsum);
   } else {
     const int e = eE / 3, t = eE % 3;
     const uchar4 ed = E[e];
@@ -471,25 +484,24 @@ __device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, con
 
 // ----------------------------------------------------- polyhedron - plane
 // Plane n . x = pd (n into the domain) against the polyhedron at x: the
-// deepest vertex's depth, the mean of the vertices below the plane.
+// deepest vertex's depth, the vertices below the plane weighted by depth.
 __device__ __forceinline__ bool hull_plane(float3 n, float pd, float3 x, const double4* V, int nv,
                                            MixHit& h) {
   const double3 nn = d3(n);
   const double base = ddot(nn, d3(x)) - (double)pd;
-  double lo = 1e300;
+  double lo = 1e300, wsum = 0.0;
   double3 acc = dv(0.0, 0.0, 0.0);
-  int m = 0;
   for (int k = 0; k < nv; ++k) {
     const double3 v = dxyz(V[k]);
     const double s = base + ddot(nn, v);
     if (s < lo) lo = s;
-    if (s < 0.0) { acc = dadd(acc, v); ++m; }
+    if (s < 0.0) { acc = dadd(acc, dscale(v, -s)); wsum = wsum - s; }
   }
   const float df = (float)(-lo);
-  if (!(df > 0.0f) || m == 0) return false;
+  if (!(df > 0.0f) || !(wsum > 0.0)) return false;
   h.n = n;
   h.delta = df;
-  h.ca = to_f3(dscale(acc, 1.0 / (double)m));
+  h.ca = to_f3(dscale(acc, 1.0 / wsum));
   h.cb = h.ca;
   return true;
 }

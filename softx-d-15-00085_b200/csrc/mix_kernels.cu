@@ -29,6 +29,7 @@ k_mix_mark(StateBuf s, MixBufs m, const int* __restrict__ caller_index,
   m.quat[p] = quat[p];
   m.pat[p] = i;
   m.ppath[p] = 0.0f;
+  m.wn[p] = 0;
   for (int c = 0; c < 2; ++c) {
     m.L[c].cnt[p] = 0;
     m.L[c].mlo[p] = 0;
@@ -244,13 +245,10 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
   const int e = ctl->epoch & 1;
   const MixList L = m.L[e];
   const size_t P = (size_t)m.npoly;
-  const size_t stride = (size_t)b.stride;
   const int i = m.pat[p];
   const float4 pa4 = in.pos[i], va4 = in.vel[i], wa4 = in.angv[i];
   const float3 xa = xyz(pa4), va = xyz(va4), wa = xyz(wa4);
-  const uint32_t bits = __float_as_uint(va4.w);
-  const uint32_t sys = bits & kSysMask;
-  const uint32_t wmask_o = bits >> kSysBits;
+  const uint32_t sys = __float_as_uint(va4.w) & kSysMask;
   const EnsSysDev& S = g.sys[sys];
   const int shp = m.shape_of[p];
   const MixShapeDev& SH = m.shapes[shp];
@@ -451,19 +449,19 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
     if (touch[0] != mlo) L.mlo[p] = touch[0];
     if (touch[1] != mhi) L.mhi[p] = touch[1];
 
-    // walls: old history slots (by wall id) in registers, new ones written
-    // in processing order over them
-    float4 oh[kWallSlots];
+    // walls: the old history slots (by wall id), new ones written in
+    // processing order over them
+    float4* wh = m.wh + (size_t)p * kMixWallSlots;
+    const int nw_o = m.wn[p];
+    float4 oh[kMixWallSlots];
 #pragma unroll
-    for (int qs = 0; qs < kWallSlots; ++qs) {
-      oh[qs] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-      if ((wmask_o >> qs) & 1u) oh[qs] = b.wh[e][(size_t)qs * stride + i];
-    }
+    for (int qs = 0; qs < kMixWallSlots; ++qs)
+      oh[qs] = qs < nw_o ? wh[qs] : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
     int nw = 0;
     auto wall = [&](int id, const MixHit& h, bool moving) {
       float3 xi = f3(0.0f, 0.0f, 0.0f);
 #pragma unroll
-      for (int qs = 0; qs < kWallSlots; ++qs)
+      for (int qs = 0; qs < kMixWallSlots; ++qs)
         if (__float_as_int(oh[qs].w) == id) xi = f3(oh[qs].x, oh[qs].y, oh[qs].z);
       const float3 vw = moving ? cross3(S.rot_a, (xa + h.ca) - S.rot_o) * S.rot_w
                                : f3(0.0f, 0.0f, 0.0f);
@@ -471,8 +469,8 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
       mix_wall_law(S, h, mass, va, wa, vw, dt, xi, F, T);
       f = f + F;
       t = t + T;
-      if (nw < kWallSlots) {
-        b.wh[e][(size_t)nw * stride + i] = make_float4(xi.x, xi.y, xi.z, __int_as_float(id));
+      if (nw < kMixWallSlots) {
+        wh[nw] = make_float4(xi.x, xi.y, xi.z, __int_as_float(id));
         ++nw;
       } else {
         st |= kStatusListOverflow;
@@ -499,7 +497,7 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
       }
       wall(sm.hid[a], h, rot);
     }
-    const uint32_t wmask = nw >= kWallSlots ? (1u << kWallSlots) - 1u : (1u << nw) - 1u;
+    m.wn[p] = nw;
 
     // symplectic Euler: translation; rotation by Euler's equations in the
     // body frame, then the quaternion
@@ -538,7 +536,7 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
     q2z = q2z * qi;
     const float path = m.ppath[p] + len3(v) * dt;
     out.pos[i] = make_float4(x.x, x.y, x.z, -rb);
-    out.vel[i] = make_float4(v.x, v.y, v.z, __uint_as_float(sys | (wmask << kSysBits)));
+    out.vel[i] = make_float4(v.x, v.y, v.z, __uint_as_float(sys));
     out.angv[i] = make_float4(w.x, w.y, w.z, __int_as_float(p));
     m.quat[p] = make_float4(q2w, q2x, q2y, q2z);
     m.ppath[p] = path;

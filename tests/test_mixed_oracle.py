@@ -1,0 +1,254 @@
+"""Mixed charge (spheres and convex polyhedra) on the CPU: the shapes' mass
+properties (the library's host function) against closed forms, the rock
+generator, and the FP64 restatement (oracle/ens_oracle.c) against
+mechanics with known answers:
+  - a cube resting on the floor: contact force = weight, overlap = m g / kn,
+    no turn;
+  - a sphere resting on a cube's face: force along the face normal;
+  - two cubes face on face and two cubes with crossing edges (each turned
+    45 degrees, about x and about y): the contact normal is the face normal /
+    the cross product of the edges, the force kn delta, no torque;
+  - a loose cluster of rocks and balls without gravity or walls: the
+    contact forces sum to zero (Newton's third law) at every step, and
+    without damping and friction the kinetic energy after the collisions
+    returns to its value before them.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from bindings import EnsRestated
+from blaze import ensemble as E
+from blaze import synth
+
+
+def hull_shape(v, density):
+    from scipy.spatial import ConvexHull
+    v = np.asarray(v, np.float64)
+    h = ConvexHull(v)
+    f = h.simplices.copy()
+    c = v.mean(axis=0)
+    for k in range(len(f)):
+        a, b, cc = v[f[k]]
+        if np.dot(np.cross(b - a, cc - a), a - c) < 0:
+            f[k] = f[k][[0, 2, 1]]
+    return E.shape(v, f, density), f
+
+
+CUBE = np.array([[x, y, z] for x in (-0.5, 0.5) for y in (-0.5, 0.5) for z in (-0.5, 0.5)])
+RHO = 2.7e-3   # kg/cm^3
+
+
+def test_mass_properties_closed_forms():
+    a = 2.0
+    s, _ = hull_shape(CUBE * a, 1e-3)
+    m, com, J, rb = E.mass_properties(s)
+    m0 = float(np.float32(1e-3)) * a ** 3
+    assert abs(m - m0) < 1e-12 * m0
+    np.testing.assert_allclose(J, np.eye(3) * m0 * a * a / 6.0, rtol=1e-12, atol=1e-15)
+    assert np.abs(com).max() < 1e-15
+    assert abs(rb - math.sqrt(3.0)) < 2e-7 and rb >= math.sqrt(3.0) * (1 - 1e-7)
+    # regular tetrahedron of edge 2 sqrt 2: I = m a^2 / 20 about any axis
+    t = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], np.float64)
+    s, _ = hull_shape(t, 1e-3)
+    m, com, J, rb = E.mass_properties(s)
+    m0 = float(np.float32(1e-3)) * 8.0 / 3.0
+    assert abs(m - m0) < 1e-12 * m0
+    np.testing.assert_allclose(J, np.eye(3) * m0 * 8.0 / 20.0, rtol=1e-12, atol=1e-15)
+
+
+def test_invalid_shapes_rejected():
+    s, f = hull_shape(CUBE, RHO)
+    bad = E.shape(CUBE, f[:, [0, 2, 1]], RHO)        # faces turned inside out
+    with pytest.raises(Exception):
+        E.mass_properties(bad)
+    dent = CUBE.copy()
+    dent[0] *= 0.3                                   # a vertex pushed in: not convex
+    bad = E.shape(dent, f, RHO)
+    with pytest.raises(Exception):
+        E.mass_properties(bad)
+    bad = E.shape(CUBE, f[:-1], RHO)                 # open
+    with pytest.raises(Exception):
+        E.mass_properties(bad)
+
+
+def test_rock_generator():
+    rng = np.random.default_rng(2)
+    for _ in range(40):
+        v, f = synth.rock_hull(rng)
+        assert 8 <= len(v) <= 16 and len(f) == 2 * len(v) - 4
+        # points on a sphere of radius <= 1 cm, moved to their centre of mass
+        r = np.linalg.norm(v, axis=1)
+        assert 0.25 <= r.max() <= 1.25
+        s = E.shape(v, f, RHO)
+        m, com, J, rb = E.mass_properties(s)
+        assert np.abs(com).max() < 1e-6 * rb
+        assert np.all(np.linalg.eigvalsh(J) > 0)
+
+
+def scene(pos, rad, shapes, shape_of, quat, L=20.0, gravity=(0.0, 0.0, -981.0), kn=1e5,
+          restitution=0.4, mu=0.6, dt=1e-5, precision="f64", vel=None, avel=None):
+    rb = max([max(rad)] + [float(np.linalg.norm(np.asarray(s.verts).reshape(-1, 3)[:s.nverts],
+                                                axis=1).max()) for s in shapes])
+    cell = 2.0 * rb + 0.04 + 1e-3
+    walls = synth.box_walls(L, L)
+    s = synth.box_system(len(pos), L, L, cell, 0, density=7.8e-3, kn=kn, restitution=restitution,
+                         mu=mu, gravity=gravity)
+    o = EnsRestated([s], walls, E.LAW_LINEAR, dt, 0.04, 32, precision=precision)
+    o.set_state(np.asarray(pos, np.float64), np.asarray(rad, np.float64), vel, avel)
+    o.set_polyhedra(shapes, np.asarray(shape_of, np.int32), np.asarray(quat, np.float64))
+    return o, s
+
+
+def quat_about(axis, ang):
+    a = np.asarray(axis, np.float64) / np.linalg.norm(axis)
+    return np.concatenate([[math.cos(ang / 2)], a * math.sin(ang / 2)])
+
+
+def test_cube_rests_on_the_floor():
+    cube, _ = hull_shape(CUBE, RHO)
+    m = E.mass_properties(cube)[0]
+    o, _ = scene([[10.0, 10.0, 0.5]], [0.87], [cube], [0], [[1, 0, 0, 0]])
+    o.step(30000)
+    f, t = o.forces()
+    st = o.state()
+    q = o.orientations()
+    delta = m * 981.0 / 1e5
+    print("cube on the floor: force %s (weight %.6g), sink %.4g (m g / kn %.4g)"
+          % (f[0], m * 981.0, 0.5 - st["pos"][0, 2], delta))
+    assert abs(f[0, 2] - m * 981.0) < 1e-3 * m * 981.0
+    assert np.abs(f[0, :2]).max() < 1e-9 * m * 981.0
+    assert abs((0.5 - st["pos"][0, 2]) - delta) < 1e-3 * delta
+    assert np.abs(st["avel"][0]).max() < 1e-9 and np.abs(q[0] - [1, 0, 0, 0]).max() < 1e-12
+    assert st["status"] == 0
+
+
+def test_sphere_rests_on_a_face():
+    cube, _ = hull_shape(CUBE, RHO)
+    r = 0.3
+    o, s = scene([[10.0, 10.0, 0.5], [10.1, 10.05, 1.0 + r]], [0.87, r], [cube], [0, -1],
+                 [[1, 0, 0, 0], [1, 0, 0, 0]])
+    o.step(30000)
+    f, t = o.forces()
+    st = o.state()
+    ms = s.density * 4.0 / 3.0 * math.pi * r ** 3
+    i = int(np.nonzero(st["pid"] == 1)[0][0])
+    print("sphere on a cube: force on the sphere %s (weight %.6g)" % (f[i], ms * 981.0))
+    assert abs(f[i, 2] - ms * 981.0) < 1e-3 * ms * 981.0
+    # under the off-centre load the cube tilts by ~4 delta x / side^2 (the
+    # depth-weighted contact point moves under the load): 1e-5 rad here
+    assert np.abs(f[i, :2]).max() < 1e-4 * ms * 981.0
+    # it settles where it was put (a slide of ~1e-4 cm while the cube tilts)
+    assert np.abs(st["pos"][i, :2] - [10.1, 10.05]).max() < 1e-3
+    assert np.abs(st["vel"]).max() < 1e-3
+
+
+@pytest.mark.parametrize("kind", ["face", "edge"])
+def test_cube_pair_normal_and_force(kind):
+    cube, _ = hull_shape(CUBE, RHO)
+    delta = 2e-4
+    if kind == "face":
+        qa, qb = [1, 0, 0, 0], [1, 0, 0, 0]
+        gap = 1.0
+    else:   # A turned 45 degrees about x (top edge along x), B about y (bottom edge along y)
+        qa, qb = quat_about([1, 0, 0], math.pi / 4), quat_about([0, 1, 0], math.pi / 4)
+        gap = math.sqrt(2.0)
+    z0 = 10.0
+    o, _ = scene([[10.0, 10.0, z0], [10.0, 10.0, z0 + gap - delta]], [0.87, 0.87], [cube], [0, 0],
+                 [qa, qb], gravity=(0.0, 0.0, 0.0))
+    o.step(1)
+    f, t = o.forces()
+    st = o.state()
+    ib = int(np.nonzero(st["pid"] == 1)[0][0])
+    ia = 1 - ib
+    d_true = gap - ((z0 + gap - delta) - z0)   # the FP64 restatement keeps the inputs exact
+    print("%s contact: force on B %s, kn delta %.6g, torque on B %s"
+          % (kind, f[ib], 1e5 * d_true, t[ib]))
+    np.testing.assert_allclose(f[ib], [0.0, 0.0, 1e5 * d_true], rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(f[ia], -f[ib], rtol=0, atol=1e-12)
+    # no lever arm (the turns are the float-rounded 45 degrees)
+    tol = 1e-6 * np.linalg.norm(f[ib]) * 1.0
+    assert np.abs(t[ib]).max() < tol and np.abs(t[ia]).max() < tol
+
+
+def cluster(seed=5, n_rocks=8, n_spheres=40):
+    rng = np.random.default_rng(seed)
+    shapes = synth.rock_shapes(n_rocks, seed=seed)
+    pts = synth.lattice_fill(None, (8.0, 8.0, 8.0), (12.5, 12.5, 12.5), 1.55, rng)
+    pts = pts[rng.permutation(len(pts))[:n_rocks + n_spheres]]
+    rad = np.concatenate([rng.uniform(0.3, 0.6, n_spheres),
+                          [synth._bounding_radius(s) for s in shapes]])
+    so = np.concatenate([np.full(n_spheres, -1), np.arange(n_rocks)])
+    q = np.zeros((len(pts), 4))
+    q[:, 0] = 1.0
+    q[n_spheres:] = synth.random_quaternions(rng, n_rocks)
+    centre = np.array([10.25, 10.25, 10.25])
+    vel = (centre - pts) * 20.0 + rng.normal(scale=5.0, size=pts.shape)   # inward
+    avel = np.zeros_like(pts)
+    avel[n_spheres:] = rng.normal(scale=20.0, size=(n_rocks, 3))
+    return pts, rad, shapes, so, q, vel, avel
+
+
+def test_third_law_in_a_cluster():
+    pts, rad, shapes, so, q, vel, avel = cluster()
+    o, _ = scene(pts, rad, shapes, so, q, gravity=(0.0, 0.0, 0.0), L=40.0, vel=vel, avel=avel)
+    worst, contacts = 0.0, 0
+    for k in range(300):
+        o.step(10)
+        f, t = o.forces()
+        nz = np.linalg.norm(f, axis=1) > 0
+        contacts = max(contacts, int(nz.sum()))
+        if nz.any():
+            worst = max(worst, np.linalg.norm(f.sum(axis=0)) / np.linalg.norm(f, axis=1).max())
+    print("cluster: up to %d particles in contact; |sum F| / max |F| = %.2e" % (contacts, worst))
+    assert contacts >= 10
+    assert worst < 1e-12
+
+
+def kinetic_energy(o, shapes, so, rho_s):
+    st = o.state()
+    q = o.orientations()
+    e = 0.0
+    for k in range(len(st["pid"])):
+        pid = st["pid"][k]
+        v, w = st["vel"][k], st["avel"][k]
+        if so[pid] < 0:
+            m = rho_s * 4.0 / 3.0 * math.pi * st["radius"][k] ** 3
+            e += 0.5 * m * v @ v + 0.5 * (0.4 * m * st["radius"][k] ** 2) * w @ w
+        else:
+            m, _, J, _ = E.mass_properties(shapes[so[pid]])
+            qw, qx, qy, qz = q[k]
+            R = np.array([[1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy)],
+                          [2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx)],
+                          [2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)]])
+            wb = R.T @ w
+            e += 0.5 * m * v @ v + 0.5 * wb @ J @ wb
+    return e
+
+
+def test_elastic_frictionless_collisions_keep_energy():
+    """Restitution 1 (no damping), no friction: two rocks and a ball meet
+    and part; the kinetic energy afterwards equals the energy before within
+    the integrator's error."""
+    shapes = synth.rock_shapes(2, seed=7)
+    pts = np.array([[9.0, 10.0, 10.0], [11.0, 10.1, 10.05], [10.0, 11.2, 10.0]])
+    rad = np.array([synth._bounding_radius(shapes[0]), synth._bounding_radius(shapes[1]), 0.4])
+    so = np.array([0, 1, -1])
+    q = np.array([quat_about([1, 2, 3], 0.7), quat_about([3, -1, 2], 1.9), [1, 0, 0, 0]])
+    vel = np.array([[50.0, 0.0, 0.0], [-50.0, 0.0, 0.0], [0.0, -40.0, 0.0]])
+    avel = np.array([[0.0, 0.0, 30.0], [10.0, 0.0, 0.0], [0.0, 0.0, 0.0]])
+    o, s = scene(pts, rad, shapes, so, q, gravity=(0.0, 0.0, 0.0), L=40.0, restitution=1.0,
+                 mu=0.0, dt=2e-6, vel=vel, avel=avel)
+    e0 = kinetic_energy(o, shapes, so, s.density)
+    touched = False
+    for _ in range(100):
+        o.step(200)
+        f, _ = o.forces()
+        touched = touched or bool(np.abs(f).max() > 0)
+    f, _ = o.forces()
+    e1 = kinetic_energy(o, shapes, so, s.density)
+    print("elastic collisions: E before %.6g after %.6g (relative change %.2e), touched %s"
+          % (e0, e1, e1 / e0 - 1.0, touched))
+    assert touched and np.abs(f).max() == 0.0
+    assert abs(e1 / e0 - 1.0) < 2e-3
