@@ -679,8 +679,8 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
             "cell_cm": float(S[0].cell), "rebuilds": rebuilds, "gpu_launches": launches,
             "status": st["status"],
             "plain_step_ms_by_phase": {k: float(v) / max(nph, 1) for k, v in
-                                       zip(("resort", "polyhedron_geometry", "sphere_step",
-                                            "polyhedron_step"), ph)},
+                                       zip(("resort", "polyhedron_geometry", "polyhedron_step",
+                                            "sphere_step"), ph)},
             "mean_tangential_velocity_cm_s": {"spheres": float(vt[~rocks].mean()),
                                               "rocks": float(vt[rocks].mean())}}
 

@@ -141,7 +141,7 @@ int blaze_ens_rebuild_kernels(blaze_ens* e);
 /* Profiling: while on, blaze_ens_step runs plain steps, each waiting for the
  * device, and adds their device time by phase: the re-sort (with the gate;
  * zero-work launches when no re-sort is due), the polyhedron geometry, the
- * sphere step, the polyhedron step.  Turning it on clears the sums. */
+ * polyhedron step, the sphere step.  Turning it on clears the sums. */
 int blaze_ens_set_profile(blaze_ens* e, int on);
 /* ms4: the four sums in ms; steps: the plain steps they cover. */
 int blaze_ens_profile(blaze_ens* e, float* ms4, int* steps);

@@ -273,7 +273,7 @@ class Ensemble:
         _check(self.lib.blaze_ens_set_profile(self.h, int(bool(on))), "blaze_ens_set_profile")
 
     def profile(self):
-        """(ms of re-sorts, polyhedron geometry, sphere step, polyhedron step)
+        """(ms of re-sorts, polyhedron geometry, polyhedron step, sphere step)
         summed over the plain steps profiled, and their count."""
         ms = np.zeros(4, np.float32)
         n = C.c_int()

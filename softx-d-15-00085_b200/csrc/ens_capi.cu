@@ -99,6 +99,9 @@ struct blaze_ens {
   double4* d_gf = nullptr;
   float4* d_pwh = nullptr;
   int* d_pwn = nullptr;
+  float4* d_psf = nullptr;
+  float4* d_pst = nullptr;
+  uint8_t* d_twin = nullptr;
   MixList ml[2] = {};
   // blaze_ens_set_profile: plain steps timed by phase
   bool prof = false;
@@ -126,11 +129,9 @@ EnsGeom geom(const blaze_ens* e) {
   g.any_rot = e->any_rot ? 1 : 0;
   g.mix = MixView{};
   if (e->npoly > 0) {
-    g.mix.shapes = e->d_shapes;
-    g.mix.shape_of = e->d_shape_of;
-    g.mix.gv = e->d_gv;
-    g.mix.gf = e->d_gf;
-    g.mix.faces = e->d_faces;
+    g.mix.twin = e->d_twin;
+    g.mix.sf = e->d_psf;
+    g.mix.st = e->d_pst;
     g.mix.npoly = e->npoly;
   }
   return g;
@@ -151,6 +152,9 @@ MixBufs mix_bufs(const blaze_ens* e) {
   m.gf = e->d_gf;
   m.wh = e->d_pwh;
   m.wn = e->d_pwn;
+  m.sf = e->d_psf;
+  m.st = e->d_pst;
+  m.twin = e->d_twin;
   m.L[0] = e->ml[0];
   m.L[1] = e->ml[1];
   m.npoly = e->npoly;
@@ -316,7 +320,7 @@ void free_ens(blaze_ens* e) {
   f(e->d_flags); f(e->cap.f); f(e->cap.t); f(e->d_pw); f(e->d_rot);
   f(e->d_shapes); f(e->d_bv); f(e->d_bn); f(e->d_faces); f(e->d_edges); f(e->d_shape_of);
   f(e->d_pidx); f(e->d_quat); f(e->d_quat0); f(e->d_pat); f(e->d_ppath); f(e->d_gv); f(e->d_gf);
-  f(e->d_pwh); f(e->d_pwn);
+  f(e->d_pwh); f(e->d_pwn); f(e->d_psf); f(e->d_pst); f(e->d_twin);
   for (int k = 0; k < 2; ++k) {
     f(e->ml[k].idx); f(e->ml[k].cnt); f(e->ml[k].mlo); f(e->ml[k].mhi);
     f(e->ml[k].hx); f(e->ml[k].hy); f(e->ml[k].hz);
@@ -369,27 +373,32 @@ int enqueue_rebuild(blaze_ens* e, const int* gate, cudaStream_t st) {
   ens_launch_reorder(e->b, e->cur, n, e->rs.keys[res], e->rs.vals[res], e->cstart, e->cend,
                      e->ncell_tab, e->ctl, gate, st);
   ens_launch_nlist(g, e->b, n, e->rs.vals[res], e->cstart, e->cend, e->ctl, gate, st);
-  if (e->npoly > 0) mix_launch_plist(g, e->b, mix_bufs(e), e->cstart, e->cend, e->ctl, gate, st);
+  if (e->npoly > 0) {
+    mix_launch_plist(g, e->b, mix_bufs(e), e->cstart, e->cend, e->ctl, gate, st);
+    mix_launch_twins(e->b, mix_bufs(e), n, e->ctl, gate, st);
+  }
   ens_launch_epoch(e->ctl, gate, st);
   return 0;
 }
 
 int rebuild_kernel_count(const blaze_ens* e) {
-  return 4 + 3 * std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits) + (e->npoly > 0 ? 1 : 0);
+  return 4 + 3 * std::max(1, (e->key_bits + kRadixBits - 1) / kRadixBits) + (e->npoly > 0 ? 2 : 0);
 }
 
 // The step's kernels: polyhedron geometry, the sphere step, the polyhedron
 // step (the last two read the same input state and write disjoint entries).
-// ev (profiling, or null): recorded after the polyhedron geometry, the
-// sphere step and the polyhedron step.
+// The step's kernels: polyhedron geometry, the polyhedron step (which leaves
+// the sphere-polyhedron pairs' forces on the spheres), the sphere step; the
+// last two read the same input state and write disjoint entries.  ev
+// (profiling, or null): recorded after each of the three.
 void launch_step_kernels(blaze_ens* e, StepLink link, cudaStream_t st,
                          const cudaEvent_t* ev = nullptr) {
   const EnsCapture* cap = e->opt.capture_forces ? &e->cap : nullptr;
   if (e->npoly > 0) mix_launch_geom(mix_bufs(e), st);
   if (ev) cudaEventRecord(ev[0], st);
-  ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, cap, e->opt.block, st);
-  if (ev) cudaEventRecord(ev[1], st);
   if (e->npoly > 0) mix_launch_poly_step(geom(e), e->b, mix_bufs(e), e->cur, e->ctl, link, cap, st);
+  if (ev) cudaEventRecord(ev[1], st);
+  ens_launch_step(geom(e), e->b, e->cur, e->n, e->ctl, link, cap, e->opt.block, st);
   if (ev) cudaEventRecord(ev[2], st);
 }
 
@@ -407,7 +416,7 @@ int enqueue_step(blaze_ens* e) {
   if (e->any_rot) ens_launch_rot_tick(geom(e), e->nsys, e->stream);
   e->last_launches += 1 + step_kernel_count(e) + rebuild_kernel_count(e);
   e->cur ^= 1;
-  if (e->prof) {   // re-sort, polyhedron geometry, sphere step, polyhedron step
+  if (e->prof) {   // re-sort, polyhedron geometry, polyhedron step, sphere step
     CK(cudaEventSynchronize(e->pev[4]));
     for (int k = 0; k < 4; ++k) {
       float ms = 0.0f;
@@ -1221,7 +1230,9 @@ int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes
         (rc = realloc_dev(&e->d_gv, (size_t)np * kMixMaxV)) ||
         (rc = realloc_dev(&e->d_gf, (size_t)np * kMixMaxF)) ||
         (rc = realloc_dev(&e->d_pwh, (size_t)np * kMixWallSlots)) ||
-        (rc = realloc_dev(&e->d_pwn, (size_t)np)))
+        (rc = realloc_dev(&e->d_pwn, (size_t)np)) ||
+        (rc = realloc_dev(&e->d_psf, (size_t)np * kMixSlots)) ||
+        (rc = realloc_dev(&e->d_pst, (size_t)np * kMixSlots)))
       return rc;
     for (int k = 0; k < 2; ++k) {
       MixList& L = e->ml[k];
@@ -1233,6 +1244,7 @@ int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes
     }
     e->poly_cap = np;
   }
+  if (!e->d_twin && (rc = realloc_dev(&e->d_twin, (size_t)e->b.cap * e->n))) return rc;
   {
     std::vector<MixShapeDev> sd(nshapes);
     std::vector<float4> bv((size_t)nshapes * kMixMaxV, make_float4(0, 0, 0, 0));

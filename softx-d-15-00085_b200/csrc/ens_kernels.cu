@@ -24,7 +24,6 @@
 //   Walls use the same law with R* = r, m* = m.
 #include "ens_kernels.cuh"
 #include "ens_device.cuh"
-#include "mix_device.cuh"
 #include "dem_laws.cuh"
 
 #include <algorithm>
@@ -319,8 +318,9 @@ __device__ __forceinline__ float ens_particle_step_ref(const EnsGeom& g, const E
 // the particle has moved since the last re-sort.  kRecord: also writes what
 // the step reads into the tape view (histories to hrec when it is not null).
 // kMix: the system holds polyhedra (linear law): a polyhedron's own entry is
-// skipped (k_mix_poly_step steps it), a polyhedron neighbour is met by the
-// sphere-hull test and the law of mix_pair_law.
+// skipped (k_mix_poly_step steps it); a polyhedron neighbour's contact force
+// and torque are the ones k_mix_poly_step left for this sphere (MixView),
+// added in slot order.
 template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kNc = true, bool kRot = false,
           bool kMix = false>
 __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBufs& b,
@@ -385,25 +385,15 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     const float4 pb4 = ld_state<kNc>(in.pos + j);
     if constexpr (kMix) {
       if (pb4.w < 0.0f) {
-        const float4 vb4 = ld_state<kNc>(in.vel + j), wb4 = ld_state<kNc>(in.angv + j);
-        const int q = __float_as_int(wb4.w);
-        const int sq = g.mix.shape_of[q];
-        const MixShapeDev& SH = g.mix.shapes[sq];
-        MixHit h;
-        if (!sphere_hull(pa, ra, xyz(pb4), g.mix.gv + (size_t)q * kMixMaxV,
-                         g.mix.gf + (size_t)q * kMixMaxF, g.mix.faces + (size_t)sq * kMixMaxF,
-                         SH.nf, h))
-          continue;
-        float3 xi = f3(0.0f, 0.0f, 0.0f);
-        if ((mask_o >> k) & 1u) xi = f3(L.hx[sk], L.hy[sk], L.hz[sk]);
-        float3 F, Ta, Tb;
-        mix_pair_law(S, h, ma, va, wa, SH.mass, xyz(vb4), xyz(wb4), dt, xi, F, Ta, Tb);
-        L.hx[sk] = xi.x;
-        L.hy[sk] = xi.y;
-        L.hz[sk] = xi.z;
-        mask |= 1u << k;
-        f = f + F;
-        t = t + Ta;
+        const uint32_t tw = g.mix.twin[sk];
+        if (tw == 0xffu) continue;
+        const int q = __float_as_int(ld_state<kNc>(in.angv + j).w);
+        const size_t sq = (size_t)tw * (size_t)g.mix.npoly + (size_t)q;
+        const float4 F4 = g.mix.sf[sq];
+        if (F4.w == 0.0f) continue;
+        const float4 T4 = g.mix.st[sq];
+        f = f + xyz(F4);
+        t = t + xyz(T4);
         continue;
       }
     }

@@ -129,14 +129,16 @@ struct EnsBufs {
 // Convex polyhedra among a system's spheres (mix_device.cuh): what the
 // sphere step reads about them.  A polyhedron's entry in the state carries
 // minus its bounding radius in pos4.w and its polyhedron id in angv4.w (its
-// path since the last re-sort is kept per polyhedron instead).
-struct MixShapeDev;
+// path since the last re-sort is kept per polyhedron instead).  A
+// sphere-polyhedron pair is evaluated once, by the polyhedron step, which
+// leaves the force and torque on the sphere in the polyhedron's slot
+// (sf / st[k * npoly + p], sf.w = 1 for a contact); the sphere step reads
+// them through twin (per sphere slot: the polyhedron's slot that holds the
+// sphere, 0xff none), which a re-sort rebuilds.
 struct MixView {
-  const MixShapeDev* shapes;
-  const int* shape_of;       // per polyhedron id
-  const double4* gv;         // per polyhedron: world-frame vertex offsets (kMixMaxV)
-  const double4* gf;         // per polyhedron: world-frame face planes (kMixMaxF)
-  const uchar4* faces;       // per shape: vertex triples (kMixMaxF)
+  const uint8_t* twin;
+  const float4* sf;
+  const float4* st;
   int npoly;                 // 0: spheres only
 };
 

@@ -90,6 +90,9 @@ struct MixBufs {
   double4* gf;
   float4* wh;
   int* wn;
+  float4* sf;           // per polyhedron slot: force on the sphere there (w = 1: contact)
+  float4* st;           // and its torque
+  uint8_t* twin;        // per sphere slot (sphere list layout): see MixView
   MixList L[2];
   int npoly;
 };

@@ -145,6 +145,36 @@ k_mix_plist(EnsGeom g, EnsBufs b, MixBufs m, const float4* __restrict__ pos,
   if (st) atomicOr(&ctl->status, st);
 }
 
+// The twin of every sphere slot that holds a polyhedron: the polyhedron's
+// slot that holds the sphere (new lists, before the epoch turns).
+__global__ void __launch_bounds__(kThreads)
+k_mix_twins(EnsBufs b, MixBufs m, const float4* __restrict__ pos,
+            const float4* __restrict__ angv, int n, StepCtl* ctl, const int* gate) {
+  if (gate && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (pos[i].w < 0.0f) return;
+  const int e = ctl->epoch & 1;
+  const EnsList Ln = b.L[e ^ 1];
+  const MixList Pn = m.L[e ^ 1];
+  const size_t stride = (size_t)b.stride, P = (size_t)m.npoly;
+  const uint32_t cnt = Ln.cnt[i];
+  uint32_t st = 0;
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const size_t sk = (size_t)k * stride + i;
+    const uint32_t j = Ln.idx[sk];
+    if (!(pos[j].w < 0.0f)) continue;
+    const int q = __float_as_int(angv[j].w);
+    const uint32_t c = Pn.cnt[q];
+    uint32_t tw = 0xffu;
+    for (uint32_t kk = 0; kk < c; ++kk)
+      if (Pn.idx[(size_t)kk * P + q] == (uint32_t)i) { tw = kk; break; }
+    if (tw == 0xffu) st |= kStatusListOverflow;
+    m.twin[sk] = (uint8_t)tw;
+  }
+  if (st) atomicOr(&ctl->status, st);
+}
+
 // -------------------------------------------------------------- the step
 // (value, index) maximum over the warp, the lowest index on ties: the
 // serial loop's first maximum.
@@ -279,10 +309,13 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
       if (pb4.w < 0.0f) {
         is_poly = true;
       } else {
+        // the pair is evaluated here only: the sphere's step reads the force
+        // and torque on it from sf / st
         const float3 rel = xyz(pb4) - xa;
         const float sr = pb4.w + rb;
         const float d2 = dot3(rel, rel);
         MixHit h;
+        float4 sfo = make_float4(0.0f, 0.0f, 0.0f, 0.0f), sto = sfo;
         if (d2 < sr * sr && sqrtf(d2) > 0.0f &&
             sphere_hull(xyz(pb4), pb4.w, xa, A.V, A.F, faces, A.nf, h)) {
           const float4 vb4 = in.vel[j], wb4 = in.angv[j];
@@ -296,8 +329,12 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
           L.hz[sk] = xi.z;
           sm.f[k] = make_float4(-F.x, -F.y, -F.z, 0.0f);
           sm.t[k] = make_float4(Tp.x, Tp.y, Tp.z, 0.0f);
+          sfo = make_float4(F.x, F.y, F.z, 1.0f);
+          sto = make_float4(Ts.x, Ts.y, Ts.z, 0.0f);
           touched = true;
         }
+        m.sf[sk] = sfo;
+        m.st[sk] = sto;
       }
     }
     touch[half] = __ballot_sync(0xffffffffu, touched);
@@ -573,6 +610,12 @@ void mix_launch_plist(const EnsGeom& g, const EnsBufs& b, const MixBufs& m,
   if (m.npoly <= 0) return;
   k_mix_plist<<<nblk(m.npoly), kThreads, 0, st>>>(g, b, m, b.S[2].pos, b.S[2].vel, cstart, cend,
                                                   ctl, gate);
+}
+
+void mix_launch_twins(const EnsBufs& b, const MixBufs& m, int n, StepCtl* ctl, const int* gate,
+                      cudaStream_t st) {
+  if (m.npoly <= 0) return;
+  k_mix_twins<<<nblk(n), kThreads, 0, st>>>(b, m, b.S[2].pos, b.S[2].angv, n, ctl, gate);
 }
 
 void mix_launch_poly_step(const EnsGeom& g, const EnsBufs& b, const MixBufs& m, int cur,
