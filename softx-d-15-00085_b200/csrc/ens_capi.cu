@@ -102,6 +102,16 @@ struct blaze_ens {
   float4* d_psf = nullptr;
   float4* d_pst = nullptr;
   uint8_t* d_twin = nullptr;
+  // a finer triangle grid for the spheres of systems with polyhedra (their
+  // hash cells are sized for the polyhedra's bounding radii): per system
+  // cell, cells and global offset; the CSR lists on it
+  std::vector<float> h_rad;               // the radii of the last set_state
+  std::vector<float> scell;
+  std::vector<int3> snc;
+  std::vector<uint32_t> scell_off;
+  bool sgrid = false;
+  uint32_t* d_stri_off = nullptr;
+  uint32_t* d_stri_ids = nullptr;
   MixList ml[2] = {};
   // blaze_ens_set_profile: plain steps timed by phase
   bool prof = false;
@@ -118,6 +128,8 @@ EnsGeom geom(const blaze_ens* e) {
   g.walls = e->d_walls;
   g.tri_off = e->d_tri_off;
   g.tri_ids = e->d_tri_ids;
+  g.stri_off = e->sgrid ? e->d_stri_off : e->d_tri_off;
+  g.stri_ids = e->sgrid ? e->d_stri_ids : e->d_tri_ids;
   g.ncell_tab = e->ncell_tab;
   g.law = e->opt.law;
   g.dt = e->opt.dt;
@@ -212,6 +224,9 @@ EnsSysDev system_constants(const blaze_system& s, uint32_t cell_off, float dt) {
     d.rot_cd = std::cos(ang);
     d.rot_sd = std::sin(ang);
   }
+  d.scell = d.cell;   // the spheres' triangle grid: the hash grid unless blaze_ens::sgrid
+  d.snc = d.nc;
+  d.scell_off = d.cell_off;
   return d;
 }
 
@@ -252,14 +267,26 @@ EnsWallDev wall_dev(const blaze_wall& w) {
 // Candidate triangles per global cell: every cell whose box meets the
 // triangle's bounding box grown by half a cell (more than the largest radius
 // a system allows), so a sphere centred in the cell touches no triangle left
-// out.  Lists are in ascending triangle order.
-void build_tri_lists(const blaze_ens* e, std::vector<uint32_t>& off, std::vector<uint32_t>& ids) {
-  off.assign((size_t)e->ncell_tab + 1, 0);
+// out.  Lists are in ascending triangle order.  spheres_grid: on the spheres'
+// finer grid of a system with polyhedra (blaze_ens::scell, half a cell is
+// more than any sphere's radius there).
+void build_tri_lists(const blaze_ens* e, std::vector<uint32_t>& off, std::vector<uint32_t>& ids,
+                     bool spheres_grid = false) {
+  uint32_t ntab = e->ncell_tab;
+  if (spheres_grid) {
+    ntab = 0;
+    for (int s = 0; s < e->nsys; ++s)
+      ntab += (uint32_t)e->snc[s].x * (uint32_t)e->snc[s].y * (uint32_t)e->snc[s].z;
+  }
+  off.assign((size_t)ntab + 1, 0);
   std::vector<std::pair<uint32_t, uint32_t>> pairs;  // (cell, triangle)
   for (int s = 0; s < e->nsys; ++s) {
     const blaze_system& S = e->sys[s];
     const EnsSysDev& D = e->hsys[s];
-    const double margin = 0.5 * (double)S.cell + 1e-4 * (double)S.cell;
+    const float cell = spheres_grid ? e->scell[s] : S.cell;
+    const int3 nc = spheres_grid ? e->snc[s] : D.nc;
+    const uint32_t coff = spheres_grid ? e->scell_off[s] : D.cell_off;
+    const double margin = 0.5 * (double)cell + 1e-4 * (double)cell;
     for (int t = S.tri0; t < S.tri0 + S.ntris; ++t) {
       const EnsWallDev& W = e->hwalls[t];
       const float3 v[3] = {W.a, W.b, W.c};
@@ -272,14 +299,14 @@ void build_tri_lists(const blaze_ens* e, std::vector<uint32_t>& off, std::vector
           mx = std::max(mx, x);
         }
         const double o = c == 0 ? D.origin.x : (c == 1 ? D.origin.y : D.origin.z);
-        const int ncs = c == 0 ? D.nc.x : (c == 1 ? D.nc.y : D.nc.z);
-        lo[c] = std::max(0, (int)std::floor((mn - margin - o) / (double)S.cell));
-        hi[c] = std::min(ncs - 1, (int)std::floor((mx + margin - o) / (double)S.cell));
+        const int ncs = c == 0 ? nc.x : (c == 1 ? nc.y : nc.z);
+        lo[c] = std::max(0, (int)std::floor((mn - margin - o) / (double)cell));
+        hi[c] = std::min(ncs - 1, (int)std::floor((mx + margin - o) / (double)cell));
       }
       for (int z = lo[2]; z <= hi[2]; ++z)
         for (int y = lo[1]; y <= hi[1]; ++y)
           for (int x = lo[0]; x <= hi[0]; ++x)
-            pairs.push_back({D.cell_off + (uint32_t)(x + D.nc.x * (y + D.nc.y * z)), (uint32_t)t});
+            pairs.push_back({coff + (uint32_t)(x + nc.x * (y + nc.y * z)), (uint32_t)t});
     }
   }
   std::stable_sort(pairs.begin(), pairs.end(),
@@ -291,7 +318,7 @@ void build_tri_lists(const blaze_ens* e, std::vector<uint32_t>& off, std::vector
     off[pairs[k].first + 1]++;
     ids[k] = pairs[k].second;
   }
-  for (size_t c = 0; c < e->ncell_tab; ++c) off[c + 1] += off[c];
+  for (size_t c = 0; c < ntab; ++c) off[c + 1] += off[c];
 }
 
 void drop_graphs(blaze_ens* e) {
@@ -321,9 +348,10 @@ void free_ens(blaze_ens* e) {
   f(e->d_shapes); f(e->d_bv); f(e->d_bn); f(e->d_faces); f(e->d_edges); f(e->d_shape_of);
   f(e->d_pidx); f(e->d_quat); f(e->d_quat0); f(e->d_pat); f(e->d_ppath); f(e->d_gv); f(e->d_gf);
   f(e->d_pwh); f(e->d_pwn); f(e->d_psf); f(e->d_pst); f(e->d_twin);
+  f(e->d_stri_off); f(e->d_stri_ids);
   for (int k = 0; k < 2; ++k) {
     f(e->ml[k].idx); f(e->ml[k].cnt); f(e->ml[k].mlo); f(e->ml[k].mhi);
-    f(e->ml[k].hx); f(e->ml[k].hy); f(e->ml[k].hz);
+    f(e->ml[k].hx); f(e->ml[k].hy); f(e->ml[k].hz); f(e->ml[k].sep);
   }
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   for (int k = 0; k < 5; ++k)
@@ -357,6 +385,11 @@ int upload_params(blaze_ens* e) {
     e->hsys[s] = system_constants(e->sys[s], off, e->opt.dt);
     off += (uint32_t)e->sys[s].ncells[0] * (uint32_t)e->sys[s].ncells[1] *
            (uint32_t)e->sys[s].ncells[2];
+    if (e->sgrid) {
+      e->hsys[s].scell = e->scell[s];
+      e->hsys[s].snc = e->snc[s];
+      e->hsys[s].scell_off = e->scell_off[s];
+    }
   }
   CK(cudaMemcpyAsync(e->d_sys, e->hsys.data(), sizeof(EnsSysDev) * e->nsys,
                      cudaMemcpyHostToDevice, e->stream));
@@ -811,6 +844,7 @@ int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, co
   }
   int rc = sync_status(e);
   if (rc < 0) return rc;
+  e->h_rad.assign(radius, radius + n);
   CK(cudaMemsetAsync(e->d_flags, 0, 2 * sizeof(int), e->stream));
   CK(cudaMemcpyAsync(e->st_pos3, pos3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemcpyAsync(e->st_rad, radius, sizeof(float) * n, cudaMemcpyHostToDevice, e->stream));
@@ -847,6 +881,11 @@ int blaze_ens_set_state(blaze_ens* e, const float* pos3, const float* radius, co
     e->b.pat = nullptr;
     e->b.ppath = nullptr;
     drop_graphs(e);
+  }
+  if (e->sgrid) {       // the spheres' triangles on the hash grid again
+    e->sgrid = false;
+    int rp = upload_params(e);
+    if (rp) return rp;
   }
   return 0;
 }
@@ -1239,12 +1278,61 @@ int blaze_ens_set_polyhedra(blaze_ens* e, const blaze_shape* shapes, int nshapes
       if ((rc = realloc_dev(&L.idx, (size_t)np * kMixSlots)) || (rc = realloc_dev(&L.cnt, (size_t)np)) ||
           (rc = realloc_dev(&L.mlo, (size_t)np)) || (rc = realloc_dev(&L.mhi, (size_t)np)) ||
           (rc = realloc_dev(&L.hx, (size_t)np * kMixSlots)) || (rc = realloc_dev(&L.hy, (size_t)np * kMixSlots)) ||
-          (rc = realloc_dev(&L.hz, (size_t)np * kMixSlots)))
+          (rc = realloc_dev(&L.hz, (size_t)np * kMixSlots)) ||
+          (rc = realloc_dev(&L.sep, (size_t)np * kMixSlots)))
         return rc;
     }
     e->poly_cap = np;
   }
   if (!e->d_twin && (rc = realloc_dev(&e->d_twin, (size_t)e->b.cap * e->n))) return rc;
+  // the spheres' triangles on a grid of cells of 2 r_max(spheres) + skin
+  // where that is finer than the hash grid (sized for the polyhedra)
+  {
+    bool any = false;
+    e->scell.assign(e->nsys, 0.0f);
+    e->snc.assign(e->nsys, make_int3(0, 0, 0));
+    e->scell_off.assign(e->nsys, 0u);
+    uint32_t off = 0;
+    int i0 = 0;
+    for (int sy = 0; sy < e->nsys; ++sy) {
+      const blaze_system& S = e->sys[sy];
+      float rmax = 0.0f;
+      bool has_poly = false;
+      for (int k = 0; k < S.n; ++k) {
+        if (shape_of[i0 + k] >= 0) has_poly = true;
+        else rmax = std::max(rmax, e->h_rad[i0 + k]);
+      }
+      i0 += S.n;
+      const float fine = (2.0f * rmax + e->opt.skin) * (1.0f + 1e-6f);
+      if (has_poly && S.ntris > 0 && rmax > 0.0f && fine < 0.8f * S.cell) {
+        e->scell[sy] = fine;
+        for (int c = 0; c < 3; ++c) {
+          const int m = (int)std::ceil((double)S.ncells[c] * (double)S.cell / (double)fine);
+          (c == 0 ? e->snc[sy].x : (c == 1 ? e->snc[sy].y : e->snc[sy].z)) = m;
+        }
+        any = true;
+      } else {
+        e->scell[sy] = S.cell;
+        e->snc[sy] = make_int3(S.ncells[0], S.ncells[1], S.ncells[2]);
+      }
+      e->scell_off[sy] = off;
+      off += (uint32_t)e->snc[sy].x * (uint32_t)e->snc[sy].y * (uint32_t)e->snc[sy].z;
+    }
+    if (any) {
+      std::vector<uint32_t> off_v, ids;
+      build_tri_lists(e, off_v, ids, true);
+      if ((rc = realloc_dev(&e->d_stri_off, off_v.size())) ||
+          (rc = realloc_dev(&e->d_stri_ids, std::max<size_t>(ids.size(), 1))))
+        return rc;
+      CK(cudaMemcpy(e->d_stri_off, off_v.data(), sizeof(uint32_t) * off_v.size(),
+                    cudaMemcpyHostToDevice));
+      if (!ids.empty())
+        CK(cudaMemcpy(e->d_stri_ids, ids.data(), sizeof(uint32_t) * ids.size(),
+                      cudaMemcpyHostToDevice));
+    }
+    e->sgrid = any;
+    if ((rc = upload_params(e))) return rc;
+  }
   {
     std::vector<MixShapeDev> sd(nshapes);
     std::vector<float4> bv((size_t)nshapes * kMixMaxV, make_float4(0, 0, 0, 0));

@@ -26,6 +26,20 @@ __device__ __forceinline__ bool ens_in(const EnsSysDev& S, int3 c) {
 __device__ __forceinline__ uint32_t ens_key(const EnsSysDev& S, int3 c) {
   return S.cell_off + (uint32_t)(c.x + S.nc.x * (c.y + S.nc.y * c.z));
 }
+// the spheres' grid of triangle candidates
+__device__ __forceinline__ int3 ens_scell(const EnsSysDev& S, float3 p) {
+  int3 c;
+  c.x = (int)floorf((p.x - S.origin.x) / S.scell);
+  c.y = (int)floorf((p.y - S.origin.y) / S.scell);
+  c.z = (int)floorf((p.z - S.origin.z) / S.scell);
+  return c;
+}
+__device__ __forceinline__ bool ens_sin(const EnsSysDev& S, int3 c) {
+  return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < S.snc.x && c.y < S.snc.y && c.z < S.snc.z;
+}
+__device__ __forceinline__ uint32_t ens_skey(const EnsSysDev& S, int3 c) {
+  return S.scell_off + (uint32_t)(c.x + S.snc.x * (c.y + S.snc.y * c.z));
+}
 // v turned by the angle with cosine c and sine s about the unit axis a
 // (Rodrigues): v c + (a x v) s + a (a . v) (1 - c)
 __device__ __forceinline__ float3 rot_about(float3 a, float c, float s, float3 v) {

@@ -514,16 +514,16 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
   }
   if (kCurved && g.tri_off) {
     const float3 pd = rot ? S.rot_o + rot_about(S.rot_a, rc, -rsn, pa - S.rot_o) : pa;
-    const int3 c = ens_cell(S, pd);
-    if (ens_in(S, c)) {
-      const uint32_t h = ens_key(S, c);
-      const uint32_t o0 = __ldg(g.tri_off + h), o1 = __ldg(g.tri_off + h + 1);
+    const int3 c = ens_scell(S, pd);
+    if (ens_sin(S, c)) {
+      const uint32_t h = ens_skey(S, c);
+      const uint32_t o0 = __ldg(g.stri_off + h), o1 = __ldg(g.stri_off + h + 1);
       // face contacts all count; without one, only the deepest edge/vertex
       // contact does (a sphere over a shared edge or vertex touches it once)
       int nface = 0, best = -1;
       float best_d = 0.0f;
       for (uint32_t q = o0; q < o1; ++q) {
-        const int id = (int)__ldg(g.tri_ids + q);
+        const int id = (int)__ldg(g.stri_ids + q);
         float3 nrm;
         float delta;
         int region;
@@ -532,7 +532,7 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
         else if (best < 0 || delta > best_d) { best = id; best_d = delta; }
       }
       for (uint32_t q = o0; q < o1; ++q) {
-        const int id = (int)__ldg(g.tri_ids + q);
+        const int id = (int)__ldg(g.stri_ids + q);
         float3 nrm;
         float delta;
         int region;

@@ -59,6 +59,12 @@ struct EnsSysDev {
   float3 rot_o, rot_a;
   float rot_w, rot_cd, rot_sd;
   int rot;
+  // the spheres' grid of triangle candidates (EnsGeom::stri_off): the hash
+  // grid, or, in a system with polyhedra, a finer one of cells of
+  // 2 r_max(spheres) + skin over the same origin and extent
+  float scell;
+  int3 snc;
+  uint32_t scell_off;
 };
 
 struct EnsWallDev {
@@ -147,6 +153,8 @@ struct EnsGeom {
   const EnsWallDev* walls;
   const uint32_t* tri_off;   // per global cell: candidate triangles (CSR), or null
   const uint32_t* tri_ids;
+  const uint32_t* stri_off;  // the same on the spheres' grid (EnsSysDev::scell)
+  const uint32_t* stri_ids;
   uint32_t ncell_tab;        // total hash-table entries
   int law;
   float dt, skin;

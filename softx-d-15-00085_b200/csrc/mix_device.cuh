@@ -56,7 +56,11 @@ struct MixShapeDev {
 
 // One copy of the polyhedra's neighbour lists, slot-major over polyhedron
 // ids (slot k of polyhedron p at k * npoly + p); a 64-bit mask of active
-// tangential histories per polyhedron (mlo: slots 0-31, mhi: 32-63).
+// tangential histories per polyhedron (mlo: slots 0-31, mhi: 32-63).  A pair
+// of polyhedra that an axis separated stays apart along it for a while:
+// that axis is tried first the next step (same answer as the full test when
+// it still separates them, since the full test takes the largest
+// separation).
 struct MixList {
   uint32_t* idx;
   uint32_t* cnt;
@@ -65,6 +69,9 @@ struct MixList {
   float* hx;
   float* hy;
   float* hz;
+  int* sep;     // per slot: the axis that last separated a polyhedron pair
+                // (kind << 16 | index: 0 a face of A, 1 a face of B, 2 an edge
+                // pair; A the lower id), -1 none
 };
 
 // Everything about the polyhedra.  Per shape: bv (kMixMaxV body vertices),
@@ -367,73 +374,15 @@ __device__ __forceinline__ bool hull_hull_finish(const SatPick& q, double3 d, co
 __device__ __forceinline__ int tri_e0(int t) { return t == 2 ? 1 : 0; }
 __device__ __forceinline__ int tri_e1(int t) { return t == 0 ? 1 : 2; }
 
-// The triangle T (vertices relative to the polyhedron's centre, unit normal
-// nt) as a flat hull against the polyhedron (V, F, E; its faces' normals
-// outward).  a = the polyhedron: n from the triangle to it, ca relative to
-// its centre.  Returns the kind of axis through `kind` (0 a face of the
-// polyhedron, 1 a face of the triangle, 2 an edge pair) and the unrounded
-// normal through `nd`, for the merging of coplanar contacts.
-__device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, const uchar4* E,
-                                         int nv, int nf, int ne, const double3* T, double3 nt,
-                                         MixHit& h, double3& nd) {
-  // faces of the polyhedron
-  double sP = -1e300;
-  int fP = 0;
-  for (int f = 0; f < nf; ++f) {
-    const double4 P = F[f];
-    double m = 1e300;
-    for (int k = 0; k < 3; ++k) {
-      const double t = (P.x * T[k].x + P.y * T[k].y) + P.z * T[k].z;
-      if (t < m) m = t;
-    }
-    const double s = m - P.w;
-    if (s > sP) { sP = s; fP = f; }
-  }
-  if (sP > 0.0) return false;
-  // the triangle's two faces
-  double lo = 1e300, hi = -1e300;
-  for (int k = 0; k < nv; ++k) {
-    const double t = ddot(nt, dxyz(V[k]));
-    if (t < lo) lo = t;
-    if (t > hi) hi = t;
-  }
-  const double h0 = ddot(nt, T[0]);
-  const double sTp = lo - h0, sTm = h0 - hi;
-  const bool tplus = sTp >= sTm;
-  const double sT = tplus ? sTp : sTm;
-  if (sT > 0.0) return false;
-  // edge pairs, full support extents along each axis
-  double sE = -1e300;
-  int eE = -1;
-  bool eplus = true;
-  for (int e = 0; e < ne; ++e) {
-    const uchar4 ed = E[e];
-    const double3 P0 = dxyz(V[ed.x]), ep = dsub(dxyz(V[ed.y]), P0);
-    for (int t = 0; t < 3; ++t) {
-      const double3 et = dsub(T[tri_e1(t)], T[tri_e0(t)]);
-      double3 ax = dcross(ep, et);
-      const double l2 = ddot(ax, ax);
-      if (!(l2 > 1e-10 * (ddot(ep, ep) * ddot(et, et)))) continue;
-      const double l = sqrt(l2);
-      ax = dv(ax.x / l, ax.y / l, ax.z / l);
-      double pmin = 1e300, pmax = -1e300;
-      for (int k = 0; k < nv; ++k) {
-        const double u = ddot(ax, dxyz(V[k]));
-        if (u < pmin) pmin = u;
-        if (u > pmax) pmax = u;
-      }
-      double tmin = 1e300, tmax = -1e300;
-      for (int k = 0; k < 3; ++k) {
-        const double u = ddot(ax, T[k]);
-        if (u < tmin) tmin = u;
-        if (u > tmax) tmax = u;
-      }
-      const double s1 = tmin - pmax, s2 = pmin - tmax;
-      const double s = s1 >= s2 ? s1 : s2;
-      if (s > 0.0) return false;
-      if (s > sE) { sE = s; eE = 3 * e + t; eplus = s1 >= s2; }
-    }
-  }
+// The contact of hull_tri from its queries' results: the triangle's face
+// (sT, tplus: +nt or -nt), the polyhedron's face (sP, fP), the edge pair
+// (sE, eE = 3 edge + triangle edge, or -1; eplus: the triangle on the + side
+// of the pair's axis).
+__device__ __forceinline__ bool hull_tri_finish(const double4* V, const double4* F,
+                                                const uchar4* E, int nv, const double3* T,
+                                                double3 nt, double sT, bool tplus, double sP,
+                                                int fP, double sE, int eE, bool eplus, MixHit& h,
+                                                double3& nd) {
   SatPick q;
   q.sA = sT;   // the wall's face plays the reference face
   q.sB = sP;
@@ -483,6 +432,95 @@ __device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, con
   h.ca = to_f3(cp);
   h.cb = h.ca;
   return true;
+}
+
+// Separation of the triangle T from the polyhedron's face plane P.
+__device__ __forceinline__ double tri_face_sep(double4 P, const double3* T) {
+  double m = 1e300;
+  for (int k = 0; k < 3; ++k) {
+    const double t = (P.x * T[k].x + P.y * T[k].y) + P.z * T[k].z;
+    if (t < m) m = t;
+  }
+  return m - P.w;
+}
+
+// Separation along the triangle's normal nt or -nt (the larger; tplus: +nt)
+// from the polyhedron's extent [lo, hi] along nt.
+__device__ __forceinline__ double tri_plane_sep(double3 nt, const double3* T, double lo,
+                                                double hi, bool& tplus) {
+  const double h0 = ddot(nt, T[0]);
+  const double sTp = lo - h0, sTm = h0 - hi;
+  tplus = sTp >= sTm;
+  return tplus ? sTp : sTm;
+}
+
+// Edge pair x = 3 e + t (edge e of the polyhedron, edge t of the triangle):
+// the separation along their cross product with full support extents of
+// both (plus: the triangle on the + side), kNoAxis for parallel edges.
+__device__ __forceinline__ double tri_edge_sep(const double4* V, const uchar4* E, int nv,
+                                               const double3* T, int x, bool& plus) {
+  const int e = x / 3, t = x % 3;
+  const uchar4 ed = E[e];
+  const double3 P0 = dxyz(V[ed.x]), ep = dsub(dxyz(V[ed.y]), P0);
+  const double3 et = dsub(T[tri_e1(t)], T[tri_e0(t)]);
+  double3 ax = dcross(ep, et);
+  const double l2 = ddot(ax, ax);
+  if (!(l2 > 1e-10 * (ddot(ep, ep) * ddot(et, et)))) return kNoAxis;
+  const double l = sqrt(l2);
+  ax = dv(ax.x / l, ax.y / l, ax.z / l);
+  double pmin = 1e300, pmax = -1e300;
+  for (int k = 0; k < nv; ++k) {
+    const double u = ddot(ax, dxyz(V[k]));
+    if (u < pmin) pmin = u;
+    if (u > pmax) pmax = u;
+  }
+  double tmin = 1e300, tmax = -1e300;
+  for (int k = 0; k < 3; ++k) {
+    const double u = ddot(ax, T[k]);
+    if (u < tmin) tmin = u;
+    if (u > tmax) tmax = u;
+  }
+  const double s1 = tmin - pmax, s2 = pmin - tmax;
+  plus = s1 >= s2;
+  return plus ? s1 : s2;
+}
+
+// The triangle T (vertices relative to the polyhedron's centre, unit normal
+// nt) as a flat hull against the polyhedron (V, F, E; its faces' normals
+// outward).  a = the polyhedron: n from the triangle to it, ca relative to
+// its centre.  Returns the kind of axis through `kind` (0 a face of the
+// polyhedron, 1 a face of the triangle, 2 an edge pair) and the unrounded
+// normal through `nd`, for the merging of coplanar contacts.
+__device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, const uchar4* E,
+                                         int nv, int nf, int ne, const double3* T, double3 nt,
+                                         MixHit& h, double3& nd) {
+  double sP = -1e300;
+  int fP = 0;
+  for (int f = 0; f < nf; ++f) {
+    const double s = tri_face_sep(F[f], T);
+    if (s > sP) { sP = s; fP = f; }
+  }
+  if (sP > 0.0) return false;
+  double lo = 1e300, hi = -1e300;
+  for (int k = 0; k < nv; ++k) {
+    const double t = ddot(nt, dxyz(V[k]));
+    if (t < lo) lo = t;
+    if (t > hi) hi = t;
+  }
+  bool tplus;
+  const double sT = tri_plane_sep(nt, T, lo, hi, tplus);
+  if (sT > 0.0) return false;
+  double sE = -1e300;
+  int eE = -1;
+  bool eplus = true;
+  for (int x = 0; x < 3 * ne; ++x) {
+    bool pl;
+    const double s = tri_edge_sep(V, E, nv, T, x, pl);
+    if (s == kNoAxis) continue;
+    if (s > 0.0) return false;
+    if (s > sE) { sE = s; eE = x; eplus = pl; }
+  }
+  return hull_tri_finish(V, F, E, nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd);
 }
 
 // ----------------------------------------------------- polyhedron - plane

@@ -111,6 +111,7 @@ k_mix_plist(EnsGeom g, EnsBufs b, MixBufs m, const float4* __restrict__ pos,
             if (!(dot3(rel, rel) < lim * lim)) continue;
             if (cnt < (uint32_t)kMixSlots) {
               Ln.idx[(size_t)cnt * P + p] = j;
+              Ln.sep[(size_t)cnt * P + p] = -1;
               unsigned long long mo = mask_o;
               if (mo) {
                 const int pj = pid_new[j];
@@ -197,10 +198,28 @@ struct HullRef {
   int nv, nf, ne;
 };
 
+// The edge pair x = ea * B.ne + eb of hulls A and B (B's centre at d).
+__device__ __forceinline__ double pair_edge_sep(double3 d, const HullRef& A, const HullRef& B,
+                                                int x) {
+  const uchar4 ea = A.E[x / B.ne], eb = B.E[x % B.ne];
+  return edge_sep(dxyz(A.F[ea.z]), dxyz(A.F[ea.w]), dxyz(B.F[eb.z]), dxyz(B.F[eb.w]),
+                  dxyz(A.V[ea.x]), dxyz(A.V[ea.y]), dadd(d, dxyz(B.V[eb.x])),
+                  dadd(d, dxyz(B.V[eb.y])));
+}
+
+// Whether the axis `code` (MixList::sep) separates hulls A and B.
+__device__ __forceinline__ bool axis_separates(int code, double3 d, const HullRef& A,
+                                               const HullRef& B) {
+  const int kind = code >> 16, x = code & 0xffff;
+  if (kind == 0) return face_sep(A.F[x], d, B.V, B.nv) > 0.0;
+  if (kind == 1) return face_sep(B.F[x], dneg(d), A.V, A.nv) > 0.0;
+  return pair_edge_sep(d, A, B, x) > 0.0;
+}
+
 // The separating-axis queries of hulls A and B (B's centre at d from A's),
-// shared by the warp: false when an axis separates them.
+// shared by the warp: false when an axis separates them (its code in sep).
 __device__ bool hull_hull_warp(int lane, double3 d, const HullRef& A, const HullRef& B,
-                               SatPick& q) {
+                               SatPick& q, int& sep) {
   double s = -1e300;
   int k = INT_MAX;
   for (int f = lane; f < A.nf; f += 32) {
@@ -208,7 +227,10 @@ __device__ bool hull_hull_warp(int lane, double3 d, const HullRef& A, const Hull
     if (t > s) { s = t; k = f; }
   }
   warp_argmax(s, k);
-  if (s > 0.0) return false;
+  if (s > 0.0) {
+    sep = k;
+    return false;
+  }
   q.sA = s;
   q.fA = k;
   const double3 md = dneg(d);
@@ -219,24 +241,85 @@ __device__ bool hull_hull_warp(int lane, double3 d, const HullRef& A, const Hull
     if (t > s) { s = t; k = f; }
   }
   warp_argmax(s, k);
-  if (s > 0.0) return false;
+  if (s > 0.0) {
+    sep = (1 << 16) | k;
+    return false;
+  }
   q.sB = s;
   q.fB = k;
   s = kNoAxis;
   k = INT_MAX;
   const int tot = A.ne * B.ne;
   for (int x = lane; x < tot; x += 32) {
-    const uchar4 ea = A.E[x / B.ne], eb = B.E[x % B.ne];
-    const double t = edge_sep(dxyz(A.F[ea.z]), dxyz(A.F[ea.w]), dxyz(B.F[eb.z]), dxyz(B.F[eb.w]),
-                              dxyz(A.V[ea.x]), dxyz(A.V[ea.y]), dadd(d, dxyz(B.V[eb.x])),
-                              dadd(d, dxyz(B.V[eb.y])));
+    const double t = pair_edge_sep(d, A, B, x);
     if (t > s) { s = t; k = x; }
   }
   warp_argmax(s, k);
-  if (s > 0.0) return false;
+  if (s > 0.0) {
+    sep = (2 << 16) | k;
+    return false;
+  }
   q.sE = s;
   q.eE = k;
   return true;
+}
+
+// warp minimum / maximum of a double (exact: no rounding)
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// hull_tri with its queries shared by the warp: the polyhedron's faces, its
+// extent along the triangle's normal and the 3 ne edge-pair axes split over
+// the lanes; the maxima taken with the lowest index on ties, which is the
+// serial loop's answer; the contact from the same hull_tri_finish.
+__device__ bool hull_tri_warp(int lane, const HullRef& D, const double3* T, double3 nt, MixHit& h,
+                              double3& nd) {
+  double sP = -1e300;
+  int fP = INT_MAX;
+  for (int f = lane; f < D.nf; f += 32) {
+    const double s = tri_face_sep(D.F[f], T);
+    if (s > sP) { sP = s; fP = f; }
+  }
+  warp_argmax(sP, fP);
+  if (sP > 0.0) return false;
+  double lo = 1e300, hi = -1e300;
+  for (int k = lane; k < D.nv; k += 32) {
+    const double t = ddot(nt, dxyz(D.V[k]));
+    lo = fmin(lo, t);
+    hi = fmax(hi, t);
+  }
+  lo = warp_min(lo);
+  hi = warp_max(hi);
+  bool tplus;
+  const double sT = tri_plane_sep(nt, T, lo, hi, tplus);
+  if (sT > 0.0) return false;
+  double sE = -1e300;
+  int eE = INT_MAX;
+  bool sep = false;
+  for (int x = lane; x < 3 * D.ne; x += 32) {
+    bool pl;
+    const double s = tri_edge_sep(D.V, D.E, D.nv, T, x, pl);
+    if (s == kNoAxis) continue;
+    if (s > 0.0) sep = true;
+    if (s > sE) { sE = s; eE = x; }
+  }
+  if (__any_sync(0xffffffffu, sep)) return false;
+  warp_argmax(sE, eE);
+  bool eplus = true;
+  if (eE == INT_MAX) {
+    eE = -1;
+  } else {
+    tri_edge_sep(D.V, D.E, D.nv, T, eE, eplus);
+  }
+  return hull_tri_finish(D.V, D.F, D.E, D.nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd);
 }
 
 struct MixSmem {
@@ -370,8 +453,14 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
       const HullRef& HA = selfA ? A : Bq;
       const HullRef& HB = selfA ? Bq : A;
       const double3 d = dsub(d3(xB), d3(xA));
+      const int code = L.sep[sk];
+      if (code >= 0 && axis_separates(code, d, HA, HB)) continue;
       SatPick pick;
-      if (!hull_hull_warp(lane, d, HA, HB, pick)) continue;
+      int scode;
+      if (!hull_hull_warp(lane, d, HA, HB, pick, scode)) {
+        if (lane == 0 && scode != code) L.sep[sk] = scode;
+        continue;
+      }
       MixHit h;
       if (!hull_hull_finish(pick, d, HA.V, HA.F, HA.E, HA.nv, HB.V, HB.F, HB.E, HB.nv, HB.ne, h))
         continue;
@@ -429,12 +518,12 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
           D.V = sm.v;
           D.F = sm.fn;
         }
+        // candidates near the polyhedron (a lane each), then the test of
+        // each, in ascending order, by the whole warp
         const float lim = rb * 1.001f + 1e-3f;
         for (uint32_t q0 = o0; q0 < o1; q0 += 32) {
           const uint32_t qq = q0 + (uint32_t)lane;
-          bool hit = false;
-          MixHit h;
-          double3 nd;
+          bool near = false;
           int id = -1;
           if (qq < o1) {
             id = (int)__ldg(g.tri_ids + qq);
@@ -442,25 +531,29 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
             int region, feat;
             const float3 cp = closest_on_triangle(pd, W.a, W.b, W.c, region, feat);
             const float3 dd = pd - cp;
-            if (dot3(dd, dd) < lim * lim) {
-              const double3 o = d3(pd);
-              double3 T[3];
-              T[0] = dsub(d3(W.a), o);
-              T[1] = dsub(d3(W.b), o);
-              T[2] = dsub(d3(W.c), o);
-              hit = hull_tri(D.V, D.F, D.E, D.nv, D.nf, D.ne, T, W.n64, h, nd);
-            }
+            near = dot3(dd, dd) < lim * lim;
           }
-          const uint32_t hb = __ballot_sync(0xffffffffu, hit);
-          if (hit) {
-            const int slot = nhit + __popc(hb & ((1u << lane) - 1u));
-            if (slot < kMixHits) {
-              sm.hit[slot] = h;
-              sm.nd[slot] = nd;
-              sm.hid[slot] = id;
+          uint32_t nb = __ballot_sync(0xffffffffu, near);
+          while (nb) {
+            const int src = __ffs(nb) - 1;
+            nb &= nb - 1u;
+            const int tid = __shfl_sync(0xffffffffu, id, src);
+            const EnsWallDev& W = g.walls[tid];
+            const double3 o = d3(pd);
+            double3 T[3];
+            T[0] = dsub(d3(W.a), o);
+            T[1] = dsub(d3(W.b), o);
+            T[2] = dsub(d3(W.c), o);
+            MixHit h;
+            double3 nd;
+            if (!hull_tri_warp(lane, D, T, W.n64, h, nd)) continue;
+            if (lane == 0 && nhit < kMixHits) {
+              sm.hit[nhit] = h;
+              sm.nd[nhit] = nd;
+              sm.hid[nhit] = tid;
             }
+            ++nhit;
           }
-          nhit += __popc(hb);
         }
         if (nhit > kMixHits) {
           st |= kStatusListOverflow;
