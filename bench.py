@@ -626,7 +626,7 @@ def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
 
 
 def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, settle=60000,
-                   skin=0.04):
+                   skin=0.04, block=256):
     """The ball mill's mixed charge (ensemble path; the reference runs
     spheres or polyhedra, never both): the turning drum of mill_mesh_leg with
     n_spheres steel balls r ~ U[0.3, 0.6] cm and n_rocks rocks (convex hulls
@@ -643,7 +643,7 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
     S, W, p, r, sh, so, q = synth.mill_mixed_ensemble(n_spheres=n_spheres, n_rocks=n_rocks,
                                                       skin=skin)
     n = len(p)
-    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=skin, use_graph=1)
+    ens = E.Ensemble(S, W, law=E.LAW_LINEAR, dt=2e-6, skin=skin, use_graph=1, block=block)
     ens.set_state(p, r)
     ens.set_polyhedra(sh, so, q)
     ens.step(settle + max(3, warmup))
@@ -676,7 +676,8 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
             "particles": n, "spheres": n_spheres, "polyhedra": n_rocks,
             "triangles": int(S[0].ntris), "value": n / (ms * 1e-3), "unit": UNIT,
             "ms_per_step": ms, "steps": steps, "settle_steps": settle, "skin_cm": skin,
-            "cell_cm": float(S[0].cell), "rebuilds": rebuilds, "gpu_launches": launches,
+            "cell_cm": float(S[0].cell), "block": block, "rebuilds": rebuilds,
+            "gpu_launches": launches,
             "status": st["status"],
             "plain_step_ms_by_phase": {k: float(v) / max(nph, 1) for k, v in
                                        zip(("resort", "polyhedron_geometry", "polyhedron_step",

@@ -345,7 +345,7 @@ __device__ __forceinline__ float3 mat_tvec_f(const float* R, float3 v) {
 // in slot order, then the walls (planes in order, then the kept triangles
 // in ascending id), as the restatement sums.
 template <bool kCapture, bool kRot>
-__global__ void __launch_bounds__(32 * kMixWarps)
+__global__ void __launch_bounds__(32 * kMixWarps, 4)
 k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_sorted,
                 StateBuf out, StepCtl* ctl, StepLink link, EnsCapture cap) {
   __shared__ MixSmem smem[kMixWarps];
