@@ -153,3 +153,46 @@ def test_mixed_forces_against_fp64(name):
                                       ef[~rocks].max(), ef[rocks].max(), et.max()))
     assert (touching & rocks).sum() >= len(sh) // 2
     assert ef.max() < 1e-5 and et.max() < 1e-5
+
+
+def test_set_polyhedra_rejections():
+    """blaze_ens_set_polyhedra refuses what the mixed step does not cover,
+    with -1 and the ensemble left usable: after a step; a law other than
+    the linear one; a bounding radius that does not fit the cells; an
+    invalid hull."""
+    from blaze import device
+    S, W, p, r, sh, so, q = box_case()
+
+    def fresh(**kw):
+        ens = E.Ensemble(S, W, dt=DT, skin=SKIN, use_graph=0, **kw)
+        ens.set_state(p, r)
+        return ens
+
+    ens = fresh()
+    ens.step(1)
+    with pytest.raises(device.BlazeError):
+        ens.set_polyhedra(sh, so, q)          # not right after set_state
+    ens.set_state(p, r)
+    ens.set_polyhedra(sh, so, q)              # fine again after set_state
+    ens.step(2)
+    assert ens.sync() == 0
+    ens.close()
+    ens = fresh(law=E.LAW_HERTZ_MINDLIN)
+    with pytest.raises(device.BlazeError):
+        ens.set_polyhedra(sh, so, q)
+    ens.close()
+    big = list(sh)
+    v = np.asarray(sh[0].verts).reshape(-1, 3)[:sh[0].nverts] * 3.0   # 3x the size: too big for a cell
+    f = np.asarray(sh[0].faces).reshape(-1, 3)[:sh[0].nfaces]
+    big[0] = E.shape(v, f, sh[0].density)
+    ens = fresh()
+    with pytest.raises(device.BlazeError):
+        ens.set_polyhedra(big, so, q)
+    bad = list(sh)
+    bad[0] = E.shape(v / 3.0, f[:, [0, 2, 1]], sh[0].density)            # inside out
+    with pytest.raises(device.BlazeError):
+        ens.set_polyhedra(bad, so, q)
+    ens.set_polyhedra(sh, so, q)
+    ens.step(2)
+    assert ens.sync() == 0
+    ens.close()
