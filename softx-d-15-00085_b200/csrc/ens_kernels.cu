@@ -566,11 +566,12 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
 
 // kRecord: also write what the step reads into tape slot tp.ctl->slot (the
 // history words are reserved first, by every thread of the block).
-template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot = false,
-          bool kMix = false>
-__global__ void __launch_bounds__(kMaxStepBlock)
-k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
-           StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot, bool kMix>
+__device__ __forceinline__ void ens_step_body(const EnsGeom& g, const EnsBufs& b,
+                                              const StateBuf& in_plain, const StateBuf& in_sorted,
+                                              const StateBuf& out, int n, StepCtl* ctl,
+                                              const StepLink& link, const EnsCapture& cap,
+                                              const EnsTape& tp) {
   const bool rebuilt = *link.rebuilt != 0;
   const StateBuf in = rebuilt ? in_sorted : in_plain;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -607,6 +608,26 @@ k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf
     }
   }
   ens_flag(ctl, st);
+}
+
+template <int kLaw, bool kCapture, bool kRecord, bool kCurved, bool kRot = false,
+          bool kMix = false>
+__global__ void __launch_bounds__(kMaxStepBlock)
+k_ens_step(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
+           StepCtl* ctl, StepLink link, EnsCapture cap, EnsTape tp) {
+  ens_step_body<kLaw, kCapture, kRecord, kCurved, kRot, kMix>(g, b, in_plain, in_sorted, out, n,
+                                                             ctl, link, cap, tp);
+}
+
+// The recording step (reverse mode, linear law, plane walls) held to the
+// plain step's 80 registers: at the 88 it takes by itself a block of 256
+// fits twice per SM instead of three times.
+constexpr int kRecordRegs = 80;
+__global__ void __maxnreg__(kRecordRegs)
+k_ens_step_rec(EnsGeom g, EnsBufs b, StateBuf in_plain, StateBuf in_sorted, StateBuf out, int n,
+               StepCtl* ctl, StepLink link, EnsTape tp) {
+  ens_step_body<kLawLinear, false, true, false, false, false>(
+      g, b, in_plain, in_sorted, out, n, ctl, link, EnsCapture{nullptr, nullptr}, tp);
 }
 
 // ------------------------------------------------------------ drum turn
@@ -873,8 +894,7 @@ void ens_launch_step_record(const EnsGeom& g, const EnsBufs& b, int cur, int n, 
   const int bs = block >= 64 && block <= kMaxStepBlock && block % 32 == 0 ? block : kThreads;
   const int gs = (n + bs - 1) / bs;
   // reverse mode accepts plane walls only (blaze_ens_adj_create)
-  k_ens_step<kLawLinear, false, true, false><<<gs, bs, 0, st>>>(
-      g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, EnsCapture{nullptr, nullptr}, tape);
+  k_ens_step_rec<<<gs, bs, 0, st>>>(g, b, b.S[cur], b.S[2], b.S[cur ^ 1], n, ctl, link, tape);
 }
 
 int ens_persist_grid(const EnsGeom& g, int block, int n) {
