@@ -603,7 +603,7 @@ static void wall_contact(wctx* c, int id, v3 n, real delta, int moving) {
  * working-precision state), laws and integration, stepped one particle at a
  * time.  The polyhedron's own force sums its list slots in slot order, then
  * the planes in order, then the kept triangles in ascending order. */
-enum { MIX_V = 16, MIX_F = 28, MIX_E = 42, MIX_SLOTS = 64, MIX_WSLOTS = 8 };
+enum { MIX_V = 16, MIX_F = 28, MIX_E = 42, MIX_SLOTS = 64, MIX_WSLOTS = 16 };
 
 typedef struct {
   int nv, nf, ne;
@@ -1331,7 +1331,7 @@ static int mix_sphere_contact(const ens_oracle* o, const sysc* S, const part* a,
   return 1;
 }
 
-enum { MIX_HITS = 16 };
+enum { MIX_HITS = 32 };
 
 /* One polyhedron's step (k_mix_poly_step): reads o->p, writes o->q. */
 static void mix_poly_step(ens_oracle* o, int p, int* req) {

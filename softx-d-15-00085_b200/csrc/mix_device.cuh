@@ -44,7 +44,7 @@ constexpr int kMixMaxV = 16;     // vertices of a shape
 constexpr int kMixMaxF = 28;     // triangular faces (2 V - 4)
 constexpr int kMixMaxE = 42;     // edges (3 V - 6)
 constexpr int kMixSlots = 64;    // neighbour slots of a polyhedron
-constexpr int kMixWallSlots = 8; // wall contacts (tangential histories) of a polyhedron
+constexpr int kMixWallSlots = 16; // wall contacts (tangential histories) of a polyhedron
 
 struct MixShapeDev {
   int nv, nf, ne, pad;

@@ -8,7 +8,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMixWarps = 4;      // warps (polyhedra) per block of the step
-constexpr int kMixHits = 16;      // touching triangles kept per polyhedron and step
+constexpr int kMixHits = 32;      // touching triangles kept per polyhedron and step
 
 inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
@@ -330,6 +330,7 @@ struct MixSmem {
   double3 nd[kMixHits];     // touching triangles: unrounded normal, contact, id
   MixHit hit[kMixHits];
   int hid[kMixHits];
+  float4 oh[kMixWallSlots]; // the polyhedron's wall histories before the step
 };
 
 __device__ __forceinline__ float3 mat_vec_f(const float* R, float3 v) {
@@ -583,15 +584,12 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
     // processing order over them
     float4* wh = m.wh + (size_t)p * kMixWallSlots;
     const int nw_o = m.wn[p];
-    float4 oh[kMixWallSlots];
-#pragma unroll
-    for (int qs = 0; qs < kMixWallSlots; ++qs)
-      oh[qs] = qs < nw_o ? wh[qs] : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+    float4* oh = sm.oh;
+    for (int qs = 0; qs < nw_o; ++qs) oh[qs] = wh[qs];
     int nw = 0;
     auto wall = [&](int id, const MixHit& h, bool moving) {
       float3 xi = f3(0.0f, 0.0f, 0.0f);
-#pragma unroll
-      for (int qs = 0; qs < kMixWallSlots; ++qs)
+      for (int qs = 0; qs < nw_o; ++qs)
         if (__float_as_int(oh[qs].w) == id) xi = f3(oh[qs].x, oh[qs].y, oh[qs].z);
       const float3 vw = moving ? cross3(S.rot_a, (xa + h.ca) - S.rot_o) * S.rot_w
                                : f3(0.0f, 0.0f, 0.0f);
