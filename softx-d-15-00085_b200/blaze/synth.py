@@ -1093,7 +1093,8 @@ def mixed_box_ensemble(n_spheres=300, n_rocks=24, L=10.0, H=20.0, r_min=0.3, r_m
                        rock_radius=(0.5, 1.0), rho=7800.0, rock_rho=2700.0, kn=1e6,
                        restitution=0.4, mu=0.6, skin=0.04, seed=2, gravity=(0.0, 0.0, -981.0)):
     """Steel balls and rocks in a closed box [0, L]^2 x [0, H] (six planes):
-    rocks (rock_shapes, seed) at random sites of a lattice of pitch 2 R_max,
+    rocks (rock_shapes, seed) at random sites of a lattice of pitch
+    2 r_bound + 0.05 (r_bound the largest rock's bounding radius),
     balls r ~ U[r_min, r_max] on a lattice of pitch 2 r_max + skin / 2 clear
     of the rocks, at rest; linear law kn (kt = 2/7 kn), restitution, mu.
     Returns (systems, walls, pos, radius, shapes, shape_of, quat)."""
@@ -1108,9 +1109,8 @@ def mixed_box_ensemble(n_spheres=300, n_rocks=24, L=10.0, H=20.0, r_min=0.3, r_m
     m = 0.05
     sph = lattice_fill(None, (r_max + m,) * 2 + (r_max + m,), (L - r_max - m,) * 2 + (H - r_max - m,),
                        2.0 * r_max + 0.5 * skin, rng)
-    rk = lattice_fill(None, (rock_radius[1] + m,) * 2 + (rock_radius[1] + m,),
-                      (L - rock_radius[1] - m,) * 2 + (H - rock_radius[1] - m,),
-                      2.0 * rock_radius[1] + 0.1, rng)
+    rk = lattice_fill(None, (rb + m,) * 2 + (rb + m,), (L - rb - m,) * 2 + (H - rb - m,),
+                      2.0 * rb + 0.05, rng)
     sph, sph_r, rocks = _mixed_placement(rng, sph, rk, n_spheres, n_rocks, r_min, r_max, rbs, 2)
     pos, rad, shape_of, quat = mixed_charge_state(sph, sph_r, rocks, shapes, rng)
     return [s], walls, pos, rad, shapes, shape_of, quat
@@ -1126,7 +1126,8 @@ def mill_mixed_ensemble(n_spheres=100_000, n_rocks=5_000, R=50.0, L=30.0, n_seg=
     balls r ~ U[r_min, r_max] (density rho) and rocks (rock_shapes: hulls of
     8-16 points on spheres of radius rock_radius, seed, density rock_rho),
     the count ratio of the configuration's 2,000,000 : 100,000; rocks at
-    random sites of a lattice of pitch 2 R_max + 0.1, balls on a lattice of
+    random sites of a lattice of pitch 2 r_bound + 0.05 (r_bound the largest
+    rock's bounding radius), balls on a lattice of
     pitch 2 r_max + skin / 2 clear of them, inside the lifter ring from the
     bottom up, at rest; linear law kn (kt = 2/7 kn), restitution, mu, rpm
     about z.  Returns (systems, walls, pos, radius, shapes, shape_of, quat)."""
@@ -1158,9 +1159,8 @@ def mill_mixed_ensemble(n_spheres=100_000, n_rocks=5_000, R=50.0, L=30.0, n_seg=
     sph = lattice_fill(None, (-r_in, -r_in, r_max + m), (r_in, r_in, L - r_max - m),
                        2.0 * r_max + 0.5 * skin, rng)
     sph = sph[np.hypot(sph[:, 0], sph[:, 1]) < r_in - r_max]
-    rk = lattice_fill(None, (-r_in, -r_in, rock_radius[1] + m),
-                      (r_in, r_in, L - rock_radius[1] - m), 2.0 * rock_radius[1] + 0.1, rng)
-    rk = rk[np.hypot(rk[:, 0], rk[:, 1]) < r_in - rock_radius[1]]
+    rk = lattice_fill(None, (-r_in, -r_in, rb + m), (r_in, r_in, L - rb - m), 2.0 * rb + 0.05, rng)
+    rk = rk[np.hypot(rk[:, 0], rk[:, 1]) < r_in - rb]
     sph, sph_r, rocks = _mixed_placement(rng, sph, rk, n_spheres, n_rocks, r_min, r_max, rbs, 1)
     pos, rad, shape_of, quat = mixed_charge_state(sph, sph_r, rocks, shapes, rng)
     return [s], walls, pos, rad, shapes, shape_of, quat

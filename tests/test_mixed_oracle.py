@@ -252,3 +252,26 @@ def test_elastic_frictionless_collisions_keep_energy():
           % (e0, e1, e1 / e0 - 1.0, touched))
     assert touched and np.abs(f).max() == 0.0
     assert abs(e1 / e0 - 1.0) < 2e-3
+
+
+def test_mixed_charge_generators():
+    """The mixed charges start without overlaps: every ball keeps 0.02 cm
+    from every rock's bounding sphere and from the other balls, rocks from
+    each other; the mill's charge holds the configuration's 20 : 1 count
+    ratio inside the lifter ring."""
+    from scipy.spatial import cKDTree
+    cases = [synth.mixed_box_ensemble(),
+             synth.mill_mixed_ensemble(n_spheres=20000, n_rocks=1000)]
+    for S, W, p, r, sh, so, q in cases:
+        p = p.astype(np.float64)
+        rk, sp = so >= 0, so < 0
+        d, k = cKDTree(p[rk]).query(p[sp])
+        assert np.all(d - r[sp] - r[rk][k] >= 0.02 - 1e-5)
+        pairs = cKDTree(p).query_pairs(2.5, output_type="ndarray")
+        gap = np.linalg.norm(p[pairs[:, 0]] - p[pairs[:, 1]], axis=1) - r[pairs[:, 0]] - r[pairs[:, 1]]
+        assert gap.min() > 0.0
+        assert np.all(2 * r + 0.04 <= S[0].cell)
+        np.testing.assert_allclose(np.linalg.norm(q, axis=1), 1.0, atol=1e-6)
+    S, W, p, r, sh, so, q = cases[1]
+    assert (so < 0).sum() == 20 * (so >= 0).sum()
+    assert np.hypot(p[:, 0], p[:, 1]).max() < 50.0 - 4.0
