@@ -164,14 +164,16 @@ int blaze_ens_profile(blaze_ens* e, float* ms4, int* steps);
  *               triangles touched together count once, the deepest),
  *   planes      at its deepest vertex,
  * all formed in FP64 from the FP32 state; the contact point is the mean of
- * the penetrating vertices, or the midpoint of two crossing edges.  The law
+ * the penetrating vertices weighted by their depths, or the midpoint of two
+ * crossing edges.  The law
  * is the linear law with tangential history and Coulomb cap on the contact
  * point's relative velocity, without rolling friction; a polyhedron
  * integrates Euler's equations in its body frame and its orientation as a
  * unit quaternion.  Systems holding polyhedra: linear law, plane and
- * triangle walls (no cylinders), 2 r_bound + skin <= cell, at most 64
- * neighbours per polyhedron; not with persistent stepping (use_graph 2
- * steps as 1) nor reverse mode. */
+ * triangle walls (no cylinders), 2 r_bound + skin <= cell; per
+ * polyhedron at most 64 neighbours, 16 wall contacts and 32 touching
+ * triangles a step (beyond them status 1); not with persistent stepping
+ * (use_graph 2 steps as 1) nor reverse mode. */
 typedef struct blaze_shape {
   int nverts;            /* 4 .. 16 */
   int nfaces;            /* 2 nverts - 4 */
