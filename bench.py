@@ -626,7 +626,7 @@ def mill_mesh_leg(steps=5000, warmup=20, n=100_000, settle=60000, skin=0.04):
 
 
 def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, settle=60000,
-                   skin=0.04, block=256):
+                   skin=0.04, block=256, cpu_seconds=10.0, want_cpu=True):
     """The ball mill's mixed charge (ensemble path; the reference runs
     spheres or polyhedra, never both): the turning drum of mill_mesh_leg with
     n_spheres steel balls r ~ U[0.3, 0.6] cm and n_rocks rocks (convex hulls
@@ -634,9 +634,11 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
     kg/m^3): the configuration's 2,000,000 : 100,000 count ratio at the
     charge the drum holds.  Linear law with tangential history kn = 1e6,
     e = 0.4, mu = 0.6, dt = 2e-6 s, 30 rpm.  `settle` untimed steps with the
-    drum turning, then `steps` graph steps timed with CUDA events.  No CPU
-    baseline: the reference cannot run the charge, and the restatement tests
-    every triangle for every particle (minutes a step at this size)."""
+    drum turning, then `steps` graph steps timed with CUDA events.  CPU: the
+    reference cannot run the charge, so the baseline is the C restatement
+    of the same step (oracle/ens_oracle.c, FP32, one host thread, kind
+    "port"), a bounded sample of whole steps from the GPU's state after its
+    timed steps (histories start empty there)."""
     import torch
     from blaze import synth
     from blaze import ensemble as E
@@ -660,12 +662,32 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
     rebuilds = ens.num_rebuilds() - rb0
     launches = ens.last_launches() + rebuilds * ens.rebuild_kernels()
     st = ens.state()
+    qq = ens.orientations()
     # device time by phase over plain steps (each waits for the device)
     ens.set_profile(True)
     ens.step(50)
     ph, nph = ens.profile()
     ens.set_profile(False)
     ens.close()
+    cpu = None
+    if want_cpu:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from bindings import EnsRestated
+        o = np.argsort(st["pid"])
+        x = EnsRestated(S, W, E.LAW_LINEAR, 2e-6, skin, 32, precision="f32")
+        x.set_state(st["pos"][o], r, st["vel"][o], st["avel"][o])
+        x.set_polyhedra(sh, so, qq[o])
+        t0 = time.perf_counter()
+        x.step(1)
+        one = time.perf_counter() - t0
+        k = max(1, min(500, int(cpu_seconds / max(one, 1e-6))))
+        t0 = time.perf_counter()
+        x.step(k)
+        dt = time.perf_counter() - t0
+        x.close()
+        cpu = {"value": n * k / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "%d whole steps (%.1f s) of the C restatement, one thread, from the "
+                         "GPU's state after its timed steps" % (k, dt)}
     rocks = so[st["pid"]] >= 0
     x, y = st["pos"][:, 0].astype(np.float64), st["pos"][:, 1].astype(np.float64)
     vt = -(x * st["vel"][:, 1] - y * st["vel"][:, 0]) / np.maximum(np.hypot(x, y), 1e-9)
@@ -683,7 +705,8 @@ def mill_mixed_leg(steps=5000, warmup=20, n_spheres=100_000, n_rocks=5_000, sett
                                        zip(("resort", "polyhedron_geometry", "polyhedron_step",
                                             "sphere_step"), ph)},
             "mean_tangential_velocity_cm_s": {"spheres": float(vt[~rocks].mean()),
-                                              "rocks": float(vt[rocks].mean())}}
+                                              "rocks": float(vt[rocks].mean())},
+            "cpu_baseline": cpu, "vs_cpu_port": None if not cpu else n / (ms * 1e-3) / cpu["value"]}
 
 
 def case_mixed(n_spheres=100_000, n_rocks=5_000, settle=60000, steps=4):
@@ -1054,7 +1077,8 @@ def main():
                                   want_cpu=not args.no_cpu_baseline)))
         return 0
     if args.mill_mixed_only:
-        print(json.dumps(mill_mixed_leg(args.mill_steps, args.warmup)))
+        print(json.dumps(mill_mixed_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                                        want_cpu=not args.no_cpu_baseline)))
         return 0
     if args.poly_only:
         print(json.dumps(poly_leg(args.poly_steps, args.warmup, cpu_seconds=args.cpu_seconds,
@@ -1204,7 +1228,8 @@ def main():
         mill_mesh = mill_mesh_leg(args.mill_steps, args.warmup)
     mill_mixed = None
     if not args.no_mill_mixed:
-        mill_mixed = mill_mixed_leg(args.mill_steps, args.warmup)
+        mill_mixed = mill_mixed_leg(args.mill_steps, args.warmup, cpu_seconds=args.cpu_seconds,
+                                    want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
     c1 = None
     if not args.no_c1:
         c1 = c1_leg(2000, args.warmup, want_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)

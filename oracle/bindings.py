@@ -393,6 +393,7 @@ class EnsRestated:
             lib.ens_adj_record.argtypes = [C.c_void_p, C.c_int]
             lib.ens_adj_reverse.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _d, _d]
             lib.ens_set_polyhedra.argtypes = [C.c_void_p, C.POINTER(E.Shape), C.c_int, _i, _d]
+            lib.ens_use_tri_lists.argtypes = [C.c_void_p, C.c_int]
             lib.ens_get_orientations.argtypes = [C.c_void_p, _d]
             EnsRestated._libs[path] = lib
         self.lib = EnsRestated._libs[path]
@@ -436,6 +437,11 @@ class EnsRestated:
         rc = self.lib.ens_set_polyhedra(self.h, arr, len(shapes), _p(so, C.c_int), _p(q, C.c_double))
         if rc != 0:
             raise ValueError("ens_set_polyhedra: %d" % rc)
+
+    def use_tri_lists(self, on):
+        """1 (default): the triangles of the particle's cell only; 0: every
+        triangle of the system (the same contacts)."""
+        self.lib.ens_use_tri_lists(self.h, int(bool(on)))
 
     def orientations(self):
         q = np.zeros((self.n, 4))

@@ -128,6 +128,13 @@ struct ens_oracle {
   struct tstep_* tape; /* recorded steps of the reverse sweep */
   int ntape;
   struct mixc_* mix;   /* polyhedra among the spheres (NULL: spheres only) */
+  /* candidate triangles per cell (CSR over the global cell table), as the
+     library bins them; with use_tri_lists 0 every triangle of the system is
+     tested (the same contacts: the lists hold every triangle a particle
+     centred in the cell can touch) */
+  uint32_t* tri_off;
+  uint32_t* tri_ids;
+  int use_tri_lists;
 };
 
 static void constants(sysc* d, const blaze_system* s, uint32_t off, float dt) {
@@ -169,6 +176,66 @@ static v3 rot_about(v3 a, real c, real s, v3 v) {
   const real av = dot(a, v);
   return add(add(mul(v, c), mul(axv, s)), mul(a, av * ((real)1.0 - c)));
 }
+
+typedef struct { uint32_t cell, tri; } ctpair;
+static int ctpair_cmp(const void* a, const void* b) {
+  const ctpair* x = (const ctpair*)a;
+  const ctpair* y = (const ctpair*)b;
+  if (x->cell != y->cell) return x->cell < y->cell ? -1 : 1;
+  return x->tri < y->tri ? -1 : (x->tri > y->tri);
+}
+
+/* Candidate triangles per cell (csrc/ens_capi.cu, build_tri_lists): every
+ * cell whose box meets the triangle's bounding box grown by half a cell,
+ * in ascending triangle order. */
+static void build_tri_lists(ens_oracle* o, const blaze_system* sys) {
+  size_t np = 0, cap = 1024;
+  ctpair* pr = (ctpair*)malloc(sizeof(ctpair) * cap);
+  for (int s = 0; s < o->nsys; ++s) {
+    const blaze_system* S = &sys[s];
+    const double cell = (double)S->cell;
+    const double margin = 0.5 * cell + 1e-4 * cell;
+    for (int t = S->tri0; t < S->tri0 + S->ntris; ++t) {
+      const wallc* W = &o->W[t];
+      const v3 v[3] = {W->a, W->b, W->c};
+      int lo[3], hi[3];
+      for (int c = 0; c < 3; ++c) {
+        double mn = 1e300, mx = -1e300;
+        for (int k = 0; k < 3; ++k) {
+          const double x = (double)(float)(c == 0 ? v[k].x : (c == 1 ? v[k].y : v[k].z));
+          if (x < mn) mn = x;
+          if (x > mx) mx = x;
+        }
+        const double og = (double)S->origin[c];
+        const int ncs = S->ncells[c];
+        const int l = (int)floor((mn - margin - og) / cell), h = (int)floor((mx + margin - og) / cell);
+        lo[c] = l > 0 ? l : 0;
+        hi[c] = h < ncs - 1 ? h : ncs - 1;
+      }
+      for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+          for (int x = lo[0]; x <= hi[0]; ++x) {
+            if (np == cap) { cap *= 2; pr = (ctpair*)realloc(pr, sizeof(ctpair) * cap); }
+            pr[np].cell = o->S[s].cell_off + (uint32_t)(x + S->ncells[0] * (y + S->ncells[1] * z));
+            pr[np].tri = (uint32_t)t;
+            ++np;
+          }
+    }
+  }
+  qsort(pr, np, sizeof(ctpair), ctpair_cmp);
+  o->tri_off = (uint32_t*)calloc((size_t)o->ncell_tab + 1, sizeof(uint32_t));
+  o->tri_ids = (uint32_t*)malloc(sizeof(uint32_t) * (np ? np : 1));
+  for (size_t k = 0; k < np; ++k) {
+    o->tri_off[pr[k].cell + 1]++;
+    o->tri_ids[k] = pr[k].tri;
+  }
+  for (uint32_t c = 0; c < o->ncell_tab; ++c) o->tri_off[c + 1] += o->tri_off[c];
+  free(pr);
+}
+
+/* Test infrastructure switch: 0 tests every triangle of a system (the
+ * restatement's first form), 1 the candidates of the particle's cell. */
+void ens_use_tri_lists(ens_oracle* o, int on) { o->use_tri_lists = on; }
 
 ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* walls, int nwalls,
                        int law, double dt, double skin, int max_nbr) {
@@ -243,6 +310,8 @@ ens_oracle* ens_create(const blaze_system* sys, int nsys, const blaze_wall* wall
   int k = 0;
   for (int s = 0; s < nsys; ++s)
     for (int m = 0; m < sys[s].n; ++m) o->sys_of[k++] = s;
+  build_tri_lists(o, sys);
+  o->use_tri_lists = 1;
   return o;
 }
 
@@ -255,7 +324,7 @@ void ens_destroy(ens_oracle* o) {
   free(o->S); free(o->W); free(o->p); free(o->q);
   for (int c = 0; c < 2; ++c) { free(o->idx[c]); free(o->cnt[c]); free(o->mask[c]); free(o->hist[c]); }
   free(o->cstart); free(o->cend); free(o->cap_f); free(o->cap_t); free(o->sys_of);
-  free(o->rot_c); free(o->rot_s);
+  free(o->rot_c); free(o->rot_s); free(o->tri_off); free(o->tri_ids);
   free(o);
 }
 
@@ -1441,6 +1510,8 @@ static void mix_poly_step(ens_oracle* o, int p, int* req) {
   int cc[3];
   const v3 pd = rot ? add(S->rot_o, rot_about(S->rot_a, rc, -rsn, sub(a->pos, S->rot_o))) : a->pos;
   if (S->ntri > 0 && cell_of(S, pd, cc)) {
+    const uint32_t tq0 = o->use_tri_lists ? o->tri_off[key_of(S, cc)] : 0u;
+    const uint32_t tq1 = o->use_tri_lists ? o->tri_off[key_of(S, cc) + 1] : (uint32_t)S->ntri;
     /* the polyhedron in the drum's frame */
     double Vd[MIX_V * 4], Fd[MIX_F * 4];
     hullr D = A;
@@ -1462,7 +1533,8 @@ static void mix_poly_step(ens_oracle* o, int p, int* req) {
     mhit hits[MIX_HITS];
     dv3 nds[MIX_HITS];
     int ids[MIX_HITS], nhit = 0;
-    for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+    for (uint32_t q_ = tq0; q_ < tq1; ++q_) {
+      const int w = o->use_tri_lists ? (int)o->tri_ids[q_] : S->tri0 + (int)q_;
       const wallc* W = &o->W[w];
       int reg, feat;
       const v3 cp = closest_tri(pd, W->a, W->b, W->c, &reg, &feat);
@@ -1657,15 +1729,19 @@ static void step_once_rec(ens_oracle* o, tstep* t) {
     const v3 pd = S->rot ? add(S->rot_o, rot_about(S->rot_a, rc, -rsn, sub(a->pos, S->rot_o)))
                          : a->pos;
     if (S->ntri > 0 && cell_of(S, pd, cc)) {
+    const uint32_t tq0 = o->use_tri_lists ? o->tri_off[key_of(S, cc)] : 0u;
+    const uint32_t tq1 = o->use_tri_lists ? o->tri_off[key_of(S, cc) + 1] : (uint32_t)S->ntri;
       int nface = 0, best = -1;
       real best_d = 0;
-      for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+      for (uint32_t q_ = tq0; q_ < tq1; ++q_) {
+      const int w = o->use_tri_lists ? (int)o->tri_ids[q_] : S->tri0 + (int)q_;
         v3 nn; real d; int reg;
         if (!wall_touch(&o->W[w], pd, ra, &nn, &d, &reg)) continue;
         if (reg == 0) ++nface;
         else if (best < 0 || d > best_d) { best = w; best_d = d; }
       }
-      for (int w = S->tri0; w < S->tri0 + S->ntri; ++w) {
+      for (uint32_t q_ = tq0; q_ < tq1; ++q_) {
+      const int w = o->use_tri_lists ? (int)o->tri_ids[q_] : S->tri0 + (int)q_;
         v3 nn; real d; int reg;
         if (!wall_touch(&o->W[w], pd, ra, &nn, &d, &reg)) continue;
         if ((nface > 0 && reg == 0) || (nface == 0 && w == best))

@@ -69,9 +69,7 @@ def run_both(case, checkpoints, use_graph=1):
     return out
 
 
-# the restatement tests every triangle of the drum for every particle (7 ms
-# a step here), so the drum runs fewer steps
-CHECKPOINTS = {"box": [1, 50, 2000, 8000, 20000], "drum": [1, 50, 2000, 6000]}
+CHECKPOINTS = {"box": [1, 50, 2000, 8000, 20000], "drum": [1, 50, 2000, 8000, 20000]}
 
 
 @pytest.mark.parametrize("name", ["box", "drum"])

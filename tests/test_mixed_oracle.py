@@ -275,3 +275,43 @@ def test_mixed_charge_generators():
     S, W, p, r, sh, so, q = cases[1]
     assert (so < 0).sum() == 20 * (so >= 0).sum()
     assert np.hypot(p[:, 0], p[:, 1]).max() < 50.0 - 4.0
+
+
+@pytest.mark.parametrize("case", ["mixed_drum", "sphere_drum"])
+def test_restatement_triangle_lists_change_nothing(case):
+    """The restatement's per-cell triangle candidates give the same run, bit
+    for bit, as testing every triangle of the system: 400 steps from the
+    state after 12,000 (the charge on the liner and lifters)."""
+    kw = dict(R=12.0, L=8.0, n_seg=48, n_len=6, n_lifters=4, lifter_w=2.0, lifter_h=2.0, kn=1e5)
+    if case == "mixed_drum":
+        S, W, p, r, sh, so, q = synth.mill_mixed_ensemble(n_spheres=400, n_rocks=24, **kw)
+    else:
+        S, W, p, r = synth.drum_mesh_ensemble(n=600, **kw)
+        sh = None
+
+    def restated(on, pos, vel=None, avel=None, quat=None):
+        o = EnsRestated(S, W, E.LAW_LINEAR, 1e-5, 0.04, 32, precision="f32")
+        o.use_tri_lists(on)
+        o.set_state(pos, r, vel, avel)
+        if sh is not None:
+            o.set_polyhedra(sh, so, quat)
+        return o
+
+    o = restated(1, p, quat=None if sh is None else q)
+    o.step(12000)
+    st = o.state()
+    qq = o.orientations()
+    o.close()
+    k = np.argsort(st["pid"])
+    pos, vel, avel, quat = st["pos"][k], st["vel"][k], st["avel"][k], qq[k]
+    reach = np.hypot(pos[:, 0], pos[:, 1]) + r
+    assert reach.max() > 12.0 * np.cos(np.pi / 48) - 0.05      # touching the liner
+    runs = []
+    for on in (1, 0):
+        o = restated(on, pos, vel, avel, quat)
+        o.step(400)
+        st = o.state()
+        runs.append((st["pos"], st["vel"], st["avel"], st["status"]))
+        o.close()
+    for a, b in zip(*runs):
+        np.testing.assert_array_equal(a, b)
