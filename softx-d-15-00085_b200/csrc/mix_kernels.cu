@@ -66,13 +66,16 @@ k_mix_geom(MixBufs m) {
 // -------------------------------------------------------------- the list
 // Pairs with |xi - xj|^2 < (ri + rj + skin)^2 (bounding radii) from the 27
 // surrounding cells, in the sphere list's order (z, y, x; j ascending); the
-// history of an old slot moves to the new slot of the same partner pid.
+// history of an old slot moves to the new slot of the same partner pid.  A
+// warp per polyhedron: the lanes take consecutive candidates of a cell and
+// a ballot hands out the slots in candidate order.
 __global__ void __launch_bounds__(kThreads)
 k_mix_plist(EnsGeom g, EnsBufs b, MixBufs m, const float4* __restrict__ pos,
             const float4* __restrict__ vel, const uint32_t* __restrict__ cstart,
             const uint32_t* __restrict__ cend, StepCtl* ctl, const int* gate) {
   if (gate && *gate == 0) return;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (p >= m.npoly) return;
   const int e = ctl->epoch & 1;
   const MixList Lo = m.L[e], Ln = m.L[e ^ 1];
@@ -90,7 +93,7 @@ k_mix_plist(EnsGeom g, EnsBufs b, MixBufs m, const float4* __restrict__ pos,
   const unsigned long long mask_o =
       (unsigned long long)Lo.mlo[p] | ((unsigned long long)Lo.mhi[p] << 32);
   uint32_t cnt = 0, st = 0;
-  unsigned long long mask = 0;
+  unsigned long long mask = 0;   // lane-local bits, merged at the end
   if (ens_in(S, c)) {
     const int x0 = c.x > 0 ? c.x - 1 : 0, x1 = c.x < S.nc.x - 1 ? c.x + 1 : c.x;
     const int y0 = c.y > 0 ? c.y - 1 : 0, y1 = c.y < S.nc.y - 1 ? c.y + 1 : c.y;
@@ -100,50 +103,63 @@ k_mix_plist(EnsGeom g, EnsBufs b, MixBufs m, const float4* __restrict__ pos,
         const uint32_t row = S.cell_off + (uint32_t)(S.nc.x * (y + S.nc.y * z));
         for (int x = x0; x <= x1; ++x) {
           const uint32_t h = row + (uint32_t)x;
-          const uint32_t s = __ldg(cstart + h);
-          if (s == 0xffffffffu) continue;
+          const uint32_t s0 = __ldg(cstart + h);
+          if (s0 == 0xffffffffu) continue;
           const uint32_t eo = __ldg(cend + h);
-          for (uint32_t j = s; j < eo; ++j) {
-            if ((int)j == i) continue;
-            const float4 pb = __ldg(pos + j);
-            const float3 rel = pa - xyz(pb);
-            const float lim = (ra + fabsf(pb.w)) + g.skin;
-            if (!(dot3(rel, rel) < lim * lim)) continue;
-            if (cnt < (uint32_t)kMixSlots) {
-              Ln.idx[(size_t)cnt * P + p] = j;
-              Ln.sep[(size_t)cnt * P + p] = -1;
-              unsigned long long mo = mask_o;
-              if (mo) {
-                const int pj = pid_new[j];
-                while (mo) {
-                  const int ko = __ffsll((long long)mo) - 1;
-                  mo &= mo - 1ull;
-                  if ((uint32_t)ko >= cnt_o) break;
-                  const size_t so = (size_t)ko * P + p;
-                  if (pid_old[Lo.idx[so]] == pj) {
-                    const size_t sn = (size_t)cnt * P + p;
-                    Ln.hx[sn] = Lo.hx[so];
-                    Ln.hy[sn] = Lo.hy[so];
-                    Ln.hz[sn] = Lo.hz[so];
-                    mask |= 1ull << cnt;
-                    break;
+          for (uint32_t j0 = s0; j0 < eo; j0 += 32) {
+            const uint32_t j = j0 + (uint32_t)lane;
+            bool hit = false;
+            if (j < eo && (int)j != i) {
+              const float4 pb = __ldg(pos + j);
+              const float3 rel = pa - xyz(pb);
+              const float lim = (ra + fabsf(pb.w)) + g.skin;
+              hit = dot3(rel, rel) < lim * lim;
+            }
+            const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+              const uint32_t k = cnt + (uint32_t)__popc(hb & ((1u << lane) - 1u));
+              if (k < (uint32_t)kMixSlots) {
+                Ln.idx[(size_t)k * P + p] = j;
+                Ln.sep[(size_t)k * P + p] = -1;
+                unsigned long long mo = mask_o;
+                if (mo) {
+                  const int pj = pid_new[j];
+                  while (mo) {
+                    const int ko = __ffsll((long long)mo) - 1;
+                    mo &= mo - 1ull;
+                    if ((uint32_t)ko >= cnt_o) break;
+                    const size_t so = (size_t)ko * P + p;
+                    if (pid_old[Lo.idx[so]] == pj) {
+                      const size_t sn = (size_t)k * P + p;
+                      Ln.hx[sn] = Lo.hx[so];
+                      Ln.hy[sn] = Lo.hy[so];
+                      Ln.hz[sn] = Lo.hz[so];
+                      mask |= 1ull << k;
+                      break;
+                    }
                   }
                 }
+              } else {
+                st |= kStatusListOverflow;
               }
-            } else {
-              st |= kStatusListOverflow;
             }
-            ++cnt;
+            cnt += (uint32_t)__popc(hb);
           }
         }
       }
   } else {
     st |= kStatusOutOfGrid;
   }
-  Ln.cnt[p] = cnt < (uint32_t)kMixSlots ? cnt : (uint32_t)kMixSlots;
-  Ln.mlo[p] = (uint32_t)mask;
-  Ln.mhi[p] = (uint32_t)(mask >> 32);
-  if (st) atomicOr(&ctl->status, st);
+  // the lanes' history bits together
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mask |= __shfl_xor_sync(0xffffffffu, mask, o);
+  st = __reduce_or_sync(0xffffffffu, st);
+  if (lane == 0) {
+    Ln.cnt[p] = cnt < (uint32_t)kMixSlots ? cnt : (uint32_t)kMixSlots;
+    Ln.mlo[p] = (uint32_t)mask;
+    Ln.mhi[p] = (uint32_t)(mask >> 32);
+    if (st) atomicOr(&ctl->status, st);
+  }
 }
 
 // The twin of every sphere slot that holds a polyhedron: the polyhedron's
@@ -699,8 +715,8 @@ void mix_launch_plist(const EnsGeom& g, const EnsBufs& b, const MixBufs& m,
                       const uint32_t* cstart, const uint32_t* cend, StepCtl* ctl,
                       const int* gate, cudaStream_t st) {
   if (m.npoly <= 0) return;
-  k_mix_plist<<<nblk(m.npoly), kThreads, 0, st>>>(g, b, m, b.S[2].pos, b.S[2].vel, cstart, cend,
-                                                  ctl, gate);
+  k_mix_plist<<<nblk(32 * m.npoly), kThreads, 0, st>>>(g, b, m, b.S[2].pos, b.S[2].vel, cstart,
+                                                       cend, ctl, gate);
 }
 
 void mix_launch_twins(const EnsBufs& b, const MixBufs& m, int n, StepCtl* ctl, const int* gate,
