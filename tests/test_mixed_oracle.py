@@ -315,3 +315,159 @@ def test_restatement_triangle_lists_change_nothing(case):
         o.close()
     for a, b in zip(*runs):
         np.testing.assert_array_equal(a, b)
+
+
+# ------------------------------------------------- narrow phases, brute force
+def _rot(q):
+    """The rotation of (w, x, y, z) as the restatement forms it: the FP32
+    quaternion, normalised in FP64 through 2 / |q|^2."""
+    q = [float(v) for v in q]
+    qn = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    w, x, y, z = (float(np.float32(v / qn)) for v in q)
+    s = 2.0 / (((w * w + x * x) + y * y) + z * z)
+    return np.array([[1 - s * (y * y + z * z), s * (x * y - w * z), s * (x * z + w * y)],
+                     [s * (x * y + w * z), 1 - s * (x * x + z * z), s * (y * z - w * x)],
+                     [s * (x * z - w * y), s * (y * z + w * x), 1 - s * (x * x + y * y)]])
+
+
+def _world(shape, q, centre):
+    v = np.asarray(shape.verts, np.float64).reshape(-1, 3)[:shape.nverts]
+    f = np.asarray(shape.faces).reshape(-1, 3)[:shape.nfaces]
+    return v @ _rot(q).T + centre, f
+
+
+def _axes(v, f):
+    n = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    e = set()
+    for t in f:
+        for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+            e.add((min(a, b), max(a, b)))
+    return n, np.array([v[b] - v[a] for a, b in e])
+
+
+def _penetration(va, fa, vb, fb):
+    """Minimum overlap of two convex hulls over every face normal and every
+    edge-pair cross product (full support extents, no pruning): their
+    penetration depth when positive, a separation when negative."""
+    na, ea = _axes(va, fa)
+    nb, eb = _axes(vb, fb)
+    cr = np.cross(ea[:, None, :], eb[None, :, :]).reshape(-1, 3)
+    ln = np.linalg.norm(cr, axis=1)
+    ax = np.concatenate([na, nb, cr[ln > 1e-9] / ln[ln > 1e-9, None]])
+    pa, pb = va @ ax.T, vb @ ax.T
+    over = np.minimum(pa.max(0) - pb.min(0), pb.max(0) - pa.min(0))
+    return over.min()
+
+
+def test_hull_pairs_against_brute_force():
+    """Two rocks at random orientations and distances: the restatement's
+    contact exists exactly when the brute-force separating-axis test finds
+    overlap on every axis, and its depth (|F| / kn from rest) lies between
+    the penetration depth and the depth over the feature tolerances (a face
+    is kept over an edge pair up to 1 / 0.9 of its depth)."""
+    rng = np.random.default_rng(11)
+    shapes = synth.rock_shapes(12, seed=11)
+    kn = 1e5
+    checked = touching = 0
+    for trial in range(150):
+        a, b = rng.choice(12, 2, replace=False)
+        qa, qb = synth.random_quaternions(rng, 2)
+        ca = np.array([10.0, 10.0, 10.0])
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        ra = synth._bounding_radius(shapes[a])
+        rb = synth._bounding_radius(shapes[b])
+        cb = ca + d * rng.uniform(0.3, 1.0) * (ra + rb)
+        va, fa = _world(shapes[a], qa, ca)
+        vb, fb = _world(shapes[b], qb, cb)
+        pen = _penetration(va, fa, vb, fb)
+        if abs(pen) < 1e-6:
+            continue
+        o, _ = scene([ca, cb], [ra, rb], [shapes[a], shapes[b]], [0, 1], [qa, qb],
+                     gravity=(0.0, 0.0, 0.0), kn=kn)
+        o.step(1)
+        f, _ = o.forces()
+        o.close()
+        depth = np.linalg.norm(f[0]) / kn
+        checked += 1
+        if pen < 0:
+            assert depth == 0.0, (trial, pen, depth)
+        else:
+            touching += 1
+            assert pen * (1 - 1e-9) <= depth <= pen / 0.9 * (1 + 1e-9), (trial, pen, depth)
+    print("hull pairs: %d checked, %d in contact" % (checked, touching))
+    assert checked > 100 and touching > 20
+
+
+def _closest_on_triangle(p, a, b, c):
+    ab, ac, ap = b - a, c - a, p - a
+    d1, d2 = ab @ ap, ac @ ap
+    if d1 <= 0 and d2 <= 0:
+        return a
+    bp = p - b
+    d3, d4 = ab @ bp, ac @ bp
+    if d3 >= 0 and d4 <= d3:
+        return b
+    vc = d1 * d4 - d3 * d2
+    if vc <= 0 and d1 >= 0 and d3 <= 0:
+        return a + ab * (d1 / (d1 - d3))
+    cp = p - c
+    d5, d6 = ab @ cp, ac @ cp
+    if d6 >= 0 and d5 <= d6:
+        return c
+    vb = d5 * d2 - d1 * d6
+    if vb <= 0 and d2 >= 0 and d6 <= 0:
+        return a + ac * (d2 / (d2 - d6))
+    va = d3 * d6 - d5 * d4
+    if va <= 0 and (d4 - d3) >= 0 and (d5 - d6) >= 0:
+        return b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)))
+    den = 1.0 / (va + vb + vc)
+    return a + ab * (vb * den) + ac * (vc * den)
+
+
+def test_sphere_hull_against_closest_point():
+    """A ball at random places around a rock: the restatement's overlap
+    (|F| / kn from rest) is r minus the distance to the hull's nearest
+    point over all its faces, or r plus the depth when the centre is
+    inside."""
+    rng = np.random.default_rng(12)
+    shapes = synth.rock_shapes(6, seed=12)
+    kn = 1e5
+    checked = touching = 0
+    for trial in range(150):
+        k = int(rng.integers(6))
+        q = synth.random_quaternions(rng, 1)[0]
+        cp = np.array([10.0, 10.0, 10.0])
+        rb = synth._bounding_radius(shapes[k])
+        r = float(np.float32(rng.uniform(0.3, 0.6)))
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        cs = cp + d * rng.uniform(0.0, 1.0) * (rb + r)
+        v, f = _world(shapes[k], q, cp)
+        n = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+        n /= np.linalg.norm(n, axis=1, keepdims=True)
+        sd = np.einsum("ij,ij->i", n, cs - v[f[:, 0]])
+        if sd.max() <= 0:
+            want = r - sd.max()
+        else:
+            dist = min(np.linalg.norm(cs - _closest_on_triangle(cs, *v[t])) for t in f)
+            want = r - dist
+        if abs(want) < 1e-6:
+            continue
+        o, _ = scene([cp, cs], [rb, r], [shapes[k]], [0, -1], [q, [1, 0, 0, 0]],
+                     gravity=(0.0, 0.0, 0.0), kn=kn)
+        o.step(1)
+        fo, _ = o.forces()
+        st = o.state()
+        o.close()
+        i = int(np.nonzero(st["pid"] == 1)[0][0])
+        got = np.linalg.norm(fo[i]) / kn
+        checked += 1
+        if want < 0:
+            assert got == 0.0, (trial, want, got)
+        else:
+            touching += 1
+            assert abs(got - want) <= 1e-9 * max(1.0, want) + 1e-12, (trial, want, got)
+    print("sphere-hull: %d checked, %d in contact" % (checked, touching))
+    assert checked > 100 and touching > 40
