@@ -1147,7 +1147,7 @@ static int hull_hull_finish(const satpick* q, dv3 d, const hullr* A, const hullr
 static int tri_e0(int t) { return t == 2 ? 1 : 0; }
 static int tri_e1(int t) { return t == 0 ? 1 : 2; }
 
-static int hull_tri(const hullr* H, const dv3* T, dv3 nt, mhit* h, dv3* nd) {
+static int hull_tri(const hullr* H, const dv3* T, dv3 nt, mhit* h, dv3* nd, int* kind_out) {
   double sP = -1e300;
   int fP = 0;
   for (int f = 0; f < H->nf; ++f) {
@@ -1246,6 +1246,7 @@ static int hull_tri(const hullr* H, const dv3* T, dv3 nt, mhit* h, dv3* nd) {
   const real df = (real)(-s);
   if (!(df > 0)) return 0;
   *nd = n_in;
+  *kind_out = kind;
   h->n = tov(n_in);
   h->delta = df;
   h->ca = tov(cp);
@@ -1532,7 +1533,7 @@ static void mix_poly_step(ens_oracle* o, int p, int* req) {
     const real lim = (real)SH->rb * (real)1.001f + (real)1e-3f;
     mhit hits[MIX_HITS];
     dv3 nds[MIX_HITS];
-    int ids[MIX_HITS], nhit = 0;
+    int ids[MIX_HITS], kinds[MIX_HITS], nhit = 0;
     for (uint32_t q_ = tq0; q_ < tq1; ++q_) {
       const int w = o->use_tri_lists ? (int)o->tri_ids[q_] : S->tri0 + (int)q_;
       const wallc* W = &o->W[w];
@@ -1547,20 +1548,29 @@ static void mix_poly_step(ens_oracle* o, int p, int* req) {
       T[2] = dsub(dof(W->c), o0);
       mhit h;
       dv3 nd;
-      if (!hull_tri(&D, T, d4v(W->n64), &h, &nd)) continue;
+      int kind;
+      if (!hull_tri(&D, T, d4v(W->n64), &h, &nd, &kind)) continue;
       if (nhit < MIX_HITS) {
         hits[nhit] = h;
         nds[nhit] = nd;
         ids[nhit] = w;
+        kinds[nhit] = kind;
         ++nhit;
       } else {
         st |= ST_OVERFLOW;
       }
     }
+    /* face contacts all count, one per plane (the deepest); without one,
+       only the deepest other contact does */
+    int anyface = 0, best = -1;
     for (int q = 0; q < nhit; ++q) {
-      int keep = 1;
-      for (int c2 = 0; c2 < nhit && keep; ++c2) {
-        if (c2 == q || !(ddot(nds[q], nds[c2]) > COPLANAR)) continue;
+      if (kinds[q] == 0) anyface = 1;
+      else if (best < 0 || hits[q].delta > hits[best].delta) best = q;
+    }
+    for (int q = 0; q < nhit; ++q) {
+      int keep = anyface ? kinds[q] == 0 : q == best;
+      for (int c2 = 0; c2 < nhit && keep && anyface; ++c2) {
+        if (c2 == q || kinds[c2] != 0 || !(ddot(nds[q], nds[c2]) > COPLANAR)) continue;
         const real da = hits[q].delta, dc = hits[c2].delta;
         if (dc > da || (dc == da && ids[c2] < ids[q])) keep = 0;
       }

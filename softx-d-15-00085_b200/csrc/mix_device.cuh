@@ -382,7 +382,7 @@ __device__ __forceinline__ bool hull_tri_finish(const double4* V, const double4*
                                                 const uchar4* E, int nv, const double3* T,
                                                 double3 nt, double sT, bool tplus, double sP,
                                                 int fP, double sE, int eE, bool eplus, MixHit& h,
-                                                double3& nd) {
+                                                double3& nd, int& kind_out) {
   SatPick q;
   q.sA = sT;   // the wall's face plays the reference face
   q.sB = sP;
@@ -427,6 +427,7 @@ __device__ __forceinline__ bool hull_tri_finish(const double4* V, const double4*
   const float df = (float)(-s);
   if (!(df > 0.0f)) return false;
   nd = n_in;
+  kind_out = kind;
   h.n = to_f3(n_in);
   h.delta = df;
   h.ca = to_f3(cp);
@@ -488,12 +489,13 @@ __device__ __forceinline__ double tri_edge_sep(const double4* V, const uchar4* E
 // The triangle T (vertices relative to the polyhedron's centre, unit normal
 // nt) as a flat hull against the polyhedron (V, F, E; its faces' normals
 // outward).  a = the polyhedron: n from the triangle to it, ca relative to
-// its centre.  Returns the kind of axis through `kind` (0 a face of the
-// polyhedron, 1 a face of the triangle, 2 an edge pair) and the unrounded
-// normal through `nd`, for the merging of coplanar contacts.
+// its centre.  Returns the kind of axis through `kind` (0 the triangle's
+// face, 1 a face of the polyhedron, 2 an edge pair) and the unrounded
+// normal through `nd`, for the choice among a polyhedron's triangle
+// contacts.
 __device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, const uchar4* E,
                                          int nv, int nf, int ne, const double3* T, double3 nt,
-                                         MixHit& h, double3& nd) {
+                                         MixHit& h, double3& nd, int& kind) {
   double sP = -1e300;
   int fP = 0;
   for (int f = 0; f < nf; ++f) {
@@ -520,7 +522,7 @@ __device__ __forceinline__ bool hull_tri(const double4* V, const double4* F, con
     if (s > 0.0) return false;
     if (s > sE) { sE = s; eE = x; eplus = pl; }
   }
-  return hull_tri_finish(V, F, E, nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd);
+  return hull_tri_finish(V, F, E, nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd, kind);
 }
 
 // ----------------------------------------------------- polyhedron - plane

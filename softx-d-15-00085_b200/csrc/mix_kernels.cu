@@ -297,7 +297,7 @@ __device__ __forceinline__ double warp_max(double v) {
 // the lanes; the maxima taken with the lowest index on ties, which is the
 // serial loop's answer; the contact from the same hull_tri_finish.
 __device__ bool hull_tri_warp(int lane, const HullRef& D, const double3* T, double3 nt, MixHit& h,
-                              double3& nd) {
+                              double3& nd, int& kind) {
   double sP = -1e300;
   int fP = INT_MAX;
   for (int f = lane; f < D.nf; f += 32) {
@@ -335,7 +335,8 @@ __device__ bool hull_tri_warp(int lane, const HullRef& D, const double3* T, doub
   } else {
     tri_edge_sep(D.V, D.E, D.nv, T, eE, eplus);
   }
-  return hull_tri_finish(D.V, D.F, D.E, D.nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd);
+  return hull_tri_finish(D.V, D.F, D.E, D.nv, T, nt, sT, tplus, sP, fP, sE, eE, eplus, h, nd,
+                         kind);
 }
 
 struct MixSmem {
@@ -346,6 +347,7 @@ struct MixSmem {
   double3 nd[kMixHits];     // touching triangles: unrounded normal, contact, id
   MixHit hit[kMixHits];
   int hid[kMixHits];
+  int hkind[kMixHits];      // 0: the triangle's face; 1, 2: a face of the polyhedron, an edge pair
   float4 oh[kMixWallSlots]; // the polyhedron's wall histories before the step
 };
 
@@ -563,11 +565,13 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
             T[2] = dsub(d3(W.c), o);
             MixHit h;
             double3 nd;
-            if (!hull_tri_warp(lane, D, T, W.n64, h, nd)) continue;
+            int kind;
+            if (!hull_tri_warp(lane, D, T, W.n64, h, nd, kind)) continue;
             if (lane == 0 && nhit < kMixHits) {
               sm.hit[nhit] = h;
               sm.nd[nhit] = nd;
               sm.hid[nhit] = tid;
+              sm.hkind[nhit] = kind;
             }
             ++nhit;
           }
@@ -626,10 +630,20 @@ k_mix_poly_step(EnsGeom g, EnsBufs b, MixBufs m, StateBuf in_plain, StateBuf in_
       if (W.kind == kWallPlane && hull_plane(W.a, W.r, xa, A.V, A.nv, h))
         wall(w, h, rot && W.turning);
     }
+    // contacts with a triangle's face all count, those of one plane once
+    // (the deepest); without one, only the deepest other contact does (a
+    // polyhedron over the shared edge of two triangles of a flat or concave
+    // region touches it once)
+    bool anyface = false;
+    int best = -1;
     for (int a = 0; a < nhit; ++a) {
-      bool keep = true;
-      for (int c2 = 0; c2 < nhit && keep; ++c2) {
-        if (c2 == a || !(ddot(sm.nd[a], sm.nd[c2]) > kMixCoplanar)) continue;
+      if (sm.hkind[a] == 0) anyface = true;
+      else if (best < 0 || sm.hit[a].delta > sm.hit[best].delta) best = a;
+    }
+    for (int a = 0; a < nhit; ++a) {
+      bool keep = anyface ? sm.hkind[a] == 0 : a == best;
+      for (int c2 = 0; c2 < nhit && keep && anyface; ++c2) {
+        if (c2 == a || sm.hkind[c2] != 0 || !(ddot(sm.nd[a], sm.nd[c2]) > kMixCoplanar)) continue;
         const float da = sm.hit[a].delta, dc = sm.hit[c2].delta;
         if (dc > da || (dc == da && sm.hid[c2] < sm.hid[a])) keep = false;
       }

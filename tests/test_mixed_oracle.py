@@ -471,3 +471,43 @@ def test_sphere_hull_against_closest_point():
             assert abs(got - want) <= 1e-9 * max(1.0, want) + 1e-12, (trial, want, got)
     print("sphere-hull: %d checked, %d in contact" % (checked, touching))
     assert checked > 100 and touching > 40
+
+
+def test_rock_on_triangles_counts_one_plane_once():
+    """A rock pressed into a floor made of triangles: the overlap is the
+    deepest vertex below the floor, along the floor's normal; a floor of two
+    coplanar triangles whose shared diagonal runs under the rock gives the
+    same force as one large triangle (coplanar contacts count once)."""
+    rng = np.random.default_rng(13)
+    shapes = synth.rock_shapes(6, seed=13)
+    kn = 1e5
+    z0 = 5.0
+    one = [((0.0, 0.0, z0), (40.0, 0.0, z0), (0.0, 40.0, z0))]
+    two = [((0.0, 0.0, z0), (20.0, 0.0, z0), (20.0, 20.0, z0)),
+           ((0.0, 0.0, z0), (20.0, 20.0, z0), (0.0, 20.0, z0))]
+    checked = 0
+    for trial in range(40):
+        k = int(rng.integers(6))
+        q = synth.random_quaternions(rng, 1)[0]
+        rb = synth._bounding_radius(shapes[k])
+        c = np.array([10.0, 10.0, 0.0])
+        v, _ = _world(shapes[k], q, np.zeros(3))
+        c[2] = z0 - v[:, 2].min() - rng.uniform(1e-4, 5e-3)   # deepest vertex below the floor
+        want = z0 - (c[2] + v[:, 2].min())
+        forces = []
+        for tris in (one, two):
+            s = synth.box_system(1, 20.0, 20.0, 2.0 * rb + 0.05, 0, density=7.8e-3, kn=kn,
+                                 gravity=(0.0, 0.0, 0.0))
+            s.nwalls, s.tri0, s.ntris = 0, 0, len(tris)
+            o = EnsRestated([s], [E.triangle(*t) for t in tris], E.LAW_LINEAR, 1e-5, 0.04, 32,
+                            precision="f64")
+            o.set_state(c[None, :], np.array([rb]))
+            o.set_polyhedra([shapes[k]], np.array([0], np.int32), np.asarray(q)[None, :])
+            o.step(1)
+            f, _ = o.forces()
+            o.close()
+            forces.append(f[0])
+        np.testing.assert_allclose(forces[0], [0.0, 0.0, kn * want], rtol=1e-9, atol=1e-12)
+        np.testing.assert_array_equal(forces[0], forces[1])
+        checked += 1
+    assert checked == 40
