@@ -160,8 +160,10 @@ int blaze_ens_profile(blaze_ens* e, float* ms4, int* steps);
  *               test (face normals of both hulls, cross products of the edge
  *               pairs that form a face of the Minkowski difference), a face
  *               preferred unless an edge pair is clearly shallower,
- *   triangles   the same test with the triangle as a flat hull (coplanar
- *               triangles touched together count once, the deepest),
+ *   triangles   the same test with the triangle as a flat hull; contacts
+ *               along a triangle's face normal all count, coplanar ones
+ *               once (the deepest), and without one only the deepest
+ *               other contact counts,
  *   planes      at its deepest vertex,
  * all formed in FP64 from the FP32 state; the contact point is the mean of
  * the penetrating vertices weighted by their depths, or the midpoint of two
