@@ -468,13 +468,27 @@ k_step(const SimParams* __restrict__ Pg, const WallOp* __restrict__ ops, WallGri
       if (k0 + u < cnt && touches(pa - xyz(pb[u]), ra + pb[u].w)) cm |= 1u << (k0 + u);
     }
   }
-  while (cm) {
-    const int k = __ffs(cm) - 1;
+  // the contacts in slot order, the next contact's gathers issued before
+  // this contact's law
+  float4 pn4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vn4 = pn4, wn4 = pn4;
+  bool more = cm != 0u;
+  if (more) {
+    const int j = (int)li[(size_t)(__ffs(cm) - 1) * nl.stride];
     cm &= cm - 1u;
-    const int j = (int)li[(size_t)k * nl.stride];
-    const float4 pb4 = __ldg(in.pos + j);
-    const float4 vb4 = __ldg(in.vel + j);
-    const float4 wb4 = kSpin ? __ldg(in.angv + j) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    pn4 = __ldg(in.pos + j);
+    vn4 = __ldg(in.vel + j);
+    if (kSpin) wn4 = __ldg(in.angv + j);
+  }
+  while (more) {
+    const float4 pb4 = pn4, vb4 = vn4, wb4 = wn4;
+    more = cm != 0u;
+    if (more) {
+      const int j = (int)li[(size_t)(__ffs(cm) - 1) * nl.stride];
+      cm &= cm - 1u;
+      pn4 = __ldg(in.pos + j);
+      vn4 = __ldg(in.vel + j);
+      if (kSpin) wn4 = __ldg(in.angv + j);
+    }
     const float3 rel = pa - xyz(pb4);
     const float dist = len3(rel);
     const int tb = __float_as_int(vb4.w);

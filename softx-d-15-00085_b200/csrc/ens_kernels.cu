@@ -377,17 +377,53 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
       if (k0 + u < cnt && d2 < sr * sr && sqrtf(d2) > 0.0f) cmask |= 1u << (k0 + u);
     }
   }
-  while (cmask) {
-    const uint32_t k = (uint32_t)(__ffs(cmask) - 1);
+  // the contacts in slot order.  On a turning drum the next contact's slot
+  // and gathers are issued before this contact's law (measured: mill mesh
+  // -6 %, mixed charge -2 % a step); the static silo and the plane-walled
+  // boxes ran faster without (+4 % and +1 % with it: more registers)
+  constexpr bool kPipe = kRot;
+  uint32_t kn = 0u, jn = 0u;
+  float4 pn4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vn4 = pn4, wn4 = pn4;
+  bool more = cmask != 0u;
+  if (kPipe && more) {
+    kn = (uint32_t)(__ffs(cmask) - 1);
     cmask &= cmask - 1u;
+    jn = L.idx[(size_t)kn * stride + i];
+    pn4 = ld_state<kNc>(in.pos + jn);
+    vn4 = ld_state<kNc>(in.vel + jn);
+    wn4 = ld_state<kNc>(in.angv + jn);
+  }
+  while (more) {
+    uint32_t k, j;
+    float4 pb4, vb4, wb4;
+    if constexpr (kPipe) {
+      k = kn;
+      j = jn;
+      pb4 = pn4;
+      vb4 = vn4;
+      wb4 = wn4;
+      more = cmask != 0u;
+      if (more) {
+        kn = (uint32_t)(__ffs(cmask) - 1);
+        cmask &= cmask - 1u;
+        jn = L.idx[(size_t)kn * stride + i];
+        pn4 = ld_state<kNc>(in.pos + jn);
+        vn4 = ld_state<kNc>(in.vel + jn);
+        wn4 = ld_state<kNc>(in.angv + jn);
+      }
+    } else {
+      k = (uint32_t)(__ffs(cmask) - 1);
+      cmask &= cmask - 1u;
+      more = cmask != 0u;
+      j = L.idx[(size_t)k * stride + i];
+      pb4 = ld_state<kNc>(in.pos + j);
+    }
     const size_t sk = (size_t)k * stride + i;
-    const uint32_t j = L.idx[sk];
-    const float4 pb4 = ld_state<kNc>(in.pos + j);
     if constexpr (kMix) {
       if (pb4.w < 0.0f) {
         const uint32_t tw = g.mix.twin[sk];
         if (tw == 0xffu) continue;
-        const int q = __float_as_int(ld_state<kNc>(in.angv + j).w);
+        const int q = __float_as_int(kPipe ? wb4.w : ld_state<kNc>(in.angv + j).w);
         const size_t sq = (size_t)tw * (size_t)g.mix.npoly + (size_t)q;
         const float4 F4 = g.mix.sf[sq];
         if (F4.w == 0.0f) continue;
@@ -409,7 +445,10 @@ __device__ __forceinline__ float ens_particle_step(const EnsGeom& g, const EnsBu
     // pass a pair whose FP64-formed overlap is not positive
     const float delta = overlap_pair(ra, rb, pa, xyz(pb4));
     if (!(delta > 0.0f)) continue;
-    const float4 vb4 = ld_state<kNc>(in.vel + j), wb4 = ld_state<kNc>(in.angv + j);
+    if constexpr (!kPipe) {
+      vb4 = ld_state<kNc>(in.vel + j);
+      wb4 = ld_state<kNc>(in.angv + j);
+    }
     const float3 vb = xyz(vb4), wb = xyz(wb4);
     const float mb = sphere_mass(S, rb);
     float3 xi = f3(0.0f, 0.0f, 0.0f);
