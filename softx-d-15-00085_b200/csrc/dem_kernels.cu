@@ -401,7 +401,9 @@ __device__ __forceinline__ DobjHit sphere_dobject(const DobjDev& D, float3 p, fl
 #define BLAZE_STEP_MIN_BLOCKS 4
 #endif
 // candidate slots tested per batch of independent loads in the contact pass
-constexpr int kMaskBatch = 8;
+// (settled 1M silo, contracted law, ms a step: 4 0.123, 5 0.122, 6 0.121,
+// 7 0.120, 8 0.125, 12 0.142, 16 0.161; wider batches spill)
+constexpr int kMaskBatch = 7;
 
 
 // kEnergy: also the energy tallies of the step's contacts, per particle in
